@@ -1,0 +1,199 @@
+/*
+ * sgh_b200.h -- C ABI of libsgh_b200.so, the B200 (sm_100a) time-step engine of
+ * the spectral-Galerkin laser heat solver.
+ *
+ * The reference solver has no native code: its time step is Python driving a
+ * MathBackend plugin (backends/base.py:38-81, registered through
+ * backends/_registry.py:45-110) whose kernel module exposes the functions
+ * listed in physics/spectral_cpu_kernels.py and physics/spectral_gpu_kernels.py.
+ * Each entry point below names the reference interface it replaces.
+ *
+ * Conventions
+ *   - Every function returns an int status: SGH_OK (0) or a negative SGH_ERR_*
+ *     code; sgh_last_error() gives a message. Nothing aborts or traps.
+ *   - Device memory is owned by the caller: the plan reports how many bytes of
+ *     workspace it needs and the caller binds a device buffer of that size.
+ *   - Streams are passed as void* (a cudaStream_t; NULL = legacy default).
+ *   - Arrays are C-ordered [z][y][x] (x contiguous), FP64 unless stated.
+ *   - One plan = one cuboid instance; a plan is used from one host thread.
+ */
+#ifndef SGH_B200_H
+#define SGH_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SGH_ABI_VERSION 1
+
+/* status codes */
+#define SGH_OK               0
+#define SGH_ERR_INVALID     -1   /* bad argument or configuration            */
+#define SGH_ERR_CUDA        -2   /* a CUDA runtime call failed               */
+#define SGH_ERR_STATE       -3   /* plan not bound / called out of order     */
+#define SGH_ERR_UNSUPPORTED -4   /* valid request this build does not handle */
+#define SGH_ERR_WORKSPACE   -5   /* workspace too small or misaligned        */
+
+/* step status (sgh_step_out.status) */
+#define SGH_STEP_CONVERGED   0   /* Picard residual fell below the tolerance */
+#define SGH_STEP_CAPPED      1   /* hit max_picard_iter                      */
+#define SGH_STEP_NONFINITE   2   /* residual became NaN/Inf; loop stopped    */
+
+/* property-expression opcodes (postfix program, see sgh_program) */
+enum {
+  SGH_OP_CONST = 1, SGH_OP_T = 2, SGH_OP_ADD = 3, SGH_OP_SUB = 4, SGH_OP_MUL = 5,
+  SGH_OP_DIV = 6, SGH_OP_POW = 7, SGH_OP_NEG = 8,
+  SGH_OP_SQRT = 16, SGH_OP_EXP = 17, SGH_OP_LOG = 18, SGH_OP_LOG2 = 19, SGH_OP_LOG10 = 20,
+  SGH_OP_SIN = 21, SGH_OP_COS = 22, SGH_OP_TAN = 23, SGH_OP_ASIN = 24, SGH_OP_ACOS = 25,
+  SGH_OP_ATAN = 26, SGH_OP_SINH = 27, SGH_OP_COSH = 28, SGH_OP_TANH = 29,
+  SGH_OP_ASINH = 30, SGH_OP_ACOSH = 31, SGH_OP_ATANH = 32, SGH_OP_FABS = 33,
+  SGH_OP_CEIL = 34, SGH_OP_FLOOR = 35, SGH_OP_TRUNC = 36, SGH_OP_LOG1P = 37,
+  SGH_OP_EXPM1 = 38, SGH_OP_ATAN2 = 48
+};
+#define SGH_MAX_PROGRAM 64
+#define SGH_MAX_CONSTS  32
+#define SGH_MAX_STACK   16
+
+/* One property branch p(T) as a postfix program. SGH_OP_CONST is followed by
+ * the index of its value in consts[]. Replaces the generated CUDA-C of
+ * core/property_expr.py:285-297 (PropertyExpr.to_c_source). */
+typedef struct {
+  int32_t n_ops;
+  int32_t n_consts;
+  int32_t ops[SGH_MAX_PROGRAM];
+  double consts[SGH_MAX_CONSTS];
+} sgh_program;
+
+#define SGH_PRECISION_FP64  0
+
+/* Everything one instance needs; mirrors SimulationContext
+ * (core/parameters.py:482-682) as consumed by SpectralSolver.initialize
+ * (solvers/spectral.py:125-217). */
+typedef struct {
+  int32_t nx, ny, nz;
+  int32_t precision;          /* SGH_PRECISION_FP64                          */
+  double Lx, Ly, Lz;          /* domain size, m                              */
+  double dt;                  /* corrected step, s                           */
+  /* material: reference constants of the propagators (MaterialParams)      */
+  double k, rho, cp;
+  double L_f, T_solidus, T_liquidus;
+  double Pa, R_v, T_boil, dH_LV, T0;
+  double h_top, h_bottom;
+  /* temperature-dependent model (MaterialModel); has_model = model present  */
+  int32_t has_model;          /* model is not None                           */
+  int32_t model_constant;     /* model.is_constant                           */
+  int32_t k_constant;         /* model.k.is_constant (k(T) = solid branch)   */
+  int32_t pad0;
+  sgh_program k_solid, k_liquid, rho_solid, rho_liquid, c_solid, c_liquid;
+  /* beam (LaserParams + LaserProfile)                                      */
+  double r_x, r_y, absorptivity;
+  double order;               /* super-Gaussian order (2 = Gaussian)        */
+  double area_factor;         /* f of I0 = A P / (f r_x r_y)                */
+  int32_t cell_integrated;
+  /* Picard controls (solvers/spectral.py:107-123)                          */
+  int32_t max_iter;
+  double omega, tol;
+} sgh_config;
+
+/* Laser state of one step (LaserState, core/laser.py:150-167). */
+typedef struct {
+  double x, y, power, vx, vy;
+  int32_t is_on;
+  int32_t pad;
+} sgh_laser;
+
+/* Metrics of one step (solvers/spectral.py:536-542), written on the device. */
+typedef struct {
+  double T_surface_max;
+  double P_laser;
+  double picard_rel_err;
+  int32_t n_iter;             /* n_evap_iter                                 */
+  int32_t converged;          /* picard_converged                            */
+  int32_t status;             /* SGH_STEP_*                                  */
+  int32_t pad;
+} sgh_step_out;
+
+/* named workspace buffers (sgh_plan_buffer) */
+enum {
+  SGH_BUF_MODES = 0,      /* (nz,ny,nx) committed modes a                      */
+  SGH_BUF_K = 1,          /* (nz,ny,nx) exp(-alpha lam dt)                     */
+  SGH_BUF_KK = 2,         /* (nz,ny,nx) phi_1 / (rho c)                        */
+  SGH_BUF_T_PREV = 3,     /* (nz,ny,nx) previous converged temperature         */
+  SGH_BUF_Q_EVAP_OLD = 4, /* (ny,nx) previous evaporation flux                 */
+  SGH_BUF_Q_MODES = 5,    /* (nz,ny,nx) latent modes of the last iteration     */
+  SGH_BUF_SURFACE = 6,    /* (ny,nx) top-surface temperature after the step    */
+  SGH_BUF_SCRATCH = 7     /* (nz,ny,nx) general scratch                        */
+};
+
+typedef struct sgh_plan sgh_plan;
+
+int sgh_abi_version(void);
+const char* sgh_last_error(void);
+
+/* Validate a configuration and create a plan (no device memory is allocated).
+ * Replaces SpectralSolverState.__init__ (physics/spectral_state.py:352-365). */
+int sgh_plan_create(const sgh_config* cfg, sgh_plan** out);
+int sgh_plan_destroy(sgh_plan* plan);
+
+/* Bytes of device workspace the plan needs (256-byte aligned base). */
+int sgh_plan_workspace_bytes(const sgh_plan* plan, uint64_t* bytes);
+
+/* Bind caller-owned workspace, build the tables on the device (grid, DCT
+ * matrices, K/KK as precompute_K_KK, physics/spectral_state.py:374-421) and
+ * capture the step graph. Leaves the state at the initial condition.
+ * The stream is synchronised before return. */
+int sgh_plan_bind(sgh_plan* plan, void* workspace, uint64_t bytes, void* stream);
+
+/* Device pointer and size of a named workspace buffer (SGH_BUF_*). */
+int sgh_plan_buffer(const sgh_plan* plan, int32_t which, void** ptr, uint64_t* bytes);
+
+/* Initial condition: a = 0, a[0,0,0] = T0 sqrt(Lx Ly Lz), T_prev = T0, no
+ * evaporation or latent history (solvers/spectral.py:176-202). Async. */
+int sgh_state_reset(sgh_plan* plan, void* stream);
+
+/* One time step: SpectralSolver.step (solvers/spectral.py:219-543). Copies the
+ * host laser state in, replays the step graph (device-resident Picard loop,
+ * no host sync per iteration) and copies the metrics back; returns after the
+ * stream has drained. */
+int sgh_step(sgh_plan* plan, const sgh_laser* laser, sgh_step_out* out, void* stream);
+
+/* n_steps time steps back to back, laser states read from a device table and
+ * metrics written to a device table; asynchronous. */
+int sgh_run(sgh_plan* plan, const sgh_laser* lasers_dev, int32_t n_steps,
+            sgh_step_out* outs_dev, void* stream);
+
+/* Orthonormal 3-D DCT over the plan's (nz,ny,nx) grid, device to device:
+ * kind 2 = DCT_II, kind 3 = IDCT_II (physics/spectral_cpu_kernels.py:374-389).
+ * Uses the plan's scratch buffers; in and out may alias. Async. */
+int sgh_dct3d(sgh_plan* plan, int32_t kind, const double* in, double* out, void* stream);
+
+/* Top (top = 1) or bottom (top = 0) surface temperature of modes (nz,ny,nx)
+ * into out (ny,nx): reconstruct_surface_temperature /
+ * reconstruct_bottom_temperature (physics/spectral_ops.py:210-231). Async. */
+int sgh_surface_temperature(sgh_plan* plan, const double* modes, int32_t top,
+                            double* out, void* stream);
+
+/* modes = sqrt(dV) * DCT_II(field) over the plan's grid: project_volume
+ * (physics/spectral_ops.py:94-102); also SpectralSolver.set_state
+ * (solvers/spectral.py:588-619). Async. */
+int sgh_project_volume(sgh_plan* plan, const double* field, double* modes, void* stream);
+
+/* field = IDCT_II(modes) / sqrt(dV): reconstruct_volume
+ * (physics/spectral_ops.py:83-91). Async. */
+int sgh_reconstruct_volume(sgh_plan* plan, const double* modes, double* field, void* stream);
+
+/* Plan-free orthonormal DCT over every axis of a C-ordered FP64 array of
+ * ndim = 1..3 dimensions (shape[0] slowest): kind 2 = DCT_II, kind 3 =
+ * IDCT_II (physics/spectral_cpu_kernels.py:374-389, any shape). The caller
+ * passes device scratch of sgh_dctn_workspace_bytes() bytes (256-byte aligned).
+ * in and out may alias. Async. */
+int sgh_dctn_workspace_bytes(int32_t ndim, const int32_t* shape, uint64_t* bytes);
+int sgh_dctn(int32_t kind, int32_t ndim, const int32_t* shape, const double* in, double* out,
+             void* workspace, uint64_t bytes, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SGH_B200_H */

@@ -1,0 +1,128 @@
+"""ctypes binding of ``libsgh_b200.so`` (declared in ``include/sgh_b200.h``).
+
+The library is built in-tree by ``spectral_galerkin_heat_b200.build`` and is
+loaded from this package directory only. There is no fallback: if the library
+is missing or fails to load, :func:`lib` raises ``RuntimeError``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+
+__all__ = ["lib", "LIB_PATH", "SghProgram", "SghConfig", "SghLaser", "SghStepOut", "check",
+           "EXPORTED", "SghError", "BUF", "STEP_STATUS"]
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libsgh_b200.so")
+
+MAX_PROGRAM = 64
+MAX_CONSTS = 32
+
+ERRORS = {-1: "SGH_ERR_INVALID", -2: "SGH_ERR_CUDA", -3: "SGH_ERR_STATE",
+          -4: "SGH_ERR_UNSUPPORTED", -5: "SGH_ERR_WORKSPACE"}
+STEP_STATUS = {0: "converged", 1: "capped", 2: "nonfinite"}
+BUF = {"modes": 0, "K": 1, "KK": 2, "T_prev": 3, "q_evap_old": 4, "Q_modes": 5,
+       "surface": 6, "scratch": 7}
+
+# Every function declared in include/sgh_b200.h (checked by the tests).
+EXPORTED = (
+    "sgh_abi_version", "sgh_last_error", "sgh_plan_create", "sgh_plan_destroy",
+    "sgh_plan_workspace_bytes", "sgh_plan_bind", "sgh_plan_buffer", "sgh_state_reset",
+    "sgh_step", "sgh_run", "sgh_dct3d", "sgh_surface_temperature", "sgh_project_volume",
+    "sgh_reconstruct_volume", "sgh_dctn_workspace_bytes", "sgh_dctn",
+)
+
+
+class SghProgram(C.Structure):
+    _fields_ = [("n_ops", C.c_int32), ("n_consts", C.c_int32),
+                ("ops", C.c_int32 * MAX_PROGRAM), ("consts", C.c_double * MAX_CONSTS)]
+
+
+class SghConfig(C.Structure):
+    _fields_ = [
+        ("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32), ("precision", C.c_int32),
+        ("Lx", C.c_double), ("Ly", C.c_double), ("Lz", C.c_double), ("dt", C.c_double),
+        ("k", C.c_double), ("rho", C.c_double), ("cp", C.c_double),
+        ("L_f", C.c_double), ("T_solidus", C.c_double), ("T_liquidus", C.c_double),
+        ("Pa", C.c_double), ("R_v", C.c_double), ("T_boil", C.c_double), ("dH_LV", C.c_double),
+        ("T0", C.c_double), ("h_top", C.c_double), ("h_bottom", C.c_double),
+        ("has_model", C.c_int32), ("model_constant", C.c_int32), ("k_constant", C.c_int32),
+        ("pad0", C.c_int32),
+        ("k_solid", SghProgram), ("k_liquid", SghProgram), ("rho_solid", SghProgram),
+        ("rho_liquid", SghProgram), ("c_solid", SghProgram), ("c_liquid", SghProgram),
+        ("r_x", C.c_double), ("r_y", C.c_double), ("absorptivity", C.c_double),
+        ("order", C.c_double), ("area_factor", C.c_double),
+        ("cell_integrated", C.c_int32), ("max_iter", C.c_int32),
+        ("omega", C.c_double), ("tol", C.c_double),
+    ]
+
+
+class SghLaser(C.Structure):
+    _fields_ = [("x", C.c_double), ("y", C.c_double), ("power", C.c_double),
+                ("vx", C.c_double), ("vy", C.c_double), ("is_on", C.c_int32), ("pad", C.c_int32)]
+
+
+class SghStepOut(C.Structure):
+    _fields_ = [("T_surface_max", C.c_double), ("P_laser", C.c_double),
+                ("picard_rel_err", C.c_double), ("n_iter", C.c_int32),
+                ("converged", C.c_int32), ("status", C.c_int32), ("pad", C.c_int32)]
+
+
+class SghError(RuntimeError):
+    """A libsgh_b200 call returned a negative status."""
+
+    def __init__(self, fn, code, msg):
+        super().__init__(f"{fn} failed with {ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+_lock = threading.Lock()
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Load (once) and return the library; raises if it is missing."""
+    global _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(
+                f"libsgh_b200.so not found at {LIB_PATH}; build it with "
+                "`python -m spectral_galerkin_heat_b200.build` (the B200 backend has no "
+                "CPU fallback).")
+        L = C.CDLL(LIB_PATH)
+        vp, u64p, i32 = C.c_void_p, C.POINTER(C.c_uint64), C.c_int32
+        sig = {
+            "sgh_abi_version": ([], C.c_int),
+            "sgh_last_error": ([], C.c_char_p),
+            "sgh_plan_create": ([C.POINTER(SghConfig), C.POINTER(vp)], C.c_int),
+            "sgh_plan_destroy": ([vp], C.c_int),
+            "sgh_plan_workspace_bytes": ([vp, u64p], C.c_int),
+            "sgh_plan_bind": ([vp, vp, C.c_uint64, vp], C.c_int),
+            "sgh_plan_buffer": ([vp, i32, C.POINTER(vp), u64p], C.c_int),
+            "sgh_state_reset": ([vp, vp], C.c_int),
+            "sgh_step": ([vp, C.POINTER(SghLaser), C.POINTER(SghStepOut), vp], C.c_int),
+            "sgh_run": ([vp, vp, i32, vp, vp], C.c_int),
+            "sgh_dct3d": ([vp, i32, vp, vp, vp], C.c_int),
+            "sgh_surface_temperature": ([vp, vp, i32, vp, vp], C.c_int),
+            "sgh_project_volume": ([vp, vp, vp, vp], C.c_int),
+            "sgh_reconstruct_volume": ([vp, vp, vp, vp], C.c_int),
+            "sgh_dctn_workspace_bytes": ([i32, C.POINTER(i32), u64p], C.c_int),
+            "sgh_dctn": ([i32, i32, C.POINTER(i32), vp, vp, vp, C.c_uint64, vp], C.c_int),
+        }
+        for name, (args, res) in sig.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = res
+        if L.sgh_abi_version() != 1:
+            raise RuntimeError("libsgh_b200.so ABI version mismatch; rebuild it")
+        _lib = L
+        return L
+
+
+def check(fn_name: str, code: int) -> None:
+    """Raise :class:`SghError` for a negative status."""
+    if code != 0:
+        msg = lib().sgh_last_error()
+        raise SghError(fn_name, code, msg.decode() if msg else "")

@@ -1,0 +1,338 @@
+// sgh_axis.cuh -- one axis of a separable orthonormal DCT as a dense FP64
+// contraction, with a fused per-element epilogue.
+//
+// View the C-ordered field as [A][N][B] with N the transformed axis. One pass
+// computes out[a][k][b] = sum_n Mat[k][n] * in[a][n][b] for all (a, k, b), i.e.
+// the GEMM  C[k, c] = sum_n Mat[k, n] X[n, c]  with c = a*B + b. Mat is the
+// orthonormal DCT-II matrix (forward) or its transpose (DCT-III, inverse), so
+// three passes give scipy.fft.dctn(type=2|3, norm='ortho') over all axes
+// (physics/spectral_cpu_kernels.py:374-389), and two passes the face transform.
+//
+// Tiling: 256 threads, BK = 16 contraction slices staged in shared memory per
+// iteration; each thread owns a 2 x 4 register tile. When B == 1 (the
+// transformed axis is the contiguous one) the 4-wide fast dimension of the
+// thread tile runs along k so that the epilogue stores are coalesced; when
+// B > 1 it runs along c (= b, contiguous).
+//
+// The epilogue functor receives (linear index of the output element in the
+// [A][N][B] layout, value) and may accumulate two partial sums or a max that
+// are reduced per CTA and written to a partials array (deterministic order).
+#pragma once
+#include "sgh_device.cuh"
+
+namespace sgh {
+
+constexpr int AX_THREADS = 256;
+constexpr int AX_BK = 16;
+
+struct Red {
+  double s0 = 0.0, s1 = 0.0, mx = -INFINITY;
+};
+
+template <bool CONTIG, class Epi>
+__global__ void __launch_bounds__(AX_THREADS)
+k_axis(const double* __restrict__ X, const double* __restrict__ Mat, int N, int A, int B, Epi epi) {
+  constexpr int TK = CONTIG ? 64 : 32;   // outputs along the transformed axis per CTA
+  constexpr int TC = CONTIG ? 32 : 64;   // outputs along c per CTA
+  __shared__ double Ms[AX_BK][TK + 1];
+  __shared__ double Xs[AX_BK][TC + 1];
+  __shared__ double red_sh[2 * (AX_THREADS / 32)];
+
+  const int tid = threadIdx.x;
+  const int f = tid & 15;   // fast index
+  const int s = tid >> 4;   // slow index
+  const int ncol = A * B;
+  const int c0 = blockIdx.x * TC;
+  const int k0 = blockIdx.y * TK;
+
+  double acc[2][4];
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+
+  for (int n0 = 0; n0 < N; n0 += AX_BK) {
+    // Mat tile: rows k0..k0+TK-1, columns n0..n0+15 (row-contiguous loads)
+#pragma unroll
+    for (int e = tid; e < TK * AX_BK; e += AX_THREADS) {
+      const int kr = e >> 4, kk = e & 15;
+      const int k = k0 + kr, n = n0 + kk;
+      Ms[kk][kr] = (k < N && n < N) ? __ldg(Mat + (size_t)k * N + n) : 0.0;
+    }
+    // X tile: slices n0..n0+15, columns c0..c0+TC-1
+    if (CONTIG) {
+#pragma unroll
+      for (int e = tid; e < TC * AX_BK; e += AX_THREADS) {
+        const int cr = e >> 4, kk = e & 15;
+        const int c = c0 + cr, n = n0 + kk;
+        Xs[kk][cr] = (c < ncol && n < N) ? X[(size_t)c * N + n] : 0.0;
+      }
+    } else {
+#pragma unroll
+      for (int e = tid; e < TC * AX_BK; e += AX_THREADS) {
+        const int cr = e % TC, kk = e / TC;
+        const int c = c0 + cr, n = n0 + kk;
+        double v = 0.0;
+        if (c < ncol && n < N) {
+          const int a = c / B, b = c - a * B;
+          v = X[((size_t)a * N + n) * B + b];
+        }
+        Xs[kk][cr] = v;
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < AX_BK; ++kk) {
+      if (CONTIG) {
+        double m[4], x[2];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) m[j] = Ms[kk][f + 16 * j];
+#pragma unroll
+        for (int i = 0; i < 2; ++i) x[i] = Xs[kk][2 * s + i];
+#pragma unroll
+        for (int i = 0; i < 2; ++i)
+#pragma unroll
+          for (int j = 0; j < 4; ++j) acc[i][j] = fma(m[j], x[i], acc[i][j]);
+      } else {
+        double m[2], x[4];
+#pragma unroll
+        for (int i = 0; i < 2; ++i) m[i] = Ms[kk][2 * s + i];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) x[j] = Xs[kk][f + 16 * j];
+#pragma unroll
+        for (int i = 0; i < 2; ++i)
+#pragma unroll
+          for (int j = 0; j < 4; ++j) acc[i][j] = fma(m[i], x[j], acc[i][j]);
+      }
+    }
+    __syncthreads();
+  }
+
+  Red r;
+#pragma unroll
+  for (int i = 0; i < 2; ++i) {
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int k = CONTIG ? (k0 + f + 16 * j) : (k0 + 2 * s + i);
+      const int c = CONTIG ? (c0 + 2 * s + i) : (c0 + f + 16 * j);
+      if (k < N && c < ncol) {
+        const int a = c / B, b = c - a * B;
+        const int idx = (a * N + k) * B + b;
+        epi(idx, acc[i][j], r);
+      }
+    }
+  }
+  if (Epi::kReduce) {
+    double p0, p1;
+    if (Epi::kReduce == 1) {
+      p0 = r.s0;
+      p1 = r.s1;
+      block_sum2<AX_THREADS>(p0, p1, red_sh);
+    } else {
+      p0 = r.mx;
+      p1 = r.s0;
+      block_max_sum<AX_THREADS>(p0, p1, red_sh);
+    }
+    if (tid == 0) {
+      const int blk = blockIdx.y * gridDim.x + blockIdx.x;
+      epi.partials[2 * blk] = p0;
+      epi.partials[2 * blk + 1] = p1;
+    }
+  }
+}
+
+// Number of CTAs of one pass (the number of partials a reducing epilogue writes).
+inline int axis_blocks(int N, int A, int B) {
+  if (B == 1) return ((A + 31) / 32) * ((N + 63) / 64);
+  return ((A * B + 63) / 64) * ((N + 31) / 32);
+}
+
+template <class Epi>
+inline void launch_axis(const double* X, const double* Mat, int N, int A, int B, const Epi& epi,
+                        cudaStream_t st) {
+  if (B == 1) {
+    dim3 grid((A + 31) / 32, (N + 63) / 64);
+    k_axis<true, Epi><<<grid, AX_THREADS, 0, st>>>(X, Mat, N, A, B, epi);
+  } else {
+    dim3 grid((A * B + 63) / 64, (N + 31) / 32);
+    k_axis<false, Epi><<<grid, AX_THREADS, 0, st>>>(X, Mat, N, A, B, epi);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// epilogues
+// ---------------------------------------------------------------------------
+
+// out = v * mul (mul = 1 for plain intermediate passes)
+struct EpiStore {
+  static constexpr int kReduce = 0;
+  double* out;
+  double mul;
+  double* partials;
+  __device__ __forceinline__ void operator()(int i, double v, Red&) const { out[i] = v * mul; }
+};
+
+// out = v / div (reconstruct_volume: IDCT_II(a) / sqrt_dV, spectral_ops.py:83-91)
+struct EpiDiv {
+  static constexpr int kReduce = 0;
+  double* out;
+  double div;
+  double* partials;
+  __device__ __forceinline__ void operator()(int i, double v, Red&) const { out[i] = v / div; }
+};
+
+// Grid-mode latent source at the reconstructed field:
+// T = IDCT(a)/sqrt_dV; Q = latent(T, T_prev) (spectral_ops.py:270-289).
+struct EpiLatent {
+  static constexpr int kReduce = 0;
+  const DevParams* P;
+  const double* Tprev;
+  double* Q;
+  double* partials;
+  __device__ __forceinline__ void operator()(int i, double v, Red&) const {
+    const double T = v / P->sqrt_dV;
+    Q[i] = latent_source(*P, T, Tprev[i]);
+  }
+};
+
+// T = IDCT(a_trial)/sqrt_dV and k'(T) for the correction stencil
+// (spectral_ops.py:142-148).
+struct EpiTemperatureKp {
+  static constexpr int kReduce = 0;
+  const DevParams* P;
+  double* T;
+  double* kp;
+  double* partials;
+  __device__ __forceinline__ void operator()(int i, double v, Red&) const {
+    const double t = v / P->sqrt_dV;
+    T[i] = t;
+    kp[i] = k_prime(*P, t);
+  }
+};
+
+// Trial modes after the top-face and latent forcing (solvers/spectral.py:431-443):
+//   Qm = sqrt_dV * DCT(Q); a = aK + KK*Ct[p]*S_top; a += KK*Qm; a += KK*Cb[p]*S_bot
+// With RELAX (no property correction) the relaxation of EpiRelax is applied too.
+template <bool RELAX>
+struct EpiTrial {
+  static constexpr int kReduce = RELAX ? 1 : 0;
+  const DevParams* P;
+  const double* aK;
+  const double* KK;
+  const double* Ct;
+  const double* Cb;
+  const double* S_top;
+  const double* S_bot;   // null when there is no bottom convection
+  double* Qm;
+  double* a_trial;       // written when !RELAX
+  double* a_it;          // read and updated when RELAX
+  double* partials;
+  __device__ __forceinline__ void operator()(int i, double v, Red& r) const {
+    const int S = P->S;
+    const int z = i / S, yx = i - z * S;
+    const double q = v * P->sqrt_dV;
+    Qm[i] = q;
+    const double kk = KK[i];
+    double t = aK[i] + kk * Ct[z] * S_top[yx];
+    t += kk * q;
+    if (S_bot) t += kk * Cb[z] * S_bot[yx];
+    if (RELAX) {
+      const double old = a_it[i];
+      const double res = t - old;
+      a_it[i] = res * P->omega + old;
+      r.s0 = fma(res, res, r.s0);
+      r.s1 = fma(old, old, r.s1);
+    } else {
+      a_trial[i] = t;
+    }
+  }
+};
+
+// Property correction and relaxation (solvers/spectral.py:448-468):
+//   C = sqrt_dV * DCT(f); a_raw = a_trial + KK*C; res = a_raw - a_old;
+//   a = res*omega + a_old; partial sums of res^2 and a_old^2.
+struct EpiRelax {
+  static constexpr int kReduce = 1;
+  const DevParams* P;
+  const double* a_trial;
+  const double* KK;
+  double* a_it;
+  double* partials;
+  __device__ __forceinline__ void operator()(int i, double v, Red& r) const {
+    const double c = v * P->sqrt_dV;
+    const double raw = a_trial[i] + KK[i] * c;
+    const double old = a_it[i];
+    const double res = raw - old;
+    a_it[i] = res * P->omega + old;
+    r.s0 = fma(res, res, r.s0);
+    r.s1 = fma(old, old, r.s1);
+  }
+};
+
+// Face: T_s = recon_scale * IDCT2(A) then evaporation, convection and the
+// optional k_bar/k(T_s) rescale of the net top flux (solvers/spectral.py:388-407).
+struct EpiTopFlux {
+  static constexpr int kReduce = 0;
+  const DevParams* P;
+  const double* q_las;
+  double* q_evap;
+  double* q_net;
+  int rescale;
+  double* partials;
+  __device__ __forceinline__ void operator()(int i, double v, Red&) const {
+    const double Ts = P->recon_scale * v;
+    const double qe = evaporation(*P, Ts);
+    q_evap[i] = qe;
+    const double qc = P->has_top_conv ? P->h_top * (Ts - P->T0) : 0.0;
+    double q = q_las[i] - qe - qc;
+    if (rescale) q = q * (P->kbar / k_blended(*P, Ts));
+    q_net[i] = q;
+  }
+};
+
+// Face: convective flux q = -h (T - T0) from a reconstructed face temperature,
+// optionally rescaled by k_bar/k(T) (solvers/spectral.py:335-379).
+struct EpiConvFace {
+  static constexpr int kReduce = 0;
+  const DevParams* P;
+  double h;
+  int rescale;
+  double* q;
+  double* partials;
+  __device__ __forceinline__ void operator()(int i, double v, Red&) const {
+    const double T = P->recon_scale * v;
+    double qc = -h * (T - P->T0);
+    if (rescale) qc = qc * (P->kbar / k_blended(*P, T));
+    q[i] = qc;
+  }
+};
+
+// Face: plain reconstruction T = recon_scale * IDCT2(A) into out.
+struct EpiFaceTemperature {
+  static constexpr int kReduce = 0;
+  const DevParams* P;
+  double* out;
+  double* partials;
+  __device__ __forceinline__ void operator()(int i, double v, Red&) const {
+    out[i] = P->recon_scale * v;
+  }
+};
+
+// Face at commit: T_temp = recon_scale * IDCT2(A) with its max
+// (solvers/spectral.py:502, 537) and the q_evap_old <- q_evap copy (:512).
+struct EpiCommitSurface {
+  static constexpr int kReduce = 2;
+  const DevParams* P;
+  double* T_surf;
+  const double* q_evap;
+  double* q_evap_old;
+  double* partials;
+  __device__ __forceinline__ void operator()(int i, double v, Red& r) const {
+    const double T = P->recon_scale * v;
+    T_surf[i] = T;
+    q_evap_old[i] = q_evap[i];
+    r.mx = fmax(r.mx, T);
+  }
+};
+
+}  // namespace sgh

@@ -1,0 +1,978 @@
+// sgh_b200.cu -- libsgh_b200.so: the spectral-Galerkin heat time step on B200.
+//
+// One plan = one cuboid instance. sgh_plan_bind() builds every table on the
+// device and captures the whole time step -- laser/face forcing, ETD1 update,
+// the Picard fixed-point loop and the commit -- into ONE CUDA graph:
+//
+//   G:  while (step < n_target) {                      <- conditional node
+//         step_begin, face forcing, initial guess, convection guesses
+//         while (Picard not converged and iter < cap) { <- conditional node
+//           surface reconstruction + evaporation / convection face flux
+//           [latent: IDCT3 -> latent source -> DCT3]  (fused epilogues)
+//           [property correction: IDCT3 -> k' -> stencil -> DCT3]
+//           relaxation + residual norms, convergence test on the device
+//         }
+//         commit: surface max, history buffers, metrics
+//       }
+//
+// so a step (or a batch of steps) costs one graph launch and no host
+// synchronisation per Picard iteration, where the reference issues ~20 array
+// operations and one device->host float() per iteration
+// (solvers/spectral.py:386-499).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "sgh_axis.cuh"
+#include "sgh_b200.h"
+#include "sgh_device.cuh"
+
+using namespace sgh;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+#define SGH_CK(call)                                                                      \
+  do {                                                                                    \
+    cudaError_t e_ = (call);                                                              \
+    if (e_ != cudaSuccess)                                                                \
+      return fail(SGH_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));      \
+  } while (0)
+
+constexpr int EW_THREADS = 256;
+
+inline int cdiv(long a, long b) { return (int)((a + b - 1) / b); }
+
+// ---------------------------------------------------------------------------
+// setup kernels
+// ---------------------------------------------------------------------------
+
+// Orthonormal DCT-II matrix C[k][n] = w_k cos(pi k (2n+1) / (2N)) and its
+// transpose. The angle is reduced exactly in integers (period 4N) before cospi.
+__global__ void k_dct_matrix(int N, double* M, double* MT) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= N * N) return;
+  const int k = e / N, n = e - k * N;
+  const long long m = ((long long)k * (2 * n + 1)) % (4LL * N);
+  const double w = (k == 0) ? sqrt(1.0 / N) : sqrt(2.0 / N);
+  const double v = w * cospi((double)m / (double)(2 * N));
+  M[k * N + n] = v;
+  MT[n * N + k] = v;
+}
+
+// Propagators exactly as precompute_K_KK (physics/spectral_state.py:374-421):
+// lam = alpha ((kz^2 + ky^2) + kx^2), K = exp(-lam dt), KK = (K - 1)/(-lam)/(rho c),
+// KK[0,0,0] = dt/(rho c).
+__global__ void k_propagators(const DevParams* __restrict__ P, double alpha, double rho_cp,
+                              double* K, double* KK) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= P->V) return;
+  const int S = P->S, nx = P->nx;
+  const int z = i / S, r = i - z * S, y = r / nx, x = r - y * nx;
+  const double kz = M_PI * (double)z / P->Lz;
+  const double ky = M_PI * (double)y / P->Ly;
+  const double kx = M_PI * (double)x / P->Lx;
+  const double lam = alpha * (kz * kz + ky * ky + kx * kx);
+  const double k = exp(-lam * P->dt);
+  K[i] = k;
+  KK[i] = (i == 0) ? P->dt / rho_cp : ((k - 1.0) / (-lam)) / rho_cp;
+}
+
+// Cell-centred coordinates and the top / bottom z-weights
+// (SpectralGrid, physics/spectral_state.py:98-122; _C_coef spectral_helpers.py:26-46).
+__global__ void k_grid_tables(const DevParams* __restrict__ P, double* xc, double* yc, double* Ct,
+                              double* Cb) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < P->nx) xc[i] = ((double)i + 0.5) * P->dx;
+  if (i < P->ny) yc[i] = ((double)i + 0.5) * P->dy;
+  if (i < P->nz) {
+    const double c = (i == 0) ? sqrt(1.0 / P->Lz) : sqrt(2.0 / P->Lz);
+    Cb[i] = c;
+    Ct[i] = (i & 1) ? -c : c;
+  }
+}
+
+// Initial condition (solvers/spectral.py:176-202).
+__global__ void k_reset(const DevParams* __restrict__ P, Ctrl* ctrl, double* a, double* Tprev,
+                        double* q_evap_old, double* q_evap, double* Qm) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < P->V) {
+    a[i] = (i == 0) ? P->T0 * sqrt(P->Lx * P->Ly * P->Lz) : 0.0;
+    Tprev[i] = P->T0;
+    Qm[i] = 0.0;
+  }
+  if (i < P->S) {
+    q_evap_old[i] = 0.0;
+    q_evap[i] = 0.0;
+  }
+  if (i == 0) {
+    ctrl->have_qprev = 0;
+    ctrl->step = 0;
+    ctrl->n_target = 0;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// step kernels
+// ---------------------------------------------------------------------------
+
+__global__ void k_run_setup(Ctrl* ctrl, sgh_laser laser, const sgh_laser* table, sgh_step_out* outs,
+                            int n) {
+  ctrl->laser = laser;
+  ctrl->table = table;
+  ctrl->out_table = outs;
+  ctrl->n_target = n;
+  ctrl->step = 0;
+}
+
+// Laser state of this step, I0 = A P / (f r_x r_y) (core/laser.py:110-112,
+// solvers/spectral.py:258-268) and the warm-start shift in pixels
+// (spectral_cpu_kernels.py:392-396); opens the Picard loop.
+__global__ void k_step_begin(const DevParams* __restrict__ P, Ctrl* ctrl,
+                             cudaGraphConditionalHandle h_picard) {
+  if (ctrl->table) ctrl->laser = ctrl->table[ctrl->step];
+  const sgh_laser L = ctrl->laser;
+  ctrl->I0 = L.is_on ? P->absorptivity * L.power / (P->area_factor * (P->r_x * P->r_y)) : 0.0;
+  ctrl->shift_x = (L.vx * P->dt) / P->dx;
+  ctrl->shift_y = (L.vy * P->dt) / P->dy;
+  ctrl->iter = 0;
+  ctrl->stop = 0;
+  ctrl->status = SGH_STEP_CAPPED;
+  ctrl->rel_err = nan("");
+  cudaGraphSetConditional(h_picard, P->max_iter > 0 ? 1u : 0u);
+}
+
+// Order-1 shift table entry for output index o (spectral_cpu_kernels.py:305-325).
+struct ShiftTap {
+  int i0, i1;
+  double w0, w1;
+  bool in;
+};
+__device__ __forceinline__ ShiftTap shift_tap(int o, int n, double shift) {
+  const double p = (double)o - shift;
+  const double fl = floor(p);
+  const double t = p - fl;
+  ShiftTap s;
+  s.in = (p >= 0.0) && (p <= (double)(n - 1));
+  long long i0 = (long long)fl;
+  long long i1 = i0 + 1;
+  s.i0 = (int)(i0 < 0 ? 0 : (i0 > n - 1 ? n - 1 : i0));
+  s.i1 = (int)(i1 < 0 ? 0 : (i1 > n - 1 ? n - 1 : i1));
+  s.w1 = t;
+  s.w0 = 1.0 - t;
+  return s;
+}
+
+// Face forcing of the initial guess: q_las, P_laser partials, and
+// q_net = q_las - shift(q_evap_old) (solvers/spectral.py:273-306).
+__global__ void __launch_bounds__(EW_THREADS)
+k_face_begin(const DevParams* __restrict__ P, const Ctrl* __restrict__ ctrl, const double* xc,
+             const double* yc, const double* q_evap_old, double* q_las, double* q_net,
+             double* partials) {
+  __shared__ double sh[2 * (EW_THREADS / 32)];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nx = P->nx, ny = P->ny;
+  double sum = 0.0, dummy = 0.0;
+  if (i < P->S) {
+    const int y = i / nx, x = i - y * nx;
+    const double q = laser_flux(*P, ctrl->I0, ctrl->laser.x, ctrl->laser.y, xc[x], yc[y]);
+    q_las[i] = q;
+    sum = q;
+    const ShiftTap ty = shift_tap(y, ny, ctrl->shift_y);
+    const ShiftTap tx = shift_tap(x, nx, ctrl->shift_x);
+    double v = ty.w0 * (tx.w0 * q_evap_old[ty.i0 * nx + tx.i0] + tx.w1 * q_evap_old[ty.i0 * nx + tx.i1]) +
+               ty.w1 * (tx.w0 * q_evap_old[ty.i1 * nx + tx.i0] + tx.w1 * q_evap_old[ty.i1 * nx + tx.i1]);
+    if (!(ty.in && tx.in)) v = 0.0;
+    q_net[i] = q - v;
+  }
+  block_sum2<EW_THREADS>(sum, dummy, sh);
+  if (threadIdx.x == 0) partials[blockIdx.x] = sum;
+}
+
+// A[y,x] = sum_p w[p] a[p,y,x]  (einsum 'p,pij->ij', spectral_ops.py:210-231)
+__global__ void __launch_bounds__(EW_THREADS)
+k_zsum(const double* __restrict__ a, const double* __restrict__ w, int nz, int S, double* A) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= S) return;
+  double s = 0.0;
+  for (int p = 0; p < nz; ++p) s = fma(w[p], a[(size_t)p * S + i], s);
+  A[i] = s;
+}
+
+// a <- K a; a_temp = aK + KK Ct[p] S_top [+ KK Q_prev]  (solvers/spectral.py:283, 320-334)
+__global__ void __launch_bounds__(EW_THREADS)
+k_init_modes(const DevParams* __restrict__ P, const Ctrl* __restrict__ ctrl, double* a_it,
+             const double* __restrict__ K, const double* __restrict__ KK, const double* __restrict__ Ct,
+             const double* __restrict__ S_top, const double* __restrict__ Qm, double* aK) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= P->V) return;
+  const int S = P->S;
+  const int z = i / S, yx = i - z * S;
+  const double ak = a_it[i] * K[i];
+  aK[i] = ak;
+  const double kk = KK[i];
+  double t = ak + kk * Ct[z] * S_top[yx];
+  if (ctrl->have_qprev) t += kk * Qm[i];
+  a_it[i] = t;
+}
+
+// a += KK w[p] S[y,x]  (add_bottom_surface_source, spectral_cpu_kernels.py:105-113)
+__global__ void __launch_bounds__(EW_THREADS)
+k_add_face(const DevParams* __restrict__ P, double* a, const double* __restrict__ KK,
+           const double* __restrict__ w, const double* __restrict__ Sf) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= P->V) return;
+  const int S = P->S;
+  const int z = i / S, yx = i - z * S;
+  a[i] += KK[i] * w[z] * Sf[yx];
+}
+
+// Trial modes without latent heat (property correction follows).
+__global__ void __launch_bounds__(EW_THREADS)
+k_trial(const DevParams* __restrict__ P, const double* __restrict__ aK, const double* __restrict__ KK,
+        const double* __restrict__ Ct, const double* __restrict__ Cb, const double* __restrict__ S_top,
+        const double* __restrict__ S_bot, double* a_trial) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= P->V) return;
+  const int S = P->S;
+  const int z = i / S, yx = i - z * S;
+  const double kk = KK[i];
+  double t = aK[i] + kk * Ct[z] * S_top[yx];
+  if (S_bot) t += kk * Cb[z] * S_bot[yx];
+  a_trial[i] = t;
+}
+
+// Trial modes and relaxation in one pass when there is neither latent heat nor
+// property correction (solvers/spectral.py:431-468).
+constexpr int RELAX_BLOCKS_MAX = 1184;  // 8 x 148 SMs
+__global__ void __launch_bounds__(EW_THREADS)
+k_trial_relax(const DevParams* __restrict__ P, const double* __restrict__ aK,
+              const double* __restrict__ KK, const double* __restrict__ Ct,
+              const double* __restrict__ Cb, const double* __restrict__ S_top,
+              const double* __restrict__ S_bot, double* a_it, double* partials) {
+  __shared__ double sh[2 * (EW_THREADS / 32)];
+  const int S = P->S, V = P->V;
+  const double om = P->omega;
+  double s0 = 0.0, s1 = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < V; i += gridDim.x * blockDim.x) {
+    const int z = i / S, yx = i - z * S;
+    const double kk = KK[i];
+    double t = aK[i] + kk * Ct[z] * S_top[yx];
+    if (S_bot) t += kk * Cb[z] * S_bot[yx];
+    const double old = a_it[i];
+    const double res = t - old;
+    a_it[i] = res * om + old;
+    s0 = fma(res, res, s0);
+    s1 = fma(old, old, s1);
+  }
+  block_sum2<EW_THREADS>(s0, s1, sh);
+  if (threadIdx.x == 0) {
+    partials[2 * blockIdx.x] = s0;
+    partials[2 * blockIdx.x + 1] = s1;
+  }
+}
+
+// f = div(k' grad T) - a'(T) (T - T_prev)/dt with the numpy.gradient
+// (edge_order=1) stencil applied twice (spectral_cpu_kernels.py:165-252).
+__global__ void __launch_bounds__(EW_THREADS)
+k_stencil(const DevParams* __restrict__ P, const double* __restrict__ T, const double* __restrict__ kp,
+          const double* __restrict__ Tprev, double* f) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= P->V) return;
+  const int nx = P->nx, ny = P->ny, nz = P->nz, S = P->S;
+  const int z = i / S, r = i - z * S, y = r / nx, x = r - y * nx;
+  const double idx = P->inv_dx, idy = P->inv_dy, idz = P->inv_dz;
+
+  // g along one axis at position q (stride st, extent n, base offset b0 of the line)
+  auto g_at = [&](int q, int n, int st, int b0, double inv) -> double {
+    double d;
+    if (q == 0) d = (T[b0 + st] - T[b0]) * inv;
+    else if (q == n - 1) d = (T[b0 + (n - 1) * st] - T[b0 + (n - 2) * st]) * inv;
+    else d = (T[b0 + (q + 1) * st] - T[b0 + (q - 1) * st]) * (0.5 * inv);
+    return kp[b0 + q * st] * d;
+  };
+  auto div_axis = [&](int q, int n, int st, int b0, double inv) -> double {
+    if (q == 0) return (g_at(1, n, st, b0, inv) - g_at(0, n, st, b0, inv)) * inv;
+    if (q == n - 1) return (g_at(n - 1, n, st, b0, inv) - g_at(n - 2, n, st, b0, inv)) * inv;
+    return (g_at(q + 1, n, st, b0, inv) - g_at(q - 1, n, st, b0, inv)) * (0.5 * inv);
+  };
+  const double dgx = div_axis(x, nx, 1, z * S + y * nx, idx);
+  const double dgy = div_axis(y, ny, nx, z * S + x, idy);
+  const double dgz = div_axis(z, nz, S, r, idz);
+  const double t = T[i];
+  const double dTdt = (t - Tprev[i]) * P->inv_dt;
+  f[i] = dgx + dgy + dgz - a_prime(*P, t) * dTdt;
+}
+
+// Convergence test of one Picard iteration (solvers/spectral.py:464-499):
+// err = sqrt(sum res^2 / n) / max(sqrt(sum a_old^2 / n), 1e-9).
+__global__ void __launch_bounds__(EW_THREADS)
+k_converge(const DevParams* __restrict__ P, Ctrl* ctrl, const double* __restrict__ partials,
+           int nparts, cudaGraphConditionalHandle h_picard) {
+  __shared__ double sh[2 * (EW_THREADS / 32)];
+  double s0 = 0.0, s1 = 0.0;
+  for (int b = threadIdx.x; b < nparts; b += EW_THREADS) {
+    s0 += partials[2 * b];
+    s1 += partials[2 * b + 1];
+  }
+  block_sum2<EW_THREADS>(s0, s1, sh);
+  if (threadIdx.x == 0) {
+    const double n = P->n_elements;
+    const double rms_d = sqrt(s0 / n);
+    const double rms_o = sqrt(s1 / n);
+    const double rel = rms_d / fmax(rms_o, 1e-9);
+    const int it = ctrl->iter + 1;
+    ctrl->iter = it;
+    ctrl->rel_err = rel;
+    int stop = 0;
+    if (rel < P->tol) {
+      ctrl->status = SGH_STEP_CONVERGED;
+      stop = 1;
+    } else if (!isfinite(rel)) {
+      ctrl->status = SGH_STEP_NONFINITE;
+      stop = 1;
+    } else if (it >= P->max_iter) {
+      ctrl->status = SGH_STEP_CAPPED;
+      stop = 1;
+    }
+    ctrl->stop = stop;
+    cudaGraphSetConditional(h_picard, stop ? 0u : 1u);
+  }
+}
+
+// Metrics and history of the committed step (solvers/spectral.py:502-542);
+// advances the step counter and decides whether the step loop continues.
+__global__ void __launch_bounds__(EW_THREADS)
+k_commit(const DevParams* __restrict__ P, Ctrl* ctrl, const double* __restrict__ las_parts,
+         int n_las, const double* __restrict__ surf_parts, int n_surf,
+         cudaGraphConditionalHandle h_steps) {
+  __shared__ double sh[2 * (EW_THREADS / 32)];
+  double s = 0.0, d = 0.0;
+  for (int b = threadIdx.x; b < n_las; b += EW_THREADS) s += las_parts[b];
+  block_sum2<EW_THREADS>(s, d, sh);
+  double m = -INFINITY, d2 = 0.0;
+  for (int b = threadIdx.x; b < n_surf; b += EW_THREADS) m = fmax(m, surf_parts[2 * b]);
+  block_max_sum<EW_THREADS>(m, d2, sh);
+  if (threadIdx.x == 0) {
+    sgh_step_out o;
+    o.T_surface_max = m;
+    o.P_laser = s * P->dx * P->dy;
+    o.picard_rel_err = ctrl->rel_err;
+    o.n_iter = ctrl->iter;
+    o.converged = ctrl->status == SGH_STEP_CONVERGED ? 1 : 0;
+    o.status = ctrl->status;
+    o.pad = 0;
+    ctrl->out = o;
+    if (ctrl->out_table) ctrl->out_table[ctrl->step] = o;
+    if (P->grid_latent && P->max_iter > 0) ctrl->have_qprev = 1;
+    const int next = ctrl->step + 1;
+    ctrl->step = next;
+    cudaGraphSetConditional(h_steps, next < ctrl->n_target ? 1u : 0u);
+  }
+}
+
+// Aligned sub-allocation of the caller's workspace.
+struct Layout {
+  size_t off = 0;
+  size_t take(size_t bytes) {
+    const size_t o = off;
+    off += (bytes + 255) & ~size_t(255);
+    return o;
+  }
+};
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// plan
+// ---------------------------------------------------------------------------
+struct sgh_plan {
+  sgh_config cfg;
+  DevParams hp;
+  int nparts_relax = 0, nparts_las = 0, nparts_surf = 0;
+  // offsets into the workspace
+  size_t o_params, o_ctrl, o_mx, o_mxt, o_my, o_myt, o_mz, o_mzt, o_xc, o_yc, o_ct, o_cb;
+  size_t o_K, o_KK, o_a, o_aK, o_trial, o_Tprev, o_Qm, o_t1, o_t2, o_vol, o_kp;
+  size_t o_qlas, o_qnet, o_qev, o_qevold, o_Stop, o_Sbot, o_f1, o_f2, o_Tsurf, o_A;
+  size_t o_prelax, o_plas, o_psurf;
+  size_t ws_need = 0;
+  char* ws = nullptr;
+  bool bound = false;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaStream_t cs1 = nullptr, cs2 = nullptr;
+
+  template <class T>
+  T* at(size_t off) const { return reinterpret_cast<T*>(ws + off); }
+  double* d(size_t off) const { return at<double>(off); }
+  DevParams* P() const { return at<DevParams>(o_params); }
+  Ctrl* ctrl() const { return at<Ctrl>(o_ctrl); }
+};
+
+namespace {
+
+int check_program(const sgh_program& p, const char* name) {
+  if (p.n_ops < 1 || p.n_ops > SGH_MAX_PROGRAM || p.n_consts < 0 || p.n_consts > SGH_MAX_CONSTS)
+    return fail(SGH_ERR_INVALID, std::string("property program ") + name + " has a bad size");
+  int depth = 0;
+  for (int i = 0; i < p.n_ops;) {
+    const int op = p.ops[i++];
+    if (op == SGH_OP_CONST) {
+      if (i >= p.n_ops || p.ops[i] < 0 || p.ops[i] >= p.n_consts)
+        return fail(SGH_ERR_INVALID, std::string("property program ") + name + " has a bad constant");
+      ++i;
+      ++depth;
+    } else if (op == SGH_OP_T) {
+      ++depth;
+    } else if ((op >= SGH_OP_ADD && op <= SGH_OP_POW) || op == SGH_OP_ATAN2) {
+      if (depth < 2) return fail(SGH_ERR_INVALID, std::string("property program ") + name + " underflows");
+      --depth;
+    } else if (op == SGH_OP_NEG || (op >= SGH_OP_SQRT && op <= SGH_OP_EXPM1)) {
+      if (depth < 1) return fail(SGH_ERR_INVALID, std::string("property program ") + name + " underflows");
+    } else {
+      return fail(SGH_ERR_INVALID, std::string("property program ") + name + " has an unknown opcode");
+    }
+    if (depth > SGH_MAX_STACK) return fail(SGH_ERR_INVALID, std::string("property program ") + name + " is too deep");
+  }
+  if (depth != 1) return fail(SGH_ERR_INVALID, std::string("property program ") + name + " leaves a bad stack");
+  return SGH_OK;
+}
+
+// ---- enqueue helpers (used both for graph capture and for direct calls) ----
+
+void face_dct2(sgh_plan* p, const double* in, double* out, double scale, cudaStream_t s) {
+  const DevParams& h = p->hp;
+  launch_axis(in, p->d(p->o_mx), h.nx, h.ny, 1, EpiStore{p->d(p->o_f1), 1.0, nullptr}, s);
+  launch_axis(p->d(p->o_f1), p->d(p->o_my), h.ny, 1, h.nx, EpiStore{out, scale, nullptr}, s);
+}
+
+template <class Epi>
+void face_idct2(sgh_plan* p, const double* modes, const double* w, const Epi& epi, cudaStream_t s) {
+  const DevParams& h = p->hp;
+  k_zsum<<<cdiv(h.S, EW_THREADS), EW_THREADS, 0, s>>>(modes, w, h.nz, h.S, p->d(p->o_A));
+  launch_axis(p->d(p->o_A), p->d(p->o_mxt), h.nx, h.ny, 1, EpiStore{p->d(p->o_f1), 1.0, nullptr}, s);
+  launch_axis(p->d(p->o_f1), p->d(p->o_myt), h.ny, 1, h.nx, epi, s);
+}
+
+// Three passes x -> y -> z through t1, t2; the last pass applies epi.
+template <class Epi>
+void volume_pass3(sgh_plan* p, const double* in, bool inverse, const Epi& epi, double* t1, double* t2,
+                  cudaStream_t s) {
+  const DevParams& h = p->hp;
+  const double* mx = p->d(inverse ? p->o_mxt : p->o_mx);
+  const double* my = p->d(inverse ? p->o_myt : p->o_my);
+  const double* mz = p->d(inverse ? p->o_mzt : p->o_mz);
+  launch_axis(in, mx, h.nx, h.ny * h.nz, 1, EpiStore{t1, 1.0, nullptr}, s);
+  launch_axis(t1, my, h.ny, h.nz, h.nx, EpiStore{t2, 1.0, nullptr}, s);
+  launch_axis(t2, mz, h.nz, 1, h.S, epi, s);
+}
+
+void enqueue_pre(sgh_plan* p, cudaStream_t s, cudaGraphConditionalHandle h_picard) {
+  const DevParams& h = p->hp;
+  DevParams* P = p->P();
+  Ctrl* C = p->ctrl();
+  const int gV = cdiv(h.V, EW_THREADS), gS = cdiv(h.S, EW_THREADS);
+  k_step_begin<<<1, 1, 0, s>>>(P, C, h_picard);
+  k_face_begin<<<gS, EW_THREADS, 0, s>>>(P, C, p->d(p->o_xc), p->d(p->o_yc), p->d(p->o_qevold),
+                                          p->d(p->o_qlas), p->d(p->o_qnet), p->d(p->o_plas));
+  face_dct2(p, p->d(p->o_qnet), p->d(p->o_Stop), h.dct_scale, s);
+  k_init_modes<<<gV, EW_THREADS, 0, s>>>(P, C, p->d(p->o_a), p->d(p->o_K), p->d(p->o_KK), p->d(p->o_ct),
+                                          p->d(p->o_Stop), p->d(p->o_Qm), p->d(p->o_aK));
+  if (h.has_top_conv) {
+    face_idct2(p, p->d(p->o_a), p->d(p->o_ct), EpiConvFace{P, h.h_top, 0, p->d(p->o_f2), nullptr}, s);
+    face_dct2(p, p->d(p->o_f2), p->d(p->o_Stop), h.dct_scale, s);
+    k_add_face<<<gV, EW_THREADS, 0, s>>>(P, p->d(p->o_a), p->d(p->o_KK), p->d(p->o_ct), p->d(p->o_Stop));
+  }
+  if (h.has_bottom_conv) {
+    face_idct2(p, p->d(p->o_a), p->d(p->o_cb), EpiConvFace{P, h.h_bottom, 0, p->d(p->o_f2), nullptr}, s);
+    face_dct2(p, p->d(p->o_f2), p->d(p->o_Sbot), h.dct_scale, s);
+    k_add_face<<<gV, EW_THREADS, 0, s>>>(P, p->d(p->o_a), p->d(p->o_KK), p->d(p->o_cb), p->d(p->o_Sbot));
+    // S_bot_raw, held fixed through the Picard loop (solvers/spectral.py:373-379)
+    face_idct2(p, p->d(p->o_a), p->d(p->o_cb),
+               EpiConvFace{P, h.h_bottom, h.prop_corr, p->d(p->o_f2), nullptr}, s);
+    face_dct2(p, p->d(p->o_f2), p->d(p->o_Sbot), h.dct_scale, s);
+  }
+}
+
+void enqueue_picard(sgh_plan* p, cudaStream_t s, cudaGraphConditionalHandle h_picard) {
+  const DevParams& h = p->hp;
+  DevParams* P = p->P();
+  Ctrl* C = p->ctrl();
+  const int gV = cdiv(h.V, EW_THREADS);
+  double* S_bot = h.has_bottom_conv ? p->d(p->o_Sbot) : nullptr;
+  // top face: T_s, evaporation, convection, rescale -> S_top
+  face_idct2(p, p->d(p->o_a), p->d(p->o_ct),
+             EpiTopFlux{P, p->d(p->o_qlas), p->d(p->o_qev), p->d(p->o_qnet), h.prop_corr, nullptr}, s);
+  face_dct2(p, p->d(p->o_qnet), p->d(p->o_Stop), h.dct_scale, s);
+  int nparts = 0;
+  if (h.grid_latent) {
+    volume_pass3(p, p->d(p->o_a), true, EpiLatent{P, p->d(p->o_Tprev), p->d(p->o_vol), nullptr},
+                 p->d(p->o_t1), p->d(p->o_t2), s);
+    if (h.prop_corr) {
+      volume_pass3(p, p->d(p->o_vol), false,
+                   EpiTrial<false>{P, p->d(p->o_aK), p->d(p->o_KK), p->d(p->o_ct), p->d(p->o_cb),
+                                   p->d(p->o_Stop), S_bot, p->d(p->o_Qm), p->d(p->o_trial), nullptr,
+                                   nullptr},
+                   p->d(p->o_t1), p->d(p->o_t2), s);
+    } else {
+      volume_pass3(p, p->d(p->o_vol), false,
+                   EpiTrial<true>{P, p->d(p->o_aK), p->d(p->o_KK), p->d(p->o_ct), p->d(p->o_cb),
+                                  p->d(p->o_Stop), S_bot, p->d(p->o_Qm), nullptr, p->d(p->o_a),
+                                  p->d(p->o_prelax)},
+                   p->d(p->o_t1), p->d(p->o_t2), s);
+      nparts = axis_blocks(h.nz, 1, h.S);
+    }
+  } else if (h.prop_corr) {
+    k_trial<<<gV, EW_THREADS, 0, s>>>(P, p->d(p->o_aK), p->d(p->o_KK), p->d(p->o_ct), p->d(p->o_cb),
+                                       p->d(p->o_Stop), S_bot, p->d(p->o_trial));
+  } else {
+    const int g = p->nparts_relax;
+    k_trial_relax<<<g, EW_THREADS, 0, s>>>(P, p->d(p->o_aK), p->d(p->o_KK), p->d(p->o_ct), p->d(p->o_cb),
+                                            p->d(p->o_Stop), S_bot, p->d(p->o_a), p->d(p->o_prelax));
+    nparts = g;
+  }
+  if (h.prop_corr) {
+    volume_pass3(p, p->d(p->o_trial), true,
+                 EpiTemperatureKp{P, p->d(p->o_vol), p->d(p->o_kp), nullptr}, p->d(p->o_t1),
+                 p->d(p->o_t2), s);
+    k_stencil<<<gV, EW_THREADS, 0, s>>>(P, p->d(p->o_vol), p->d(p->o_kp), p->d(p->o_Tprev), p->d(p->o_t1));
+    volume_pass3(p, p->d(p->o_t1), false,
+                 EpiRelax{P, p->d(p->o_trial), p->d(p->o_KK), p->d(p->o_a), p->d(p->o_prelax)},
+                 p->d(p->o_t2), p->d(p->o_vol), s);
+    nparts = axis_blocks(h.nz, 1, h.S);
+  }
+  k_converge<<<1, EW_THREADS, 0, s>>>(P, C, p->d(p->o_prelax), nparts, h_picard);
+}
+
+void enqueue_post(sgh_plan* p, cudaStream_t s, cudaGraphConditionalHandle h_steps) {
+  const DevParams& h = p->hp;
+  DevParams* P = p->P();
+  face_idct2(p, p->d(p->o_a), p->d(p->o_ct),
+             EpiCommitSurface{P, p->d(p->o_Tsurf), p->d(p->o_qev), p->d(p->o_qevold), p->d(p->o_psurf)}, s);
+  if (h.grid_latent || h.prop_corr)
+    volume_pass3(p, p->d(p->o_a), true, EpiDiv{p->d(p->o_Tprev), h.sqrt_dV, nullptr}, p->d(p->o_t1),
+                 p->d(p->o_t2), s);
+  k_commit<<<1, EW_THREADS, 0, s>>>(P, p->ctrl(), p->d(p->o_plas), p->nparts_las, p->d(p->o_psurf),
+                                     p->nparts_surf, h_steps);
+}
+
+int capture(sgh_plan* p) {
+  cudaGraph_t G;
+  SGH_CK(cudaGraphCreate(&G, 0));
+  p->graph = G;
+  cudaGraphConditionalHandle h_steps;
+  SGH_CK(cudaGraphConditionalHandleCreate(&h_steps, G, 1, cudaGraphCondAssignDefault));
+  cudaGraphNodeParams outer = {};
+  outer.type = cudaGraphNodeTypeConditional;
+  outer.conditional.handle = h_steps;
+  outer.conditional.type = cudaGraphCondTypeWhile;
+  outer.conditional.size = 1;
+  cudaGraphNode_t outer_node;
+  SGH_CK(cudaGraphAddNode(&outer_node, G, nullptr, 0, &outer));
+  cudaGraph_t body = outer.conditional.phGraph_out[0];
+
+  SGH_CK(cudaStreamBeginCaptureToGraph(p->cs1, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+  cudaGraphConditionalHandle h_picard;
+  SGH_CK(cudaGraphConditionalHandleCreate(&h_picard, body, 0, 0));
+  enqueue_pre(p, p->cs1, h_picard);
+  cudaStreamCaptureStatus status;
+  cudaGraph_t cur;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t ndeps = 0;
+  SGH_CK(cudaStreamGetCaptureInfo(p->cs1, &status, nullptr, &cur, &deps, &ndeps));
+  cudaGraphNodeParams inner = {};
+  inner.type = cudaGraphNodeTypeConditional;
+  inner.conditional.handle = h_picard;
+  inner.conditional.type = cudaGraphCondTypeWhile;
+  inner.conditional.size = 1;
+  cudaGraphNode_t inner_node;
+  SGH_CK(cudaGraphAddNode(&inner_node, cur, deps, ndeps, &inner));
+  SGH_CK(cudaStreamUpdateCaptureDependencies(p->cs1, &inner_node, 1, cudaStreamSetCaptureDependencies));
+  cudaGraph_t ibody = inner.conditional.phGraph_out[0];
+  SGH_CK(cudaStreamBeginCaptureToGraph(p->cs2, ibody, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+  enqueue_picard(p, p->cs2, h_picard);
+  SGH_CK(cudaStreamEndCapture(p->cs2, &ibody));
+  enqueue_post(p, p->cs1, h_steps);
+  SGH_CK(cudaStreamEndCapture(p->cs1, &body));
+  SGH_CK(cudaGetLastError());
+  SGH_CK(cudaGraphInstantiate(&p->exec, G, 0));
+  return SGH_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+int sgh_abi_version(void) { return SGH_ABI_VERSION; }
+
+const char* sgh_last_error(void) { return g_last_error.c_str(); }
+
+int sgh_plan_create(const sgh_config* cfg, sgh_plan** out) {
+  if (!cfg || !out) return fail(SGH_ERR_INVALID, "null argument");
+  *out = nullptr;
+  const sgh_config& c = *cfg;
+  if (c.nx < 2 || c.ny < 2 || c.nz < 2) return fail(SGH_ERR_INVALID, "every axis needs at least 2 modes");
+  if (c.nx > 4096 || c.ny > 4096 || c.nz > 4096) return fail(SGH_ERR_INVALID, "an axis exceeds 4096 modes");
+  if ((long long)c.nx * c.ny * c.nz > (1LL << 28)) return fail(SGH_ERR_INVALID, "grid exceeds 2^28 modes");
+  if (c.precision != SGH_PRECISION_FP64) return fail(SGH_ERR_UNSUPPORTED, "only SGH_PRECISION_FP64 is built");
+  if (!(c.Lx > 0 && c.Ly > 0 && c.Lz > 0 && c.dt > 0))
+    return fail(SGH_ERR_INVALID, "domain size and dt must be positive");
+  if (!(c.r_x > 0 && c.r_y > 0 && c.area_factor > 0 && c.order > 0))
+    return fail(SGH_ERR_INVALID, "beam radii, order and area factor must be positive");
+  if (c.max_iter < 0 || c.max_iter > 1000000)
+    return fail(SGH_ERR_INVALID, "max_iter must be in [0, 1e6]");
+  if (c.cell_integrated && c.order != 2.0)
+    return fail(SGH_ERR_INVALID, "cell_integrated flux is only defined for the Gaussian (order 2)");
+  const bool prop_corr = c.has_model && !c.model_constant;
+  const bool latent = c.L_f > 0.0;
+  if (latent && !(c.has_model && !c.model_constant) && !(c.T_liquidus > c.T_solidus))
+    return fail(SGH_ERR_INVALID, "latent heat with constant properties needs T_liquidus > T_solidus");
+  if (c.has_model) {
+    const sgh_program* progs[6] = {&c.k_solid, &c.k_liquid, &c.rho_solid, &c.rho_liquid, &c.c_solid, &c.c_liquid};
+    const char* names[6] = {"k_solid", "k_liquid", "rho_solid", "rho_liquid", "c_solid", "c_liquid"};
+    for (int i = 0; i < 6; ++i) {
+      const int rc = check_program(*progs[i], names[i]);
+      if (rc) return rc;
+    }
+  }
+
+  sgh_plan* p = new sgh_plan();
+  p->cfg = c;
+  DevParams& h = p->hp;
+  std::memset(&h, 0, sizeof(h));
+  h.nx = c.nx; h.ny = c.ny; h.nz = c.nz;
+  h.S = c.nx * c.ny;
+  h.V = h.S * c.nz;
+  h.grid_latent = latent;
+  h.prop_corr = prop_corr;
+  h.latent_model = prop_corr;  // blended-rho source only for a non-constant model
+  h.k_constant = c.k_constant;
+  h.has_top_conv = c.h_top > 0.0;
+  h.has_bottom_conv = c.h_bottom > 0.0;
+  h.cell_integrated = c.cell_integrated;
+  h.max_iter = c.max_iter;
+  h.Lx = c.Lx; h.Ly = c.Ly; h.Lz = c.Lz;
+  h.dx = c.Lx / c.nx; h.dy = c.Ly / c.ny; h.dz = c.Lz / c.nz;
+  h.inv_dx = 1.0 / h.dx; h.inv_dy = 1.0 / h.dy; h.inv_dz = 1.0 / h.dz;
+  h.dt = c.dt;
+  h.inv_dt = 1.0 / c.dt;
+  // SpectralGrid scales (physics/spectral_state.py:112-133)
+  h.dct_scale = (h.dx * h.dy) * std::sqrt((double)(c.nx * c.ny) / (c.Lx * c.Ly));
+  h.recon_scale = std::sqrt((double)(c.nx * c.ny)) / std::sqrt(c.Lx * c.Ly);
+  h.sqrt_dV = std::sqrt(h.dx * h.dy * h.dz);
+  h.n_elements = (double)h.V;
+  h.kbar = c.k;
+  h.abar = c.rho * c.cp;
+  h.T0 = c.T0;
+  h.h_top = c.h_top;
+  h.h_bottom = c.h_bottom;
+  // evaporation constants (physics/spectral_cpu_kernels.py:150-151)
+  h.evap_f1 = 0.82 * c.dH_LV * c.Pa / std::sqrt(2 * M_PI * c.R_v);
+  h.evap_f2 = c.dH_LV / (c.R_v * c.T_boil);
+  h.T_boil = c.T_boil;
+  h.T_liquidus = c.T_liquidus;
+  h.T_solidus = c.T_solidus;
+  h.degenerate_band = !(c.T_liquidus > c.T_solidus);
+  h.band_inv = h.degenerate_band ? 0.0 : 1.0 / (c.T_liquidus - c.T_solidus);
+  h.latent_factor = -c.rho * c.L_f / c.dt;
+  h.L_f = c.L_f;
+  h.r_x = c.r_x; h.r_y = c.r_y;
+  h.absorptivity = c.absorptivity;
+  h.order = c.order;
+  h.area_factor = c.area_factor;
+  h.omega = c.omega;
+  h.tol = c.tol;
+  if (c.has_model) {
+    h.prog[P_K_SOLID] = c.k_solid;
+    h.prog[P_K_LIQUID] = c.k_liquid;
+    h.prog[P_RHO_SOLID] = c.rho_solid;
+    h.prog[P_RHO_LIQUID] = c.rho_liquid;
+    h.prog[P_C_SOLID] = c.c_solid;
+    h.prog[P_C_LIQUID] = c.c_liquid;
+  }
+
+  p->nparts_relax = std::min(RELAX_BLOCKS_MAX, cdiv(h.V, EW_THREADS));
+  p->nparts_las = cdiv(h.S, EW_THREADS);
+  p->nparts_surf = axis_blocks(h.ny, 1, h.nx);
+  const int nparts_axis = axis_blocks(h.nz, 1, h.S);
+
+  Layout L;
+  const size_t V8 = sizeof(double) * (size_t)h.V, S8 = sizeof(double) * (size_t)h.S;
+  p->o_params = L.take(sizeof(DevParams));
+  p->o_ctrl = L.take(sizeof(Ctrl));
+  p->o_mx = L.take(sizeof(double) * c.nx * c.nx);
+  p->o_mxt = L.take(sizeof(double) * c.nx * c.nx);
+  p->o_my = L.take(sizeof(double) * c.ny * c.ny);
+  p->o_myt = L.take(sizeof(double) * c.ny * c.ny);
+  p->o_mz = L.take(sizeof(double) * c.nz * c.nz);
+  p->o_mzt = L.take(sizeof(double) * c.nz * c.nz);
+  p->o_xc = L.take(sizeof(double) * c.nx);
+  p->o_yc = L.take(sizeof(double) * c.ny);
+  p->o_ct = L.take(sizeof(double) * c.nz);
+  p->o_cb = L.take(sizeof(double) * c.nz);
+  p->o_K = L.take(V8);
+  p->o_KK = L.take(V8);
+  p->o_a = L.take(V8);
+  p->o_aK = L.take(V8);
+  p->o_trial = L.take(V8);
+  p->o_Tprev = L.take(V8);
+  p->o_Qm = L.take(V8);
+  p->o_t1 = L.take(V8);
+  p->o_t2 = L.take(V8);
+  p->o_vol = L.take(V8);
+  p->o_kp = L.take(V8);
+  p->o_qlas = L.take(S8);
+  p->o_qnet = L.take(S8);
+  p->o_qev = L.take(S8);
+  p->o_qevold = L.take(S8);
+  p->o_Stop = L.take(S8);
+  p->o_Sbot = L.take(S8);
+  p->o_f1 = L.take(S8);
+  p->o_f2 = L.take(S8);
+  p->o_Tsurf = L.take(S8);
+  p->o_A = L.take(S8);
+  p->o_prelax = L.take(sizeof(double) * 2 * std::max(p->nparts_relax, nparts_axis));
+  p->o_plas = L.take(sizeof(double) * p->nparts_las);
+  p->o_psurf = L.take(sizeof(double) * 2 * p->nparts_surf);
+  p->ws_need = L.off;
+  *out = p;
+  return SGH_OK;
+}
+
+int sgh_plan_destroy(sgh_plan* p) {
+  if (!p) return SGH_OK;
+  if (p->exec) cudaGraphExecDestroy(p->exec);
+  if (p->graph) cudaGraphDestroy(p->graph);
+  if (p->cs1) cudaStreamDestroy(p->cs1);
+  if (p->cs2) cudaStreamDestroy(p->cs2);
+  delete p;
+  return SGH_OK;
+}
+
+int sgh_plan_workspace_bytes(const sgh_plan* p, uint64_t* bytes) {
+  if (!p || !bytes) return fail(SGH_ERR_INVALID, "null argument");
+  *bytes = p->ws_need;
+  return SGH_OK;
+}
+
+int sgh_plan_bind(sgh_plan* p, void* workspace, uint64_t bytes, void* stream) {
+  if (!p || !workspace) return fail(SGH_ERR_INVALID, "null argument");
+  if (p->bound) return fail(SGH_ERR_STATE, "plan is already bound");
+  if (bytes < p->ws_need) return fail(SGH_ERR_WORKSPACE, "workspace is smaller than sgh_plan_workspace_bytes()");
+  if (reinterpret_cast<uintptr_t>(workspace) % 256 != 0)
+    return fail(SGH_ERR_WORKSPACE, "workspace must be 256-byte aligned");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  p->ws = static_cast<char*>(workspace);
+  const DevParams& h = p->hp;
+  SGH_CK(cudaMemcpyAsync(p->P(), &h, sizeof(DevParams), cudaMemcpyHostToDevice, s));
+  SGH_CK(cudaMemsetAsync(p->ctrl(), 0, sizeof(Ctrl), s));
+  struct { int n; size_t m, mt; } mats[3] = {{h.nx, p->o_mx, p->o_mxt}, {h.ny, p->o_my, p->o_myt},
+                                             {h.nz, p->o_mz, p->o_mzt}};
+  for (auto& m : mats)
+    k_dct_matrix<<<cdiv((long)m.n * m.n, EW_THREADS), EW_THREADS, 0, s>>>(m.n, p->d(m.m), p->d(m.mt));
+  const int gmax = cdiv(std::max(std::max(h.nx, h.ny), h.nz), EW_THREADS);
+  k_grid_tables<<<gmax, EW_THREADS, 0, s>>>(p->P(), p->d(p->o_xc), p->d(p->o_yc), p->d(p->o_ct), p->d(p->o_cb));
+  const sgh_config& c = p->cfg;
+  const double alpha = c.k / (c.rho * c.cp);
+  k_propagators<<<cdiv(h.V, EW_THREADS), EW_THREADS, 0, s>>>(p->P(), alpha, c.rho * c.cp, p->d(p->o_K),
+                                                             p->d(p->o_KK));
+  SGH_CK(cudaMemsetAsync(p->ws + p->o_Sbot, 0, sizeof(double) * h.S, s));
+  SGH_CK(cudaGetLastError());
+  SGH_CK(cudaStreamSynchronize(s));
+  SGH_CK(cudaStreamCreateWithFlags(&p->cs1, cudaStreamNonBlocking));
+  SGH_CK(cudaStreamCreateWithFlags(&p->cs2, cudaStreamNonBlocking));
+  const int rc = capture(p);
+  if (rc) return rc;
+  p->bound = true;
+  const int rr = sgh_state_reset(p, stream);
+  if (rr) return rr;
+  SGH_CK(cudaStreamSynchronize(s));
+  return SGH_OK;
+}
+
+int sgh_plan_buffer(const sgh_plan* p, int32_t which, void** ptr, uint64_t* bytes) {
+  if (!p || !ptr) return fail(SGH_ERR_INVALID, "null argument");
+  if (!p->ws) return fail(SGH_ERR_STATE, "plan is not bound");
+  const size_t V8 = sizeof(double) * (size_t)p->hp.V, S8 = sizeof(double) * (size_t)p->hp.S;
+  size_t off, n;
+  switch (which) {
+    case SGH_BUF_MODES: off = p->o_a; n = V8; break;
+    case SGH_BUF_K: off = p->o_K; n = V8; break;
+    case SGH_BUF_KK: off = p->o_KK; n = V8; break;
+    case SGH_BUF_T_PREV: off = p->o_Tprev; n = V8; break;
+    case SGH_BUF_Q_EVAP_OLD: off = p->o_qevold; n = S8; break;
+    case SGH_BUF_Q_MODES: off = p->o_Qm; n = V8; break;
+    case SGH_BUF_SURFACE: off = p->o_Tsurf; n = S8; break;
+    case SGH_BUF_SCRATCH: off = p->o_vol; n = V8; break;
+    default: return fail(SGH_ERR_INVALID, "unknown buffer id");
+  }
+  *ptr = p->ws + off;
+  if (bytes) *bytes = n;
+  return SGH_OK;
+}
+
+int sgh_state_reset(sgh_plan* p, void* stream) {
+  if (!p || !p->bound) return fail(SGH_ERR_STATE, "plan is not bound");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const int n = std::max(p->hp.V, p->hp.S);
+  k_reset<<<cdiv(n, EW_THREADS), EW_THREADS, 0, s>>>(p->P(), p->ctrl(), p->d(p->o_a), p->d(p->o_Tprev),
+                                                     p->d(p->o_qevold), p->d(p->o_qev), p->d(p->o_Qm));
+  SGH_CK(cudaGetLastError());
+  return SGH_OK;
+}
+
+int sgh_step(sgh_plan* p, const sgh_laser* laser, sgh_step_out* out, void* stream) {
+  if (!p || !laser) return fail(SGH_ERR_INVALID, "null argument");
+  if (!p->bound) return fail(SGH_ERR_STATE, "plan is not bound");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  k_run_setup<<<1, 1, 0, s>>>(p->ctrl(), *laser, nullptr, nullptr, 1);
+  SGH_CK(cudaGetLastError());
+  SGH_CK(cudaGraphLaunch(p->exec, s));
+  if (out) SGH_CK(cudaMemcpyAsync(out, &p->ctrl()->out, sizeof(sgh_step_out), cudaMemcpyDeviceToHost, s));
+  SGH_CK(cudaStreamSynchronize(s));
+  return SGH_OK;
+}
+
+int sgh_run(sgh_plan* p, const sgh_laser* lasers_dev, int32_t n_steps, sgh_step_out* outs_dev, void* stream) {
+  if (!p || !lasers_dev) return fail(SGH_ERR_INVALID, "null argument");
+  if (!p->bound) return fail(SGH_ERR_STATE, "plan is not bound");
+  if (n_steps < 0) return fail(SGH_ERR_INVALID, "n_steps must be >= 0");
+  if (n_steps == 0) return SGH_OK;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  sgh_laser dummy = {};
+  k_run_setup<<<1, 1, 0, s>>>(p->ctrl(), dummy, lasers_dev, outs_dev, n_steps);
+  SGH_CK(cudaGetLastError());
+  SGH_CK(cudaGraphLaunch(p->exec, s));
+  return SGH_OK;
+}
+
+int sgh_dct3d(sgh_plan* p, int32_t kind, const double* in, double* out, void* stream) {
+  if (!p || !in || !out) return fail(SGH_ERR_INVALID, "null argument");
+  if (!p->bound) return fail(SGH_ERR_STATE, "plan is not bound");
+  if (kind != 2 && kind != 3) return fail(SGH_ERR_INVALID, "kind must be 2 (DCT_II) or 3 (IDCT_II)");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  volume_pass3(p, in, kind == 3, EpiStore{out, 1.0, nullptr}, p->d(p->o_t1), p->d(p->o_t2), s);
+  SGH_CK(cudaGetLastError());
+  return SGH_OK;
+}
+
+int sgh_surface_temperature(sgh_plan* p, const double* modes, int32_t top, double* out, void* stream) {
+  if (!p || !modes || !out) return fail(SGH_ERR_INVALID, "null argument");
+  if (!p->bound) return fail(SGH_ERR_STATE, "plan is not bound");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  face_idct2(p, modes, p->d(top ? p->o_ct : p->o_cb), EpiFaceTemperature{p->P(), out, nullptr}, s);
+  SGH_CK(cudaGetLastError());
+  return SGH_OK;
+}
+
+int sgh_project_volume(sgh_plan* p, const double* field, double* modes, void* stream) {
+  if (!p || !field || !modes) return fail(SGH_ERR_INVALID, "null argument");
+  if (!p->bound) return fail(SGH_ERR_STATE, "plan is not bound");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  volume_pass3(p, field, false, EpiStore{modes, p->hp.sqrt_dV, nullptr}, p->d(p->o_t1), p->d(p->o_t2), s);
+  SGH_CK(cudaGetLastError());
+  return SGH_OK;
+}
+
+int sgh_reconstruct_volume(sgh_plan* p, const double* modes, double* field, void* stream) {
+  if (!p || !field || !modes) return fail(SGH_ERR_INVALID, "null argument");
+  if (!p->bound) return fail(SGH_ERR_STATE, "plan is not bound");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  volume_pass3(p, modes, true, EpiDiv{field, p->hp.sqrt_dV, nullptr}, p->d(p->o_t1), p->d(p->o_t2), s);
+  SGH_CK(cudaGetLastError());
+  return SGH_OK;
+}
+
+namespace {
+struct DctnLayout {
+  int n[3] = {1, 1, 1};   // (n0, n1, n2), n2 fastest; unused leading axes are 1
+  int ndim = 0;
+  size_t o_mat[3] = {0, 0, 0}, o_t1 = 0, o_t2 = 0, total = 0;
+};
+
+int dctn_layout(int32_t ndim, const int32_t* shape, DctnLayout* L) {
+  if (ndim < 1 || ndim > 3 || !shape) return fail(SGH_ERR_INVALID, "ndim must be 1, 2 or 3");
+  long long vol = 1;
+  for (int i = 0; i < ndim; ++i) {
+    if (shape[i] < 1 || shape[i] > 4096) return fail(SGH_ERR_INVALID, "axis length must be in [1, 4096]");
+    vol *= shape[i];
+  }
+  if (vol > (1LL << 28)) return fail(SGH_ERR_INVALID, "array exceeds 2^28 elements");
+  L->ndim = ndim;
+  for (int i = 0; i < ndim; ++i) L->n[3 - ndim + i] = shape[i];
+  Layout lay;
+  for (int a = 0; a < 3; ++a) L->o_mat[a] = lay.take(sizeof(double) * 2 * L->n[a] * L->n[a]);
+  L->o_t1 = lay.take(sizeof(double) * vol);
+  L->o_t2 = lay.take(sizeof(double) * vol);
+  L->total = lay.off;
+  return SGH_OK;
+}
+}  // namespace
+
+int sgh_dctn_workspace_bytes(int32_t ndim, const int32_t* shape, uint64_t* bytes) {
+  if (!bytes) return fail(SGH_ERR_INVALID, "null argument");
+  DctnLayout L;
+  const int rc = dctn_layout(ndim, shape, &L);
+  if (rc) return rc;
+  *bytes = L.total;
+  return SGH_OK;
+}
+
+int sgh_dctn(int32_t kind, int32_t ndim, const int32_t* shape, const double* in, double* out,
+             void* workspace, uint64_t bytes, void* stream) {
+  if (!in || !out || !workspace) return fail(SGH_ERR_INVALID, "null argument");
+  if (kind != 2 && kind != 3) return fail(SGH_ERR_INVALID, "kind must be 2 (DCT_II) or 3 (IDCT_II)");
+  DctnLayout L;
+  const int rc = dctn_layout(ndim, shape, &L);
+  if (rc) return rc;
+  if (bytes < L.total) return fail(SGH_ERR_WORKSPACE, "workspace is smaller than sgh_dctn_workspace_bytes()");
+  if (reinterpret_cast<uintptr_t>(workspace) % 256 != 0)
+    return fail(SGH_ERR_WORKSPACE, "workspace must be 256-byte aligned");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  char* ws = static_cast<char*>(workspace);
+  const double* mats[3];
+  for (int a = 0; a < 3; ++a) {
+    const int N = L.n[a];
+    double* M = reinterpret_cast<double*>(ws + L.o_mat[a]);
+    k_dct_matrix<<<cdiv((long)N * N, EW_THREADS), EW_THREADS, 0, s>>>(N, M, M + (size_t)N * N);
+    mats[a] = (kind == 2) ? M : M + (size_t)N * N;
+  }
+  double* t1 = reinterpret_cast<double*>(ws + L.o_t1);
+  double* t2 = reinterpret_cast<double*>(ws + L.o_t2);
+  const int n0 = L.n[0], n1 = L.n[1], n2 = L.n[2];
+  // passes over the last ndim axes, fastest first; the final pass writes out
+  const int first = 3 - L.ndim;
+  const double* src = in;
+  double* bufs[2] = {t1, t2};
+  int nb = 0;
+  if (L.ndim == 1 && in == out) {  // a single pass must not read what it writes
+    SGH_CK(cudaMemcpyAsync(t2, in, sizeof(double) * (size_t)n2, cudaMemcpyDeviceToDevice, s));
+    src = t2;
+  }
+  for (int a = 2; a >= first; --a) {
+    double* dst = (a == first) ? out : bufs[nb++ & 1];
+    const int N = L.n[a];
+    const int A = (a == 2) ? n0 * n1 : (a == 1 ? n0 : 1);
+    const int B = (a == 2) ? 1 : (a == 1 ? n2 : n1 * n2);
+    launch_axis(src, mats[a], N, A, B, EpiStore{dst, 1.0, nullptr}, s);
+    src = dst;
+  }
+  SGH_CK(cudaGetLastError());
+  return SGH_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,234 @@
+// sgh_device.cuh -- device-side parameter block and pointwise physics of the
+// time step. Every formula cites the reference routine it restates; all
+// arithmetic is FP64 and follows the reference's operation order.
+#pragma once
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include "sgh_b200.h"
+
+namespace sgh {
+
+// Program slots inside DevParams::prog.
+enum { P_K_SOLID = 0, P_K_LIQUID, P_RHO_SOLID, P_RHO_LIQUID, P_C_SOLID, P_C_LIQUID, P_COUNT };
+
+// Per-instance constants, built on the host from sgh_config and copied into
+// the workspace once at bind time. Kernels read it through a const pointer.
+struct DevParams {
+  int nx, ny, nz, S, V;
+  int grid_latent, prop_corr, latent_model, k_constant;
+  int has_top_conv, has_bottom_conv, cell_integrated, max_iter;
+  int degenerate_band;
+  int pad_i;
+  double Lx, Ly, Lz, dx, dy, dz, inv_dx, inv_dy, inv_dz, dt, inv_dt;
+  double dct_scale, recon_scale, sqrt_dV, n_elements;
+  double kbar, abar, T0, h_top, h_bottom;
+  double evap_f1, evap_f2, T_boil, T_liquidus, T_solidus;
+  double band_inv;          // 1/(T_l - T_s) (multiplication form of the kernels)
+  double latent_factor;     // -rho L / dt (constant-property latent source)
+  double L_f;
+  double r_x, r_y, absorptivity, order, area_factor;
+  double omega, tol;
+  sgh_program prog[P_COUNT];
+};
+
+// Per-step control block (device resident; written by the step kernels).
+struct Ctrl {
+  sgh_laser laser;          // current laser state
+  const sgh_laser* table;   // laser table (sgh_run) or null (sgh_step)
+  sgh_step_out* out_table;  // metrics table (sgh_run) or null
+  int n_target, step;       // steps requested / done in this launch
+  int iter, stop;           // Picard iteration counter / loop-exit flag
+  int have_qprev, status;
+  double I0, shift_x, shift_y;  // peak intensity and warm-start shift (pixels)
+  double rel_err;
+  sgh_step_out out;         // metrics of the last step
+};
+
+// ---------------------------------------------------------------------------
+// property programs (core/property_expr.py grammar; postfix, FP64)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double eval_program(const sgh_program& p, double T) {
+  double st[SGH_MAX_STACK];
+  int sp = 0;
+  const int n = p.n_ops;
+  for (int i = 0; i < n;) {
+    const int op = p.ops[i++];
+    switch (op) {
+      case SGH_OP_CONST: st[sp++] = p.consts[p.ops[i++]]; break;
+      case SGH_OP_T: st[sp++] = T; break;
+      case SGH_OP_ADD: --sp; st[sp - 1] = st[sp - 1] + st[sp]; break;
+      case SGH_OP_SUB: --sp; st[sp - 1] = st[sp - 1] - st[sp]; break;
+      case SGH_OP_MUL: --sp; st[sp - 1] = st[sp - 1] * st[sp]; break;
+      case SGH_OP_DIV: --sp; st[sp - 1] = st[sp - 1] / st[sp]; break;
+      case SGH_OP_POW: --sp; st[sp - 1] = pow(st[sp - 1], st[sp]); break;
+      case SGH_OP_ATAN2: --sp; st[sp - 1] = atan2(st[sp - 1], st[sp]); break;
+      case SGH_OP_NEG: st[sp - 1] = -st[sp - 1]; break;
+      case SGH_OP_SQRT: st[sp - 1] = sqrt(st[sp - 1]); break;
+      case SGH_OP_EXP: st[sp - 1] = exp(st[sp - 1]); break;
+      case SGH_OP_LOG: st[sp - 1] = log(st[sp - 1]); break;
+      case SGH_OP_LOG2: st[sp - 1] = log2(st[sp - 1]); break;
+      case SGH_OP_LOG10: st[sp - 1] = log10(st[sp - 1]); break;
+      case SGH_OP_SIN: st[sp - 1] = sin(st[sp - 1]); break;
+      case SGH_OP_COS: st[sp - 1] = cos(st[sp - 1]); break;
+      case SGH_OP_TAN: st[sp - 1] = tan(st[sp - 1]); break;
+      case SGH_OP_ASIN: st[sp - 1] = asin(st[sp - 1]); break;
+      case SGH_OP_ACOS: st[sp - 1] = acos(st[sp - 1]); break;
+      case SGH_OP_ATAN: st[sp - 1] = atan(st[sp - 1]); break;
+      case SGH_OP_SINH: st[sp - 1] = sinh(st[sp - 1]); break;
+      case SGH_OP_COSH: st[sp - 1] = cosh(st[sp - 1]); break;
+      case SGH_OP_TANH: st[sp - 1] = tanh(st[sp - 1]); break;
+      case SGH_OP_ASINH: st[sp - 1] = asinh(st[sp - 1]); break;
+      case SGH_OP_ACOSH: st[sp - 1] = acosh(st[sp - 1]); break;
+      case SGH_OP_ATANH: st[sp - 1] = atanh(st[sp - 1]); break;
+      case SGH_OP_FABS: st[sp - 1] = fabs(st[sp - 1]); break;
+      case SGH_OP_CEIL: st[sp - 1] = ceil(st[sp - 1]); break;
+      case SGH_OP_FLOOR: st[sp - 1] = floor(st[sp - 1]); break;
+      case SGH_OP_TRUNC: st[sp - 1] = trunc(st[sp - 1]); break;
+      case SGH_OP_LOG1P: st[sp - 1] = log1p(st[sp - 1]); break;
+      case SGH_OP_EXPM1: st[sp - 1] = expm1(st[sp - 1]); break;
+      default: return nan("");
+    }
+  }
+  return sp > 0 ? st[0] : nan("");
+}
+
+// Liquid fraction as the fused kernels compute it: clip((T - T_s) * inv, 0, 1),
+// a step at T_s for a degenerate band (core/properties.py:175-183, 218-229).
+__device__ __forceinline__ double fl_kernel(const DevParams& P, double T) {
+  if (P.degenerate_band) return T >= P.T_solidus ? 1.0 : 0.0;
+  double f = (T - P.T_solidus) * P.band_inv;
+  return f < 0.0 ? 0.0 : (f > 1.0 ? 1.0 : f);
+}
+
+// k(T) as TempProperty.__call__ evaluates it (core/properties.py:96-103,
+// liquid_fraction :61-77 by division).
+__device__ __forceinline__ double k_blended(const DevParams& P, double T) {
+  const double ks = eval_program(P.prog[P_K_SOLID], T);
+  if (P.k_constant) return ks;
+  const double kl = eval_program(P.prog[P_K_LIQUID], T);
+  double fl;
+  if (P.degenerate_band) {
+    fl = T >= P.T_solidus ? 1.0 : 0.0;
+  } else {
+    fl = (T - P.T_solidus) / (P.T_liquidus - P.T_solidus);
+    fl = fl < 0.0 ? 0.0 : (fl > 1.0 ? 1.0 : fl);
+  }
+  return (1.0 - fl) * ks + fl * kl;
+}
+
+// k'(T) = k(T) - kbar of the fused kernel (core/properties.py:185-191).
+__device__ __forceinline__ double k_prime(const DevParams& P, double T) {
+  const double fl = fl_kernel(P, T);
+  const double om = 1.0 - fl;
+  const double kv = om * eval_program(P.prog[P_K_SOLID], T) + fl * eval_program(P.prog[P_K_LIQUID], T);
+  return kv - P.kbar;
+}
+
+// a'(T) = rho(T) c(T) - abar (core/properties.py:188-192).
+__device__ __forceinline__ double a_prime(const DevParams& P, double T) {
+  const double fl = fl_kernel(P, T);
+  const double om = 1.0 - fl;
+  const double rv = om * eval_program(P.prog[P_RHO_SOLID], T) + fl * eval_program(P.prog[P_RHO_LIQUID], T);
+  const double cv = om * eval_program(P.prog[P_C_SOLID], T) + fl * eval_program(P.prog[P_C_LIQUID], T);
+  return rv * cv - P.abar;
+}
+
+// Latent sink Q = -rho(T) L_f (f_l(T) - f_l(T_prev)) / dt: blended-rho form
+// (core/properties.py:212-236) or constant form
+// (physics/spectral_cpu_kernels.py:115-140).
+__device__ __forceinline__ double latent_source(const DevParams& P, double T, double Tp) {
+  if (P.latent_model) {
+    const double flc = fl_kernel(P, T);
+    const double flp = fl_kernel(P, Tp);
+    const double om = 1.0 - flc;
+    const double rho = om * eval_program(P.prog[P_RHO_SOLID], T) + flc * eval_program(P.prog[P_RHO_LIQUID], T);
+    return -rho * P.L_f * (flc - flp) * P.inv_dt;
+  }
+  double fc = (T - P.T_solidus) * P.band_inv;
+  fc = fc < 0.0 ? 0.0 : (fc > 1.0 ? 1.0 : fc);
+  double fp = (Tp - P.T_solidus) * P.band_inv;
+  fp = fp < 0.0 ? 0.0 : (fp > 1.0 ? 1.0 : fp);
+  return P.latent_factor * (fc - fp);
+}
+
+// Evaporation flux (physics/spectral_cpu_kernels.py:144-162).
+__device__ __forceinline__ double evaporation(const DevParams& P, double T) {
+  if (T < P.T_liquidus) return 0.0;
+  const double term = (1.0 / sqrt(T)) * exp(P.evap_f2 * (1.0 - P.T_boil / T));
+  return P.evap_f1 * term;
+}
+
+// Laser flux at cell (x, y) (core/laser.py:42-53 point-sampled super-Gaussian,
+// :65-91 cell-integrated Gaussian).
+__device__ __forceinline__ double laser_flux(const DevParams& P, double I0, double x0, double y0,
+                                             double x, double y) {
+  if (P.cell_integrated) {
+    const double s2 = sqrt(2.0);
+    const double hx = P.dx, hy = P.dy;
+    const double nxm = P.r_x * sqrt(M_PI / 8.0);
+    const double nym = P.r_y * sqrt(M_PI / 8.0);
+    const double ax = (x - x0 - hx / 2.0) * s2 / P.r_x;
+    const double bx = (x - x0 + hx / 2.0) * s2 / P.r_x;
+    const double ay = (y - y0 - hy / 2.0) * s2 / P.r_y;
+    const double by = (y - y0 + hy / 2.0) * s2 / P.r_y;
+    const double mx = nxm * (erf(bx) - erf(ax)) / hx;
+    const double my = nym * (erf(by) - erf(ay)) / hy;
+    return I0 * (my * mx);
+  }
+  const double ux = (x - x0) / P.r_x;
+  const double uy = (y - y0) / P.r_y;
+  const double r2 = ux * ux + uy * uy;
+  const double shape = (P.order == 2.0) ? exp(-2.0 * r2) : exp(-2.0 * pow(r2, P.order / 2.0));
+  return I0 * shape;
+}
+
+// ---------------------------------------------------------------------------
+// block reductions (deterministic: fixed shuffle tree, then warp 0)
+// ---------------------------------------------------------------------------
+template <int NT>
+__device__ __forceinline__ void block_sum2(double& a, double& b, double* sh) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    a += __shfl_down_sync(0xffffffffu, a, o);
+    b += __shfl_down_sync(0xffffffffu, b, o);
+  }
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) { sh[2 * w] = a; sh[2 * w + 1] = b; }
+  __syncthreads();
+  if (w == 0) {
+    a = lane < NT / 32 ? sh[2 * lane] : 0.0;
+    b = lane < NT / 32 ? sh[2 * lane + 1] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      a += __shfl_down_sync(0xffffffffu, a, o);
+      b += __shfl_down_sync(0xffffffffu, b, o);
+    }
+  }
+}
+
+template <int NT>
+__device__ __forceinline__ void block_max_sum(double& m, double& s, double* sh) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
+    s += __shfl_down_sync(0xffffffffu, s, o);
+  }
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) { sh[2 * w] = m; sh[2 * w + 1] = s; }
+  __syncthreads();
+  if (w == 0) {
+    m = lane < NT / 32 ? sh[2 * lane] : -INFINITY;
+    s = lane < NT / 32 ? sh[2 * lane + 1] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
+      s += __shfl_down_sync(0xffffffffu, s, o);
+    }
+  }
+}
+
+}  // namespace sgh

@@ -1,0 +1,138 @@
+"""Laser state, laser paths and beam profiles.
+
+Mirrors the reference's laser API (``core/laser.py``): ``LaserState`` :150-167,
+the ``LaserPath`` ABC :169-217, the super-Gaussian area factor :34-39 and
+``build_laser_profile`` :143-166, so user code written against the reference
+(``get_state(t, dt) -> LaserState``) drives this backend unchanged.
+
+The flux itself is evaluated on the device (``sgh_face_*`` kernels); the host
+side here only resolves the profile and the energy-conserving peak intensity
+``I0 = A*P / (f * r_x * r_y)`` (``core/laser.py:110-112``).
+
+Two synthetic paths used by the benchmark workloads live here as well: a
+constant-velocity straight track and a bidirectional raster.
+"""
+from __future__ import annotations
+
+import math
+from abc import ABC, abstractmethod
+from dataclasses import dataclass
+
+__all__ = [
+    "LaserState", "LaserPath", "LaserProfile", "build_laser_profile",
+    "super_gaussian_area_factor", "StraightTrack", "RasterPath", "FixedLaser",
+]
+
+
+@dataclass
+class LaserState:
+    """Laser snapshot at one time: position (m), power (W), on/off, velocity (m/s)."""
+
+    x: float
+    y: float
+    power: float
+    is_on: bool
+    v: tuple = (0.0, 0.0)
+
+
+class LaserPath(ABC):
+    """Laser trajectory; ``get_state`` is called once per time step."""
+
+    @abstractmethod
+    def get_state(self, time: float, dt: float) -> LaserState:
+        """Return the laser state at ``time`` for a step of length ``dt``."""
+
+
+def super_gaussian_area_factor(order: float) -> float:
+    """``f`` with ``integral exp(-2 rho^n) dA = f r_x r_y``:
+    ``f(n) = pi 2^(1-2/n) Gamma(2/n) / n`` (``f(2) = pi/2``)."""
+    n = float(order)
+    return math.pi * 2.0 ** (1.0 - 2.0 / n) * math.gamma(2.0 / n) / n
+
+
+_PROFILE_ORDERS = {"gaussian": 2.0, "flat_top": 12.0, "super_gaussian": None}
+
+
+@dataclass(frozen=True)
+class LaserProfile:
+    """Beam shape ``exp(-2 rho^order)`` and its normalisation."""
+
+    name: str
+    order: float
+    cell_integrated: bool = False
+
+    @property
+    def area_factor(self) -> float:
+        return super_gaussian_area_factor(self.order)
+
+    def peak_intensity(self, power: float, absorptivity: float, ref_area: float) -> float:
+        """``I0 = A*P / (f * ref_area)``."""
+        return absorptivity * power / (self.area_factor * ref_area)
+
+
+def build_laser_profile(name: str, order: float = 2.0,
+                        cell_integrated: bool = False) -> LaserProfile:
+    """Resolve ``"gaussian"`` / ``"flat_top"`` / ``"super_gaussian"``; ``ValueError`` otherwise."""
+    key = str(name).lower()
+    if key not in _PROFILE_ORDERS:
+        raise ValueError(f"Unknown laser profile: {name!r}. Choose one of: "
+                         f"{', '.join(sorted(_PROFILE_ORDERS))}.")
+    canonical = _PROFILE_ORDERS[key]
+    resolved = float(order) if canonical is None else canonical
+    if cell_integrated and resolved != 2.0:
+        raise ValueError("cell_integrated flux is only defined for the Gaussian "
+                         f"(order 2), got order {resolved}.")
+    return LaserProfile(name=key, order=resolved, cell_integrated=bool(cell_integrated))
+
+
+class FixedLaser(LaserPath):
+    """Stationary beam at ``(x, y)``."""
+
+    def __init__(self, x, y, power, is_on=True):
+        self.x, self.y, self.power, self.is_on = x, y, power, is_on
+
+    def get_state(self, time, dt):
+        return LaserState(x=self.x, y=self.y, power=self.power, is_on=self.is_on)
+
+
+class StraightTrack(LaserPath):
+    """Constant velocity ``(vx, vy)`` from ``(x0, y0)``: position ``x0 + vx*t``."""
+
+    def __init__(self, x0, y0, vx, vy, power, is_on=True):
+        self.x0, self.y0, self.vx, self.vy = x0, y0, vx, vy
+        self.power, self.is_on = power, is_on
+
+    def get_state(self, time, dt):
+        return LaserState(x=self.x0 + self.vx * time, y=self.y0 + self.vy * time,
+                          power=self.power, is_on=self.is_on, v=(self.vx, self.vy))
+
+
+class RasterPath(LaserPath):
+    """Bidirectional raster along x: ``n_lines`` tracks of ``length`` metres,
+    ``hatch`` metres apart in y, scanned at ``speed`` m/s, alternating direction.
+
+    Track ``j`` starts at ``(x0, y0 + j*hatch)`` when ``j`` is even and at
+    ``(x0 + length, y0 + j*hatch)`` when odd. The turn between tracks is
+    instantaneous. After the last track the beam switches off.
+    """
+
+    def __init__(self, x0, y0, length, hatch, n_lines, speed, power):
+        self.x0, self.y0, self.length, self.hatch = x0, y0, length, hatch
+        self.n_lines, self.speed, self.power = int(n_lines), speed, power
+
+    def get_state(self, time, dt):
+        t_line = self.length / self.speed
+        j = int(math.floor(time / t_line)) if time >= 0.0 else 0
+        if j >= self.n_lines:
+            j = self.n_lines - 1
+            s = self.length
+            on = False
+        else:
+            s = (time - j * t_line) * self.speed
+            on = True
+        y = self.y0 + j * self.hatch
+        if j % 2 == 0:
+            x, vx = self.x0 + s, self.speed
+        else:
+            x, vx = self.x0 + self.length - s, -self.speed
+        return LaserState(x=x, y=y, power=self.power if on else 0.0, is_on=on, v=(vx, 0.0))

@@ -1,0 +1,371 @@
+"""``B200SpectralSolver``: the reference's ``HeatSolver`` contract on one B200.
+
+Drop-in for ``SpectralSolver`` (``solvers/spectral.py:38-628``) behind the same
+lifecycle (``solvers/base.py:31-91``):
+
+* ``initialize(context) -> state``; ``RuntimeError`` without a context;
+* ``step(t, dt) -> (state, metrics)`` with the metric keys ``T_surface_max``,
+  ``P_laser``, ``n_evap_iter``, ``picard_converged``, ``picard_rel_err``;
+* ``set_state(T)``; ``RuntimeError`` before ``initialize``;
+* ``finalize()``;
+* Picard controls resolved as constructor argument > config > default
+  (0.1 / 1e-4 / 30) (``solvers/spectral.py:107-123``); a one-time warning when
+  a step hits the iteration cap (``:486-499``) and a one-time warning for the
+  grid-mode T-dependent configuration (``:210-216``).
+
+The whole step runs on the device (``libsgh_b200.so``): the host calls
+``LaserPath.get_state(t, dt)``, hands the laser state to ``sgh_step`` and reads
+back the metrics once per step. ``run()`` advances many steps with the laser
+states precomputed into a device table and no host round trip per step.
+
+PyTorch provides the device buffer (one workspace tensor per instance) and the
+stream; all arithmetic is in the library. There is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import logging
+import math
+from abc import ABC, abstractmethod
+from typing import Any, Optional
+
+import numpy as np
+
+from . import _lib
+from .laser import build_laser_profile
+from .properties import PropertyExpr
+
+logger = logging.getLogger(__name__)
+
+__all__ = ["HeatSolver", "B200SpectralSolver", "B200State", "make_config", "laser_struct"]
+
+
+class HeatSolver(ABC):
+    """Lifecycle of a heat solver: ``initialize`` once, ``step`` repeatedly, ``finalize``."""
+
+    @abstractmethod
+    def initialize(self, context) -> Any:
+        """Allocate and set the initial condition; return the state."""
+
+    @abstractmethod
+    def step(self, t: float, dt: float):
+        """Advance by ``dt``; return ``(state, metrics)``."""
+
+    @abstractmethod
+    def finalize(self) -> None:
+        """Release resources."""
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def _program(source) -> _lib.SghProgram:
+    ops, consts = PropertyExpr(source).program()
+    p = _lib.SghProgram()
+    p.n_ops = len(ops)
+    p.n_consts = len(consts)
+    for i, v in enumerate(ops):
+        p.ops[i] = int(v)
+    if len(consts) > _lib.MAX_CONSTS:
+        raise ValueError(f"property expression {source!r} has more than "
+                         f"{_lib.MAX_CONSTS} constants")
+    for i, v in enumerate(consts):
+        p.consts[i] = float(v)
+    return p
+
+
+def make_config(ctx, omega: float, tol: float, max_iter: int) -> _lib.SghConfig:
+    """Translate a ``SimulationContext`` into the library's ``sgh_config``."""
+    g, mat, lp, num = ctx.geom, ctx.mat, ctx.laser, ctx.num
+    c = _lib.SghConfig()
+    c.nx, c.ny, c.nz = int(num.nx), int(num.ny), int(num.nz)
+    if (c.nx, c.ny, c.nz) != (int(g.n.x), int(g.n.y), int(g.n.z)):
+        raise ValueError("num.(nx, ny, nz) and geom.n disagree")
+    c.precision = 0
+    c.Lx, c.Ly, c.Lz = float(g.size.x), float(g.size.y), float(g.size.z)
+    c.dt = float(num.dt)
+    c.k, c.rho, c.cp = float(mat.k), float(mat.rho), float(mat.Cp)
+    c.L_f = float(getattr(mat, "L_f", 0.0))
+    c.T_solidus, c.T_liquidus = float(mat.T_solidus), float(mat.T_liquidus)
+    c.Pa, c.R_v, c.T_boil = float(mat.Pa), float(mat.R_v), float(mat.T_boil)
+    c.dH_LV, c.T0 = float(mat.DeltaH_LV), float(mat.T0)
+    c.h_top = float(getattr(mat, "h_conv_top", 0.0))
+    c.h_bottom = float(getattr(mat, "h_conv_bottom", 0.0))
+    model = getattr(mat, "model", None)
+    if model is not None:
+        c.has_model = 1
+        c.model_constant = int(bool(model.is_constant))
+        c.k_constant = int(bool(model.k.is_constant))
+        for name, prop in (("k", model.k), ("rho", model.rho), ("c", model.c)):
+            setattr(c, f"{name}_solid", _program(prop.solid.source))
+            setattr(c, f"{name}_liquid", _program(prop.liquid.source))
+    prof = build_laser_profile(getattr(lp, "profile", "gaussian"),
+                               getattr(lp, "super_gaussian_order", 2.0),
+                               cell_integrated=bool(getattr(lp, "cell_integrated", False)))
+    c.r_x, c.r_y = float(lp.r_x), float(lp.r_y)
+    c.absorptivity = float(lp.absorptivity)
+    c.order = float(prof.order)
+    c.area_factor = float(prof.area_factor)
+    c.cell_integrated = int(prof.cell_integrated)
+    c.max_iter = int(max_iter)
+    c.omega, c.tol = float(omega), float(tol)
+    return c
+
+
+def laser_struct(state, dt: float, plan_dt: float) -> _lib.SghLaser:
+    """``LaserState`` -> ``sgh_laser``. The library shifts the warm-start flux by
+    ``v * plan_dt``; a call with another ``dt`` rescales ``v`` to keep ``v * dt``."""
+    L = _lib.SghLaser()
+    L.x, L.y, L.power = float(state.x), float(state.y), float(state.power)
+    vx, vy = state.v
+    if dt != plan_dt:
+        vx, vy = vx * dt / plan_dt, vy * dt / plan_dt
+    L.vx, L.vy = float(vx), float(vy)
+    L.is_on = 1 if state.is_on else 0
+    return L
+
+
+class B200State:
+    """Device-resident state of one instance; arrays are views into the workspace."""
+
+    def __init__(self, plan, workspace, shape, stream, sqrt_dV, dtype=np.float64):
+        self.plan = plan
+        self.workspace = workspace
+        self.shape = shape
+        self.stream = stream
+        self.dtype = dtype
+        self.sqrt_dV = sqrt_dV
+        self.a = self.buffer("modes")
+        self.K = self.buffer("K")
+        self.KK = self.buffer("KK")
+        self.T_prev = self.buffer("T_prev")
+        self.q_evap_old = self.buffer("q_evap_old")
+
+    def buffer(self, name):
+        """torch float64 view of a named workspace buffer."""
+        torch = _torch()
+        ptr = C.c_void_p()
+        nbytes = C.c_uint64()
+        _lib.check("sgh_plan_buffer",
+                   _lib.lib().sgh_plan_buffer(self.plan, _lib.BUF[name], C.byref(ptr), C.byref(nbytes)))
+        off = ptr.value - self.workspace.data_ptr()
+        view = self.workspace[off:off + nbytes.value].view(torch.float64)
+        nz, ny, nx = self.shape
+        return view.view(nz, ny, nx) if view.numel() == nz * ny * nx else view.view(ny, nx)
+
+
+class B200SpectralSolver(HeatSolver):
+    """Spectral-Galerkin heat step on one B200 (FP64, grid mode)."""
+
+    def __init__(self, backend=None, context=None, *, mixing_omega=None,
+                 convergence_tol=None, max_picard_iter=None, device=None):
+        self.backend = backend
+        self.context = context
+        self.state: Optional[B200State] = None
+        self.device = device
+        self._req = (mixing_omega, convergence_tol, max_picard_iter)
+        self._resolve_picard_params(np.float32)
+        self.track_picard_history = False
+        self.picard_history = []
+        self._plan = None
+        self._picard_cap_warned = False
+        self._property_correction = False
+        self._grid_latent = False
+
+    # ---- configuration -------------------------------------------------
+    def _resolve_picard_params(self, dtype) -> None:
+        num = self.context.num if self.context is not None else None
+
+        def pick(explicit, attr, default):
+            if explicit is not None:
+                return explicit
+            if num is not None and getattr(num, attr, None) is not None:
+                return getattr(num, attr)
+            return default
+
+        om, tol, mx = self._req
+        self.mixing_omega = dtype(pick(om, "picard_omega", 0.1))
+        self.convergence_tol = dtype(pick(tol, "picard_tol", 1e-4))
+        self.max_picard_iter = int(pick(mx, "max_picard_iter", 30))
+
+    def initialize(self, context=None) -> B200State:
+        if context is not None:
+            self.context = context
+        if self.context is None:
+            raise RuntimeError("SimulationContext must be provided either at construction "
+                               "or in initialize().")
+        ctx = self.context
+        if getattr(ctx, "fine", None) is not None:
+            raise NotImplementedError("box mode (fine_mesh) is not supported by the b200 "
+                                      "backend; remove the fine_mesh section (grid mode)")
+        torch = _torch()
+        if not torch.cuda.is_available():
+            raise RuntimeError("the b200 backend needs a CUDA device (no CPU fallback)")
+        L = _lib.lib()
+        self.finalize()
+        self._resolve_picard_params(np.float64)
+        cfg = make_config(ctx, float(self.mixing_omega), float(self.convergence_tol),
+                          self.max_picard_iter)
+        plan = C.c_void_p()
+        _lib.check("sgh_plan_create", L.sgh_plan_create(C.byref(cfg), C.byref(plan)))
+        self._plan = plan
+        nbytes = C.c_uint64()
+        _lib.check("sgh_plan_workspace_bytes", L.sgh_plan_workspace_bytes(plan, C.byref(nbytes)))
+        dev = torch.device("cuda", torch.cuda.current_device()) if self.device is None \
+            else torch.device(self.device)
+        ws = torch.empty(int(nbytes.value), dtype=torch.uint8, device=dev)
+        if ws.data_ptr() % 256:
+            raise RuntimeError("workspace allocation is not 256-byte aligned")
+        with torch.cuda.device(dev):
+            stream = torch.cuda.current_stream(dev)
+        _lib.check("sgh_plan_bind",
+                   L.sgh_plan_bind(plan, C.c_void_p(ws.data_ptr()), nbytes.value,
+                                   C.c_void_p(stream.cuda_stream)))
+        g = ctx.geom
+        sqrt_dV = math.sqrt(float(g.d.x * g.d.y * g.d.z))
+        self.state = B200State(plan, ws, (cfg.nz, cfg.ny, cfg.nx), stream, sqrt_dV)
+        self._cfg = cfg
+        model = getattr(ctx.mat, "model", None)
+        self._property_correction = model is not None and not model.is_constant
+        self._grid_latent = float(getattr(ctx.mat, "L_f", 0.0)) > 0.0
+        if self._property_correction and self._grid_latent:
+            logger.warning(
+                "Temperature-dependent run in grid mode (no fine_mesh): the sharp latent-heat "
+                "source is projected on the coarse grid and can ring.")
+        self._picard_cap_warned = False
+        return self.state
+
+    # ---- stepping --------------------------------------------------------
+    def _require(self):
+        if self.state is None or self._plan is None:
+            raise RuntimeError("Solver must be initialized before stepping.")
+
+    def step(self, t: float, dt: float):
+        self._require()
+        st = self.context.laser_path.get_state(t, dt)
+        laser = laser_struct(st, dt, self._cfg.dt)
+        out = _lib.SghStepOut()
+        _lib.check("sgh_step", _lib.lib().sgh_step(self._plan, C.byref(laser), C.byref(out),
+                                                   C.c_void_p(self.state.stream.cuda_stream)))
+        metrics = self._metrics(out, t)
+        if self.track_picard_history:
+            self.picard_history = [{"iter": metrics["n_evap_iter"] - 1, "rms_diff": None,
+                                    "rho": None, "true_rel_err": metrics["picard_rel_err"]}]
+        return self.state, metrics
+
+    def _metrics(self, out, t):
+        conv = bool(out.converged)
+        if not conv and out.n_iter > 0 and not self._picard_cap_warned:
+            self._picard_cap_warned = True
+            logger.warning(
+                "Picard iteration hit max_picard_iter=%d at t=%.6g s without reaching "
+                "picard_tol=%g (last relative residual %.3g, status %s). The returned field "
+                "is not converged. Warned once per run.", self.max_picard_iter, t,
+                float(self.convergence_tol), out.picard_rel_err,
+                _lib.STEP_STATUS.get(out.status, out.status))
+        return {"T_surface_max": float(out.T_surface_max), "P_laser": float(out.P_laser),
+                "n_evap_iter": int(out.n_iter), "picard_converged": conv,
+                "picard_rel_err": float(out.picard_rel_err)}
+
+    def run(self, t0: float, n_steps: int, dt: Optional[float] = None):
+        """Advance ``n_steps`` steps from time ``t0`` in one asynchronous launch.
+
+        Laser states for ``t0 + i*dt`` are evaluated on the host up front and
+        uploaded as a device table; the metrics of every step come back in one
+        copy at the end. Returns the list of per-step metric dicts.
+        """
+        self._require()
+        torch = _torch()
+        dt = self._cfg.dt if dt is None else dt
+        n = int(n_steps)
+        if n <= 0:
+            return []
+        table = self.laser_table(t0, n, dt)
+        outs = torch.empty(n * C.sizeof(_lib.SghStepOut), dtype=torch.uint8,
+                           device=self.state.workspace.device)
+        self.run_table(table, outs, n)
+        host = outs.cpu().numpy()
+        res = []
+        for i in range(n):
+            o = _lib.SghStepOut.from_buffer_copy(host[i * C.sizeof(_lib.SghStepOut):
+                                                      (i + 1) * C.sizeof(_lib.SghStepOut)])
+            res.append(self._metrics(o, t0 + i * dt))
+        return res
+
+    def laser_table(self, t0: float, n: int, dt: Optional[float] = None):
+        """Device table (uint8 tensor) of ``sgh_laser`` for steps ``t0 + i*dt``."""
+        torch = _torch()
+        dt = self._cfg.dt if dt is None else dt
+        arr = (_lib.SghLaser * n)()
+        for i in range(n):
+            arr[i] = laser_struct(self.context.laser_path.get_state(t0 + i * dt, dt), dt,
+                                  self._cfg.dt)
+        host = torch.frombuffer(bytearray(bytes(arr)), dtype=torch.uint8)
+        return host.to(self.state.workspace.device)
+
+    def run_table(self, table, outs, n: int) -> None:
+        """Enqueue ``n`` steps reading laser states from ``table`` (device) and writing
+        ``sgh_step_out`` records into ``outs`` (device); returns without waiting."""
+        _lib.check("sgh_run", _lib.lib().sgh_run(
+            self._plan, C.c_void_p(table.data_ptr()), int(n), C.c_void_p(outs.data_ptr()),
+            C.c_void_p(self.state.stream.cuda_stream)))
+
+    # ---- state access ------------------------------------------------------
+    def set_state(self, temperature_field) -> None:
+        """Modes from a cell-centred field: ``a = sqrt(dV) DCT_II(T)`` (``solvers/spectral.py:588-619``)."""
+        if self.state is None or self._plan is None:
+            raise RuntimeError("Solver must be initialized before calling set_state().")
+        torch = _torch()
+        T = torch.as_tensor(temperature_field, dtype=torch.float64,
+                            device=self.state.workspace.device).contiguous()
+        if tuple(T.shape) != self.state.shape:
+            raise ValueError(f"field shape {tuple(T.shape)} != modes shape {self.state.shape}")
+        _lib.check("sgh_project_volume", _lib.lib().sgh_project_volume(
+            self._plan, C.c_void_p(T.data_ptr()), C.c_void_p(self.state.a.data_ptr()),
+            C.c_void_p(self.state.stream.cuda_stream)))
+        self.state.stream.synchronize()
+
+    def surface_temperature(self, top: bool = True, modes=None):
+        """Top (or bottom) face temperature of ``modes`` (default: the state), (ny, nx)."""
+        self._require()
+        torch = _torch()
+        a = self.state.a if modes is None else modes
+        nz, ny, nx = self.state.shape
+        out = torch.empty((ny, nx), dtype=torch.float64, device=self.state.workspace.device)
+        _lib.check("sgh_surface_temperature", _lib.lib().sgh_surface_temperature(
+            self._plan, C.c_void_p(a.data_ptr()), 1 if top else 0, C.c_void_p(out.data_ptr()),
+            C.c_void_p(self.state.stream.cuda_stream)))
+        return out
+
+    def volume_temperature(self, modes=None):
+        """Cell-centred temperature ``IDCT_II(a)/sqrt(dV)``, (nz, ny, nx)."""
+        self._require()
+        torch = _torch()
+        a = self.state.a if modes is None else modes
+        out = torch.empty(self.state.shape, dtype=torch.float64, device=self.state.workspace.device)
+        _lib.check("sgh_reconstruct_volume", _lib.lib().sgh_reconstruct_volume(
+            self._plan, C.c_void_p(a.data_ptr()), C.c_void_p(out.data_ptr()),
+            C.c_void_p(self.state.stream.cuda_stream)))
+        return out
+
+    def reset(self) -> None:
+        """Back to the initial condition (keeps the plan and its graph)."""
+        self._require()
+        _lib.check("sgh_state_reset", _lib.lib().sgh_state_reset(
+            self._plan, C.c_void_p(self.state.stream.cuda_stream)))
+
+    def finalize(self) -> None:
+        if self._plan is not None:
+            if self.state is not None:
+                self.state.stream.synchronize()
+            _lib.lib().sgh_plan_destroy(self._plan)
+            self._plan = None
+        self.state = None
+
+    def __del__(self):
+        try:
+            self.finalize()
+        except Exception:
+            pass

@@ -1,0 +1,99 @@
+"""Synthetic workloads: configuration dicts and laser paths.
+
+Each function returns a config dict in the reference's YAML schema (plain SI
+scalars) plus the :class:`LaserPath` that drives it. All randomness comes from
+``numpy.random.default_rng(seed)``.
+
+* ``straight_track``: 316L cuboid 2.0 x 1.0 x 0.5 mm, 64 x 32 x 16 modes,
+  constant properties (k = 20, rho = 7900, c_p = 500), T0 = 300 K, Gaussian
+  beam 200 W / 50 um / A = 0.35 on a straight track along x at y = 0.5 mm,
+  1 m/s from x = 0.25 mm; evaporation on the top face only; 300 ETD1 steps of
+  5 us; one forcing pass per step (``max_picard_iter = 1``, ``omega = 1``).
+* ``nonlinear_raster``: same cuboid at 128 x 64 x 32 modes; k(T) = 15 + 20
+  (T - 300)/2700 and c_p(T) = 450 + 350 (T - 300)/2700 on both phase branches
+  (reference constants 25 and 625), rho = 7900; latent heat 2.7e5 J/kg over
+  1658-1723 K (grid mode); evaporation plus top convection h = 10 W/m^2K;
+  Picard to 1e-8 with omega = 0.1 (cap 400); 1000 steps of 2 us; 5-line
+  bidirectional raster, 0.4 mm lines, 100 um hatch, 1 m/s, start jittered by
+  U[-50, 50] um from the seed.
+* ``precision_track``: 256 x 128 x 64 modes on a 4 x 2 x 1 mm cuboid with the
+  straight-track physics; P ~ U[150, 400] W and v ~ U[0.5, 2] m/s from the
+  seed; 500 steps of 5 us from x = 0.5 mm.
+"""
+from __future__ import annotations
+
+import copy
+
+import numpy as np
+
+from .laser import RasterPath, StraightTrack
+
+__all__ = ["MATERIAL_316L", "straight_track", "nonlinear_raster", "precision_track",
+           "scaled"]
+
+MATERIAL_316L = {
+    "name": "316L", "rho": 7900.0, "k": 20.0, "Cp": 500.0, "L_f": 0.0,
+    "T_solidus": 1658.0, "T_liquidus": 1723.0, "T0": 300.0,
+    "DeltaH_LV": 7.416e6, "R_v": 150.774, "Pa": 101325.0, "T_boil": 3090.0,
+}
+
+
+def straight_track(nx=64, ny=32, nz=16, steps=300, dt=5e-6, size=(2e-3, 1e-3, 0.5e-3),
+                   x0=0.25e-3, y0=None, speed=1.0, power=200.0, absorptivity=0.35):
+    """Constant-property straight track; returns ``(cfg, path)``."""
+    cfg = {
+        "simulation": {"backend": "b200", "dtype": "float64", "dt": dt,
+                       "duration": steps * dt, "max_picard_iter": 1, "picard_omega": 1.0},
+        "domain": {"size": list(size), "mesh": [nx, ny, nz]},
+        "material": dict(MATERIAL_316L),
+        "laser": {"radius": 50e-6, "absorptivity": absorptivity, "power_nominal": power},
+    }
+    y = size[1] / 2.0 if y0 is None else y0
+    return cfg, StraightTrack(x0, y, speed, 0.0, power)
+
+
+def nonlinear_raster(nx=128, ny=64, nz=32, steps=1000, dt=2e-6, seed=0,
+                     size=(2e-3, 1e-3, 0.5e-3), line_length=0.4e-3, hatch=100e-6,
+                     n_lines=5, speed=1.0, power=200.0, tol=1e-8, omega=0.1, cap=400):
+    """T-dependent raster with latent heat, evaporation and convection; ``(cfg, path)``."""
+    mat = dict(MATERIAL_316L)
+    mat.update({
+        "k": {"solid": "15 + 20*(T - 300)/2700", "liquid": "15 + 20*(T - 300)/2700",
+              "reference": 25.0},
+        "Cp": {"solid": "450 + 350*(T - 300)/2700", "liquid": "450 + 350*(T - 300)/2700",
+               "reference": 625.0},
+        "rho": 7900.0, "L_f": 2.7e5, "h_conv_top": 10.0,
+    })
+    cfg = {
+        "simulation": {"backend": "b200", "dtype": "float64", "dt": dt,
+                       "duration": steps * dt, "max_picard_iter": cap,
+                       "picard_tol": tol, "picard_omega": omega},
+        "domain": {"size": list(size), "mesh": [nx, ny, nz]},
+        "material": mat,
+        "laser": {"radius": 50e-6, "absorptivity": 0.35, "power_nominal": power},
+    }
+    rng = np.random.default_rng(seed)
+    jx, jy = rng.uniform(-50e-6, 50e-6, size=2)
+    x_start = 0.5 * size[0] - 0.5 * line_length + jx
+    y_start = 0.5 * size[1] - 0.5 * (n_lines - 1) * hatch + jy
+    return cfg, RasterPath(x_start, y_start, line_length, hatch, n_lines, speed, power)
+
+
+def precision_track(seed=0, nx=256, ny=128, nz=64, steps=500, dt=5e-6):
+    """Large straight track with seeded power and speed; ``(cfg, path)``."""
+    rng = np.random.default_rng(seed)
+    power = float(rng.uniform(150.0, 400.0))
+    speed = float(rng.uniform(0.5, 2.0))
+    return straight_track(nx, ny, nz, steps=steps, dt=dt, size=(4e-3, 2e-3, 1e-3),
+                          x0=0.5e-3, speed=speed, power=power)
+
+
+def scaled(cfg, nx, ny, nz, size=None, steps=None):
+    """Copy of ``cfg`` with another mesh (and optionally domain size / step count)."""
+    out = copy.deepcopy(cfg)
+    out["domain"]["mesh"] = [nx, ny, nz]
+    if size is not None:
+        out["domain"]["size"] = list(size)
+    if steps is not None:
+        out["simulation"]["duration"] = steps * out["simulation"]["dt"]
+    return out

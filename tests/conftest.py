@@ -1,0 +1,69 @@
+"""Shared test setup: markers, import path, golden-fixture loader."""
+import os
+import sys
+import warnings
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA device (B200) and libsgh_b200.so")
+    config.addinivalue_line("markers", "slow: takes more than a few seconds")
+
+
+def load_golden(name):
+    with np.load(os.path.join(GOLDEN, f"{name}.npz")) as f:
+        return {k: f[k] for k in f.files}
+
+
+def golden_case(name):
+    """(cfg, path, steps, snapshot steps, block) of a fixture, as make_golden built it."""
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    import make_golden
+    return make_golden.cases()[name]
+
+
+def make_context(cfg, path):
+    from spectral_galerkin_heat_b200 import SimulationContext
+    import copy
+    ctx = SimulationContext.from_dict(copy.deepcopy(cfg))
+    ctx.laser_path = path
+    return ctx
+
+
+def rel_l2(a, b):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    nb = np.linalg.norm(b)
+    return float(np.linalg.norm(a - b) / (nb if nb > 0 else 1.0))
+
+
+@pytest.fixture(autouse=True)
+def _quiet_warnings():
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore", RuntimeWarning)
+        yield
+
+
+def cuda_ok():
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+def pytest_collection_modifyitems(config, items):
+    if cuda_ok():
+        return
+    skip = pytest.mark.skip(reason="no CUDA device")
+    for item in items:
+        if "gpu" in item.keywords:
+            item.add_marker(skip)

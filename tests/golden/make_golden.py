@@ -1,0 +1,174 @@
+"""Generate the golden fixtures under ``tests/golden/`` from the reference itself.
+
+Run in a container where the reference checkout exists (read-only) at
+``/root/reference`` (override with ``SGH_REFERENCE``)::
+
+    python tests/golden/make_golden.py
+
+The reference is the pure-Python package ``spectral_galerkin_heat``. Its module
+imports pull in ``pint``, ``h5py``, ``matplotlib`` and ``pyfftw``, which are
+absent from this image and unused on the time-step path, so empty stand-ins are
+registered first (configs use plain SI numbers, so no unit conversion runs).
+``NUMBA_CACHE_DIR`` is pointed at a temporary directory so nothing is written
+into the reference tree.
+
+For each case the reference ``SpectralSolver(NumpyBackend())`` is stepped
+directly (no runner, so exactly ``steps`` calls of ``step(t, dt)`` with
+``t = i * dt``), the CPU oracle (``oracle/sgh_oracle.py``) is stepped beside it
+on the same context object, the two are required to agree, and the reference's
+outputs are stored: modes at chosen steps (optionally a low-index block only),
+the top-surface temperature, and per-step metrics. The versions of the
+libraries used are written into every file.
+"""
+from __future__ import annotations
+
+import copy
+import os
+import platform
+import sys
+import tempfile
+import time
+import types
+import warnings
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+REPO = HERE.parent.parent
+REF = Path(os.environ.get("SGH_REFERENCE", "/root/reference"))
+
+
+def import_reference():
+    os.environ.setdefault("NUMBA_CACHE_DIR", tempfile.mkdtemp(prefix="sgh_numba_"))
+    sys.dont_write_bytecode = True
+    for name in ("pint", "h5py", "matplotlib", "matplotlib.pyplot", "pyfftw"):
+        if name in sys.modules:
+            continue
+        mod = types.ModuleType(name)
+        if name == "pint":
+            class _Registry:
+                def Quantity(self, *a, **k):
+                    raise RuntimeError("unit conversion is not available (stand-in module)")
+            mod.UnitRegistry = _Registry
+        sys.modules[name] = mod
+    sys.modules["matplotlib"].pyplot = sys.modules["matplotlib.pyplot"]
+    sys.path.insert(0, str(REF / "src"))
+    sys.path.insert(0, str(REPO))
+    import spectral_galerkin_heat as ref  # noqa: F401
+    from spectral_galerkin_heat.backends import NumpyBackend
+    from spectral_galerkin_heat.core.parameters import SimulationContext
+    from spectral_galerkin_heat.solvers.spectral import SpectralSolver
+    return SimulationContext, SpectralSolver, NumpyBackend
+
+
+def cases():
+    """Name -> (cfg, path, steps, snapshot steps, mode block or None)."""
+    sys.path.insert(0, str(REPO))
+    from spectral_galerkin_heat_b200 import workloads as W
+    from spectral_galerkin_heat_b200.laser import FixedLaser, StraightTrack
+
+    out = {}
+    # straight track, full size: 300 steps of metrics; modes inside the
+    # 60-step horizon over which this explicit (one-pass) scheme is not chaotic
+    cfg, path = W.straight_track()
+    out["track_64x32x16"] = (cfg, path, 300, [1, 30, 60], None)
+    # nonlinear raster at reduced size on a reduced domain (melts in a few steps)
+    cfg, path = W.nonlinear_raster(nx=32, ny=16, nz=8, size=(0.5e-3, 0.25e-3, 0.125e-3),
+                                   line_length=0.1e-3, hatch=25e-6, steps=40)
+    out["raster_32x16x8"] = (cfg, path, 40, [1, 10, 40], None)
+    # nonlinear raster at the full mode count, first steps; low-index block stored
+    cfg, path = W.nonlinear_raster(steps=3)
+    out["raster_128x64x32"] = (cfg, path, 3, [3], (8, 16, 32))
+    # odd sizes, bottom + top convection, cell-integrated beam, T-dependent k only
+    cfg, _ = W.nonlinear_raster(nx=13, ny=10, nz=6, size=(0.4e-3, 0.3e-3, 0.1e-3), steps=6,
+                                tol=1e-9, omega=0.2, cap=200)
+    cfg["material"]["h_conv_bottom"] = 5.0e3
+    cfg["material"]["h_conv_top"] = 2.0e3
+    cfg["material"]["Cp"] = 500.0
+    cfg["laser"]["cell_integrated"] = True
+    path = StraightTrack(0.1e-3, 0.14e-3, 0.7, 0.3, 180.0)
+    out["odd_13x10x6_conv"] = (cfg, path, 6, [1, 6], None)
+    # constant properties with latent heat (latent source without the property model)
+    cfg, _ = W.straight_track(nx=24, ny=12, nz=8, steps=8, dt=2e-6,
+                              size=(0.6e-3, 0.3e-3, 0.15e-3))
+    cfg["material"]["L_f"] = 2.7e5
+    cfg["simulation"].update({"max_picard_iter": 400, "picard_omega": 0.1, "picard_tol": 1e-8})
+    path = StraightTrack(0.2e-3, 0.15e-3, 0.8, 0.0, 220.0)
+    out["latent_const_24x12x8"] = (cfg, path, 8, [8], None)
+    # super-Gaussian beam, elliptical, reference Picard defaults, laser moves in y
+    cfg, _ = W.straight_track(nx=20, ny=18, nz=5, steps=5, dt=3e-6,
+                              size=(0.5e-3, 0.45e-3, 0.1e-3))
+    cfg["laser"].update({"profile": "super_gaussian", "super_gaussian_order": 4.0,
+                         "r_x": 60e-6, "r_y": 40e-6})
+    cfg["simulation"].pop("max_picard_iter")
+    cfg["simulation"].pop("picard_omega")
+    path = StraightTrack(0.25e-3, 0.1e-3, 0.0, 1.2, 250.0)
+    out["supergauss_20x18x5"] = (cfg, path, 5, [5], None)
+    # laser off: the field must stay at T0
+    cfg, _ = W.straight_track(nx=8, ny=6, nz=4, steps=3)
+    path = FixedLaser(1e-3, 0.5e-3, 200.0, is_on=False)
+    out["laser_off_8x6x4"] = (cfg, path, 3, [3], None)
+    return out
+
+
+def run_case(name, spec, Ctx, Solver, Numpy):
+    sys.path.insert(0, str(REPO))
+    from oracle.sgh_oracle import OracleSolver
+
+    cfg, path, steps, snaps, block = spec
+    ctx = Ctx.from_dict(copy.deepcopy(cfg))
+    ctx.laser_path = path
+    ref = Solver(Numpy(), ctx)
+    ref.initialize()
+    orc = OracleSolver(ctx)
+    orc.initialize()
+    dt = ctx.num.dt
+    rec = {k: [] for k in ("T_surface_max", "P_laser", "n_evap_iter", "picard_converged",
+                           "picard_rel_err")}
+    files = {}
+    worst = 0.0
+    t0 = time.time()
+    for i in range(steps):
+        t = i * dt
+        _, m = ref.step(t, dt)
+        _, mo = orc.step(t, dt)
+        for k in rec:
+            rec[k].append(float(m[k]))
+        a = np.array(ref.state.a, dtype=np.float64, copy=True)
+        if (i + 1) in snaps:
+            rel = float(np.linalg.norm(orc.a - a) / np.linalg.norm(a))
+            worst = max(worst, rel)
+            assert rel < 1e-12, f"{name}: oracle differs from the reference at step {i+1}: {rel}"
+            assert mo["n_evap_iter"] == int(m["n_evap_iter"]), f"{name}: Picard count differs"
+            key = f"modes_step{i+1}"
+            files[key] = a if block is None else a[:block[0], :block[1], :block[2]].copy()
+            files[f"modes_norm_step{i+1}"] = np.array(np.linalg.norm(a))
+            files[f"surface_step{i+1}"] = np.asarray(
+                orc.surface_T(a, top=True), dtype=np.float64)
+    for k, v in rec.items():
+        files[f"metric_{k}"] = np.asarray(v)
+    import numba
+    import scipy
+    files["meta"] = np.array(str({
+        "case": name, "steps": steps, "snapshots": snaps, "block": block, "dt": dt,
+        "numpy": np.__version__, "scipy": scipy.__version__, "numba": numba.__version__,
+        "python": platform.python_version(), "oracle_vs_reference_worst_relL2": worst,
+    }))
+    np.savez_compressed(HERE / f"{name}.npz", **files)
+    print(f"{name}: {steps} steps in {time.time()-t0:.1f}s, oracle vs reference worst "
+          f"rel L2 {worst:.2e}")
+
+
+def main(argv):
+    warnings.simplefilter("ignore")
+    Ctx, Solver, Numpy = import_reference()
+    sel = set(argv[1:])
+    for name, spec in cases().items():
+        if sel and name not in sel:
+            continue
+        run_case(name, spec, Ctx, Solver, Numpy)
+
+
+if __name__ == "__main__":
+    main(sys.argv)
