@@ -149,6 +149,12 @@ int sgh_plan_bind(sgh_plan* plan, void* workspace, uint64_t bytes, void* stream)
 /* Device pointer and size of a named workspace buffer (SGH_BUF_*). */
 int sgh_plan_buffer(const sgh_plan* plan, int32_t which, void** ptr, uint64_t* bytes);
 
+/* Kernels launched per step: *pre before the Picard loop (including the
+ * launch-setup kernel), *per_iter per Picard iteration, *post after it. A step
+ * with n iterations launches pre + n * per_iter + post kernels. No reference
+ * counterpart (launch accounting for benchmarks). */
+int sgh_plan_launch_counts(const sgh_plan* plan, int32_t* pre, int32_t* per_iter, int32_t* post);
+
 /* Initial condition: a = 0, a[0,0,0] = T0 sqrt(Lx Ly Lz), T_prev = T0, no
  * evaporation or latent history (solvers/spectral.py:176-202). Async. */
 int sgh_state_reset(sgh_plan* plan, void* stream);
@@ -158,6 +164,13 @@ int sgh_state_reset(sgh_plan* plan, void* stream);
  * no host sync per iteration) and copies the metrics back; returns after the
  * stream has drained. */
 int sgh_step(sgh_plan* plan, const sgh_laser* laser, sgh_step_out* out, void* stream);
+
+/* The same step as sgh_step with the same kernels launched one by one on the
+ * stream and the Picard loop driven from the host (one device->host read of
+ * the stop flag per iteration) -- the reference's own control flow
+ * (solvers/spectral.py:386-499). For profilers that cannot see kernels inside
+ * conditional graph nodes, and for debugging. */
+int sgh_step_eager(sgh_plan* plan, const sgh_laser* laser, sgh_step_out* out, void* stream);
 
 /* n_steps time steps back to back, laser states read from a device table and
  * metrics written to a device table; asynchronous. */

@@ -27,8 +27,8 @@ BUF = {"modes": 0, "K": 1, "KK": 2, "T_prev": 3, "q_evap_old": 4, "Q_modes": 5,
 # Every function declared in include/sgh_b200.h (checked by the tests).
 EXPORTED = (
     "sgh_abi_version", "sgh_last_error", "sgh_plan_create", "sgh_plan_destroy",
-    "sgh_plan_workspace_bytes", "sgh_plan_bind", "sgh_plan_buffer", "sgh_state_reset",
-    "sgh_step", "sgh_run", "sgh_dct3d", "sgh_surface_temperature", "sgh_project_volume",
+    "sgh_plan_workspace_bytes", "sgh_plan_bind", "sgh_plan_buffer", "sgh_plan_launch_counts", "sgh_state_reset",
+    "sgh_step", "sgh_step_eager", "sgh_run", "sgh_dct3d", "sgh_surface_temperature", "sgh_project_volume",
     "sgh_reconstruct_volume", "sgh_dctn_workspace_bytes", "sgh_dctn",
 )
 
@@ -101,8 +101,10 @@ def lib() -> C.CDLL:
             "sgh_plan_workspace_bytes": ([vp, u64p], C.c_int),
             "sgh_plan_bind": ([vp, vp, C.c_uint64, vp], C.c_int),
             "sgh_plan_buffer": ([vp, i32, C.POINTER(vp), u64p], C.c_int),
+            "sgh_plan_launch_counts": ([vp, C.POINTER(i32), C.POINTER(i32), C.POINTER(i32)], C.c_int),
             "sgh_state_reset": ([vp, vp], C.c_int),
             "sgh_step": ([vp, C.POINTER(SghLaser), C.POINTER(SghStepOut), vp], C.c_int),
+            "sgh_step_eager": ([vp, C.POINTER(SghLaser), C.POINTER(SghStepOut), vp], C.c_int),
             "sgh_run": ([vp, vp, i32, vp, vp], C.c_int),
             "sgh_dct3d": ([vp, i32, vp, vp, vp], C.c_int),
             "sgh_surface_temperature": ([vp, vp, i32, vp, vp], C.c_int),

@@ -37,6 +37,7 @@ using namespace sgh;
 namespace {
 
 thread_local std::string g_last_error;
+thread_local int g_launches = 0;  // kernels enqueued by the enqueue_* helpers
 
 int fail(int code, const std::string& msg) {
   g_last_error = msg;
@@ -140,7 +141,7 @@ __global__ void k_run_setup(Ctrl* ctrl, sgh_laser laser, const sgh_laser* table,
 // solvers/spectral.py:258-268) and the warm-start shift in pixels
 // (spectral_cpu_kernels.py:392-396); opens the Picard loop.
 __global__ void k_step_begin(const DevParams* __restrict__ P, Ctrl* ctrl,
-                             cudaGraphConditionalHandle h_picard) {
+                             cudaGraphConditionalHandle h_picard, int in_graph) {
   if (ctrl->table) ctrl->laser = ctrl->table[ctrl->step];
   const sgh_laser L = ctrl->laser;
   ctrl->I0 = L.is_on ? P->absorptivity * L.power / (P->area_factor * (P->r_x * P->r_y)) : 0.0;
@@ -150,7 +151,7 @@ __global__ void k_step_begin(const DevParams* __restrict__ P, Ctrl* ctrl,
   ctrl->stop = 0;
   ctrl->status = SGH_STEP_CAPPED;
   ctrl->rel_err = nan("");
-  cudaGraphSetConditional(h_picard, P->max_iter > 0 ? 1u : 0u);
+  if (in_graph) cudaGraphSetConditional(h_picard, P->max_iter > 0 ? 1u : 0u);
 }
 
 // Order-1 shift table entry for output index o (spectral_cpu_kernels.py:305-325).
@@ -319,7 +320,7 @@ k_stencil(const DevParams* __restrict__ P, const double* __restrict__ T, const d
 // err = sqrt(sum res^2 / n) / max(sqrt(sum a_old^2 / n), 1e-9).
 __global__ void __launch_bounds__(EW_THREADS)
 k_converge(const DevParams* __restrict__ P, Ctrl* ctrl, const double* __restrict__ partials,
-           int nparts, cudaGraphConditionalHandle h_picard) {
+           int nparts, cudaGraphConditionalHandle h_picard, int in_graph) {
   __shared__ double sh[2 * (EW_THREADS / 32)];
   double s0 = 0.0, s1 = 0.0;
   for (int b = threadIdx.x; b < nparts; b += EW_THREADS) {
@@ -347,7 +348,7 @@ k_converge(const DevParams* __restrict__ P, Ctrl* ctrl, const double* __restrict
       stop = 1;
     }
     ctrl->stop = stop;
-    cudaGraphSetConditional(h_picard, stop ? 0u : 1u);
+    if (in_graph) cudaGraphSetConditional(h_picard, stop ? 0u : 1u);
   }
 }
 
@@ -356,7 +357,7 @@ k_converge(const DevParams* __restrict__ P, Ctrl* ctrl, const double* __restrict
 __global__ void __launch_bounds__(EW_THREADS)
 k_commit(const DevParams* __restrict__ P, Ctrl* ctrl, const double* __restrict__ las_parts,
          int n_las, const double* __restrict__ surf_parts, int n_surf,
-         cudaGraphConditionalHandle h_steps) {
+         cudaGraphConditionalHandle h_steps, int in_graph) {
   __shared__ double sh[2 * (EW_THREADS / 32)];
   double s = 0.0, d = 0.0;
   for (int b = threadIdx.x; b < n_las; b += EW_THREADS) s += las_parts[b];
@@ -378,7 +379,7 @@ k_commit(const DevParams* __restrict__ P, Ctrl* ctrl, const double* __restrict__
     if (P->grid_latent && P->max_iter > 0) ctrl->have_qprev = 1;
     const int next = ctrl->step + 1;
     ctrl->step = next;
-    cudaGraphSetConditional(h_steps, next < ctrl->n_target ? 1u : 0u);
+    if (in_graph) cudaGraphSetConditional(h_steps, next < ctrl->n_target ? 1u : 0u);
   }
 }
 
@@ -401,6 +402,7 @@ struct sgh_plan {
   sgh_config cfg;
   DevParams hp;
   int nparts_relax = 0, nparts_las = 0, nparts_surf = 0;
+  int n_pre = 0, n_iter = 0, n_post = 0;  // kernels per step part (launch accounting)
   // offsets into the workspace
   size_t o_params, o_ctrl, o_mx, o_mxt, o_my, o_myt, o_mz, o_mzt, o_xc, o_yc, o_ct, o_cb;
   size_t o_K, o_KK, o_a, o_aK, o_trial, o_Tprev, o_Qm, o_t1, o_t2, o_vol, o_kp;
@@ -451,18 +453,25 @@ int check_program(const sgh_program& p, const char* name) {
 
 // ---- enqueue helpers (used both for graph capture and for direct calls) ----
 
+template <class Epi>
+inline void axis(const double* X, const double* Mat, int N, int A, int B, const Epi& epi, cudaStream_t st) {
+  launch_axis(X, Mat, N, A, B, epi, st);
+  ++g_launches;
+}
+
 void face_dct2(sgh_plan* p, const double* in, double* out, double scale, cudaStream_t s) {
   const DevParams& h = p->hp;
-  launch_axis(in, p->d(p->o_mx), h.nx, h.ny, 1, EpiStore{p->d(p->o_f1), 1.0, nullptr}, s);
-  launch_axis(p->d(p->o_f1), p->d(p->o_my), h.ny, 1, h.nx, EpiStore{out, scale, nullptr}, s);
+  axis(in, p->d(p->o_mx), h.nx, h.ny, 1, EpiStore{p->d(p->o_f1), 1.0, nullptr}, s);
+  axis(p->d(p->o_f1), p->d(p->o_my), h.ny, 1, h.nx, EpiStore{out, scale, nullptr}, s);
 }
 
 template <class Epi>
 void face_idct2(sgh_plan* p, const double* modes, const double* w, const Epi& epi, cudaStream_t s) {
   const DevParams& h = p->hp;
   k_zsum<<<cdiv(h.S, EW_THREADS), EW_THREADS, 0, s>>>(modes, w, h.nz, h.S, p->d(p->o_A));
-  launch_axis(p->d(p->o_A), p->d(p->o_mxt), h.nx, h.ny, 1, EpiStore{p->d(p->o_f1), 1.0, nullptr}, s);
-  launch_axis(p->d(p->o_f1), p->d(p->o_myt), h.ny, 1, h.nx, epi, s);
+  ++g_launches;
+  axis(p->d(p->o_A), p->d(p->o_mxt), h.nx, h.ny, 1, EpiStore{p->d(p->o_f1), 1.0, nullptr}, s);
+  axis(p->d(p->o_f1), p->d(p->o_myt), h.ny, 1, h.nx, epi, s);
 }
 
 // Three passes x -> y -> z through t1, t2; the last pass applies epi.
@@ -473,31 +482,36 @@ void volume_pass3(sgh_plan* p, const double* in, bool inverse, const Epi& epi, d
   const double* mx = p->d(inverse ? p->o_mxt : p->o_mx);
   const double* my = p->d(inverse ? p->o_myt : p->o_my);
   const double* mz = p->d(inverse ? p->o_mzt : p->o_mz);
-  launch_axis(in, mx, h.nx, h.ny * h.nz, 1, EpiStore{t1, 1.0, nullptr}, s);
-  launch_axis(t1, my, h.ny, h.nz, h.nx, EpiStore{t2, 1.0, nullptr}, s);
-  launch_axis(t2, mz, h.nz, 1, h.S, epi, s);
+  axis(in, mx, h.nx, h.ny * h.nz, 1, EpiStore{t1, 1.0, nullptr}, s);
+  axis(t1, my, h.ny, h.nz, h.nx, EpiStore{t2, 1.0, nullptr}, s);
+  axis(t2, mz, h.nz, 1, h.S, epi, s);
 }
 
-void enqueue_pre(sgh_plan* p, cudaStream_t s, cudaGraphConditionalHandle h_picard) {
+void enqueue_pre(sgh_plan* p, cudaStream_t s, cudaGraphConditionalHandle h_picard, int in_graph) {
   const DevParams& h = p->hp;
   DevParams* P = p->P();
   Ctrl* C = p->ctrl();
   const int gV = cdiv(h.V, EW_THREADS), gS = cdiv(h.S, EW_THREADS);
-  k_step_begin<<<1, 1, 0, s>>>(P, C, h_picard);
+  k_step_begin<<<1, 1, 0, s>>>(P, C, h_picard, in_graph);
+  ++g_launches;
   k_face_begin<<<gS, EW_THREADS, 0, s>>>(P, C, p->d(p->o_xc), p->d(p->o_yc), p->d(p->o_qevold),
                                           p->d(p->o_qlas), p->d(p->o_qnet), p->d(p->o_plas));
+  ++g_launches;
   face_dct2(p, p->d(p->o_qnet), p->d(p->o_Stop), h.dct_scale, s);
   k_init_modes<<<gV, EW_THREADS, 0, s>>>(P, C, p->d(p->o_a), p->d(p->o_K), p->d(p->o_KK), p->d(p->o_ct),
                                           p->d(p->o_Stop), p->d(p->o_Qm), p->d(p->o_aK));
+  ++g_launches;
   if (h.has_top_conv) {
     face_idct2(p, p->d(p->o_a), p->d(p->o_ct), EpiConvFace{P, h.h_top, 0, p->d(p->o_f2), nullptr}, s);
     face_dct2(p, p->d(p->o_f2), p->d(p->o_Stop), h.dct_scale, s);
     k_add_face<<<gV, EW_THREADS, 0, s>>>(P, p->d(p->o_a), p->d(p->o_KK), p->d(p->o_ct), p->d(p->o_Stop));
+  ++g_launches;
   }
   if (h.has_bottom_conv) {
     face_idct2(p, p->d(p->o_a), p->d(p->o_cb), EpiConvFace{P, h.h_bottom, 0, p->d(p->o_f2), nullptr}, s);
     face_dct2(p, p->d(p->o_f2), p->d(p->o_Sbot), h.dct_scale, s);
     k_add_face<<<gV, EW_THREADS, 0, s>>>(P, p->d(p->o_a), p->d(p->o_KK), p->d(p->o_cb), p->d(p->o_Sbot));
+  ++g_launches;
     // S_bot_raw, held fixed through the Picard loop (solvers/spectral.py:373-379)
     face_idct2(p, p->d(p->o_a), p->d(p->o_cb),
                EpiConvFace{P, h.h_bottom, h.prop_corr, p->d(p->o_f2), nullptr}, s);
@@ -505,7 +519,7 @@ void enqueue_pre(sgh_plan* p, cudaStream_t s, cudaGraphConditionalHandle h_picar
   }
 }
 
-void enqueue_picard(sgh_plan* p, cudaStream_t s, cudaGraphConditionalHandle h_picard) {
+void enqueue_picard(sgh_plan* p, cudaStream_t s, cudaGraphConditionalHandle h_picard, int in_graph) {
   const DevParams& h = p->hp;
   DevParams* P = p->P();
   Ctrl* C = p->ctrl();
@@ -536,10 +550,12 @@ void enqueue_picard(sgh_plan* p, cudaStream_t s, cudaGraphConditionalHandle h_pi
   } else if (h.prop_corr) {
     k_trial<<<gV, EW_THREADS, 0, s>>>(P, p->d(p->o_aK), p->d(p->o_KK), p->d(p->o_ct), p->d(p->o_cb),
                                        p->d(p->o_Stop), S_bot, p->d(p->o_trial));
+  ++g_launches;
   } else {
     const int g = p->nparts_relax;
     k_trial_relax<<<g, EW_THREADS, 0, s>>>(P, p->d(p->o_aK), p->d(p->o_KK), p->d(p->o_ct), p->d(p->o_cb),
                                             p->d(p->o_Stop), S_bot, p->d(p->o_a), p->d(p->o_prelax));
+  ++g_launches;
     nparts = g;
   }
   if (h.prop_corr) {
@@ -547,15 +563,17 @@ void enqueue_picard(sgh_plan* p, cudaStream_t s, cudaGraphConditionalHandle h_pi
                  EpiTemperatureKp{P, p->d(p->o_vol), p->d(p->o_kp), nullptr}, p->d(p->o_t1),
                  p->d(p->o_t2), s);
     k_stencil<<<gV, EW_THREADS, 0, s>>>(P, p->d(p->o_vol), p->d(p->o_kp), p->d(p->o_Tprev), p->d(p->o_t1));
+  ++g_launches;
     volume_pass3(p, p->d(p->o_t1), false,
                  EpiRelax{P, p->d(p->o_trial), p->d(p->o_KK), p->d(p->o_a), p->d(p->o_prelax)},
                  p->d(p->o_t2), p->d(p->o_vol), s);
     nparts = axis_blocks(h.nz, 1, h.S);
   }
-  k_converge<<<1, EW_THREADS, 0, s>>>(P, C, p->d(p->o_prelax), nparts, h_picard);
+  k_converge<<<1, EW_THREADS, 0, s>>>(P, C, p->d(p->o_prelax), nparts, h_picard, in_graph);
+  ++g_launches;
 }
 
-void enqueue_post(sgh_plan* p, cudaStream_t s, cudaGraphConditionalHandle h_steps) {
+void enqueue_post(sgh_plan* p, cudaStream_t s, cudaGraphConditionalHandle h_steps, int in_graph) {
   const DevParams& h = p->hp;
   DevParams* P = p->P();
   face_idct2(p, p->d(p->o_a), p->d(p->o_ct),
@@ -564,7 +582,8 @@ void enqueue_post(sgh_plan* p, cudaStream_t s, cudaGraphConditionalHandle h_step
     volume_pass3(p, p->d(p->o_a), true, EpiDiv{p->d(p->o_Tprev), h.sqrt_dV, nullptr}, p->d(p->o_t1),
                  p->d(p->o_t2), s);
   k_commit<<<1, EW_THREADS, 0, s>>>(P, p->ctrl(), p->d(p->o_plas), p->nparts_las, p->d(p->o_psurf),
-                                     p->nparts_surf, h_steps);
+                                     p->nparts_surf, h_steps, in_graph);
+  ++g_launches;
 }
 
 int capture(sgh_plan* p) {
@@ -585,7 +604,9 @@ int capture(sgh_plan* p) {
   SGH_CK(cudaStreamBeginCaptureToGraph(p->cs1, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
   cudaGraphConditionalHandle h_picard;
   SGH_CK(cudaGraphConditionalHandleCreate(&h_picard, body, 0, 0));
-  enqueue_pre(p, p->cs1, h_picard);
+  g_launches = 0;
+  enqueue_pre(p, p->cs1, h_picard, 1);
+  p->n_pre = g_launches;
   cudaStreamCaptureStatus status;
   cudaGraph_t cur;
   const cudaGraphNode_t* deps = nullptr;
@@ -601,9 +622,13 @@ int capture(sgh_plan* p) {
   SGH_CK(cudaStreamUpdateCaptureDependencies(p->cs1, &inner_node, 1, cudaStreamSetCaptureDependencies));
   cudaGraph_t ibody = inner.conditional.phGraph_out[0];
   SGH_CK(cudaStreamBeginCaptureToGraph(p->cs2, ibody, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-  enqueue_picard(p, p->cs2, h_picard);
+  g_launches = 0;
+  enqueue_picard(p, p->cs2, h_picard, 1);
+  p->n_iter = g_launches;
   SGH_CK(cudaStreamEndCapture(p->cs2, &ibody));
-  enqueue_post(p, p->cs1, h_steps);
+  g_launches = 0;
+  enqueue_post(p, p->cs1, h_steps, 1);
+  p->n_post = g_launches;
   SGH_CK(cudaStreamEndCapture(p->cs1, &body));
   SGH_CK(cudaGetLastError());
   SGH_CK(cudaGraphInstantiate(&p->exec, G, 0));
@@ -804,6 +829,15 @@ int sgh_plan_bind(sgh_plan* p, void* workspace, uint64_t bytes, void* stream) {
   return SGH_OK;
 }
 
+int sgh_plan_launch_counts(const sgh_plan* p, int32_t* pre, int32_t* per_iter, int32_t* post) {
+  if (!p || !pre || !per_iter || !post) return fail(SGH_ERR_INVALID, "null argument");
+  if (!p->bound) return fail(SGH_ERR_STATE, "plan is not bound");
+  *pre = p->n_pre + 1;  // + the launch-setup kernel of sgh_step / sgh_run
+  *per_iter = p->n_iter;
+  *post = p->n_post;
+  return SGH_OK;
+}
+
 int sgh_plan_buffer(const sgh_plan* p, int32_t which, void** ptr, uint64_t* bytes) {
   if (!p || !ptr) return fail(SGH_ERR_INVALID, "null argument");
   if (!p->ws) return fail(SGH_ERR_STATE, "plan is not bound");
@@ -842,6 +876,26 @@ int sgh_step(sgh_plan* p, const sgh_laser* laser, sgh_step_out* out, void* strea
   k_run_setup<<<1, 1, 0, s>>>(p->ctrl(), *laser, nullptr, nullptr, 1);
   SGH_CK(cudaGetLastError());
   SGH_CK(cudaGraphLaunch(p->exec, s));
+  if (out) SGH_CK(cudaMemcpyAsync(out, &p->ctrl()->out, sizeof(sgh_step_out), cudaMemcpyDeviceToHost, s));
+  SGH_CK(cudaStreamSynchronize(s));
+  return SGH_OK;
+}
+
+int sgh_step_eager(sgh_plan* p, const sgh_laser* laser, sgh_step_out* out, void* stream) {
+  if (!p || !laser) return fail(SGH_ERR_INVALID, "null argument");
+  if (!p->bound) return fail(SGH_ERR_STATE, "plan is not bound");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  k_run_setup<<<1, 1, 0, s>>>(p->ctrl(), *laser, nullptr, nullptr, 1);
+  enqueue_pre(p, s, 0, 0);
+  for (int it = 0; it < p->hp.max_iter; ++it) {
+    enqueue_picard(p, s, 0, 0);
+    int stop = 0;
+    SGH_CK(cudaMemcpyAsync(&stop, &p->ctrl()->stop, sizeof(int), cudaMemcpyDeviceToHost, s));
+    SGH_CK(cudaStreamSynchronize(s));
+    if (stop) break;
+  }
+  enqueue_post(p, s, 0, 0);
+  SGH_CK(cudaGetLastError());
   if (out) SGH_CK(cudaMemcpyAsync(out, &p->ctrl()->out, sizeof(sgh_step_out), cudaMemcpyDeviceToHost, s));
   SGH_CK(cudaStreamSynchronize(s));
   return SGH_OK;

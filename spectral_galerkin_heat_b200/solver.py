@@ -242,13 +242,16 @@ class B200SpectralSolver(HeatSolver):
         if self.state is None or self._plan is None:
             raise RuntimeError("Solver must be initialized before stepping.")
 
-    def step(self, t: float, dt: float):
+    def step(self, t: float, dt: float, eager: bool = False):
+        """One time step. ``eager=True`` launches the same kernels one by one with
+        the Picard loop driven from the host (for profilers and debugging)."""
         self._require()
         st = self.context.laser_path.get_state(t, dt)
         laser = laser_struct(st, dt, self._cfg.dt)
         out = _lib.SghStepOut()
-        _lib.check("sgh_step", _lib.lib().sgh_step(self._plan, C.byref(laser), C.byref(out),
-                                                   C.c_void_p(self.state.stream.cuda_stream)))
+        fn = "sgh_step_eager" if eager else "sgh_step"
+        _lib.check(fn, getattr(_lib.lib(), fn)(self._plan, C.byref(laser), C.byref(out),
+                                               C.c_void_p(self.state.stream.cuda_stream)))
         metrics = self._metrics(out, t)
         if self.track_picard_history:
             self.picard_history = [{"iter": metrics["n_evap_iter"] - 1, "rms_diff": None,
@@ -305,12 +308,30 @@ class B200SpectralSolver(HeatSolver):
         host = torch.frombuffer(bytearray(bytes(arr)), dtype=torch.uint8)
         return host.to(self.state.workspace.device)
 
-    def run_table(self, table, outs, n: int) -> None:
-        """Enqueue ``n`` steps reading laser states from ``table`` (device) and writing
-        ``sgh_step_out`` records into ``outs`` (device); returns without waiting."""
+    def run_table(self, table, outs, n: int, start: int = 0) -> None:
+        """Enqueue ``n`` steps reading laser states ``start..start+n-1`` from ``table``
+        (device) and writing ``sgh_step_out`` records into the same slots of ``outs``
+        (device); returns without waiting."""
+        lsz, osz = C.sizeof(_lib.SghLaser), C.sizeof(_lib.SghStepOut)
+        if table.numel() < (start + n) * lsz or outs.numel() < (start + n) * osz:
+            raise ValueError("laser or metrics table too short")
         _lib.check("sgh_run", _lib.lib().sgh_run(
-            self._plan, C.c_void_p(table.data_ptr()), int(n), C.c_void_p(outs.data_ptr()),
-            C.c_void_p(self.state.stream.cuda_stream)))
+            self._plan, C.c_void_p(table.data_ptr() + start * lsz), int(n),
+            C.c_void_p(outs.data_ptr() + start * osz), C.c_void_p(self.state.stream.cuda_stream)))
+
+    def launch_counts(self):
+        """``(pre, per_iteration, post)`` kernel launches of one step."""
+        self._require()
+        a, b, c = C.c_int32(), C.c_int32(), C.c_int32()
+        _lib.check("sgh_plan_launch_counts", _lib.lib().sgh_plan_launch_counts(
+            self._plan, C.byref(a), C.byref(b), C.byref(c)))
+        return a.value, b.value, c.value
+
+    @staticmethod
+    def decode_outs(host_bytes, n):
+        """Decode ``n`` ``sgh_step_out`` records from a host byte buffer."""
+        sz = C.sizeof(_lib.SghStepOut)
+        return [_lib.SghStepOut.from_buffer_copy(host_bytes[i * sz:(i + 1) * sz]) for i in range(n)]
 
     # ---- state access ------------------------------------------------------
     def set_state(self, temperature_field) -> None:
