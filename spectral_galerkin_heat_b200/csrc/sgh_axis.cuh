@@ -2,11 +2,13 @@
 // contraction, with a fused per-element epilogue.
 //
 // View the C-ordered field as [A][N][B] with N the transformed axis. One pass
-// computes out[a][k][b] = sum_n Mat[k][n] * in[a][n][b] for all (a, k, b), i.e.
-// the GEMM  C[k, c] = sum_n Mat[k, n] X[n, c]  with c = a*B + b. Mat is the
-// orthonormal DCT-II matrix (forward) or its transpose (DCT-III, inverse), so
-// three passes give scipy.fft.dctn(type=2|3, norm='ortho') over all axes
-// (physics/spectral_cpu_kernels.py:374-389), and two passes the face transform.
+// computes out[a][k][b] = sum_n Mat[k][n] * in[a][n][b], i.e. the GEMM
+// C[k, c] = sum_n Mat[k, n] X[n, c] with c = a*B + b. Mat is Nout x Nin: the
+// orthonormal DCT-II matrix (forward), its transpose (DCT-III, inverse), or
+// either with extra output rows appended (Nout > Nin) that yield face values
+// from the same contraction (see the z-pass of the volume transforms). Three
+// passes give scipy.fft.dctn(type=2|3, norm='ortho') over all axes
+// (physics/spectral_cpu_kernels.py:374-389), two passes the face transform.
 //
 // Tiling: 256 threads, BK = 16 contraction slices staged in shared memory per
 // iteration; each thread owns a 2 x 4 register tile. When B == 1 (the
@@ -14,9 +16,9 @@
 // thread tile runs along k so that the epilogue stores are coalesced; when
 // B > 1 it runs along c (= b, contiguous).
 //
-// The epilogue functor receives (linear index of the output element in the
-// [A][N][B] layout, value) and may accumulate two partial sums or a max that
-// are reduced per CTA and written to a partials array (deterministic order).
+// The epilogue functor receives (linear output index (a*Nout + k)*B + b, k, b,
+// value) and may accumulate two partial sums or a max that are reduced per CTA
+// and written to a partials array (deterministic order).
 #pragma once
 #include "sgh_device.cuh"
 
@@ -31,7 +33,8 @@ struct Red {
 
 template <bool CONTIG, class Epi>
 __global__ void __launch_bounds__(AX_THREADS)
-k_axis(const double* __restrict__ X, const double* __restrict__ Mat, int N, int A, int B, Epi epi) {
+k_axis(const double* __restrict__ X, const double* __restrict__ Mat, int Nout, int N, int A, int B,
+       Epi epi) {
   constexpr int TK = CONTIG ? 64 : 32;   // outputs along the transformed axis per CTA
   constexpr int TC = CONTIG ? 32 : 64;   // outputs along c per CTA
   __shared__ double Ms[AX_BK][TK + 1];
@@ -57,7 +60,7 @@ k_axis(const double* __restrict__ X, const double* __restrict__ Mat, int N, int 
     for (int e = tid; e < TK * AX_BK; e += AX_THREADS) {
       const int kr = e >> 4, kk = e & 15;
       const int k = k0 + kr, n = n0 + kk;
-      Ms[kk][kr] = (k < N && n < N) ? __ldg(Mat + (size_t)k * N + n) : 0.0;
+      Ms[kk][kr] = (k < Nout && n < N) ? __ldg(Mat + (size_t)k * N + n) : 0.0;
     }
     // X tile: slices n0..n0+15, columns c0..c0+TC-1
     if (CONTIG) {
@@ -115,10 +118,10 @@ k_axis(const double* __restrict__ X, const double* __restrict__ Mat, int N, int 
     for (int j = 0; j < 4; ++j) {
       const int k = CONTIG ? (k0 + f + 16 * j) : (k0 + 2 * s + i);
       const int c = CONTIG ? (c0 + 2 * s + i) : (c0 + f + 16 * j);
-      if (k < N && c < ncol) {
+      if (k < Nout && c < ncol) {
         const int a = c / B, b = c - a * B;
-        const int idx = (a * N + k) * B + b;
-        epi(idx, acc[i][j], r);
+        const int idx = (a * Nout + k) * B + b;
+        epi(idx, k, b, acc[i][j], r);
       }
     }
   }
@@ -142,20 +145,21 @@ k_axis(const double* __restrict__ X, const double* __restrict__ Mat, int N, int 
 }
 
 // Number of CTAs of one pass (the number of partials a reducing epilogue writes).
-inline int axis_blocks(int N, int A, int B) {
-  if (B == 1) return ((A + 31) / 32) * ((N + 63) / 64);
-  return ((A * B + 63) / 64) * ((N + 31) / 32);
+inline int axis_blocks(int Nout, int A, int B) {
+  if (B == 1) return ((A + 31) / 32) * ((Nout + 63) / 64);
+  return ((A * B + 63) / 64) * ((Nout + 31) / 32);
 }
 
+// One pass with Mat of Nout x N (N = contraction length).
 template <class Epi>
-inline void launch_axis(const double* X, const double* Mat, int N, int A, int B, const Epi& epi,
-                        cudaStream_t st) {
+inline void launch_axis(const double* X, const double* Mat, int Nout, int N, int A, int B,
+                        const Epi& epi, cudaStream_t st) {
   if (B == 1) {
-    dim3 grid((A + 31) / 32, (N + 63) / 64);
-    k_axis<true, Epi><<<grid, AX_THREADS, 0, st>>>(X, Mat, N, A, B, epi);
+    dim3 grid((A + 31) / 32, (Nout + 63) / 64);
+    k_axis<true, Epi><<<grid, AX_THREADS, 0, st>>>(X, Mat, Nout, N, A, B, epi);
   } else {
-    dim3 grid((A * B + 63) / 64, (N + 31) / 32);
-    k_axis<false, Epi><<<grid, AX_THREADS, 0, st>>>(X, Mat, N, A, B, epi);
+    dim3 grid((A * B + 63) / 64, (Nout + 31) / 32);
+    k_axis<false, Epi><<<grid, AX_THREADS, 0, st>>>(X, Mat, Nout, N, A, B, epi);
   }
 }
 
@@ -169,7 +173,7 @@ struct EpiStore {
   double* out;
   double mul;
   double* partials;
-  __device__ __forceinline__ void operator()(int i, double v, Red&) const { out[i] = v * mul; }
+  __device__ __forceinline__ void operator()(int i, int, int, double v, Red&) const { out[i] = v * mul; }
 };
 
 // out = v / div (reconstruct_volume: IDCT_II(a) / sqrt_dV, spectral_ops.py:83-91)
@@ -178,7 +182,7 @@ struct EpiDiv {
   double* out;
   double div;
   double* partials;
-  __device__ __forceinline__ void operator()(int i, double v, Red&) const { out[i] = v / div; }
+  __device__ __forceinline__ void operator()(int i, int, int, double v, Red&) const { out[i] = v / div; }
 };
 
 // Grid-mode latent source at the reconstructed field:
@@ -189,7 +193,7 @@ struct EpiLatent {
   const double* Tprev;
   double* Q;
   double* partials;
-  __device__ __forceinline__ void operator()(int i, double v, Red&) const {
+  __device__ __forceinline__ void operator()(int i, int, int, double v, Red&) const {
     const double T = v / P->sqrt_dV;
     Q[i] = latent_source(*P, T, Tprev[i]);
   }
@@ -203,7 +207,7 @@ struct EpiTemperatureKp {
   double* T;
   double* kp;
   double* partials;
-  __device__ __forceinline__ void operator()(int i, double v, Red&) const {
+  __device__ __forceinline__ void operator()(int i, int, int, double v, Red&) const {
     const double t = v / P->sqrt_dV;
     T[i] = t;
     kp[i] = k_prime(*P, t);
@@ -221,19 +225,20 @@ struct EpiTrial {
   const double* KK;
   const double* Ct;
   const double* Cb;
-  const double* S_top;
+  const double* S_top;   // DCT2 of the net top flux, times s_top_scale
+  double s_top_scale;
   const double* S_bot;   // null when there is no bottom convection
   double* Qm;
   double* a_trial;       // written when !RELAX
   double* a_it;          // read and updated when RELAX
   double* partials;
-  __device__ __forceinline__ void operator()(int i, double v, Red& r) const {
+  __device__ __forceinline__ void operator()(int i, int, int, double v, Red& r) const {
     const int S = P->S;
     const int z = i / S, yx = i - z * S;
     const double q = v * P->sqrt_dV;
     Qm[i] = q;
     const double kk = KK[i];
-    double t = aK[i] + kk * Ct[z] * S_top[yx];
+    double t = aK[i] + kk * Ct[z] * (s_top_scale * S_top[yx]);
     t += kk * q;
     if (S_bot) t += kk * Cb[z] * S_bot[yx];
     if (RELAX) {
@@ -258,7 +263,7 @@ struct EpiRelax {
   const double* KK;
   double* a_it;
   double* partials;
-  __device__ __forceinline__ void operator()(int i, double v, Red& r) const {
+  __device__ __forceinline__ void operator()(int i, int, int, double v, Red& r) const {
     const double c = v * P->sqrt_dV;
     const double raw = a_trial[i] + KK[i] * c;
     const double old = a_it[i];
@@ -279,7 +284,7 @@ struct EpiTopFlux {
   double* q_net;
   int rescale;
   double* partials;
-  __device__ __forceinline__ void operator()(int i, double v, Red&) const {
+  __device__ __forceinline__ void operator()(int i, int, int, double v, Red&) const {
     const double Ts = P->recon_scale * v;
     const double qe = evaporation(*P, Ts);
     q_evap[i] = qe;
@@ -299,7 +304,7 @@ struct EpiConvFace {
   int rescale;
   double* q;
   double* partials;
-  __device__ __forceinline__ void operator()(int i, double v, Red&) const {
+  __device__ __forceinline__ void operator()(int i, int, int, double v, Red&) const {
     const double T = P->recon_scale * v;
     double qc = -h * (T - P->T0);
     if (rescale) qc = qc * (P->kbar / k_blended(*P, T));
@@ -313,7 +318,7 @@ struct EpiFaceTemperature {
   const DevParams* P;
   double* out;
   double* partials;
-  __device__ __forceinline__ void operator()(int i, double v, Red&) const {
+  __device__ __forceinline__ void operator()(int i, int, int, double v, Red&) const {
     out[i] = P->recon_scale * v;
   }
 };
@@ -327,11 +332,66 @@ struct EpiCommitSurface {
   const double* q_evap;
   double* q_evap_old;
   double* partials;
-  __device__ __forceinline__ void operator()(int i, double v, Red& r) const {
+  __device__ __forceinline__ void operator()(int i, int, int, double v, Red& r) const {
     const double T = P->recon_scale * v;
     T_surf[i] = T;
     q_evap_old[i] = q_evap[i];
     r.mx = fmax(r.mx, T);
+  }
+};
+
+// z-pass of IDCT3(a_old) with one extra output row (Mat row nz = recon_scale *
+// Ct[p]): rows k < nz give the cell-centred field, T = v / sqrt_dV, and the
+// latent source Q = latent(T, T_prev) (spectral_ops.py:270-289); row nz gives
+// the top-surface temperature T_s of the same modes (the 2-D IDCT commutes
+// with the z-weighted sum of reconstruct_surface_temperature,
+// spectral_ops.py:210-219) and the evaporation / convection / rescaled net
+// top flux (solvers/spectral.py:388-407), stored as slab nz of Q so that the
+// following DCT3(Q) x- and y-passes also produce DCT2(q_net).
+struct EpiLatentSurface {
+  static constexpr int kReduce = 0;
+  const DevParams* P;
+  const double* Tprev;
+  double* Q;             // (nz + 1) slabs
+  const double* q_las;
+  double* q_evap;
+  int rescale;
+  double* partials;
+  __device__ __forceinline__ void operator()(int i, int k, int b, double v, Red&) const {
+    if (k < P->nz) {
+      Q[i] = latent_source(*P, v / P->sqrt_dV, Tprev[i]);
+    } else {
+      const double Ts = v;
+      const double qe = evaporation(*P, Ts);
+      q_evap[b] = qe;
+      const double qc = P->has_top_conv ? P->h_top * (Ts - P->T0) : 0.0;
+      double q = q_las[b] - qe - qc;
+      if (rescale) q = q * (P->kbar / k_blended(*P, Ts));
+      Q[i] = q;
+    }
+  }
+};
+
+// Commit: z-pass of IDCT3(a) with the extra surface row. Rows k < nz give
+// T_prev = IDCT3(a)/sqrt_dV (solvers/spectral.py:520-521); row nz gives the
+// surface temperature of the committed modes with its max (:502, :537) and
+// the q_evap_old <- q_evap copy (:512).
+struct EpiCommitVolume {
+  static constexpr int kReduce = 2;
+  const DevParams* P;
+  double* Tprev;
+  double* T_surf;
+  const double* q_evap;
+  double* q_evap_old;
+  double* partials;
+  __device__ __forceinline__ void operator()(int i, int k, int b, double v, Red& r) const {
+    if (k < P->nz) {
+      Tprev[i] = v / P->sqrt_dV;
+    } else {
+      T_surf[b] = v;
+      q_evap_old[b] = q_evap[b];
+      r.mx = fmax(r.mx, v);
+    }
   }
 };
 

@@ -92,15 +92,22 @@ __global__ void k_propagators(const DevParams* __restrict__ P, double alpha, dou
 
 // Cell-centred coordinates and the top / bottom z-weights
 // (SpectralGrid, physics/spectral_state.py:98-122; _C_coef spectral_helpers.py:26-46).
+// Also appends to the inverse z-matrix MzT (nz x nz) the rows recon_scale *
+// Ct[p] (top) and recon_scale * Cb[p] (bottom), so that an inverse z-pass
+// yields the surface temperatures beside the cell-centred field.
 __global__ void k_grid_tables(const DevParams* __restrict__ P, double* xc, double* yc, double* Ct,
-                              double* Cb) {
+                              double* Cb, double* MzT_aug) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < P->nx) xc[i] = ((double)i + 0.5) * P->dx;
   if (i < P->ny) yc[i] = ((double)i + 0.5) * P->dy;
   if (i < P->nz) {
+    const int nz = P->nz;
     const double c = (i == 0) ? sqrt(1.0 / P->Lz) : sqrt(2.0 / P->Lz);
+    const double ct = (i & 1) ? -c : c;
     Cb[i] = c;
-    Ct[i] = (i & 1) ? -c : c;
+    Ct[i] = ct;
+    MzT_aug[(size_t)nz * nz + i] = P->recon_scale * ct;
+    MzT_aug[(size_t)(nz + 1) * nz + i] = P->recon_scale * c;
   }
 }
 
@@ -451,18 +458,94 @@ int check_program(const sgh_program& p, const char* name) {
   return SGH_OK;
 }
 
+// Abstract interpretation of a property program over affine forms a + b T:
+// true (with the coefficients) when the program is affine in T, as the
+// piecewise-linear property tables are; constants are folded with host libm.
+bool program_affine(const sgh_program& p, double* A, double* B) {
+  double sa[SGH_MAX_STACK + 1], sb[SGH_MAX_STACK + 1];
+  int sp = 0;
+  for (int i = 0; i < p.n_ops;) {
+    const int op = p.ops[i++];
+    if (op == SGH_OP_CONST) { sa[sp] = p.consts[p.ops[i++]]; sb[sp] = 0.0; ++sp; continue; }
+    if (op == SGH_OP_T) { sa[sp] = 0.0; sb[sp] = 1.0; ++sp; continue; }
+    if ((op >= SGH_OP_ADD && op <= SGH_OP_POW) || op == SGH_OP_ATAN2) {
+      --sp;
+      const double xa = sa[sp - 1], xb = sb[sp - 1], ya = sa[sp], yb = sb[sp];
+      double ra, rb;
+      switch (op) {
+        case SGH_OP_ADD: ra = xa + ya; rb = xb + yb; break;
+        case SGH_OP_SUB: ra = xa - ya; rb = xb - yb; break;
+        case SGH_OP_MUL:
+          if (xb == 0.0) { ra = xa * ya; rb = xa * yb; }
+          else if (yb == 0.0) { ra = xa * ya; rb = xb * ya; }
+          else return false;
+          break;
+        case SGH_OP_DIV:
+          if (yb != 0.0) return false;
+          ra = xa / ya; rb = xb / ya;
+          break;
+        case SGH_OP_POW:
+          if (xb != 0.0 || yb != 0.0) return false;
+          ra = std::pow(xa, ya); rb = 0.0;
+          break;
+        default:  // atan2
+          if (xb != 0.0 || yb != 0.0) return false;
+          ra = std::atan2(xa, ya); rb = 0.0;
+      }
+      sa[sp - 1] = ra; sb[sp - 1] = rb;
+      continue;
+    }
+    if (op == SGH_OP_NEG) { sa[sp - 1] = -sa[sp - 1]; sb[sp - 1] = -sb[sp - 1]; continue; }
+    if (sb[sp - 1] != 0.0) return false;  // a function of T: not affine
+    const double x = sa[sp - 1];
+    double r;
+    switch (op) {
+      case SGH_OP_SQRT: r = std::sqrt(x); break;
+      case SGH_OP_EXP: r = std::exp(x); break;
+      case SGH_OP_LOG: r = std::log(x); break;
+      case SGH_OP_LOG2: r = std::log2(x); break;
+      case SGH_OP_LOG10: r = std::log10(x); break;
+      case SGH_OP_SIN: r = std::sin(x); break;
+      case SGH_OP_COS: r = std::cos(x); break;
+      case SGH_OP_TAN: r = std::tan(x); break;
+      case SGH_OP_ASIN: r = std::asin(x); break;
+      case SGH_OP_ACOS: r = std::acos(x); break;
+      case SGH_OP_ATAN: r = std::atan(x); break;
+      case SGH_OP_SINH: r = std::sinh(x); break;
+      case SGH_OP_COSH: r = std::cosh(x); break;
+      case SGH_OP_TANH: r = std::tanh(x); break;
+      case SGH_OP_ASINH: r = std::asinh(x); break;
+      case SGH_OP_ACOSH: r = std::acosh(x); break;
+      case SGH_OP_ATANH: r = std::atanh(x); break;
+      case SGH_OP_FABS: r = std::fabs(x); break;
+      case SGH_OP_CEIL: r = std::ceil(x); break;
+      case SGH_OP_FLOOR: r = std::floor(x); break;
+      case SGH_OP_TRUNC: r = std::trunc(x); break;
+      case SGH_OP_LOG1P: r = std::log1p(x); break;
+      case SGH_OP_EXPM1: r = std::expm1(x); break;
+      default: return false;
+    }
+    sa[sp - 1] = r;
+  }
+  if (sp != 1) return false;
+  *A = sa[0];
+  *B = sb[0];
+  return std::isfinite(*A) && std::isfinite(*B);
+}
+
 // ---- enqueue helpers (used both for graph capture and for direct calls) ----
 
 template <class Epi>
-inline void axis(const double* X, const double* Mat, int N, int A, int B, const Epi& epi, cudaStream_t st) {
-  launch_axis(X, Mat, N, A, B, epi, st);
+inline void axis(const double* X, const double* Mat, int Nout, int N, int A, int B, const Epi& epi,
+                 cudaStream_t st) {
+  launch_axis(X, Mat, Nout, N, A, B, epi, st);
   ++g_launches;
 }
 
 void face_dct2(sgh_plan* p, const double* in, double* out, double scale, cudaStream_t s) {
   const DevParams& h = p->hp;
-  axis(in, p->d(p->o_mx), h.nx, h.ny, 1, EpiStore{p->d(p->o_f1), 1.0, nullptr}, s);
-  axis(p->d(p->o_f1), p->d(p->o_my), h.ny, 1, h.nx, EpiStore{out, scale, nullptr}, s);
+  axis(in, p->d(p->o_mx), h.nx, h.nx, h.ny, 1, EpiStore{p->d(p->o_f1), 1.0, nullptr}, s);
+  axis(p->d(p->o_f1), p->d(p->o_my), h.ny, h.ny, 1, h.nx, EpiStore{out, scale, nullptr}, s);
 }
 
 template <class Epi>
@@ -470,21 +553,26 @@ void face_idct2(sgh_plan* p, const double* modes, const double* w, const Epi& ep
   const DevParams& h = p->hp;
   k_zsum<<<cdiv(h.S, EW_THREADS), EW_THREADS, 0, s>>>(modes, w, h.nz, h.S, p->d(p->o_A));
   ++g_launches;
-  axis(p->d(p->o_A), p->d(p->o_mxt), h.nx, h.ny, 1, EpiStore{p->d(p->o_f1), 1.0, nullptr}, s);
-  axis(p->d(p->o_f1), p->d(p->o_myt), h.ny, 1, h.nx, epi, s);
+  axis(p->d(p->o_A), p->d(p->o_mxt), h.nx, h.nx, h.ny, 1, EpiStore{p->d(p->o_f1), 1.0, nullptr}, s);
+  axis(p->d(p->o_f1), p->d(p->o_myt), h.ny, h.ny, 1, h.nx, epi, s);
 }
 
 // Three passes x -> y -> z through t1, t2; the last pass applies epi.
+// slabs: z-slabs run through the x and y passes (nz, or nz + 1 when the
+// input carries a face field as slab nz); z_rows: output rows of the z-pass
+// (nz, or nz + 1 / nz + 2 for the inverse with the surface rows appended).
 template <class Epi>
 void volume_pass3(sgh_plan* p, const double* in, bool inverse, const Epi& epi, double* t1, double* t2,
-                  cudaStream_t s) {
+                  cudaStream_t s, int slabs = -1, int z_rows = -1) {
   const DevParams& h = p->hp;
+  if (slabs < 0) slabs = h.nz;
+  if (z_rows < 0) z_rows = h.nz;
   const double* mx = p->d(inverse ? p->o_mxt : p->o_mx);
   const double* my = p->d(inverse ? p->o_myt : p->o_my);
   const double* mz = p->d(inverse ? p->o_mzt : p->o_mz);
-  axis(in, mx, h.nx, h.ny * h.nz, 1, EpiStore{t1, 1.0, nullptr}, s);
-  axis(t1, my, h.ny, h.nz, h.nx, EpiStore{t2, 1.0, nullptr}, s);
-  axis(t2, mz, h.nz, 1, h.S, epi, s);
+  axis(in, mx, h.nx, h.nx, h.ny * slabs, 1, EpiStore{t1, 1.0, nullptr}, s);
+  axis(t1, my, h.ny, h.ny, slabs, h.nx, EpiStore{t2, 1.0, nullptr}, s);
+  axis(t2, mz, z_rows, h.nz, 1, h.S, epi, s);
 }
 
 void enqueue_pre(sgh_plan* p, cudaStream_t s, cudaGraphConditionalHandle h_picard, int in_graph) {
@@ -525,37 +613,45 @@ void enqueue_picard(sgh_plan* p, cudaStream_t s, cudaGraphConditionalHandle h_pi
   Ctrl* C = p->ctrl();
   const int gV = cdiv(h.V, EW_THREADS);
   double* S_bot = h.has_bottom_conv ? p->d(p->o_Sbot) : nullptr;
-  // top face: T_s, evaporation, convection, rescale -> S_top
-  face_idct2(p, p->d(p->o_a), p->d(p->o_ct),
-             EpiTopFlux{P, p->d(p->o_qlas), p->d(p->o_qev), p->d(p->o_qnet), h.prop_corr, nullptr}, s);
-  face_dct2(p, p->d(p->o_qnet), p->d(p->o_Stop), h.dct_scale, s);
   int nparts = 0;
   if (h.grid_latent) {
-    volume_pass3(p, p->d(p->o_a), true, EpiLatent{P, p->d(p->o_Tprev), p->d(p->o_vol), nullptr},
-                 p->d(p->o_t1), p->d(p->o_t2), s);
+    // IDCT3(a_old) with the surface row: latent source in slabs 0..nz-1 and
+    // the net top flux in slab nz of vol; then DCT3 over nz + 1 slabs turns
+    // slab nz into DCT2(q_net), read by the trial epilogue as S_top.
+    volume_pass3(p, p->d(p->o_a), true,
+                 EpiLatentSurface{P, p->d(p->o_Tprev), p->d(p->o_vol), p->d(p->o_qlas), p->d(p->o_qev),
+                                  h.prop_corr, nullptr},
+                 p->d(p->o_t1), p->d(p->o_t2), s, h.nz, h.nz + 1);
+    const double* S_top = p->d(p->o_t2) + (size_t)h.nz * h.S;
     if (h.prop_corr) {
       volume_pass3(p, p->d(p->o_vol), false,
                    EpiTrial<false>{P, p->d(p->o_aK), p->d(p->o_KK), p->d(p->o_ct), p->d(p->o_cb),
-                                   p->d(p->o_Stop), S_bot, p->d(p->o_Qm), p->d(p->o_trial), nullptr,
+                                   S_top, h.dct_scale, S_bot, p->d(p->o_Qm), p->d(p->o_trial), nullptr,
                                    nullptr},
-                   p->d(p->o_t1), p->d(p->o_t2), s);
+                   p->d(p->o_t1), p->d(p->o_t2), s, h.nz + 1, h.nz);
     } else {
       volume_pass3(p, p->d(p->o_vol), false,
                    EpiTrial<true>{P, p->d(p->o_aK), p->d(p->o_KK), p->d(p->o_ct), p->d(p->o_cb),
-                                  p->d(p->o_Stop), S_bot, p->d(p->o_Qm), nullptr, p->d(p->o_a),
+                                  S_top, h.dct_scale, S_bot, p->d(p->o_Qm), nullptr, p->d(p->o_a),
                                   p->d(p->o_prelax)},
-                   p->d(p->o_t1), p->d(p->o_t2), s);
+                   p->d(p->o_t1), p->d(p->o_t2), s, h.nz + 1, h.nz);
       nparts = axis_blocks(h.nz, 1, h.S);
     }
-  } else if (h.prop_corr) {
+  } else {
+    // top face: T_s, evaporation, convection, rescale -> S_top
+    face_idct2(p, p->d(p->o_a), p->d(p->o_ct),
+               EpiTopFlux{P, p->d(p->o_qlas), p->d(p->o_qev), p->d(p->o_qnet), h.prop_corr, nullptr}, s);
+    face_dct2(p, p->d(p->o_qnet), p->d(p->o_Stop), h.dct_scale, s);
+  }
+  if (!h.grid_latent && h.prop_corr) {
     k_trial<<<gV, EW_THREADS, 0, s>>>(P, p->d(p->o_aK), p->d(p->o_KK), p->d(p->o_ct), p->d(p->o_cb),
                                        p->d(p->o_Stop), S_bot, p->d(p->o_trial));
-  ++g_launches;
-  } else {
+    ++g_launches;
+  } else if (!h.grid_latent) {
     const int g = p->nparts_relax;
     k_trial_relax<<<g, EW_THREADS, 0, s>>>(P, p->d(p->o_aK), p->d(p->o_KK), p->d(p->o_ct), p->d(p->o_cb),
                                             p->d(p->o_Stop), S_bot, p->d(p->o_a), p->d(p->o_prelax));
-  ++g_launches;
+    ++g_launches;
     nparts = g;
   }
   if (h.prop_corr) {
@@ -563,7 +659,7 @@ void enqueue_picard(sgh_plan* p, cudaStream_t s, cudaGraphConditionalHandle h_pi
                  EpiTemperatureKp{P, p->d(p->o_vol), p->d(p->o_kp), nullptr}, p->d(p->o_t1),
                  p->d(p->o_t2), s);
     k_stencil<<<gV, EW_THREADS, 0, s>>>(P, p->d(p->o_vol), p->d(p->o_kp), p->d(p->o_Tprev), p->d(p->o_t1));
-  ++g_launches;
+    ++g_launches;
     volume_pass3(p, p->d(p->o_t1), false,
                  EpiRelax{P, p->d(p->o_trial), p->d(p->o_KK), p->d(p->o_a), p->d(p->o_prelax)},
                  p->d(p->o_t2), p->d(p->o_vol), s);
@@ -576,13 +672,21 @@ void enqueue_picard(sgh_plan* p, cudaStream_t s, cudaGraphConditionalHandle h_pi
 void enqueue_post(sgh_plan* p, cudaStream_t s, cudaGraphConditionalHandle h_steps, int in_graph) {
   const DevParams& h = p->hp;
   DevParams* P = p->P();
-  face_idct2(p, p->d(p->o_a), p->d(p->o_ct),
-             EpiCommitSurface{P, p->d(p->o_Tsurf), p->d(p->o_qev), p->d(p->o_qevold), p->d(p->o_psurf)}, s);
-  if (h.grid_latent || h.prop_corr)
-    volume_pass3(p, p->d(p->o_a), true, EpiDiv{p->d(p->o_Tprev), h.sqrt_dV, nullptr}, p->d(p->o_t1),
-                 p->d(p->o_t2), s);
+  int n_surf;
+  if (h.grid_latent || h.prop_corr) {
+    // T_prev and the surface temperature from one IDCT3 with the surface row
+    volume_pass3(p, p->d(p->o_a), true,
+                 EpiCommitVolume{P, p->d(p->o_Tprev), p->d(p->o_Tsurf), p->d(p->o_qev), p->d(p->o_qevold),
+                                 p->d(p->o_psurf)},
+                 p->d(p->o_t1), p->d(p->o_t2), s, h.nz, h.nz + 1);
+    n_surf = axis_blocks(h.nz + 1, 1, h.S);
+  } else {
+    face_idct2(p, p->d(p->o_a), p->d(p->o_ct),
+               EpiCommitSurface{P, p->d(p->o_Tsurf), p->d(p->o_qev), p->d(p->o_qevold), p->d(p->o_psurf)}, s);
+    n_surf = p->nparts_surf;
+  }
   k_commit<<<1, EW_THREADS, 0, s>>>(P, p->ctrl(), p->d(p->o_plas), p->nparts_las, p->d(p->o_psurf),
-                                     p->nparts_surf, h_steps, in_graph);
+                                     n_surf, h_steps, in_graph);
   ++g_launches;
 }
 
@@ -728,6 +832,8 @@ int sgh_plan_create(const sgh_config* cfg, sgh_plan** out) {
     h.prog[P_RHO_LIQUID] = c.rho_liquid;
     h.prog[P_C_SOLID] = c.c_solid;
     h.prog[P_C_LIQUID] = c.c_liquid;
+    for (int i = 0; i < P_COUNT; ++i)
+      h.affine[i] = program_affine(h.prog[i], &h.aff_a[i], &h.aff_b[i]) ? 1 : 0;
   }
 
   p->nparts_relax = std::min(RELAX_BLOCKS_MAX, cdiv(h.V, EW_THREADS));
@@ -744,7 +850,7 @@ int sgh_plan_create(const sgh_config* cfg, sgh_plan** out) {
   p->o_my = L.take(sizeof(double) * c.ny * c.ny);
   p->o_myt = L.take(sizeof(double) * c.ny * c.ny);
   p->o_mz = L.take(sizeof(double) * c.nz * c.nz);
-  p->o_mzt = L.take(sizeof(double) * c.nz * c.nz);
+  p->o_mzt = L.take(sizeof(double) * (c.nz + 2) * c.nz);  // + top and bottom surface rows
   p->o_xc = L.take(sizeof(double) * c.nx);
   p->o_yc = L.take(sizeof(double) * c.ny);
   p->o_ct = L.take(sizeof(double) * c.nz);
@@ -756,9 +862,10 @@ int sgh_plan_create(const sgh_config* cfg, sgh_plan** out) {
   p->o_trial = L.take(V8);
   p->o_Tprev = L.take(V8);
   p->o_Qm = L.take(V8);
-  p->o_t1 = L.take(V8);
-  p->o_t2 = L.take(V8);
-  p->o_vol = L.take(V8);
+  const size_t VX8 = sizeof(double) * (size_t)h.S * (c.nz + 2);  // volume + face slabs
+  p->o_t1 = L.take(VX8);
+  p->o_t2 = L.take(VX8);
+  p->o_vol = L.take(VX8);
   p->o_kp = L.take(V8);
   p->o_qlas = L.take(S8);
   p->o_qnet = L.take(S8);
@@ -772,7 +879,7 @@ int sgh_plan_create(const sgh_config* cfg, sgh_plan** out) {
   p->o_A = L.take(S8);
   p->o_prelax = L.take(sizeof(double) * 2 * std::max(p->nparts_relax, nparts_axis));
   p->o_plas = L.take(sizeof(double) * p->nparts_las);
-  p->o_psurf = L.take(sizeof(double) * 2 * p->nparts_surf);
+  p->o_psurf = L.take(sizeof(double) * 2 * std::max(p->nparts_surf, axis_blocks(h.nz + 1, 1, h.S)));
   p->ws_need = L.off;
   *out = p;
   return SGH_OK;
@@ -810,7 +917,8 @@ int sgh_plan_bind(sgh_plan* p, void* workspace, uint64_t bytes, void* stream) {
   for (auto& m : mats)
     k_dct_matrix<<<cdiv((long)m.n * m.n, EW_THREADS), EW_THREADS, 0, s>>>(m.n, p->d(m.m), p->d(m.mt));
   const int gmax = cdiv(std::max(std::max(h.nx, h.ny), h.nz), EW_THREADS);
-  k_grid_tables<<<gmax, EW_THREADS, 0, s>>>(p->P(), p->d(p->o_xc), p->d(p->o_yc), p->d(p->o_ct), p->d(p->o_cb));
+  k_grid_tables<<<gmax, EW_THREADS, 0, s>>>(p->P(), p->d(p->o_xc), p->d(p->o_yc), p->d(p->o_ct), p->d(p->o_cb),
+                                            p->d(p->o_mzt));
   const sgh_config& c = p->cfg;
   const double alpha = c.k / (c.rho * c.cp);
   k_propagators<<<cdiv(h.V, EW_THREADS), EW_THREADS, 0, s>>>(p->P(), alpha, c.rho * c.cp, p->d(p->o_K),
@@ -1022,7 +1130,7 @@ int sgh_dctn(int32_t kind, int32_t ndim, const int32_t* shape, const double* in,
     const int N = L.n[a];
     const int A = (a == 2) ? n0 * n1 : (a == 1 ? n0 : 1);
     const int B = (a == 2) ? 1 : (a == 1 ? n2 : n1 * n2);
-    launch_axis(src, mats[a], N, A, B, EpiStore{dst, 1.0, nullptr}, s);
+    launch_axis(src, mats[a], N, N, A, B, EpiStore{dst, 1.0, nullptr}, s);
     src = dst;
   }
   SGH_CK(cudaGetLastError());

@@ -30,6 +30,8 @@ struct DevParams {
   double L_f;
   double r_x, r_y, absorptivity, order, area_factor;
   double omega, tol;
+  int affine[P_COUNT];       // program reduces to aff_a + aff_b * T (host analysis)
+  double aff_a[P_COUNT], aff_b[P_COUNT];
   sgh_program prog[P_COUNT];
 };
 
@@ -94,6 +96,13 @@ __device__ __forceinline__ double eval_program(const sgh_program& p, double T) {
   return sp > 0 ? st[0] : nan("");
 }
 
+// One property branch: affine programs (the common piecewise-linear tables)
+// take one FMA; anything else runs the postfix interpreter.
+__device__ __forceinline__ double prop(const DevParams& P, int slot, double T) {
+  if (P.affine[slot]) return fma(P.aff_b[slot], T, P.aff_a[slot]);
+  return eval_program(P.prog[slot], T);
+}
+
 // Liquid fraction as the fused kernels compute it: clip((T - T_s) * inv, 0, 1),
 // a step at T_s for a degenerate band (core/properties.py:175-183, 218-229).
 __device__ __forceinline__ double fl_kernel(const DevParams& P, double T) {
@@ -105,9 +114,9 @@ __device__ __forceinline__ double fl_kernel(const DevParams& P, double T) {
 // k(T) as TempProperty.__call__ evaluates it (core/properties.py:96-103,
 // liquid_fraction :61-77 by division).
 __device__ __forceinline__ double k_blended(const DevParams& P, double T) {
-  const double ks = eval_program(P.prog[P_K_SOLID], T);
+  const double ks = prop(P, P_K_SOLID, T);
   if (P.k_constant) return ks;
-  const double kl = eval_program(P.prog[P_K_LIQUID], T);
+  const double kl = prop(P, P_K_LIQUID, T);
   double fl;
   if (P.degenerate_band) {
     fl = T >= P.T_solidus ? 1.0 : 0.0;
@@ -122,7 +131,7 @@ __device__ __forceinline__ double k_blended(const DevParams& P, double T) {
 __device__ __forceinline__ double k_prime(const DevParams& P, double T) {
   const double fl = fl_kernel(P, T);
   const double om = 1.0 - fl;
-  const double kv = om * eval_program(P.prog[P_K_SOLID], T) + fl * eval_program(P.prog[P_K_LIQUID], T);
+  const double kv = om * prop(P, P_K_SOLID, T) + fl * prop(P, P_K_LIQUID, T);
   return kv - P.kbar;
 }
 
@@ -130,8 +139,8 @@ __device__ __forceinline__ double k_prime(const DevParams& P, double T) {
 __device__ __forceinline__ double a_prime(const DevParams& P, double T) {
   const double fl = fl_kernel(P, T);
   const double om = 1.0 - fl;
-  const double rv = om * eval_program(P.prog[P_RHO_SOLID], T) + fl * eval_program(P.prog[P_RHO_LIQUID], T);
-  const double cv = om * eval_program(P.prog[P_C_SOLID], T) + fl * eval_program(P.prog[P_C_LIQUID], T);
+  const double rv = om * prop(P, P_RHO_SOLID, T) + fl * prop(P, P_RHO_LIQUID, T);
+  const double cv = om * prop(P, P_C_SOLID, T) + fl * prop(P, P_C_LIQUID, T);
   return rv * cv - P.abar;
 }
 
@@ -143,7 +152,7 @@ __device__ __forceinline__ double latent_source(const DevParams& P, double T, do
     const double flc = fl_kernel(P, T);
     const double flp = fl_kernel(P, Tp);
     const double om = 1.0 - flc;
-    const double rho = om * eval_program(P.prog[P_RHO_SOLID], T) + flc * eval_program(P.prog[P_RHO_LIQUID], T);
+    const double rho = om * prop(P, P_RHO_SOLID, T) + flc * prop(P, P_RHO_LIQUID, T);
     return -rho * P.L_f * (flc - flp) * P.inv_dt;
   }
   double fc = (T - P.T_solidus) * P.band_inv;
