@@ -49,8 +49,8 @@ import numpy as np  # noqa: E402
 METRIC = "timesteps/s"
 L2_FLUSH_BYTES = 256 << 20
 # dram__bytes_read.sum + dram__bytes_write.sum per launch of the dominant kernel
-# (k_axis, x-pass of the 128x64x32 transform) from the ncu capture summarised in
-# profiles/k_axis_raster_128x64x32.md; None until that capture exists.
+# (k_axis on the 128x64x32 transform) from an ncu capture of this workload;
+# None until that capture exists.
 NCU_TRAFFIC_BYTES = None
 
 
