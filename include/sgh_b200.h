@@ -206,6 +206,31 @@ int sgh_dctn_workspace_bytes(int32_t ndim, const int32_t* shape, uint64_t* bytes
 int sgh_dctn(int32_t kind, int32_t ndim, const int32_t* shape, const double* in, double* out,
              void* workspace, uint64_t bytes, void* stream);
 
+/* sgh_dctn without a workspace argument, for callers that hold device arrays
+ * but cannot allocate device memory themselves -- for example a plain
+ * ctypes/FFI host that has no CUDA array library to allocate with, or an
+ * application whose memory manager owns the whole device and allows no other
+ * allocation. No counterpart in the reference (its DCT_II / IDCT_II allocate
+ * freely through NumPy/CuPy).
+ *
+ * Same transform, arguments and result as sgh_dctn. Its scratch is a fixed
+ * array inside the library's device module, SGH_NOALLOC_SCRATCH_BYTES bytes
+ * on every GPU that loads the library, held until the process exits; it calls
+ * no cudaMalloc/cudaFree and no allocating library routine. An array whose
+ * sgh_dctn_workspace_bytes() exceeds that size is rejected with
+ * SGH_ERR_WORKSPACE (about 10^6 elements for a 3-D array).
+ *
+ * The first call on a device looks up the scratch's device address
+ * (cudaGetSymbolAddress) and caches it; make that first call before any
+ * stream capture. All calls share the one scratch array: calls that overlap
+ * on the GPU (different streams, or several threads) race and must be
+ * serialised by the caller. The scratch keeps the previous call's contents;
+ * this transform writes every scratch element it reads, so none needs
+ * clearing. Async. */
+#define SGH_NOALLOC_SCRATCH_BYTES (16ull << 20)
+int sgh_dctn_noalloc(int32_t kind, int32_t ndim, const int32_t* shape, const double* in, double* out,
+                     void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -29,7 +29,7 @@ EXPORTED = (
     "sgh_abi_version", "sgh_last_error", "sgh_plan_create", "sgh_plan_destroy",
     "sgh_plan_workspace_bytes", "sgh_plan_bind", "sgh_plan_buffer", "sgh_plan_launch_counts", "sgh_state_reset",
     "sgh_step", "sgh_step_eager", "sgh_run", "sgh_dct3d", "sgh_surface_temperature", "sgh_project_volume",
-    "sgh_reconstruct_volume", "sgh_dctn_workspace_bytes", "sgh_dctn",
+    "sgh_reconstruct_volume", "sgh_dctn_workspace_bytes", "sgh_dctn", "sgh_dctn_noalloc",
 )
 
 
@@ -112,6 +112,7 @@ def lib() -> C.CDLL:
             "sgh_reconstruct_volume": ([vp, vp, vp, vp], C.c_int),
             "sgh_dctn_workspace_bytes": ([i32, C.POINTER(i32), u64p], C.c_int),
             "sgh_dctn": ([i32, i32, C.POINTER(i32), vp, vp, vp, C.c_uint64, vp], C.c_int),
+            "sgh_dctn_noalloc": ([i32, i32, C.POINTER(i32), vp, vp, vp], C.c_int),
         }
         for name, (args, res) in sig.items():
             fn = getattr(L, name)

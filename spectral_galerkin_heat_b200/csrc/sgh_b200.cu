@@ -23,6 +23,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <mutex>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -1122,6 +1123,86 @@ int sgh_dctn(int32_t kind, int32_t ndim, const int32_t* shape, const double* in,
   double* bufs[2] = {t1, t2};
   int nb = 0;
   if (L.ndim == 1 && in == out) {  // a single pass must not read what it writes
+    SGH_CK(cudaMemcpyAsync(t2, in, sizeof(double) * (size_t)n2, cudaMemcpyDeviceToDevice, s));
+    src = t2;
+  }
+  for (int a = 2; a >= first; --a) {
+    double* dst = (a == first) ? out : bufs[nb++ & 1];
+    const int N = L.n[a];
+    const int A = (a == 2) ? n0 * n1 : (a == 1 ? n0 : 1);
+    const int B = (a == 2) ? 1 : (a == 1 ? n2 : n1 * n2);
+    launch_axis(src, mats[a], N, N, A, B, EpiStore{dst, 1.0, nullptr}, s);
+    src = dst;
+  }
+  SGH_CK(cudaGetLastError());
+  return SGH_OK;
+}
+
+// ---------------------------------------------------------------------------
+// allocation-free DCT
+// ---------------------------------------------------------------------------
+// Scratch of sgh_dctn_noalloc: a fixed array in the module's global memory.
+// Every device that loads the library holds it (SGH_NOALLOC_SCRATCH_BYTES)
+// until the process exits. The host reaches it only through the address that
+// cudaGetSymbolAddress returns for the current device; the symbol name itself
+// is not a device address in host code.
+static __device__ __align__(256) double g_noalloc_scratch[SGH_NOALLOC_SCRATCH_BYTES / sizeof(double)];
+
+namespace {
+constexpr int kMaxNoallocDevices = 64;
+std::mutex g_noalloc_mutex;
+void* g_noalloc_ptr[kMaxNoallocDevices] = {};
+
+// Device address of g_noalloc_scratch on the current device, looked up once per
+// device (first call on that device) and cached.
+int noalloc_scratch(void** out) {
+  int dev = -1;
+  SGH_CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxNoallocDevices) return fail(SGH_ERR_UNSUPPORTED, "device ordinal out of range");
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (!g_noalloc_ptr[dev]) {
+    void* ptr = nullptr;
+    SGH_CK(cudaGetSymbolAddress(&ptr, g_noalloc_scratch));
+    if (!ptr) return fail(SGH_ERR_CUDA, "cudaGetSymbolAddress returned a null scratch address");
+    g_noalloc_ptr[dev] = ptr;
+  }
+  *out = g_noalloc_ptr[dev];
+  return SGH_OK;
+}
+}  // namespace
+
+int sgh_dctn_noalloc(int32_t kind, int32_t ndim, const int32_t* shape, const double* in, double* out,
+                     void* stream) {
+  if (!in || !out) return fail(SGH_ERR_INVALID, "null argument");
+  if (kind != 2 && kind != 3) return fail(SGH_ERR_INVALID, "kind must be 2 (DCT_II) or 3 (IDCT_II)");
+  DctnLayout L;
+  const int rc = dctn_layout(ndim, shape, &L);
+  if (rc) return rc;
+  if (L.total > SGH_NOALLOC_SCRATCH_BYTES)
+    return fail(SGH_ERR_WORKSPACE,
+                "array too large for sgh_dctn_noalloc: needs " + std::to_string(L.total) +
+                    " bytes of scratch, the built-in scratch holds " +
+                    std::to_string((unsigned long long)SGH_NOALLOC_SCRATCH_BYTES) + "; use sgh_dctn");
+  void* scratch = nullptr;
+  const int rs = noalloc_scratch(&scratch);
+  if (rs) return rs;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  char* ws = static_cast<char*>(scratch);
+  const double* mats[3];
+  for (int a = 0; a < 3; ++a) {
+    const int N = L.n[a];
+    double* M = reinterpret_cast<double*>(ws + L.o_mat[a]);
+    k_dct_matrix<<<cdiv((long)N * N, EW_THREADS), EW_THREADS, 0, s>>>(N, M, M + (size_t)N * N);
+    mats[a] = (kind == 2) ? M : M + (size_t)N * N;
+  }
+  double* t1 = reinterpret_cast<double*>(ws + L.o_t1);
+  double* t2 = reinterpret_cast<double*>(ws + L.o_t2);
+  const int n0 = L.n[0], n1 = L.n[1], n2 = L.n[2];
+  const int first = 3 - L.ndim;
+  const double* src = in;
+  double* bufs[2] = {t1, t2};
+  int nb = 0;
+  if (L.ndim == 1 && in == out) {
     SGH_CK(cudaMemcpyAsync(t2, in, sizeof(double) * (size_t)n2, cudaMemcpyDeviceToDevice, s));
     src = t2;
   }
