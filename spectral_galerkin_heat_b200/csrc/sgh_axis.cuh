@@ -10,11 +10,12 @@
 // passes give scipy.fft.dctn(type=2|3, norm='ortho') over all axes
 // (physics/spectral_cpu_kernels.py:374-389), two passes the face transform.
 //
-// Tiling: 256 threads, BK = 16 contraction slices staged in shared memory per
-// iteration; each thread owns a 2 x 4 register tile. When B == 1 (the
-// transformed axis is the contiguous one) the 4-wide fast dimension of the
-// thread tile runs along k so that the epilogue stores are coalesced; when
-// B > 1 it runs along c (= b, contiguous).
+// Tiling: 256 threads; contraction slices stream through a 3-stage cp.async
+// pipeline of 16-slice stages in shared memory; each thread owns a 2 x 4
+// register tile (1 x 1 for passes too small to fill the SMs otherwise). When
+// B == 1 (the transformed axis is the contiguous one) the fast dimension of
+// the thread tile runs along k so that the epilogue stores are coalesced;
+// when B > 1 it runs along c (= b, contiguous).
 //
 // The epilogue functor receives (linear output index (a*Nout + k)*B + b, k, b,
 // value) and may accumulate two partial sums or a max that are reduced per CTA
@@ -25,20 +26,33 @@
 namespace sgh {
 
 constexpr int AX_THREADS = 256;
-constexpr int AX_BK = 16;
+constexpr int AX_BK = 16;      // contraction slices per pipeline stage
+constexpr int AX_STAGES = 3;   // cp.async pipeline depth
 
 struct Red {
   double s0 = 0.0, s1 = 0.0, mx = -INFINITY;
 };
 
-template <bool CONTIG, class Epi>
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem, int src_bytes) {
+  const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(gmem), "r"(src_bytes));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+// 16 x 16 threads; each owns a TI (slow) x TJ (fast) register tile. The fast
+// thread index runs along the contiguous output dimension: k when B == 1
+// (CONTIG), c otherwise. Mat and X panels stream through an AX_STAGES-deep
+// cp.async pipeline of AX_BK-slice stages (out-of-range elements zero-filled).
+template <bool CONTIG, int TI, int TJ, class Epi>
 __global__ void __launch_bounds__(AX_THREADS)
 k_axis(const double* __restrict__ X, const double* __restrict__ Mat, int Nout, int N, int A, int B,
        Epi epi) {
-  constexpr int TK = CONTIG ? 64 : 32;   // outputs along the transformed axis per CTA
-  constexpr int TC = CONTIG ? 32 : 64;   // outputs along c per CTA
-  __shared__ double Ms[AX_BK][TK + 1];
-  __shared__ double Xs[AX_BK][TC + 1];
+  constexpr int TK = CONTIG ? 16 * TJ : 16 * TI;  // outputs along the transformed axis per CTA
+  constexpr int TC = CONTIG ? 16 * TI : 16 * TJ;  // outputs along c per CTA
+  __shared__ double Ms[AX_STAGES][AX_BK][TK + 1];
+  __shared__ double Xs[AX_STAGES][AX_BK][TC + 1];
   __shared__ double red_sh[2 * (AX_THREADS / 32)];
 
   const int tid = threadIdx.x;
@@ -47,77 +61,89 @@ k_axis(const double* __restrict__ X, const double* __restrict__ Mat, int Nout, i
   const int ncol = A * B;
   const int c0 = blockIdx.x * TC;
   const int k0 = blockIdx.y * TK;
+  const int nchunks = (N + AX_BK - 1) / AX_BK;
 
-  double acc[2][4];
-#pragma unroll
-  for (int i = 0; i < 2; ++i)
-#pragma unroll
-    for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
-
-  for (int n0 = 0; n0 < N; n0 += AX_BK) {
-    // Mat tile: rows k0..k0+TK-1, columns n0..n0+15 (row-contiguous loads)
-#pragma unroll
+  auto issue = [&](int stage, int n0) {
     for (int e = tid; e < TK * AX_BK; e += AX_THREADS) {
-      const int kr = e >> 4, kk = e & 15;
+      const int kr = e / AX_BK, kk = e % AX_BK;
       const int k = k0 + kr, n = n0 + kk;
-      Ms[kk][kr] = (k < Nout && n < N) ? __ldg(Mat + (size_t)k * N + n) : 0.0;
+      const bool ok = k < Nout && n < N;
+      cp_async8(&Ms[stage][kk][kr], ok ? Mat + (size_t)k * N + n : Mat, ok ? 8 : 0);
     }
-    // X tile: slices n0..n0+15, columns c0..c0+TC-1
     if (CONTIG) {
-#pragma unroll
       for (int e = tid; e < TC * AX_BK; e += AX_THREADS) {
-        const int cr = e >> 4, kk = e & 15;
+        const int cr = e / AX_BK, kk = e % AX_BK;
         const int c = c0 + cr, n = n0 + kk;
-        Xs[kk][cr] = (c < ncol && n < N) ? X[(size_t)c * N + n] : 0.0;
+        const bool ok = c < ncol && n < N;
+        cp_async8(&Xs[stage][kk][cr], ok ? X + (size_t)c * N + n : X, ok ? 8 : 0);
       }
     } else {
-#pragma unroll
       for (int e = tid; e < TC * AX_BK; e += AX_THREADS) {
         const int cr = e % TC, kk = e / TC;
         const int c = c0 + cr, n = n0 + kk;
-        double v = 0.0;
-        if (c < ncol && n < N) {
+        const bool ok = c < ncol && n < N;
+        const double* src = X;
+        if (ok) {
           const int a = c / B, b = c - a * B;
-          v = X[((size_t)a * N + n) * B + b];
+          src = X + ((size_t)a * N + n) * B + b;
         }
-        Xs[kk][cr] = v;
+        cp_async8(&Xs[stage][kk][cr], src, ok ? 8 : 0);
       }
     }
+    cp_async_commit();
+  };
+
+  double acc[TI][TJ];
+#pragma unroll
+  for (int i = 0; i < TI; ++i)
+#pragma unroll
+    for (int j = 0; j < TJ; ++j) acc[i][j] = 0.0;
+
+#pragma unroll
+  for (int st = 0; st < AX_STAGES - 1; ++st) {
+    if (st < nchunks) issue(st, st * AX_BK);
+    else cp_async_commit();
+  }
+  for (int ch = 0; ch < nchunks; ++ch) {
+    cp_async_wait<AX_STAGES - 2>();
     __syncthreads();
+    const int nxt = ch + AX_STAGES - 1;
+    if (nxt < nchunks) issue(nxt % AX_STAGES, nxt * AX_BK);
+    else cp_async_commit();
+    const int stg = ch % AX_STAGES;
 #pragma unroll
     for (int kk = 0; kk < AX_BK; ++kk) {
+      double m[CONTIG ? TJ : TI], x[CONTIG ? TI : TJ];
       if (CONTIG) {
-        double m[4], x[2];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) m[j] = Ms[kk][f + 16 * j];
+        for (int j = 0; j < TJ; ++j) m[j] = Ms[stg][kk][f + 16 * j];
 #pragma unroll
-        for (int i = 0; i < 2; ++i) x[i] = Xs[kk][2 * s + i];
+        for (int i = 0; i < TI; ++i) x[i] = Xs[stg][kk][TI * s + i];
 #pragma unroll
-        for (int i = 0; i < 2; ++i)
+        for (int i = 0; i < TI; ++i)
 #pragma unroll
-          for (int j = 0; j < 4; ++j) acc[i][j] = fma(m[j], x[i], acc[i][j]);
+          for (int j = 0; j < TJ; ++j) acc[i][j] = fma(m[j], x[i], acc[i][j]);
       } else {
-        double m[2], x[4];
 #pragma unroll
-        for (int i = 0; i < 2; ++i) m[i] = Ms[kk][2 * s + i];
+        for (int i = 0; i < TI; ++i) m[i] = Ms[stg][kk][TI * s + i];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) x[j] = Xs[kk][f + 16 * j];
+        for (int j = 0; j < TJ; ++j) x[j] = Xs[stg][kk][f + 16 * j];
 #pragma unroll
-        for (int i = 0; i < 2; ++i)
+        for (int i = 0; i < TI; ++i)
 #pragma unroll
-          for (int j = 0; j < 4; ++j) acc[i][j] = fma(m[i], x[j], acc[i][j]);
+          for (int j = 0; j < TJ; ++j) acc[i][j] = fma(m[i], x[j], acc[i][j]);
       }
     }
-    __syncthreads();
   }
+  cp_async_wait<0>();
 
   Red r;
 #pragma unroll
-  for (int i = 0; i < 2; ++i) {
+  for (int i = 0; i < TI; ++i) {
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const int k = CONTIG ? (k0 + f + 16 * j) : (k0 + 2 * s + i);
-      const int c = CONTIG ? (c0 + 2 * s + i) : (c0 + f + 16 * j);
+    for (int j = 0; j < TJ; ++j) {
+      const int k = CONTIG ? (k0 + f + 16 * j) : (k0 + TI * s + i);
+      const int c = CONTIG ? (c0 + TI * s + i) : (c0 + f + 16 * j);
       if (k < Nout && c < ncol) {
         const int a = c / B, b = c - a * B;
         const int idx = (a * Nout + k) * B + b;
@@ -144,22 +170,42 @@ k_axis(const double* __restrict__ X, const double* __restrict__ Mat, int Nout, i
   }
 }
 
+// Launch shape of one pass: the 2 x 4 thread tile when it yields enough CTAs
+// to cover the SMs, else the 1 x 1 tile (small faces, short axes).
+struct AxisShape {
+  bool big;
+  dim3 grid;
+};
+constexpr int AX_MIN_CTAS = 132;
+inline AxisShape axis_shape(int Nout, int A, int B) {
+  const int ncol = A * B;
+  auto grid_of = [&](int ti, int tj) {
+    const int tk = (B == 1) ? 16 * tj : 16 * ti;
+    const int tc = (B == 1) ? 16 * ti : 16 * tj;
+    return dim3((ncol + tc - 1) / tc, (Nout + tk - 1) / tk);
+  };
+  const dim3 g = grid_of(2, 4);
+  if ((long)g.x * g.y >= AX_MIN_CTAS) return {true, g};
+  return {false, grid_of(1, 1)};
+}
+
 // Number of CTAs of one pass (the number of partials a reducing epilogue writes).
 inline int axis_blocks(int Nout, int A, int B) {
-  if (B == 1) return ((A + 31) / 32) * ((Nout + 63) / 64);
-  return ((A * B + 63) / 64) * ((Nout + 31) / 32);
+  const AxisShape sh = axis_shape(Nout, A, B);
+  return (int)(sh.grid.x * sh.grid.y);
 }
 
 // One pass with Mat of Nout x N (N = contraction length).
 template <class Epi>
 inline void launch_axis(const double* X, const double* Mat, int Nout, int N, int A, int B,
                         const Epi& epi, cudaStream_t st) {
+  const AxisShape sh = axis_shape(Nout, A, B);
   if (B == 1) {
-    dim3 grid((A + 31) / 32, (Nout + 63) / 64);
-    k_axis<true, Epi><<<grid, AX_THREADS, 0, st>>>(X, Mat, Nout, N, A, B, epi);
+    if (sh.big) k_axis<true, 2, 4, Epi><<<sh.grid, AX_THREADS, 0, st>>>(X, Mat, Nout, N, A, B, epi);
+    else k_axis<true, 1, 1, Epi><<<sh.grid, AX_THREADS, 0, st>>>(X, Mat, Nout, N, A, B, epi);
   } else {
-    dim3 grid((A * B + 63) / 64, (Nout + 31) / 32);
-    k_axis<false, Epi><<<grid, AX_THREADS, 0, st>>>(X, Mat, Nout, N, A, B, epi);
+    if (sh.big) k_axis<false, 2, 4, Epi><<<sh.grid, AX_THREADS, 0, st>>>(X, Mat, Nout, N, A, B, epi);
+    else k_axis<false, 1, 1, Epi><<<sh.grid, AX_THREADS, 0, st>>>(X, Mat, Nout, N, A, B, epi);
   }
 }
 
@@ -174,6 +220,15 @@ struct EpiStore {
   double mul;
   double* partials;
   __device__ __forceinline__ void operator()(int i, int, int, double v, Red&) const { out[i] = v * mul; }
+};
+
+// out += v * mul (accumulate a face source into a face state)
+struct EpiAdd {
+  static constexpr int kReduce = 0;
+  double* out;
+  double mul;
+  double* partials;
+  __device__ __forceinline__ void operator()(int i, int, int, double v, Red&) const { out[i] += v * mul; }
 };
 
 // out = v / div (reconstruct_volume: IDCT_II(a) / sqrt_dV, spectral_ops.py:83-91)

@@ -52,6 +52,10 @@ int fail(int code, const std::string& msg) {
       return fail(SGH_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));      \
   } while (0)
 
+// In the void enqueue helpers a failed async call is reported by the
+// cudaGetLastError / capture-end checks of the caller.
+#define SGH_CK_VOID(call) (void)(call)
+
 constexpr int EW_THREADS = 256;
 
 inline int cdiv(long a, long b) { return (int)((a + b - 1) / b); }
@@ -328,13 +332,15 @@ k_stencil(const DevParams* __restrict__ P, const double* __restrict__ T, const d
 // err = sqrt(sum res^2 / n) / max(sqrt(sum a_old^2 / n), 1e-9).
 __global__ void __launch_bounds__(EW_THREADS)
 k_converge(const DevParams* __restrict__ P, Ctrl* ctrl, const double* __restrict__ partials,
-           int nparts, cudaGraphConditionalHandle h_picard, int in_graph) {
+           int nparts, const double* __restrict__ extra_old, int n_extra,
+           cudaGraphConditionalHandle h_picard, int in_graph) {
   __shared__ double sh[2 * (EW_THREADS / 32)];
   double s0 = 0.0, s1 = 0.0;
   for (int b = threadIdx.x; b < nparts; b += EW_THREADS) {
     s0 += partials[2 * b];
     s1 += partials[2 * b + 1];
   }
+  for (int b = threadIdx.x; b < n_extra; b += EW_THREADS) s1 += extra_old[b];
   block_sum2<EW_THREADS>(s0, s1, sh);
   if (threadIdx.x == 0) {
     const double n = P->n_elements;
@@ -391,6 +397,128 @@ k_commit(const DevParams* __restrict__ P, Ctrl* ctrl, const double* __restrict__
   }
 }
 
+// ---------------------------------------------------------------------------
+// face-space Picard (no latent heat, no property correction)
+// ---------------------------------------------------------------------------
+// Without the volume forcing terms every iterate of the step is
+//   a_it = aK + KK (Ct[p] sigma[y,x] + Cb[p] beta[y,x])
+// with face fields sigma (top) and beta (bottom): the initial guess
+// (solvers/spectral.py:320-351), each trial (:431-443) and each relaxation
+// (:459-462) keep that form. The surface temperatures, the residual and the
+// norm of the iterate then reduce to face fields built once per step from the
+// modes, and the Picard loop runs on faces only. Per step the volume is read
+// twice and written once, whatever the iteration count.
+
+// Constant face weights of KK (bind time):
+// W_tt = sum Ct^2 KK, W_tb = sum Ct Cb KK, W_bb = sum Cb^2 KK,
+// Q_tt = sum (KK Ct)^2, Q_tb = sum KK^2 Ct Cb, Q_bb = sum (KK Cb)^2.
+__global__ void __launch_bounds__(EW_THREADS)
+k_fs_weights(const DevParams* __restrict__ P, const double* __restrict__ KK, const double* __restrict__ Ct,
+             const double* __restrict__ Cb, double* W) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int S = P->S;
+  if (i >= S) return;
+  double wtt = 0, wtb = 0, wbb = 0, qtt = 0, qtb = 0, qbb = 0;
+  for (int p = 0; p < P->nz; ++p) {
+    const double kk = KK[(size_t)p * S + i], ct = Ct[p], cb = Cb[p];
+    wtt += ct * ct * kk;
+    wtb += ct * cb * kk;
+    wbb += cb * cb * kk;
+    qtt += (kk * ct) * (kk * ct);
+    qtb += kk * kk * ct * cb;
+    qbb += (kk * cb) * (kk * cb);
+  }
+  W[0 * S + i] = wtt; W[1 * S + i] = wtb; W[2 * S + i] = wbb;
+  W[3 * S + i] = qtt; W[4 * S + i] = qtb; W[5 * S + i] = qbb;
+}
+
+// Per step: with aK = K a (not stored), the face fields
+// Zt = sum Ct aK, Zb = sum Cb aK, Yt = sum aK KK Ct, Yb = sum aK KK Cb, and
+// per-CTA partial sums of aK^2. Also opens the face state: sigma = beta = 0.
+__global__ void __launch_bounds__(EW_THREADS)
+k_fs_pass1(const DevParams* __restrict__ P, const double* __restrict__ a, const double* __restrict__ K,
+           const double* __restrict__ KK, const double* __restrict__ Ct, const double* __restrict__ Cb,
+           double* F, double* n1_parts) {
+  __shared__ double sh[2 * (EW_THREADS / 32)];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int S = P->S;
+  double n1 = 0.0, dummy = 0.0;
+  if (i < S) {
+    double zt = 0, zb = 0, yt = 0, yb = 0;
+    for (int p = 0; p < P->nz; ++p) {
+      const size_t j = (size_t)p * S + i;
+      const double ak = a[j] * K[j];
+      const double kk = KK[j];
+      zt = fma(Ct[p], ak, zt);
+      zb = fma(Cb[p], ak, zb);
+      yt = fma(ak * kk, Ct[p], yt);
+      yb = fma(ak * kk, Cb[p], yb);
+      n1 = fma(ak, ak, n1);
+    }
+    F[0 * S + i] = zt; F[1 * S + i] = zb; F[2 * S + i] = yt; F[3 * S + i] = yb;
+  }
+  block_sum2<EW_THREADS>(n1, dummy, sh);
+  if (threadIdx.x == 0) n1_parts[blockIdx.x] = n1;
+}
+
+// Face inputs of the two surface reconstructions of the current iterate:
+// At = Zt + W_tt sigma + W_tb beta (top), Ab = Zb + W_tb sigma + W_bb beta (bottom).
+__global__ void __launch_bounds__(EW_THREADS)
+k_fs_assemble(const DevParams* __restrict__ P, const double* __restrict__ F, const double* __restrict__ W,
+              const double* __restrict__ sigma, const double* __restrict__ beta, double* At, double* Ab) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int S = P->S;
+  if (i >= S) return;
+  const double sg = sigma[i], bt = beta[i];
+  At[i] = F[0 * S + i] + W[0 * S + i] * sg + W[1 * S + i] * bt;
+  if (Ab) Ab[i] = F[1 * S + i] + W[1 * S + i] * sg + W[2 * S + i] * bt;
+}
+
+// Face state update of one Picard iteration: trial S_top (and fixed S_bot),
+// residual and iterate norms from the constant weights, relaxation of sigma
+// and beta, and the top reconstruction input of the relaxed iterate.
+__global__ void __launch_bounds__(EW_THREADS)
+k_fs_relax(const DevParams* __restrict__ P, const double* __restrict__ F, const double* __restrict__ W,
+           const double* __restrict__ S_top, const double* __restrict__ S_bot, double* sigma, double* beta,
+           double* At, double* partials) {
+  __shared__ double sh[2 * (EW_THREADS / 32)];
+  const int S = P->S;
+  const double om = P->omega;
+  double r2 = 0.0, o2 = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < S; i += gridDim.x * blockDim.x) {
+    const double sg = sigma[i], bt = beta[i];
+    const double dt_ = S_top[i] - sg;
+    const double db_ = (S_bot ? S_bot[i] : 0.0) - bt;
+    const double qtt = W[3 * S + i], qtb = W[4 * S + i], qbb = W[5 * S + i];
+    r2 += dt_ * dt_ * qtt + 2.0 * dt_ * db_ * qtb + db_ * db_ * qbb;
+    o2 += 2.0 * (sg * F[2 * S + i] + bt * F[3 * S + i]) + sg * sg * qtt + 2.0 * sg * bt * qtb +
+          bt * bt * qbb;
+    const double ns = dt_ * om + sg;
+    const double nb = db_ * om + bt;
+    sigma[i] = ns;
+    beta[i] = nb;
+    At[i] = F[0 * S + i] + W[0 * S + i] * ns + W[1 * S + i] * nb;
+  }
+  block_sum2<EW_THREADS>(r2, o2, sh);
+  if (threadIdx.x == 0) {
+    partials[2 * blockIdx.x] = r2;
+    partials[2 * blockIdx.x + 1] = o2;
+  }
+}
+
+// Commit of the modes: a = K a + KK (Ct sigma + Cb beta).
+__global__ void __launch_bounds__(EW_THREADS)
+k_fs_commit_modes(const DevParams* __restrict__ P, double* a, const double* __restrict__ K,
+                  const double* __restrict__ KK, const double* __restrict__ Ct, const double* __restrict__ Cb,
+                  const double* __restrict__ sigma, const double* __restrict__ beta) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= P->V) return;
+  const int S = P->S;
+  const int z = i / S, yx = i - z * S;
+  const double kk = KK[i];
+  a[i] = a[i] * K[i] + kk * (Ct[z] * sigma[yx] + Cb[z] * beta[yx]);
+}
+
 // Aligned sub-allocation of the caller's workspace.
 struct Layout {
   size_t off = 0;
@@ -416,6 +544,10 @@ struct sgh_plan {
   size_t o_K, o_KK, o_a, o_aK, o_trial, o_Tprev, o_Qm, o_t1, o_t2, o_vol, o_kp;
   size_t o_qlas, o_qnet, o_qev, o_qevold, o_Stop, o_Sbot, o_f1, o_f2, o_Tsurf, o_A;
   size_t o_prelax, o_plas, o_psurf;
+  // face-space Picard state: F (Zt, Zb, Yt, Yb), W (6 weights), sigma, beta, Ab, n1 partials
+  bool face_space = false;
+  int nparts_fs = 0, nparts_n1 = 0;
+  size_t o_fsF = 0, o_fsW = 0, o_sigma = 0, o_beta = 0, o_Ab = 0, o_pn1 = 0;
   size_t ws_need = 0;
   char* ws = nullptr;
   bool bound = false;
@@ -543,10 +675,23 @@ inline void axis(const double* X, const double* Mat, int Nout, int N, int A, int
   ++g_launches;
 }
 
-void face_dct2(sgh_plan* p, const double* in, double* out, double scale, cudaStream_t s) {
+template <class Epi>
+void face_dct2_epi(sgh_plan* p, const double* in, const Epi& epi, cudaStream_t s) {
   const DevParams& h = p->hp;
   axis(in, p->d(p->o_mx), h.nx, h.nx, h.ny, 1, EpiStore{p->d(p->o_f1), 1.0, nullptr}, s);
-  axis(p->d(p->o_f1), p->d(p->o_my), h.ny, h.ny, 1, h.nx, EpiStore{out, scale, nullptr}, s);
+  axis(p->d(p->o_f1), p->d(p->o_my), h.ny, h.ny, 1, h.nx, epi, s);
+}
+
+void face_dct2(sgh_plan* p, const double* in, double* out, double scale, cudaStream_t s) {
+  face_dct2_epi(p, in, EpiStore{out, scale, nullptr}, s);
+}
+
+// Face IDCT2 of a prepared face input A (no z-sum).
+template <class Epi>
+void face_idct2_from(sgh_plan* p, const double* A, const Epi& epi, cudaStream_t s) {
+  const DevParams& h = p->hp;
+  axis(A, p->d(p->o_mxt), h.nx, h.nx, h.ny, 1, EpiStore{p->d(p->o_f1), 1.0, nullptr}, s);
+  axis(p->d(p->o_f1), p->d(p->o_myt), h.ny, h.ny, 1, h.nx, epi, s);
 }
 
 template <class Epi>
@@ -576,6 +721,59 @@ void volume_pass3(sgh_plan* p, const double* in, bool inverse, const Epi& epi, d
   axis(t2, mz, z_rows, h.nz, 1, h.S, epi, s);
 }
 
+void enqueue_pre_face_space(sgh_plan* p, cudaStream_t s) {
+  const DevParams& h = p->hp;
+  DevParams* P = p->P();
+  const int gS = cdiv(h.S, EW_THREADS);
+  double* F = p->d(p->o_fsF);
+  double* W = p->d(p->o_fsW);
+  double* sg = p->d(p->o_sigma);
+  double* bt = p->d(p->o_beta);
+  double* At = p->d(p->o_A);
+  double* Ab = p->d(p->o_Ab);
+  k_fs_pass1<<<gS, EW_THREADS, 0, s>>>(P, p->d(p->o_a), p->d(p->o_K), p->d(p->o_KK), p->d(p->o_ct),
+                                        p->d(p->o_cb), F, p->d(p->o_pn1));
+  ++g_launches;
+  SGH_CK_VOID(cudaMemsetAsync(bt, 0, sizeof(double) * h.S, s));
+  face_dct2(p, p->d(p->o_qnet), sg, h.dct_scale, s);  // initial guess sigma = S_top
+  if (h.has_top_conv) {
+    k_fs_assemble<<<gS, EW_THREADS, 0, s>>>(P, F, W, sg, bt, At, nullptr);
+    ++g_launches;
+    face_idct2_from(p, At, EpiConvFace{P, h.h_top, 0, p->d(p->o_f2), nullptr}, s);
+    face_dct2_epi(p, p->d(p->o_f2), EpiAdd{sg, h.dct_scale, nullptr}, s);
+  }
+  if (h.has_bottom_conv) {
+    k_fs_assemble<<<gS, EW_THREADS, 0, s>>>(P, F, W, sg, bt, At, Ab);
+    ++g_launches;
+    face_idct2_from(p, Ab, EpiConvFace{P, h.h_bottom, 0, p->d(p->o_f2), nullptr}, s);
+    face_dct2_epi(p, p->d(p->o_f2), EpiAdd{bt, h.dct_scale, nullptr}, s);
+    // S_bot_raw, held fixed through the Picard loop (solvers/spectral.py:373-379)
+    k_fs_assemble<<<gS, EW_THREADS, 0, s>>>(P, F, W, sg, bt, At, Ab);
+    ++g_launches;
+    face_idct2_from(p, Ab, EpiConvFace{P, h.h_bottom, 0, p->d(p->o_f2), nullptr}, s);
+    face_dct2(p, p->d(p->o_f2), p->d(p->o_Sbot), h.dct_scale, s);
+  }
+  k_fs_assemble<<<gS, EW_THREADS, 0, s>>>(P, F, W, sg, bt, At, nullptr);
+  ++g_launches;
+}
+
+void enqueue_picard_face_space(sgh_plan* p, cudaStream_t s, cudaGraphConditionalHandle h_picard,
+                               int in_graph) {
+  const DevParams& h = p->hp;
+  DevParams* P = p->P();
+  face_idct2_from(p, p->d(p->o_A),
+                  EpiTopFlux{P, p->d(p->o_qlas), p->d(p->o_qev), p->d(p->o_qnet), 0, nullptr}, s);
+  face_dct2(p, p->d(p->o_qnet), p->d(p->o_Stop), h.dct_scale, s);
+  k_fs_relax<<<p->nparts_fs, EW_THREADS, 0, s>>>(P, p->d(p->o_fsF), p->d(p->o_fsW), p->d(p->o_Stop),
+                                                 h.has_bottom_conv ? p->d(p->o_Sbot) : nullptr,
+                                                 p->d(p->o_sigma), p->d(p->o_beta), p->d(p->o_A),
+                                                 p->d(p->o_prelax));
+  ++g_launches;
+  k_converge<<<1, EW_THREADS, 0, s>>>(P, p->ctrl(), p->d(p->o_prelax), p->nparts_fs, p->d(p->o_pn1),
+                                       p->nparts_n1, h_picard, in_graph);
+  ++g_launches;
+}
+
 void enqueue_pre(sgh_plan* p, cudaStream_t s, cudaGraphConditionalHandle h_picard, int in_graph) {
   const DevParams& h = p->hp;
   DevParams* P = p->P();
@@ -586,6 +784,10 @@ void enqueue_pre(sgh_plan* p, cudaStream_t s, cudaGraphConditionalHandle h_picar
   k_face_begin<<<gS, EW_THREADS, 0, s>>>(P, C, p->d(p->o_xc), p->d(p->o_yc), p->d(p->o_qevold),
                                           p->d(p->o_qlas), p->d(p->o_qnet), p->d(p->o_plas));
   ++g_launches;
+  if (p->face_space) {
+    enqueue_pre_face_space(p, s);
+    return;
+  }
   face_dct2(p, p->d(p->o_qnet), p->d(p->o_Stop), h.dct_scale, s);
   k_init_modes<<<gV, EW_THREADS, 0, s>>>(P, C, p->d(p->o_a), p->d(p->o_K), p->d(p->o_KK), p->d(p->o_ct),
                                           p->d(p->o_Stop), p->d(p->o_Qm), p->d(p->o_aK));
@@ -609,6 +811,10 @@ void enqueue_pre(sgh_plan* p, cudaStream_t s, cudaGraphConditionalHandle h_picar
 }
 
 void enqueue_picard(sgh_plan* p, cudaStream_t s, cudaGraphConditionalHandle h_picard, int in_graph) {
+  if (p->face_space) {
+    enqueue_picard_face_space(p, s, h_picard, in_graph);
+    return;
+  }
   const DevParams& h = p->hp;
   DevParams* P = p->P();
   Ctrl* C = p->ctrl();
@@ -666,7 +872,7 @@ void enqueue_picard(sgh_plan* p, cudaStream_t s, cudaGraphConditionalHandle h_pi
                  p->d(p->o_t2), p->d(p->o_vol), s);
     nparts = axis_blocks(h.nz, 1, h.S);
   }
-  k_converge<<<1, EW_THREADS, 0, s>>>(P, C, p->d(p->o_prelax), nparts, h_picard, in_graph);
+  k_converge<<<1, EW_THREADS, 0, s>>>(P, C, p->d(p->o_prelax), nparts, nullptr, 0, h_picard, in_graph);
   ++g_launches;
 }
 
@@ -674,7 +880,16 @@ void enqueue_post(sgh_plan* p, cudaStream_t s, cudaGraphConditionalHandle h_step
   const DevParams& h = p->hp;
   DevParams* P = p->P();
   int n_surf;
-  if (h.grid_latent || h.prop_corr) {
+  if (p->face_space) {
+    face_idct2_from(p, p->d(p->o_A),
+                    EpiCommitSurface{P, p->d(p->o_Tsurf), p->d(p->o_qev), p->d(p->o_qevold), p->d(p->o_psurf)},
+                    s);
+    k_fs_commit_modes<<<cdiv(h.V, EW_THREADS), EW_THREADS, 0, s>>>(
+        P, p->d(p->o_a), p->d(p->o_K), p->d(p->o_KK), p->d(p->o_ct), p->d(p->o_cb), p->d(p->o_sigma),
+        p->d(p->o_beta));
+    ++g_launches;
+    n_surf = p->nparts_surf;
+  } else if (h.grid_latent || h.prop_corr) {
     // T_prev and the surface temperature from one IDCT3 with the surface row
     volume_pass3(p, p->d(p->o_a), true,
                  EpiCommitVolume{P, p->d(p->o_Tprev), p->d(p->o_Tsurf), p->d(p->o_qev), p->d(p->o_qevold),
@@ -881,6 +1096,15 @@ int sgh_plan_create(const sgh_config* cfg, sgh_plan** out) {
   p->o_prelax = L.take(sizeof(double) * 2 * std::max(p->nparts_relax, nparts_axis));
   p->o_plas = L.take(sizeof(double) * p->nparts_las);
   p->o_psurf = L.take(sizeof(double) * 2 * std::max(p->nparts_surf, axis_blocks(h.nz + 1, 1, h.S)));
+  p->face_space = !latent && !prop_corr;
+  p->nparts_n1 = cdiv(h.S, EW_THREADS);
+  p->nparts_fs = std::min(RELAX_BLOCKS_MAX, cdiv(h.S, EW_THREADS));
+  p->o_fsF = L.take(S8 * 4);
+  p->o_fsW = L.take(S8 * 6);
+  p->o_sigma = L.take(S8);
+  p->o_beta = L.take(S8);
+  p->o_Ab = L.take(S8);
+  p->o_pn1 = L.take(sizeof(double) * p->nparts_n1);
   p->ws_need = L.off;
   *out = p;
   return SGH_OK;
@@ -925,6 +1149,9 @@ int sgh_plan_bind(sgh_plan* p, void* workspace, uint64_t bytes, void* stream) {
   k_propagators<<<cdiv(h.V, EW_THREADS), EW_THREADS, 0, s>>>(p->P(), alpha, c.rho * c.cp, p->d(p->o_K),
                                                              p->d(p->o_KK));
   SGH_CK(cudaMemsetAsync(p->ws + p->o_Sbot, 0, sizeof(double) * h.S, s));
+  if (p->face_space)
+    k_fs_weights<<<cdiv(h.S, EW_THREADS), EW_THREADS, 0, s>>>(p->P(), p->d(p->o_KK), p->d(p->o_ct),
+                                                              p->d(p->o_cb), p->d(p->o_fsW));
   SGH_CK(cudaGetLastError());
   SGH_CK(cudaStreamSynchronize(s));
   SGH_CK(cudaStreamCreateWithFlags(&p->cs1, cudaStreamNonBlocking));
