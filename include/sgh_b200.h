@@ -206,6 +206,67 @@ int sgh_dctn_workspace_bytes(int32_t ndim, const int32_t* shape, uint64_t* bytes
 int sgh_dctn(int32_t kind, int32_t ndim, const int32_t* shape, const double* in, double* out,
              void* workspace, uint64_t bytes, void* stream);
 
+/* ------------------------------------------------------------------------
+ * Batched instances (many cuboids of uneven sizes, one launch per stage).
+ *
+ * A batch holds n slots, each with its own sgh_config (shape and physics).
+ * One batch step advances every active slot by one time step: laser/face
+ * forcing, the Picard loop and the commit run as batched kernels over all
+ * slots inside one CUDA graph, and a slot whose Picard loop has converged
+ * stays frozen while the others iterate, so each slot's result equals the
+ * result of stepping it alone. Supported physics: what the face-space
+ * Picard form covers -- laser, evaporation, no convection, no latent heat,
+ * no temperature-dependent model; other configurations are rejected with
+ * SGH_ERR_UNSUPPORTED. No reference counterpart: the reference steps one
+ * instance per solver (solvers/spectral.py:219-543).
+ * ------------------------------------------------------------------------ */
+#define SGH_PRECISION_MIXED 1   /* FP32 modes and K/KK (computed in FP64); FP64 faces and norms */
+
+typedef struct sgh_batch sgh_batch;
+
+typedef struct {
+  int32_t active;     /* 1 while the slot still has steps to run          */
+  int32_t step;       /* steps done since sgh_batch_slot_start            */
+  int32_t n_steps;    /* steps requested                                  */
+  int32_t iters;      /* Picard iterations summed over the steps done     */
+  sgh_step_out last;  /* metrics of the last step                         */
+} sgh_batch_slot_info;
+
+int sgh_batch_create(const sgh_config* cfgs, int32_t n, int32_t precision, sgh_batch** out);
+int sgh_batch_destroy(sgh_batch* batch);
+int sgh_batch_workspace_bytes(const sgh_batch* batch, uint64_t* bytes);
+/* Bind workspace, build per-slot tables, capture the batch step graph. All
+ * slots start inactive. Synchronises the stream. */
+int sgh_batch_bind(sgh_batch* batch, void* workspace, uint64_t bytes, void* stream);
+/* (Re)start a slot: initial condition, laser table (n_steps entries, device),
+ * optional per-step metrics table (device, may be NULL). Async. */
+int sgh_batch_slot_start(sgh_batch* batch, int32_t slot, const sgh_laser* lasers_dev, int32_t n_steps,
+                         sgh_step_out* outs_dev, void* stream);
+/* Stop a slot (it is skipped by later steps). Async. */
+int sgh_batch_slot_stop(sgh_batch* batch, int32_t slot, void* stream);
+/* n_steps batch steps (each active slot advances until its table ends). Async. */
+int sgh_batch_step(sgh_batch* batch, int32_t n_steps, void* stream);
+/* Per-slot status (n entries) into a host array; synchronises the stream. */
+int sgh_batch_status(const sgh_batch* batch, sgh_batch_slot_info* out, void* stream);
+/* Device pointer / size of a slot buffer: SGH_BUF_MODES, SGH_BUF_K, SGH_BUF_KK
+ * (element type FP64 or FP32 by precision), SGH_BUF_Q_EVAP_OLD, SGH_BUF_SURFACE (FP64). */
+int sgh_batch_buffer(const sgh_batch* batch, int32_t slot, int32_t which, void** ptr, uint64_t* bytes);
+/* Kernels per batch step: *pre + n_iter * *per_iter + *post, n_iter = the
+ * largest iteration count over the active slots. */
+int sgh_batch_launch_counts(const sgh_batch* batch, int32_t* pre, int32_t* per_iter, int32_t* post);
+
+/* Orthonormal 2-D DCT-II (kind 2) or DCT-III (kind 3) of an (ny, nx) FP64
+ * face with both contractions on the tensor cores (tcgen05) in split-BF16
+ * form: each operand is split into BF16 hi + lo, three products per k-step
+ * accumulate in FP32 (relative error ~1e-5). The face contraction of the
+ * mixed-precision step; no reference counterpart (the reference's
+ * DCT_II / IDCT_II, physics/spectral_cpu_kernels.py:374-389, are FP64/FP32).
+ * After completion the first int32 of the workspace is 0, or nonzero when a
+ * tensor-core wait expired (the output is then not written). Async. */
+int sgh_dct2_bf16x3_workspace_bytes(int32_t ny, int32_t nx, uint64_t* bytes);
+int sgh_dct2_bf16x3(int32_t kind, int32_t ny, int32_t nx, const double* in, double* out, void* workspace,
+                    uint64_t bytes, void* stream);
+
 /* sgh_dctn without a workspace argument, for callers that hold device arrays
  * but cannot allocate device memory themselves -- for example a plain
  * ctypes/FFI host that has no CUDA array library to allocate with, or an

@@ -11,7 +11,7 @@ import os
 import threading
 
 __all__ = ["lib", "LIB_PATH", "SghProgram", "SghConfig", "SghLaser", "SghStepOut", "check",
-           "EXPORTED", "SghError", "BUF", "STEP_STATUS"]
+           "EXPORTED", "SghError", "BUF", "STEP_STATUS", "SghBatchSlotInfo", "PRECISION"]
 
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libsgh_b200.so")
 
@@ -21,6 +21,7 @@ MAX_CONSTS = 32
 ERRORS = {-1: "SGH_ERR_INVALID", -2: "SGH_ERR_CUDA", -3: "SGH_ERR_STATE",
           -4: "SGH_ERR_UNSUPPORTED", -5: "SGH_ERR_WORKSPACE"}
 STEP_STATUS = {0: "converged", 1: "capped", 2: "nonfinite"}
+PRECISION = {"fp64": 0, "mixed": 1}
 BUF = {"modes": 0, "K": 1, "KK": 2, "T_prev": 3, "q_evap_old": 4, "Q_modes": 5,
        "surface": 6, "scratch": 7}
 
@@ -30,6 +31,10 @@ EXPORTED = (
     "sgh_plan_workspace_bytes", "sgh_plan_bind", "sgh_plan_buffer", "sgh_plan_launch_counts", "sgh_state_reset",
     "sgh_step", "sgh_step_eager", "sgh_run", "sgh_dct3d", "sgh_surface_temperature", "sgh_project_volume",
     "sgh_reconstruct_volume", "sgh_dctn_workspace_bytes", "sgh_dctn", "sgh_dctn_noalloc",
+    "sgh_batch_create", "sgh_batch_destroy", "sgh_batch_workspace_bytes", "sgh_batch_bind",
+    "sgh_batch_slot_start", "sgh_batch_slot_stop", "sgh_batch_step", "sgh_batch_status",
+    "sgh_batch_buffer", "sgh_batch_launch_counts", "sgh_dct2_bf16x3_workspace_bytes",
+    "sgh_dct2_bf16x3",
 )
 
 
@@ -66,6 +71,11 @@ class SghStepOut(C.Structure):
     _fields_ = [("T_surface_max", C.c_double), ("P_laser", C.c_double),
                 ("picard_rel_err", C.c_double), ("n_iter", C.c_int32),
                 ("converged", C.c_int32), ("status", C.c_int32), ("pad", C.c_int32)]
+
+
+class SghBatchSlotInfo(C.Structure):
+    _fields_ = [("active", C.c_int32), ("step", C.c_int32), ("n_steps", C.c_int32),
+                ("iters", C.c_int32), ("last", SghStepOut)]
 
 
 class SghError(RuntimeError):
@@ -113,6 +123,18 @@ def lib() -> C.CDLL:
             "sgh_dctn_workspace_bytes": ([i32, C.POINTER(i32), u64p], C.c_int),
             "sgh_dctn": ([i32, i32, C.POINTER(i32), vp, vp, vp, C.c_uint64, vp], C.c_int),
             "sgh_dctn_noalloc": ([i32, i32, C.POINTER(i32), vp, vp, vp], C.c_int),
+            "sgh_dct2_bf16x3_workspace_bytes": ([i32, i32, u64p], C.c_int),
+            "sgh_dct2_bf16x3": ([i32, i32, i32, vp, vp, vp, C.c_uint64, vp], C.c_int),
+            "sgh_batch_create": ([C.POINTER(SghConfig), i32, i32, C.POINTER(vp)], C.c_int),
+            "sgh_batch_destroy": ([vp], C.c_int),
+            "sgh_batch_workspace_bytes": ([vp, u64p], C.c_int),
+            "sgh_batch_bind": ([vp, vp, C.c_uint64, vp], C.c_int),
+            "sgh_batch_slot_start": ([vp, i32, vp, i32, vp, vp], C.c_int),
+            "sgh_batch_slot_stop": ([vp, i32, vp], C.c_int),
+            "sgh_batch_step": ([vp, i32, vp], C.c_int),
+            "sgh_batch_status": ([vp, C.POINTER(SghBatchSlotInfo), vp], C.c_int),
+            "sgh_batch_buffer": ([vp, i32, i32, C.POINTER(vp), u64p], C.c_int),
+            "sgh_batch_launch_counts": ([vp, C.POINTER(i32), C.POINTER(i32), C.POINTER(i32)], C.c_int),
         }
         for name, (args, res) in sig.items():
             fn = getattr(L, name)

@@ -1,0 +1,170 @@
+"""Batched stepping of many independent cuboids (``sgh_batch_*`` of the C ABI).
+
+:class:`BatchSolver` holds a fixed set of slots, each with its own
+:class:`SimulationContext` (grid shape and physics may differ between slots).
+A slot is started with a laser path and a step count; every call of
+:meth:`BatchSolver.step` advances all active slots together, one launch per
+stage. Each slot runs the reference step (``solvers/spectral.py:219-543``) in
+its face-space form, so the supported physics is laser + evaporation without
+convection, latent heat or a T-dependent model.
+
+``precision="fp64"`` keeps the modes and K/KK in FP64; ``precision="mixed"``
+stores them in FP32 (computed in FP64 and rounded once) with FP64 faces and
+norms, halving the bytes each step moves.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _lib
+from .solver import laser_struct, make_config
+
+__all__ = ["BatchSolver"]
+
+
+def _picard(ctx, omega=None, tol=None, max_iter=None):
+    num = ctx.num
+
+    def pick(explicit, attr, default):
+        if explicit is not None:
+            return explicit
+        v = getattr(num, attr, None)
+        return default if v is None else v
+
+    return (float(pick(omega, "picard_omega", 0.1)), float(pick(tol, "picard_tol", 1e-4)),
+            int(pick(max_iter, "max_picard_iter", 30)))
+
+
+class BatchSolver:
+    """A bound batch of slots on one device."""
+
+    def __init__(self, contexts: Sequence, precision: str = "fp64", device=None):
+        import torch
+        if precision not in _lib.PRECISION:
+            raise ValueError(f"precision must be one of {sorted(_lib.PRECISION)}")
+        if not torch.cuda.is_available():
+            raise RuntimeError("BatchSolver needs a CUDA device (no CPU fallback)")
+        self.contexts = list(contexts)
+        self.precision = precision
+        self.n = len(self.contexts)
+        cfgs = (_lib.SghConfig * self.n)()
+        for i, ctx in enumerate(self.contexts):
+            if getattr(ctx, "fine", None) is not None:
+                raise NotImplementedError("box mode (fine_mesh) is not supported")
+            cfgs[i] = make_config(ctx, *_picard(ctx))
+        self._cfgs = cfgs
+        L = _lib.lib()
+        h = C.c_void_p()
+        _lib.check("sgh_batch_create", L.sgh_batch_create(cfgs, self.n, _lib.PRECISION[precision],
+                                                          C.byref(h)))
+        self._h = h
+        nbytes = C.c_uint64()
+        _lib.check("sgh_batch_workspace_bytes", L.sgh_batch_workspace_bytes(h, C.byref(nbytes)))
+        self.device = torch.device("cuda", torch.cuda.current_device()) if device is None \
+            else torch.device(device)
+        self.workspace = torch.empty(int(nbytes.value), dtype=torch.uint8, device=self.device)
+        self.stream = torch.cuda.current_stream(self.device)
+        _lib.check("sgh_batch_bind", L.sgh_batch_bind(h, C.c_void_p(self.workspace.data_ptr()),
+                                                      nbytes.value, self._s()))
+        self._tables = [None] * self.n
+        self._outs = [None] * self.n
+
+    def _s(self):
+        return C.c_void_p(self.stream.cuda_stream)
+
+    @property
+    def workspace_bytes(self) -> int:
+        return self.workspace.numel()
+
+    def laser_table(self, ctx, t0: float, n_steps: int):
+        """Device table of ``sgh_laser`` for steps ``t0 + i*dt`` of ``ctx.laser_path``."""
+        import torch
+        dt = float(ctx.num.dt)
+        arr = (_lib.SghLaser * n_steps)()
+        for i in range(n_steps):
+            arr[i] = laser_struct(ctx.laser_path.get_state(t0 + i * dt, dt), dt, dt)
+        return torch.frombuffer(bytearray(bytes(arr)), dtype=torch.uint8).to(self.device)
+
+    def start(self, slot: int, n_steps: int, t0: float = 0.0, record: bool = True,
+              table=None) -> None:
+        """Restart ``slot`` at the initial condition for ``n_steps`` steps of its path."""
+        import torch
+        ctx = self.contexts[slot]
+        if table is None:
+            table = self.laser_table(ctx, t0, n_steps)
+        self._tables[slot] = table
+        outs = None
+        if record:
+            outs = torch.zeros(max(1, n_steps) * C.sizeof(_lib.SghStepOut), dtype=torch.uint8,
+                               device=self.device)
+        self._outs[slot] = outs
+        _lib.check("sgh_batch_slot_start", _lib.lib().sgh_batch_slot_start(
+            self._h, int(slot), C.c_void_p(table.data_ptr()), int(n_steps),
+            C.c_void_p(outs.data_ptr()) if outs is not None else None, self._s()))
+
+    def stop(self, slot: int) -> None:
+        _lib.check("sgh_batch_slot_stop", _lib.lib().sgh_batch_slot_stop(self._h, int(slot), self._s()))
+
+    def step(self, n_steps: int = 1) -> None:
+        """Advance every active slot by ``n_steps`` steps (asynchronous)."""
+        _lib.check("sgh_batch_step", _lib.lib().sgh_batch_step(self._h, int(n_steps), self._s()))
+
+    def status(self):
+        """Per-slot ``SghBatchSlotInfo`` (synchronises the stream)."""
+        arr = (_lib.SghBatchSlotInfo * self.n)()
+        _lib.check("sgh_batch_status", _lib.lib().sgh_batch_status(self._h, arr, self._s()))
+        return list(arr)
+
+    def metrics(self, slot: int):
+        """Per-step metric dicts recorded for ``slot`` since its start."""
+        info = self.status()[slot]
+        outs = self._outs[slot]
+        if outs is None:
+            return []
+        host = outs.cpu().numpy().tobytes()
+        sz = C.sizeof(_lib.SghStepOut)
+        res = []
+        for i in range(info.step):
+            o = _lib.SghStepOut.from_buffer_copy(host[i * sz:(i + 1) * sz])
+            res.append({"T_surface_max": o.T_surface_max, "P_laser": o.P_laser,
+                        "n_evap_iter": o.n_iter, "picard_converged": bool(o.converged),
+                        "picard_rel_err": o.picard_rel_err})
+        return res
+
+    def buffer(self, slot: int, name: str):
+        """torch view of a slot buffer: ``modes``, ``K``, ``KK`` (FP64 or FP32),
+        ``q_evap_old``, ``surface`` (FP64)."""
+        import torch
+        ptr, nb = C.c_void_p(), C.c_uint64()
+        _lib.check("sgh_batch_buffer", _lib.lib().sgh_batch_buffer(
+            self._h, int(slot), _lib.BUF[name], C.byref(ptr), C.byref(nb)))
+        off = ptr.value - self.workspace.data_ptr()
+        c = self._cfgs[slot]
+        vol = name in ("modes", "K", "KK")
+        dt = torch.float32 if (vol and self.precision == "mixed") else torch.float64
+        view = self.workspace[off:off + nb.value].view(dt)
+        return view.view(c.nz, c.ny, c.nx) if vol else view.view(c.ny, c.nx)
+
+    def modes(self, slot: int):
+        return self.buffer(slot, "modes")
+
+    def launch_counts(self):
+        a, b, c = C.c_int32(), C.c_int32(), C.c_int32()
+        _lib.check("sgh_batch_launch_counts", _lib.lib().sgh_batch_launch_counts(
+            self._h, C.byref(a), C.byref(b), C.byref(c)))
+        return a.value, b.value, c.value
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) is not None:
+            self.stream.synchronize()
+            _lib.lib().sgh_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

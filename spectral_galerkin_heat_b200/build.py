@@ -14,9 +14,10 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 LIB = os.path.join(PKG, "libsgh_b200.so")
-SOURCES = [os.path.join(CSRC, "sgh_b200.cu")]
+SOURCES = [os.path.join(CSRC, "sgh_b200.cu"), os.path.join(CSRC, "sgh_batch.cu"),
+           os.path.join(CSRC, "sgh_mixed.cu")]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
-              "-Xcompiler", "-fPIC", "-shared", "--expt-relaxed-constexpr"]
+              "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]
 
 
 def _nvcc() -> str:
@@ -35,14 +36,27 @@ def _stale() -> bool:
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
-    """Compile the library if needed; return its path."""
+    """Compile the library if needed (translation units in parallel); return its path."""
     if not force and not _stale():
         return LIB
-    cmd = [_nvcc(), *NVCC_FLAGS, "-I", INCLUDE, "-I", CSRC, *SOURCES, "-o", LIB + ".tmp"]
+    objs, procs = [], []
+    for src in SOURCES:
+        obj = os.path.join(CSRC, os.path.basename(src) + ".o")
+        cmd = [_nvcc(), *NVCC_FLAGS, "-I", INCLUDE, "-I", CSRC, "-c", src, "-o", obj]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        procs.append(subprocess.Popen(cmd))
+        objs.append(obj)
+    if any(p.wait() != 0 for p in procs):
+        raise RuntimeError("nvcc failed")
+    link = [_nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", *objs,
+            "-o", LIB + ".tmp"]
     if verbose:
-        print(" ".join(cmd), flush=True)
-    subprocess.run(cmd, check=True)
+        print(" ".join(link), flush=True)
+    subprocess.run(link, check=True)
     os.replace(LIB + ".tmp", LIB)
+    for obj in objs:
+        os.remove(obj)
     return LIB
 
 

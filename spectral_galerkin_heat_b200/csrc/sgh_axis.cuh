@@ -45,22 +45,21 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 // thread index runs along the contiguous output dimension: k when B == 1
 // (CONTIG), c otherwise. Mat and X panels stream through an AX_STAGES-deep
 // cp.async pipeline of AX_BK-slice stages (out-of-range elements zero-filled).
+// Computes the output tile at (c0, k0) and hands every element to epi; the
+// caller reduces r over the block.
 template <bool CONTIG, int TI, int TJ, class Epi>
-__global__ void __launch_bounds__(AX_THREADS)
-k_axis(const double* __restrict__ X, const double* __restrict__ Mat, int Nout, int N, int A, int B,
-       Epi epi) {
-  constexpr int TK = CONTIG ? 16 * TJ : 16 * TI;  // outputs along the transformed axis per CTA
-  constexpr int TC = CONTIG ? 16 * TI : 16 * TJ;  // outputs along c per CTA
+__device__ __forceinline__ void axis_tile(const double* __restrict__ X, const double* __restrict__ Mat,
+                                          int Nout, int N, int A, int B, int c0, int k0, const Epi& epi,
+                                          Red& r) {
+  constexpr int TK = CONTIG ? 16 * TJ : 16 * TI;  // outputs along the transformed axis per tile
+  constexpr int TC = CONTIG ? 16 * TI : 16 * TJ;  // outputs along c per tile
   __shared__ double Ms[AX_STAGES][AX_BK][TK + 1];
   __shared__ double Xs[AX_STAGES][AX_BK][TC + 1];
-  __shared__ double red_sh[2 * (AX_THREADS / 32)];
 
   const int tid = threadIdx.x;
   const int f = tid & 15;   // fast index
   const int s = tid >> 4;   // slow index
   const int ncol = A * B;
-  const int c0 = blockIdx.x * TC;
-  const int k0 = blockIdx.y * TK;
   const int nchunks = (N + AX_BK - 1) / AX_BK;
 
   auto issue = [&](int stage, int n0) {
@@ -137,7 +136,6 @@ k_axis(const double* __restrict__ X, const double* __restrict__ Mat, int Nout, i
   }
   cp_async_wait<0>();
 
-  Red r;
 #pragma unroll
   for (int i = 0; i < TI; ++i) {
 #pragma unroll
@@ -151,6 +149,17 @@ k_axis(const double* __restrict__ X, const double* __restrict__ Mat, int Nout, i
       }
     }
   }
+}
+
+template <bool CONTIG, int TI, int TJ, class Epi>
+__global__ void __launch_bounds__(AX_THREADS)
+k_axis(const double* __restrict__ X, const double* __restrict__ Mat, int Nout, int N, int A, int B,
+       Epi epi) {
+  constexpr int TK = CONTIG ? 16 * TJ : 16 * TI;
+  constexpr int TC = CONTIG ? 16 * TI : 16 * TJ;
+  __shared__ double red_sh[2 * (AX_THREADS / 32)];
+  Red r;
+  axis_tile<CONTIG, TI, TJ>(X, Mat, Nout, N, A, B, blockIdx.x * TC, blockIdx.y * TK, epi, r);
   if (Epi::kReduce) {
     double p0, p1;
     if (Epi::kReduce == 1) {
@@ -162,7 +171,7 @@ k_axis(const double* __restrict__ X, const double* __restrict__ Mat, int Nout, i
       p1 = r.s0;
       block_max_sum<AX_THREADS>(p0, p1, red_sh);
     }
-    if (tid == 0) {
+    if (threadIdx.x == 0) {
       const int blk = blockIdx.y * gridDim.x + blockIdx.x;
       epi.partials[2 * blk] = p0;
       epi.partials[2 * blk + 1] = p1;

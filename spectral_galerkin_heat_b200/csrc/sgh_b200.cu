@@ -33,11 +33,19 @@
 #include "sgh_b200.h"
 #include "sgh_device.cuh"
 
+namespace {
+thread_local std::string g_last_error;
+}  // namespace
+
+int sgh::set_error(int code, const char* msg) {
+  g_last_error = msg;
+  return code;
+}
+
 using namespace sgh;
 
 namespace {
 
-thread_local std::string g_last_error;
 thread_local int g_launches = 0;  // kernels enqueued by the enqueue_* helpers
 
 int fail(int code, const std::string& msg) {
@@ -164,27 +172,6 @@ __global__ void k_step_begin(const DevParams* __restrict__ P, Ctrl* ctrl,
   ctrl->status = SGH_STEP_CAPPED;
   ctrl->rel_err = nan("");
   if (in_graph) cudaGraphSetConditional(h_picard, P->max_iter > 0 ? 1u : 0u);
-}
-
-// Order-1 shift table entry for output index o (spectral_cpu_kernels.py:305-325).
-struct ShiftTap {
-  int i0, i1;
-  double w0, w1;
-  bool in;
-};
-__device__ __forceinline__ ShiftTap shift_tap(int o, int n, double shift) {
-  const double p = (double)o - shift;
-  const double fl = floor(p);
-  const double t = p - fl;
-  ShiftTap s;
-  s.in = (p >= 0.0) && (p <= (double)(n - 1));
-  long long i0 = (long long)fl;
-  long long i1 = i0 + 1;
-  s.i0 = (int)(i0 < 0 ? 0 : (i0 > n - 1 ? n - 1 : i0));
-  s.i1 = (int)(i1 < 0 ? 0 : (i1 > n - 1 ? n - 1 : i1));
-  s.w1 = t;
-  s.w0 = 1.0 - t;
-  return s;
 }
 
 // Face forcing of the initial guess: q_las, P_laser partials, and

@@ -162,16 +162,20 @@ __device__ __forceinline__ double latent_source(const DevParams& P, double T, do
   return P.latent_factor * (fc - fp);
 }
 
-// Evaporation flux (physics/spectral_cpu_kernels.py:144-162).
-__device__ __forceinline__ double evaporation(const DevParams& P, double T) {
+// Evaporation flux (physics/spectral_cpu_kernels.py:144-162). PP is any
+// parameter block with T_liquidus, T_boil, evap_f1, evap_f2.
+template <class PP>
+__device__ __forceinline__ double evaporation(const PP& P, double T) {
   if (T < P.T_liquidus) return 0.0;
   const double term = (1.0 / sqrt(T)) * exp(P.evap_f2 * (1.0 - P.T_boil / T));
   return P.evap_f1 * term;
 }
 
 // Laser flux at cell (x, y) (core/laser.py:42-53 point-sampled super-Gaussian,
-// :65-91 cell-integrated Gaussian).
-__device__ __forceinline__ double laser_flux(const DevParams& P, double I0, double x0, double y0,
+// :65-91 cell-integrated Gaussian). PP is any parameter block with dx, dy,
+// r_x, r_y, order, cell_integrated.
+template <class PP>
+__device__ __forceinline__ double laser_flux(const PP& P, double I0, double x0, double y0,
                                              double x, double y) {
   if (P.cell_integrated) {
     const double s2 = sqrt(2.0);
@@ -191,6 +195,27 @@ __device__ __forceinline__ double laser_flux(const DevParams& P, double I0, doub
   const double r2 = ux * ux + uy * uy;
   const double shape = (P.order == 2.0) ? exp(-2.0 * r2) : exp(-2.0 * pow(r2, P.order / 2.0));
   return I0 * shape;
+}
+
+// Order-1 shift table entry for output index o (physics/spectral_cpu_kernels.py:305-325).
+struct ShiftTap {
+  int i0, i1;
+  double w0, w1;
+  bool in;
+};
+__device__ __forceinline__ ShiftTap shift_tap(int o, int n, double shift) {
+  const double p = (double)o - shift;
+  const double fl = floor(p);
+  const double t = p - fl;
+  ShiftTap s;
+  s.in = (p >= 0.0) && (p <= (double)(n - 1));
+  long long i0 = (long long)fl;
+  long long i1 = i0 + 1;
+  s.i0 = (int)(i0 < 0 ? 0 : (i0 > n - 1 ? n - 1 : i0));
+  s.i1 = (int)(i1 < 0 ? 0 : (i1 > n - 1 ? n - 1 : i1));
+  s.w1 = t;
+  s.w0 = 1.0 - t;
+  return s;
 }
 
 // ---------------------------------------------------------------------------
@@ -239,5 +264,8 @@ __device__ __forceinline__ void block_max_sum(double& m, double& s, double* sh) 
     }
   }
 }
+
+// Error reporting shared by the library's translation units (sgh_last_error).
+int set_error(int code, const char* msg);
 
 }  // namespace sgh

@@ -1,0 +1,109 @@
+"""Batched slots of uneven size: each slot equals its single-instance run and
+the oracle, is the same alone and in a mix, and the mixed (FP32-state) form
+stays within 1e-4 relative L2 of the FP64 oracle on a converged-Picard case."""
+import numpy as np
+import pytest
+
+from conftest import golden_case, make_context, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+def _ctx(nx, ny, nz, seed, steps, **kw):
+    from spectral_galerkin_heat_b200 import workloads
+    from spectral_galerkin_heat_b200.laser import StraightTrack
+    rng = np.random.default_rng(seed)
+    cfg, _ = workloads.straight_track(nx=nx, ny=ny, nz=nz, steps=steps,
+                                      size=(2e-3 * nx / 64, 1e-3 * ny / 32, 0.5e-3), **kw)
+    cfg["simulation"].update({"max_picard_iter": 30, "picard_omega": 0.1, "picard_tol": 1e-4})
+    power = float(rng.uniform(150.0, 400.0))
+    v = float(rng.uniform(0.5, 2.0))
+    path = StraightTrack(0.3e-3, cfg["domain"]["size"][1] / 2, v, 0.0, power)
+    return make_context(cfg, path)
+
+
+SHAPES = [(32, 16, 8), (48, 24, 16), (40, 20, 6), (64, 32, 16)]
+
+
+def test_batch_matches_single_instance_and_oracle():
+    from oracle.sgh_oracle import OracleSolver
+    from spectral_galerkin_heat_b200 import B200SpectralSolver
+    from spectral_galerkin_heat_b200.batch import BatchSolver
+    steps = 8
+    ctxs = [_ctx(*sh, seed=i, steps=steps) for i, sh in enumerate(SHAPES)]
+    b = BatchSolver(ctxs, "fp64")
+    for i in range(len(ctxs)):
+        b.start(i, steps)
+    b.step(steps)
+    info = b.status()
+    assert all(x.step == steps and not x.active for x in info)
+    for i, ctx in enumerate(ctxs):
+        single = B200SpectralSolver(None, ctx)
+        single.initialize()
+        o = OracleSolver(ctx)
+        o.initialize()
+        dt = ctx.num.dt
+        ms, mo = [], []
+        for k in range(steps):
+            ms.append(single.step(k * dt, dt)[1])
+            mo.append(o.step(k * dt, dt)[1])
+        a = b.modes(i).cpu().numpy()
+        assert rel_l2(a, single.state.a.cpu().numpy()) < 1e-12
+        assert rel_l2(a, o.a) < 1e-10
+        mb = b.metrics(i)
+        assert [m["n_evap_iter"] for m in mb] == [m["n_evap_iter"] for m in mo]
+        np.testing.assert_allclose([m["T_surface_max"] for m in mb],
+                                   [m["T_surface_max"] for m in mo], rtol=1e-10)
+        single.finalize()
+    b.close()
+
+
+def test_slot_alone_equals_slot_in_mix():
+    """Continuous-batching invariant: a slot's result does not depend on its neighbours."""
+    from spectral_galerkin_heat_b200.batch import BatchSolver
+    steps = 6
+    ctxs = [_ctx(*sh, seed=10 + i, steps=steps) for i, sh in enumerate(SHAPES)]
+    mix = BatchSolver(ctxs, "mixed")
+    for i in range(len(ctxs)):
+        mix.start(i, steps)
+    mix.step(2)
+    late = len(ctxs) - 1                    # restart one slot while the others run
+    mix.start(late, steps)
+    mix.step(steps)
+    alone = BatchSolver([ctxs[late]], "mixed")
+    alone.start(0, steps)
+    alone.step(steps)
+    assert np.array_equal(mix.modes(late).cpu().numpy(), alone.modes(0).cpu().numpy())
+    assert [m["n_evap_iter"] for m in mix.metrics(late)] == \
+        [m["n_evap_iter"] for m in alone.metrics(0)]
+    mix.close()
+    alone.close()
+
+
+def test_mixed_precision_error_vs_fp64_oracle():
+    """FP32 state: temperature rel L2 vs the FP64 oracle <= 1e-4 (stated target)."""
+    from oracle.sgh_oracle import OracleSolver
+    from spectral_galerkin_heat_b200.batch import BatchSolver
+    steps = 40
+    ctx = _ctx(64, 32, 16, seed=3, steps=steps)
+    ctx.num.picard_tol = 1e-8
+    ctx.num.max_picard_iter = 300
+    b = BatchSolver([ctx], "mixed")
+    b.start(0, steps)
+    b.step(steps)
+    o = OracleSolver(ctx)
+    o.initialize()
+    for k in range(steps):
+        o.step(k * ctx.num.dt, ctx.num.dt)
+    from oracle.sgh_oracle import dct3
+    T_mixed = dct3(b.modes(0).double().cpu().numpy())
+    T_ref = dct3(o.a)
+    assert rel_l2(T_mixed, T_ref) < 1e-4
+    b.close()
+
+
+def test_batch_rejects_unsupported_physics():
+    from spectral_galerkin_heat_b200.batch import BatchSolver
+    cfg, path, *_ = golden_case("raster_32x16x8")
+    with pytest.raises(Exception, match="face-space"):
+        BatchSolver([make_context(cfg, path)], "fp64")
