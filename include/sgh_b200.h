@@ -220,7 +220,8 @@ int sgh_dctn(int32_t kind, int32_t ndim, const int32_t* shape, const double* in,
  * SGH_ERR_UNSUPPORTED. No reference counterpart: the reference steps one
  * instance per solver (solvers/spectral.py:219-543).
  * ------------------------------------------------------------------------ */
-#define SGH_PRECISION_MIXED 1   /* FP32 modes and K/KK (computed in FP64); FP64 faces and norms */
+#define SGH_PRECISION_MIXED 1   /* FP32 modes and K/KK (computed in FP64); face contractions in
+                                   split-BF16 on the tensor cores; FP64 faces and norms */
 
 typedef struct sgh_batch sgh_batch;
 
@@ -246,11 +247,17 @@ int sgh_batch_slot_start(sgh_batch* batch, int32_t slot, const sgh_laser* lasers
 int sgh_batch_slot_stop(sgh_batch* batch, int32_t slot, void* stream);
 /* n_steps batch steps (each active slot advances until its table ends). Async. */
 int sgh_batch_step(sgh_batch* batch, int32_t n_steps, void* stream);
+/* One batch step with the same kernels launched one by one and the Picard
+ * loop driven from the host (for profilers and debugging). Synchronous. */
+int sgh_batch_step_eager(sgh_batch* batch, void* stream);
 /* Per-slot status (n entries) into a host array; synchronises the stream. */
 int sgh_batch_status(const sgh_batch* batch, sgh_batch_slot_info* out, void* stream);
 /* Device pointer / size of a slot buffer: SGH_BUF_MODES, SGH_BUF_K, SGH_BUF_KK
  * (element type FP64 or FP32 by precision), SGH_BUF_Q_EVAP_OLD, SGH_BUF_SURFACE (FP64). */
 int sgh_batch_buffer(const sgh_batch* batch, int32_t slot, int32_t which, void** ptr, uint64_t* bytes);
+/* *err = nonzero once a tensor-core wait of a mixed-precision batch expired
+ * (the affected face pass wrote no results). Synchronises the stream. */
+int sgh_batch_error(const sgh_batch* batch, int32_t* err, void* stream);
 /* Kernels per batch step: *pre + n_iter * *per_iter + *post, n_iter = the
  * largest iteration count over the active slots. */
 int sgh_batch_launch_counts(const sgh_batch* batch, int32_t* pre, int32_t* per_iter, int32_t* post);

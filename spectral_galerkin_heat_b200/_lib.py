@@ -32,8 +32,9 @@ EXPORTED = (
     "sgh_step", "sgh_step_eager", "sgh_run", "sgh_dct3d", "sgh_surface_temperature", "sgh_project_volume",
     "sgh_reconstruct_volume", "sgh_dctn_workspace_bytes", "sgh_dctn", "sgh_dctn_noalloc",
     "sgh_batch_create", "sgh_batch_destroy", "sgh_batch_workspace_bytes", "sgh_batch_bind",
-    "sgh_batch_slot_start", "sgh_batch_slot_stop", "sgh_batch_step", "sgh_batch_status",
-    "sgh_batch_buffer", "sgh_batch_launch_counts", "sgh_dct2_bf16x3_workspace_bytes",
+    "sgh_batch_slot_start", "sgh_batch_slot_stop", "sgh_batch_step", "sgh_batch_step_eager",
+    "sgh_batch_status",
+    "sgh_batch_buffer", "sgh_batch_launch_counts", "sgh_batch_error", "sgh_dct2_bf16x3_workspace_bytes",
     "sgh_dct2_bf16x3",
 )
 
@@ -132,8 +133,10 @@ def lib() -> C.CDLL:
             "sgh_batch_slot_start": ([vp, i32, vp, i32, vp, vp], C.c_int),
             "sgh_batch_slot_stop": ([vp, i32, vp], C.c_int),
             "sgh_batch_step": ([vp, i32, vp], C.c_int),
+            "sgh_batch_step_eager": ([vp, vp], C.c_int),
             "sgh_batch_status": ([vp, C.POINTER(SghBatchSlotInfo), vp], C.c_int),
             "sgh_batch_buffer": ([vp, i32, i32, C.POINTER(vp), u64p], C.c_int),
+            "sgh_batch_error": ([vp, C.POINTER(i32), vp], C.c_int),
             "sgh_batch_launch_counts": ([vp, C.POINTER(i32), C.POINTER(i32), C.POINTER(i32)], C.c_int),
         }
         for name, (args, res) in sig.items():

@@ -112,6 +112,10 @@ class BatchSolver:
         """Advance every active slot by ``n_steps`` steps (asynchronous)."""
         _lib.check("sgh_batch_step", _lib.lib().sgh_batch_step(self._h, int(n_steps), self._s()))
 
+    def step_eager(self) -> None:
+        """One step with the kernels launched one by one (profilers, debugging)."""
+        _lib.check("sgh_batch_step_eager", _lib.lib().sgh_batch_step_eager(self._h, self._s()))
+
     def status(self):
         """Per-slot ``SghBatchSlotInfo`` (synchronises the stream)."""
         arr = (_lib.SghBatchSlotInfo * self.n)()
@@ -150,6 +154,12 @@ class BatchSolver:
 
     def modes(self, slot: int):
         return self.buffer(slot, "modes")
+
+    def tensor_core_error(self) -> int:
+        """Nonzero once a tensor-core wait expired in a mixed-precision face pass."""
+        e = C.c_int32()
+        _lib.check("sgh_batch_error", _lib.lib().sgh_batch_error(self._h, C.byref(e), self._s()))
+        return e.value
 
     def launch_counts(self):
         a, b, c = C.c_int32(), C.c_int32(), C.c_int32()

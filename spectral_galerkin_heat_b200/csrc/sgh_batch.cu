@@ -29,6 +29,7 @@
 #include "sgh_b200.h"
 #include "sgh_axis.cuh"
 #include "sgh_device.cuh"
+#include "sgh_umma.cuh"
 
 namespace sgh {
 namespace batch {
@@ -48,6 +49,10 @@ struct BSlot {
   int blk0, nblk;  // element / column blocks
   int tile0, ntile;  // face transform tiles
   int vblk0, nvblk;  // volume blocks (setup kernels)
+  int utile0, nutile;  // tensor-core face tiles (mixed precision)
+  long long xa, yb;    // byte offsets of the slot's x-pass A plane and y-pass B plane
+  long long mpx, mpy;  // byte offsets of the forward x / y matrix planes (inverse at + mp_inv)
+  long long mpx_inv, mpy_inv;
   double dx, dy, dt, Lx, Ly, Lz;
   double dct_scale, recon_scale, n_elements;
   double T0, evap_f1, evap_f2, T_boil, T_liquidus;
@@ -68,7 +73,9 @@ struct BState {
 
 struct BGlobal {
   int steps_left;
-  int pad[3];
+  int umma_err;     // nonzero once a tensor-core wait expired
+  int picard_any;   // some slot is still iterating (read by the eager step)
+  int pad;
 };
 
 // Device view of a bound batch (passed by value to every kernel).
@@ -79,6 +86,13 @@ struct BView {
   const int* blk_start;   // n + 1
   const int* tile_start;  // n + 1
   const int* vblk_start;  // n + 1
+  const int* utile_start; // n + 1 (tensor-core face tiles)
+  __nv_bfloat16* xa_hi;   // operand planes (mixed precision; null otherwise)
+  __nv_bfloat16* xa_lo;
+  __nv_bfloat16* yb_hi;
+  __nv_bfloat16* yb_lo;
+  const char* mp_hi;      // DCT matrix planes
+  const char* mp_lo;
   const double* mats;
   const double* Ct;
   int n;
@@ -94,6 +108,13 @@ __device__ __forceinline__ int find_slot(const int* start, int n, int b) {
   return lo;
 }
 
+// x-pass A-operand plane element (y, x) of slot sl (mixed precision only).
+__device__ __forceinline__ void xa_put(const BView& v, const BSlot& sl, int y, int x, double val) {
+  if (!v.xa_hi) return;
+  const int nkc = (sl.nx + umma::KC - 1) / umma::KC;
+  umma::plane_put(v.xa_hi + sl.xa / 2, v.xa_lo + sl.xa / 2, y, x, nkc, val);
+}
+
 // ---------------------------------------------------------------------------
 // setup
 // ---------------------------------------------------------------------------
@@ -107,6 +128,16 @@ __global__ void kb_dct_matrix(int N, double* M) {
   const double v = w * cospi((double)m / (double)(2 * N));
   M[k * N + n] = v;
   M[(size_t)N * N + n * N + k] = v;
+}
+
+// BF16 hi/lo planes of an N x N DCT matrix (inv: its transpose), rows = the
+// output index, k = the contracted index.
+__global__ void kb_matrix_planes(int N, const double* M, int inv, __nv_bfloat16* hi, __nv_bfloat16* lo) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= N * N) return;
+  const int r = e / N, k = e - r * N;
+  const double val = inv ? M[(size_t)k * N + r] : M[(size_t)r * N + k];
+  umma::plane_put(hi, lo, r, k, (N + umma::KC - 1) / umma::KC, val);
 }
 
 // K, KK of every slot exactly as precompute_K_KK (physics/spectral_state.py:374-421),
@@ -215,7 +246,10 @@ __global__ void __launch_bounds__(CT) kb_begin(BView v, cudaGraphConditionalHand
     if (!st.done) any = 1;
   }
   __syncthreads();
-  if (threadIdx.x == 0 && in_graph) cudaGraphSetConditional(h_picard, any ? 1u : 0u);
+  if (threadIdx.x == 0) {
+    v.g->picard_any = any;
+    if (in_graph) cudaGraphSetConditional(h_picard, any ? 1u : 0u);
+  }
 }
 
 // q_las, P_laser partials and q_net = q_las - shift(q_evap_old) per slot
@@ -244,6 +278,7 @@ kb_face_begin(BView v, double* q_las, double* q_net, const double* q_evold, doub
                  ty.w1 * (tx.w0 * f[ty.i1 * nx + tx.i0] + tx.w1 * f[ty.i1 * nx + tx.i1]);
     if (!(ty.in && tx.in)) val = 0.0;
     q_net[sl.face + i] = q - val;
+    xa_put(v, sl, y, x, q - val);
   }
   block_sum2<BT>(sum, dummy, sh);
   if (threadIdx.x == 0) part_las[b] = sum;
@@ -287,7 +322,11 @@ kb_assemble(BView v, const double* Zt, const double* Wtt, const double* sigma, d
   const BSlot& sl = v.slot[s];
   if (!v.st[s].active) return;
   const int i = (b - sl.blk0) * BT + threadIdx.x;
-  if (i < sl.S) A[sl.face + i] = Zt[sl.face + i] + Wtt[sl.face + i] * sigma[sl.face + i];
+  if (i < sl.S) {
+    const double a = Zt[sl.face + i] + Wtt[sl.face + i] * sigma[sl.face + i];
+    A[sl.face + i] = a;
+    xa_put(v, sl, i / sl.nx, i % sl.nx, a);
+  }
 }
 
 // ---- batched face transform: one 2 x 4-register-tile block per tile ------
@@ -345,6 +384,183 @@ __global__ void __launch_bounds__(AX_THREADS) kb_face_axis(BView v, const double
   }
 }
 
+// ---- batched face transform on the tensor cores (mixed precision) ---------
+// Same contraction as kb_face_axis, as 128 x UNT tiles of split-BF16 products
+// accumulated in FP32 in tensor memory (sgh_umma.cuh); slot tiles:
+// ceil(ny / 128) * ceil(nx / UNT) in both directions.
+constexpr int UNT = 128;
+inline __host__ __device__ int face_utiles(int nx, int ny) {
+  return ((ny + umma::TM - 1) / umma::TM) * ((nx + UNT - 1) / UNT);
+}
+
+struct ULoadX {  // DIR 0, A(m = y, k = n) = in[y][n]
+  const double* p;
+  int nx;
+  __device__ __forceinline__ double operator()(int m, int k) const { return p[(size_t)m * nx + k]; }
+};
+struct ULoadM {  // matrix rows: M(r, k) = M[r * N + k]
+  const double* p;
+  int N;
+  __device__ __forceinline__ double operator()(int r, int k) const { return p[(size_t)r * N + k]; }
+};
+struct ULoadT {  // DIR 1, B(n = x, k = n') = in[n'][x]
+  const double* p;
+  int nx;
+  __device__ __forceinline__ double operator()(int r, int k) const { return p[(size_t)k * nx + r]; }
+};
+
+template <class Epi>
+struct UEpi {  // (m, n, v) -> batched epilogue on face index m * nx + n
+  const BSlot* sl;
+  BState* st;
+  Epi e;
+  Red* r;
+  __device__ __forceinline__ void operator()(int m, int n, double v) const {
+    e(*sl, *st, sl->face + (long long)m * sl->nx + n, v, *r);
+  }
+};
+
+template <int DIR, bool INV, bool SKIP_DONE, class Epi>
+__global__ void __launch_bounds__(umma::THREADS)
+kb_face_umma(BView v, const double* in, Epi epi, double* part_tile) {
+  extern __shared__ __align__(128) char usmem[];
+  __shared__ double red[umma::THREADS / 32];
+  const int b = blockIdx.x;
+  const int s = find_slot(v.utile_start, v.n, b);
+  const BSlot& sl = v.slot[s];
+  BState& st = v.st[s];
+  if (!st.active || (SKIP_DONE && st.done)) return;
+  const int t = b - sl.utile0;
+  const int nx = sl.nx, ny = sl.ny;
+  const int nct = (nx + UNT - 1) / UNT;
+  const int n0 = (t % nct) * UNT, m0 = (t / nct) * umma::TM;
+  const int N = DIR == 0 ? nx : ny;
+  const double* M = v.mats + (DIR == 0 ? sl.mx : sl.my) + (INV ? (size_t)N * N : 0);
+  const double* X = in + sl.face;
+  Red r;
+  UEpi<Epi> ue{&sl, &st, epi, &r};
+  if (DIR == 0)
+    umma::tile_bf16x3<UNT>(ny, nx, nx, m0, n0, ULoadX{X, nx}, ULoadM{M, nx}, ue, usmem, &v.g->umma_err);
+  else
+    umma::tile_bf16x3<UNT>(ny, nx, ny, m0, n0, ULoadM{M, ny}, ULoadT{X, nx}, ue, usmem, &v.g->umma_err);
+  if (Epi::kMax) {
+    double m = r.mx;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double mm = red[0];
+      for (int w = 1; w < umma::THREADS / 32; ++w) mm = fmax(mm, red[w]);
+      part_tile[b] = mm;
+    }
+  }
+}
+
+// ---- batched face transform fed from operand planes (mixed precision) ---
+// DIR 0 (x-pass): A = the slot's x-pass plane (rows y, k = x), B = the x
+// matrix plane (rows k, k = n); DIR 1 (y-pass): A = the y matrix plane, B =
+// the slot's y-pass plane (rows x, k = y). epi(sl, st, m, n, value, r) gets
+// every in-range element, (m, n) = (y, k) for DIR 0 and (k, x) for DIR 1.
+template <int DIR, bool INV, bool SKIP_DONE, class Epi>
+__global__ void __launch_bounds__(umma::THREADS) kb_face_tc(BView v, Epi epi, double* part_tile) {
+  extern __shared__ __align__(128) char usmem[];
+  __shared__ double red[umma::THREADS / 32];
+  const int b = blockIdx.x;
+  const int s = find_slot(v.utile_start, v.n, b);
+  const BSlot& sl = v.slot[s];
+  BState& st = v.st[s];
+  if (!st.active || (SKIP_DONE && st.done)) return;
+  const int t = b - sl.utile0;
+  const int nx = sl.nx, ny = sl.ny;
+  const int nct = (nx + UNT - 1) / UNT;
+  const int rt = t / nct, ct = t % nct;
+  const int nkc = ((DIR == 0 ? nx : ny) + umma::KC - 1) / umma::KC;
+  const size_t cb = (size_t)umma::CHUNK_BYTES;
+  const char *ah, *al, *bh, *bl;
+  if (DIR == 0) {
+    ah = reinterpret_cast<const char*>(v.xa_hi) + sl.xa + rt * nkc * cb;
+    al = reinterpret_cast<const char*>(v.xa_lo) + sl.xa + rt * nkc * cb;
+    const long long mp = INV ? sl.mpx_inv : sl.mpx;
+    bh = v.mp_hi + mp + ct * nkc * cb;
+    bl = v.mp_lo + mp + ct * nkc * cb;
+  } else {
+    const long long mp = INV ? sl.mpy_inv : sl.mpy;
+    ah = v.mp_hi + mp + rt * nkc * cb;
+    al = v.mp_lo + mp + rt * nkc * cb;
+    bh = reinterpret_cast<const char*>(v.yb_hi) + sl.yb + ct * nkc * cb;
+    bl = reinterpret_cast<const char*>(v.yb_lo) + sl.yb + ct * nkc * cb;
+  }
+  Red r;
+  const int m0 = rt * umma::TM, n0 = ct * UNT;
+  const int Mrows = ny;  // both directions: rows y (DIR 0) or k over ny (DIR 1)
+  auto tepi = [&](int ml, int nl, double val) {
+    const int m = m0 + ml, n = n0 + nl;
+    if (m < Mrows && n < nx) epi(v, sl, st, m, n, val, r);
+  };
+  umma::tile_planes(ah, al, bh, bl, nkc, tepi, usmem, &v.g->umma_err);
+  if (Epi::kMax) {
+    double m = r.mx;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double mm = red[0];
+      for (int w = 1; w < umma::THREADS / 32; ++w) mm = fmax(mm, red[w]);
+      part_tile[b] = mm;
+    }
+  }
+}
+
+struct TE_ToYB {  // x-pass result (y, k) -> y-pass B plane element (row k, k-index y)
+  static constexpr int kMax = 0;
+  __device__ __forceinline__ void operator()(const BView& v, const BSlot& sl, const BState&, int y, int k,
+                                             double val, Red&) const {
+    const int nkc = (sl.ny + umma::KC - 1) / umma::KC;
+    umma::plane_put(v.yb_hi + sl.yb / 2, v.yb_lo + sl.yb / 2, k, y, nkc, val);
+  }
+};
+struct TE_Store {  // y-pass result -> FP64 face array (times dct_scale if scaled)
+  static constexpr int kMax = 0;
+  double* out;
+  int scaled;
+  __device__ __forceinline__ void operator()(const BView&, const BSlot& sl, const BState&, int k, int x,
+                                             double val, Red&) const {
+    out[sl.face + (long long)k * sl.nx + x] = scaled ? val * sl.dct_scale : val;
+  }
+};
+struct TE_TopFlux {  // T_s -> evaporation -> q_net into the x-pass A plane (solvers/spectral.py:388-404)
+  static constexpr int kMax = 0;
+  const double* q_las;
+  double* q_ev;
+  double* q_net;
+  __device__ __forceinline__ void operator()(const BView& v, const BSlot& sl, const BState&, int y, int x,
+                                             double val, Red&) const {
+    const long long i = sl.face + (long long)y * sl.nx + x;
+    const double Ts = sl.recon_scale * val;
+    const double qe = evaporation(sl, Ts);
+    q_ev[i] = qe;
+    const double qn = q_las[i] - qe;
+    q_net[i] = qn;
+    xa_put(v, sl, y, x, qn);
+  }
+};
+struct TE_CommitSurface {  // T_temp, its max, q_evap_old <- q_evap
+  static constexpr int kMax = 1;
+  double* T_surf;
+  const double* q_ev;
+  double* q_evold;
+  __device__ __forceinline__ void operator()(const BView&, const BSlot& sl, const BState&, int y, int x,
+                                             double val, Red& r) const {
+    const long long i = sl.face + (long long)y * sl.nx + x;
+    const double T = sl.recon_scale * val;
+    T_surf[i] = T;
+    q_evold[i] = q_ev[i];
+    r.mx = fmax(r.mx, T);
+  }
+};
+
 struct EB_Store {  // out = v * (scaled ? dct_scale : 1)
   static constexpr int kMax = 0;
   double* out;
@@ -401,7 +617,9 @@ kb_relax(BView v, const double* Zt, const double* Yt, const double* Wtt, const d
     o2 = 2.0 * sg * Yt[j] + sg * sg * q;
     const double ns = d * sl.omega + sg;
     sigma[j] = ns;
-    A[j] = Zt[j] + Wtt[j] * ns;
+    const double a = Zt[j] + Wtt[j] * ns;
+    A[j] = a;
+    xa_put(v, sl, i / sl.nx, i % sl.nx, a);
   }
   block_sum2<BT>(r2, o2, sh);
   if (threadIdx.x == 0) {
@@ -445,7 +663,10 @@ kb_converge(BView v, const double* part, const double* part_n1, cudaGraphConditi
     if (!st.done) any = 1;
   }
   __syncthreads();
-  if (threadIdx.x == 0 && in_graph) cudaGraphSetConditional(h_picard, any ? 1u : 0u);
+  if (threadIdx.x == 0) {
+    v.g->picard_any = any;
+    if (in_graph) cudaGraphSetConditional(h_picard, any ? 1u : 0u);
+  }
 }
 
 // a = K a + KK Ct sigma (commit of the modes).
@@ -469,8 +690,8 @@ kb_commit_modes(BView v, R* a, const R* K, const R* KK, const double* sigma) {
 // Metrics of every active slot (solvers/spectral.py:536-542); advances the
 // step counters and decides whether the step loop continues.
 __global__ void __launch_bounds__(CT)
-kb_commit(BView v, const double* part_las, const double* part_tile, cudaGraphConditionalHandle h_steps,
-          int in_graph) {
+kb_commit(BView v, const double* part_las, const double* part_tile, int umma_tiles,
+          cudaGraphConditionalHandle h_steps, int in_graph) {
   __shared__ int any;
   if (threadIdx.x == 0) any = 0;
   __syncthreads();
@@ -480,7 +701,8 @@ kb_commit(BView v, const double* part_las, const double* part_tile, cudaGraphCon
     const BSlot& sl = v.slot[s];
     double p = 0.0, m = -INFINITY;
     for (int b = sl.blk0; b < sl.blk0 + sl.nblk; ++b) p += part_las[b];
-    for (int b = sl.tile0; b < sl.tile0 + sl.ntile; ++b) m = fmax(m, part_tile[b]);
+    const int t0 = umma_tiles ? sl.utile0 : sl.tile0, nt = umma_tiles ? sl.nutile : sl.ntile;
+    for (int b = t0; b < t0 + nt; ++b) m = fmax(m, part_tile[b]);
     sgh_step_out o;
     o.T_surface_max = m;
     o.P_laser = p * sl.dx * sl.dy;
@@ -515,16 +737,19 @@ struct sgh_batch {
   int precision = 0;
   std::vector<sgh_config> cfg;
   std::vector<BSlot> slots;
-  std::vector<int> blk_start, tile_start, vblk_start;
+  std::vector<int> blk_start, tile_start, vblk_start, utile_start;
   std::vector<std::pair<int, long long>> mat_list;  // (N, element offset)
   long long tot_vol = 0, tot_face = 0;
-  int tot_blk = 0, tot_tile = 0, tot_vblk = 0, tot_z = 0;
+  int tot_blk = 0, tot_tile = 0, tot_vblk = 0, tot_z = 0, tot_utile = 0;
   long long mat_elems = 0;
   // workspace offsets (bytes)
-  size_t o_slot, o_state, o_g, o_blk, o_tile, o_vblk, o_mats, o_ct;
+  size_t o_slot, o_state, o_g, o_blk, o_tile, o_vblk, o_utile, o_mats, o_ct;
   size_t o_a, o_K, o_KK;
   size_t o_qlas, o_qnet, o_qev, o_qevold, o_Stop, o_f1, o_sigma, o_A, o_Tsurf, o_Zt, o_Yt, o_Wtt, o_Qtt;
   size_t o_plas, o_pn1, o_prelax, o_ptile;
+  size_t o_xah = 0, o_xal = 0, o_ybh = 0, o_ybl = 0, o_mph = 0, o_mpl = 0;  // operand planes (mixed)
+  size_t xa_bytes = 0, yb_bytes = 0, mp_bytes = 0;
+  std::vector<std::pair<int, long long>> mplane_list;  // (N, byte offset of the forward plane)
   size_t ws_need = 0;
   char* ws = nullptr;
   bool bound = false;
@@ -543,6 +768,14 @@ struct sgh_batch {
     v.blk_start = reinterpret_cast<const int*>(ws + o_blk);
     v.tile_start = reinterpret_cast<const int*>(ws + o_tile);
     v.vblk_start = reinterpret_cast<const int*>(ws + o_vblk);
+    v.utile_start = reinterpret_cast<const int*>(ws + o_utile);
+    const bool mixed = precision == SGH_PRECISION_MIXED;
+    v.xa_hi = mixed ? reinterpret_cast<__nv_bfloat16*>(ws + o_xah) : nullptr;
+    v.xa_lo = mixed ? reinterpret_cast<__nv_bfloat16*>(ws + o_xal) : nullptr;
+    v.yb_hi = mixed ? reinterpret_cast<__nv_bfloat16*>(ws + o_ybh) : nullptr;
+    v.yb_lo = mixed ? reinterpret_cast<__nv_bfloat16*>(ws + o_ybl) : nullptr;
+    v.mp_hi = mixed ? ws + o_mph : nullptr;
+    v.mp_lo = mixed ? ws + o_mpl : nullptr;
     v.mats = d(o_mats);
     v.Ct = d(o_ct);
     v.n = n;
@@ -564,6 +797,22 @@ inline int cdivl(long long a, long long b) { return (int)((a + b - 1) / b); }
 
 thread_local int g_blaunch = 0;
 
+// One face pass over all slots: the FP64 register-tiled contraction on the
+// FP64 input (plain), or tensor-core split-BF16 tiles fed by bulk copies
+// from the operand planes (mixed).
+template <int DIR, bool INV, bool SKIP, class EpiF, class EpiT>
+void face_pass(sgh_batch* B, cudaStream_t s, const double* in, const EpiF& ef, const EpiT& et, double* part) {
+  const BView v = B->view();
+  if (B->precision == SGH_PRECISION_MIXED) {
+    const int smem = umma::planes_smem_bytes();
+    (void)cudaFuncSetAttribute(kb_face_tc<DIR, INV, SKIP, EpiT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    kb_face_tc<DIR, INV, SKIP, EpiT><<<B->tot_utile, umma::THREADS, smem, s>>>(v, et, part);
+  } else {
+    kb_face_axis<DIR, INV, SKIP, EpiF><<<B->tot_tile, AX_THREADS, 0, s>>>(v, in, ef, part);
+  }
+  ++g_blaunch;
+}
+
 template <class R>
 void enqueue_pre(sgh_batch* B, cudaStream_t s, cudaGraphConditionalHandle h, int in_graph) {
   const BView v = B->view();
@@ -573,29 +822,27 @@ void enqueue_pre(sgh_batch* B, cudaStream_t s, cudaGraphConditionalHandle h, int
   kb_begin<<<1, CT, 0, s>>>(v, h, in_graph);
   kb_face_begin<<<B->tot_blk, BT, 0, s>>>(v, B->d(B->o_qlas), B->d(B->o_qnet), B->d(B->o_qevold), B->d(B->o_plas));
   kb_pass1<R><<<B->tot_blk, BT, 0, s>>>(v, a, K, KK, B->d(B->o_Zt), B->d(B->o_Yt), B->d(B->o_pn1));
+  g_blaunch += 3;
   // initial guess: sigma = dct_scale * DCT2(q_las - shift(q_evap_old))
-  kb_face_axis<0, false, false, EB_Store><<<B->tot_tile, AX_THREADS, 0, s>>>(v, B->d(B->o_qnet),
-                                                                      EB_Store{B->d(B->o_f1), 0}, nullptr);
-  kb_face_axis<1, false, false, EB_Store><<<B->tot_tile, AX_THREADS, 0, s>>>(v, B->d(B->o_f1),
-                                                                      EB_Store{B->d(B->o_sigma), 1}, nullptr);
+  face_pass<0, false, false>(B, s, B->d(B->o_qnet), EB_Store{B->d(B->o_f1), 0}, TE_ToYB{}, nullptr);
+  face_pass<1, false, false>(B, s, B->d(B->o_f1), EB_Store{B->d(B->o_sigma), 1}, TE_Store{B->d(B->o_sigma), 1},
+                             nullptr);
   kb_assemble<<<B->tot_blk, BT, 0, s>>>(v, B->d(B->o_Zt), B->d(B->o_Wtt), B->d(B->o_sigma), B->d(B->o_A));
-  g_blaunch += 6;
+  g_blaunch += 1;
 }
 
 void enqueue_picard(sgh_batch* B, cudaStream_t s, cudaGraphConditionalHandle h, int in_graph) {
   const BView v = B->view();
-  kb_face_axis<0, true, true, EB_Store><<<B->tot_tile, AX_THREADS, 0, s>>>(v, B->d(B->o_A), EB_Store{B->d(B->o_f1), 0},
-                                                                    nullptr);
-  kb_face_axis<1, true, true, EB_TopFlux><<<B->tot_tile, AX_THREADS, 0, s>>>(
-      v, B->d(B->o_f1), EB_TopFlux{B->d(B->o_qlas), B->d(B->o_qev), B->d(B->o_qnet)}, nullptr);
-  kb_face_axis<0, false, true, EB_Store><<<B->tot_tile, AX_THREADS, 0, s>>>(v, B->d(B->o_qnet),
-                                                                     EB_Store{B->d(B->o_f1), 0}, nullptr);
-  kb_face_axis<1, false, true, EB_Store><<<B->tot_tile, AX_THREADS, 0, s>>>(v, B->d(B->o_f1),
-                                                                     EB_Store{B->d(B->o_Stop), 1}, nullptr);
+  face_pass<0, true, true>(B, s, B->d(B->o_A), EB_Store{B->d(B->o_f1), 0}, TE_ToYB{}, nullptr);
+  face_pass<1, true, true>(B, s, B->d(B->o_f1), EB_TopFlux{B->d(B->o_qlas), B->d(B->o_qev), B->d(B->o_qnet)},
+                           TE_TopFlux{B->d(B->o_qlas), B->d(B->o_qev), B->d(B->o_qnet)}, nullptr);
+  face_pass<0, false, true>(B, s, B->d(B->o_qnet), EB_Store{B->d(B->o_f1), 0}, TE_ToYB{}, nullptr);
+  face_pass<1, false, true>(B, s, B->d(B->o_f1), EB_Store{B->d(B->o_Stop), 1}, TE_Store{B->d(B->o_Stop), 1},
+                            nullptr);
   kb_relax<<<B->tot_blk, BT, 0, s>>>(v, B->d(B->o_Zt), B->d(B->o_Yt), B->d(B->o_Wtt), B->d(B->o_Qtt),
                                      B->d(B->o_Stop), B->d(B->o_sigma), B->d(B->o_A), B->d(B->o_prelax));
   kb_converge<<<1, CT, 0, s>>>(v, B->d(B->o_prelax), B->d(B->o_pn1), h, in_graph);
-  g_blaunch += 6;
+  g_blaunch += 2;
 }
 
 template <class R>
@@ -604,14 +851,15 @@ void enqueue_post(sgh_batch* B, cudaStream_t s, cudaGraphConditionalHandle h, in
   R* a = reinterpret_cast<R*>(B->ws + B->o_a);
   R* K = reinterpret_cast<R*>(B->ws + B->o_K);
   R* KK = reinterpret_cast<R*>(B->ws + B->o_KK);
-  kb_face_axis<0, true, false, EB_Store><<<B->tot_tile, AX_THREADS, 0, s>>>(v, B->d(B->o_A), EB_Store{B->d(B->o_f1), 0},
-                                                                     nullptr);
-  kb_face_axis<1, true, false, EB_CommitSurface><<<B->tot_tile, AX_THREADS, 0, s>>>(
-      v, B->d(B->o_f1), EB_CommitSurface{B->d(B->o_Tsurf), B->d(B->o_qev), B->d(B->o_qevold)},
-      B->d(B->o_ptile));
+  face_pass<0, true, false>(B, s, B->d(B->o_A), EB_Store{B->d(B->o_f1), 0}, TE_ToYB{}, nullptr);
+  face_pass<1, true, false>(B, s, B->d(B->o_f1),
+                            EB_CommitSurface{B->d(B->o_Tsurf), B->d(B->o_qev), B->d(B->o_qevold)},
+                            TE_CommitSurface{B->d(B->o_Tsurf), B->d(B->o_qev), B->d(B->o_qevold)},
+                            B->d(B->o_ptile));
   kb_commit_modes<R><<<B->tot_blk, BT, 0, s>>>(v, a, K, KK, B->d(B->o_sigma));
-  kb_commit<<<1, CT, 0, s>>>(v, B->d(B->o_plas), B->d(B->o_ptile), h, in_graph);
-  g_blaunch += 4;
+  kb_commit<<<1, CT, 0, s>>>(v, B->d(B->o_plas), B->d(B->o_ptile),
+                             B->precision == SGH_PRECISION_MIXED ? 1 : 0, h, in_graph);
+  g_blaunch += 2;
 }
 
 template <class R>
@@ -720,9 +968,20 @@ int sgh_batch_create(const sgh_config* cfgs, int32_t n, int32_t precision, sgh_b
     moff += 2LL * kv.first * kv.first;
   }
   B->mat_elems = moff;
+  std::map<int, long long> mplane;
+  if (precision == SGH_PRECISION_MIXED) {
+    long long po = 0;
+    for (auto& kv : mats) {
+      mplane[kv.first] = po;
+      B->mplane_list.push_back({kv.first, po});
+      po += 2LL * (long long)umma::plane_bytes(kv.first, kv.first);
+    }
+    B->mp_bytes = (size_t)po;
+  }
   B->blk_start.assign(n + 1, 0);
   B->tile_start.assign(n + 1, 0);
   B->vblk_start.assign(n + 1, 0);
+  B->utile_start.assign(n + 1, 0);
   for (int i = 0; i < n; ++i) {
     const sgh_config& c = cfgs[i];
     BSlot sl;
@@ -743,6 +1002,18 @@ int sgh_batch_create(const sgh_config* cfgs, int32_t n, int32_t precision, sgh_b
     sl.ntile = face_tiles(c.nx, c.ny);
     sl.vblk0 = B->tot_vblk;
     sl.nvblk = cdivl(sl.V, BT);
+    sl.utile0 = B->tot_utile;
+    sl.nutile = face_utiles(c.nx, c.ny);
+    if (precision == SGH_PRECISION_MIXED) {
+      sl.xa = (long long)B->xa_bytes;
+      sl.yb = (long long)B->yb_bytes;
+      B->xa_bytes += umma::plane_bytes(c.ny, c.nx);
+      B->yb_bytes += umma::plane_bytes(c.nx, c.ny);
+      sl.mpx = mplane[c.nx];
+      sl.mpx_inv = sl.mpx + (long long)umma::plane_bytes(c.nx, c.nx);
+      sl.mpy = mplane[c.ny];
+      sl.mpy_inv = sl.mpy + (long long)umma::plane_bytes(c.ny, c.ny);
+    }
     sl.Lx = c.Lx; sl.Ly = c.Ly; sl.Lz = c.Lz;
     sl.dx = c.Lx / c.nx; sl.dy = c.Ly / c.ny;
     sl.dt = c.dt;
@@ -770,9 +1041,11 @@ int sgh_batch_create(const sgh_config* cfgs, int32_t n, int32_t precision, sgh_b
     B->tot_blk += sl.nblk;
     B->tot_tile += sl.ntile;
     B->tot_vblk += sl.nvblk;
+    B->tot_utile += sl.nutile;
     B->blk_start[i + 1] = B->tot_blk;
     B->tile_start[i + 1] = B->tot_tile;
     B->vblk_start[i + 1] = B->tot_vblk;
+    B->utile_start[i + 1] = B->tot_utile;
   }
   LayoutB L;
   const size_t F8 = sizeof(double) * (size_t)B->tot_face;
@@ -783,6 +1056,7 @@ int sgh_batch_create(const sgh_config* cfgs, int32_t n, int32_t precision, sgh_b
   B->o_blk = L.take(sizeof(int) * (n + 1));
   B->o_tile = L.take(sizeof(int) * (n + 1));
   B->o_vblk = L.take(sizeof(int) * (n + 1));
+  B->o_utile = L.take(sizeof(int) * (n + 1));
   B->o_mats = L.take(sizeof(double) * (size_t)B->mat_elems);
   B->o_ct = L.take(sizeof(double) * (size_t)B->tot_z);
   B->o_a = L.take(VE);
@@ -804,7 +1078,15 @@ int sgh_batch_create(const sgh_config* cfgs, int32_t n, int32_t precision, sgh_b
   B->o_plas = L.take(sizeof(double) * B->tot_blk);
   B->o_pn1 = L.take(sizeof(double) * B->tot_blk);
   B->o_prelax = L.take(sizeof(double) * 2 * B->tot_blk);
-  B->o_ptile = L.take(sizeof(double) * B->tot_tile);
+  B->o_ptile = L.take(sizeof(double) * std::max(B->tot_tile, B->tot_utile));
+  if (precision == SGH_PRECISION_MIXED) {
+    B->o_xah = L.take(B->xa_bytes);
+    B->o_xal = L.take(B->xa_bytes);
+    B->o_ybh = L.take(B->yb_bytes);
+    B->o_ybl = L.take(B->yb_bytes);
+    B->o_mph = L.take(B->mp_bytes);
+    B->o_mpl = L.take(B->mp_bytes);
+  }
   B->ws_need = L.off;
   *out = B;
   return SGH_OK;
@@ -841,12 +1123,31 @@ int sgh_batch_bind(sgh_batch* B, void* workspace, uint64_t bytes, void* stream) 
   SGB_CK(cudaMemcpyAsync(B->ws + B->o_blk, B->blk_start.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice, s));
   SGB_CK(cudaMemcpyAsync(B->ws + B->o_tile, B->tile_start.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice, s));
   SGB_CK(cudaMemcpyAsync(B->ws + B->o_vblk, B->vblk_start.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice, s));
+  SGB_CK(cudaMemcpyAsync(B->ws + B->o_utile, B->utile_start.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice, s));
   SGB_CK(cudaMemsetAsync(B->ws + B->o_qevold, 0, sizeof(double) * B->tot_face, s));
   SGB_CK(cudaMemsetAsync(B->ws + B->o_qev, 0, sizeof(double) * B->tot_face, s));
   for (auto& m : B->mat_list)
     kb_dct_matrix<<<cdivl((long long)m.first * m.first, BT), BT, 0, s>>>(m.first, B->d(B->o_mats) + m.second);
   const BView v = B->view();
   if (B->precision == SGH_PRECISION_MIXED) {
+    SGB_CK(cudaMemsetAsync(B->ws + B->o_xah, 0, B->xa_bytes, s));
+    SGB_CK(cudaMemsetAsync(B->ws + B->o_xal, 0, B->xa_bytes, s));
+    SGB_CK(cudaMemsetAsync(B->ws + B->o_ybh, 0, B->yb_bytes, s));
+    SGB_CK(cudaMemsetAsync(B->ws + B->o_ybl, 0, B->yb_bytes, s));
+    SGB_CK(cudaMemsetAsync(B->ws + B->o_mph, 0, B->mp_bytes, s));
+    SGB_CK(cudaMemsetAsync(B->ws + B->o_mpl, 0, B->mp_bytes, s));
+    for (size_t j = 0; j < B->mplane_list.size(); ++j) {
+      const int N = B->mplane_list[j].first;
+      const long long po = B->mplane_list[j].second;
+      long long moff = -1;
+      for (auto& m : B->mat_list)
+        if (m.first == N) moff = m.second;
+      const size_t pb = umma::plane_bytes(N, N);
+      for (int inv = 0; inv < 2; ++inv)
+        kb_matrix_planes<<<cdivl((long long)N * N, BT), BT, 0, s>>>(
+            N, B->d(B->o_mats) + moff, inv, reinterpret_cast<__nv_bfloat16*>(B->ws + B->o_mph + po + inv * pb),
+            reinterpret_cast<__nv_bfloat16*>(B->ws + B->o_mpl + po + inv * pb));
+    }
     float* K = reinterpret_cast<float*>(B->ws + B->o_K);
     float* KK = reinterpret_cast<float*>(B->ws + B->o_KK);
     kb_tables<float><<<B->tot_vblk, BT, 0, s>>>(v, K, KK, B->d(B->o_ct));
@@ -905,6 +1206,27 @@ int sgh_batch_step(sgh_batch* B, int32_t n_steps, void* stream) {
   return SGH_OK;
 }
 
+int sgh_batch_step_eager(sgh_batch* B, void* stream) {
+  if (!B || !B->bound) return bfail(SGH_ERR_STATE, "batch is not bound");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  kb_run_setup<<<1, 1, 0, s>>>(B->view(), 1);
+  const bool mixed = B->precision == SGH_PRECISION_MIXED;
+  if (mixed) enqueue_pre<float>(B, s, 0, 0);
+  else enqueue_pre<double>(B, s, 0, 0);
+  for (int it = 0; it < 1000000; ++it) {
+    BGlobal g;
+    SGB_CK(cudaMemcpyAsync(&g, B->ws + B->o_g, sizeof(BGlobal), cudaMemcpyDeviceToHost, s));
+    SGB_CK(cudaStreamSynchronize(s));
+    if (!g.picard_any) break;
+    enqueue_picard(B, s, 0, 0);
+  }
+  if (mixed) enqueue_post<float>(B, s, 0, 0);
+  else enqueue_post<double>(B, s, 0, 0);
+  SGB_CK(cudaGetLastError());
+  SGB_CK(cudaStreamSynchronize(s));
+  return SGH_OK;
+}
+
 int sgh_batch_status(const sgh_batch* B, sgh_batch_slot_info* out, void* stream) {
   if (!B || !B->bound || !out) return bfail(SGH_ERR_INVALID, "batch not bound or null output");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -938,6 +1260,16 @@ int sgh_batch_buffer(const sgh_batch* B, int32_t slot, int32_t which, void** ptr
   }
   *ptr = B->ws + off;
   if (bytes) *bytes = nb;
+  return SGH_OK;
+}
+
+int sgh_batch_error(const sgh_batch* B, int32_t* err, void* stream) {
+  if (!B || !B->bound || !err) return bfail(SGH_ERR_INVALID, "batch not bound or null output");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  BGlobal g;
+  SGB_CK(cudaMemcpyAsync(&g, B->ws + B->o_g, sizeof(BGlobal), cudaMemcpyDeviceToHost, s));
+  SGB_CK(cudaStreamSynchronize(s));
+  *err = g.umma_err;
   return SGH_OK;
 }
 

@@ -256,5 +256,148 @@ __device__ void tile_bf16x3(int M, int N, int K, int m0, int n0, const LA& la, c
   if (warp == 0) tmem_dealloc(tmem, NCOLS);
 }
 
+// ---------------------------------------------------------------------------
+// Operand planes fed by bulk copies
+// ---------------------------------------------------------------------------
+// A plane holds one BF16 part (hi or lo) of an R x K operand, K-major, cut into
+// 128-row x 32-wide chunks of 8 KB; each chunk is contiguous and laid out in
+// core matrices exactly as the shared-memory stage (core_off), so one bulk
+// copy moves it. Chunk (rt, kc) sits at byte (rt * nkc + kc) * CHUNK_BYTES.
+// Rows and k beyond the operand are zero (planes are cleared once).
+constexpr int CHUNK_BYTES = TM * KC * 2;  // 8192
+
+__host__ __device__ inline size_t plane_bytes(int rows, int k) {
+  return (size_t)((rows + TM - 1) / TM) * (size_t)((k + KC - 1) / KC) * CHUNK_BYTES;
+}
+__device__ __forceinline__ size_t plane_off(int r, int k, int nkc) {
+  const int rt = r / TM, kc = k / KC;
+  return (size_t)(rt * nkc + kc) * CHUNK_BYTES + core_off(r % TM, k % KC, TM);
+}
+__device__ __forceinline__ void plane_put(__nv_bfloat16* hi, __nv_bfloat16* lo, int r, int k, int nkc, double x) {
+  __nv_bfloat16 h, l;
+  split_bf16(x, h, l);
+  const size_t o = plane_off(r, k, nkc) / 2;
+  hi[o] = h;
+  lo[o] = l;
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// Dynamic shared memory of tile_planes (bytes): 2 stages x 4 chunks + barriers.
+__host__ __device__ constexpr int planes_smem_bytes() { return 2 * 4 * CHUNK_BYTES + 128; }
+
+// One 128 x 128 tile D[m][n] = sum_k A(m, k) B(n, k) from operand planes.
+// a_hi/a_lo point at chunk (rt, 0) of A's planes, b_hi/b_lo at chunk (ct, 0)
+// of B's; nkc chunks along k. Thread 0 drives the bulk copies and the MMAs
+// (copies of chunk c+1 overlap the MMAs of chunk c); all 128 threads run the
+// epilogue epi(m_local, n_local, value) for every element of the tile (the
+// caller bounds-checks). Bounded waits as in tile_bf16x3.
+template <class EPI>
+__device__ void tile_planes(const char* a_hi, const char* a_lo, const char* b_hi, const char* b_lo, int nkc,
+                            const EPI& epi, char* smem, int* err) {
+  constexpr uint32_t NT = 128, NCOLS = 128;
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + 8 * CHUNK_BYTES);
+  uint64_t* done = full + 2;
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(full + 4);
+  volatile int* okflag = reinterpret_cast<volatile int*>(full + 5);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const uint32_t idesc = idesc_bf16_f32(TM, NT);
+
+  if (warp == 0) tmem_alloc(tslot, NCOLS);
+  if (tid == 0) {
+    mbar_init(&full[0], 1);
+    mbar_init(&full[1], 1);
+    mbar_init(&done[0], 1);
+    mbar_init(&done[1], 1);
+    *okflag = 1;
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tslot;
+
+  if (tid == 0) {
+    uint32_t fph[2] = {0u, 0u}, dph[2] = {0u, 0u};
+    bool ok = true;
+    auto load = [&](int ch) {
+      const int b = ch & 1;
+      char* st = smem + b * 4 * CHUNK_BYTES;
+      const size_t off = (size_t)ch * CHUNK_BYTES;
+      mbar_expect_tx(&full[b], 4 * CHUNK_BYTES);
+      bulk_g2s(st, a_hi + off, CHUNK_BYTES, &full[b]);
+      bulk_g2s(st + CHUNK_BYTES, a_lo + off, CHUNK_BYTES, &full[b]);
+      bulk_g2s(st + 2 * CHUNK_BYTES, b_hi + off, CHUNK_BYTES, &full[b]);
+      bulk_g2s(st + 3 * CHUNK_BYTES, b_lo + off, CHUNK_BYTES, &full[b]);
+    };
+    if (nkc > 0) load(0);
+    for (int ch = 0; ch < nkc && ok; ++ch) {
+      const int b = ch & 1;
+      if (!mbar_wait_bounded(&full[b], fph[b])) { ok = false; break; }
+      fph[b] ^= 1u;
+      tc_fence_after();
+      const uint32_t s0 = smem_u32(smem + b * 4 * CHUNK_BYTES);
+      const uint32_t ah = s0, al = s0 + CHUNK_BYTES, bh = s0 + 2 * CHUNK_BYTES, bl = s0 + 3 * CHUNK_BYTES;
+#pragma unroll
+      for (int s = 0; s < KC / 16; ++s) {
+        const uint32_t o = (uint32_t)(2 * s * (TM / 8) * 128);
+        const uint64_t dah = smem_desc(ah + o, (TM / 8) * 128, 128);
+        const uint64_t dal = smem_desc(al + o, (TM / 8) * 128, 128);
+        const uint64_t dbh = smem_desc(bh + o, (TM / 8) * 128, 128);
+        const uint64_t dbl = smem_desc(bl + o, (TM / 8) * 128, 128);
+        mma_bf16(tmem, dah, dbh, idesc, (ch > 0 || s > 0) ? 1u : 0u);
+        mma_bf16(tmem, dah, dbl, idesc, 1u);
+        mma_bf16(tmem, dal, dbh, idesc, 1u);
+      }
+      mma_commit(&done[b]);
+      if (ch + 1 < nkc) {
+        const int nb = (ch + 1) & 1;
+        if (ch >= 1) {  // stage nb was read by the MMAs of chunk ch-1
+          if (!mbar_wait_bounded(&done[nb], dph[nb])) { ok = false; break; }
+          dph[nb] ^= 1u;
+        }
+        load(ch + 1);
+      }
+    }
+    if (ok && nkc > 0) {
+      const int b = (nkc - 1) & 1;
+      if (!mbar_wait_bounded(&done[b], dph[b])) ok = false;
+    }
+    if (!ok) {
+      atomicExch(err, 1);
+      *okflag = 0;
+      for (int b = 0; b < 2; ++b) {  // drain (bounded) before the memory is freed
+        mbar_wait_bounded(&full[b], fph[b]);
+        mbar_wait_bounded(&done[b], dph[b]);
+      }
+    }
+  }
+  __syncthreads();
+  if (*okflag) {
+    tc_fence_after();
+    const int m = warp * 32 + lane;
+#pragma unroll 1
+    for (int c = 0; c < (int)NT; c += 16) {
+      float v[16];
+      tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c, v);
+#pragma unroll
+      for (int i = 0; i < 16; ++i) epi(m, c + i, (double)v[i]);
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tmem_dealloc(tmem, NCOLS);
+}
+
 }  // namespace umma
 }  // namespace sgh

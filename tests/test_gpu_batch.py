@@ -1,6 +1,7 @@
 """Batched slots of uneven size: each slot equals its single-instance run and
-the oracle, is the same alone and in a mix, and the mixed (FP32-state) form
-stays within 1e-4 relative L2 of the FP64 oracle on a converged-Picard case."""
+the oracle, is the same alone and in a mix, and the mixed form (FP32 state,
+split-BF16 tensor-core face contractions) stays within 1e-4 relative L2 of
+the FP64 oracle on a converged-Picard case."""
 import numpy as np
 import pytest
 
@@ -73,6 +74,7 @@ def test_slot_alone_equals_slot_in_mix():
     alone = BatchSolver([ctxs[late]], "mixed")
     alone.start(0, steps)
     alone.step(steps)
+    assert mix.tensor_core_error() == 0 and alone.tensor_core_error() == 0
     assert np.array_equal(mix.modes(late).cpu().numpy(), alone.modes(0).cpu().numpy())
     assert [m["n_evap_iter"] for m in mix.metrics(late)] == \
         [m["n_evap_iter"] for m in alone.metrics(0)]
@@ -98,6 +100,7 @@ def test_mixed_precision_error_vs_fp64_oracle():
     from oracle.sgh_oracle import dct3
     T_mixed = dct3(b.modes(0).double().cpu().numpy())
     T_ref = dct3(o.a)
+    assert b.tensor_core_error() == 0
     assert rel_l2(T_mixed, T_ref) < 1e-4
     b.close()
 
