@@ -35,7 +35,6 @@ namespace sgh {
 namespace batch {
 
 constexpr int BT = 256;   // threads of element / column / face kernels
-constexpr int FT = 16;    // face transform tile edge
 constexpr int CT = 1024;  // threads of the per-slot control kernels
 
 struct BSlot {
@@ -50,7 +49,7 @@ struct BSlot {
   int tile0, ntile;  // face transform tiles
   int vblk0, nvblk;  // volume blocks (setup kernels)
   int utile0, nutile;  // tensor-core face tiles (mixed precision)
-  long long xa, yb;    // byte offsets of the slot's x-pass A plane and y-pass B plane
+  long long xa;        // byte offset of the slot's face planes (rows y, k = x) in the xa / xq arenas
   long long mpx, mpy;  // byte offsets of the forward x / y matrix planes (inverse at + mp_inv)
   long long mpx_inv, mpy_inv;
   double dx, dy, dt, Lx, Ly, Lz;
@@ -66,7 +65,8 @@ struct BState {
   const sgh_laser* table;
   sgh_step_out* outs;
   int n_steps, step, active, iters;
-  int iter, done, status, pad;
+  int iter, done, status;
+  unsigned tickets;  // kb_relax blocks of this slot done in the current launch
   double I0, shift_x, shift_y, rel_err;
   sgh_step_out last;
 };
@@ -75,7 +75,7 @@ struct BGlobal {
   int steps_left;
   int umma_err;     // nonzero once a tensor-core wait expired
   int picard_any;   // some slot is still iterating (read by the eager step)
-  int pad;
+  unsigned blocks_done;  // ticket counter of kb_relax (back to 0 after each launch)
 };
 
 // Device view of a bound batch (passed by value to every kernel).
@@ -87,10 +87,10 @@ struct BView {
   const int* tile_start;  // n + 1
   const int* vblk_start;  // n + 1
   const int* utile_start; // n + 1 (tensor-core face tiles)
-  __nv_bfloat16* xa_hi;   // operand planes (mixed precision; null otherwise)
-  __nv_bfloat16* xa_lo;
-  __nv_bfloat16* yb_hi;
-  __nv_bfloat16* yb_lo;
+  __nv_bfloat16* xa_hi;   // operand planes (mixed precision; null otherwise):
+  __nv_bfloat16* xa_lo;   //   xa = A = Zt + W_tt sigma, input of the inverse transform
+  __nv_bfloat16* xq_hi;   //   xq = q_net, input of the forward transform
+  __nv_bfloat16* xq_lo;
   const char* mp_hi;      // DCT matrix planes
   const char* mp_lo;
   const double* mats;
@@ -108,11 +108,39 @@ __device__ __forceinline__ int find_slot(const int* start, int n, int b) {
   return lo;
 }
 
-// x-pass A-operand plane element (y, x) of slot sl (mixed precision only).
-__device__ __forceinline__ void xa_put(const BView& v, const BSlot& sl, int y, int x, double val) {
-  if (!v.xa_hi) return;
+// Eight lanes 8g..8g+7 of a warp hold consecutive k = k0..k0+7 (k0 % 8 == 0)
+// of one plane row; lane 8g writes the group's 16-byte hi and lo rows. Call
+// from all 32 lanes; `store` is read on lane 8g only.
+__device__ __forceinline__ void plane_put8_warp(__nv_bfloat16* hi, __nv_bfloat16* lo, int r, int k0, int nkc,
+                                                double val, bool store) {
+  __nv_bfloat16 h, l;
+  umma::split_bf16(val, h, l);
+  const uint32_t hv = __bfloat16_as_ushort(h), lv = __bfloat16_as_ushort(l);
+  const uint32_t hp = hv | (__shfl_down_sync(0xffffffffu, hv, 1) << 16);
+  const uint32_t lp = lv | (__shfl_down_sync(0xffffffffu, lv, 1) << 16);
+  const uint32_t h1 = __shfl_down_sync(0xffffffffu, hp, 2), l1 = __shfl_down_sync(0xffffffffu, lp, 2);
+  const uint32_t h2 = __shfl_down_sync(0xffffffffu, hp, 4), l2 = __shfl_down_sync(0xffffffffu, lp, 4);
+  const uint32_t h3 = __shfl_down_sync(0xffffffffu, hp, 6), l3 = __shfl_down_sync(0xffffffffu, lp, 6);
+  if ((threadIdx.x & 7) == 0 && store) {
+    const size_t o = umma::plane_off(r, k0, nkc);
+    *reinterpret_cast<uint4*>(reinterpret_cast<char*>(hi) + o) = make_uint4(hp, h1, h2, h3);
+    *reinterpret_cast<uint4*>(reinterpret_cast<char*>(lo) + o) = make_uint4(lp, l1, l2, l3);
+  }
+}
+
+// Face-plane element i = y * nx + x of slot sl (hi/lo: the xa or xq arena,
+// null in FP64 batches), written by a whole block of consecutive i (one slot
+// per block). When nx % 8 == 0 every aligned group of 8 lanes is 8
+// consecutive x of one row and goes out as one 16-byte store per part.
+__device__ __forceinline__ void plane_put_block(__nv_bfloat16* hi, __nv_bfloat16* lo, const BSlot& sl, int i,
+                                                double val, bool valid) {
+  if (!hi) return;
   const int nkc = (sl.nx + umma::KC - 1) / umma::KC;
-  umma::plane_put(v.xa_hi + sl.xa / 2, v.xa_lo + sl.xa / 2, y, x, nkc, val);
+  const int y = i / sl.nx, x = i - (i / sl.nx) * sl.nx;
+  if ((sl.nx & 7) == 0)
+    plane_put8_warp(hi + sl.xa / 2, lo + sl.xa / 2, y, x, nkc, valid ? val : 0.0, valid);
+  else if (valid)
+    umma::plane_put(hi + sl.xa / 2, lo + sl.xa / 2, y, x, nkc, val);
 }
 
 // ---------------------------------------------------------------------------
@@ -263,7 +291,7 @@ kb_face_begin(BView v, double* q_las, double* q_net, const double* q_evold, doub
   const BState& st = v.st[s];
   if (!st.active) return;
   const int i = (b - sl.blk0) * BT + threadIdx.x;
-  double sum = 0.0, dummy = 0.0;
+  double sum = 0.0, dummy = 0.0, qn = 0.0;
   if (i < sl.S) {
     const int nx = sl.nx, ny = sl.ny;
     const int y = i / nx, x = i - y * nx;
@@ -277,9 +305,10 @@ kb_face_begin(BView v, double* q_las, double* q_net, const double* q_evold, doub
     double val = ty.w0 * (tx.w0 * f[ty.i0 * nx + tx.i0] + tx.w1 * f[ty.i0 * nx + tx.i1]) +
                  ty.w1 * (tx.w0 * f[ty.i1 * nx + tx.i0] + tx.w1 * f[ty.i1 * nx + tx.i1]);
     if (!(ty.in && tx.in)) val = 0.0;
-    q_net[sl.face + i] = q - val;
-    xa_put(v, sl, y, x, q - val);
+    qn = q - val;
+    q_net[sl.face + i] = qn;
   }
+  plane_put_block(v.xq_hi, v.xq_lo, sl, i, qn, i < sl.S);
   block_sum2<BT>(sum, dummy, sh);
   if (threadIdx.x == 0) part_las[b] = sum;
 }
@@ -322,11 +351,12 @@ kb_assemble(BView v, const double* Zt, const double* Wtt, const double* sigma, d
   const BSlot& sl = v.slot[s];
   if (!v.st[s].active) return;
   const int i = (b - sl.blk0) * BT + threadIdx.x;
+  double a = 0.0;
   if (i < sl.S) {
-    const double a = Zt[sl.face + i] + Wtt[sl.face + i] * sigma[sl.face + i];
+    a = Zt[sl.face + i] + Wtt[sl.face + i] * sigma[sl.face + i];
     A[sl.face + i] = a;
-    xa_put(v, sl, i / sl.nx, i % sl.nx, a);
   }
+  plane_put_block(v.xa_hi, v.xa_lo, sl, i, a, i < sl.S);
 }
 
 // ---- batched face transform: one 2 x 4-register-tile block per tile ------
@@ -384,182 +414,330 @@ __global__ void __launch_bounds__(AX_THREADS) kb_face_axis(BView v, const double
   }
 }
 
-// ---- batched face transform on the tensor cores (mixed precision) ---------
-// Same contraction as kb_face_axis, as 128 x UNT tiles of split-BF16 products
-// accumulated in FP32 in tensor memory (sgh_umma.cuh); slot tiles:
-// ceil(ny / 128) * ceil(nx / UNT) in both directions.
-constexpr int UNT = 128;
-inline __host__ __device__ int face_utiles(int nx, int ny) {
-  return ((ny + umma::TM - 1) / umma::TM) * ((nx + UNT - 1) / UNT);
+// ---- fused 2-D face transform on the tensor cores (mixed precision) -------
+// One CTA transforms one 128-column block of a slot's face along both axes:
+//   x-pass  X1[y][c] = sum_x P[y][x] Mx[c][x]    (P: the slot's xa or xq plane)
+//   y-pass  G[r][c]  = sum_y My[r][y] X1[y][c]
+// for every row y < ny (ny <= 256: one or two 128-row tiles). Each x-pass row
+// tile accumulates in tensor memory, is split into BF16 hi/lo and written to
+// shared memory as the K-major B operand of the y-pass; the y-pass row tiles
+// accumulate in tensor memory and reach the epilogue through a shared-memory
+// tile. Separability makes the column blocks independent: a slot's transform
+// needs no exchange between CTAs. One thread streams every operand chunk (the
+// x-pass P and Mx chunks, then the My chunks) through one ring of bulk-copy
+// stages and issues the MMAs, so the My copies are in flight while the x-pass
+// result is being converted. Operands are split-BF16 (three MMAs per k-step,
+// FP32 accumulation), as in tile_planes.
+namespace f2 {
+constexpr int THREADS = 256;
+constexpr int CB = umma::CHUNK_BYTES;  // one 128 x 32 BF16 chunk (8 KB)
+constexpr int STAGE = 4 * CB;          // 32 KB
+constexpr int MAX_STAGES = 6;
+constexpr int SMEM_LIMIT = 227 * 1024;
+constexpr int TAIL = 256;              // barriers, TMEM address, status flag
+constexpr int MAX_NY = 256;
+inline int bop_bytes(int max_ny) { return ((max_ny + 31) / 32) * 2 * CB; }
+inline int stages(int max_ny) {
+  const int s = (SMEM_LIMIT - 1024 - TAIL - bop_bytes(max_ny)) / STAGE;
+  return s < MAX_STAGES ? s : MAX_STAGES;
 }
+inline int smem_bytes(int max_ny) { return bop_bytes(max_ny) + stages(max_ny) * STAGE + TAIL; }
+}  // namespace f2
 
-struct ULoadX {  // DIR 0, A(m = y, k = n) = in[y][n]
-  const double* p;
-  int nx;
-  __device__ __forceinline__ double operator()(int m, int k) const { return p[(size_t)m * nx + k]; }
-};
-struct ULoadM {  // matrix rows: M(r, k) = M[r * N + k]
-  const double* p;
-  int N;
-  __device__ __forceinline__ double operator()(int r, int k) const { return p[(size_t)r * N + k]; }
-};
-struct ULoadT {  // DIR 1, B(n = x, k = n') = in[n'][x]
-  const double* p;
-  int nx;
-  __device__ __forceinline__ double operator()(int r, int k) const { return p[(size_t)k * nx + r]; }
-};
+inline __host__ __device__ int face_utiles(int nx, int) { return (nx + 127) / 128; }
 
-template <class Epi>
-struct UEpi {  // (m, n, v) -> batched epilogue on face index m * nx + n
-  const BSlot* sl;
-  BState* st;
-  Epi e;
-  Red* r;
-  __device__ __forceinline__ void operator()(int m, int n, double v) const {
-    e(*sl, *st, sl->face + (long long)m * sl->nx + n, v, *r);
-  }
+// Epilogue of the fused transform, on output element (r, c) of the slot's face:
+//   F2_STORE    FP64 face array (x dct_scale if scaled)
+//   F2_TOPFLUX  T_s -> evaporation -> q_evap (FP64), q_net -> xq plane
+//   F2_COMMIT   T_temp, its block max, q_evap_old <- q_evap
+enum { F2_STORE = 0, F2_TOPFLUX = 1, F2_COMMIT = 2 };
+
+struct FaceParams {  // per-slot constants held in registers by the epilogues
+  long long face, xa;
+  int nx, ny;
+  double recon_scale, dct_scale, T_liquidus, T_boil, evap_f1, evap_f2;
 };
 
-template <int DIR, bool INV, bool SKIP_DONE, class Epi>
-__global__ void __launch_bounds__(umma::THREADS)
-kb_face_umma(BView v, const double* in, Epi epi, double* part_tile) {
-  extern __shared__ __align__(128) char usmem[];
-  __shared__ double red[umma::THREADS / 32];
-  const int b = blockIdx.x;
-  const int s = find_slot(v.utile_start, v.n, b);
-  const BSlot& sl = v.slot[s];
-  BState& st = v.st[s];
-  if (!st.active || (SKIP_DONE && st.done)) return;
-  const int t = b - sl.utile0;
-  const int nx = sl.nx, ny = sl.ny;
-  const int nct = (nx + UNT - 1) / UNT;
-  const int n0 = (t % nct) * UNT, m0 = (t / nct) * umma::TM;
-  const int N = DIR == 0 ? nx : ny;
-  const double* M = v.mats + (DIR == 0 ? sl.mx : sl.my) + (INV ? (size_t)N * N : 0);
-  const double* X = in + sl.face;
-  Red r;
-  UEpi<Epi> ue{&sl, &st, epi, &r};
-  if (DIR == 0)
-    umma::tile_bf16x3<UNT>(ny, nx, nx, m0, n0, ULoadX{X, nx}, ULoadM{M, nx}, ue, usmem, &v.g->umma_err);
-  else
-    umma::tile_bf16x3<UNT>(ny, nx, ny, m0, n0, ULoadM{M, ny}, ULoadT{X, nx}, ue, usmem, &v.g->umma_err);
-  if (Epi::kMax) {
-    double m = r.mx;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double mm = red[0];
-      for (int w = 1; w < umma::THREADS / 32; ++w) mm = fmax(mm, red[w]);
-      part_tile[b] = mm;
-    }
-  }
-}
-
-// ---- batched face transform fed from operand planes (mixed precision) ---
-// DIR 0 (x-pass): A = the slot's x-pass plane (rows y, k = x), B = the x
-// matrix plane (rows k, k = n); DIR 1 (y-pass): A = the y matrix plane, B =
-// the slot's y-pass plane (rows x, k = y). epi(sl, st, m, n, value, r) gets
-// every in-range element, (m, n) = (y, k) for DIR 0 and (k, x) for DIR 1.
-template <int DIR, bool INV, bool SKIP_DONE, class Epi>
-__global__ void __launch_bounds__(umma::THREADS) kb_face_tc(BView v, Epi epi, double* part_tile) {
-  extern __shared__ __align__(128) char usmem[];
-  __shared__ double red[umma::THREADS / 32];
-  const int b = blockIdx.x;
-  const int s = find_slot(v.utile_start, v.n, b);
-  const BSlot& sl = v.slot[s];
-  BState& st = v.st[s];
-  if (!st.active || (SKIP_DONE && st.done)) return;
-  const int t = b - sl.utile0;
-  const int nx = sl.nx, ny = sl.ny;
-  const int nct = (nx + UNT - 1) / UNT;
-  const int rt = t / nct, ct = t % nct;
-  const int nkc = ((DIR == 0 ? nx : ny) + umma::KC - 1) / umma::KC;
-  const size_t cb = (size_t)umma::CHUNK_BYTES;
-  const char *ah, *al, *bh, *bl;
-  if (DIR == 0) {
-    ah = reinterpret_cast<const char*>(v.xa_hi) + sl.xa + rt * nkc * cb;
-    al = reinterpret_cast<const char*>(v.xa_lo) + sl.xa + rt * nkc * cb;
-    const long long mp = INV ? sl.mpx_inv : sl.mpx;
-    bh = v.mp_hi + mp + ct * nkc * cb;
-    bl = v.mp_lo + mp + ct * nkc * cb;
-  } else {
-    const long long mp = INV ? sl.mpy_inv : sl.mpy;
-    ah = v.mp_hi + mp + rt * nkc * cb;
-    al = v.mp_lo + mp + rt * nkc * cb;
-    bh = reinterpret_cast<const char*>(v.yb_hi) + sl.yb + ct * nkc * cb;
-    bl = reinterpret_cast<const char*>(v.yb_lo) + sl.yb + ct * nkc * cb;
-  }
-  Red r;
-  const int m0 = rt * umma::TM, n0 = ct * UNT;
-  const int Mrows = ny;  // both directions: rows y (DIR 0) or k over ny (DIR 1)
-  auto tepi = [&](int ml, int nl, double val) {
-    const int m = m0 + ml, n = n0 + nl;
-    if (m < Mrows && n < nx) epi(v, sl, st, m, n, val, r);
-  };
-  umma::tile_planes(ah, al, bh, bl, nkc, tepi, usmem, &v.g->umma_err);
-  if (Epi::kMax) {
-    double m = r.mx;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double mm = red[0];
-      for (int w = 1; w < umma::THREADS / 32; ++w) mm = fmax(mm, red[w]);
-      part_tile[b] = mm;
-    }
-  }
-}
-
-struct TE_ToYB {  // x-pass result (y, k) -> y-pass B plane element (row k, k-index y)
-  static constexpr int kMax = 0;
-  __device__ __forceinline__ void operator()(const BView& v, const BSlot& sl, const BState&, int y, int k,
-                                             double val, Red&) const {
-    const int nkc = (sl.ny + umma::KC - 1) / umma::KC;
-    umma::plane_put(v.yb_hi + sl.yb / 2, v.yb_lo + sl.yb / 2, k, y, nkc, val);
-  }
-};
-struct TE_Store {  // y-pass result -> FP64 face array (times dct_scale if scaled)
-  static constexpr int kMax = 0;
-  double* out;
+struct F2Args {
+  double* out;        // F2_STORE target, F2_TOPFLUX q_evap, F2_COMMIT T_surf
+  double* out2;       // F2_COMMIT q_evap_old
+  const double* in2;  // F2_TOPFLUX q_las, F2_COMMIT q_evap
   int scaled;
-  __device__ __forceinline__ void operator()(const BView&, const BSlot& sl, const BState&, int k, int x,
-                                             double val, Red&) const {
-    out[sl.face + (long long)k * sl.nx + x] = scaled ? val * sl.dct_scale : val;
-  }
 };
-struct TE_TopFlux {  // T_s -> evaporation -> q_net into the x-pass A plane (solvers/spectral.py:388-404)
-  static constexpr int kMax = 0;
-  const double* q_las;
-  double* q_ev;
-  double* q_net;
-  __device__ __forceinline__ void operator()(const BView& v, const BSlot& sl, const BState&, int y, int x,
-                                             double val, Red&) const {
-    const long long i = sl.face + (long long)y * sl.nx + x;
-    const double Ts = sl.recon_scale * val;
-    const double qe = evaporation(sl, Ts);
-    q_ev[i] = qe;
-    const double qn = q_las[i] - qe;
-    q_net[i] = qn;
-    xa_put(v, sl, y, x, qn);
+
+template <bool INV, bool SKIP_DONE, int KIND>
+__global__ void __launch_bounds__(f2::THREADS, 1)
+kb_face2d(BView v, F2Args args, double* part_tile, int n_stages, int bop_max) {
+  using namespace umma;
+  constexpr int CB = f2::CB;
+  extern __shared__ __align__(128) char sm[];
+  __shared__ double red[f2::THREADS / 32];
+  const int b = blockIdx.x;
+  const int s = find_slot(v.utile_start, v.n, b);
+  const BSlot& sl = v.slot[s];
+  const BState& st = v.st[s];
+  if (!st.active || (SKIP_DONE && st.done)) return;
+  FaceParams fp;
+  fp.face = sl.face; fp.xa = sl.xa; fp.nx = sl.nx; fp.ny = sl.ny;
+  fp.recon_scale = sl.recon_scale; fp.dct_scale = sl.dct_scale; fp.T_liquidus = sl.T_liquidus;
+  fp.T_boil = sl.T_boil; fp.evap_f1 = sl.evap_f1; fp.evap_f2 = sl.evap_f2;
+  const int nx = fp.nx, ny = fp.ny;
+  const int ct = b - sl.utile0;
+  const int nkx = (nx + KC - 1) / KC, nky = (ny + KC - 1) / KC;
+  const int nrt = (ny + TM - 1) / TM;
+  const int S = n_stages;
+  const int n_x = nrt * nkx, total = n_x + nky;
+  char* bop = sm;                // y-pass B operand: nky chunks of {hi, lo}
+  char* ring = sm + bop_max;     // S stages; later the epilogue tile
+  uint64_t* full = reinterpret_cast<uint64_t*>(ring + S * f2::STAGE);
+  uint64_t* done = full + f2::MAX_STAGES;
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(done + f2::MAX_STAGES);
+  volatile int* okflag = reinterpret_cast<volatile int*>(tslot + 1);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const uint32_t ncols = nrt > 1 ? 256u : 128u;
+  const char* p_hi = reinterpret_cast<const char*>(INV ? v.xa_hi : v.xq_hi) + fp.xa;
+  const char* p_lo = reinterpret_cast<const char*>(INV ? v.xa_lo : v.xq_lo) + fp.xa;
+  const long long mxo = (INV ? sl.mpx_inv : sl.mpx) + (long long)ct * nkx * CB;
+  const long long myo = INV ? sl.mpy_inv : sl.mpy;
+  const uint32_t idesc = idesc_bf16_f32(TM, 128);
+
+  if (warp == 0) tmem_alloc(tslot, ncols);
+  if (tid == 0) {
+    for (int i = 0; i < S; ++i) {
+      mbar_init(&full[i], 1);
+      mbar_init(&done[i], 1);
+    }
+    *okflag = 1;
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
-};
-struct TE_CommitSurface {  // T_temp, its max, q_evap_old <- q_evap
-  static constexpr int kMax = 1;
-  double* T_surf;
-  const double* q_ev;
-  double* q_evold;
-  __device__ __forceinline__ void operator()(const BView&, const BSlot& sl, const BState&, int y, int x,
-                                             double val, Red& r) const {
-    const long long i = sl.face + (long long)y * sl.nx + x;
-    const double T = sl.recon_scale * val;
-    T_surf[i] = T;
-    q_evold[i] = q_ev[i];
-    r.mx = fmax(r.mx, T);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tslot;
+
+  // Thread 0's ring: chunk g lives in stage g % S; each barrier completes one
+  // phase per use of its stage, so chunk g waits for parity (g / S) & 1.
+  int issued = 0, committed = 0;
+  auto load = [&](int g) {
+    char* stg = ring + (g % S) * f2::STAGE;
+    uint64_t* bar = &full[g % S];
+    if (g < n_x) {
+      const int rt = g / nkx, kc = g - rt * nkx;
+      const size_t po = (size_t)(rt * nkx + kc) * CB;
+      mbar_expect_tx(bar, 4 * CB);
+      bulk_g2s(stg, p_hi + po, CB, bar);
+      bulk_g2s(stg + CB, p_lo + po, CB, bar);
+      bulk_g2s(stg + 2 * CB, v.mp_hi + mxo + (size_t)kc * CB, CB, bar);
+      bulk_g2s(stg + 3 * CB, v.mp_lo + mxo + (size_t)kc * CB, CB, bar);
+    } else {
+      const int kc = g - n_x;
+      mbar_expect_tx(bar, 2 * nrt * CB);
+      for (int rt = 0; rt < nrt; ++rt) {
+        const size_t mo = (size_t)myo + (size_t)(rt * nky + kc) * CB;
+        bulk_g2s(stg + 2 * rt * CB, v.mp_hi + mo, CB, bar);
+        bulk_g2s(stg + (2 * rt + 1) * CB, v.mp_lo + mo, CB, bar);
+      }
+    }
+  };
+  auto wait_full = [&](int g) { return mbar_wait_bounded(&full[g % S], (uint32_t)((g / S) & 1)); };
+  auto wait_done = [&](int g) { return mbar_wait_bounded(&done[g % S], (uint32_t)((g / S) & 1)); };
+  auto step = [&](int g) -> bool {
+    if (!wait_full(g)) return false;
+    tc_fence_after();
+    const uint32_t s0 = smem_u32(ring + (g % S) * f2::STAGE);
+    if (g < n_x) {
+      const int kc = g % nkx;
+#pragma unroll
+      for (int k = 0; k < KC / 16; ++k) {
+        const uint32_t o = (uint32_t)(2 * k * (TM / 8) * 128);
+        const uint64_t dah = smem_desc(s0 + o, (TM / 8) * 128, 128);
+        const uint64_t dal = smem_desc(s0 + CB + o, (TM / 8) * 128, 128);
+        const uint64_t dbh = smem_desc(s0 + 2 * CB + o, (TM / 8) * 128, 128);
+        const uint64_t dbl = smem_desc(s0 + 3 * CB + o, (TM / 8) * 128, 128);
+        mma_bf16(tmem, dah, dbh, idesc, (kc > 0 || k > 0) ? 1u : 0u);
+        mma_bf16(tmem, dah, dbl, idesc, 1u);
+        mma_bf16(tmem, dal, dbh, idesc, 1u);
+      }
+    } else {
+      const int kc = g - n_x;
+      const uint32_t b0 = smem_u32(bop + kc * 2 * CB);
+      for (int rt = 0; rt < nrt; ++rt) {
+#pragma unroll
+        for (int k = 0; k < KC / 16; ++k) {
+          const uint32_t o = (uint32_t)(2 * k * (TM / 8) * 128);
+          const uint64_t dah = smem_desc(s0 + 2 * rt * CB + o, (TM / 8) * 128, 128);
+          const uint64_t dal = smem_desc(s0 + (2 * rt + 1) * CB + o, (TM / 8) * 128, 128);
+          const uint64_t dbh = smem_desc(b0 + o, (TM / 8) * 128, 128);
+          const uint64_t dbl = smem_desc(b0 + CB + o, (TM / 8) * 128, 128);
+          const uint32_t d = tmem + (uint32_t)(rt * 128);
+          mma_bf16(d, dah, dbh, idesc, (kc > 0 || k > 0) ? 1u : 0u);
+          mma_bf16(d, dah, dbl, idesc, 1u);
+          mma_bf16(d, dal, dbh, idesc, 1u);
+        }
+      }
+    }
+    mma_commit(&done[g % S]);
+    committed = g + 1;
+    const int nxt = g - 1 + S;  // the stage of chunk g - 1 takes chunk g - 1 + S
+    if (g >= 1 && nxt < total && nxt >= issued) {
+      if (!wait_done(g - 1)) return false;
+      load(nxt);
+      issued = nxt + 1;
+    }
+    return true;
+  };
+  auto fail = [&]() {  // thread 0: record, then wait (bounded) for in-flight copies and MMAs
+    atomicExch(&v.g->umma_err, 1);
+    *okflag = 0;
+    for (int g = issued - S < 0 ? 0 : issued - S; g < issued; ++g) wait_full(g);
+    for (int g = committed - S < 0 ? 0 : committed - S; g < committed; ++g) wait_done(g);
+  };
+
+  if (tid == 0) {
+    const int pre = total < S ? total : S;
+    for (int g = 0; g < pre; ++g) load(g);
+    issued = pre;
   }
-};
+  const int q = warp & 3, half = warp >> 2;
+  for (int rt = 0; rt < nrt; ++rt) {
+    if (tid == 0 && *okflag) {
+      bool ok = true;
+      for (int kc = 0; kc < nkx && ok; ++kc) ok = step(rt * nkx + kc);
+      if (ok) ok = wait_done(rt * nkx + nkx - 1);
+      if (!ok) fail();
+    }
+    __syncthreads();
+    if (*okflag) {
+      // X1 row y = TMEM lane -> B operand element (row c, k = y); rows y and
+      // y + 1 (lanes l, l + 1) go out as one 32-bit store per part
+      tc_fence_after();
+      const int y = rt * TM + q * 32 + lane;
+      const bool keep = y < nky * KC;
+#pragma unroll 1
+      for (int c = half * 64; c < half * 64 + 64; c += 16) {
+        float x16[16];
+        tmem_ld16(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)c, x16);
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+          __nv_bfloat16 h, l;
+          split_bf16((double)x16[i], h, l);
+          const uint32_t hv = __bfloat16_as_ushort(h), lv = __bfloat16_as_ushort(l);
+          const uint32_t hn = __shfl_down_sync(0xffffffffu, hv, 1);
+          const uint32_t ln = __shfl_down_sync(0xffffffffu, lv, 1);
+          if ((lane & 1) == 0 && keep) {
+            const uint32_t o = (uint32_t)((y >> 5) * 2 * CB) + core_off(c + i, y & 31, TM);
+            *reinterpret_cast<uint32_t*>(bop + o) = hv | (hn << 16);
+            *reinterpret_cast<uint32_t*>(bop + CB + o) = lv | (ln << 16);
+          }
+        }
+      }
+      fence_proxy_async();
+    }
+    tc_fence_before();
+    __syncthreads();
+  }
+  if (tid == 0 && *okflag) {
+    tc_fence_after();
+    bool ok = true;
+    for (int kc = 0; kc < nky && ok; ++kc) ok = step(n_x + kc);
+    if (ok) ok = wait_done(total - 1);
+    if (!ok) fail();
+  }
+  __syncthreads();
+
+  constexpr int ITEMS = TM * 128 / f2::THREADS;  // tile elements per thread
+  double mx = -INFINITY;
+  const int c0 = ct * 128;
+  for (int rt = 0; rt < nrt; ++rt) {
+    const bool good = *okflag != 0;
+    if (good) {
+      tc_fence_after();
+      const int m = q * 32 + lane;
+      float* tile = reinterpret_cast<float*>(ring);
+#pragma unroll 1
+      for (int c = half * 64; c < half * 64 + 64; c += 16) {
+        float x16[16];
+        tmem_ld16(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(rt * 128 + c), x16);
+#pragma unroll
+        for (int i = 0; i < 16; ++i) tile[m * 128 + ((c + i) ^ (m & 31))] = x16[i];
+      }
+    }
+    __syncthreads();
+    if (good) {
+      const int r0 = rt * TM;
+      if (KIND == F2_TOPFLUX) {
+        // a warp covers 32 consecutive x of one row (coalesced FP64 traffic);
+        // the loads of U elements are issued ahead of their stores
+        constexpr int U = 8;
+        for (int it0 = 0; it0 < ITEMS; it0 += U) {
+          double ql[U];
+#pragma unroll
+          for (int u = 0; u < U; ++u) {
+            const int e = tid + (it0 + u) * f2::THREADS;
+            const int y = r0 + e / 128, x = c0 + e % 128;
+            ql[u] = (y < ny && x < nx) ? __ldg(args.in2 + fp.face + (long long)y * nx + x) : 0.0;
+          }
+#pragma unroll
+          for (int u = 0; u < U; ++u) {
+            const int e = tid + (it0 + u) * f2::THREADS;
+            const int m = e / 128, n = e % 128;
+            const int y = r0 + m, x = c0 + n;
+            const bool in = y < ny && x < nx;
+            double qn = 0.0;
+            if (in) {
+              const double qe = evaporation(fp, fp.recon_scale * (double)tile_value(ring, m, n));
+              args.out[fp.face + (long long)y * nx + x] = qe;
+              qn = ql[u] - qe;
+            }
+            plane_put8_warp(v.xq_hi + fp.xa / 2, v.xq_lo + fp.xa / 2, y, x, nkx, qn, in);
+          }
+        }
+      } else {
+        constexpr int U = 4;
+        for (int it0 = 0; it0 < ITEMS; it0 += U) {
+          long long idx[U];
+          double src[U];
+#pragma unroll
+          for (int u = 0; u < U; ++u) {
+            const int e = tid + (it0 + u) * f2::THREADS;
+            const int y = r0 + e / 128, x = c0 + e % 128;
+            idx[u] = (y < ny && x < nx) ? fp.face + (long long)y * nx + x : -1;
+            src[u] = (KIND == F2_COMMIT && idx[u] >= 0) ? __ldg(args.in2 + idx[u]) : 0.0;
+          }
+#pragma unroll
+          for (int u = 0; u < U; ++u) {
+            if (idx[u] < 0) continue;
+            const int e = tid + (it0 + u) * f2::THREADS;
+            const double val = (double)tile_value(ring, e / 128, e % 128);
+            if (KIND == F2_STORE) {
+              args.out[idx[u]] = args.scaled ? val * fp.dct_scale : val;
+            } else {  // F2_COMMIT
+              const double T = fp.recon_scale * val;
+              args.out[idx[u]] = T;
+              args.out2[idx[u]] = src[u];
+              mx = fmax(mx, T);
+            }
+          }
+        }
+      }
+    }
+    __syncthreads();
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tmem_dealloc(tmem, ncols);
+  if (KIND == F2_COMMIT) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_down_sync(0xffffffffu, mx, o));
+    if (lane == 0) red[warp] = mx;
+    __syncthreads();
+    if (tid == 0) {
+      double mm = red[0];
+      for (int w = 1; w < f2::THREADS / 32; ++w) mm = fmax(mm, red[w]);
+      part_tile[b] = mm;
+    }
+  }
+}
 
 struct EB_Store {  // out = v * (scaled ? dct_scale : 1)
   static constexpr int kMax = 0;
@@ -597,73 +775,90 @@ struct EB_CommitSurface {  // T_temp, its max, q_evap_old <- q_evap (solvers/spe
 };
 
 // Face-state update of one Picard iteration (see k_fs_relax in sgh_b200.cu):
-// residual and iterate norms from the constant weights, relaxation of sigma.
+// residual and iterate norms from the constant weights, relaxation of sigma
+// and the next top-surface input A = Zt + W_tt sigma (FP64 array when A is
+// given, xa operand plane in mixed precision). Then the per-slot convergence
+// test (solvers/spectral.py:464-499) without a second launch: every block of
+// a slot takes a ticket after publishing its partials, and the block that
+// draws the slot's last ticket sums that slot's partials in a fixed order
+// (so a slot's result does not depend on the rest of the batch) and updates
+// its state; the last block of the launch sets the Picard loop condition.
+// No block waits on another.
 __global__ void __launch_bounds__(BT)
 kb_relax(BView v, const double* Zt, const double* Yt, const double* Wtt, const double* Qtt,
-         const double* S_top, double* sigma, double* A, double* part) {
+         const double* S_top, double* sigma, double* A, double* part, const double* part_n1,
+         cudaGraphConditionalHandle h_picard, int in_graph) {
   __shared__ double sh[2 * (BT / 32)];
+  __shared__ unsigned ticket;
   const int b = blockIdx.x;
   const int s = find_slot(v.blk_start, v.n, b);
   const BSlot& sl = v.slot[s];
-  const BState& st = v.st[s];
-  if (!st.active || st.done) return;
-  const int i = (b - sl.blk0) * BT + threadIdx.x;
-  double r2 = 0.0, o2 = 0.0;
-  if (i < sl.S) {
-    const long long j = sl.face + i;
-    const double sg = sigma[j], q = Qtt[j];
-    const double d = S_top[j] - sg;
-    r2 = d * d * q;
-    o2 = 2.0 * sg * Yt[j] + sg * sg * q;
-    const double ns = d * sl.omega + sg;
-    sigma[j] = ns;
-    const double a = Zt[j] + Wtt[j] * ns;
-    A[j] = a;
-    xa_put(v, sl, i / sl.nx, i % sl.nx, a);
-  }
-  block_sum2<BT>(r2, o2, sh);
-  if (threadIdx.x == 0) {
-    part[2 * b] = r2;
-    part[2 * b + 1] = o2;
-  }
-}
-
-// Per-slot convergence test (solvers/spectral.py:464-499); the loop goes on
-// while any slot is still iterating.
-__global__ void __launch_bounds__(CT)
-kb_converge(BView v, const double* part, const double* part_n1, cudaGraphConditionalHandle h_picard,
-            int in_graph) {
-  __shared__ int any;
-  if (threadIdx.x == 0) any = 0;
-  __syncthreads();
-  for (int s = threadIdx.x; s < v.n; s += CT) {
-    BState& st = v.st[s];
-    if (!st.active || st.done) continue;
-    const BSlot& sl = v.slot[s];
-    double r2 = 0.0, o2 = 0.0;
-    for (int b = sl.blk0; b < sl.blk0 + sl.nblk; ++b) {
-      r2 += part[2 * b];
-      o2 += part[2 * b + 1] + part_n1[b];
+  BState& st = v.st[s];
+  if (st.active && !st.done) {
+    const int i = (b - sl.blk0) * BT + threadIdx.x;
+    const bool valid = i < sl.S;
+    double r2 = 0.0, o2 = 0.0, a = 0.0;
+    if (valid) {
+      const long long j = sl.face + i;
+      const double sg = sigma[j], q = Qtt[j], yt = Yt[j], stop = S_top[j], zt = Zt[j], wt = Wtt[j];
+      const double d = stop - sg;
+      r2 = d * d * q;
+      o2 = 2.0 * sg * yt + sg * sg * q;
+      const double ns = d * sl.omega + sg;
+      sigma[j] = ns;
+      a = zt + wt * ns;
+      if (A) A[j] = a;
     }
-    const double n = sl.n_elements;
-    const double rel = sqrt(r2 / n) / fmax(sqrt(o2 / n), 1e-9);
-    const int it = st.iter + 1;
-    st.iter = it;
-    st.rel_err = rel;
-    if (rel < sl.tol) {
-      st.status = SGH_STEP_CONVERGED;
-      st.done = 1;
-    } else if (!isfinite(rel)) {
-      st.status = SGH_STEP_NONFINITE;
-      st.done = 1;
-    } else if (it >= sl.max_iter) {
-      st.status = SGH_STEP_CAPPED;
-      st.done = 1;
+    plane_put_block(v.xa_hi, v.xa_lo, sl, i, a, valid);
+    block_sum2<BT>(r2, o2, sh);
+    if (threadIdx.x == 0) {
+      part[2 * b] = r2;
+      part[2 * b + 1] = o2;
+      __threadfence();
+      ticket = atomicAdd(&st.tickets, 1u);
     }
-    if (!st.done) any = 1;
+    __syncthreads();
+    if (ticket == (unsigned)sl.nblk - 1u) {
+      __threadfence();
+      double rs = 0.0, os = 0.0;
+      for (int k = threadIdx.x; k < sl.nblk; k += BT) {
+        const int bb = sl.blk0 + k;
+        rs += __ldcg(part + 2 * bb);
+        os += __ldcg(part + 2 * bb + 1) + __ldcg(part_n1 + bb);
+      }
+      block_sum2<BT>(rs, os, sh);
+      if (threadIdx.x == 0) {
+        const double n = sl.n_elements;
+        const double rel = sqrt(rs / n) / fmax(sqrt(os / n), 1e-9);
+        const int it = st.iter + 1;
+        st.iter = it;
+        st.rel_err = rel;
+        if (rel < sl.tol) {
+          st.status = SGH_STEP_CONVERGED;
+          st.done = 1;
+        } else if (!isfinite(rel)) {
+          st.status = SGH_STEP_NONFINITE;
+          st.done = 1;
+        } else if (it >= sl.max_iter) {
+          st.status = SGH_STEP_CAPPED;
+          st.done = 1;
+        }
+        st.tickets = 0u;
+      }
+    }
   }
+  __threadfence();
   __syncthreads();
+  if (threadIdx.x == 0) ticket = atomicAdd(&v.g->blocks_done, 1u);
+  __syncthreads();
+  if (ticket != gridDim.x - 1) return;
+  __threadfence();
+  int any = 0;
+  for (int k = threadIdx.x; k < v.n; k += BT)
+    if (__ldcg(&v.st[k].active) && !__ldcg(&v.st[k].done)) any = 1;
+  any = __syncthreads_or(any);
   if (threadIdx.x == 0) {
+    v.g->blocks_done = 0u;
     v.g->picard_any = any;
     if (in_graph) cudaGraphSetConditional(h_picard, any ? 1u : 0u);
   }
@@ -687,22 +882,29 @@ kb_commit_modes(BView v, R* a, const R* K, const R* KK, const double* sigma) {
   }
 }
 
-// Metrics of every active slot (solvers/spectral.py:536-542); advances the
-// step counters and decides whether the step loop continues.
+// Metrics of every active slot (solvers/spectral.py:536-542), one warp per
+// slot; advances the step counters and decides whether the step loop goes on.
 __global__ void __launch_bounds__(CT)
 kb_commit(BView v, const double* part_las, const double* part_tile, int umma_tiles,
           cudaGraphConditionalHandle h_steps, int in_graph) {
   __shared__ int any;
   if (threadIdx.x == 0) any = 0;
   __syncthreads();
-  for (int s = threadIdx.x; s < v.n; s += CT) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int s = warp; s < v.n; s += CT / 32) {
     BState& st = v.st[s];
     if (!st.active) continue;
     const BSlot& sl = v.slot[s];
     double p = 0.0, m = -INFINITY;
-    for (int b = sl.blk0; b < sl.blk0 + sl.nblk; ++b) p += part_las[b];
+    for (int b = sl.blk0 + lane; b < sl.blk0 + sl.nblk; b += 32) p += part_las[b];
     const int t0 = umma_tiles ? sl.utile0 : sl.tile0, nt = umma_tiles ? sl.nutile : sl.ntile;
-    for (int b = t0; b < t0 + nt; ++b) m = fmax(m, part_tile[b]);
+    for (int b = t0 + lane; b < t0 + nt; b += 32) m = fmax(m, part_tile[b]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      p += __shfl_down_sync(0xffffffffu, p, o);
+      m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
+    }
+    if (lane != 0) continue;
     sgh_step_out o;
     o.T_surface_max = m;
     o.P_laser = p * sl.dx * sl.dy;
@@ -716,7 +918,7 @@ kb_commit(BView v, const double* part_las, const double* part_tile, int umma_til
     st.iters += st.iter;
     st.step += 1;
     if (st.step >= st.n_steps) st.active = 0;
-    if (st.active) any = 1;
+    if (st.active) atomicOr(&any, 1);
   }
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -747,8 +949,9 @@ struct sgh_batch {
   size_t o_a, o_K, o_KK;
   size_t o_qlas, o_qnet, o_qev, o_qevold, o_Stop, o_f1, o_sigma, o_A, o_Tsurf, o_Zt, o_Yt, o_Wtt, o_Qtt;
   size_t o_plas, o_pn1, o_prelax, o_ptile;
-  size_t o_xah = 0, o_xal = 0, o_ybh = 0, o_ybl = 0, o_mph = 0, o_mpl = 0;  // operand planes (mixed)
-  size_t xa_bytes = 0, yb_bytes = 0, mp_bytes = 0;
+  size_t o_xah = 0, o_xal = 0, o_xqh = 0, o_xql = 0, o_mph = 0, o_mpl = 0;  // operand planes (mixed)
+  size_t xa_bytes = 0, mp_bytes = 0;
+  int f2_stages = 0, f2_bop = 0, f2_smem = 0;  // fused face transform: ring stages, operand bytes, smem
   std::vector<std::pair<int, long long>> mplane_list;  // (N, byte offset of the forward plane)
   size_t ws_need = 0;
   char* ws = nullptr;
@@ -772,8 +975,8 @@ struct sgh_batch {
     const bool mixed = precision == SGH_PRECISION_MIXED;
     v.xa_hi = mixed ? reinterpret_cast<__nv_bfloat16*>(ws + o_xah) : nullptr;
     v.xa_lo = mixed ? reinterpret_cast<__nv_bfloat16*>(ws + o_xal) : nullptr;
-    v.yb_hi = mixed ? reinterpret_cast<__nv_bfloat16*>(ws + o_ybh) : nullptr;
-    v.yb_lo = mixed ? reinterpret_cast<__nv_bfloat16*>(ws + o_ybl) : nullptr;
+    v.xq_hi = mixed ? reinterpret_cast<__nv_bfloat16*>(ws + o_xqh) : nullptr;
+    v.xq_lo = mixed ? reinterpret_cast<__nv_bfloat16*>(ws + o_xql) : nullptr;
     v.mp_hi = mixed ? ws + o_mph : nullptr;
     v.mp_lo = mixed ? ws + o_mpl : nullptr;
     v.mats = d(o_mats);
@@ -797,20 +1000,24 @@ inline int cdivl(long long a, long long b) { return (int)((a + b - 1) / b); }
 
 thread_local int g_blaunch = 0;
 
-// One face pass over all slots: the FP64 register-tiled contraction on the
-// FP64 input (plain), or tensor-core split-BF16 tiles fed by bulk copies
-// from the operand planes (mixed).
-template <int DIR, bool INV, bool SKIP, class EpiF, class EpiT>
-void face_pass(sgh_batch* B, cudaStream_t s, const double* in, const EpiF& ef, const EpiT& et, double* part) {
+// One 2-D transform of the top faces of all slots: the FP64 register-tiled
+// contraction as an x-pass (in -> f1) and a y-pass (f1 -> epilogue ef), or,
+// in mixed precision, one fused tensor-core launch with epilogue KIND
+// reading the xa (inverse) or xq (forward) operand plane.
+template <bool INV, bool SKIP, int KIND, class EpiF>
+void face2d(sgh_batch* B, cudaStream_t s, const double* in, const EpiF& ef, const F2Args& fa, double* part) {
   const BView v = B->view();
   if (B->precision == SGH_PRECISION_MIXED) {
-    const int smem = umma::planes_smem_bytes();
-    (void)cudaFuncSetAttribute(kb_face_tc<DIR, INV, SKIP, EpiT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    kb_face_tc<DIR, INV, SKIP, EpiT><<<B->tot_utile, umma::THREADS, smem, s>>>(v, et, part);
+    (void)cudaFuncSetAttribute(kb_face2d<INV, SKIP, KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               B->f2_smem);
+    kb_face2d<INV, SKIP, KIND><<<B->tot_utile, f2::THREADS, B->f2_smem, s>>>(v, fa, part, B->f2_stages, B->f2_bop);
+    ++g_blaunch;
   } else {
-    kb_face_axis<DIR, INV, SKIP, EpiF><<<B->tot_tile, AX_THREADS, 0, s>>>(v, in, ef, part);
+    kb_face_axis<0, INV, SKIP, EB_Store><<<B->tot_tile, AX_THREADS, 0, s>>>(v, in, EB_Store{B->d(B->o_f1), 0},
+                                                                            nullptr);
+    kb_face_axis<1, INV, SKIP, EpiF><<<B->tot_tile, AX_THREADS, 0, s>>>(v, B->d(B->o_f1), ef, part);
+    g_blaunch += 2;
   }
-  ++g_blaunch;
 }
 
 template <class R>
@@ -824,25 +1031,25 @@ void enqueue_pre(sgh_batch* B, cudaStream_t s, cudaGraphConditionalHandle h, int
   kb_pass1<R><<<B->tot_blk, BT, 0, s>>>(v, a, K, KK, B->d(B->o_Zt), B->d(B->o_Yt), B->d(B->o_pn1));
   g_blaunch += 3;
   // initial guess: sigma = dct_scale * DCT2(q_las - shift(q_evap_old))
-  face_pass<0, false, false>(B, s, B->d(B->o_qnet), EB_Store{B->d(B->o_f1), 0}, TE_ToYB{}, nullptr);
-  face_pass<1, false, false>(B, s, B->d(B->o_f1), EB_Store{B->d(B->o_sigma), 1}, TE_Store{B->d(B->o_sigma), 1},
-                             nullptr);
+  face2d<false, false, F2_STORE>(B, s, B->d(B->o_qnet), EB_Store{B->d(B->o_sigma), 1},
+                                 F2Args{B->d(B->o_sigma), nullptr, nullptr, 1}, nullptr);
   kb_assemble<<<B->tot_blk, BT, 0, s>>>(v, B->d(B->o_Zt), B->d(B->o_Wtt), B->d(B->o_sigma), B->d(B->o_A));
   g_blaunch += 1;
 }
 
 void enqueue_picard(sgh_batch* B, cudaStream_t s, cudaGraphConditionalHandle h, int in_graph) {
   const BView v = B->view();
-  face_pass<0, true, true>(B, s, B->d(B->o_A), EB_Store{B->d(B->o_f1), 0}, TE_ToYB{}, nullptr);
-  face_pass<1, true, true>(B, s, B->d(B->o_f1), EB_TopFlux{B->d(B->o_qlas), B->d(B->o_qev), B->d(B->o_qnet)},
-                           TE_TopFlux{B->d(B->o_qlas), B->d(B->o_qev), B->d(B->o_qnet)}, nullptr);
-  face_pass<0, false, true>(B, s, B->d(B->o_qnet), EB_Store{B->d(B->o_f1), 0}, TE_ToYB{}, nullptr);
-  face_pass<1, false, true>(B, s, B->d(B->o_f1), EB_Store{B->d(B->o_Stop), 1}, TE_Store{B->d(B->o_Stop), 1},
-                            nullptr);
+  const bool mixed = B->precision == SGH_PRECISION_MIXED;
+  // T_s = IDCT2(A) -> evaporation -> q_net; S_top = dct_scale * DCT2(q_net)
+  face2d<true, true, F2_TOPFLUX>(B, s, B->d(B->o_A), EB_TopFlux{B->d(B->o_qlas), B->d(B->o_qev), B->d(B->o_qnet)},
+                                 F2Args{B->d(B->o_qev), nullptr, B->d(B->o_qlas), 0}, nullptr);
+  face2d<false, true, F2_STORE>(B, s, B->d(B->o_qnet), EB_Store{B->d(B->o_Stop), 1},
+                                F2Args{B->d(B->o_Stop), nullptr, nullptr, 1}, nullptr);
+  // mixed precision keeps A only as the xa operand plane
   kb_relax<<<B->tot_blk, BT, 0, s>>>(v, B->d(B->o_Zt), B->d(B->o_Yt), B->d(B->o_Wtt), B->d(B->o_Qtt),
-                                     B->d(B->o_Stop), B->d(B->o_sigma), B->d(B->o_A), B->d(B->o_prelax));
-  kb_converge<<<1, CT, 0, s>>>(v, B->d(B->o_prelax), B->d(B->o_pn1), h, in_graph);
-  g_blaunch += 2;
+                                     B->d(B->o_Stop), B->d(B->o_sigma), mixed ? nullptr : B->d(B->o_A),
+                                     B->d(B->o_prelax), B->d(B->o_pn1), h, in_graph);
+  g_blaunch += 1;
 }
 
 template <class R>
@@ -851,11 +1058,9 @@ void enqueue_post(sgh_batch* B, cudaStream_t s, cudaGraphConditionalHandle h, in
   R* a = reinterpret_cast<R*>(B->ws + B->o_a);
   R* K = reinterpret_cast<R*>(B->ws + B->o_K);
   R* KK = reinterpret_cast<R*>(B->ws + B->o_KK);
-  face_pass<0, true, false>(B, s, B->d(B->o_A), EB_Store{B->d(B->o_f1), 0}, TE_ToYB{}, nullptr);
-  face_pass<1, true, false>(B, s, B->d(B->o_f1),
-                            EB_CommitSurface{B->d(B->o_Tsurf), B->d(B->o_qev), B->d(B->o_qevold)},
-                            TE_CommitSurface{B->d(B->o_Tsurf), B->d(B->o_qev), B->d(B->o_qevold)},
-                            B->d(B->o_ptile));
+  face2d<true, false, F2_COMMIT>(B, s, B->d(B->o_A),
+                                 EB_CommitSurface{B->d(B->o_Tsurf), B->d(B->o_qev), B->d(B->o_qevold)},
+                                 F2Args{B->d(B->o_Tsurf), B->d(B->o_qevold), B->d(B->o_qev), 0}, B->d(B->o_ptile));
   kb_commit_modes<R><<<B->tot_blk, BT, 0, s>>>(v, a, K, KK, B->d(B->o_sigma));
   kb_commit<<<1, CT, 0, s>>>(v, B->d(B->o_plas), B->d(B->o_ptile),
                              B->precision == SGH_PRECISION_MIXED ? 1 : 0, h, in_graph);
@@ -954,6 +1159,8 @@ int sgh_batch_create(const sgh_config* cfgs, int32_t n, int32_t precision, sgh_b
       rc = bfail(SGH_ERR_UNSUPPORTED,
                  where + "batches step the face-space form only (no latent heat, no T-dependent model, "
                          "no convection); use a single-instance plan");
+    else if (precision == SGH_PRECISION_MIXED && c.ny > f2::MAX_NY)
+      rc = bfail(SGH_ERR_UNSUPPORTED, where + "mixed-precision batches need ny <= 256");
     if (rc) {
       delete B;
       return rc;
@@ -1006,9 +1213,7 @@ int sgh_batch_create(const sgh_config* cfgs, int32_t n, int32_t precision, sgh_b
     sl.nutile = face_utiles(c.nx, c.ny);
     if (precision == SGH_PRECISION_MIXED) {
       sl.xa = (long long)B->xa_bytes;
-      sl.yb = (long long)B->yb_bytes;
       B->xa_bytes += umma::plane_bytes(c.ny, c.nx);
-      B->yb_bytes += umma::plane_bytes(c.nx, c.ny);
       sl.mpx = mplane[c.nx];
       sl.mpx_inv = sl.mpx + (long long)umma::plane_bytes(c.nx, c.nx);
       sl.mpy = mplane[c.ny];
@@ -1082,10 +1287,17 @@ int sgh_batch_create(const sgh_config* cfgs, int32_t n, int32_t precision, sgh_b
   if (precision == SGH_PRECISION_MIXED) {
     B->o_xah = L.take(B->xa_bytes);
     B->o_xal = L.take(B->xa_bytes);
-    B->o_ybh = L.take(B->yb_bytes);
-    B->o_ybl = L.take(B->yb_bytes);
+    B->o_xqh = L.take(B->xa_bytes);
+    B->o_xql = L.take(B->xa_bytes);
     B->o_mph = L.take(B->mp_bytes);
     B->o_mpl = L.take(B->mp_bytes);
+  }
+  if (precision == SGH_PRECISION_MIXED) {
+    int max_ny = 0;
+    for (int i = 0; i < n; ++i) max_ny = std::max(max_ny, cfgs[i].ny);
+    B->f2_bop = f2::bop_bytes(max_ny);
+    B->f2_stages = f2::stages(max_ny);
+    B->f2_smem = f2::smem_bytes(max_ny);
   }
   B->ws_need = L.off;
   *out = B;
@@ -1132,8 +1344,8 @@ int sgh_batch_bind(sgh_batch* B, void* workspace, uint64_t bytes, void* stream) 
   if (B->precision == SGH_PRECISION_MIXED) {
     SGB_CK(cudaMemsetAsync(B->ws + B->o_xah, 0, B->xa_bytes, s));
     SGB_CK(cudaMemsetAsync(B->ws + B->o_xal, 0, B->xa_bytes, s));
-    SGB_CK(cudaMemsetAsync(B->ws + B->o_ybh, 0, B->yb_bytes, s));
-    SGB_CK(cudaMemsetAsync(B->ws + B->o_ybl, 0, B->yb_bytes, s));
+    SGB_CK(cudaMemsetAsync(B->ws + B->o_xqh, 0, B->xa_bytes, s));
+    SGB_CK(cudaMemsetAsync(B->ws + B->o_xql, 0, B->xa_bytes, s));
     SGB_CK(cudaMemsetAsync(B->ws + B->o_mph, 0, B->mp_bytes, s));
     SGB_CK(cudaMemsetAsync(B->ws + B->o_mpl, 0, B->mp_bytes, s));
     for (size_t j = 0; j < B->mplane_list.size(); ++j) {

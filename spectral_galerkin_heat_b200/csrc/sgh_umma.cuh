@@ -293,32 +293,66 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
       : "memory");
 }
 
-// Dynamic shared memory of tile_planes (bytes): 2 stages x 4 chunks + barriers.
-__host__ __device__ constexpr int planes_smem_bytes() { return 2 * 4 * CHUNK_BYTES + 128; }
+// 8 consecutive k (k0 % 8 == 0) of row r: one 16-byte row of a core matrix
+// in each plane, written with one vector store per part.
+__device__ __forceinline__ void plane_put8(__nv_bfloat16* hi, __nv_bfloat16* lo, int r, int k0, int nkc,
+                                           const double (&x)[8]) {
+  uint32_t h[4], l[4];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    __nv_bfloat16 h0, l0, h1, l1;
+    split_bf16(x[2 * j], h0, l0);
+    split_bf16(x[2 * j + 1], h1, l1);
+    h[j] = (uint32_t)__bfloat16_as_ushort(h0) | ((uint32_t)__bfloat16_as_ushort(h1) << 16);
+    l[j] = (uint32_t)__bfloat16_as_ushort(l0) | ((uint32_t)__bfloat16_as_ushort(l1) << 16);
+  }
+  const size_t o = plane_off(r, k0, nkc);
+  *reinterpret_cast<uint4*>(reinterpret_cast<char*>(hi) + o) = make_uint4(h[0], h[1], h[2], h[3]);
+  *reinterpret_cast<uint4*>(reinterpret_cast<char*>(lo) + o) = make_uint4(l[0], l[1], l[2], l[3]);
+}
+
+// ---- plane tiles: a ring of bulk-copy stages feeding the tensor cores -----
+constexpr int PLANE_STAGES = 6;                 // k-chunks in flight
+constexpr int PLANE_THREADS = 256;              // 2 warpgroups
+constexpr int STAGE_BYTES = 4 * CHUNK_BYTES;    // A hi, A lo, B hi, B lo
+// Dynamic shared memory of tile_planes (bytes): the stage ring, then barriers.
+__host__ __device__ constexpr int planes_smem_bytes() { return PLANE_STAGES * STAGE_BYTES + 256; }
+
+// FP32 result tile left in shared memory by tile_planes (it reuses the first
+// 64 KB of the stage ring once every MMA has completed). Element (m, n) sits
+// at float m * 128 + (n ^ (m & 31)): the XOR spreads a column over all 32
+// banks for the TMEM -> shared copy and keeps rows conflict-free.
+__device__ __forceinline__ float tile_value(const char* smem, int m, int n) {
+  return reinterpret_cast<const float*>(smem)[m * 128 + (n ^ (m & 31))];
+}
 
 // One 128 x 128 tile D[m][n] = sum_k A(m, k) B(n, k) from operand planes.
 // a_hi/a_lo point at chunk (rt, 0) of A's planes, b_hi/b_lo at chunk (ct, 0)
-// of B's; nkc chunks along k. Thread 0 drives the bulk copies and the MMAs
-// (copies of chunk c+1 overlap the MMAs of chunk c); all 128 threads run the
-// epilogue epi(m_local, n_local, value) for every element of the tile (the
-// caller bounds-checks). Bounded waits as in tile_bf16x3.
-template <class EPI>
-__device__ void tile_planes(const char* a_hi, const char* a_lo, const char* b_hi, const char* b_lo, int nkc,
-                            const EPI& epi, char* smem, int* err) {
+// of B's; nkc chunks along k. Thread 0 drives the ring: it issues the bulk
+// copies of the first PLANE_STAGES chunks at once, then per chunk waits for
+// its data, issues the three split-BF16 MMAs per 16-wide k-step, commits them,
+// and refills the stage of the previous chunk as soon as that chunk's MMAs
+// have drained. All waits are bounded: on expiry *err is set, in-flight work
+// is waited for (bounded), tensor memory is freed and false is returned.
+// On success the tile is in shared memory (tile_value) when this returns.
+// Call from all PLANE_THREADS threads.
+static __device__ bool tile_planes(const char* a_hi, const char* a_lo, const char* b_hi, const char* b_lo,
+                                   int nkc, char* smem, int* err) {
   constexpr uint32_t NT = 128, NCOLS = 128;
-  uint64_t* full = reinterpret_cast<uint64_t*>(smem + 8 * CHUNK_BYTES);
-  uint64_t* done = full + 2;
-  uint32_t* tslot = reinterpret_cast<uint32_t*>(full + 4);
-  volatile int* okflag = reinterpret_cast<volatile int*>(full + 5);
+  constexpr int S = PLANE_STAGES;
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + S * STAGE_BYTES);
+  uint64_t* done = full + S;
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(done + S);
+  volatile int* okflag = reinterpret_cast<volatile int*>(tslot + 1);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const uint32_t idesc = idesc_bf16_f32(TM, NT);
 
   if (warp == 0) tmem_alloc(tslot, NCOLS);
   if (tid == 0) {
-    mbar_init(&full[0], 1);
-    mbar_init(&full[1], 1);
-    mbar_init(&done[0], 1);
-    mbar_init(&done[1], 1);
+    for (int b = 0; b < S; ++b) {
+      mbar_init(&full[b], 1);
+      mbar_init(&done[b], 1);
+    }
     *okflag = 1;
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
@@ -328,25 +362,26 @@ __device__ void tile_planes(const char* a_hi, const char* a_lo, const char* b_hi
   const uint32_t tmem = *tslot;
 
   if (tid == 0) {
-    uint32_t fph[2] = {0u, 0u}, dph[2] = {0u, 0u};
+    uint32_t fph = 0u, dph = 0u;  // parity bit per stage
     bool ok = true;
     auto load = [&](int ch) {
-      const int b = ch & 1;
-      char* st = smem + b * 4 * CHUNK_BYTES;
+      const int b = ch % S;
+      char* st = smem + b * STAGE_BYTES;
       const size_t off = (size_t)ch * CHUNK_BYTES;
-      mbar_expect_tx(&full[b], 4 * CHUNK_BYTES);
+      mbar_expect_tx(&full[b], STAGE_BYTES);
       bulk_g2s(st, a_hi + off, CHUNK_BYTES, &full[b]);
       bulk_g2s(st + CHUNK_BYTES, a_lo + off, CHUNK_BYTES, &full[b]);
       bulk_g2s(st + 2 * CHUNK_BYTES, b_hi + off, CHUNK_BYTES, &full[b]);
       bulk_g2s(st + 3 * CHUNK_BYTES, b_lo + off, CHUNK_BYTES, &full[b]);
     };
-    if (nkc > 0) load(0);
-    for (int ch = 0; ch < nkc && ok; ++ch) {
-      const int b = ch & 1;
-      if (!mbar_wait_bounded(&full[b], fph[b])) { ok = false; break; }
-      fph[b] ^= 1u;
+    const int pre = nkc < S ? nkc : S;
+    for (int ch = 0; ch < pre; ++ch) load(ch);
+    for (int ch = 0; ch < nkc; ++ch) {
+      const int b = ch % S;
+      if (!mbar_wait_bounded(&full[b], (fph >> b) & 1u)) { ok = false; break; }
+      fph ^= 1u << b;
       tc_fence_after();
-      const uint32_t s0 = smem_u32(smem + b * 4 * CHUNK_BYTES);
+      const uint32_t s0 = smem_u32(smem + b * STAGE_BYTES);
       const uint32_t ah = s0, al = s0 + CHUNK_BYTES, bh = s0 + 2 * CHUNK_BYTES, bl = s0 + 3 * CHUNK_BYTES;
 #pragma unroll
       for (int s = 0; s < KC / 16; ++s) {
@@ -360,43 +395,48 @@ __device__ void tile_planes(const char* a_hi, const char* a_lo, const char* b_hi
         mma_bf16(tmem, dal, dbh, idesc, 1u);
       }
       mma_commit(&done[b]);
-      if (ch + 1 < nkc) {
-        const int nb = (ch + 1) & 1;
-        if (ch >= 1) {  // stage nb was read by the MMAs of chunk ch-1
-          if (!mbar_wait_bounded(&done[nb], dph[nb])) { ok = false; break; }
-          dph[nb] ^= 1u;
-        }
-        load(ch + 1);
+      // the stage of chunk ch-1 takes chunk ch-1+S once its MMAs are done
+      if (ch >= 1 && ch - 1 + S < nkc) {
+        const int pb = (ch - 1) % S;
+        if (!mbar_wait_bounded(&done[pb], (dph >> pb) & 1u)) { ok = false; break; }
+        dph ^= 1u << pb;
+        load(ch - 1 + S);
       }
     }
+    // the last commit covers every MMA issued before it
     if (ok && nkc > 0) {
-      const int b = (nkc - 1) & 1;
-      if (!mbar_wait_bounded(&done[b], dph[b])) ok = false;
+      const int b = (nkc - 1) % S;
+      if (!mbar_wait_bounded(&done[b], (dph >> b) & 1u)) ok = false;
     }
     if (!ok) {
       atomicExch(err, 1);
       *okflag = 0;
-      for (int b = 0; b < 2; ++b) {  // drain (bounded) before the memory is freed
-        mbar_wait_bounded(&full[b], fph[b]);
-        mbar_wait_bounded(&done[b], dph[b]);
+      for (int b = 0; b < S; ++b) {  // drain (bounded) before the memory is reused
+        mbar_wait_bounded(&full[b], (fph >> b) & 1u);
+        mbar_wait_bounded(&done[b], (dph >> b) & 1u);
       }
     }
   }
   __syncthreads();
-  if (*okflag) {
+  const bool good = *okflag != 0;
+  if (good) {
+    // warps w and w + 4 read TMEM lanes 32 (w % 4) .. +31, one column half each
     tc_fence_after();
-    const int m = warp * 32 + lane;
+    const int q = warp & 3, half = warp >> 2;
+    const int m = q * 32 + lane;
+    float* tile = reinterpret_cast<float*>(smem);
 #pragma unroll 1
-    for (int c = 0; c < (int)NT; c += 16) {
+    for (int c = half * 64; c < half * 64 + 64; c += 16) {
       float v[16];
-      tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c, v);
+      tmem_ld16(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)c, v);
 #pragma unroll
-      for (int i = 0; i < 16; ++i) epi(m, c + i, (double)v[i]);
+      for (int i = 0; i < 16; ++i) tile[m * 128 + ((c + i) ^ (m & 31))] = v[i];
     }
   }
   tc_fence_before();
   __syncthreads();
   if (warp == 0) tmem_dealloc(tmem, NCOLS);
+  return good;
 }
 
 }  // namespace umma

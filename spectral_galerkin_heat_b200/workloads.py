@@ -19,6 +19,12 @@ scalars) plus the :class:`LaserPath` that drives it. All randomness comes from
 * ``precision_track``: 256 x 128 x 64 modes on a 4 x 2 x 1 mm cuboid with the
   straight-track physics; P ~ U[150, 400] W and v ~ U[0.5, 2] m/s from the
   seed; 500 steps of 5 us from x = 0.5 mm.
+* ``uneven_batch``: many cuboids of uneven grid size for batched stepping:
+  Nx from {64, 96, 128, 192, 256}, Ny = Nx/2, Nz from {16, 32, 64}, the
+  64 x 32 x 16 cell size kept (Lx = 2 mm * Nx/64, Ly = Lx/2, Lz = 0.5 mm);
+  straight-track physics with P ~ U[150, 400] W, v ~ U[0.5, 2] m/s and
+  absorptivity ~ U[0.3, 0.4] per instance; Picard with the reference defaults
+  (omega 0.1, tol 1e-4, cap 30).
 """
 from __future__ import annotations
 
@@ -29,7 +35,7 @@ import numpy as np
 from .laser import RasterPath, StraightTrack
 
 __all__ = ["MATERIAL_316L", "straight_track", "nonlinear_raster", "precision_track",
-           "scaled"]
+           "uneven_batch", "scaled"]
 
 MATERIAL_316L = {
     "name": "316L", "rho": 7900.0, "k": 20.0, "Cp": 500.0, "L_f": 0.0,
@@ -86,6 +92,26 @@ def precision_track(seed=0, nx=256, ny=128, nz=64, steps=500, dt=5e-6):
     speed = float(rng.uniform(0.5, 2.0))
     return straight_track(nx, ny, nz, steps=steps, dt=dt, size=(4e-3, 2e-3, 1e-3),
                           x0=0.5e-3, speed=speed, power=power)
+
+
+def uneven_batch(n=64, seed=0, steps=200, dt=5e-6, nx_choices=(64, 96, 128, 192, 256),
+                 nz_choices=(16, 32, 64)):
+    """``n`` seeded ``(cfg, path)`` pairs of uneven grid size (see the module docstring)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        nx = int(rng.choice(nx_choices))
+        nz = int(rng.choice(nz_choices))
+        ny = nx // 2
+        power = float(rng.uniform(150.0, 400.0))
+        speed = float(rng.uniform(0.5, 2.0))
+        absorptivity = float(rng.uniform(0.3, 0.4))
+        size = (2e-3 * nx / 64, 1e-3 * ny / 32, 0.5e-3)
+        cfg, _ = straight_track(nx, ny, nz, steps=steps, dt=dt, size=size, power=power,
+                                absorptivity=absorptivity)
+        cfg["simulation"].update({"max_picard_iter": 30, "picard_omega": 0.1, "picard_tol": 1e-4})
+        out.append((cfg, StraightTrack(0.3e-3, size[1] / 2.0, speed, 0.0, power)))
+    return out
 
 
 def scaled(cfg, nx, ny, nz, size=None, steps=None):
