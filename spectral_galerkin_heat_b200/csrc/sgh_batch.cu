@@ -2,21 +2,24 @@
 //
 // Every stage of the time step runs as ONE launch over all slots of a batch.
 // Work is decomposed per slot: element/column kernels give each slot
-// ceil(S_i / 256) blocks, face transforms give each slot its 16 x 16 output
-// tiles; a block finds its slot by binary search in a prefix table. Per-slot
-// reductions (P_laser, Picard norms, surface max) are per-block partials that
-// a single-block kernel sums slot by slot in a fixed order.
+// ceil(S_i / 256) blocks, face transforms give each slot its tiles (FP64) or
+// 64-column blocks (mixed); a block reads its slot from a block -> slot
+// table. Per-slot reductions (P_laser, Picard norms, surface max) are
+// per-block partials summed slot by slot in a fixed order.
 //
 // The physics is the face-space Picard form (see sgh_b200.cu): every iterate
 // of a slot is aK + KK Ct[p] sigma[y,x], so each step reads the modes twice
-// (K a and the face sums; the commit) and the Picard loop runs on faces. The
-// loop is a conditional graph node that repeats while any slot is still
-// iterating; converged (or inactive) slots skip every kernel of the body, so
-// a slot's result does not depend on what else is in the batch.
+// (K a and the face sums; the commit) and the Picard loop runs on faces: an
+// inverse 2-D transform with the evaporation epilogue, a forward 2-D
+// transform, and the relaxation, whose last blocks also run the convergence
+// test. The loop is a conditional graph node that repeats while any slot is
+// still iterating; converged (or inactive) slots skip every kernel of the
+// body, so a slot's result does not depend on what else is in the batch.
 //
 // Volume state (modes a, K, KK) is FP64 (plain) or FP32 (mixed: K/KK computed
 // in FP64 and rounded once; all arithmetic on them in FP64 registers). Faces,
-// face sums and norms are FP64 in both.
+// face sums and norms are FP64 in both; in mixed precision the face
+// transforms run on the tensor cores from split-BF16 operand planes.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -36,6 +39,8 @@ namespace batch {
 
 constexpr int BT = 256;   // threads of element / column / face kernels
 constexpr int CT = 1024;  // threads of the per-slot control kernels
+constexpr int RPT = 8;    // elements per thread of the relaxation
+constexpr int RB = RPT * BT;
 
 struct BSlot {
   int nx, ny, nz, S;
@@ -46,6 +51,7 @@ struct BSlot {
   int zoff;        // offset in the Ct table
   int mx, my;      // element offsets of the x / y DCT matrices (M, then M^T)
   int blk0, nblk;  // element / column blocks
+  int rblk0, nrblk;  // relaxation blocks (RB elements)
   int tile0, ntile;  // face transform tiles
   int vblk0, nvblk;  // volume blocks (setup kernels)
   int utile0, nutile;  // tensor-core face tiles (mixed precision)
@@ -75,7 +81,9 @@ struct BGlobal {
   int steps_left;
   int umma_err;     // nonzero once a tensor-core wait expired
   int picard_any;   // some slot is still iterating (read by the eager step)
-  unsigned blocks_done;  // ticket counter of kb_relax (back to 0 after each launch)
+  unsigned slots_done;   // slots finished in the current kb_relax launch (back to 0 after it)
+  int n_iter_slots;      // slots iterating in the current Picard iteration
+  int pad;
 };
 
 // Device view of a bound batch (passed by value to every kernel).
@@ -83,10 +91,11 @@ struct BView {
   const BSlot* slot;
   BState* st;
   BGlobal* g;
-  const int* blk_start;   // n + 1
-  const int* tile_start;  // n + 1
-  const int* vblk_start;  // n + 1
-  const int* utile_start; // n + 1 (tensor-core face tiles)
+  const int* blk_slot;    // slot of each element / column block
+  const int* rblk_slot;   // slot of each relaxation block
+  const int* tile_slot;   // slot of each FP64 face-transform tile
+  const int* vblk_slot;   // slot of each volume block
+  const int* utile_slot;  // slot of each tensor-core column block
   __nv_bfloat16* xa_hi;   // operand planes (mixed precision; null otherwise):
   __nv_bfloat16* xa_lo;   //   xa = A = Zt + W_tt sigma, input of the inverse transform
   __nv_bfloat16* xq_hi;   //   xq = q_net, input of the forward transform
@@ -97,16 +106,6 @@ struct BView {
   const double* Ct;
   int n;
 };
-
-__device__ __forceinline__ int find_slot(const int* start, int n, int b) {
-  int lo = 0, hi = n;  // largest s with start[s] <= b
-  while (hi - lo > 1) {
-    const int mid = (lo + hi) >> 1;
-    if (start[mid] <= b) lo = mid;
-    else hi = mid;
-  }
-  return lo;
-}
 
 // Eight lanes 8g..8g+7 of a warp hold consecutive k = k0..k0+7 (k0 % 8 == 0)
 // of one plane row; lane 8g writes the group's 16-byte hi and lo rows. Call
@@ -159,13 +158,14 @@ __global__ void kb_dct_matrix(int N, double* M) {
 }
 
 // BF16 hi/lo planes of an N x N DCT matrix (inv: its transpose), rows = the
-// output index, k = the contracted index.
+// output index, k = the contracted index, in R-row chunks.
+template <int R>
 __global__ void kb_matrix_planes(int N, const double* M, int inv, __nv_bfloat16* hi, __nv_bfloat16* lo) {
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= N * N) return;
   const int r = e / N, k = e - r * N;
   const double val = inv ? M[(size_t)k * N + r] : M[(size_t)r * N + k];
-  umma::plane_put(hi, lo, r, k, (N + umma::KC - 1) / umma::KC, val);
+  umma::plane_put_r<R>(hi, lo, r, k, (N + umma::KC - 1) / umma::KC, val);
 }
 
 // K, KK of every slot exactly as precompute_K_KK (physics/spectral_state.py:374-421),
@@ -173,7 +173,7 @@ __global__ void kb_matrix_planes(int N, const double* M, int inv, __nv_bfloat16*
 template <class R>
 __global__ void __launch_bounds__(BT) kb_tables(BView v, R* K, R* KK, double* Ct) {
   const int b = blockIdx.x;
-  const int s = find_slot(v.vblk_start, v.n, b);
+  const int s = v.vblk_slot[b];
   const BSlot& sl = v.slot[s];
   const long long i = (long long)(b - sl.vblk0) * BT + threadIdx.x;
   if (i < sl.V) {
@@ -200,7 +200,7 @@ __global__ void __launch_bounds__(BT) kb_tables(BView v, R* K, R* KK, double* Ct
 template <class R>
 __global__ void __launch_bounds__(BT) kb_weights(BView v, const R* KK, double* Wtt, double* Qtt) {
   const int b = blockIdx.x;
-  const int s = find_slot(v.blk_start, v.n, b);
+  const int s = v.blk_slot[b];
   const BSlot& sl = v.slot[s];
   const int i = (b - sl.blk0) * BT + threadIdx.x;
   if (i >= sl.S) return;
@@ -271,12 +271,15 @@ __global__ void __launch_bounds__(CT) kb_begin(BView v, cudaGraphConditionalHand
     st.status = SGH_STEP_CAPPED;
     st.rel_err = nan("");
     st.done = sl.max_iter > 0 ? 0 : 1;
-    if (!st.done) any = 1;
+    st.tickets = 0u;
+    if (!st.done) atomicAdd(&any, 1);
   }
   __syncthreads();
   if (threadIdx.x == 0) {
-    v.g->picard_any = any;
-    if (in_graph) cudaGraphSetConditional(h_picard, any ? 1u : 0u);
+    v.g->picard_any = any > 0;
+    v.g->n_iter_slots = any;
+    v.g->slots_done = 0u;
+    if (in_graph) cudaGraphSetConditional(h_picard, any > 0 ? 1u : 0u);
   }
 }
 
@@ -286,7 +289,7 @@ __global__ void __launch_bounds__(BT)
 kb_face_begin(BView v, double* q_las, double* q_net, const double* q_evold, double* part_las) {
   __shared__ double sh[2 * (BT / 32)];
   const int b = blockIdx.x;
-  const int s = find_slot(v.blk_start, v.n, b);
+  const int s = v.blk_slot[b];
   const BSlot& sl = v.slot[s];
   const BState& st = v.st[s];
   if (!st.active) return;
@@ -320,7 +323,7 @@ __global__ void __launch_bounds__(BT)
 kb_pass1(BView v, const R* a, const R* K, const R* KK, double* Zt, double* Yt, double* part_n1) {
   __shared__ double sh[2 * (BT / 32)];
   const int b = blockIdx.x;
-  const int s = find_slot(v.blk_start, v.n, b);
+  const int s = v.blk_slot[b];
   const BSlot& sl = v.slot[s];
   if (!v.st[s].active) return;
   const int i = (b - sl.blk0) * BT + threadIdx.x;
@@ -347,7 +350,7 @@ kb_pass1(BView v, const R* a, const R* K, const R* KK, double* Zt, double* Yt, d
 __global__ void __launch_bounds__(BT)
 kb_assemble(BView v, const double* Zt, const double* Wtt, const double* sigma, double* A) {
   const int b = blockIdx.x;
-  const int s = find_slot(v.blk_start, v.n, b);
+  const int s = v.blk_slot[b];
   const BSlot& sl = v.slot[s];
   if (!v.st[s].active) return;
   const int i = (b - sl.blk0) * BT + threadIdx.x;
@@ -383,7 +386,7 @@ template <int DIR, bool INV, bool SKIP_DONE, class Epi>
 __global__ void __launch_bounds__(AX_THREADS) kb_face_axis(BView v, const double* in, Epi epi, double* part_tile) {
   __shared__ double red[AX_THREADS / 32];
   const int b = blockIdx.x;
-  const int s = find_slot(v.tile_start, v.n, b);
+  const int s = v.tile_slot[b];
   const BSlot& sl = v.slot[s];
   BState& st = v.st[s];
   if (!st.active || (SKIP_DONE && st.done)) return;
@@ -415,36 +418,41 @@ __global__ void __launch_bounds__(AX_THREADS) kb_face_axis(BView v, const double
 }
 
 // ---- fused 2-D face transform on the tensor cores (mixed precision) -------
-// One CTA transforms one 128-column block of a slot's face along both axes:
+// One CTA transforms one NB-column block of a slot's face along both axes:
 //   x-pass  X1[y][c] = sum_x P[y][x] Mx[c][x]    (P: the slot's xa or xq plane)
 //   y-pass  G[r][c]  = sum_y My[r][y] X1[y][c]
 // for every row y < ny (ny <= 256: one or two 128-row tiles). Each x-pass row
-// tile accumulates in tensor memory, is split into BF16 hi/lo and written to
-// shared memory as the K-major B operand of the y-pass; the y-pass row tiles
-// accumulate in tensor memory and reach the epilogue through a shared-memory
-// tile. Separability makes the column blocks independent: a slot's transform
-// needs no exchange between CTAs. One thread streams every operand chunk (the
-// x-pass P and Mx chunks, then the My chunks) through one ring of bulk-copy
-// stages and issues the MMAs, so the My copies are in flight while the x-pass
-// result is being converted. Operands are split-BF16 (three MMAs per k-step,
-// FP32 accumulation), as in tile_planes.
+// tile accumulates in tensor memory (M = 128, N = NB), is split into BF16
+// hi/lo and written to shared memory as the K-major B operand of the y-pass;
+// the y-pass row tiles accumulate in tensor memory and reach the epilogue
+// through a shared-memory tile. Separability makes the column blocks
+// independent: a slot's transform needs no exchange between CTAs. One thread
+// streams every operand chunk (the x-pass P and Mx chunks, then the My
+// chunks) through one ring of bulk-copy stages and issues the MMAs, so the My
+// copies are in flight while the x-pass result is converted. Operands are
+// split-BF16 (three MMAs per k-step, FP32 accumulation), as in tile_planes.
+// Shared memory is sized for two CTAs per SM, so one CTA's epilogue overlaps
+// another's copies and MMAs.
 namespace f2 {
 constexpr int THREADS = 256;
-constexpr int CB = umma::CHUNK_BYTES;  // one 128 x 32 BF16 chunk (8 KB)
-constexpr int STAGE = 4 * CB;          // 32 KB
-constexpr int MAX_STAGES = 6;
-constexpr int SMEM_LIMIT = 227 * 1024;
-constexpr int TAIL = 256;              // barriers, TMEM address, status flag
+constexpr int NB = 64;                       // column block (MMA N)
+constexpr int CA = umma::CHUNK_BYTES;        // 128 x 32 BF16 chunk of an A operand (8 KB)
+constexpr int CBN = NB * umma::KC * 2;       // NB x 32 BF16 chunk of a B operand (4 KB)
+constexpr int STAGE = 2 * CA + 2 * CBN;      // 24 KB: P hi/lo + Mx hi/lo, or My hi/lo
+constexpr int MAX_STAGES = 4;
+constexpr int SMEM_PER_CTA = 233472 / 2 - 1024;  // two CTAs per SM
+constexpr int TAIL = 256;                    // barriers, TMEM address, status flag
+constexpr int STATIC = 512;                  // static shared memory of the kernel (upper bound)
 constexpr int MAX_NY = 256;
-inline int bop_bytes(int max_ny) { return ((max_ny + 31) / 32) * 2 * CB; }
+inline int bop_bytes(int max_ny) { return ((max_ny + 31) / 32) * 2 * CBN; }
 inline int stages(int max_ny) {
-  const int s = (SMEM_LIMIT - 1024 - TAIL - bop_bytes(max_ny)) / STAGE;
+  const int s = (SMEM_PER_CTA - STATIC - TAIL - bop_bytes(max_ny)) / STAGE;
   return s < MAX_STAGES ? s : MAX_STAGES;
 }
 inline int smem_bytes(int max_ny) { return bop_bytes(max_ny) + stages(max_ny) * STAGE + TAIL; }
 }  // namespace f2
 
-inline __host__ __device__ int face_utiles(int nx, int) { return (nx + 127) / 128; }
+inline __host__ __device__ int face_utiles(int nx, int) { return (nx + f2::NB - 1) / f2::NB; }
 
 // Epilogue of the fused transform, on output element (r, c) of the slot's face:
 //   F2_STORE    FP64 face array (x dct_scale if scaled)
@@ -465,15 +473,20 @@ struct F2Args {
   int scaled;
 };
 
+// FP32 tile of 128 x NB results in shared memory: element (m, n) at
+// m * NB + (n ^ (m & 31)) -- a column spreads over all banks for the TMEM
+// copy, a row stays conflict-free for the epilogue.
+__device__ __forceinline__ float f2_tile(const float* t, int m, int n) { return t[m * f2::NB + (n ^ (m & 31))]; }
+
 template <bool INV, bool SKIP_DONE, int KIND>
-__global__ void __launch_bounds__(f2::THREADS, 1)
+__global__ void __launch_bounds__(f2::THREADS, 2)
 kb_face2d(BView v, F2Args args, double* part_tile, int n_stages, int bop_max) {
   using namespace umma;
-  constexpr int CB = f2::CB;
+  constexpr int CA = f2::CA, CBN = f2::CBN, NB = f2::NB;
   extern __shared__ __align__(128) char sm[];
   __shared__ double red[f2::THREADS / 32];
   const int b = blockIdx.x;
-  const int s = find_slot(v.utile_start, v.n, b);
+  const int s = v.utile_slot[b];
   const BSlot& sl = v.slot[s];
   const BState& st = v.st[s];
   if (!st.active || (SKIP_DONE && st.done)) return;
@@ -486,7 +499,7 @@ kb_face2d(BView v, F2Args args, double* part_tile, int n_stages, int bop_max) {
   const int nkx = (nx + KC - 1) / KC, nky = (ny + KC - 1) / KC;
   const int nrt = (ny + TM - 1) / TM;
   const int S = n_stages;
-  const int n_x = nrt * nkx, total = n_x + nky;
+  const int n_x = nrt * nkx, total = n_x + nrt * nky;
   char* bop = sm;                // y-pass B operand: nky chunks of {hi, lo}
   char* ring = sm + bop_max;     // S stages; later the epilogue tile
   uint64_t* full = reinterpret_cast<uint64_t*>(ring + S * f2::STAGE);
@@ -494,49 +507,35 @@ kb_face2d(BView v, F2Args args, double* part_tile, int n_stages, int bop_max) {
   uint32_t* tslot = reinterpret_cast<uint32_t*>(done + f2::MAX_STAGES);
   volatile int* okflag = reinterpret_cast<volatile int*>(tslot + 1);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const uint32_t ncols = nrt > 1 ? 256u : 128u;
+  const uint32_t ncols = nrt > 1 ? 128u : 64u;
   const char* p_hi = reinterpret_cast<const char*>(INV ? v.xa_hi : v.xq_hi) + fp.xa;
   const char* p_lo = reinterpret_cast<const char*>(INV ? v.xa_lo : v.xq_lo) + fp.xa;
-  const long long mxo = (INV ? sl.mpx_inv : sl.mpx) + (long long)ct * nkx * CB;
-  const long long myo = INV ? sl.mpy_inv : sl.mpy;
-  const uint32_t idesc = idesc_bf16_f32(TM, 128);
+  const long long mxo = (INV ? sl.mpx_inv : sl.mpx) + (long long)ct * nkx * CBN;  // NB-row chunks
+  const long long myo = INV ? sl.mpy_inv : sl.mpy;                                // 128-row chunks
+  const uint32_t idesc = idesc_bf16_f32(TM, NB);
 
-  if (warp == 0) tmem_alloc(tslot, ncols);
-  if (tid == 0) {
-    for (int i = 0; i < S; ++i) {
-      mbar_init(&full[i], 1);
-      mbar_init(&done[i], 1);
-    }
-    *okflag = 1;
-    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
-  }
-  tc_fence_before();
-  __syncthreads();
-  tc_fence_after();
-  const uint32_t tmem = *tslot;
-
+  uint32_t tmem = 0;  // tensor-memory base, set once allocated
   // Thread 0's ring: chunk g lives in stage g % S; each barrier completes one
   // phase per use of its stage, so chunk g waits for parity (g / S) & 1.
+  // Chunks: x-pass (rt, kc) = P hi/lo + Mx hi/lo; then y-pass (rt, kc) = My hi/lo.
   int issued = 0, committed = 0;
   auto load = [&](int g) {
     char* stg = ring + (g % S) * f2::STAGE;
     uint64_t* bar = &full[g % S];
     if (g < n_x) {
       const int rt = g / nkx, kc = g - rt * nkx;
-      const size_t po = (size_t)(rt * nkx + kc) * CB;
-      mbar_expect_tx(bar, 4 * CB);
-      bulk_g2s(stg, p_hi + po, CB, bar);
-      bulk_g2s(stg + CB, p_lo + po, CB, bar);
-      bulk_g2s(stg + 2 * CB, v.mp_hi + mxo + (size_t)kc * CB, CB, bar);
-      bulk_g2s(stg + 3 * CB, v.mp_lo + mxo + (size_t)kc * CB, CB, bar);
+      const size_t po = (size_t)(rt * nkx + kc) * CA;
+      mbar_expect_tx(bar, 2 * CA + 2 * CBN);
+      bulk_g2s(stg, p_hi + po, CA, bar);
+      bulk_g2s(stg + CA, p_lo + po, CA, bar);
+      bulk_g2s(stg + 2 * CA, v.mp_hi + mxo + (size_t)kc * CBN, CBN, bar);
+      bulk_g2s(stg + 2 * CA + CBN, v.mp_lo + mxo + (size_t)kc * CBN, CBN, bar);
     } else {
-      const int kc = g - n_x;
-      mbar_expect_tx(bar, 2 * nrt * CB);
-      for (int rt = 0; rt < nrt; ++rt) {
-        const size_t mo = (size_t)myo + (size_t)(rt * nky + kc) * CB;
-        bulk_g2s(stg + 2 * rt * CB, v.mp_hi + mo, CB, bar);
-        bulk_g2s(stg + (2 * rt + 1) * CB, v.mp_lo + mo, CB, bar);
-      }
+      const int gy = g - n_x, rt = gy / nky, kc = gy - rt * nky;
+      const size_t mo = (size_t)myo + (size_t)(rt * nky + kc) * CA;
+      mbar_expect_tx(bar, 2 * CA);
+      bulk_g2s(stg, v.mp_hi + mo, CA, bar);
+      bulk_g2s(stg + CA, v.mp_lo + mo, CA, bar);
     }
   };
   auto wait_full = [&](int g) { return mbar_wait_bounded(&full[g % S], (uint32_t)((g / S) & 1)); };
@@ -545,36 +544,29 @@ kb_face2d(BView v, F2Args args, double* part_tile, int n_stages, int bop_max) {
     if (!wait_full(g)) return false;
     tc_fence_after();
     const uint32_t s0 = smem_u32(ring + (g % S) * f2::STAGE);
+    uint32_t ah, al, bh, bl, d;
+    int kc;
     if (g < n_x) {
-      const int kc = g % nkx;
-#pragma unroll
-      for (int k = 0; k < KC / 16; ++k) {
-        const uint32_t o = (uint32_t)(2 * k * (TM / 8) * 128);
-        const uint64_t dah = smem_desc(s0 + o, (TM / 8) * 128, 128);
-        const uint64_t dal = smem_desc(s0 + CB + o, (TM / 8) * 128, 128);
-        const uint64_t dbh = smem_desc(s0 + 2 * CB + o, (TM / 8) * 128, 128);
-        const uint64_t dbl = smem_desc(s0 + 3 * CB + o, (TM / 8) * 128, 128);
-        mma_bf16(tmem, dah, dbh, idesc, (kc > 0 || k > 0) ? 1u : 0u);
-        mma_bf16(tmem, dah, dbl, idesc, 1u);
-        mma_bf16(tmem, dal, dbh, idesc, 1u);
-      }
+      kc = g % nkx;
+      ah = s0; al = s0 + CA; bh = s0 + 2 * CA; bl = s0 + 2 * CA + CBN;
+      d = tmem;
     } else {
-      const int kc = g - n_x;
-      const uint32_t b0 = smem_u32(bop + kc * 2 * CB);
-      for (int rt = 0; rt < nrt; ++rt) {
+      const int gy = g - n_x, rt = gy / nky;
+      kc = gy - rt * nky;
+      ah = s0; al = s0 + CA;
+      bh = smem_u32(bop + kc * 2 * CBN); bl = bh + CBN;
+      d = tmem + (uint32_t)(rt * NB);
+    }
 #pragma unroll
-        for (int k = 0; k < KC / 16; ++k) {
-          const uint32_t o = (uint32_t)(2 * k * (TM / 8) * 128);
-          const uint64_t dah = smem_desc(s0 + 2 * rt * CB + o, (TM / 8) * 128, 128);
-          const uint64_t dal = smem_desc(s0 + (2 * rt + 1) * CB + o, (TM / 8) * 128, 128);
-          const uint64_t dbh = smem_desc(b0 + o, (TM / 8) * 128, 128);
-          const uint64_t dbl = smem_desc(b0 + CB + o, (TM / 8) * 128, 128);
-          const uint32_t d = tmem + (uint32_t)(rt * 128);
-          mma_bf16(d, dah, dbh, idesc, (kc > 0 || k > 0) ? 1u : 0u);
-          mma_bf16(d, dah, dbl, idesc, 1u);
-          mma_bf16(d, dal, dbh, idesc, 1u);
-        }
-      }
+    for (int k = 0; k < KC / 16; ++k) {
+      const uint32_t oa = (uint32_t)(2 * k * (TM / 8) * 128), ob = (uint32_t)(2 * k * (NB / 8) * 128);
+      const uint64_t dah = smem_desc(ah + oa, (TM / 8) * 128, 128);
+      const uint64_t dal = smem_desc(al + oa, (TM / 8) * 128, 128);
+      const uint64_t dbh = smem_desc(bh + ob, (NB / 8) * 128, 128);
+      const uint64_t dbl = smem_desc(bl + ob, (NB / 8) * 128, 128);
+      mma_bf16(d, dah, dbh, idesc, (kc > 0 || k > 0) ? 1u : 0u);
+      mma_bf16(d, dah, dbl, idesc, 1u);
+      mma_bf16(d, dal, dbh, idesc, 1u);
     }
     mma_commit(&done[g % S]);
     committed = g + 1;
@@ -593,12 +585,25 @@ kb_face2d(BView v, F2Args args, double* part_tile, int n_stages, int bop_max) {
     for (int g = committed - S < 0 ? 0 : committed - S; g < committed; ++g) wait_done(g);
   };
 
+  // the first copies go out before the tensor memory is allocated
   if (tid == 0) {
+    for (int i = 0; i < S; ++i) {
+      mbar_init(&full[i], 1);
+      mbar_init(&done[i], 1);
+    }
+    *okflag = 1;
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     const int pre = total < S ? total : S;
     for (int g = 0; g < pre; ++g) load(g);
     issued = pre;
   }
-  const int q = warp & 3, half = warp >> 2;
+  __syncwarp();
+  if (warp == 0) tmem_alloc(tslot, ncols);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  tmem = *tslot;
+  const int q = warp & 3, half = warp >> 2;  // TMEM lane quarter, column half
   for (int rt = 0; rt < nrt; ++rt) {
     if (tid == 0 && *okflag) {
       bool ok = true;
@@ -613,10 +618,11 @@ kb_face2d(BView v, F2Args args, double* part_tile, int n_stages, int bop_max) {
       tc_fence_after();
       const int y = rt * TM + q * 32 + lane;
       const bool keep = y < nky * KC;
-#pragma unroll 1
-      for (int c = half * 64; c < half * 64 + 64; c += 16) {
+      const int c = half * 32;
+#pragma unroll
+      for (int cc = 0; cc < 32; cc += 16) {
         float x16[16];
-        tmem_ld16(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)c, x16);
+        tmem_ld16(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(c + cc), x16);
 #pragma unroll
         for (int i = 0; i < 16; ++i) {
           __nv_bfloat16 h, l;
@@ -625,9 +631,9 @@ kb_face2d(BView v, F2Args args, double* part_tile, int n_stages, int bop_max) {
           const uint32_t hn = __shfl_down_sync(0xffffffffu, hv, 1);
           const uint32_t ln = __shfl_down_sync(0xffffffffu, lv, 1);
           if ((lane & 1) == 0 && keep) {
-            const uint32_t o = (uint32_t)((y >> 5) * 2 * CB) + core_off(c + i, y & 31, TM);
+            const uint32_t o = (uint32_t)((y >> 5) * 2 * CBN) + core_off(c + cc + i, y & 31, NB);
             *reinterpret_cast<uint32_t*>(bop + o) = hv | (hn << 16);
-            *reinterpret_cast<uint32_t*>(bop + CB + o) = lv | (ln << 16);
+            *reinterpret_cast<uint32_t*>(bop + CBN + o) = lv | (ln << 16);
           }
         }
       }
@@ -639,27 +645,28 @@ kb_face2d(BView v, F2Args args, double* part_tile, int n_stages, int bop_max) {
   if (tid == 0 && *okflag) {
     tc_fence_after();
     bool ok = true;
-    for (int kc = 0; kc < nky && ok; ++kc) ok = step(n_x + kc);
+    for (int g = n_x; g < total && ok; ++g) ok = step(g);
     if (ok) ok = wait_done(total - 1);
     if (!ok) fail();
   }
   __syncthreads();
 
-  constexpr int ITEMS = TM * 128 / f2::THREADS;  // tile elements per thread
+  constexpr int ITEMS = TM * NB / f2::THREADS;  // tile elements per thread
   double mx = -INFINITY;
-  const int c0 = ct * 128;
+  const int c0 = ct * NB;
+  float* tile = reinterpret_cast<float*>(ring);
   for (int rt = 0; rt < nrt; ++rt) {
     const bool good = *okflag != 0;
     if (good) {
       tc_fence_after();
       const int m = q * 32 + lane;
-      float* tile = reinterpret_cast<float*>(ring);
-#pragma unroll 1
-      for (int c = half * 64; c < half * 64 + 64; c += 16) {
-        float x16[16];
-        tmem_ld16(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(rt * 128 + c), x16);
+      const int c = half * 32;
 #pragma unroll
-        for (int i = 0; i < 16; ++i) tile[m * 128 + ((c + i) ^ (m & 31))] = x16[i];
+      for (int cc = 0; cc < 32; cc += 16) {
+        float x16[16];
+        tmem_ld16(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(rt * NB + c + cc), x16);
+#pragma unroll
+        for (int i = 0; i < 16; ++i) tile[m * NB + ((c + cc + i) ^ (m & 31))] = x16[i];
       }
     }
     __syncthreads();
@@ -674,18 +681,18 @@ kb_face2d(BView v, F2Args args, double* part_tile, int n_stages, int bop_max) {
 #pragma unroll
           for (int u = 0; u < U; ++u) {
             const int e = tid + (it0 + u) * f2::THREADS;
-            const int y = r0 + e / 128, x = c0 + e % 128;
+            const int y = r0 + e / NB, x = c0 + e % NB;
             ql[u] = (y < ny && x < nx) ? __ldg(args.in2 + fp.face + (long long)y * nx + x) : 0.0;
           }
 #pragma unroll
           for (int u = 0; u < U; ++u) {
             const int e = tid + (it0 + u) * f2::THREADS;
-            const int m = e / 128, n = e % 128;
+            const int m = e / NB, n = e % NB;
             const int y = r0 + m, x = c0 + n;
             const bool in = y < ny && x < nx;
             double qn = 0.0;
             if (in) {
-              const double qe = evaporation(fp, fp.recon_scale * (double)tile_value(ring, m, n));
+              const double qe = evaporation(fp, fp.recon_scale * (double)f2_tile(tile, m, n));
               args.out[fp.face + (long long)y * nx + x] = qe;
               qn = ql[u] - qe;
             }
@@ -700,7 +707,7 @@ kb_face2d(BView v, F2Args args, double* part_tile, int n_stages, int bop_max) {
 #pragma unroll
           for (int u = 0; u < U; ++u) {
             const int e = tid + (it0 + u) * f2::THREADS;
-            const int y = r0 + e / 128, x = c0 + e % 128;
+            const int y = r0 + e / NB, x = c0 + e % NB;
             idx[u] = (y < ny && x < nx) ? fp.face + (long long)y * nx + x : -1;
             src[u] = (KIND == F2_COMMIT && idx[u] >= 0) ? __ldg(args.in2 + idx[u]) : 0.0;
           }
@@ -708,7 +715,7 @@ kb_face2d(BView v, F2Args args, double* part_tile, int n_stages, int bop_max) {
           for (int u = 0; u < U; ++u) {
             if (idx[u] < 0) continue;
             const int e = tid + (it0 + u) * f2::THREADS;
-            const double val = (double)tile_value(ring, e / 128, e % 128);
+            const double val = (double)f2_tile(tile, e / NB, e % NB);
             if (KIND == F2_STORE) {
               args.out[idx[u]] = args.scaled ? val * fp.dct_scale : val;
             } else {  // F2_COMMIT
@@ -777,90 +784,116 @@ struct EB_CommitSurface {  // T_temp, its max, q_evap_old <- q_evap (solvers/spe
 // Face-state update of one Picard iteration (see k_fs_relax in sgh_b200.cu):
 // residual and iterate norms from the constant weights, relaxation of sigma
 // and the next top-surface input A = Zt + W_tt sigma (FP64 array when A is
-// given, xa operand plane in mixed precision). Then the per-slot convergence
-// test (solvers/spectral.py:464-499) without a second launch: every block of
-// a slot takes a ticket after publishing its partials, and the block that
-// draws the slot's last ticket sums that slot's partials in a fixed order
-// (so a slot's result does not depend on the rest of the batch) and updates
-// its state; the last block of the launch sets the Picard loop condition.
-// No block waits on another.
+// given, xa operand plane in mixed precision); RPT elements per thread, loads
+// ahead of stores. Then the per-slot convergence test
+// (solvers/spectral.py:464-499) without a second launch: every block of a
+// slot takes a ticket after publishing its partials; the block that draws the
+// slot's last ticket sums that slot's partials in a fixed order (so a slot's
+// result does not depend on the rest of the batch) and updates its state;
+// the finisher of the last iterating slot sets the Picard loop condition and
+// the number of slots that iterate next. No block waits on another.
 __global__ void __launch_bounds__(BT)
 kb_relax(BView v, const double* Zt, const double* Yt, const double* Wtt, const double* Qtt,
          const double* S_top, double* sigma, double* A, double* part, const double* part_n1,
          cudaGraphConditionalHandle h_picard, int in_graph) {
   __shared__ double sh[2 * (BT / 32)];
   __shared__ unsigned ticket;
+  __shared__ int last, count;
   const int b = blockIdx.x;
-  const int s = find_slot(v.blk_start, v.n, b);
+  const int s = v.rblk_slot[b];
   const BSlot& sl = v.slot[s];
   BState& st = v.st[s];
-  if (st.active && !st.done) {
-    const int i = (b - sl.blk0) * BT + threadIdx.x;
-    const bool valid = i < sl.S;
-    double r2 = 0.0, o2 = 0.0, a = 0.0;
-    if (valid) {
-      const long long j = sl.face + i;
-      const double sg = sigma[j], q = Qtt[j], yt = Yt[j], stop = S_top[j], zt = Zt[j], wt = Wtt[j];
-      const double d = stop - sg;
-      r2 = d * d * q;
-      o2 = 2.0 * sg * yt + sg * sg * q;
-      const double ns = d * sl.omega + sg;
-      sigma[j] = ns;
-      a = zt + wt * ns;
-      if (A) A[j] = a;
+  if (!st.active || st.done) return;
+  const int i0 = (b - sl.rblk0) * RB;
+  const long long face = sl.face;
+  const double omega = sl.omega;
+  double r2 = 0.0, o2 = 0.0;
+  constexpr int U = 4;
+#pragma unroll 1
+  for (int u0 = 0; u0 < RPT; u0 += U) {
+    double sg[U], q[U], yt[U], stp[U], zt[U], wt[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int i = i0 + (u0 + u) * BT + threadIdx.x;
+      const bool ok = i < sl.S;
+      const long long j = face + i;
+      sg[u] = ok ? sigma[j] : 0.0;
+      q[u] = ok ? __ldg(Qtt + j) : 0.0;
+      yt[u] = ok ? __ldg(Yt + j) : 0.0;
+      stp[u] = ok ? __ldg(S_top + j) : 0.0;
+      zt[u] = ok ? __ldg(Zt + j) : 0.0;
+      wt[u] = ok ? __ldg(Wtt + j) : 0.0;
     }
-    plane_put_block(v.xa_hi, v.xa_lo, sl, i, a, valid);
-    block_sum2<BT>(r2, o2, sh);
-    if (threadIdx.x == 0) {
-      part[2 * b] = r2;
-      part[2 * b + 1] = o2;
-      __threadfence();
-      ticket = atomicAdd(&st.tickets, 1u);
-    }
-    __syncthreads();
-    if (ticket == (unsigned)sl.nblk - 1u) {
-      __threadfence();
-      double rs = 0.0, os = 0.0;
-      for (int k = threadIdx.x; k < sl.nblk; k += BT) {
-        const int bb = sl.blk0 + k;
-        rs += __ldcg(part + 2 * bb);
-        os += __ldcg(part + 2 * bb + 1) + __ldcg(part_n1 + bb);
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int i = i0 + (u0 + u) * BT + threadIdx.x;
+      const bool ok = i < sl.S;
+      const double d = stp[u] - sg[u];
+      r2 += d * d * q[u];
+      o2 += 2.0 * sg[u] * yt[u] + sg[u] * sg[u] * q[u];
+      const double ns = d * omega + sg[u];
+      const double a = zt[u] + wt[u] * ns;
+      if (ok) {
+        sigma[face + i] = ns;
+        if (A) A[face + i] = a;
       }
-      block_sum2<BT>(rs, os, sh);
-      if (threadIdx.x == 0) {
-        const double n = sl.n_elements;
-        const double rel = sqrt(rs / n) / fmax(sqrt(os / n), 1e-9);
-        const int it = st.iter + 1;
-        st.iter = it;
-        st.rel_err = rel;
-        if (rel < sl.tol) {
-          st.status = SGH_STEP_CONVERGED;
-          st.done = 1;
-        } else if (!isfinite(rel)) {
-          st.status = SGH_STEP_NONFINITE;
-          st.done = 1;
-        } else if (it >= sl.max_iter) {
-          st.status = SGH_STEP_CAPPED;
-          st.done = 1;
-        }
-        st.tickets = 0u;
-      }
+      plane_put_block(v.xa_hi, v.xa_lo, sl, i, ok ? a : 0.0, ok);
     }
   }
-  __threadfence();
-  __syncthreads();
-  if (threadIdx.x == 0) ticket = atomicAdd(&v.g->blocks_done, 1u);
-  __syncthreads();
-  if (ticket != gridDim.x - 1) return;
-  __threadfence();
-  int any = 0;
-  for (int k = threadIdx.x; k < v.n; k += BT)
-    if (__ldcg(&v.st[k].active) && !__ldcg(&v.st[k].done)) any = 1;
-  any = __syncthreads_or(any);
+  block_sum2<BT>(r2, o2, sh);
   if (threadIdx.x == 0) {
-    v.g->blocks_done = 0u;
-    v.g->picard_any = any;
-    if (in_graph) cudaGraphSetConditional(h_picard, any ? 1u : 0u);
+    part[2 * b] = r2;
+    part[2 * b + 1] = o2;
+    __threadfence();
+    ticket = atomicAdd(&st.tickets, 1u);
+  }
+  __syncthreads();
+  if (ticket != (unsigned)sl.nrblk - 1u) return;
+  // this block finishes the slot
+  __threadfence();
+  double rs = 0.0, os = 0.0;
+  for (int k = threadIdx.x; k < sl.nrblk; k += BT) {
+    rs += __ldcg(part + 2 * (sl.rblk0 + k));
+    os += __ldcg(part + 2 * (sl.rblk0 + k) + 1);
+  }
+  for (int k = threadIdx.x; k < sl.nblk; k += BT) os += __ldcg(part_n1 + sl.blk0 + k);
+  block_sum2<BT>(rs, os, sh);
+  if (threadIdx.x == 0) {
+    const double n = sl.n_elements;
+    const double rel = sqrt(rs / n) / fmax(sqrt(os / n), 1e-9);
+    const int it = st.iter + 1;
+    st.iter = it;
+    st.rel_err = rel;
+    if (rel < sl.tol) {
+      st.status = SGH_STEP_CONVERGED;
+      st.done = 1;
+    } else if (!isfinite(rel)) {
+      st.status = SGH_STEP_NONFINITE;
+      st.done = 1;
+    } else if (it >= sl.max_iter) {
+      st.status = SGH_STEP_CAPPED;
+      st.done = 1;
+    }
+    st.tickets = 0u;
+    const int expect = __ldcg(&v.g->n_iter_slots);  // read before the ticket: the last finisher rewrites it
+    __threadfence();
+    last = atomicAdd(&v.g->slots_done, 1u) == (unsigned)expect - 1u;
+    count = 0;
+  }
+  __syncthreads();
+  if (!last) return;
+  // the last finisher: slots iterating next, loop condition
+  __threadfence();
+  int c = 0;
+  for (int k = threadIdx.x; k < v.n; k += BT)
+    if (__ldcg(&v.st[k].active) && !__ldcg(&v.st[k].done)) ++c;
+  if (c) atomicAdd(&count, c);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    v.g->slots_done = 0u;
+    v.g->n_iter_slots = count;
+    v.g->picard_any = count > 0;
+    if (in_graph) cudaGraphSetConditional(h_picard, count > 0 ? 1u : 0u);
   }
 }
 
@@ -869,7 +902,7 @@ template <class R>
 __global__ void __launch_bounds__(BT)
 kb_commit_modes(BView v, R* a, const R* K, const R* KK, const double* sigma) {
   const int b = blockIdx.x;
-  const int s = find_slot(v.blk_start, v.n, b);
+  const int s = v.blk_slot[b];
   const BSlot& sl = v.slot[s];
   if (!v.st[s].active) return;
   const int i = (b - sl.blk0) * BT + threadIdx.x;
@@ -939,13 +972,13 @@ struct sgh_batch {
   int precision = 0;
   std::vector<sgh_config> cfg;
   std::vector<BSlot> slots;
-  std::vector<int> blk_start, tile_start, vblk_start, utile_start;
+  std::vector<int> blk_slot, rblk_slot, tile_slot, vblk_slot, utile_slot;  // block -> slot maps
   std::vector<std::pair<int, long long>> mat_list;  // (N, element offset)
   long long tot_vol = 0, tot_face = 0;
-  int tot_blk = 0, tot_tile = 0, tot_vblk = 0, tot_z = 0, tot_utile = 0;
+  int tot_blk = 0, tot_rblk = 0, tot_tile = 0, tot_vblk = 0, tot_z = 0, tot_utile = 0;
   long long mat_elems = 0;
   // workspace offsets (bytes)
-  size_t o_slot, o_state, o_g, o_blk, o_tile, o_vblk, o_utile, o_mats, o_ct;
+  size_t o_slot, o_state, o_g, o_blk, o_rblk, o_tile, o_vblk, o_utile, o_mats, o_ct;
   size_t o_a, o_K, o_KK;
   size_t o_qlas, o_qnet, o_qev, o_qevold, o_Stop, o_f1, o_sigma, o_A, o_Tsurf, o_Zt, o_Yt, o_Wtt, o_Qtt;
   size_t o_plas, o_pn1, o_prelax, o_ptile;
@@ -968,10 +1001,11 @@ struct sgh_batch {
     v.slot = reinterpret_cast<const BSlot*>(ws + o_slot);
     v.st = reinterpret_cast<BState*>(ws + o_state);
     v.g = reinterpret_cast<BGlobal*>(ws + o_g);
-    v.blk_start = reinterpret_cast<const int*>(ws + o_blk);
-    v.tile_start = reinterpret_cast<const int*>(ws + o_tile);
-    v.vblk_start = reinterpret_cast<const int*>(ws + o_vblk);
-    v.utile_start = reinterpret_cast<const int*>(ws + o_utile);
+    v.blk_slot = reinterpret_cast<const int*>(ws + o_blk);
+    v.rblk_slot = reinterpret_cast<const int*>(ws + o_rblk);
+    v.tile_slot = reinterpret_cast<const int*>(ws + o_tile);
+    v.vblk_slot = reinterpret_cast<const int*>(ws + o_vblk);
+    v.utile_slot = reinterpret_cast<const int*>(ws + o_utile);
     const bool mixed = precision == SGH_PRECISION_MIXED;
     v.xa_hi = mixed ? reinterpret_cast<__nv_bfloat16*>(ws + o_xah) : nullptr;
     v.xa_lo = mixed ? reinterpret_cast<__nv_bfloat16*>(ws + o_xal) : nullptr;
@@ -1046,7 +1080,7 @@ void enqueue_picard(sgh_batch* B, cudaStream_t s, cudaGraphConditionalHandle h, 
   face2d<false, true, F2_STORE>(B, s, B->d(B->o_qnet), EB_Store{B->d(B->o_Stop), 1},
                                 F2Args{B->d(B->o_Stop), nullptr, nullptr, 1}, nullptr);
   // mixed precision keeps A only as the xa operand plane
-  kb_relax<<<B->tot_blk, BT, 0, s>>>(v, B->d(B->o_Zt), B->d(B->o_Yt), B->d(B->o_Wtt), B->d(B->o_Qtt),
+  kb_relax<<<B->tot_rblk, BT, 0, s>>>(v, B->d(B->o_Zt), B->d(B->o_Yt), B->d(B->o_Wtt), B->d(B->o_Qtt),
                                      B->d(B->o_Stop), B->d(B->o_sigma), mixed ? nullptr : B->d(B->o_A),
                                      B->d(B->o_prelax), B->d(B->o_pn1), h, in_graph);
   g_blaunch += 1;
@@ -1179,16 +1213,14 @@ int sgh_batch_create(const sgh_config* cfgs, int32_t n, int32_t precision, sgh_b
   if (precision == SGH_PRECISION_MIXED) {
     long long po = 0;
     for (auto& kv : mats) {
+      // per N: forward, inverse in 128-row chunks; forward, inverse in NB-row chunks
       mplane[kv.first] = po;
       B->mplane_list.push_back({kv.first, po});
-      po += 2LL * (long long)umma::plane_bytes(kv.first, kv.first);
+      po += 2LL * (long long)(umma::plane_bytes_r<128>(kv.first, kv.first) +
+                              umma::plane_bytes_r<f2::NB>(kv.first, kv.first));
     }
     B->mp_bytes = (size_t)po;
   }
-  B->blk_start.assign(n + 1, 0);
-  B->tile_start.assign(n + 1, 0);
-  B->vblk_start.assign(n + 1, 0);
-  B->utile_start.assign(n + 1, 0);
   for (int i = 0; i < n; ++i) {
     const sgh_config& c = cfgs[i];
     BSlot sl;
@@ -1205,6 +1237,8 @@ int sgh_batch_create(const sgh_config* cfgs, int32_t n, int32_t precision, sgh_b
     sl.my = (int)mats[c.ny];
     sl.blk0 = B->tot_blk;
     sl.nblk = cdivl(sl.S, BT);
+    sl.rblk0 = B->tot_rblk;
+    sl.nrblk = cdivl(sl.S, RB);
     sl.tile0 = B->tot_tile;
     sl.ntile = face_tiles(c.nx, c.ny);
     sl.vblk0 = B->tot_vblk;
@@ -1214,10 +1248,10 @@ int sgh_batch_create(const sgh_config* cfgs, int32_t n, int32_t precision, sgh_b
     if (precision == SGH_PRECISION_MIXED) {
       sl.xa = (long long)B->xa_bytes;
       B->xa_bytes += umma::plane_bytes(c.ny, c.nx);
-      sl.mpx = mplane[c.nx];
-      sl.mpx_inv = sl.mpx + (long long)umma::plane_bytes(c.nx, c.nx);
+      sl.mpx = mplane[c.nx] + 2LL * (long long)umma::plane_bytes_r<128>(c.nx, c.nx);
+      sl.mpx_inv = sl.mpx + (long long)umma::plane_bytes_r<f2::NB>(c.nx, c.nx);
       sl.mpy = mplane[c.ny];
-      sl.mpy_inv = sl.mpy + (long long)umma::plane_bytes(c.ny, c.ny);
+      sl.mpy_inv = sl.mpy + (long long)umma::plane_bytes_r<128>(c.ny, c.ny);
     }
     sl.Lx = c.Lx; sl.Ly = c.Ly; sl.Lz = c.Lz;
     sl.dx = c.Lx / c.nx; sl.dy = c.Ly / c.ny;
@@ -1244,13 +1278,15 @@ int sgh_batch_create(const sgh_config* cfgs, int32_t n, int32_t precision, sgh_b
     B->tot_face += sl.S;
     B->tot_z += c.nz;
     B->tot_blk += sl.nblk;
+    B->tot_rblk += sl.nrblk;
     B->tot_tile += sl.ntile;
     B->tot_vblk += sl.nvblk;
     B->tot_utile += sl.nutile;
-    B->blk_start[i + 1] = B->tot_blk;
-    B->tile_start[i + 1] = B->tot_tile;
-    B->vblk_start[i + 1] = B->tot_vblk;
-    B->utile_start[i + 1] = B->tot_utile;
+    B->blk_slot.insert(B->blk_slot.end(), sl.nblk, i);
+    B->rblk_slot.insert(B->rblk_slot.end(), sl.nrblk, i);
+    B->tile_slot.insert(B->tile_slot.end(), sl.ntile, i);
+    B->vblk_slot.insert(B->vblk_slot.end(), sl.nvblk, i);
+    B->utile_slot.insert(B->utile_slot.end(), sl.nutile, i);
   }
   LayoutB L;
   const size_t F8 = sizeof(double) * (size_t)B->tot_face;
@@ -1258,10 +1294,11 @@ int sgh_batch_create(const sgh_config* cfgs, int32_t n, int32_t precision, sgh_b
   B->o_slot = L.take(sizeof(BSlot) * n);
   B->o_state = L.take(sizeof(BState) * n);
   B->o_g = L.take(sizeof(BGlobal));
-  B->o_blk = L.take(sizeof(int) * (n + 1));
-  B->o_tile = L.take(sizeof(int) * (n + 1));
-  B->o_vblk = L.take(sizeof(int) * (n + 1));
-  B->o_utile = L.take(sizeof(int) * (n + 1));
+  B->o_blk = L.take(sizeof(int) * (size_t)B->tot_blk);
+  B->o_rblk = L.take(sizeof(int) * (size_t)B->tot_rblk);
+  B->o_tile = L.take(sizeof(int) * (size_t)B->tot_tile);
+  B->o_vblk = L.take(sizeof(int) * (size_t)B->tot_vblk);
+  B->o_utile = L.take(sizeof(int) * (size_t)B->tot_utile);
   B->o_mats = L.take(sizeof(double) * (size_t)B->mat_elems);
   B->o_ct = L.take(sizeof(double) * (size_t)B->tot_z);
   B->o_a = L.take(VE);
@@ -1332,10 +1369,14 @@ int sgh_batch_bind(sgh_batch* B, void* workspace, uint64_t bytes, void* stream) 
   SGB_CK(cudaMemcpyAsync(B->ws + B->o_slot, B->slots.data(), sizeof(BSlot) * n, cudaMemcpyHostToDevice, s));
   SGB_CK(cudaMemsetAsync(B->ws + B->o_state, 0, sizeof(BState) * n, s));
   SGB_CK(cudaMemsetAsync(B->ws + B->o_g, 0, sizeof(BGlobal), s));
-  SGB_CK(cudaMemcpyAsync(B->ws + B->o_blk, B->blk_start.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice, s));
-  SGB_CK(cudaMemcpyAsync(B->ws + B->o_tile, B->tile_start.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice, s));
-  SGB_CK(cudaMemcpyAsync(B->ws + B->o_vblk, B->vblk_start.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice, s));
-  SGB_CK(cudaMemcpyAsync(B->ws + B->o_utile, B->utile_start.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice, s));
+  const auto put = [&](size_t off, const std::vector<int>& m) {
+    return cudaMemcpyAsync(B->ws + off, m.data(), sizeof(int) * m.size(), cudaMemcpyHostToDevice, s);
+  };
+  SGB_CK(put(B->o_blk, B->blk_slot));
+  SGB_CK(put(B->o_rblk, B->rblk_slot));
+  SGB_CK(put(B->o_tile, B->tile_slot));
+  SGB_CK(put(B->o_vblk, B->vblk_slot));
+  SGB_CK(put(B->o_utile, B->utile_slot));
   SGB_CK(cudaMemsetAsync(B->ws + B->o_qevold, 0, sizeof(double) * B->tot_face, s));
   SGB_CK(cudaMemsetAsync(B->ws + B->o_qev, 0, sizeof(double) * B->tot_face, s));
   for (auto& m : B->mat_list)
@@ -1354,11 +1395,15 @@ int sgh_batch_bind(sgh_batch* B, void* workspace, uint64_t bytes, void* stream) 
       long long moff = -1;
       for (auto& m : B->mat_list)
         if (m.first == N) moff = m.second;
-      const size_t pb = umma::plane_bytes(N, N);
-      for (int inv = 0; inv < 2; ++inv)
-        kb_matrix_planes<<<cdivl((long long)N * N, BT), BT, 0, s>>>(
-            N, B->d(B->o_mats) + moff, inv, reinterpret_cast<__nv_bfloat16*>(B->ws + B->o_mph + po + inv * pb),
-            reinterpret_cast<__nv_bfloat16*>(B->ws + B->o_mpl + po + inv * pb));
+      const size_t pb = umma::plane_bytes_r<128>(N, N), pn = umma::plane_bytes_r<f2::NB>(N, N);
+      auto hi = [&](size_t o) { return reinterpret_cast<__nv_bfloat16*>(B->ws + B->o_mph + po + o); };
+      auto lo = [&](size_t o) { return reinterpret_cast<__nv_bfloat16*>(B->ws + B->o_mpl + po + o); };
+      const int g = cdivl((long long)N * N, BT);
+      for (int inv = 0; inv < 2; ++inv) {
+        kb_matrix_planes<128><<<g, BT, 0, s>>>(N, B->d(B->o_mats) + moff, inv, hi(inv * pb), lo(inv * pb));
+        kb_matrix_planes<f2::NB><<<g, BT, 0, s>>>(N, B->d(B->o_mats) + moff, inv, hi(2 * pb + inv * pn),
+                                                 lo(2 * pb + inv * pn));
+      }
     }
     float* K = reinterpret_cast<float*>(B->ws + B->o_K);
     float* KK = reinterpret_cast<float*>(B->ws + B->o_KK);

@@ -281,6 +281,22 @@ __device__ __forceinline__ void plane_put(__nv_bfloat16* hi, __nv_bfloat16* lo, 
   lo[o] = l;
 }
 
+// The same layout with R-row chunks (R = 64 or 128): chunk (r / R, k / KC)
+// of R * KC * 2 bytes, core matrices as core_off(r % R, k % KC, R).
+template <int R>
+__host__ __device__ inline size_t plane_bytes_r(int rows, int k) {
+  return (size_t)((rows + R - 1) / R) * (size_t)((k + KC - 1) / KC) * (size_t)(R * KC * 2);
+}
+template <int R>
+__device__ __forceinline__ void plane_put_r(__nv_bfloat16* hi, __nv_bfloat16* lo, int r, int k, int nkc,
+                                            double x) {
+  __nv_bfloat16 h, l;
+  split_bf16(x, h, l);
+  const size_t o = ((size_t)((r / R) * nkc + k / KC) * (R * KC * 2) + core_off(r % R, k % KC, R)) / 2;
+  hi[o] = h;
+  lo[o] = l;
+}
+
 __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
                : "memory");
