@@ -261,6 +261,12 @@ int sgh_batch_error(const sgh_batch* batch, int32_t* err, void* stream);
 /* Kernels per batch step: *pre + n_iter * *per_iter + *post, n_iter = the
  * largest iteration count over the active slots. */
 int sgh_batch_launch_counts(const sgh_batch* batch, int32_t* pre, int32_t* per_iter, int32_t* post);
+/* The step's volume pass by itself, over every active slot: the modal commit
+ * a <- K a + KK Ct sigma (solvers/spectral.py:502-512 with
+ * spectral_cpu_kernels.py:83-91), fused with the next step's face sums. For
+ * timing and profiling the memory-bound pass of a batch; the slots' modes
+ * advance as in a commit. Async. */
+int sgh_batch_volume_pass(sgh_batch* batch, void* stream);
 
 /* Orthonormal 2-D DCT-II (kind 2) or DCT-III (kind 3) of an (ny, nx) FP64
  * face with both contractions on the tensor cores (tcgen05) in split-BF16

@@ -34,7 +34,7 @@ EXPORTED = (
     "sgh_batch_create", "sgh_batch_destroy", "sgh_batch_workspace_bytes", "sgh_batch_bind",
     "sgh_batch_slot_start", "sgh_batch_slot_stop", "sgh_batch_step", "sgh_batch_step_eager",
     "sgh_batch_status",
-    "sgh_batch_buffer", "sgh_batch_launch_counts", "sgh_batch_error", "sgh_dct2_bf16x3_workspace_bytes",
+    "sgh_batch_buffer", "sgh_batch_launch_counts", "sgh_batch_volume_pass", "sgh_batch_error", "sgh_dct2_bf16x3_workspace_bytes",
     "sgh_dct2_bf16x3",
 )
 
@@ -138,6 +138,7 @@ def lib() -> C.CDLL:
             "sgh_batch_buffer": ([vp, i32, i32, C.POINTER(vp), u64p], C.c_int),
             "sgh_batch_error": ([vp, C.POINTER(i32), vp], C.c_int),
             "sgh_batch_launch_counts": ([vp, C.POINTER(i32), C.POINTER(i32), C.POINTER(i32)], C.c_int),
+            "sgh_batch_volume_pass": ([vp, vp], C.c_int),
         }
         for name, (args, res) in sig.items():
             fn = getattr(L, name)

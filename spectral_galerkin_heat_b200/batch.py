@@ -75,6 +75,23 @@ class BatchSolver:
     def _s(self):
         return C.c_void_p(self.stream.cuda_stream)
 
+    @staticmethod
+    def workspace_bytes_for(contexts: Sequence, precision: str = "fp64") -> int:
+        """Device bytes a batch of these contexts would bind (computed on the host)."""
+        n = len(contexts)
+        cfgs = (_lib.SghConfig * n)()
+        for i, ctx in enumerate(contexts):
+            cfgs[i] = make_config(ctx, *_picard(ctx))
+        L = _lib.lib()
+        h = C.c_void_p()
+        _lib.check("sgh_batch_create", L.sgh_batch_create(cfgs, n, _lib.PRECISION[precision], C.byref(h)))
+        try:
+            nbytes = C.c_uint64()
+            _lib.check("sgh_batch_workspace_bytes", L.sgh_batch_workspace_bytes(h, C.byref(nbytes)))
+            return int(nbytes.value)
+        finally:
+            L.sgh_batch_destroy(h)
+
     @property
     def workspace_bytes(self) -> int:
         return self.workspace.numel()
@@ -154,6 +171,33 @@ class BatchSolver:
 
     def modes(self, slot: int):
         return self.buffer(slot, "modes")
+
+    def upload_table(self, records: np.ndarray):
+        """Device copy (raw bytes) of a host table of ``sgh_laser`` records,
+        from pinned memory on this batch's stream."""
+        import torch
+        host = torch.from_numpy(np.ascontiguousarray(records).view(np.uint8)).pin_memory()
+        with torch.cuda.stream(self.stream):
+            return host.to(self.device, non_blocking=True)
+
+    def fetch(self, slot: int, name: str) -> np.ndarray:
+        """Host copy of a slot buffer (synchronises the stream)."""
+        return self.buffer(slot, name).to("cpu").numpy()
+
+    def snapshot(self, slot: int, name: str):
+        """Device copy of a slot buffer (the slot may be reused afterwards)."""
+        return self.buffer(slot, name).clone()
+
+    def volume_pass(self) -> None:
+        """The step's volume pass alone over every active slot (timing, profiling)."""
+        _lib.check("sgh_batch_volume_pass", _lib.lib().sgh_batch_volume_pass(self._h, self._s()))
+
+    def active_modes(self) -> int:
+        """Modes of the slots that are active now (synchronises)."""
+        return sum(int(c.nx) * int(c.ny) * int(c.nz) for c, st in zip(self._cfgs, self.status()) if st.active)
+
+    def synchronize(self) -> None:
+        self.stream.synchronize()
 
     def tensor_core_error(self) -> int:
         """Nonzero once a tensor-core wait expired in a mixed-precision face pass."""

@@ -49,6 +49,7 @@ struct BSlot {
   long long vol;   // element offset of this slot in the volume arenas
   long long face;  // element offset in the face arenas
   int zoff;        // offset in the Ct table
+  int eoff;        // offset of the slot's 1-D decay tables Ex (nx), Ey (ny), Ez (nz)
   int mx, my;      // element offsets of the x / y DCT matrices (M, then M^T)
   int blk0, nblk;  // element / column blocks
   int rblk0, nrblk;  // relaxation blocks (RB elements)
@@ -73,6 +74,8 @@ struct BState {
   int n_steps, step, active, iters;
   int iter, done, status;
   unsigned tickets;  // kb_relax blocks of this slot done in the current launch
+  int pass1_ready;   // the commit already formed the next step's face sums
+  int pad2;
   double I0, shift_x, shift_y, rel_err;
   sgh_step_out last;
 };
@@ -104,6 +107,7 @@ struct BView {
   const char* mp_lo;
   const double* mats;
   const double* Ct;
+  const double* E;        // 1-D decay tables exp(-alpha dt k_i^2) per slot and axis
   int n;
 };
 
@@ -169,9 +173,12 @@ __global__ void kb_matrix_planes(int N, const double* M, int inv, __nv_bfloat16*
 }
 
 // K, KK of every slot exactly as precompute_K_KK (physics/spectral_state.py:374-421),
-// in FP64, stored as R; Ct tables.
+// in FP64, stored as R (K only when K is given); Ct tables; and the 1-D decay
+// tables E_axis[i] = exp(-alpha dt k_i^2). K = exp(-alpha dt (kx^2 + ky^2 +
+// kz^2)) is exactly separable, so K = Ex[x] Ey[y] Ez[z]: the mixed-precision
+// form evaluates it in FP64 from these tables instead of storing it.
 template <class R>
-__global__ void __launch_bounds__(BT) kb_tables(BView v, R* K, R* KK, double* Ct) {
+__global__ void __launch_bounds__(BT) kb_tables(BView v, R* K, R* KK, double* Ct, double* E) {
   const int b = blockIdx.x;
   const int s = v.vblk_slot[b];
   const BSlot& sl = v.slot[s];
@@ -187,7 +194,19 @@ __global__ void __launch_bounds__(BT) kb_tables(BView v, R* K, R* KK, double* Ct
     const double kx = M_PI * (double)x / sl.Lx;
     const double lam = alpha * (kz * kz + ky * ky + kx * kx);
     const double k = exp(-lam * sl.dt);
-    K[sl.vol + i] = (R)k;
+    if (K) K[sl.vol + i] = (R)k;
+    if (i < sl.nx) {
+      const double q = M_PI * (double)i / sl.Lx;
+      E[sl.eoff + i] = exp(-(alpha * (q * q)) * sl.dt);
+    }
+    if (i < sl.ny) {
+      const double q = M_PI * (double)i / sl.Ly;
+      E[sl.eoff + sl.nx + i] = exp(-(alpha * (q * q)) * sl.dt);
+    }
+    if (i < sl.nz) {
+      const double q = M_PI * (double)i / sl.Lz;
+      E[sl.eoff + sl.nx + sl.ny + i] = exp(-(alpha * (q * q)) * sl.dt);
+    }
     KK[sl.vol + i] = (R)((i == 0) ? sl.dt / rho_cp : ((k - 1.0) / (-lam)) / rho_cp);
     if (i < sl.nz) {
       const double c = (i == 0) ? sqrt(1.0 / sl.Lz) : sqrt(2.0 / sl.Lz);
@@ -238,6 +257,7 @@ kb_slot_start(BView v, int s, R* a, double* q_evold, double* q_ev, double* sigma
     st.iters = 0;
     st.done = 1;
     st.iter = 0;
+    st.pass1_ready = 0;
   }
 }
 
@@ -317,7 +337,9 @@ kb_face_begin(BView v, double* q_las, double* q_net, const double* q_evold, doub
 }
 
 // Face sums of the propagated modes: Zt = sum Ct K a, Yt = sum (K a) KK Ct and
-// partials of sum (K a)^2.
+// partials of sum (K a)^2 -- for the first step of a slot; later steps get
+// them from the previous commit (kb_commit_modes). K is read from the K array
+// or, when K is null, formed from the separable decay tables.
 template <class R>
 __global__ void __launch_bounds__(BT)
 kb_pass1(BView v, const R* a, const R* K, const R* KK, double* Zt, double* Yt, double* part_n1) {
@@ -325,15 +347,19 @@ kb_pass1(BView v, const R* a, const R* K, const R* KK, double* Zt, double* Yt, d
   const int b = blockIdx.x;
   const int s = v.blk_slot[b];
   const BSlot& sl = v.slot[s];
-  if (!v.st[s].active) return;
+  if (!v.st[s].active || v.st[s].pass1_ready) return;
   const int i = (b - sl.blk0) * BT + threadIdx.x;
   double n1 = 0.0, dummy = 0.0;
   if (i < sl.S) {
     double zt = 0.0, yt = 0.0;
     const double* ct = v.Ct + sl.zoff;
+    const double* ez = v.E + sl.eoff + sl.nx + sl.ny;
+    const double exy = K ? 0.0 : v.E[sl.eoff + i % sl.nx] * v.E[sl.eoff + sl.nx + i / sl.nx];
+#pragma unroll 4
     for (int p = 0; p < sl.nz; ++p) {
       const long long j = sl.vol + (long long)p * sl.S + i;
-      const double ak = (double)a[j] * (double)K[j];
+      const double kv = K ? (double)K[j] : exy * ez[p];
+      const double ak = (double)a[j] * kv;
       const double kk = (double)KK[j];
       zt = fma(ct[p], ak, zt);
       yt = fma(ak * kk, ct[p], yt);
@@ -897,21 +923,48 @@ kb_relax(BView v, const double* Zt, const double* Yt, const double* Wtt, const d
   }
 }
 
-// a = K a + KK Ct sigma (commit of the modes).
+// a = K a + KK Ct sigma (commit of the modes), fused with the next step's
+// face sums: with the new modes in registers, Zt = sum Ct K a, Yt = sum (K a)
+// KK Ct and the partials of sum (K a)^2 come for free, so the next step skips
+// kb_pass1 and the volume is read once per step. The sums use the stored
+// (type R) value of a, exactly as kb_pass1 would read it back.
 template <class R>
 __global__ void __launch_bounds__(BT)
-kb_commit_modes(BView v, R* a, const R* K, const R* KK, const double* sigma) {
+kb_commit_modes(BView v, R* a, const R* K, const R* KK, const double* sigma, double* Zt, double* Yt,
+                double* part_n1) {
+  __shared__ double sh[2 * (BT / 32)];
   const int b = blockIdx.x;
   const int s = v.blk_slot[b];
   const BSlot& sl = v.slot[s];
-  if (!v.st[s].active) return;
+  BState& st = v.st[s];
+  if (!st.active) return;
   const int i = (b - sl.blk0) * BT + threadIdx.x;
-  if (i >= sl.S) return;
-  const double sg = sigma[sl.face + i];
-  const double* ct = v.Ct + sl.zoff;
-  for (int p = 0; p < sl.nz; ++p) {
-    const long long j = sl.vol + (long long)p * sl.S + i;
-    a[j] = (R)((double)a[j] * (double)K[j] + (double)KK[j] * (ct[p] * sg));
+  double n1 = 0.0, dummy = 0.0;
+  if (i < sl.S) {
+    const double sg = sigma[sl.face + i];
+    const double* ct = v.Ct + sl.zoff;
+    const double* ez = v.E + sl.eoff + sl.nx + sl.ny;
+    const double exy = K ? 0.0 : v.E[sl.eoff + i % sl.nx] * v.E[sl.eoff + sl.nx + i / sl.nx];
+    double zt = 0.0, yt = 0.0;
+#pragma unroll 4
+    for (int p = 0; p < sl.nz; ++p) {
+      const long long j = sl.vol + (long long)p * sl.S + i;
+      const double kv = K ? (double)K[j] : exy * ez[p];
+      const double kk = (double)KK[j];
+      const R an = (R)((double)a[j] * kv + kk * (ct[p] * sg));
+      a[j] = an;
+      const double ak = (double)an * kv;
+      zt = fma(ct[p], ak, zt);
+      yt = fma(ak * kk, ct[p], yt);
+      n1 = fma(ak, ak, n1);
+    }
+    Zt[sl.face + i] = zt;
+    Yt[sl.face + i] = yt;
+  }
+  block_sum2<BT>(n1, dummy, sh);
+  if (threadIdx.x == 0) {
+    part_n1[b] = n1;
+    st.pass1_ready = 1;
   }
 }
 
@@ -979,7 +1032,8 @@ struct sgh_batch {
   long long mat_elems = 0;
   // workspace offsets (bytes)
   size_t o_slot, o_state, o_g, o_blk, o_rblk, o_tile, o_vblk, o_utile, o_mats, o_ct;
-  size_t o_a, o_K, o_KK;
+  size_t o_a, o_K, o_KK, o_E;
+  long long tot_e = 0;
   size_t o_qlas, o_qnet, o_qev, o_qevold, o_Stop, o_f1, o_sigma, o_A, o_Tsurf, o_Zt, o_Yt, o_Wtt, o_Qtt;
   size_t o_plas, o_pn1, o_prelax, o_ptile;
   size_t o_xah = 0, o_xal = 0, o_xqh = 0, o_xql = 0, o_mph = 0, o_mpl = 0;  // operand planes (mixed)
@@ -1015,6 +1069,7 @@ struct sgh_batch {
     v.mp_lo = mixed ? ws + o_mpl : nullptr;
     v.mats = d(o_mats);
     v.Ct = d(o_ct);
+    v.E = d(o_E);
     v.n = n;
     return v;
   }
@@ -1058,7 +1113,7 @@ template <class R>
 void enqueue_pre(sgh_batch* B, cudaStream_t s, cudaGraphConditionalHandle h, int in_graph) {
   const BView v = B->view();
   R* a = reinterpret_cast<R*>(B->ws + B->o_a);
-  R* K = reinterpret_cast<R*>(B->ws + B->o_K);
+  R* K = B->precision == SGH_PRECISION_MIXED ? nullptr : reinterpret_cast<R*>(B->ws + B->o_K);
   R* KK = reinterpret_cast<R*>(B->ws + B->o_KK);
   kb_begin<<<1, CT, 0, s>>>(v, h, in_graph);
   kb_face_begin<<<B->tot_blk, BT, 0, s>>>(v, B->d(B->o_qlas), B->d(B->o_qnet), B->d(B->o_qevold), B->d(B->o_plas));
@@ -1090,12 +1145,13 @@ template <class R>
 void enqueue_post(sgh_batch* B, cudaStream_t s, cudaGraphConditionalHandle h, int in_graph) {
   const BView v = B->view();
   R* a = reinterpret_cast<R*>(B->ws + B->o_a);
-  R* K = reinterpret_cast<R*>(B->ws + B->o_K);
+  R* K = B->precision == SGH_PRECISION_MIXED ? nullptr : reinterpret_cast<R*>(B->ws + B->o_K);
   R* KK = reinterpret_cast<R*>(B->ws + B->o_KK);
   face2d<true, false, F2_COMMIT>(B, s, B->d(B->o_A),
                                  EB_CommitSurface{B->d(B->o_Tsurf), B->d(B->o_qev), B->d(B->o_qevold)},
                                  F2Args{B->d(B->o_Tsurf), B->d(B->o_qevold), B->d(B->o_qev), 0}, B->d(B->o_ptile));
-  kb_commit_modes<R><<<B->tot_blk, BT, 0, s>>>(v, a, K, KK, B->d(B->o_sigma));
+  kb_commit_modes<R><<<B->tot_blk, BT, 0, s>>>(v, a, K, KK, B->d(B->o_sigma), B->d(B->o_Zt), B->d(B->o_Yt),
+                                               B->d(B->o_pn1));
   kb_commit<<<1, CT, 0, s>>>(v, B->d(B->o_plas), B->d(B->o_ptile),
                              B->precision == SGH_PRECISION_MIXED ? 1 : 0, h, in_graph);
   g_blaunch += 2;
@@ -1233,6 +1289,7 @@ int sgh_batch_create(const sgh_config* cfgs, int32_t n, int32_t precision, sgh_b
     sl.vol = B->tot_vol;
     sl.face = B->tot_face;
     sl.zoff = B->tot_z;
+    sl.eoff = (int)B->tot_e;
     sl.mx = (int)mats[c.nx];
     sl.my = (int)mats[c.ny];
     sl.blk0 = B->tot_blk;
@@ -1277,6 +1334,7 @@ int sgh_batch_create(const sgh_config* cfgs, int32_t n, int32_t precision, sgh_b
     B->tot_vol += sl.V;
     B->tot_face += sl.S;
     B->tot_z += c.nz;
+    B->tot_e += c.nx + c.ny + c.nz;
     B->tot_blk += sl.nblk;
     B->tot_rblk += sl.nrblk;
     B->tot_tile += sl.ntile;
@@ -1302,8 +1360,9 @@ int sgh_batch_create(const sgh_config* cfgs, int32_t n, int32_t precision, sgh_b
   B->o_mats = L.take(sizeof(double) * (size_t)B->mat_elems);
   B->o_ct = L.take(sizeof(double) * (size_t)B->tot_z);
   B->o_a = L.take(VE);
-  B->o_K = L.take(VE);
+  B->o_K = L.take(precision == SGH_PRECISION_MIXED ? 0 : VE);  // mixed: K from the decay tables
   B->o_KK = L.take(VE);
+  B->o_E = L.take(sizeof(double) * (size_t)B->tot_e);
   B->o_qlas = L.take(F8);
   B->o_qnet = L.take(F8);
   B->o_qev = L.take(F8);
@@ -1405,14 +1464,13 @@ int sgh_batch_bind(sgh_batch* B, void* workspace, uint64_t bytes, void* stream) 
                                                  lo(2 * pb + inv * pn));
       }
     }
-    float* K = reinterpret_cast<float*>(B->ws + B->o_K);
     float* KK = reinterpret_cast<float*>(B->ws + B->o_KK);
-    kb_tables<float><<<B->tot_vblk, BT, 0, s>>>(v, K, KK, B->d(B->o_ct));
+    kb_tables<float><<<B->tot_vblk, BT, 0, s>>>(v, nullptr, KK, B->d(B->o_ct), B->d(B->o_E));
     kb_weights<float><<<B->tot_blk, BT, 0, s>>>(v, KK, B->d(B->o_Wtt), B->d(B->o_Qtt));
   } else {
     double* K = B->d(B->o_K);
     double* KK = B->d(B->o_KK);
-    kb_tables<double><<<B->tot_vblk, BT, 0, s>>>(v, K, KK, B->d(B->o_ct));
+    kb_tables<double><<<B->tot_vblk, BT, 0, s>>>(v, K, KK, B->d(B->o_ct), B->d(B->o_E));
     kb_weights<double><<<B->tot_blk, BT, 0, s>>>(v, KK, B->d(B->o_Wtt), B->d(B->o_Qtt));
   }
   SGB_CK(cudaGetLastError());
@@ -1509,7 +1567,12 @@ int sgh_batch_buffer(const sgh_batch* B, int32_t slot, int32_t which, void** ptr
   size_t off, nb;
   switch (which) {
     case SGH_BUF_MODES: off = B->o_a + e * sl.vol; nb = e * sl.V; break;
-    case SGH_BUF_K: off = B->o_K + e * sl.vol; nb = e * sl.V; break;
+    case SGH_BUF_K:
+      if (B->precision == SGH_PRECISION_MIXED)
+        return bfail(SGH_ERR_INVALID, "mixed-precision batches do not store K (it is formed from 1-D tables)");
+      off = B->o_K + e * sl.vol;
+      nb = e * sl.V;
+      break;
     case SGH_BUF_KK: off = B->o_KK + e * sl.vol; nb = e * sl.V; break;
     case SGH_BUF_Q_EVAP_OLD: off = B->o_qevold + sizeof(double) * sl.face; nb = sizeof(double) * sl.S; break;
     case SGH_BUF_SURFACE: off = B->o_Tsurf + sizeof(double) * sl.face; nb = sizeof(double) * sl.S; break;
@@ -1527,6 +1590,23 @@ int sgh_batch_error(const sgh_batch* B, int32_t* err, void* stream) {
   SGB_CK(cudaMemcpyAsync(&g, B->ws + B->o_g, sizeof(BGlobal), cudaMemcpyDeviceToHost, s));
   SGB_CK(cudaStreamSynchronize(s));
   *err = g.umma_err;
+  return SGH_OK;
+}
+
+int sgh_batch_volume_pass(sgh_batch* B, void* stream) {
+  if (!B || !B->bound) return bfail(SGH_ERR_STATE, "batch is not bound");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const BView v = B->view();
+  if (B->precision == SGH_PRECISION_MIXED)
+    kb_commit_modes<float><<<B->tot_blk, BT, 0, s>>>(v, reinterpret_cast<float*>(B->ws + B->o_a), nullptr,
+                                                     reinterpret_cast<const float*>(B->ws + B->o_KK),
+                                                     B->d(B->o_sigma), B->d(B->o_Zt), B->d(B->o_Yt),
+                                                     B->d(B->o_pn1));
+  else
+    kb_commit_modes<double><<<B->tot_blk, BT, 0, s>>>(v, B->d(B->o_a), B->d(B->o_K), B->d(B->o_KK),
+                                                      B->d(B->o_sigma), B->d(B->o_Zt), B->d(B->o_Yt),
+                                                      B->d(B->o_pn1));
+  SGB_CK(cudaGetLastError());
   return SGH_OK;
 }
 

@@ -18,9 +18,12 @@ import math
 from abc import ABC, abstractmethod
 from dataclasses import dataclass
 
+import numpy as np
+
 __all__ = [
     "LaserState", "LaserPath", "LaserProfile", "build_laser_profile",
     "super_gaussian_area_factor", "StraightTrack", "RasterPath", "FixedLaser",
+    "LASER_DTYPE", "laser_table",
 ]
 
 
@@ -136,3 +139,43 @@ class RasterPath(LaserPath):
         else:
             x, vx = self.x0 + self.length - s, -self.speed
         return LaserState(x=x, y=y, power=self.power if on else 0.0, is_on=on, v=(vx, 0.0))
+
+
+# One ``sgh_laser`` record (include/sgh_b200.h): x, y, power, vx, vy, is_on, pad.
+LASER_DTYPE = np.dtype([("x", "<f8"), ("y", "<f8"), ("power", "<f8"), ("vx", "<f8"),
+                        ("vy", "<f8"), ("is_on", "<i4"), ("pad", "<i4")])
+
+
+def laser_table(path: LaserPath, t0: float, dt: float, n: int) -> np.ndarray:
+    """``n`` laser states at ``t0 + i*dt`` as ``sgh_laser`` records.
+
+    Same values as calling ``path.get_state(t0 + i*dt, dt)`` per step (the
+    times and positions use the same float64 operations); straight tracks and
+    rasters are evaluated in one vectorised pass, other paths step by step.
+    """
+    out = np.zeros(n, dtype=LASER_DTYPE)
+    times = t0 + np.arange(n, dtype=np.float64) * dt
+    if isinstance(path, StraightTrack):
+        out["x"] = path.x0 + path.vx * times
+        out["y"] = path.y0 + path.vy * times
+        out["power"] = path.power
+        out["vx"], out["vy"] = path.vx, path.vy
+        out["is_on"] = 1 if path.is_on else 0
+        return out
+    if isinstance(path, RasterPath):
+        t_line = path.length / path.speed
+        j = np.where(times >= 0.0, np.floor(times / t_line), 0.0).astype(np.int64)
+        off = j >= path.n_lines
+        j = np.where(off, path.n_lines - 1, j)
+        s = np.where(off, path.length, (times - j * t_line) * path.speed)
+        even = (j % 2) == 0
+        out["x"] = np.where(even, path.x0 + s, path.x0 + path.length - s)
+        out["y"] = path.y0 + j * path.hatch
+        out["power"] = np.where(off, 0.0, path.power)
+        out["vx"] = np.where(even, path.speed, -path.speed)
+        out["is_on"] = np.where(off, 0, 1)
+        return out
+    for i, t in enumerate(times):
+        st = path.get_state(float(t), dt)
+        out[i] = (st.x, st.y, st.power, st.v[0], st.v[1], 1 if st.is_on else 0, 0)
+    return out

@@ -1,0 +1,284 @@
+"""Continuous-batching serving loop for laser-scan solves of uneven size.
+
+A request is one solve: a grid and physics (a :class:`SimulationContext`), a
+laser path and a step count. Requests arrive over time. The engine holds ONE
+batch (``sgh_batch_*`` of the C ABI) whose slots are grouped into classes of
+identical configuration (same grid and physics; only the laser differs). Its
+capacity is sized from the free device memory when the engine starts: slots
+are handed to the classes in proportion to their expected share of the
+traffic until the memory budget is spent (admission by free HBM). A request
+is admitted as soon as a slot of its class is free: its laser table goes to
+the device, the slot restarts at the initial condition, and its modal state
+stays resident in the slot until the solve completes. Every chunk of steps
+advances all active requests together, one launch per stage of the time step,
+so a request that arrives while others are on the GPU overlaps with them. A
+chunk ends at the next completion (and, with an arrival due, after an
+estimate of the steps that fit before it), so slots free up promptly.
+
+A slot's result does not depend on what else runs in the batch (the batch
+kernels reduce per slot in a fixed order), so a request gives the same result
+alone and in the mix.
+
+Latency is completion minus arrival on the host clock; throughput is the
+timesteps of all completed requests divided by the span from the first
+arrival to the last completion.
+"""
+from __future__ import annotations
+
+import copy
+import time
+from collections import deque
+from dataclasses import dataclass, field
+from typing import Callable, Dict, List, Optional, Sequence, Tuple
+
+import numpy as np
+
+from .batch import BatchSolver
+from .laser import laser_table
+
+__all__ = ["Request", "ServingEngine", "latency_percentiles"]
+
+
+@dataclass
+class Request:
+    """One solve. ``key`` names its class (requests of a class share the
+    context's grid and physics); ``table`` may hold its laser records already
+    (host NumPy structured array or a device tensor of raw bytes)."""
+
+    id: int
+    key: Tuple
+    context: object
+    steps: int
+    arrival: float = 0.0
+    table: object = None
+    # filled in by the engine
+    admitted: float = float("nan")
+    finished: float = float("nan")
+    slot: int = -1
+    last: Optional[dict] = None
+    modes: object = None
+    surface: object = None
+
+    @property
+    def latency(self) -> float:
+        return self.finished - self.arrival
+
+
+def latency_percentiles(requests: Sequence[Request], qs=(50, 99)) -> Dict[str, float]:
+    lat = np.array([r.latency for r in requests if np.isfinite(r.finished)])
+    if lat.size == 0:
+        return {f"p{q}": float("nan") for q in qs}
+    return {f"p{q}": float(np.percentile(lat, q)) for q in qs}
+
+
+@dataclass
+class _Stats:
+    chunks: int = 0
+    steps_launched: int = 0
+    h2d_bytes: int = 0
+    d2h_bytes: int = 0
+    admitted: int = 0
+    completed: int = 0
+    slot_steps: int = 0
+    busy_s: float = 0.0
+    launches: int = 0
+    extra: dict = field(default_factory=dict)
+
+
+class ServingEngine:
+    """Continuous batching of solve requests on one device.
+
+    ``classes`` maps a class key to a template context (its laser path is not
+    used) and ``weights`` gives each class's expected share of the device
+    memory demand (default: equal). Slot capacity: starting from one slot per
+    class, slots go to the class with the lowest slots/weight ratio while the
+    batch workspace fits in ``memory_fraction`` of the free device memory and
+    stays within ``max_slots`` slots per class.
+    """
+
+    def __init__(self, classes: Dict[Tuple, object], precision: str = "mixed",
+                 memory_fraction: float = 0.5, max_slots: int = 16,
+                 weights: Optional[Dict[Tuple, float]] = None, slots: Optional[Dict[Tuple, int]] = None,
+                 keep_modes: bool = False, max_chunk: int = 64,
+                 batch_factory: Optional[Callable] = None, mem_info: Optional[Callable] = None,
+                 slot_bytes: Optional[Callable] = None):
+        if batch_factory is None:
+            import torch
+            if not torch.cuda.is_available():
+                raise RuntimeError("ServingEngine needs a CUDA device (no CPU fallback)")
+            batch_factory = BatchSolver
+            mem_info = mem_info or torch.cuda.mem_get_info
+        slot_bytes = slot_bytes or (lambda ctx: BatchSolver.workspace_bytes_for([ctx], precision))
+        self.precision = precision
+        self.keys = list(classes)
+        self.templates = {k: classes[k] for k in self.keys}
+        self.keep_modes = keep_modes
+        self.max_chunk = int(max_chunk)
+        free, total = mem_info()
+        self.budget = int(memory_fraction * free)
+        per_slot = {k: int(slot_bytes(self.templates[k])) for k in self.keys}
+        if slots is None:
+            w = {k: float((weights or {}).get(k, 1.0)) for k in self.keys}
+            slots = {k: 1 for k in self.keys}
+            used = sum(per_slot[k] for k in self.keys)
+            if used > self.budget:
+                raise RuntimeError(f"one slot per class needs {used} bytes; the budget is {self.budget}")
+            while True:
+                cand = [k for k in self.keys if slots[k] < max_slots and used + per_slot[k] <= self.budget]
+                if not cand:
+                    break
+                k = min(cand, key=lambda c: slots[c] / max(w[c], 1e-12))
+                slots[k] += 1
+                used += per_slot[k]
+        self.slots_per_class = dict(slots)
+        contexts, self.slot_key = [], []
+        for k in self.keys:
+            for _ in range(slots[k]):
+                contexts.append(self.templates[k])
+                self.slot_key.append(k)
+        self.batch = batch_factory(contexts, precision)
+        self.free = {k: deque(i for i, kk in enumerate(self.slot_key) if kk == k) for k in self.keys}
+        self.stats = _Stats()
+        self._active: Dict[int, Request] = {}
+        self._done_steps: Dict[int, int] = {}
+        self.memory = {"free_bytes_at_start": int(free), "total_bytes": int(total),
+                       "budget_bytes": self.budget, "workspace_bytes": self.batch.workspace_bytes,
+                       "slots": len(contexts)}
+
+    # ---- one request -------------------------------------------------------
+    def _device_table(self, req: Request):
+        if req.table is None:
+            ctx = req.context
+            req.table = laser_table(ctx.laser_path, 0.0, float(ctx.num.dt), req.steps)
+        if isinstance(req.table, np.ndarray):
+            self.stats.h2d_bytes += req.table.nbytes
+            return self.batch.upload_table(req.table)
+        return req.table
+
+    def _admit(self, req: Request, now: float) -> bool:
+        fr = self.free[req.key]
+        if not fr:
+            return False
+        slot = fr.popleft()
+        table = self._device_table(req)
+        self.batch.start(slot, req.steps, table=table, record=False)
+        req.slot, req.admitted = slot, now
+        req._dev_table = table  # keep the device table alive while the slot runs
+        self.stats.admitted += 1
+        return True
+
+    def _complete(self, req: Request, info, now: float) -> None:
+        req.finished = now
+        o = info.last
+        req.last = {"T_surface_max": o.T_surface_max, "P_laser": o.P_laser, "n_evap_iter": o.n_iter,
+                    "picard_converged": bool(o.converged), "picard_rel_err": o.picard_rel_err}
+        req.surface = self.batch.fetch(req.slot, "surface")  # device -> host
+        self.stats.d2h_bytes += req.surface.nbytes
+        if self.keep_modes:
+            req.modes = self.batch.snapshot(req.slot, "modes")  # device copy
+        req._dev_table = None
+        self.free[req.key].append(req.slot)
+        self.stats.completed += 1
+
+    # ---- the loop ------------------------------------------------------------
+    def run(self, requests: Sequence[Request], realtime: bool = True, max_steps: Optional[int] = None,
+            clock: Callable[[], float] = time.perf_counter) -> List[Request]:
+        """Serve ``requests`` (``arrival`` in seconds from the start of this call).
+
+        ``realtime``: a request becomes visible at its arrival time on the host
+        clock; otherwise all are queued at once (a saturated queue).
+        ``max_steps``: stop after this many batched steps (one batched step
+        advances every active request by one time step); requests still in
+        flight then stay in their slots until :meth:`reset`. Returns the
+        requests with their timings and results filled in.
+        """
+        pending = deque(sorted(requests, key=lambda r: r.arrival))
+        if not realtime:
+            for r in pending:
+                r.arrival = 0.0
+        queue: List[Request] = []
+        active, done_steps = self._active, self._done_steps
+        pre, per_it, post = self.batch.launch_counts()
+        launched = 0
+        t0 = clock()
+        step_time = None  # running estimate of one batched step (s)
+        while (pending or queue or active) and (max_steps is None or launched < max_steps):
+            now = clock() - t0
+            while pending and pending[0].arrival <= now:
+                queue.append(pending.popleft())
+            if queue:
+                still = []
+                for r in queue:
+                    if self._admit(r, now):
+                        active[r.slot] = r
+                        done_steps[r.slot] = 0
+                    else:
+                        still.append(r)
+                queue = still
+            if not active:
+                if pending:
+                    wait = pending[0].arrival - (clock() - t0)
+                    if wait > 0:
+                        time.sleep(min(wait, 0.01))
+                continue
+            chunk = min(r.steps - done_steps[s] for s, r in active.items())
+            if pending and step_time:
+                until = pending[0].arrival - now
+                chunk = min(chunk, max(1, int(until / step_time)))
+            if max_steps is not None:
+                chunk = min(chunk, max_steps - launched)
+            chunk = max(1, min(chunk, self.max_chunk))
+            c0 = clock()
+            self.batch.step(chunk)
+            info = self.batch.status()  # synchronises
+            dt_chunk = clock() - c0
+            self.stats.busy_s += dt_chunk
+            self.stats.d2h_bytes += len(info) * 64
+            est = dt_chunk / chunk
+            step_time = est if step_time is None else 0.7 * step_time + 0.3 * est
+            launched += chunk
+            self.stats.chunks += 1
+            self.stats.steps_launched += chunk
+            self.stats.launches += 1 + chunk * (pre + post + per_it)
+            now = clock() - t0
+            iters = 1
+            for s in list(active):
+                st = info[s]
+                self.stats.slot_steps += st.step - done_steps[s]
+                iters = max(iters, st.last.n_iter)
+                done_steps[s] = st.step
+                if not st.active:
+                    self._complete(active.pop(s), st, now)
+            # Picard iterations beyond the first (upper bound: the largest count
+            # of the last step, for every step of the chunk)
+            self.stats.launches += chunk * per_it * (iters - 1)
+        self.batch.synchronize()
+        return list(requests)
+
+    def reset(self) -> None:
+        """Stop every request in flight and free its slot."""
+        for s, r in list(self._active.items()):
+            self.batch.stop(s)
+            self.free[r.key].append(s)
+            r._dev_table = None
+        self._active.clear()
+        self._done_steps.clear()
+        self.batch.synchronize()
+
+    @property
+    def in_flight(self) -> int:
+        return len(self._active)
+
+    def close(self) -> None:
+        self.batch.close()
+
+
+def requests_from_stream(stream: Sequence[dict], contexts: Dict[Tuple, object]) -> List[Request]:
+    """Requests of a ``workloads.serving_stream`` list; ``contexts`` holds one
+    template context per mesh (built with ``SimulationContext.from_dict``)."""
+    out = []
+    for r in stream:
+        ctx = copy.copy(contexts[r["mesh"]])
+        ctx.laser_path = r["path"]
+        out.append(Request(id=r["id"], key=r["mesh"], context=ctx, steps=r["steps"], arrival=r["arrival"]))
+    return out

@@ -23,8 +23,14 @@ scalars) plus the :class:`LaserPath` that drives it. All randomness comes from
   Nx from {64, 96, 128, 192, 256}, Ny = Nx/2, Nz from {16, 32, 64}, the
   64 x 32 x 16 cell size kept (Lx = 2 mm * Nx/64, Ly = Lx/2, Lz = 0.5 mm);
   straight-track physics with P ~ U[150, 400] W, v ~ U[0.5, 2] m/s and
-  absorptivity ~ U[0.3, 0.4] per instance; Picard with the reference defaults
+  absorptivity ~ U[0.3, 0.45] per instance; Picard with the reference defaults
   (omega 0.1, tol 1e-4, cap 30).
+* ``serving_stream``: a seeded Poisson stream of laser-scan solve requests
+  (mean rate 200 requests/s): grids Nx from {64, 128, 256, 512}, Ny = Nx/2,
+  Nz from {16, 32, 64} on the fixed 2 x 1 x 0.5 mm cuboid; straight-track
+  physics (one forcing pass per step); 200-2000 steps of 5 us; P ~ U[150, 400]
+  W and v ~ U[0.5, 2] m/s per request on a bidirectional raster (1.5 mm lines,
+  50 um hatch) that keeps the beam on the part.
 """
 from __future__ import annotations
 
@@ -35,7 +41,7 @@ import numpy as np
 from .laser import RasterPath, StraightTrack
 
 __all__ = ["MATERIAL_316L", "straight_track", "nonlinear_raster", "precision_track",
-           "uneven_batch", "scaled"]
+           "uneven_batch", "serving_stream", "serving_config", "scaled"]
 
 MATERIAL_316L = {
     "name": "316L", "rho": 7900.0, "k": 20.0, "Cp": 500.0, "L_f": 0.0,
@@ -94,7 +100,7 @@ def precision_track(seed=0, nx=256, ny=128, nz=64, steps=500, dt=5e-6):
                           x0=0.5e-3, speed=speed, power=power)
 
 
-def uneven_batch(n=64, seed=0, steps=200, dt=5e-6, nx_choices=(64, 96, 128, 192, 256),
+def uneven_batch(n=64, seed=0, steps=300, dt=5e-6, nx_choices=(64, 96, 128, 192, 256),
                  nz_choices=(16, 32, 64)):
     """``n`` seeded ``(cfg, path)`` pairs of uneven grid size (see the module docstring)."""
     rng = np.random.default_rng(seed)
@@ -105,12 +111,41 @@ def uneven_batch(n=64, seed=0, steps=200, dt=5e-6, nx_choices=(64, 96, 128, 192,
         ny = nx // 2
         power = float(rng.uniform(150.0, 400.0))
         speed = float(rng.uniform(0.5, 2.0))
-        absorptivity = float(rng.uniform(0.3, 0.4))
+        absorptivity = float(rng.uniform(0.3, 0.45))
         size = (2e-3 * nx / 64, 1e-3 * ny / 32, 0.5e-3)
         cfg, _ = straight_track(nx, ny, nz, steps=steps, dt=dt, size=size, power=power,
                                 absorptivity=absorptivity)
         cfg["simulation"].update({"max_picard_iter": 30, "picard_omega": 0.1, "picard_tol": 1e-4})
         out.append((cfg, StraightTrack(0.3e-3, size[1] / 2.0, speed, 0.0, power)))
+    return out
+
+
+def serving_config(nx, ny, nz, dt=5e-6):
+    """Config of one serving request class: straight-track physics, fixed cuboid."""
+    cfg, _ = straight_track(nx, ny, nz, steps=1, dt=dt)
+    return cfg
+
+
+def serving_stream(n_requests=200, seed=0, rate=200.0, dt=5e-6, nx_choices=(64, 128, 256, 512),
+                   nz_choices=(16, 32, 64), steps_range=(200, 2000)):
+    """Seeded Poisson request stream: a list of dicts with ``arrival`` (s from the
+    stream start), ``mesh`` (nx, ny, nz), ``steps``, ``cfg`` and ``path``."""
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    for i in range(n_requests):
+        t += float(rng.exponential(1.0 / rate))
+        nx = int(rng.choice(nx_choices))
+        nz = int(rng.choice(nz_choices))
+        ny = nx // 2
+        steps = int(rng.integers(steps_range[0], steps_range[1] + 1))
+        power = float(rng.uniform(150.0, 400.0))
+        speed = float(rng.uniform(0.5, 2.0))
+        length, hatch = 1.5e-3, 50e-6
+        n_lines = max(1, min(14, int(np.ceil(steps * dt * speed / length))))
+        path = RasterPath(0.25e-3, 0.2e-3, length, hatch, n_lines, speed, power)
+        out.append({"id": i, "arrival": t, "mesh": (nx, ny, nz), "steps": steps,
+                    "cfg": serving_config(nx, ny, nz, dt), "path": path})
     return out
 
 
