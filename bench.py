@@ -591,7 +591,7 @@ def run_serving(args, rank, world, local_rank):
         "e2e": {"value": e_steps / (t[1] * 1e-3), "unit": "timesteps/s",
                 "h2d_bytes_per_step": e_h2d / K, "d2h_bytes_per_step": e_d2h / K,
                 "api": "ServingEngine.run (host laser tables in, result surfaces out)"},
-        "roofline": {"kernel": "kb_commit_modes (volume pass, fused next-step face sums)", "bound": "hbm",
+        "roofline": {"kernel": "kb_volume<float,4,commit> (modal commit fused with the next step face sums)", "bound": "hbm",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_source": peak_kind, "traffic": NCU_TRAFFIC_BYTES,
                      "algorithmic_bytes_per_launch": vp_bytes, "modes": modes},

@@ -336,42 +336,6 @@ kb_face_begin(BView v, double* q_las, double* q_net, const double* q_evold, doub
   if (threadIdx.x == 0) part_las[b] = sum;
 }
 
-// Face sums of the propagated modes: Zt = sum Ct K a, Yt = sum (K a) KK Ct and
-// partials of sum (K a)^2 -- for the first step of a slot; later steps get
-// them from the previous commit (kb_commit_modes). K is read from the K array
-// or, when K is null, formed from the separable decay tables.
-template <class R>
-__global__ void __launch_bounds__(BT)
-kb_pass1(BView v, const R* a, const R* K, const R* KK, double* Zt, double* Yt, double* part_n1) {
-  __shared__ double sh[2 * (BT / 32)];
-  const int b = blockIdx.x;
-  const int s = v.blk_slot[b];
-  const BSlot& sl = v.slot[s];
-  if (!v.st[s].active || v.st[s].pass1_ready) return;
-  const int i = (b - sl.blk0) * BT + threadIdx.x;
-  double n1 = 0.0, dummy = 0.0;
-  if (i < sl.S) {
-    double zt = 0.0, yt = 0.0;
-    const double* ct = v.Ct + sl.zoff;
-    const double* ez = v.E + sl.eoff + sl.nx + sl.ny;
-    const double exy = K ? 0.0 : v.E[sl.eoff + i % sl.nx] * v.E[sl.eoff + sl.nx + i / sl.nx];
-#pragma unroll 4
-    for (int p = 0; p < sl.nz; ++p) {
-      const long long j = sl.vol + (long long)p * sl.S + i;
-      const double kv = K ? (double)K[j] : exy * ez[p];
-      const double ak = (double)a[j] * kv;
-      const double kk = (double)KK[j];
-      zt = fma(ct[p], ak, zt);
-      yt = fma(ak * kk, ct[p], yt);
-      n1 = fma(ak, ak, n1);
-    }
-    Zt[sl.face + i] = zt;
-    Yt[sl.face + i] = yt;
-  }
-  block_sum2<BT>(n1, dummy, sh);
-  if (threadIdx.x == 0) part_n1[b] = n1;
-}
-
 // A = Zt + W_tt sigma (top-surface input of the current iterate).
 __global__ void __launch_bounds__(BT)
 kb_assemble(BView v, const double* Zt, const double* Wtt, const double* sigma, double* A) {
@@ -923,48 +887,96 @@ kb_relax(BView v, const double* Zt, const double* Yt, const double* Wtt, const d
   }
 }
 
-// a = K a + KK Ct sigma (commit of the modes), fused with the next step's
-// face sums: with the new modes in registers, Zt = sum Ct K a, Yt = sum (K a)
-// KK Ct and the partials of sum (K a)^2 come for free, so the next step skips
-// kb_pass1 and the volume is read once per step. The sums use the stored
-// (type R) value of a, exactly as kb_pass1 would read it back.
-template <class R>
-__global__ void __launch_bounds__(BT)
-kb_commit_modes(BView v, R* a, const R* K, const R* KK, const double* sigma, double* Zt, double* Yt,
-                double* part_n1) {
-  __shared__ double sh[2 * (BT / 32)];
+// ---- volume passes ----------------------------------------------------------
+// One thread per VEC consecutive (y, x) columns of a slot, looping over z;
+// a, K and KK move as VEC-wide vectors (the slot's volume offset and face
+// size are multiples of VEC). K comes from the K array or, when K is null,
+// from the separable decay tables.
+//   COMMIT = false: face sums of the propagated modes for the first step of a
+//     slot: Zt = sum Ct K a, Yt = sum (K a) KK Ct, partials of sum (K a)^2
+//     (later steps get them from the previous commit).
+//   COMMIT = true: a = K a + KK Ct sigma (the modal commit), fused with the
+//     same face sums for the next step, formed from the stored (type R) value
+//     of a exactly as the first variant reads it back: the volume is read
+//     once per step.
+template <class R, int VEC>
+struct VecOf { using T = R; };
+template <>
+struct VecOf<float, 4> { using T = float4; };
+template <>
+struct VecOf<double, 2> { using T = double2; };
+
+template <class R, int VEC>
+__device__ __forceinline__ void vload(const R* p, R (&o)[VEC]) {
+  using T = typename VecOf<R, VEC>::T;
+  const T t = *reinterpret_cast<const T*>(p);
+#pragma unroll
+  for (int c = 0; c < VEC; ++c) o[c] = reinterpret_cast<const R*>(&t)[c];
+}
+template <class R, int VEC>
+__device__ __forceinline__ void vstore(R* p, const R (&o)[VEC]) {
+  using T = typename VecOf<R, VEC>::T;
+  T t;
+#pragma unroll
+  for (int c = 0; c < VEC; ++c) reinterpret_cast<R*>(&t)[c] = o[c];
+  *reinterpret_cast<T*>(p) = t;
+}
+
+template <class R, int VEC, bool COMMIT>
+__global__ void __launch_bounds__(BT / VEC)
+kb_volume(BView v, R* a, const R* K, const R* KK, const double* sigma, double* Zt, double* Yt,
+          double* part_n1) {
+  constexpr int NT = BT / VEC;
+  __shared__ double sh[2 * (NT / 32)];
   const int b = blockIdx.x;
   const int s = v.blk_slot[b];
   const BSlot& sl = v.slot[s];
   BState& st = v.st[s];
-  if (!st.active) return;
-  const int i = (b - sl.blk0) * BT + threadIdx.x;
+  if (!st.active || (!COMMIT && st.pass1_ready)) return;
+  const int i0 = (b - sl.blk0) * BT + VEC * threadIdx.x;
   double n1 = 0.0, dummy = 0.0;
-  if (i < sl.S) {
-    const double sg = sigma[sl.face + i];
+  if (i0 < sl.S) {
     const double* ct = v.Ct + sl.zoff;
     const double* ez = v.E + sl.eoff + sl.nx + sl.ny;
-    const double exy = K ? 0.0 : v.E[sl.eoff + i % sl.nx] * v.E[sl.eoff + sl.nx + i / sl.nx];
-    double zt = 0.0, yt = 0.0;
-#pragma unroll 4
-    for (int p = 0; p < sl.nz; ++p) {
-      const long long j = sl.vol + (long long)p * sl.S + i;
-      const double kv = K ? (double)K[j] : exy * ez[p];
-      const double kk = (double)KK[j];
-      const R an = (R)((double)a[j] * kv + kk * (ct[p] * sg));
-      a[j] = an;
-      const double ak = (double)an * kv;
-      zt = fma(ct[p], ak, zt);
-      yt = fma(ak * kk, ct[p], yt);
-      n1 = fma(ak, ak, n1);
+    double sg[VEC], exy[VEC], zt[VEC], yt[VEC];
+#pragma unroll
+    for (int c = 0; c < VEC; ++c) {
+      const int i = i0 + c;
+      sg[c] = COMMIT ? sigma[sl.face + i] : 0.0;
+      exy[c] = K ? 0.0 : v.E[sl.eoff + i % sl.nx] * v.E[sl.eoff + sl.nx + i / sl.nx];
+      zt[c] = 0.0;
+      yt[c] = 0.0;
     }
-    Zt[sl.face + i] = zt;
-    Yt[sl.face + i] = yt;
+#pragma unroll 2
+    for (int p = 0; p < sl.nz; ++p) {
+      const long long j0 = sl.vol + (long long)p * sl.S + i0;
+      R av[VEC], kkv[VEC], kvv[VEC];
+      vload<R, VEC>(a + j0, av);
+      vload<R, VEC>(KK + j0, kkv);
+      if (K) vload<R, VEC>(K + j0, kvv);
+      const double cp = ct[p];
+#pragma unroll
+      for (int c = 0; c < VEC; ++c) {
+        const double kv = K ? (double)kvv[c] : exy[c] * ez[p];
+        const double kk = (double)kkv[c];
+        if (COMMIT) av[c] = (R)((double)av[c] * kv + kk * (cp * sg[c]));
+        const double ak = (double)av[c] * kv;
+        zt[c] = fma(cp, ak, zt[c]);
+        yt[c] = fma(ak * kk, cp, yt[c]);
+        n1 = fma(ak, ak, n1);
+      }
+      if (COMMIT) vstore<R, VEC>(a + j0, av);
+    }
+#pragma unroll
+    for (int c = 0; c < VEC; ++c) {
+      Zt[sl.face + i0 + c] = zt[c];
+      Yt[sl.face + i0 + c] = yt[c];
+    }
   }
-  block_sum2<BT>(n1, dummy, sh);
+  block_sum2<NT>(n1, dummy, sh);
   if (threadIdx.x == 0) {
     part_n1[b] = n1;
-    st.pass1_ready = 1;
+    if (COMMIT) st.pass1_ready = 1;
   }
 }
 
@@ -1039,6 +1051,7 @@ struct sgh_batch {
   size_t o_xah = 0, o_xal = 0, o_xqh = 0, o_xql = 0, o_mph = 0, o_mpl = 0;  // operand planes (mixed)
   size_t xa_bytes = 0, mp_bytes = 0;
   int f2_stages = 0, f2_bop = 0, f2_smem = 0;  // fused face transform: ring stages, operand bytes, smem
+  int vec = 1;  // columns per thread of the volume passes
   std::vector<std::pair<int, long long>> mplane_list;  // (N, byte offset of the forward plane)
   size_t ws_need = 0;
   char* ws = nullptr;
@@ -1109,6 +1122,18 @@ void face2d(sgh_batch* B, cudaStream_t s, const double* in, const EpiF& ef, cons
   }
 }
 
+// One volume pass over all slots at the batch's vector width.
+template <class R, bool COMMIT>
+void launch_volume(sgh_batch* B, cudaStream_t s, R* a, const R* K, const R* KK) {
+  const BView v = B->view();
+  double *sg = B->d(B->o_sigma), *zt = B->d(B->o_Zt), *yt = B->d(B->o_Yt), *pn = B->d(B->o_pn1);
+  constexpr int VW = sizeof(R) == 4 ? 4 : 2;
+  if (B->vec == VW)
+    kb_volume<R, VW, COMMIT><<<B->tot_blk, BT / VW, 0, s>>>(v, a, K, KK, sg, zt, yt, pn);
+  else
+    kb_volume<R, 1, COMMIT><<<B->tot_blk, BT, 0, s>>>(v, a, K, KK, sg, zt, yt, pn);
+}
+
 template <class R>
 void enqueue_pre(sgh_batch* B, cudaStream_t s, cudaGraphConditionalHandle h, int in_graph) {
   const BView v = B->view();
@@ -1117,7 +1142,7 @@ void enqueue_pre(sgh_batch* B, cudaStream_t s, cudaGraphConditionalHandle h, int
   R* KK = reinterpret_cast<R*>(B->ws + B->o_KK);
   kb_begin<<<1, CT, 0, s>>>(v, h, in_graph);
   kb_face_begin<<<B->tot_blk, BT, 0, s>>>(v, B->d(B->o_qlas), B->d(B->o_qnet), B->d(B->o_qevold), B->d(B->o_plas));
-  kb_pass1<R><<<B->tot_blk, BT, 0, s>>>(v, a, K, KK, B->d(B->o_Zt), B->d(B->o_Yt), B->d(B->o_pn1));
+  launch_volume<R, false>(B, s, a, K, KK);
   g_blaunch += 3;
   // initial guess: sigma = dct_scale * DCT2(q_las - shift(q_evap_old))
   face2d<false, false, F2_STORE>(B, s, B->d(B->o_qnet), EB_Store{B->d(B->o_sigma), 1},
@@ -1150,8 +1175,7 @@ void enqueue_post(sgh_batch* B, cudaStream_t s, cudaGraphConditionalHandle h, in
   face2d<true, false, F2_COMMIT>(B, s, B->d(B->o_A),
                                  EB_CommitSurface{B->d(B->o_Tsurf), B->d(B->o_qev), B->d(B->o_qevold)},
                                  F2Args{B->d(B->o_Tsurf), B->d(B->o_qevold), B->d(B->o_qev), 0}, B->d(B->o_ptile));
-  kb_commit_modes<R><<<B->tot_blk, BT, 0, s>>>(v, a, K, KK, B->d(B->o_sigma), B->d(B->o_Zt), B->d(B->o_Yt),
-                                               B->d(B->o_pn1));
+  launch_volume<R, true>(B, s, a, K, KK);
   kb_commit<<<1, CT, 0, s>>>(v, B->d(B->o_plas), B->d(B->o_ptile),
                              B->precision == SGH_PRECISION_MIXED ? 1 : 0, h, in_graph);
   g_blaunch += 2;
@@ -1286,7 +1310,7 @@ int sgh_batch_create(const sgh_config* cfgs, int32_t n, int32_t precision, sgh_b
     sl.V = (long long)sl.S * c.nz;
     sl.max_iter = c.max_iter;
     sl.cell_integrated = c.cell_integrated;
-    sl.vol = B->tot_vol;
+    sl.vol = (B->tot_vol + 3) / 4 * 4;  // aligned for the vector volume passes
     sl.face = B->tot_face;
     sl.zoff = B->tot_z;
     sl.eoff = (int)B->tot_e;
@@ -1331,7 +1355,7 @@ int sgh_batch_create(const sgh_config* cfgs, int32_t n, int32_t precision, sgh_b
     sl.tol = c.tol;
     sl.k = c.k; sl.rho = c.rho; sl.cp = c.cp;
     B->slots.push_back(sl);
-    B->tot_vol += sl.V;
+    B->tot_vol = sl.vol + sl.V;
     B->tot_face += sl.S;
     B->tot_z += c.nz;
     B->tot_e += c.nx + c.ny + c.nz;
@@ -1345,6 +1369,12 @@ int sgh_batch_create(const sgh_config* cfgs, int32_t n, int32_t precision, sgh_b
     B->tile_slot.insert(B->tile_slot.end(), sl.ntile, i);
     B->vblk_slot.insert(B->vblk_slot.end(), sl.nvblk, i);
     B->utile_slot.insert(B->utile_slot.end(), sl.nutile, i);
+  }
+  {
+    const int vw = precision == SGH_PRECISION_MIXED ? 4 : 2;
+    bool ok = true;
+    for (const BSlot& sl : B->slots) ok = ok && (sl.S % vw == 0);
+    B->vec = ok ? vw : 1;
   }
   LayoutB L;
   const size_t F8 = sizeof(double) * (size_t)B->tot_face;
@@ -1596,16 +1626,11 @@ int sgh_batch_error(const sgh_batch* B, int32_t* err, void* stream) {
 int sgh_batch_volume_pass(sgh_batch* B, void* stream) {
   if (!B || !B->bound) return bfail(SGH_ERR_STATE, "batch is not bound");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  const BView v = B->view();
   if (B->precision == SGH_PRECISION_MIXED)
-    kb_commit_modes<float><<<B->tot_blk, BT, 0, s>>>(v, reinterpret_cast<float*>(B->ws + B->o_a), nullptr,
-                                                     reinterpret_cast<const float*>(B->ws + B->o_KK),
-                                                     B->d(B->o_sigma), B->d(B->o_Zt), B->d(B->o_Yt),
-                                                     B->d(B->o_pn1));
+    launch_volume<float, true>(B, s, reinterpret_cast<float*>(B->ws + B->o_a), nullptr,
+                               reinterpret_cast<const float*>(B->ws + B->o_KK));
   else
-    kb_commit_modes<double><<<B->tot_blk, BT, 0, s>>>(v, B->d(B->o_a), B->d(B->o_K), B->d(B->o_KK),
-                                                      B->d(B->o_sigma), B->d(B->o_Zt), B->d(B->o_Yt),
-                                                      B->d(B->o_pn1));
+    launch_volume<double, true>(B, s, B->d(B->o_a), B->d(B->o_K), B->d(B->o_KK));
   SGB_CK(cudaGetLastError());
   return SGH_OK;
 }
