@@ -61,10 +61,14 @@ import numpy as np  # noqa: E402
 
 METRIC = "timesteps/s"
 L2_FLUSH_BYTES = 256 << 20
-# dram__bytes_read.sum + dram__bytes_write.sum per launch of the dominant kernel
-# (k_axis on the 128x64x32 transform) from an ncu capture of this workload;
-# None until that capture exists.
-NCU_TRAFFIC_BYTES = None
+# dram__bytes_read.sum + dram__bytes_write.sum of the dominant kernel from ncu
+# captures (ncu --set full, one launch): the serving volume pass on the 24-slot
+# case (2 slots per class) moved 449.26 MB for 38,993,920 modes; the benchmark's
+# 192-slot case has the same class mix, so traffic scales with the modes.
+NCU_VOLUME_TRAFFIC_PER_MODE = 449.26e6 / 38993920
+# the raster workload's dominant kernel (k_axis) was captured on the same
+# 128x64x32 case: 2.14 MB for one contiguous-axis pass (field resident in L2)
+NCU_TRAFFIC_BYTES = 2.14e6
 
 
 def _peaks():
@@ -593,7 +597,8 @@ def run_serving(args, rank, world, local_rank):
                 "api": "ServingEngine.run (host laser tables in, result surfaces out)"},
         "roofline": {"kernel": "kb_volume<float,4,commit> (modal commit fused with the next step face sums)", "bound": "hbm",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "peak_source": peak_kind, "traffic": NCU_TRAFFIC_BYTES,
+                     "peak_source": peak_kind, "traffic": NCU_VOLUME_TRAFFIC_PER_MODE * modes,
+                     "traffic_note": "ncu capture of the 24-slot case scaled by active modes",
                      "algorithmic_bytes_per_launch": vp_bytes, "modes": modes},
     }
     if world == 1 and not args.no_cpu_baseline:
@@ -602,6 +607,48 @@ def run_serving(args, rank, world, local_rank):
                                 "sample": f"{n} timesteps over the first {touched} requests of the stream "
                                           f"(<= {args.cpu_steps_per_request} steps each, {el:.1f} s)"}
     return line
+
+
+def run_profile(args):
+    """--profile: launch the step kernels one by one (no graph) for ncu.
+
+    ``serving-step``: the serving engine as in the benchmark (slots per class
+    from --max-slots), every slot filled from the saturated stream, then
+    --steps eager batched steps and three volume passes. ``raster-step``: the
+    nonlinear raster workload through ``B200SpectralSolver.step(eager=True)``
+    for --warmup + --steps steps. Prints one line; no timing."""
+    import copy
+
+    import torch
+    if args.profile == "serving-step":
+        from spectral_galerkin_heat_b200 import workloads
+        from spectral_galerkin_heat_b200.serving import ServingEngine
+        sat = workloads.serving_stream(n_requests=args.requests, seed=0)
+        meshes = sorted({r["mesh"] for r in sat})
+        templates = {m: _context(workloads.serving_config(*m), None) for m in meshes}
+        weights = {m: float(sum(r["steps"] for r in sat if r["mesh"] == m)) + 1.0 for m in meshes}
+        eng = ServingEngine(templates, precision=args.precision, memory_fraction=args.memory_fraction,
+                            max_slots=args.max_slots, weights=weights)
+        eng.run(_serving_requests(sat, templates), realtime=False, max_steps=1)
+        for _ in range(args.steps):
+            eng.batch.step_eager()
+        for _ in range(3):
+            eng.batch.volume_pass()
+        torch.cuda.synchronize()
+        print(json.dumps({"profile": args.profile, "precision": args.precision, "slots": eng.memory["slots"],
+                          "active_modes": eng.batch.active_modes(), "workspace_gb": eng.batch.workspace_bytes / 1e9}))
+        eng.close()
+    elif args.profile == "raster-step":
+        from spectral_galerkin_heat_b200 import B200SpectralSolver
+        cfg, path, desc = _workload("raster", seed=0)
+        s = B200SpectralSolver(None, _context(cfg, path))
+        s.initialize()
+        dt = s.context.num.dt
+        for i in range(args.warmup + args.steps):
+            s.step(i * dt, dt, eager=True)
+        torch.cuda.synchronize()
+        print(json.dumps({"profile": args.profile, "steps": args.warmup + args.steps}))
+        s.finalize()
 
 
 def main():
@@ -621,11 +668,17 @@ def main():
     ap.add_argument("--plain-steps", type=int, default=300)
     ap.add_argument("--cpu-steps-per-request", type=int, default=20)
     ap.add_argument("--accuracy-steps", type=int, default=100)
+    ap.add_argument("--profile", choices=["serving-step", "raster-step"], default=None,
+                    help="launch the step kernels one by one for a profiler and exit (no timing)")
+    ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed", help="--profile serving-step")
     args = ap.parse_args()
     if args.steps is None:
-        args.steps = 1000 if args.workload == "serving" else 200
+        args.steps = 2 if args.profile else (1000 if args.workload == "serving" else 200)
     if args.warmup < 3:
         args.warmup = 3
+    if args.profile:
+        run_profile(args)
+        return
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

@@ -26,7 +26,7 @@
 extern "C" {
 #endif
 
-#define SGH_ABI_VERSION 1
+#define SGH_ABI_VERSION 2
 
 /* status codes */
 #define SGH_OK               0
@@ -95,6 +95,12 @@ typedef struct {
   /* Picard controls (solvers/spectral.py:107-123)                          */
   int32_t max_iter;
   double omega, tol;
+  /* Tile policy of the FP64 axis passes of a plan (no reference
+   * counterpart): a pass uses 2 x 4 register tiles when that grid has at
+   * least this many CTAs, else 1 x 1 tiles; 0 = the built-in default (132).
+   * Chosen per (nx, ny, nz) by the autotuner (autotune.py). Batches ignore it. */
+  int32_t axis_min_ctas;
+  int32_t pad1;
 } sgh_config;
 
 /* Laser state of one step (LaserState, core/laser.py:150-167). */

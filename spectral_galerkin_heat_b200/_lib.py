@@ -60,6 +60,7 @@ class SghConfig(C.Structure):
         ("order", C.c_double), ("area_factor", C.c_double),
         ("cell_integrated", C.c_int32), ("max_iter", C.c_int32),
         ("omega", C.c_double), ("tol", C.c_double),
+        ("axis_min_ctas", C.c_int32), ("pad1", C.c_int32),
     ]
 
 
@@ -144,7 +145,7 @@ def lib() -> C.CDLL:
             fn = getattr(L, name)
             fn.argtypes = args
             fn.restype = res
-        if L.sgh_abi_version() != 1:
+        if L.sgh_abi_version() != 2:
             raise RuntimeError("libsgh_b200.so ABI version mismatch; rebuild it")
         _lib = L
         return L

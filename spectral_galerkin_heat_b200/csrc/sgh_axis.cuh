@@ -186,6 +186,19 @@ struct AxisShape {
   dim3 grid;
 };
 constexpr int AX_MIN_CTAS = 132;
+// Tile policy of the calling thread: 2 x 4 tiles when that grid has at least
+// this many CTAs. Set for the duration of a plan's call by AxisPolicy, so the
+// captured graph, eager launches and the partial-buffer sizing agree.
+inline thread_local int g_axis_min_ctas = AX_MIN_CTAS;
+
+struct AxisPolicy {
+  int saved;
+  explicit AxisPolicy(int min_ctas) : saved(g_axis_min_ctas) {
+    g_axis_min_ctas = min_ctas > 0 ? min_ctas : AX_MIN_CTAS;
+  }
+  ~AxisPolicy() { g_axis_min_ctas = saved; }
+};
+
 inline AxisShape axis_shape(int Nout, int A, int B) {
   const int ncol = A * B;
   auto grid_of = [&](int ti, int tj) {
@@ -194,7 +207,7 @@ inline AxisShape axis_shape(int Nout, int A, int B) {
     return dim3((ncol + tc - 1) / tc, (Nout + tk - 1) / tk);
   };
   const dim3 g = grid_of(2, 4);
-  if ((long)g.x * g.y >= AX_MIN_CTAS) return {true, g};
+  if ((long)g.x * g.y >= g_axis_min_ctas) return {true, g};
   return {false, grid_of(1, 1)};
 }
 

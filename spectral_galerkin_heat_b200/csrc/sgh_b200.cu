@@ -957,6 +957,8 @@ int sgh_plan_create(const sgh_config* cfg, sgh_plan** out) {
   if (!cfg || !out) return fail(SGH_ERR_INVALID, "null argument");
   *out = nullptr;
   const sgh_config& c = *cfg;
+  if (c.axis_min_ctas < 0) return fail(SGH_ERR_INVALID, "axis_min_ctas must be >= 0");
+  AxisPolicy policy(c.axis_min_ctas);
   if (c.nx < 2 || c.ny < 2 || c.nz < 2) return fail(SGH_ERR_INVALID, "every axis needs at least 2 modes");
   if (c.nx > 4096 || c.ny > 4096 || c.nz > 4096) return fail(SGH_ERR_INVALID, "an axis exceeds 4096 modes");
   if ((long long)c.nx * c.ny * c.nz > (1LL << 28)) return fail(SGH_ERR_INVALID, "grid exceeds 2^28 modes");
@@ -1114,6 +1116,7 @@ int sgh_plan_workspace_bytes(const sgh_plan* p, uint64_t* bytes) {
 }
 
 int sgh_plan_bind(sgh_plan* p, void* workspace, uint64_t bytes, void* stream) {
+  AxisPolicy policy(p ? p->cfg.axis_min_ctas : 0);
   if (!p || !workspace) return fail(SGH_ERR_INVALID, "null argument");
   if (p->bound) return fail(SGH_ERR_STATE, "plan is already bound");
   if (bytes < p->ws_need) return fail(SGH_ERR_WORKSPACE, "workspace is smaller than sgh_plan_workspace_bytes()");
@@ -1205,6 +1208,7 @@ int sgh_step(sgh_plan* p, const sgh_laser* laser, sgh_step_out* out, void* strea
 }
 
 int sgh_step_eager(sgh_plan* p, const sgh_laser* laser, sgh_step_out* out, void* stream) {
+  AxisPolicy policy(p ? p->cfg.axis_min_ctas : 0);
   if (!p || !laser) return fail(SGH_ERR_INVALID, "null argument");
   if (!p->bound) return fail(SGH_ERR_STATE, "plan is not bound");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -1238,6 +1242,7 @@ int sgh_run(sgh_plan* p, const sgh_laser* lasers_dev, int32_t n_steps, sgh_step_
 }
 
 int sgh_dct3d(sgh_plan* p, int32_t kind, const double* in, double* out, void* stream) {
+  AxisPolicy policy(p ? p->cfg.axis_min_ctas : 0);
   if (!p || !in || !out) return fail(SGH_ERR_INVALID, "null argument");
   if (!p->bound) return fail(SGH_ERR_STATE, "plan is not bound");
   if (kind != 2 && kind != 3) return fail(SGH_ERR_INVALID, "kind must be 2 (DCT_II) or 3 (IDCT_II)");
@@ -1248,6 +1253,7 @@ int sgh_dct3d(sgh_plan* p, int32_t kind, const double* in, double* out, void* st
 }
 
 int sgh_surface_temperature(sgh_plan* p, const double* modes, int32_t top, double* out, void* stream) {
+  AxisPolicy policy(p ? p->cfg.axis_min_ctas : 0);
   if (!p || !modes || !out) return fail(SGH_ERR_INVALID, "null argument");
   if (!p->bound) return fail(SGH_ERR_STATE, "plan is not bound");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -1257,6 +1263,7 @@ int sgh_surface_temperature(sgh_plan* p, const double* modes, int32_t top, doubl
 }
 
 int sgh_project_volume(sgh_plan* p, const double* field, double* modes, void* stream) {
+  AxisPolicy policy(p ? p->cfg.axis_min_ctas : 0);
   if (!p || !field || !modes) return fail(SGH_ERR_INVALID, "null argument");
   if (!p->bound) return fail(SGH_ERR_STATE, "plan is not bound");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -1266,6 +1273,7 @@ int sgh_project_volume(sgh_plan* p, const double* field, double* modes, void* st
 }
 
 int sgh_reconstruct_volume(sgh_plan* p, const double* modes, double* field, void* stream) {
+  AxisPolicy policy(p ? p->cfg.axis_min_ctas : 0);
   if (!p || !field || !modes) return fail(SGH_ERR_INVALID, "null argument");
   if (!p->bound) return fail(SGH_ERR_STATE, "plan is not bound");
   cudaStream_t s = static_cast<cudaStream_t>(stream);

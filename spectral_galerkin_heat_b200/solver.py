@@ -160,9 +160,11 @@ class B200SpectralSolver(HeatSolver):
     """Spectral-Galerkin heat step on one B200 (FP64, grid mode)."""
 
     def __init__(self, backend=None, context=None, *, mixing_omega=None,
-                 convergence_tol=None, max_picard_iter=None, device=None):
+                 convergence_tol=None, max_picard_iter=None, device=None, axis_min_ctas=None):
         self.backend = backend
         self.context = context
+        # tile policy of the axis passes: explicit, else the autotuner's table, else default
+        self.axis_min_ctas = axis_min_ctas
         self.state: Optional[B200State] = None
         self.device = device
         self._req = (mixing_omega, convergence_tol, max_picard_iter)
@@ -208,6 +210,12 @@ class B200SpectralSolver(HeatSolver):
         self._resolve_picard_params(np.float64)
         cfg = make_config(ctx, float(self.mixing_omega), float(self.convergence_tol),
                           self.max_picard_iter)
+        policy = self.axis_min_ctas
+        if policy is None:
+            from .autotune import lookup
+            policy = lookup(cfg)
+        cfg.axis_min_ctas = int(policy or 0)
+        self.tile_policy = int(cfg.axis_min_ctas)
         plan = C.c_void_p()
         _lib.check("sgh_plan_create", L.sgh_plan_create(C.byref(cfg), C.byref(plan)))
         self._plan = plan

@@ -28,7 +28,7 @@ def test_library_loads_and_exports_every_declared_symbol():
     for n in names:
         assert hasattr(L, n), n
     assert sorted(_lib.EXPORTED) == names
-    assert L.sgh_abi_version() == 1
+    assert L.sgh_abi_version() == 2
 
 
 def test_struct_layout_matches_header():

@@ -1,0 +1,25 @@
+"""Autotuner table: keys by shape and step form, lookup order (user table
+first, then the shipped one), and the plan config picks the entry up."""
+import json
+
+from spectral_galerkin_heat_b200 import autotune
+from spectral_galerkin_heat_b200._lib import SghConfig
+
+
+def _cfg(nx, ny, nz, latent=False):
+    c = SghConfig()
+    c.nx, c.ny, c.nz = nx, ny, nz
+    c.L_f = 2.7e5 if latent else 0.0
+    return c
+
+
+def test_keys_and_lookup(tmp_path, monkeypatch):
+    assert autotune.key_of(_cfg(128, 64, 32)) == "128x64x32:face"
+    assert autotune.key_of(_cfg(128, 64, 32, latent=True)) == "128x64x32:volume"
+    table = tmp_path / "t.json"
+    table.write_text(json.dumps({"entries": {"40x20x6:face": {"axis_min_ctas": 264}}}))
+    monkeypatch.setenv("SGH_TUNE_TABLE", str(table))
+    autotune._cache.clear()
+    assert autotune.lookup(_cfg(40, 20, 6)) == 264
+    assert autotune.lookup(_cfg(40, 20, 7)) is None  # in neither table: built-in default
+    autotune._cache.clear()

@@ -1,0 +1,22 @@
+"""The precision study's report on a small well-conditioned case: the mixed
+form stays within 1e-4 relative L2 of FP64 with the same melt pool, and the
+perturbed FP64 run stays within rounding of FP64."""
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def test_precision_report_small_case():
+    from spectral_galerkin_heat_b200 import workloads
+    from spectral_galerkin_heat_b200.precision import run_study
+    cfg, path = workloads.precision_track(seed=0, nx=64, ny=32, nz=16, steps=60)
+    rep = run_study(cfg, path, [10, 40], picard={"max_picard_iter": 300, "picard_omega": 0.1,
+                                                 "picard_tol": 1e-8})
+    for r in rep:
+        assert r["tensor_core_error"] == 0
+        assert r["mixed"]["rel_l2"] < 1e-4
+        assert r["fp64_perturbed"]["rel_l2"] < 1e-9
+        assert abs(r["mixed"]["peak_T_err_K"]) < 1.0
+    last = rep[-1]["mixed"]
+    assert last["melt_pool"]["cells"] > 0
+    assert all(abs(v) <= 62.5e-6 + 1e-12 for v in last["melt_pool_err_m"].values())  # one cell
