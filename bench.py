@@ -71,6 +71,18 @@ NCU_VOLUME_TRAFFIC_PER_MODE = 449.26e6 / 38993920
 NCU_TRAFFIC_BYTES = 2.14e6
 
 
+def reduce_over_ranks(times_ms, counts, device="cpu"):
+    """Replicas' aggregate: max over ranks of each timed interval (ms) and sum
+    over ranks of each work count. The only cross-rank traffic of a run."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x) for x in times_ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    c = torch.tensor([float(x) for x in counts], dtype=torch.float64, device=device)
+    dist.all_reduce(c, op=dist.ReduceOp.SUM)
+    return [float(x) for x in t], [int(round(float(x))) for x in c]
+
+
 def _peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -353,9 +365,7 @@ def run_b200(args, rank, world, local_rank):
     t_max = dev_ms
     e2e_max = e2e_ms
     if world > 1:
-        t = torch.tensor([dev_ms, e2e_ms], dtype=torch.float64, device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        t_max, e2e_max = float(t[0]), float(t[1])
+        (t_max, e2e_max), _ = reduce_over_ranks([dev_ms, e2e_ms], [K], device=dev)
     if rank != 0:
         return None
     total_steps = K * world
@@ -551,12 +561,7 @@ def run_serving(args, rank, world, local_rank):
 
     t = [v_ms, e_ms]
     if world > 1:
-        tt = torch.tensor(t, dtype=torch.float64, device="cuda")
-        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-        t = [float(x) for x in tt]
-        st = torch.tensor([v_steps, e_steps], dtype=torch.float64, device="cuda")
-        torch.distributed.all_reduce(st)
-        v_steps, e_steps = int(st[0]), int(st[1])
+        t, (v_steps, e_steps) = reduce_over_ranks(t, [v_steps, e_steps], device="cuda")
     if rank != 0:
         return None
     value = v_steps / (t[0] * 1e-3)
