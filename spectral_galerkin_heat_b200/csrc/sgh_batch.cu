@@ -307,31 +307,57 @@ __global__ void __launch_bounds__(CT) kb_begin(BView v, cudaGraphConditionalHand
 // (solvers/spectral.py:273-306).
 __global__ void __launch_bounds__(BT)
 kb_face_begin(BView v, double* q_las, double* q_net, const double* q_evold, double* part_las) {
+  // RB elements per block (RPT per thread, consecutive across the block per
+  // round); the four shift taps of U elements are gathered before their use
   __shared__ double sh[2 * (BT / 32)];
   const int b = blockIdx.x;
-  const int s = v.blk_slot[b];
+  const int s = v.rblk_slot[b];
   const BSlot& sl = v.slot[s];
   const BState& st = v.st[s];
   if (!st.active) return;
-  const int i = (b - sl.blk0) * BT + threadIdx.x;
-  double sum = 0.0, dummy = 0.0, qn = 0.0;
-  if (i < sl.S) {
-    const int nx = sl.nx, ny = sl.ny;
-    const int y = i / nx, x = i - y * nx;
-    const double xc = ((double)x + 0.5) * sl.dx, yc = ((double)y + 0.5) * sl.dy;
-    const double q = laser_flux(sl, st.I0, st.laser.x, st.laser.y, xc, yc);
-    const double* f = q_evold + sl.face;
-    q_las[sl.face + i] = q;
-    sum = q;
-    const ShiftTap ty = shift_tap(y, ny, st.shift_y);
-    const ShiftTap tx = shift_tap(x, nx, st.shift_x);
-    double val = ty.w0 * (tx.w0 * f[ty.i0 * nx + tx.i0] + tx.w1 * f[ty.i0 * nx + tx.i1]) +
-                 ty.w1 * (tx.w0 * f[ty.i1 * nx + tx.i0] + tx.w1 * f[ty.i1 * nx + tx.i1]);
-    if (!(ty.in && tx.in)) val = 0.0;
-    qn = q - val;
-    q_net[sl.face + i] = qn;
+  const int nx = sl.nx, ny = sl.ny;
+  const double* f = q_evold + sl.face;
+  const double I0 = st.I0, lx = st.laser.x, ly = st.laser.y, sx = st.shift_x, sy = st.shift_y;
+  const int i0 = (b - sl.rblk0) * RB;
+  double sum = 0.0, dummy = 0.0;
+  constexpr int U = 4;
+#pragma unroll 1
+  for (int u0 = 0; u0 < RPT; u0 += U) {
+    double g[U][4], wy0[U], wy1[U], wx0[U], wx1[U];
+    bool ok[U], in[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int i = i0 + (u0 + u) * BT + threadIdx.x;
+      ok[u] = i < sl.S;
+      const int y = ok[u] ? i / nx : 0, x = ok[u] ? i - y * nx : 0;
+      const ShiftTap ty = shift_tap(y, ny, sy);
+      const ShiftTap tx = shift_tap(x, nx, sx);
+      in[u] = ok[u] && ty.in && tx.in;
+      wy0[u] = ty.w0; wy1[u] = ty.w1; wx0[u] = tx.w0; wx1[u] = tx.w1;
+      g[u][0] = in[u] ? f[ty.i0 * nx + tx.i0] : 0.0;
+      g[u][1] = in[u] ? f[ty.i0 * nx + tx.i1] : 0.0;
+      g[u][2] = in[u] ? f[ty.i1 * nx + tx.i0] : 0.0;
+      g[u][3] = in[u] ? f[ty.i1 * nx + tx.i1] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int i = i0 + (u0 + u) * BT + threadIdx.x;
+      double qn = 0.0;
+      if (ok[u]) {
+        const int y = i / nx, x = i - y * nx;
+        const double xc = ((double)x + 0.5) * sl.dx, yc = ((double)y + 0.5) * sl.dy;
+        const double q = laser_flux(sl, I0, lx, ly, xc, yc);
+        q_las[sl.face + i] = q;
+        sum += q;
+        // the bilinear shift (spectral_cpu_kernels.py:328-371), zero outside the grid
+        double val = wy0[u] * (wx0[u] * g[u][0] + wx1[u] * g[u][1]) + wy1[u] * (wx0[u] * g[u][2] + wx1[u] * g[u][3]);
+        if (!in[u]) val = 0.0;
+        qn = q - val;
+        q_net[sl.face + i] = qn;
+      }
+      plane_put_block(v.xq_hi, v.xq_lo, sl, i, qn, ok[u]);
+    }
   }
-  plane_put_block(v.xq_hi, v.xq_lo, sl, i, qn, i < sl.S);
   block_sum2<BT>(sum, dummy, sh);
   if (threadIdx.x == 0) part_las[b] = sum;
 }
@@ -448,7 +474,9 @@ inline __host__ __device__ int face_utiles(int nx, int) { return (nx + f2::NB - 
 //   F2_STORE    FP64 face array (x dct_scale if scaled)
 //   F2_TOPFLUX  T_s -> evaporation -> q_evap (FP64), q_net -> xq plane
 //   F2_COMMIT   T_temp, its block max, q_evap_old <- q_evap
-enum { F2_STORE = 0, F2_TOPFLUX = 1, F2_COMMIT = 2 };
+//   F2_SIGMA    sigma = dct_scale * G (FP64) and the first iterate's
+//               A = Zt + W_tt sigma into the xa plane (replaces kb_assemble)
+enum { F2_STORE = 0, F2_TOPFLUX = 1, F2_COMMIT = 2, F2_SIGMA = 3 };
 
 struct FaceParams {  // per-slot constants held in registers by the epilogues
   long long face, xa;
@@ -457,10 +485,11 @@ struct FaceParams {  // per-slot constants held in registers by the epilogues
 };
 
 struct F2Args {
-  double* out;        // F2_STORE target, F2_TOPFLUX q_evap, F2_COMMIT T_surf
+  double* out;        // F2_STORE target, F2_TOPFLUX q_evap, F2_COMMIT T_surf, F2_SIGMA sigma
   double* out2;       // F2_COMMIT q_evap_old
-  const double* in2;  // F2_TOPFLUX q_las, F2_COMMIT q_evap
+  const double* in2;  // F2_TOPFLUX q_las, F2_COMMIT q_evap, F2_SIGMA Zt
   int scaled;
+  const double* in3;  // F2_SIGMA W_tt
 };
 
 // FP32 tile of 128 x NB results in shared memory: element (m, n) at
@@ -497,7 +526,11 @@ kb_face2d(BView v, F2Args args, double* part_tile, int n_stages, int bop_max) {
   uint32_t* tslot = reinterpret_cast<uint32_t*>(done + f2::MAX_STAGES);
   volatile int* okflag = reinterpret_cast<volatile int*>(tslot + 1);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const uint32_t ncols = nrt > 1 ? 128u : 64u;
+  // TMEM: the x-pass keeps hi*hi, hi*lo and lo*hi in three accumulators
+  // (columns 0, 64, 128: three independent MMA chains); y-pass row tile rt
+  // keeps hi*hi and hi*lo + lo*hi in two (columns 128 rt and 128 rt + 64).
+  // The parts are summed when read out.
+  constexpr uint32_t ncols = 256u;
   const char* p_hi = reinterpret_cast<const char*>(INV ? v.xa_hi : v.xq_hi) + fp.xa;
   const char* p_lo = reinterpret_cast<const char*>(INV ? v.xa_lo : v.xq_lo) + fp.xa;
   const long long mxo = (INV ? sl.mpx_inv : sl.mpx) + (long long)ct * nkx * CBN;  // NB-row chunks
@@ -534,18 +567,18 @@ kb_face2d(BView v, F2Args args, double* part_tile, int n_stages, int bop_max) {
     if (!wait_full(g)) return false;
     tc_fence_after();
     const uint32_t s0 = smem_u32(ring + (g % S) * f2::STAGE);
-    uint32_t ah, al, bh, bl, d;
+    uint32_t ah, al, bh, bl, d0, d1, d2;
     int kc;
     if (g < n_x) {
       kc = g % nkx;
       ah = s0; al = s0 + CA; bh = s0 + 2 * CA; bl = s0 + 2 * CA + CBN;
-      d = tmem;
+      d0 = tmem; d1 = tmem + NB; d2 = tmem + 2 * NB;
     } else {
       const int gy = g - n_x, rt = gy / nky;
       kc = gy - rt * nky;
       ah = s0; al = s0 + CA;
       bh = smem_u32(bop + kc * 2 * CBN); bl = bh + CBN;
-      d = tmem + (uint32_t)(rt * NB);
+      d0 = tmem + (uint32_t)(rt * 2 * NB); d1 = d0 + NB; d2 = d1;
     }
 #pragma unroll
     for (int k = 0; k < KC / 16; ++k) {
@@ -554,9 +587,10 @@ kb_face2d(BView v, F2Args args, double* part_tile, int n_stages, int bop_max) {
       const uint64_t dal = smem_desc(al + oa, (TM / 8) * 128, 128);
       const uint64_t dbh = smem_desc(bh + ob, (NB / 8) * 128, 128);
       const uint64_t dbl = smem_desc(bl + ob, (NB / 8) * 128, 128);
-      mma_bf16(d, dah, dbh, idesc, (kc > 0 || k > 0) ? 1u : 0u);
-      mma_bf16(d, dah, dbl, idesc, 1u);
-      mma_bf16(d, dal, dbh, idesc, 1u);
+      const uint32_t acc = (kc > 0 || k > 0) ? 1u : 0u;
+      mma_bf16(d0, dah, dbh, idesc, acc);
+      mma_bf16(d1, dah, dbl, idesc, acc);
+      mma_bf16(d2, dal, dbh, idesc, (d2 == d1) ? 1u : acc);
     }
     mma_commit(&done[g % S]);
     committed = g + 1;
@@ -611,8 +645,13 @@ kb_face2d(BView v, F2Args args, double* part_tile, int n_stages, int bop_max) {
       const int c = half * 32;
 #pragma unroll
       for (int cc = 0; cc < 32; cc += 16) {
-        float x16[16];
-        tmem_ld16(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(c + cc), x16);
+        float x16[16], p1[16], p2[16];
+        const uint32_t ta = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(c + cc);
+        tmem_ld16(ta, x16);
+        tmem_ld16(ta + NB, p1);
+        tmem_ld16(ta + 2 * NB, p2);
+#pragma unroll
+        for (int i = 0; i < 16; ++i) x16[i] = x16[i] + (p1[i] + p2[i]);
 #pragma unroll
         for (int i = 0; i < 16; ++i) {
           __nv_bfloat16 h, l;
@@ -653,10 +692,12 @@ kb_face2d(BView v, F2Args args, double* part_tile, int n_stages, int bop_max) {
       const int c = half * 32;
 #pragma unroll
       for (int cc = 0; cc < 32; cc += 16) {
-        float x16[16];
-        tmem_ld16(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(rt * NB + c + cc), x16);
+        float x16[16], p1[16];
+        const uint32_t ta = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(rt * 2 * NB + c + cc);
+        tmem_ld16(ta, x16);
+        tmem_ld16(ta + NB, p1);
 #pragma unroll
-        for (int i = 0; i < 16; ++i) tile[m * NB + ((c + cc + i) ^ (m & 31))] = x16[i];
+        for (int i = 0; i < 16; ++i) tile[m * NB + ((c + cc + i) ^ (m & 31))] = x16[i] + p1[i];
       }
     }
     __syncthreads();
@@ -687,6 +728,34 @@ kb_face2d(BView v, F2Args args, double* part_tile, int n_stages, int bop_max) {
               qn = ql[u] - qe;
             }
             plane_put8_warp(v.xq_hi + fp.xa / 2, v.xq_lo + fp.xa / 2, y, x, nkx, qn, in);
+          }
+        }
+      } else if (KIND == F2_SIGMA) {
+        constexpr int U = 8;
+        for (int it0 = 0; it0 < ITEMS; it0 += U) {
+          double zt[U], wt[U];
+#pragma unroll
+          for (int u = 0; u < U; ++u) {
+            const int e = tid + (it0 + u) * f2::THREADS;
+            const int y = r0 + e / NB, x = c0 + e % NB;
+            const bool in = y < ny && x < nx;
+            const long long j = fp.face + (long long)y * nx + x;
+            zt[u] = in ? __ldg(args.in2 + j) : 0.0;
+            wt[u] = in ? __ldg(args.in3 + j) : 0.0;
+          }
+#pragma unroll
+          for (int u = 0; u < U; ++u) {
+            const int e = tid + (it0 + u) * f2::THREADS;
+            const int m = e / NB, n = e % NB;
+            const int y = r0 + m, x = c0 + n;
+            const bool in = y < ny && x < nx;
+            double a = 0.0;
+            if (in) {
+              const double sg = fp.dct_scale * (double)f2_tile(tile, m, n);
+              args.out[fp.face + (long long)y * nx + x] = sg;
+              a = zt[u] + wt[u] * sg;
+            }
+            plane_put8_warp(v.xa_hi + fp.xa / 2, v.xa_lo + fp.xa / 2, y, x, nkx, a, in);
           }
         }
       } else {
@@ -994,7 +1063,7 @@ kb_commit(BView v, const double* part_las, const double* part_tile, int umma_til
     if (!st.active) continue;
     const BSlot& sl = v.slot[s];
     double p = 0.0, m = -INFINITY;
-    for (int b = sl.blk0 + lane; b < sl.blk0 + sl.nblk; b += 32) p += part_las[b];
+    for (int b = sl.rblk0 + lane; b < sl.rblk0 + sl.nrblk; b += 32) p += part_las[b];
     const int t0 = umma_tiles ? sl.utile0 : sl.tile0, nt = umma_tiles ? sl.nutile : sl.ntile;
     for (int b = t0 + lane; b < t0 + nt; b += 32) m = fmax(m, part_tile[b]);
 #pragma unroll
@@ -1141,14 +1210,19 @@ void enqueue_pre(sgh_batch* B, cudaStream_t s, cudaGraphConditionalHandle h, int
   R* K = B->precision == SGH_PRECISION_MIXED ? nullptr : reinterpret_cast<R*>(B->ws + B->o_K);
   R* KK = reinterpret_cast<R*>(B->ws + B->o_KK);
   kb_begin<<<1, CT, 0, s>>>(v, h, in_graph);
-  kb_face_begin<<<B->tot_blk, BT, 0, s>>>(v, B->d(B->o_qlas), B->d(B->o_qnet), B->d(B->o_qevold), B->d(B->o_plas));
+  kb_face_begin<<<B->tot_rblk, BT, 0, s>>>(v, B->d(B->o_qlas), B->d(B->o_qnet), B->d(B->o_qevold), B->d(B->o_plas));
   launch_volume<R, false>(B, s, a, K, KK);
   g_blaunch += 3;
-  // initial guess: sigma = dct_scale * DCT2(q_las - shift(q_evap_old))
-  face2d<false, false, F2_STORE>(B, s, B->d(B->o_qnet), EB_Store{B->d(B->o_sigma), 1},
-                                 F2Args{B->d(B->o_sigma), nullptr, nullptr, 1}, nullptr);
-  kb_assemble<<<B->tot_blk, BT, 0, s>>>(v, B->d(B->o_Zt), B->d(B->o_Wtt), B->d(B->o_sigma), B->d(B->o_A));
-  g_blaunch += 1;
+  // initial guess: sigma = dct_scale * DCT2(q_las - shift(q_evap_old)), then A = Zt + W_tt sigma
+  if (B->precision == SGH_PRECISION_MIXED) {
+    face2d<false, false, F2_SIGMA>(B, s, B->d(B->o_qnet), EB_Store{B->d(B->o_sigma), 1},
+                                   F2Args{B->d(B->o_sigma), nullptr, B->d(B->o_Zt), 1, B->d(B->o_Wtt)}, nullptr);
+  } else {
+    face2d<false, false, F2_STORE>(B, s, B->d(B->o_qnet), EB_Store{B->d(B->o_sigma), 1},
+                                   F2Args{B->d(B->o_sigma), nullptr, nullptr, 1, nullptr}, nullptr);
+    kb_assemble<<<B->tot_blk, BT, 0, s>>>(v, B->d(B->o_Zt), B->d(B->o_Wtt), B->d(B->o_sigma), B->d(B->o_A));
+    g_blaunch += 1;
+  }
 }
 
 void enqueue_picard(sgh_batch* B, cudaStream_t s, cudaGraphConditionalHandle h, int in_graph) {
