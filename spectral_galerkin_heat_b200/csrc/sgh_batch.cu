@@ -99,12 +99,9 @@ struct BView {
   const int* tile_slot;   // slot of each FP64 face-transform tile
   const int* vblk_slot;   // slot of each volume block
   const int* utile_slot;  // slot of each tensor-core column block
-  __nv_bfloat16* xa_hi;   // operand planes (mixed precision; null otherwise):
-  __nv_bfloat16* xa_lo;   //   xa = A = Zt + W_tt sigma, input of the inverse transform
-  __nv_bfloat16* xq_hi;   //   xq = q_net, input of the forward transform
-  __nv_bfloat16* xq_lo;
-  const char* mp_hi;      // DCT matrix planes
-  const char* mp_lo;
+  char* xa;               // operand pair planes (mixed precision; null otherwise):
+  char* xq;               //   xa = A = Zt + W_tt sigma (inverse transform input), xq = q_net (forward)
+  const char* mp;         // DCT matrix pair planes
   const double* mats;
   const double* Ct;
   const double* E;        // 1-D decay tables exp(-alpha dt k_i^2) per slot and axis
@@ -114,8 +111,7 @@ struct BView {
 // Eight lanes 8g..8g+7 of a warp hold consecutive k = k0..k0+7 (k0 % 8 == 0)
 // of one plane row; lane 8g writes the group's 16-byte hi and lo rows. Call
 // from all 32 lanes; `store` is read on lane 8g only.
-__device__ __forceinline__ void plane_put8_warp(__nv_bfloat16* hi, __nv_bfloat16* lo, int r, int k0, int nkc,
-                                                double val, bool store) {
+__device__ __forceinline__ void plane_put8_warp(char* plane, int r, int k0, int nkc, double val, bool store) {
   __nv_bfloat16 h, l;
   umma::split_bf16(val, h, l);
   const uint32_t hv = __bfloat16_as_ushort(h), lv = __bfloat16_as_ushort(l);
@@ -125,25 +121,24 @@ __device__ __forceinline__ void plane_put8_warp(__nv_bfloat16* hi, __nv_bfloat16
   const uint32_t h2 = __shfl_down_sync(0xffffffffu, hp, 4), l2 = __shfl_down_sync(0xffffffffu, lp, 4);
   const uint32_t h3 = __shfl_down_sync(0xffffffffu, hp, 6), l3 = __shfl_down_sync(0xffffffffu, lp, 6);
   if ((threadIdx.x & 7) == 0 && store) {
-    const size_t o = umma::plane_off(r, k0, nkc);
-    *reinterpret_cast<uint4*>(reinterpret_cast<char*>(hi) + o) = make_uint4(hp, h1, h2, h3);
-    *reinterpret_cast<uint4*>(reinterpret_cast<char*>(lo) + o) = make_uint4(lp, l1, l2, l3);
+    const size_t o = umma::pair_off<umma::TM>(r, k0, nkc);
+    *reinterpret_cast<uint4*>(plane + o) = make_uint4(hp, h1, h2, h3);
+    *reinterpret_cast<uint4*>(plane + o + umma::pair_chunk_bytes<umma::TM>()) = make_uint4(lp, l1, l2, l3);
   }
 }
 
-// Face-plane element i = y * nx + x of slot sl (hi/lo: the xa or xq arena,
-// null in FP64 batches), written by a whole block of consecutive i (one slot
-// per block). When nx % 8 == 0 every aligned group of 8 lanes is 8
+// Face-plane element i = y * nx + x of slot sl (plane: the xa or xq pair
+// arena, null in FP64 batches), written by a whole block of consecutive i (one
+// slot per block). When nx % 8 == 0 every aligned group of 8 lanes is 8
 // consecutive x of one row and goes out as one 16-byte store per part.
-__device__ __forceinline__ void plane_put_block(__nv_bfloat16* hi, __nv_bfloat16* lo, const BSlot& sl, int i,
-                                                double val, bool valid) {
-  if (!hi) return;
+__device__ __forceinline__ void plane_put_block(char* plane, const BSlot& sl, int i, double val, bool valid) {
+  if (!plane) return;
   const int nkc = (sl.nx + umma::KC - 1) / umma::KC;
   const int y = i / sl.nx, x = i - (i / sl.nx) * sl.nx;
   if ((sl.nx & 7) == 0)
-    plane_put8_warp(hi + sl.xa / 2, lo + sl.xa / 2, y, x, nkc, valid ? val : 0.0, valid);
+    plane_put8_warp(plane + sl.xa, y, x, nkc, valid ? val : 0.0, valid);
   else if (valid)
-    umma::plane_put(hi + sl.xa / 2, lo + sl.xa / 2, y, x, nkc, val);
+    umma::pair_put<umma::TM>(plane + sl.xa, y, x, nkc, val);
 }
 
 // ---------------------------------------------------------------------------
@@ -161,15 +156,15 @@ __global__ void kb_dct_matrix(int N, double* M) {
   M[(size_t)N * N + n * N + k] = v;
 }
 
-// BF16 hi/lo planes of an N x N DCT matrix (inv: its transpose), rows = the
+// BF16 hi/lo pair planes of an N x N DCT matrix (inv: its transpose), rows = the
 // output index, k = the contracted index, in R-row chunks.
 template <int R>
-__global__ void kb_matrix_planes(int N, const double* M, int inv, __nv_bfloat16* hi, __nv_bfloat16* lo) {
+__global__ void kb_matrix_planes(int N, const double* M, int inv, char* plane) {
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= N * N) return;
   const int r = e / N, k = e - r * N;
   const double val = inv ? M[(size_t)k * N + r] : M[(size_t)r * N + k];
-  umma::plane_put_r<R>(hi, lo, r, k, (N + umma::KC - 1) / umma::KC, val);
+  umma::pair_put<R>(plane, r, k, (N + umma::KC - 1) / umma::KC, val);
 }
 
 // K, KK of every slot exactly as precompute_K_KK (physics/spectral_state.py:374-421),
@@ -355,7 +350,7 @@ kb_face_begin(BView v, double* q_las, double* q_net, const double* q_evold, doub
         qn = q - val;
         q_net[sl.face + i] = qn;
       }
-      plane_put_block(v.xq_hi, v.xq_lo, sl, i, qn, ok[u]);
+      plane_put_block(v.xq, sl, i, qn, ok[u]);
     }
   }
   block_sum2<BT>(sum, dummy, sh);
@@ -375,7 +370,7 @@ kb_assemble(BView v, const double* Zt, const double* Wtt, const double* sigma, d
     a = Zt[sl.face + i] + Wtt[sl.face + i] * sigma[sl.face + i];
     A[sl.face + i] = a;
   }
-  plane_put_block(v.xa_hi, v.xa_lo, sl, i, a, i < sl.S);
+  plane_put_block(v.xa, sl, i, a, i < sl.S);
 }
 
 // ---- batched face transform: one 2 x 4-register-tile block per tile ------
@@ -446,7 +441,7 @@ __global__ void __launch_bounds__(AX_THREADS) kb_face_axis(BView v, const double
 // streams every operand chunk (the x-pass P and Mx chunks, then the My
 // chunks) through one ring of bulk-copy stages and issues the MMAs, so the My
 // copies are in flight while the x-pass result is converted. Operands are
-// split-BF16 (three MMAs per k-step, FP32 accumulation), as in tile_planes.
+// split-BF16 (three MMAs per k-step, FP32 accumulation), as in tile_bf16x3.
 // Shared memory is sized for two CTAs per SM, so one CTA's epilogue overlaps
 // another's copies and MMAs.
 namespace f2 {
@@ -531,10 +526,9 @@ kb_face2d(BView v, F2Args args, double* part_tile, int n_stages, int bop_max) {
   // keeps hi*hi and hi*lo + lo*hi in two (columns 128 rt and 128 rt + 64).
   // The parts are summed when read out.
   constexpr uint32_t ncols = 256u;
-  const char* p_hi = reinterpret_cast<const char*>(INV ? v.xa_hi : v.xq_hi) + fp.xa;
-  const char* p_lo = reinterpret_cast<const char*>(INV ? v.xa_lo : v.xq_lo) + fp.xa;
-  const long long mxo = (INV ? sl.mpx_inv : sl.mpx) + (long long)ct * nkx * CBN;  // NB-row chunks
-  const long long myo = INV ? sl.mpy_inv : sl.mpy;                                // 128-row chunks
+  const char* pp = (INV ? v.xa : v.xq) + fp.xa;                                        // pair chunks of 2 CA
+  const long long mxo = (INV ? sl.mpx_inv : sl.mpx) + (long long)ct * nkx * 2 * CBN;  // NB-row pairs
+  const long long myo = INV ? sl.mpy_inv : sl.mpy;                                     // 128-row pairs
   const uint32_t idesc = idesc_bf16_f32(TM, NB);
 
   uint32_t tmem = 0;  // tensor-memory base, set once allocated
@@ -545,20 +539,15 @@ kb_face2d(BView v, F2Args args, double* part_tile, int n_stages, int bop_max) {
   auto load = [&](int g) {
     char* stg = ring + (g % S) * f2::STAGE;
     uint64_t* bar = &full[g % S];
-    if (g < n_x) {
+    if (g < n_x) {  // one copy of P's hi + lo chunk, one of Mx's
       const int rt = g / nkx, kc = g - rt * nkx;
-      const size_t po = (size_t)(rt * nkx + kc) * CA;
       mbar_expect_tx(bar, 2 * CA + 2 * CBN);
-      bulk_g2s(stg, p_hi + po, CA, bar);
-      bulk_g2s(stg + CA, p_lo + po, CA, bar);
-      bulk_g2s(stg + 2 * CA, v.mp_hi + mxo + (size_t)kc * CBN, CBN, bar);
-      bulk_g2s(stg + 2 * CA + CBN, v.mp_lo + mxo + (size_t)kc * CBN, CBN, bar);
-    } else {
+      bulk_g2s(stg, pp + (size_t)(rt * nkx + kc) * 2 * CA, 2 * CA, bar);
+      bulk_g2s(stg + 2 * CA, v.mp + mxo + (size_t)kc * 2 * CBN, 2 * CBN, bar);
+    } else {        // one copy of My's hi + lo chunk
       const int gy = g - n_x, rt = gy / nky, kc = gy - rt * nky;
-      const size_t mo = (size_t)myo + (size_t)(rt * nky + kc) * CA;
       mbar_expect_tx(bar, 2 * CA);
-      bulk_g2s(stg, v.mp_hi + mo, CA, bar);
-      bulk_g2s(stg + CA, v.mp_lo + mo, CA, bar);
+      bulk_g2s(stg, v.mp + (size_t)myo + (size_t)(rt * nky + kc) * 2 * CA, 2 * CA, bar);
     }
   };
   auto wait_full = [&](int g) { return mbar_wait_bounded(&full[g % S], (uint32_t)((g / S) & 1)); };
@@ -727,7 +716,7 @@ kb_face2d(BView v, F2Args args, double* part_tile, int n_stages, int bop_max) {
               args.out[fp.face + (long long)y * nx + x] = qe;
               qn = ql[u] - qe;
             }
-            plane_put8_warp(v.xq_hi + fp.xa / 2, v.xq_lo + fp.xa / 2, y, x, nkx, qn, in);
+            plane_put8_warp(v.xq + fp.xa, y, x, nkx, qn, in);
           }
         }
       } else if (KIND == F2_SIGMA) {
@@ -755,7 +744,7 @@ kb_face2d(BView v, F2Args args, double* part_tile, int n_stages, int bop_max) {
               args.out[fp.face + (long long)y * nx + x] = sg;
               a = zt[u] + wt[u] * sg;
             }
-            plane_put8_warp(v.xa_hi + fp.xa / 2, v.xa_lo + fp.xa / 2, y, x, nkx, a, in);
+            plane_put8_warp(v.xa + fp.xa, y, x, nkx, a, in);
           }
         }
       } else {
@@ -896,7 +885,7 @@ kb_relax(BView v, const double* Zt, const double* Yt, const double* Wtt, const d
         sigma[face + i] = ns;
         if (A) A[face + i] = a;
       }
-      plane_put_block(v.xa_hi, v.xa_lo, sl, i, ok ? a : 0.0, ok);
+      plane_put_block(v.xa, sl, i, ok ? a : 0.0, ok);
     }
   }
   block_sum2<BT>(r2, o2, sh);
@@ -1117,7 +1106,7 @@ struct sgh_batch {
   long long tot_e = 0;
   size_t o_qlas, o_qnet, o_qev, o_qevold, o_Stop, o_f1, o_sigma, o_A, o_Tsurf, o_Zt, o_Yt, o_Wtt, o_Qtt;
   size_t o_plas, o_pn1, o_prelax, o_ptile;
-  size_t o_xah = 0, o_xal = 0, o_xqh = 0, o_xql = 0, o_mph = 0, o_mpl = 0;  // operand planes (mixed)
+  size_t o_xa = 0, o_xq = 0, o_mp = 0;  // operand pair planes (mixed)
   size_t xa_bytes = 0, mp_bytes = 0;
   int f2_stages = 0, f2_bop = 0, f2_smem = 0;  // fused face transform: ring stages, operand bytes, smem
   int vec = 1;  // columns per thread of the volume passes
@@ -1143,12 +1132,9 @@ struct sgh_batch {
     v.vblk_slot = reinterpret_cast<const int*>(ws + o_vblk);
     v.utile_slot = reinterpret_cast<const int*>(ws + o_utile);
     const bool mixed = precision == SGH_PRECISION_MIXED;
-    v.xa_hi = mixed ? reinterpret_cast<__nv_bfloat16*>(ws + o_xah) : nullptr;
-    v.xa_lo = mixed ? reinterpret_cast<__nv_bfloat16*>(ws + o_xal) : nullptr;
-    v.xq_hi = mixed ? reinterpret_cast<__nv_bfloat16*>(ws + o_xqh) : nullptr;
-    v.xq_lo = mixed ? reinterpret_cast<__nv_bfloat16*>(ws + o_xql) : nullptr;
-    v.mp_hi = mixed ? ws + o_mph : nullptr;
-    v.mp_lo = mixed ? ws + o_mpl : nullptr;
+    v.xa = mixed ? ws + o_xa : nullptr;
+    v.xq = mixed ? ws + o_xq : nullptr;
+    v.mp = mixed ? ws + o_mp : nullptr;
     v.mats = d(o_mats);
     v.Ct = d(o_ct);
     v.E = d(o_E);
@@ -1370,8 +1356,8 @@ int sgh_batch_create(const sgh_config* cfgs, int32_t n, int32_t precision, sgh_b
       // per N: forward, inverse in 128-row chunks; forward, inverse in NB-row chunks
       mplane[kv.first] = po;
       B->mplane_list.push_back({kv.first, po});
-      po += 2LL * (long long)(umma::plane_bytes_r<128>(kv.first, kv.first) +
-                              umma::plane_bytes_r<f2::NB>(kv.first, kv.first));
+      po += 2LL * (long long)(umma::pair_bytes<128>(kv.first, kv.first) +
+                              umma::pair_bytes<f2::NB>(kv.first, kv.first));
     }
     B->mp_bytes = (size_t)po;
   }
@@ -1402,11 +1388,11 @@ int sgh_batch_create(const sgh_config* cfgs, int32_t n, int32_t precision, sgh_b
     sl.nutile = face_utiles(c.nx, c.ny);
     if (precision == SGH_PRECISION_MIXED) {
       sl.xa = (long long)B->xa_bytes;
-      B->xa_bytes += umma::plane_bytes(c.ny, c.nx);
-      sl.mpx = mplane[c.nx] + 2LL * (long long)umma::plane_bytes_r<128>(c.nx, c.nx);
-      sl.mpx_inv = sl.mpx + (long long)umma::plane_bytes_r<f2::NB>(c.nx, c.nx);
+      B->xa_bytes += umma::pair_bytes<128>(c.ny, c.nx);
+      sl.mpx = mplane[c.nx] + 2LL * (long long)umma::pair_bytes<128>(c.nx, c.nx);
+      sl.mpx_inv = sl.mpx + (long long)umma::pair_bytes<f2::NB>(c.nx, c.nx);
       sl.mpy = mplane[c.ny];
-      sl.mpy_inv = sl.mpy + (long long)umma::plane_bytes_r<128>(c.ny, c.ny);
+      sl.mpy_inv = sl.mpy + (long long)umma::pair_bytes<128>(c.ny, c.ny);
     }
     sl.Lx = c.Lx; sl.Ly = c.Ly; sl.Lz = c.Lz;
     sl.dx = c.Lx / c.nx; sl.dy = c.Ly / c.ny;
@@ -1485,12 +1471,9 @@ int sgh_batch_create(const sgh_config* cfgs, int32_t n, int32_t precision, sgh_b
   B->o_prelax = L.take(sizeof(double) * 2 * B->tot_blk);
   B->o_ptile = L.take(sizeof(double) * std::max(B->tot_tile, B->tot_utile));
   if (precision == SGH_PRECISION_MIXED) {
-    B->o_xah = L.take(B->xa_bytes);
-    B->o_xal = L.take(B->xa_bytes);
-    B->o_xqh = L.take(B->xa_bytes);
-    B->o_xql = L.take(B->xa_bytes);
-    B->o_mph = L.take(B->mp_bytes);
-    B->o_mpl = L.take(B->mp_bytes);
+    B->o_xa = L.take(B->xa_bytes);
+    B->o_xq = L.take(B->xa_bytes);
+    B->o_mp = L.take(B->mp_bytes);
   }
   if (precision == SGH_PRECISION_MIXED) {
     int max_ny = 0;
@@ -1546,26 +1529,21 @@ int sgh_batch_bind(sgh_batch* B, void* workspace, uint64_t bytes, void* stream) 
     kb_dct_matrix<<<cdivl((long long)m.first * m.first, BT), BT, 0, s>>>(m.first, B->d(B->o_mats) + m.second);
   const BView v = B->view();
   if (B->precision == SGH_PRECISION_MIXED) {
-    SGB_CK(cudaMemsetAsync(B->ws + B->o_xah, 0, B->xa_bytes, s));
-    SGB_CK(cudaMemsetAsync(B->ws + B->o_xal, 0, B->xa_bytes, s));
-    SGB_CK(cudaMemsetAsync(B->ws + B->o_xqh, 0, B->xa_bytes, s));
-    SGB_CK(cudaMemsetAsync(B->ws + B->o_xql, 0, B->xa_bytes, s));
-    SGB_CK(cudaMemsetAsync(B->ws + B->o_mph, 0, B->mp_bytes, s));
-    SGB_CK(cudaMemsetAsync(B->ws + B->o_mpl, 0, B->mp_bytes, s));
+    SGB_CK(cudaMemsetAsync(B->ws + B->o_xa, 0, B->xa_bytes, s));
+    SGB_CK(cudaMemsetAsync(B->ws + B->o_xq, 0, B->xa_bytes, s));
+    SGB_CK(cudaMemsetAsync(B->ws + B->o_mp, 0, B->mp_bytes, s));
     for (size_t j = 0; j < B->mplane_list.size(); ++j) {
       const int N = B->mplane_list[j].first;
       const long long po = B->mplane_list[j].second;
       long long moff = -1;
       for (auto& m : B->mat_list)
         if (m.first == N) moff = m.second;
-      const size_t pb = umma::plane_bytes_r<128>(N, N), pn = umma::plane_bytes_r<f2::NB>(N, N);
-      auto hi = [&](size_t o) { return reinterpret_cast<__nv_bfloat16*>(B->ws + B->o_mph + po + o); };
-      auto lo = [&](size_t o) { return reinterpret_cast<__nv_bfloat16*>(B->ws + B->o_mpl + po + o); };
+      const size_t pb = umma::pair_bytes<128>(N, N), pn = umma::pair_bytes<f2::NB>(N, N);
+      auto pl = [&](size_t o) { return B->ws + B->o_mp + po + o; };
       const int g = cdivl((long long)N * N, BT);
       for (int inv = 0; inv < 2; ++inv) {
-        kb_matrix_planes<128><<<g, BT, 0, s>>>(N, B->d(B->o_mats) + moff, inv, hi(inv * pb), lo(inv * pb));
-        kb_matrix_planes<f2::NB><<<g, BT, 0, s>>>(N, B->d(B->o_mats) + moff, inv, hi(2 * pb + inv * pn),
-                                                 lo(2 * pb + inv * pn));
+        kb_matrix_planes<128><<<g, BT, 0, s>>>(N, B->d(B->o_mats) + moff, inv, pl(inv * pb));
+        kb_matrix_planes<f2::NB><<<g, BT, 0, s>>>(N, B->d(B->o_mats) + moff, inv, pl(2 * pb + inv * pn));
       }
     }
     float* KK = reinterpret_cast<float*>(B->ws + B->o_KK);

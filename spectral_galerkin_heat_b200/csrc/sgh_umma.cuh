@@ -1,20 +1,26 @@
-// sgh_umma.cuh -- split-BF16 contraction tiles on the 5th-generation tensor
-// cores (tcgen05.mma, accumulator in tensor memory).
+// sgh_umma.cuh -- split-BF16 contractions on the 5th-generation tensor cores
+// (tcgen05.mma, accumulator in tensor memory), shared by the kernels that use
+// them.
 //
-// One CTA of 128 threads computes a 128 x NT tile of
-//     D[m][n] = sum_k A(m, k) B(n, k)
-// for FP64 operands A, B delivered by loader functors. Each operand is split
-// into BF16 hi + lo parts (x = hi + lo + O(2^-16 x)); per 16-wide k-step the
-// tile issues three kind::f16 MMAs -- hi*hi, hi*lo, lo*hi -- accumulating in
-// FP32 in tensor memory. Operands are staged by the CTA's threads into shared
-// memory (converted on the way, so no TMA), K-major, no swizzle, in 8 x 8
-// "core matrices" of 128 contiguous bytes, double-buffered over 32-wide
-// k-chunks; one elected thread issues the MMAs and commits them to an
-// mbarrier per buffer.
+// * PTX wrappers: mbarriers with bounded waits, TMEM allocation, shared-memory
+//   matrix descriptors (K-major, no swizzle, 8 x 8 core matrices of 128
+//   contiguous bytes), the kind::f16 instruction descriptor, tcgen05.mma /
+//   commit / ld, and bulk global -> shared copies completing on an mbarrier.
+// * tile_bf16x3: one 128 x NT tile of D[m][n] = sum_k A(m, k) B(n, k) for FP64
+//   operands delivered by loader functors. Each operand is split into BF16
+//   hi + lo (x = hi + lo + O(2^-18 x)); per 16-wide k-step the tile issues
+//   three MMAs -- hi*hi, hi*lo, lo*hi -- accumulating in FP32. The CTA's
+//   threads stage the operands (converted on the way) double-buffered over
+//   32-wide k-chunks; one thread issues the MMAs. Used by the stand-alone
+//   tensor-core face DCT (sgh_mixed.cu).
+// * Operand planes: BF16 hi / lo copies of an operand laid out chunk by chunk
+//   exactly as a shared-memory stage, so that one bulk copy moves a chunk.
+//   The batched fused face transform (sgh_batch.cu) streams its operands from
+//   these planes.
 //
-// Every wait on an mbarrier is bounded: on expiry the tile records an error
-// code in *err, waits (again bounded) for its MMAs, frees its tensor memory
-// and returns without writing results.
+// Every wait on an mbarrier is bounded: on expiry the caller records an error,
+// waits (again bounded) for its work in flight, frees its tensor memory and
+// returns without writing results.
 #pragma once
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
@@ -297,6 +303,27 @@ __device__ __forceinline__ void plane_put_r(__nv_bfloat16* hi, __nv_bfloat16* lo
   lo[o] = l;
 }
 
+// Pair planes: the hi and lo parts of each chunk sit next to each other (hi at
+// 2 ci C, lo at 2 ci C + C for chunk index ci = (r / R) nkc + k / KC and
+// C = R * KC * 2 bytes), so ONE bulk copy moves both parts of a chunk. The
+// shared-memory stage then holds hi followed by lo, as the MMAs read them.
+template <int R>
+__host__ __device__ constexpr size_t pair_chunk_bytes() { return (size_t)R * KC * 2; }
+template <int R>
+__host__ __device__ inline size_t pair_bytes(int rows, int k) { return 2 * plane_bytes_r<R>(rows, k); }
+template <int R>
+__device__ __forceinline__ size_t pair_off(int r, int k, int nkc) {
+  return (size_t)((r / R) * nkc + k / KC) * 2 * pair_chunk_bytes<R>() + core_off(r % R, k % KC, R);
+}
+template <int R>
+__device__ __forceinline__ void pair_put(char* plane, int r, int k, int nkc, double x) {
+  __nv_bfloat16 h, l;
+  split_bf16(x, h, l);
+  const size_t o = pair_off<R>(r, k, nkc);
+  *reinterpret_cast<__nv_bfloat16*>(plane + o) = h;
+  *reinterpret_cast<__nv_bfloat16*>(plane + o + pair_chunk_bytes<R>()) = l;
+}
+
 __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
                : "memory");
@@ -307,152 +334,6 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
           smem_u32(dst)),
       "l"(src), "r"(bytes), "r"(smem_u32(bar))
       : "memory");
-}
-
-// 8 consecutive k (k0 % 8 == 0) of row r: one 16-byte row of a core matrix
-// in each plane, written with one vector store per part.
-__device__ __forceinline__ void plane_put8(__nv_bfloat16* hi, __nv_bfloat16* lo, int r, int k0, int nkc,
-                                           const double (&x)[8]) {
-  uint32_t h[4], l[4];
-#pragma unroll
-  for (int j = 0; j < 4; ++j) {
-    __nv_bfloat16 h0, l0, h1, l1;
-    split_bf16(x[2 * j], h0, l0);
-    split_bf16(x[2 * j + 1], h1, l1);
-    h[j] = (uint32_t)__bfloat16_as_ushort(h0) | ((uint32_t)__bfloat16_as_ushort(h1) << 16);
-    l[j] = (uint32_t)__bfloat16_as_ushort(l0) | ((uint32_t)__bfloat16_as_ushort(l1) << 16);
-  }
-  const size_t o = plane_off(r, k0, nkc);
-  *reinterpret_cast<uint4*>(reinterpret_cast<char*>(hi) + o) = make_uint4(h[0], h[1], h[2], h[3]);
-  *reinterpret_cast<uint4*>(reinterpret_cast<char*>(lo) + o) = make_uint4(l[0], l[1], l[2], l[3]);
-}
-
-// ---- plane tiles: a ring of bulk-copy stages feeding the tensor cores -----
-constexpr int PLANE_STAGES = 6;                 // k-chunks in flight
-constexpr int PLANE_THREADS = 256;              // 2 warpgroups
-constexpr int STAGE_BYTES = 4 * CHUNK_BYTES;    // A hi, A lo, B hi, B lo
-// Dynamic shared memory of tile_planes (bytes): the stage ring, then barriers.
-__host__ __device__ constexpr int planes_smem_bytes() { return PLANE_STAGES * STAGE_BYTES + 256; }
-
-// FP32 result tile left in shared memory by tile_planes (it reuses the first
-// 64 KB of the stage ring once every MMA has completed). Element (m, n) sits
-// at float m * 128 + (n ^ (m & 31)): the XOR spreads a column over all 32
-// banks for the TMEM -> shared copy and keeps rows conflict-free.
-__device__ __forceinline__ float tile_value(const char* smem, int m, int n) {
-  return reinterpret_cast<const float*>(smem)[m * 128 + (n ^ (m & 31))];
-}
-
-// One 128 x 128 tile D[m][n] = sum_k A(m, k) B(n, k) from operand planes.
-// a_hi/a_lo point at chunk (rt, 0) of A's planes, b_hi/b_lo at chunk (ct, 0)
-// of B's; nkc chunks along k. Thread 0 drives the ring: it issues the bulk
-// copies of the first PLANE_STAGES chunks at once, then per chunk waits for
-// its data, issues the three split-BF16 MMAs per 16-wide k-step, commits them,
-// and refills the stage of the previous chunk as soon as that chunk's MMAs
-// have drained. All waits are bounded: on expiry *err is set, in-flight work
-// is waited for (bounded), tensor memory is freed and false is returned.
-// On success the tile is in shared memory (tile_value) when this returns.
-// Call from all PLANE_THREADS threads.
-static __device__ bool tile_planes(const char* a_hi, const char* a_lo, const char* b_hi, const char* b_lo,
-                                   int nkc, char* smem, int* err) {
-  constexpr uint32_t NT = 128, NCOLS = 128;
-  constexpr int S = PLANE_STAGES;
-  uint64_t* full = reinterpret_cast<uint64_t*>(smem + S * STAGE_BYTES);
-  uint64_t* done = full + S;
-  uint32_t* tslot = reinterpret_cast<uint32_t*>(done + S);
-  volatile int* okflag = reinterpret_cast<volatile int*>(tslot + 1);
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const uint32_t idesc = idesc_bf16_f32(TM, NT);
-
-  if (warp == 0) tmem_alloc(tslot, NCOLS);
-  if (tid == 0) {
-    for (int b = 0; b < S; ++b) {
-      mbar_init(&full[b], 1);
-      mbar_init(&done[b], 1);
-    }
-    *okflag = 1;
-    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
-  }
-  tc_fence_before();
-  __syncthreads();
-  tc_fence_after();
-  const uint32_t tmem = *tslot;
-
-  if (tid == 0) {
-    uint32_t fph = 0u, dph = 0u;  // parity bit per stage
-    bool ok = true;
-    auto load = [&](int ch) {
-      const int b = ch % S;
-      char* st = smem + b * STAGE_BYTES;
-      const size_t off = (size_t)ch * CHUNK_BYTES;
-      mbar_expect_tx(&full[b], STAGE_BYTES);
-      bulk_g2s(st, a_hi + off, CHUNK_BYTES, &full[b]);
-      bulk_g2s(st + CHUNK_BYTES, a_lo + off, CHUNK_BYTES, &full[b]);
-      bulk_g2s(st + 2 * CHUNK_BYTES, b_hi + off, CHUNK_BYTES, &full[b]);
-      bulk_g2s(st + 3 * CHUNK_BYTES, b_lo + off, CHUNK_BYTES, &full[b]);
-    };
-    const int pre = nkc < S ? nkc : S;
-    for (int ch = 0; ch < pre; ++ch) load(ch);
-    for (int ch = 0; ch < nkc; ++ch) {
-      const int b = ch % S;
-      if (!mbar_wait_bounded(&full[b], (fph >> b) & 1u)) { ok = false; break; }
-      fph ^= 1u << b;
-      tc_fence_after();
-      const uint32_t s0 = smem_u32(smem + b * STAGE_BYTES);
-      const uint32_t ah = s0, al = s0 + CHUNK_BYTES, bh = s0 + 2 * CHUNK_BYTES, bl = s0 + 3 * CHUNK_BYTES;
-#pragma unroll
-      for (int s = 0; s < KC / 16; ++s) {
-        const uint32_t o = (uint32_t)(2 * s * (TM / 8) * 128);
-        const uint64_t dah = smem_desc(ah + o, (TM / 8) * 128, 128);
-        const uint64_t dal = smem_desc(al + o, (TM / 8) * 128, 128);
-        const uint64_t dbh = smem_desc(bh + o, (TM / 8) * 128, 128);
-        const uint64_t dbl = smem_desc(bl + o, (TM / 8) * 128, 128);
-        mma_bf16(tmem, dah, dbh, idesc, (ch > 0 || s > 0) ? 1u : 0u);
-        mma_bf16(tmem, dah, dbl, idesc, 1u);
-        mma_bf16(tmem, dal, dbh, idesc, 1u);
-      }
-      mma_commit(&done[b]);
-      // the stage of chunk ch-1 takes chunk ch-1+S once its MMAs are done
-      if (ch >= 1 && ch - 1 + S < nkc) {
-        const int pb = (ch - 1) % S;
-        if (!mbar_wait_bounded(&done[pb], (dph >> pb) & 1u)) { ok = false; break; }
-        dph ^= 1u << pb;
-        load(ch - 1 + S);
-      }
-    }
-    // the last commit covers every MMA issued before it
-    if (ok && nkc > 0) {
-      const int b = (nkc - 1) % S;
-      if (!mbar_wait_bounded(&done[b], (dph >> b) & 1u)) ok = false;
-    }
-    if (!ok) {
-      atomicExch(err, 1);
-      *okflag = 0;
-      for (int b = 0; b < S; ++b) {  // drain (bounded) before the memory is reused
-        mbar_wait_bounded(&full[b], (fph >> b) & 1u);
-        mbar_wait_bounded(&done[b], (dph >> b) & 1u);
-      }
-    }
-  }
-  __syncthreads();
-  const bool good = *okflag != 0;
-  if (good) {
-    // warps w and w + 4 read TMEM lanes 32 (w % 4) .. +31, one column half each
-    tc_fence_after();
-    const int q = warp & 3, half = warp >> 2;
-    const int m = q * 32 + lane;
-    float* tile = reinterpret_cast<float*>(smem);
-#pragma unroll 1
-    for (int c = half * 64; c < half * 64 + 64; c += 16) {
-      float v[16];
-      tmem_ld16(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)c, v);
-#pragma unroll
-      for (int i = 0; i < 16; ++i) tile[m * 128 + ((c + i) ^ (m & 31))] = v[i];
-    }
-  }
-  tc_fence_before();
-  __syncthreads();
-  if (warp == 0) tmem_dealloc(tmem, NCOLS);
-  return good;
 }
 
 }  // namespace umma

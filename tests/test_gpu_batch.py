@@ -110,3 +110,61 @@ def test_batch_rejects_unsupported_physics():
     cfg, path, *_ = golden_case("raster_32x16x8")
     with pytest.raises(Exception, match="face-space"):
         BatchSolver([make_context(cfg, path)], "fp64")
+
+
+ODD = [(37, 19, 7), (50, 26, 9), (33, 17, 5)]   # nx % 8 != 0 and S % 4 != 0: scalar plane and volume paths
+
+
+def test_odd_shapes_fp64_batch_matches_single_instance():
+    from spectral_galerkin_heat_b200 import B200SpectralSolver
+    from spectral_galerkin_heat_b200.batch import BatchSolver
+    steps = 6
+    ctxs = [_ctx(*sh, seed=20 + i, steps=steps) for i, sh in enumerate(ODD)]
+    b = BatchSolver(ctxs, "fp64")
+    for i in range(len(ctxs)):
+        b.start(i, steps)
+    b.step(steps)
+    for i, ctx in enumerate(ctxs):
+        s = B200SpectralSolver(None, ctx)
+        s.initialize()
+        dt = ctx.num.dt
+        for k in range(steps):
+            s.step(k * dt, dt)
+        assert rel_l2(b.modes(i).cpu().numpy(), s.state.a.cpu().numpy()) < 1e-12
+        s.finalize()
+    b.close()
+
+
+def test_odd_shapes_mixed_batch_vs_oracle_and_alone():
+    from oracle.sgh_oracle import OracleSolver
+    from spectral_galerkin_heat_b200.batch import BatchSolver
+    steps = 12
+    ctxs = []
+    for i, sh in enumerate(ODD):
+        c = _ctx(*sh, seed=30 + i, steps=steps)
+        c.num.picard_tol = 1e-8
+        c.num.max_picard_iter = 300
+        ctxs.append(c)
+    mix = BatchSolver(ctxs, "mixed")
+    for i in range(len(ctxs)):
+        mix.start(i, steps)
+    mix.step(steps)
+    assert mix.tensor_core_error() == 0
+    for i, ctx in enumerate(ctxs):
+        o = OracleSolver(ctx)
+        o.initialize()
+        for k in range(steps):
+            o.step(k * ctx.num.dt, ctx.num.dt)
+        assert rel_l2(mix.modes(i).double().cpu().numpy(), o.a) < 1e-4
+    alone = BatchSolver([ctxs[1]], "mixed")
+    alone.start(0, steps)
+    alone.step(steps)
+    assert np.array_equal(alone.modes(0).cpu().numpy(), mix.modes(1).cpu().numpy())
+    alone.close()
+    mix.close()
+
+
+def test_mixed_batch_rejects_tall_faces():
+    from spectral_galerkin_heat_b200.batch import BatchSolver
+    with pytest.raises(Exception, match="ny <= 256"):
+        BatchSolver([_ctx(64, 300, 8, seed=1, steps=2)], "mixed")
