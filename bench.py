@@ -811,6 +811,84 @@ def run_batch(args, rank, world, local_rank):
     return line
 
 
+def run_outputs(args, rank, world, local_rank):
+    """--workload outputs: output reconstruction of a modal field -- the
+    node-centred volume field of a full-volume output (sgh_nodal_temperature)
+    and 3 x 1000 profile points (sgh_points_temperature) -- at 128 x 64 x 32
+    and at the serving maximum 512 x 256 x 64, against the reference's host
+    algorithm (weighted DCT-I, all host threads) on the same modes."""
+    from types import SimpleNamespace
+
+    import torch
+
+    from oracle.sgh_oracle import nodal_temperature_dct1
+    from spectral_galerkin_heat_b200 import kernels as Kn
+    torch.cuda.set_device(local_rank)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+    K, W = args.steps, args.warmup
+    rows = {}
+    for shape, L in (((32, 64, 128), (2e-3, 1e-3, 0.5e-3)), ((64, 256, 512), (2e-3, 1e-3, 0.5e-3))):
+        nz, ny, nx = shape
+        rng = np.random.default_rng(0)
+        a = rng.standard_normal(shape)
+        ad = torch.as_tensor(a, device="cuda")
+        st = SimpleNamespace(size=L)
+        geom = SimpleNamespace(size=SimpleNamespace(x=L[0], y=L[1], z=L[2]))
+        pts = np.concatenate([np.stack([np.linspace(0, L[0], 1000), np.full(1000, L[1] / 2), np.full(1000, L[2])], 1),
+                              np.stack([np.full(1000, L[0] / 2), np.linspace(0, L[1], 1000), np.full(1000, L[2])], 1),
+                              np.stack([np.full(1000, L[0] / 2), np.full(1000, L[1] / 2), np.linspace(0, L[2], 1000)], 1)])
+        ptd = torch.as_tensor(pts, device="cuda")
+
+        def timed(fn):
+            for _ in range(W):
+                fn()
+            ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+            for k in range(K):
+                flush.fill_(k & 0xFF)
+                ev[k][0].record()
+                fn()
+                ev[k][1].record()
+            torch.cuda.synchronize()
+            return sum(x.elapsed_time(y) for x, y in ev) / K
+        nodal_ms = timed(lambda: Kn.reconstruct_temperature_DCT(ad, st))
+        points_ms = timed(lambda: Kn.reconstruct_temperature_volume_at_points(ad, None, geom, st, ptd))
+        # e2e: modes from host memory in, the node field back to host memory
+        host_a = torch.as_tensor(a).pin_memory()
+
+        def e2e():
+            d = host_a.to("cuda", non_blocking=True)
+            return Kn.reconstruct_temperature_DCT(d, st).to("cpu")
+        e2e_ms = timed(e2e)
+        nodal_bytes = 8 * (nx * ny * nz + (nx + 1) * (ny + 1) * (nz + 1))
+        t0 = time.perf_counter()
+        n_cpu = 0
+        while time.perf_counter() - t0 < min(args.cpu_budget, 10.0) or n_cpu < 1:
+            nodal_temperature_dct1(a, L)
+            n_cpu += 1
+        cpu_ms = (time.perf_counter() - t0) * 1e3 / n_cpu
+        rows[f"{nx}x{ny}x{nz}"] = {
+            "nodal_ms": nodal_ms, "nodal_e2e_ms": e2e_ms, "points_3000_ms": points_ms,
+            "nodal_cpu_reference_algorithm_ms": cpu_ms, "cpu_over_gpu": cpu_ms / nodal_ms,
+            "nodal_gbs_min_traffic": nodal_bytes / (nodal_ms * 1e-3) / 1e9}
+    if rank != 0:
+        return None
+    big = rows["512x256x64"]
+    peak, peak_kind = _peaks()
+    return {"metric": "node-field reconstructions/s", "value": 1e3 / big["nodal_ms"], "unit": "1/s",
+            "n_gpus": world, "steps": K, "warmup": W, "ms_per_step": big["nodal_ms"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded random modes)",
+            "config": {"workload": "output_reconstruction", "shapes": rows,
+                       "l2": "flushed between timed launches (256 MB write)"},
+            "e2e": {"value": 1e3 / big["nodal_e2e_ms"], "unit": "1/s", "h2d_bytes_per_step": 8 * 512 * 256 * 64,
+                    "d2h_bytes_per_step": 8 * 513 * 257 * 65},
+            "roofline": {"kernel": "3 axis passes of the node field", "bound": "hbm",
+                         "achieved": big["nodal_gbs_min_traffic"], "peak": peak, "unit": "GB/s",
+                         "frac": big["nodal_gbs_min_traffic"] / peak, "peak_source": peak_kind, "traffic": None},
+            "cpu_baseline": {"value": 1e3 / big["nodal_cpu_reference_algorithm_ms"], "unit": "1/s",
+                             "cores": os.cpu_count(), "kind": "port",
+                             "sample": "the reference's weighted DCT-I (scipy, all threads) on the same modes"}}
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -818,7 +896,7 @@ def main():
                     help="timed steps (serving: batched steps, default 1000; otherwise 200)")
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
-    ap.add_argument("--workload", choices=["serving", "batch", "raster", "track"], default="serving")
+    ap.add_argument("--workload", choices=["serving", "batch", "raster", "track", "outputs"], default="serving")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--requests", type=int, default=600, help="serving: saturated stream length")
@@ -833,7 +911,7 @@ def main():
     ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed", help="--profile serving-step")
     args = ap.parse_args()
     if args.steps is None:
-        args.steps = 2 if args.profile else {"serving": 1000, "batch": 100}.get(args.workload, 200)
+        args.steps = 2 if args.profile else {"serving": 1000, "batch": 100, "outputs": 20}.get(args.workload, 200)
     if args.warmup < 3:
         args.warmup = 3
     if args.profile:
@@ -855,6 +933,8 @@ def main():
             line = run_serving(args, rank, world, local_rank)
         elif args.workload == "batch":
             line = run_batch(args, rank, world, local_rank)
+        elif args.workload == "outputs":
+            line = run_outputs(args, rank, world, local_rank)
         else:
             line = run_b200(args, rank, world, local_rank)
         if line is not None:

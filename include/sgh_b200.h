@@ -311,6 +311,31 @@ int sgh_dct2_bf16x3(int32_t kind, int32_t ny, int32_t nx, const double* in, doub
 int sgh_dctn_noalloc(int32_t kind, int32_t ndim, const int32_t* shape, const double* in, double* out,
                      void* stream);
 
+/* ---- output reconstruction on the device -------------------------------- */
+
+/* Node-centred temperature of FP64 modes (nz, ny, nx) on a cuboid of size
+ * Lx x Ly x Lz: out[l][k][j] = sum a[p][n][m] C_m cos(pi m j / nx)
+ * C_n cos(pi n k / ny) C_p cos(pi p l / nz) for j = 0..nx, k = 0..ny,
+ * l = 0..nz, with C_0 = sqrt(1/L), C_m = sqrt(2/L); out is C-ordered
+ * (nz+1, ny+1, nx+1) (the reference returns its transpose). Replaces
+ * reconstruct_temperature_DCT (physics/spectral_helpers.py:146-204), which
+ * evaluates the same series as a weighted DCT-I on the host. workspace:
+ * sgh_nodal_workspace_bytes() bytes, caller-owned, 8-byte aligned. Async. */
+int sgh_nodal_workspace_bytes(int32_t nx, int32_t ny, int32_t nz, uint64_t* bytes);
+int sgh_nodal_temperature(int32_t nx, int32_t ny, int32_t nz, double Lx, double Ly, double Lz,
+                          const double* modes, double* out, void* workspace, uint64_t bytes, void* stream);
+
+/* Temperature of FP64 modes at n_points points coords[3 i + 0..2] = (x, y, z),
+ * each clipped to the domain: out[i] = sum a[p][n][m] C_m cos(pi m x / Lx)
+ * C_n cos(pi n y / Ly) C_p cos(pi p z / Lz). Replaces
+ * reconstruct_temperature_volume_at_points (physics/spectral_helpers.py:206-248),
+ * the point evaluation behind save_temp_profiles (:251-333). coords and out
+ * are device arrays; workspace: sgh_points_workspace_bytes() bytes. Async. */
+int sgh_points_workspace_bytes(int32_t nx, int32_t ny, int32_t nz, int32_t n_points, uint64_t* bytes);
+int sgh_points_temperature(int32_t nx, int32_t ny, int32_t nz, double Lx, double Ly, double Lz,
+                           const double* modes, int32_t n_points, const double* coords, double* out,
+                           void* workspace, uint64_t bytes, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -25,7 +25,11 @@ the pieces it calls:
   (``core/properties.py:154-194``, ``spectral_cpu_kernels.py:165-252``,
   ``physics/spectral_ops.py:105-170``);
 * surface / volume reconstructions and projections
-  (``physics/spectral_ops.py:83-102, 210-231``).
+  (``physics/spectral_ops.py:83-102, 210-231``);
+* output reconstruction: the node-centred field, point values and the three
+  temperature profiles (``physics/spectral_helpers.py:146-333``), written as
+  explicit cosine-series contractions (the reference evaluates the node
+  field as a weighted DCT-I; both give the same series).
 
 The orthonormal DCT-II/III pair is ``scipy.fft.dctn(type=2|3, norm='ortho')``,
 the same third-party routine the reference calls
@@ -500,3 +504,85 @@ class OracleSolver:
 
     def volume_temperature(self):
         return self.reconstruct_volume(self.a)
+
+
+# ---- output reconstruction (physics/spectral_helpers.py:146-333) -----------------
+
+
+def _coef(n, length):
+    """C_0 = sqrt(1/L), C_m = sqrt(2/L) (physics/spectral_helpers.py:26-46)."""
+    c = np.full(n, np.sqrt(2.0 / length))
+    c[0] = np.sqrt(1.0 / length)
+    return c
+
+
+def nodal_temperature(a, lengths):
+    """Node-centred field of modes ``a`` (nz, ny, nx) at x_j = j Lx / nx,
+    j = 0..nx (likewise y, z), shape (nx+1, ny+1, nz+1)
+    (``reconstruct_temperature_DCT``, physics/spectral_helpers.py:146-204)."""
+    nz, ny, nx = a.shape
+    Lx, Ly, Lz = lengths
+    B = []
+    for n, L in ((nx, Lx), (ny, Ly), (nz, Lz)):
+        j = np.arange(n + 1)[:, None]
+        m = np.arange(n)[None, :]
+        B.append(_coef(n, L)[None, :] * np.cos(np.pi * ((m * j) % (2 * n)) / n))
+    Bx, By, Bz = B
+    return np.einsum("jm,kn,lp,pnm->jkl", Bx, By, Bz, a, optimize=True)
+
+
+def nodal_temperature_dct1(a, lengths, workers=-1):
+    """The node-centred field as the reference computes it on the host: the
+    modes weighted by C (halved beyond index 0), zero-padded by one plane per
+    axis, and an unnormalised 3-D DCT-I (physics/spectral_helpers.py:146-204).
+    Same result as :func:`nodal_temperature`; used as the CPU baseline."""
+    nz, ny, nx = a.shape
+    Lx, Ly, Lz = lengths
+    w = []
+    for n, L in ((nz, Lz), (ny, Ly), (nx, Lx)):
+        c = _coef(n, L)
+        c[1:] *= 0.5
+        w.append(c)
+    padded = np.zeros((nz + 1, ny + 1, nx + 1))
+    padded[:nz, :ny, :nx] = a * w[0][:, None, None] * w[1][None, :, None] * w[2][None, None, :]
+    T = scipy.fft.dctn(padded, type=1, norm=None, workers=workers)
+    return np.ascontiguousarray(T.transpose(2, 1, 0))
+
+
+def points_temperature(a, lengths, coords):
+    """Temperature at points ``coords`` (N, 3), clipped to the domain
+    (``reconstruct_temperature_volume_at_points``, physics/spectral_helpers.py:206-248)."""
+    coords = np.asarray(coords, dtype=np.float64)
+    if coords.ndim != 2 or coords.shape[1] != 3:
+        raise ValueError("coords must be of shape (N, 3)")
+    nz, ny, nx = a.shape
+    B = []
+    for col, (n, L) in enumerate(((nx, lengths[0]), (ny, lengths[1]), (nz, lengths[2]))):
+        x = np.clip(coords[:, col], 0.0, L)
+        B.append(_coef(n, L)[:, None] * np.cos(np.pi * np.arange(n)[:, None] * x[None, :] / L))
+    Bx, By, Bz = B
+    return np.einsum("pnm,pi,ni,mi->i", a, Bz, By, Bx, optimize=True)
+
+
+def temp_profiles(a, lengths, surface, laser_position=None, center="laser", num_points=1000):
+    """Profiles along x, y and z through a centre on the top face
+    (``save_temp_profiles``, physics/spectral_helpers.py:251-333); ``surface``
+    is the top-face field used by ``center="hotspot"``."""
+    Lx, Ly, Lz = lengths
+    nz, ny, nx = a.shape
+    if center == "hotspot":
+        iy, ix = np.unravel_index(int(np.argmax(surface)), surface.shape)
+        xc, yc = (ix + 0.5) * (Lx / nx), (iy + 0.5) * (Ly / ny)
+    elif center == "laser":
+        if laser_position is None:
+            raise ValueError("Laser position required for center='laser'")
+        xc, yc = float(laser_position[0]), float(laser_position[1])
+    else:
+        raise ValueError(f"Unknown center method: {center}")
+    xc, yc = float(np.clip(xc, 0.0, Lx)), float(np.clip(yc, 0.0, Ly))
+    out = {}
+    for key, L_axis, fixed in (("x", Lx, (None, yc, Lz)), ("y", Ly, (xc, None, Lz)), ("z", Lz, (xc, yc, None))):
+        c = np.linspace(0.0, L_axis, num_points)
+        pts = np.stack([c if v is None else np.full(num_points, v) for v in fixed], axis=1)
+        out[key] = (c, points_temperature(a, lengths, pts))
+    return out

@@ -31,6 +31,8 @@ EXPORTED = (
     "sgh_plan_workspace_bytes", "sgh_plan_bind", "sgh_plan_buffer", "sgh_plan_launch_counts", "sgh_state_reset",
     "sgh_step", "sgh_step_eager", "sgh_run", "sgh_dct3d", "sgh_surface_temperature", "sgh_project_volume",
     "sgh_reconstruct_volume", "sgh_dctn_workspace_bytes", "sgh_dctn", "sgh_dctn_noalloc",
+    "sgh_nodal_workspace_bytes", "sgh_nodal_temperature", "sgh_points_workspace_bytes",
+    "sgh_points_temperature",
     "sgh_batch_create", "sgh_batch_destroy", "sgh_batch_workspace_bytes", "sgh_batch_bind",
     "sgh_batch_slot_start", "sgh_batch_slot_stop", "sgh_batch_step", "sgh_batch_step_eager",
     "sgh_batch_status",
@@ -125,6 +127,12 @@ def lib() -> C.CDLL:
             "sgh_dctn_workspace_bytes": ([i32, C.POINTER(i32), u64p], C.c_int),
             "sgh_dctn": ([i32, i32, C.POINTER(i32), vp, vp, vp, C.c_uint64, vp], C.c_int),
             "sgh_dctn_noalloc": ([i32, i32, C.POINTER(i32), vp, vp, vp], C.c_int),
+            "sgh_nodal_workspace_bytes": ([i32, i32, i32, u64p], C.c_int),
+            "sgh_nodal_temperature": ([i32, i32, i32, C.c_double, C.c_double, C.c_double, vp, vp, vp,
+                                       C.c_uint64, vp], C.c_int),
+            "sgh_points_workspace_bytes": ([i32, i32, i32, i32, u64p], C.c_int),
+            "sgh_points_temperature": ([i32, i32, i32, C.c_double, C.c_double, C.c_double, vp, i32, vp, vp,
+                                        vp, C.c_uint64, vp], C.c_int),
             "sgh_dct2_bf16x3_workspace_bytes": ([i32, i32, u64p], C.c_int),
             "sgh_dct2_bf16x3": ([i32, i32, i32, vp, vp, vp, C.c_uint64, vp], C.c_int),
             "sgh_batch_create": ([C.POINTER(SghConfig), i32, i32, C.POINTER(vp)], C.c_int),

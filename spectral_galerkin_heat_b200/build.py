@@ -15,7 +15,7 @@ CSRC = os.path.join(PKG, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 LIB = os.path.join(PKG, "libsgh_b200.so")
 SOURCES = [os.path.join(CSRC, "sgh_b200.cu"), os.path.join(CSRC, "sgh_batch.cu"),
-           os.path.join(CSRC, "sgh_mixed.cu")]
+           os.path.join(CSRC, "sgh_mixed.cu"), os.path.join(CSRC, "sgh_outputs.cu")]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
               "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]
 

@@ -9,7 +9,14 @@ Functions with the reference kernel modules' names and meanings
   (``physics/spectral_ops.py:210-231``) -> ``sgh_surface_temperature``;
 * ``reconstruct_volume(a, state)`` / ``project_volume(f, state)``
   (``physics/spectral_ops.py:83-102``) -> ``sgh_reconstruct_volume`` /
-  ``sgh_project_volume``.
+  ``sgh_project_volume``;
+* output reconstruction with the reference's names and arguments
+  (``physics/spectral_helpers.py``): ``reconstruct_temperature_DCT(a, state)``
+  (node-centred field, :146-204) -> ``sgh_nodal_temperature``;
+  ``reconstruct_temperature_volume_at_points(a, num, geom, state, coords)``
+  (:206-248) -> ``sgh_points_temperature``; ``save_temp_profiles(a, num, geom,
+  state, laser_position, center, num_points)`` (:251-333) on top of them. The
+  results stay on the device (torch tensors); the reference returns NumPy.
 
 ``state`` is the :class:`~spectral_galerkin_heat_b200.solver.B200State` returned
 by ``B200SpectralSolver.initialize``. The time step itself is not exposed
@@ -22,7 +29,9 @@ import ctypes as C
 from . import _lib
 
 __all__ = ["DCT_II", "IDCT_II", "reconstruct_surface_temperature",
-           "reconstruct_bottom_temperature", "reconstruct_volume", "project_volume"]
+           "reconstruct_bottom_temperature", "reconstruct_volume", "project_volume",
+           "reconstruct_temperature_DCT", "reconstruct_temperature_volume_at_points",
+           "save_temp_profiles"]
 
 _scratch = {}
 
@@ -102,3 +111,109 @@ def project_volume(f, state):
         state.plan, C.c_void_p(f.data_ptr()), C.c_void_p(out.data_ptr()),
         C.c_void_p(state.stream.cuda_stream)))
     return out
+
+
+# ---- output reconstruction -----------------------------------------------------
+
+
+def _workspace(key, nbytes, device):
+    import torch
+    ws = _scratch.get((device, key))
+    if ws is None or ws.numel() < nbytes:
+        ws = torch.empty(max(int(nbytes), 8), dtype=torch.uint8, device=device)
+        _scratch[(device, key)] = ws
+    return ws
+
+
+def _lengths(state, geom=None):
+    if geom is not None:
+        return float(geom.size.x), float(geom.size.y), float(geom.size.z)
+    return tuple(float(v) for v in state.size)
+
+
+def reconstruct_temperature_DCT(a, state):
+    """Node-centred temperature ``T(x_j, y_k, z_l)`` at ``x_j = j Lx / nx``
+    (``j = 0..nx``, likewise y, z) of modes ``a`` (nz, ny, nx), returned as
+    (nx+1, ny+1, nz+1) like the reference (``spectral_helpers.py:146-204``)."""
+    import torch
+    if not (isinstance(a, torch.Tensor) and a.is_cuda):
+        raise TypeError("b200 kernels take CUDA tensors")
+    a = a.to(torch.float64).contiguous()
+    nz, ny, nx = a.shape
+    Lx, Ly, Lz = _lengths(state)
+    L = _lib.lib()
+    nbytes = C.c_uint64()
+    _lib.check("sgh_nodal_workspace_bytes", L.sgh_nodal_workspace_bytes(nx, ny, nz, C.byref(nbytes)))
+    ws = _workspace("nodal", nbytes.value, a.device)
+    out = torch.empty((nz + 1, ny + 1, nx + 1), dtype=torch.float64, device=a.device)
+    _lib.check("sgh_nodal_temperature", L.sgh_nodal_temperature(
+        nx, ny, nz, Lx, Ly, Lz, C.c_void_p(a.data_ptr()), C.c_void_p(out.data_ptr()),
+        C.c_void_p(ws.data_ptr()), ws.numel(), C.c_void_p(torch.cuda.current_stream(a.device).cuda_stream)))
+    return out.permute(2, 1, 0).contiguous()
+
+
+def reconstruct_temperature_volume_at_points(a, num, geom, state, coords):
+    """Temperature of modes ``a`` at points ``coords`` (N, 3), each clipped to
+    the domain (``spectral_helpers.py:206-248``); returns (N,) on the device.
+    ``ValueError`` unless ``coords`` has shape (N, 3)."""
+    import numpy as np
+    import torch
+    c = coords if isinstance(coords, torch.Tensor) else np.asarray(coords)
+    if c.ndim != 2 or c.shape[1] != 3:
+        raise ValueError("coords must be of shape (N, 3)")
+    if not (isinstance(a, torch.Tensor) and a.is_cuda):
+        raise TypeError("b200 kernels take CUDA tensors")
+    a = a.to(torch.float64).contiguous()
+    pts = torch.as_tensor(c, dtype=torch.float64, device=a.device).contiguous()
+    nz, ny, nx = a.shape
+    Lx, Ly, Lz = _lengths(state, geom)
+    n = int(pts.shape[0])
+    out = torch.empty(n, dtype=torch.float64, device=a.device)
+    if n == 0:
+        return out
+    L = _lib.lib()
+    nbytes = C.c_uint64()
+    _lib.check("sgh_points_workspace_bytes", L.sgh_points_workspace_bytes(nx, ny, nz, n, C.byref(nbytes)))
+    ws = _workspace("points", nbytes.value, a.device)
+    _lib.check("sgh_points_temperature", L.sgh_points_temperature(
+        nx, ny, nz, Lx, Ly, Lz, C.c_void_p(a.data_ptr()), n, C.c_void_p(pts.data_ptr()),
+        C.c_void_p(out.data_ptr()), C.c_void_p(ws.data_ptr()), ws.numel(),
+        C.c_void_p(torch.cuda.current_stream(a.device).cuda_stream)))
+    return out
+
+
+def save_temp_profiles(a, num, geom, state, laser_position, center="laser", num_points=1000):
+    """Temperature along three lines through a centre on the top face z = Lz
+    (``spectral_helpers.py:251-333``): along x at (y_c, Lz), along y at
+    (x_c, Lz), along z at (x_c, y_c), ``num_points`` points each from 0 to the
+    domain length. ``center="laser"`` uses ``laser_position``; ``"hotspot"`` the
+    cell centre of the hottest top-face cell. Returns ``{"x": (coords, T), ...}``
+    with host coordinates and device temperatures."""
+    import numpy as np
+    import torch
+    Lx, Ly, Lz = _lengths(state, geom)
+    nz, ny, nx = a.shape
+    z_top = float(Lz)
+    if center == "hotspot":
+        T_surf = reconstruct_surface_temperature(a, state)
+        iy, ix = np.unravel_index(int(torch.argmax(T_surf).item()), tuple(T_surf.shape))
+        x_center = (ix + 0.5) * (Lx / nx)
+        y_center = (iy + 0.5) * (Ly / ny)
+    elif center == "laser":
+        if laser_position is None:
+            raise ValueError("Laser position required for center='laser'")
+        x_center, y_center = float(laser_position[0]), float(laser_position[1])
+    else:
+        raise ValueError(f"Unknown center method: {center}")
+    x_center = float(np.clip(x_center, 0.0, Lx))
+    y_center = float(np.clip(y_center, 0.0, Ly))
+    axes_cfg = [("x", Lx, (None, y_center, z_top)), ("y", Ly, (x_center, None, z_top)),
+                ("z", Lz, (x_center, y_center, None))]
+    profiles = {}
+    for key, L_axis, fixed in axes_cfg:
+        coords = np.linspace(0.0, L_axis, num_points, dtype=np.float64)
+        pts = np.empty((num_points, 3), dtype=np.float64)
+        for col, v in enumerate(fixed):
+            pts[:, col] = coords if v is None else v
+        profiles[key] = (coords, reconstruct_temperature_volume_at_points(a, num, geom, state, pts))
+    return profiles

@@ -234,6 +234,7 @@ class B200SpectralSolver(HeatSolver):
         g = ctx.geom
         sqrt_dV = math.sqrt(float(g.d.x * g.d.y * g.d.z))
         self.state = B200State(plan, ws, (cfg.nz, cfg.ny, cfg.nx), stream, sqrt_dV)
+        self.state.size = (float(g.size.x), float(g.size.y), float(g.size.z))
         self._cfg = cfg
         model = getattr(ctx.mat, "model", None)
         self._property_correction = model is not None and not model.is_constant

@@ -17,8 +17,10 @@ directly (no runner, so exactly ``steps`` calls of ``step(t, dt)`` with
 ``t = i * dt``), the CPU oracle (``oracle/sgh_oracle.py``) is stepped beside it
 on the same context object, the two are required to agree, and the reference's
 outputs are stored: modes at chosen steps (optionally a low-index block only),
-the top-surface temperature, and per-step metrics. The versions of the
-libraries used are written into every file.
+the top-surface temperature, and per-step metrics. The ``outputs_*`` files hold
+the reference's output reconstruction (node-centred field, point values,
+profiles) of a case's modes. The versions of the libraries used are written
+into every file.
 """
 from __future__ import annotations
 
@@ -160,6 +162,69 @@ def run_case(name, spec, Ctx, Solver, Numpy):
           f"rel L2 {worst:.2e}")
 
 
+def output_cases():
+    """Name -> (case of :func:`cases`, steps): the modes on which the reference's
+    output reconstruction is evaluated."""
+    return {"outputs_odd_13x10x6": ("odd_13x10x6_conv", 6),
+            "outputs_raster_32x16x8": ("raster_32x16x8", 40)}
+
+
+def run_outputs(name, case, steps, Ctx, Solver, Numpy):
+    """Step the reference to ``steps`` and store its output reconstruction of
+    the modes: the node-centred field (``reconstruct_temperature_DCT``), values
+    at seeded points partly outside the domain
+    (``reconstruct_temperature_volume_at_points``) and the three profiles for
+    ``center="laser"`` and ``"hotspot"`` (``save_temp_profiles``); the oracle's
+    restatement is required to agree."""
+    sys.path.insert(0, str(REPO))
+    from spectral_galerkin_heat.physics import spectral_helpers as H
+
+    from oracle.sgh_oracle import nodal_temperature, points_temperature, temp_profiles
+    cfg, path, *_ = cases()[case]
+    ctx = Ctx.from_dict(copy.deepcopy(cfg))
+    ctx.laser_path = path
+    ref = Solver(Numpy(), ctx)
+    ref.initialize()
+    dt = ctx.num.dt
+    for i in range(steps):
+        ref.step(i * dt, dt)
+    a = np.array(ref.state.a, dtype=np.float64, copy=True)
+    st = ref.state
+    lengths = (float(ctx.geom.size.x), float(ctx.geom.size.y), float(ctx.geom.size.z))
+    files = {"modes": a, "lengths": np.array(lengths)}
+    nodal = np.asarray(H.reconstruct_temperature_DCT(a, st), dtype=np.float64)
+    rng = np.random.default_rng(7)
+    coords = rng.uniform(-0.1, 1.1, size=(64, 3)) * np.array(lengths)
+    pts = np.asarray(H.reconstruct_temperature_volume_at_points(a, ctx.num, ctx.geom, st, coords))
+    lp = path.get_state(steps * dt, dt)
+    files.update(nodal=nodal, coords=coords, points=pts, laser_position=np.array([lp.x, lp.y]))
+
+    def rel(x, y):
+        return float(np.linalg.norm(x - y) / np.linalg.norm(y))
+    worst = max(rel(nodal_temperature(a, lengths), nodal), rel(points_temperature(a, lengths, coords), pts))
+    surface = np.asarray(ref.kernels.reconstruct_surface_temperature(a, st)) \
+        if hasattr(ref, "kernels") else None
+    for center, pos in (("laser", (lp.x, lp.y)), ("hotspot", None)):
+        prof = H.save_temp_profiles(a, ctx.num, ctx.geom, st, pos, center=center, num_points=40)
+        if surface is None:
+            from oracle.sgh_oracle import OracleSolver
+            o = OracleSolver(ctx)
+            o.initialize()
+            surface = o.surface_T(a, top=True)
+        mine = temp_profiles(a, lengths, surface, pos, center=center, num_points=40)
+        for key in "xyz":
+            c, T = prof[key]
+            files[f"profile_{center}_{key}_coords"] = np.asarray(c)
+            files[f"profile_{center}_{key}_T"] = np.asarray(T)
+            worst = max(worst, rel(mine[key][1], np.asarray(T)))
+    assert worst < 1e-12, f"{name}: oracle differs from the reference output reconstruction: {worst}"
+    import scipy
+    files["meta"] = np.array(str({"case": case, "steps": steps, "numpy": np.__version__,
+                                  "scipy": scipy.__version__, "oracle_vs_reference_worst_relL2": worst}))
+    np.savez_compressed(HERE / f"{name}.npz", **files)
+    print(f"{name}: outputs of {case} after {steps} steps, oracle vs reference worst rel L2 {worst:.2e}")
+
+
 def main(argv):
     warnings.simplefilter("ignore")
     Ctx, Solver, Numpy = import_reference()
@@ -168,6 +233,10 @@ def main(argv):
         if sel and name not in sel:
             continue
         run_case(name, spec, Ctx, Solver, Numpy)
+    for name, (case, steps) in output_cases().items():
+        if sel and name not in sel:
+            continue
+        run_outputs(name, case, steps, Ctx, Solver, Numpy)
 
 
 if __name__ == "__main__":

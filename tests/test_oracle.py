@@ -109,3 +109,41 @@ def test_propagators_known_values():
     assert K[1, 0, 0] == pytest.approx(np.exp(-alpha * (np.pi / 1e-3) ** 2 * dt), rel=1e-14)
     assert K[0, 0, 1] == pytest.approx(np.exp(-alpha * (np.pi / 4e-3) ** 2 * dt), rel=1e-14)
     assert K.shape == (4, 6, 8)
+
+
+@pytest.mark.parametrize("name", ["outputs_odd_13x10x6", "outputs_raster_32x16x8"])
+def test_output_reconstruction_matches_reference_fixtures(name):
+    """The oracle's node field, point values and profiles equal the reference's
+    (physics/spectral_helpers.py:146-333) on the fixture's modes."""
+    from oracle.sgh_oracle import OracleSolver, nodal_temperature, points_temperature, temp_profiles
+    g = load_golden(name)
+    a, L = g["modes"], tuple(g["lengths"])
+    assert rel_l2(nodal_temperature(a, L), g["nodal"]) < 1e-13
+    assert rel_l2(points_temperature(a, L, g["coords"]), g["points"]) < 1e-13
+    nz, ny, nx = a.shape
+    surface = None
+    for center in ("laser", "hotspot"):
+        if center == "hotspot":
+            case = name.replace("outputs_", "")
+            cfg, path, *_ = golden_case({"odd_13x10x6": "odd_13x10x6_conv"}.get(case, case))
+            o = OracleSolver(make_context(cfg, path))
+            o.initialize()
+            surface = o.surface_T(a, top=True)
+        prof = temp_profiles(a, L, surface, tuple(g["laser_position"]), center=center, num_points=40)
+        for key in "xyz":
+            np.testing.assert_allclose(prof[key][0], g[f"profile_{center}_{key}_coords"], rtol=0, atol=0)
+            assert rel_l2(prof[key][1], g[f"profile_{center}_{key}_T"]) < 1e-13
+
+
+def test_points_reject_bad_shapes():
+    from oracle.sgh_oracle import points_temperature
+    with pytest.raises(ValueError, match=r"\(N, 3\)"):
+        points_temperature(np.zeros((2, 2, 2)), (1.0, 1.0, 1.0), np.zeros((4, 2)))
+
+
+def test_nodal_dct1_form_equals_series_form():
+    from oracle.sgh_oracle import nodal_temperature, nodal_temperature_dct1
+    g = load_golden("outputs_odd_13x10x6")
+    a, L = g["modes"], tuple(g["lengths"])
+    assert rel_l2(nodal_temperature_dct1(a, L), g["nodal"]) < 1e-13
+    assert rel_l2(nodal_temperature_dct1(a, L), nodal_temperature(a, L)) < 1e-13
