@@ -26,7 +26,7 @@
 extern "C" {
 #endif
 
-#define SGH_ABI_VERSION 2
+#define SGH_ABI_VERSION 3
 
 /* status codes */
 #define SGH_OK               0
@@ -101,6 +101,14 @@ typedef struct {
    * Chosen per (nx, ny, nz) by the autotuner (autotune.py). Batches ignore it. */
   int32_t axis_min_ctas;
   int32_t pad1;
+  /* Laser-following refined sub-box (FineMeshParams, core/parameters.py:391-410;
+   * FineMeshState, physics/spectral_state.py:166-239). box = 1 selects box
+   * mode: the latent-heat source is evaluated on a fine box of
+   * box_refinement cells per coarse cell that follows the laser in x and y
+   * and spans the top box_size[2] metres in z. box = 0 is grid mode. */
+  int32_t box;
+  int32_t box_refinement;
+  double box_size[3];         /* Lx_box, Ly_box, Lz_box, m                   */
 } sgh_config;
 
 /* Laser state of one step (LaserState, core/laser.py:150-167). */
@@ -118,8 +126,17 @@ typedef struct {
   int32_t n_iter;             /* n_evap_iter                                 */
   int32_t converged;          /* picard_converged                            */
   int32_t status;             /* SGH_STEP_*                                  */
-  int32_t pad;
+  int32_t flags;              /* SGH_STEP_FLAG_* (box mode)                  */
 } sgh_step_out;
+
+/* sgh_step_out.flags: the latent-heat source of the step reaches a face of
+ * the fine box with more than 1% of its peak magnitude, so the melt pool
+ * extends past the box (SpectralSolver._check_latent_box_truncation,
+ * solvers/spectral.py:545-586). The x and y flags are raised only for an
+ * axis on which the box is narrower than the domain. */
+#define SGH_STEP_FLAG_BOX_FLOOR  1
+#define SGH_STEP_FLAG_BOX_X      2
+#define SGH_STEP_FLAG_BOX_Y      4
 
 /* named workspace buffers (sgh_plan_buffer) */
 enum {
@@ -130,8 +147,26 @@ enum {
   SGH_BUF_Q_EVAP_OLD = 4, /* (ny,nx) previous evaporation flux                 */
   SGH_BUF_Q_MODES = 5,    /* (nz,ny,nx) latent modes of the last iteration     */
   SGH_BUF_SURFACE = 6,    /* (ny,nx) top-surface temperature after the step    */
-  SGH_BUF_SCRATCH = 7     /* (nz,ny,nx) general scratch                        */
+  SGH_BUF_SCRATCH = 7,    /* (nz,ny,nx) general scratch                        */
+  /* box mode only */
+  SGH_BUF_BOX_T_PREV = 8, /* (nz_box,ny_box,nx_box) FineMeshState.T_prev       */
+  SGH_BUF_BOX_Q_PREV = 9, /* (nz_box,ny_box,nx_box) FineMeshState.Q_prev       */
+  SGH_BUF_BOX_BX = 10,    /* (nx_fine_total, nx) B_fine_full[0] transposed     */
+  SGH_BUF_BOX_BY = 11,    /* (ny_fine_total, ny) B_fine_full[1] transposed     */
+  SGH_BUF_BOX_BZ = 12     /* (nz_box + 1, nz) B_fine_full[2] transposed, then
+                             the top-surface weights Ct                      */
 };
+
+/* Geometry of the fine box of a box-mode plan (FineMeshState.__init__,
+ * physics/spectral_state.py:189-227). */
+typedef struct {
+  int32_t n_box[3];           /* nx_box, ny_box, nz_box                      */
+  int32_t n_fine_total[3];    /* n_fine_totals (x, y over the domain; z over
+                                 the box depth)                              */
+  double d_fine[3];           /* dx_fine, dy_fine, dz_fine                   */
+  double dV_fine;
+  double z0;                  /* Lz - Lz_box: height of the box floor        */
+} sgh_box_geom;
 
 typedef struct sgh_plan sgh_plan;
 
@@ -202,6 +237,27 @@ int sgh_project_volume(sgh_plan* plan, const double* field, double* modes, void*
 /* field = IDCT_II(modes) / sqrt(dV): reconstruct_volume
  * (physics/spectral_ops.py:83-91). Async. */
 int sgh_reconstruct_volume(sgh_plan* plan, const double* modes, double* field, void* stream);
+
+/* Box mode. Geometry of the fine box (host values, no device work);
+ * SGH_ERR_STATE for a grid-mode plan. */
+int sgh_box_geometry(const sgh_plan* plan, sgh_box_geom* out);
+
+/* Start indices (x, y) of the box window of the last step on the fine grid
+ * (_calculate_subgrid_indices, physics/spectral_helpers.py:49-85, as applied
+ * by FineMeshState.update, physics/spectral_state.py:229-237). Copies from
+ * the device and synchronises the stream. Both are -1 before the first
+ * step, when the window bases are still zero as in the reference. */
+int sgh_box_window(sgh_plan* plan, int32_t* i0, void* stream);
+
+/* out (nz_box, ny_box, nx_box) = the temperature of modes on the fine box at
+ * the current window: reconstruct_temperature_box
+ * (physics/spectral_ops.py:173-179). Async. */
+int sgh_box_temperature(sgh_plan* plan, const double* modes, double* out, void* stream);
+
+/* modes = dV_fine * the contraction of field_box (nz_box, ny_box, nx_box)
+ * against the window bases: project_box_to_modes
+ * (physics/spectral_ops.py:53-74). Async. */
+int sgh_box_project(sgh_plan* plan, const double* field_box, double* modes, void* stream);
 
 /* Plan-free orthonormal DCT over every axis of a C-ordered FP64 array of
  * ndim = 1..3 dimensions (shape[0] slowest): kind 2 = DCT_II, kind 3 =

@@ -42,7 +42,13 @@ Pinning: ``tests/golden/make_golden.py`` runs the reference itself on the same
 inputs and stores its outputs under ``tests/golden/``; ``tests/test_oracle.py``
 checks this module against those fixtures.
 
-Box mode (``fine_mesh``) is not restated: the B200 backend runs grid mode only.
+Box mode (``fine_mesh``): the laser-following fine box ``FineMeshState``
+(``physics/spectral_state.py:166-239``) with its window
+``_calculate_subgrid_indices`` (``physics/spectral_helpers.py:49-85``), the box
+reconstruction and projection (``physics/spectral_ops.py:53-74, 173-207``), the
+3-D history shift (``physics/spectral_ops.py:292-306`` with the tables of
+``_ndshift``, ``spectral_cpu_kernels.py:302-371``) and the truncation check
+(``solvers/spectral.py:545-586``) are restated in :class:`FineBox`.
 """
 from __future__ import annotations
 
@@ -54,7 +60,7 @@ import numpy as np
 import scipy.fft
 import scipy.special
 
-__all__ = ["OracleSolver", "dct2", "dct3", "dct_matrix", "evaluate_expression"]
+__all__ = ["OracleSolver", "FineBox", "dct2", "dct3", "dct_matrix", "evaluate_expression"]
 
 
 # --------------------------------------------------------------------------
@@ -155,6 +161,124 @@ def _fl_kernel(T, t_sol, inv_band, degenerate):
 
 
 # --------------------------------------------------------------------------
+# box mode
+# --------------------------------------------------------------------------
+
+def _ccoef(n, L):
+    c = math.sqrt(2.0 / L) * np.ones(n)
+    c[0] = math.sqrt(1.0 / L)
+    return c
+
+
+def _shift_table(n, shift):
+    """Clamped neighbours, linear weights and in-range mask of an order-1 shift
+    (``_shift_axis_tables``, ``spectral_cpu_kernels.py:328-350``)."""
+    p = np.arange(n, dtype=np.float64) - float(shift)
+    i0 = np.floor(p).astype(np.int64)
+    t = p - i0
+    inside = (p >= 0.0) & (p <= n - 1)
+    return np.clip(i0, 0, n - 1), np.clip(i0 + 1, 0, n - 1), 1.0 - t, t, inside
+
+
+def shift_xy(f, sy, sx, nearest):
+    """Order-1 translation of a 2-D field or of every z-layer of a 3-D field by
+    ``(sy, sx)`` pixels, ``mode='nearest'`` or ``'constant'`` with 0 outside
+    (``_ndshift``, ``spectral_cpu_kernels.py:353-371``)."""
+    ny, nx = f.shape[-2:]
+    a, b, wy0, wy1, iny = _shift_table(ny, sy)
+    c, d, wx0, wx1, inx = _shift_table(nx, sx)
+    wy0, wy1 = wy0[:, None], wy1[:, None]
+    fa, fb = f[..., a, :], f[..., b, :]
+    out = (wy0 * (wx0 * fa[..., c] + wx1 * fa[..., d])
+           + wy1 * (wx0 * fb[..., c] + wx1 * fb[..., d]))
+    if not nearest:
+        out[..., ~(iny[:, None] & inx[None, :])] = 0.0
+    return out
+
+
+def subgrid_start(pos, d, n_total, n_box):
+    """Window start (``_calculate_subgrid_indices``, ``physics/spectral_helpers.py:49-85``)."""
+    idx_global = round(max(0.0, min(pos / d, n_total - 1)))
+    start = idx_global - n_box // 2
+    max_start = max(0, n_total - n_box)
+    return max(0, min(start, max_start))
+
+
+class FineBox:
+    """Laser-following fine box (``FineMeshState``, ``physics/spectral_state.py:166-239``)."""
+
+    def __init__(self, fine, d, size, n):
+        dx, dy, dz = d
+        Lx, Ly, Lz = size
+        self.refinement = int(fine.refinement)
+        Lxb, Lyb, Lzb = (float(v) for v in fine.box_size)
+        r = self.refinement
+        self.dx_fine, self.dy_fine, self.dz_fine = dx / r, dy / r, dz / r
+        dfine = (self.dx_fine, self.dy_fine, self.dz_fine)
+        self.n_fine_totals = [int(np.ceil(L / q)) for L, q in zip((Lx, Ly, Lzb), dfine)]
+        coords = [(np.arange(m) + 0.5) * q for m, q in zip(self.n_fine_totals, dfine)]
+        coords[2] = (Lz - Lzb) + coords[2]
+        self.B_fine_full = [_ccoef(nm, L)[:, None] * np.cos(np.pi * np.arange(nm)[:, None] * c[None, :] / L)
+                            for nm, c, L in zip(n, coords, (Lx, Ly, Lz))]
+        self.nx_box = min(int(np.ceil(Lxb / self.dx_fine)), self.n_fine_totals[0])
+        self.ny_box = min(int(np.ceil(Lyb / self.dy_fine)), self.n_fine_totals[1])
+        self.nz_box = min(int(np.ceil(Lzb / self.dz_fine)), self.n_fine_totals[2])
+        self.B_fine = [np.zeros((n[0], self.nx_box)), np.zeros((n[1], self.ny_box)),
+                       self.B_fine_full[2][:, :self.nz_box]]
+        self.dV_fine = self.dx_fine * self.dy_fine * self.dz_fine
+        self.window = (-1, -1)
+        self.T_prev = None
+        self.Q_prev = None
+
+    @property
+    def shape(self):
+        return (self.nz_box, self.ny_box, self.nx_box)
+
+    def update(self, x, y):
+        """Slide the x and y windows to the laser (``FineMeshState.update``)."""
+        ix = subgrid_start(x, self.dx_fine, self.n_fine_totals[0], self.nx_box)
+        iy = subgrid_start(y, self.dy_fine, self.n_fine_totals[1], self.ny_box)
+        self.B_fine[0][:, :] = self.B_fine_full[0][:, ix:ix + self.nx_box]
+        self.B_fine[1][:, :] = self.B_fine_full[1][:, iy:iy + self.ny_box]
+        self.window = (ix, iy)
+
+    def reconstruct(self, a):
+        """``reconstruct_temperature_box`` (``physics/spectral_ops.py:173-179``)."""
+        return np.einsum("ZYX,Zz,Yy,Xx->zyx", a, self.B_fine[2], self.B_fine[1], self.B_fine[0],
+                         optimize=True)
+
+    def project(self, f):
+        """``project_box_to_modes`` (``physics/spectral_ops.py:53-74``)."""
+        return np.einsum("zyx,Zz,Yy,Xx->ZYX", f, self.B_fine[2], self.B_fine[1], self.B_fine[0],
+                         optimize=True) * self.dV_fine
+
+    def shift_history(self, vx, vy, dt):
+        """``shift_latent_heat_history`` (``physics/spectral_ops.py:292-306``)."""
+        if self.T_prev is None:
+            return
+        sy, sx = -(vy * dt) / self.dy_fine, -(vx * dt) / self.dx_fine
+        self.T_prev = shift_xy(self.T_prev, sy, sx, nearest=True)
+        if self.Q_prev is not None:
+            self.Q_prev = shift_xy(self.Q_prev, sy, sx, nearest=False)
+
+    def truncation(self, Q):
+        """Faces of the box reached by the source (``solvers/spectral.py:545-586``):
+        flag bits 1 (floor), 2 (x window edge), 4 (y window edge)."""
+        peak = float(np.max(np.abs(Q)))
+        if peak <= 0.0:
+            return 0
+        thr = 1e-2 * peak
+        flags = 0
+        if float(np.max(np.abs(Q[0, :, :]))) > thr:
+            flags |= 1
+        if self.nx_box < self.n_fine_totals[0] and float(np.max(np.abs(Q[:, :, (0, -1)]))) > thr:
+            flags |= 2
+        if self.ny_box < self.n_fine_totals[1] and float(np.max(np.abs(Q[:, (0, -1), :]))) > thr:
+            flags |= 4
+        return flags
+
+
+# --------------------------------------------------------------------------
 # the solver
 # --------------------------------------------------------------------------
 
@@ -197,8 +321,6 @@ class OracleSolver:
             raise RuntimeError("SimulationContext must be provided either at construction "
                                "or in initialize().")
         ctx = self.context
-        if getattr(ctx, "fine", None) is not None:
-            raise NotImplementedError("the oracle restates grid mode only")
         g, mat, num = ctx.geom, ctx.mat, ctx.num
         nx, ny, nz = int(g.n.x), int(g.n.y), int(g.n.z)
         Lx, Ly, Lz = float(g.size.x), float(g.size.y), float(g.size.z)
@@ -231,7 +353,10 @@ class OracleSolver:
         self.a_temp = np.zeros(self.shape)
 
         model = getattr(mat, "model", None)
-        self.grid_latent = float(getattr(mat, "L_f", 0.0)) > 0.0
+        fine = getattr(ctx, "fine", None)
+        self.box = None if fine is None else FineBox(fine, (dx, dy, dz), (Lx, Ly, Lz), (nx, ny, nz))
+        self.box_flags = 0
+        self.grid_latent = fine is None and float(getattr(mat, "L_f", 0.0)) > 0.0
         self.prop_corr = model is not None and not model.is_constant
         Ts, Tl = float(mat.T_solidus), float(mat.T_liquidus)
         self.T_s, self.T_l = Ts, Tl
@@ -417,11 +542,22 @@ class OracleSolver:
         T0 = float(mat.T0)
         htop, hbot = float(mat.h_conv_top), float(mat.h_conv_bottom)
         Ct, Cb = self.Cp_top[:, None, None], self.Cp_bot[:, None, None]
+        box = self.box
+        if box is not None:
+            # reposition, seed the history on the first step, shift it (solvers/spectral.py:288-294)
+            box.update(st.x, st.y)
+            if box.T_prev is None:
+                box.T_prev = box.reconstruct(aK).copy()
+                if box.Q_prev is None:
+                    box.Q_prev = np.zeros(box.shape)
+            box.shift_history(vx, vy, ctx.num.dt)
 
         q_shift = self.shift(self.q_evap_old, vx * dt, vy * dt)
         S_top = self.face_dct(q_las - q_shift)
         a_temp = aK + KK * Ct * S_top
-        if self.grid_latent and self.Q_modes_prev is not None:
+        if box is not None and box.T_prev is not None and box.Q_prev is not None:
+            a_temp += KK * box.project(box.Q_prev)
+        elif self.grid_latent and self.Q_modes_prev is not None:
             a_temp += KK * self.Q_modes_prev
         if htop > 0:
             Ts0 = self.surface_T(a_temp, top=True)
@@ -441,6 +577,7 @@ class OracleSolver:
         n_el = float(a_temp.size)
         it, rel, converged = -1, float("nan"), False
         Qm = None
+        Q_raw = None
         if self.track_picard_history:
             self.picard_history = []
         for it in range(self.max_iter):
@@ -455,7 +592,10 @@ class OracleSolver:
                 if htop > 0:
                     S_raw = S_raw - self.face_dct(q_cv)
             Qm = None
-            if self.grid_latent:
+            if box is not None and box.T_prev is not None:
+                Q_raw = self.latent_source(box.reconstruct(a_old), box.T_prev)
+                Qm = box.project(Q_raw)
+            elif self.grid_latent:
                 Tf = self.reconstruct_volume(a_old)
                 Qm = self.project_volume(self.latent_source(Tf, self.T_prev_full))
             a_new = aK + KK * Ct * S_raw
@@ -489,6 +629,15 @@ class OracleSolver:
         self.a_temp = a_temp
         if self.prop_corr or self.grid_latent:
             self.T_prev_full = self.reconstruct_volume(self.a)
+        self.box_flags = 0
+        if box is not None:
+            # history of the converged step (solvers/spectral.py:525-533)
+            box.T_prev = box.reconstruct(a_temp)
+            if box.Q_prev is None:
+                box.Q_prev = np.zeros(box.shape)
+            if Q_raw is not None:
+                box.Q_prev = Q_raw.copy()
+                self.box_flags = box.truncation(Q_raw)
         metrics = {"T_surface_max": float(np.max(T_temp)), "P_laser": P_laser,
                    "n_evap_iter": it + 1, "picard_converged": converged,
                    "picard_rel_err": rel}

@@ -11,7 +11,10 @@ import os
 import threading
 
 __all__ = ["lib", "LIB_PATH", "SghProgram", "SghConfig", "SghLaser", "SghStepOut", "check",
-           "EXPORTED", "SghError", "BUF", "STEP_STATUS", "SghBatchSlotInfo", "PRECISION"]
+           "EXPORTED", "SghError", "BUF", "STEP_STATUS", "SghBatchSlotInfo", "PRECISION",
+           "SghBoxGeom", "STEP_FLAGS", "ABI_VERSION"]
+
+ABI_VERSION = 3
 
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libsgh_b200.so")
 
@@ -23,7 +26,10 @@ ERRORS = {-1: "SGH_ERR_INVALID", -2: "SGH_ERR_CUDA", -3: "SGH_ERR_STATE",
 STEP_STATUS = {0: "converged", 1: "capped", 2: "nonfinite"}
 PRECISION = {"fp64": 0, "mixed": 1}
 BUF = {"modes": 0, "K": 1, "KK": 2, "T_prev": 3, "q_evap_old": 4, "Q_modes": 5,
-       "surface": 6, "scratch": 7}
+       "surface": 6, "scratch": 7, "box_T_prev": 8, "box_Q_prev": 9, "box_Bx": 10,
+       "box_By": 11, "box_Bz": 12}
+# sgh_step_out.flags: faces of the fine box reached by the latent source
+STEP_FLAGS = {1: "floor (depth)", 2: "x window edge", 4: "y window edge"}
 
 # Every function declared in include/sgh_b200.h (checked by the tests).
 EXPORTED = (
@@ -32,7 +38,8 @@ EXPORTED = (
     "sgh_step", "sgh_step_eager", "sgh_run", "sgh_dct3d", "sgh_surface_temperature", "sgh_project_volume",
     "sgh_reconstruct_volume", "sgh_dctn_workspace_bytes", "sgh_dctn", "sgh_dctn_noalloc",
     "sgh_nodal_workspace_bytes", "sgh_nodal_temperature", "sgh_points_workspace_bytes",
-    "sgh_points_temperature",
+    "sgh_points_temperature", "sgh_box_geometry", "sgh_box_window", "sgh_box_temperature",
+    "sgh_box_project",
     "sgh_batch_create", "sgh_batch_destroy", "sgh_batch_workspace_bytes", "sgh_batch_bind",
     "sgh_batch_slot_start", "sgh_batch_slot_stop", "sgh_batch_step", "sgh_batch_step_eager",
     "sgh_batch_status",
@@ -63,6 +70,7 @@ class SghConfig(C.Structure):
         ("cell_integrated", C.c_int32), ("max_iter", C.c_int32),
         ("omega", C.c_double), ("tol", C.c_double),
         ("axis_min_ctas", C.c_int32), ("pad1", C.c_int32),
+        ("box", C.c_int32), ("box_refinement", C.c_int32), ("box_size", C.c_double * 3),
     ]
 
 
@@ -74,7 +82,12 @@ class SghLaser(C.Structure):
 class SghStepOut(C.Structure):
     _fields_ = [("T_surface_max", C.c_double), ("P_laser", C.c_double),
                 ("picard_rel_err", C.c_double), ("n_iter", C.c_int32),
-                ("converged", C.c_int32), ("status", C.c_int32), ("pad", C.c_int32)]
+                ("converged", C.c_int32), ("status", C.c_int32), ("flags", C.c_int32)]
+
+
+class SghBoxGeom(C.Structure):
+    _fields_ = [("n_box", C.c_int32 * 3), ("n_fine_total", C.c_int32 * 3),
+                ("d_fine", C.c_double * 3), ("dV_fine", C.c_double), ("z0", C.c_double)]
 
 
 class SghBatchSlotInfo(C.Structure):
@@ -148,12 +161,16 @@ def lib() -> C.CDLL:
             "sgh_batch_error": ([vp, C.POINTER(i32), vp], C.c_int),
             "sgh_batch_launch_counts": ([vp, C.POINTER(i32), C.POINTER(i32), C.POINTER(i32)], C.c_int),
             "sgh_batch_volume_pass": ([vp, vp], C.c_int),
+            "sgh_box_geometry": ([vp, C.POINTER(SghBoxGeom)], C.c_int),
+            "sgh_box_window": ([vp, C.POINTER(i32), vp], C.c_int),
+            "sgh_box_temperature": ([vp, vp, vp, vp], C.c_int),
+            "sgh_box_project": ([vp, vp, vp, vp], C.c_int),
         }
         for name, (args, res) in sig.items():
             fn = getattr(L, name)
             fn.argtypes = args
             fn.restype = res
-        if L.sgh_abi_version() != 2:
+        if L.sgh_abi_version() != ABI_VERSION:
             raise RuntimeError("libsgh_b200.so ABI version mismatch; rebuild it")
         _lib = L
         return L

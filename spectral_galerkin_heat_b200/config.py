@@ -164,8 +164,9 @@ class LaserParams:
 
 @dataclass
 class FineMeshParams:
-    """Laser-following refined sub-box (box mode). Parsed for schema parity;
-    the B200 backend runs grid mode only and rejects a context that sets it."""
+    """Laser-following refined sub-box (box mode, ``core/parameters.py:391-410``):
+    ``refinement`` fine cells per coarse cell on each axis, ``box_size`` the
+    box extents in metres. ``None`` on the context selects grid mode."""
 
     refinement: int = 4
     box_size: Vec3 = Vec3(0.9e-3, 0.9e-3, 0.04e-3)

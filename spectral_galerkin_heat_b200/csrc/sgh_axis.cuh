@@ -292,7 +292,10 @@ struct EpiTemperatureKp {
 };
 
 // Trial modes after the top-face and latent forcing (solvers/spectral.py:431-443):
-//   Qm = sqrt_dV * DCT(Q); a = aK + KK*Ct[p]*S_top; a += KK*Qm; a += KK*Cb[p]*S_bot
+//   Qm = q_scale * v; a = aK + KK*Ct[p]*S_top; a += KK*Qm; a += KK*Cb[p]*S_bot
+// where v is the last pass of the latent projection: DCT(Q) in grid mode
+// (q_scale = sqrt_dV, project_volume) or the box contraction in box mode
+// (q_scale = dV_fine, project_box_to_modes). Qm is stored when non-null.
 // With RELAX (no property correction) the relaxation of EpiRelax is applied too.
 template <bool RELAX>
 struct EpiTrial {
@@ -304,6 +307,7 @@ struct EpiTrial {
   const double* Cb;
   const double* S_top;   // DCT2 of the net top flux, times s_top_scale
   double s_top_scale;
+  double q_scale;
   const double* S_bot;   // null when there is no bottom convection
   double* Qm;
   double* a_trial;       // written when !RELAX
@@ -312,8 +316,8 @@ struct EpiTrial {
   __device__ __forceinline__ void operator()(int i, int, int, double v, Red& r) const {
     const int S = P->S;
     const int z = i / S, yx = i - z * S;
-    const double q = v * P->sqrt_dV;
-    Qm[i] = q;
+    const double q = v * q_scale;
+    if (Qm) Qm[i] = q;
     const double kk = KK[i];
     double t = aK[i] + kk * Ct[z] * (s_top_scale * S_top[yx]);
     t += kk * q;
@@ -469,6 +473,56 @@ struct EpiCommitVolume {
       q_evap_old[b] = q_evap[b];
       r.mx = fmax(r.mx, v);
     }
+  }
+};
+
+// ---- box mode (latent heat on the laser-following fine box) ----
+// The box passes contract the modes against the cosine bases of the fine
+// cells: T_box = sum a[p][n][m] Bz[p][l] By[n][k] Bx[m][j] with no further
+// scale (reconstruct_temperature_box, physics/spectral_ops.py:173-179).
+
+// First step only (initialize_latent_heat_if_needed,
+// physics/spectral_ops.py:182-194): T_prev = T_box(aK), Q_prev = 0.
+struct EpiBoxInit {
+  static constexpr int kReduce = 0;
+  const Ctrl* ctrl;
+  double* Tprev;
+  double* Qprev;
+  double* partials;
+  __device__ __forceinline__ void operator()(int i, int, int, double v, Red&) const {
+    if (ctrl->have_tprev) return;
+    Tprev[i] = v;
+    Qprev[i] = 0.0;
+  }
+};
+
+// Picard iteration: the latent source on the box from the current iterate and
+// the shifted history (compute_latent_heat_source, physics/spectral_ops.py:234-267).
+struct EpiBoxLatent {
+  static constexpr int kReduce = 0;
+  const DevParams* P;
+  const double* Tprev;
+  double* Q;
+  double* partials;
+  __device__ __forceinline__ void operator()(int i, int, int, double v, Red&) const {
+    Q[i] = latent_source(*P, v, Tprev[i]);
+  }
+};
+
+// Commit (update_latent_heat_history, physics/spectral_ops.py:197-207, and
+// solvers/spectral.py:528-533): T_prev = T_box(a); Q_prev = the source of the
+// last Picard iteration, or the shifted history when no iteration ran.
+struct EpiBoxCommit {
+  static constexpr int kReduce = 0;
+  const Ctrl* ctrl;
+  double* Tprev;
+  double* Qprev;
+  const double* Qlast;
+  const double* Qshift;
+  double* partials;
+  __device__ __forceinline__ void operator()(int i, int, int, double v, Red&) const {
+    Tprev[i] = v;
+    Qprev[i] = ctrl->iter > 0 ? Qlast[i] : Qshift[i];
   }
 };
 

@@ -141,6 +141,131 @@ __global__ void k_reset(const DevParams* __restrict__ P, Ctrl* ctrl, double* a, 
     ctrl->have_qprev = 0;
     ctrl->step = 0;
     ctrl->n_target = 0;
+    ctrl->have_tprev = 0;
+    ctrl->box_i0x = -1;
+    ctrl->box_i0y = -1;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// box mode: tables, window, history
+// ---------------------------------------------------------------------------
+
+// Fine-cell cosine bases (FineMeshState.__init__, physics/spectral_state.py:194-219):
+// B[m][i] = C_m cos(pi m c_i / L) at the fine cell centres c_i = z0 + (i + 0.5) d
+// (z0 = 0 for x and y, Lz - Lz_box for z), C_m = sqrt(1/L), sqrt(2/L)
+// (physics/spectral_helpers.py:26-46). Written point-major, T[i][m] (the
+// matrix of a reconstruction pass), and, when F is non-null, mode-major
+// F[m][i] (the matrix of a projection pass).
+__global__ void k_fine_basis(int n_modes, int n_pts, double L, double d, double z0, double* T, double* F) {
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (long long)n_modes * n_pts) return;
+  const int i = (int)(e / n_modes), m = (int)(e - (long long)i * n_modes);
+  const double c = (m == 0) ? sqrt(1.0 / L) : sqrt(2.0 / L);
+  const double coord = z0 + ((double)i + 0.5) * d;
+  const double v = c * cos(((M_PI * (double)m) * coord) / L);
+  T[e] = v;
+  if (F) F[(size_t)m * n_pts + i] = v;
+}
+
+// Start of the window of n_box fine cells centred on pos, clamped to the fine
+// grid (_calculate_subgrid_indices, physics/spectral_helpers.py:49-85).
+// Python's round() rounds half to even, as rint() does.
+__device__ int box_start(double pos, double d, int n_total, int n_box) {
+  const double g = rint(fmax(0.0, fmin(pos / d, (double)(n_total - 1))));
+  long long st = (long long)g - n_box / 2;
+  const long long max_start = n_total > n_box ? n_total - n_box : 0;
+  if (st > max_start) st = max_start;
+  if (st < 0) st = 0;
+  return (int)st;
+}
+
+// Window bases of this step (FineMeshState.update, physics/spectral_state.py:229-237):
+// rows i0 .. i0 + n_box - 1 of the point-major x and y tables, stored for the
+// reconstruction passes (Wi, n_box x n) and the projection passes (Wf, n x n_box).
+__global__ void __launch_bounds__(EW_THREADS)
+k_box_window(const DevParams* __restrict__ P, const Ctrl* __restrict__ ctrl, const double* __restrict__ BxT,
+             const double* __restrict__ ByT, double* Wxi, double* Wxf, double* Wyi, double* Wyf) {
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long nX = (long long)P->xb * P->nx;
+  if (e < nX) {
+    const int j = (int)(e / P->nx), m = (int)(e - (long long)j * P->nx);
+    const double v = BxT[(size_t)(ctrl->box_i0x + j) * P->nx + m];
+    Wxi[e] = v;
+    Wxf[(size_t)m * P->xb + j] = v;
+    return;
+  }
+  const long long f = e - nX;
+  if (f < (long long)P->yb * P->ny) {
+    const int j = (int)(f / P->ny), n = (int)(f - (long long)j * P->ny);
+    const double v = ByT[(size_t)(ctrl->box_i0y + j) * P->ny + n];
+    Wyi[f] = v;
+    Wyf[(size_t)n * P->yb + j] = v;
+  }
+}
+
+// First step only: aK = a K, the modes the history is seeded from
+// (solvers/spectral.py:283, 292-293).
+__global__ void __launch_bounds__(EW_THREADS)
+k_box_seed(const DevParams* __restrict__ P, const Ctrl* __restrict__ ctrl, const double* __restrict__ a,
+           const double* __restrict__ K, double* aK) {
+  if (ctrl->have_tprev) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < P->V) aK[i] = a[i] * K[i];
+}
+
+// History shift (shift_latent_heat_history, physics/spectral_ops.py:292-306):
+// order-1 translation of every z-layer of T_prev ('nearest') and Q_prev
+// ('constant', 0 outside) by -v dt / d_fine pixels (the tables of _ndshift,
+// physics/spectral_cpu_kernels.py:302-371). Marks the history present.
+__global__ void __launch_bounds__(EW_THREADS)
+k_box_shift(const DevParams* __restrict__ P, Ctrl* ctrl, const double* __restrict__ Tp,
+            const double* __restrict__ Qp, double* Ts, double* Qs) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < P->Nb) {
+    const int xb = P->xb, yb = P->yb, L = xb * yb;
+    const int z = i / L, r = i - z * L, y = r / xb, x = r - y * xb;
+    const ShiftTap ty = shift_tap(y, yb, ctrl->box_sy);
+    const ShiftTap tx = shift_tap(x, xb, ctrl->box_sx);
+    const size_t r0 = (size_t)z * L + (size_t)ty.i0 * xb, r1 = (size_t)z * L + (size_t)ty.i1 * xb;
+    Ts[i] = ty.w0 * (tx.w0 * Tp[r0 + tx.i0] + tx.w1 * Tp[r0 + tx.i1]) +
+            ty.w1 * (tx.w0 * Tp[r1 + tx.i0] + tx.w1 * Tp[r1 + tx.i1]);
+    double q = ty.w0 * (tx.w0 * Qp[r0 + tx.i0] + tx.w1 * Qp[r0 + tx.i1]) +
+               ty.w1 * (tx.w0 * Qp[r1 + tx.i0] + tx.w1 * Qp[r1 + tx.i1]);
+    if (!(ty.in && tx.in)) q = 0.0;
+    Qs[i] = q;
+  }
+  if (i == 0) ctrl->have_tprev = 1;
+}
+
+// Magnitude maxima of the committed latent source over the box, its floor
+// (z = 0) and its x and y edge columns, for the truncation check
+// (SpectralSolver._check_latent_box_truncation, solvers/spectral.py:545-586).
+// Skipped when no Picard iteration ran (no source of this step).
+__global__ void __launch_bounds__(EW_THREADS)
+k_box_check(const DevParams* __restrict__ P, Ctrl* ctrl, const double* __restrict__ Q) {
+  if (ctrl->iter <= 0) return;
+  const int xb = P->xb, yb = P->yb, L = xb * yb;
+  double m0 = 0.0, m1 = 0.0, m2 = 0.0, m3 = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < P->Nb; i += gridDim.x * blockDim.x) {
+    const int z = i / L, r = i - z * L, y = r / xb, x = r - y * xb;
+    const double q = fabs(Q[i]);
+    m0 = fmax(m0, q);
+    if (z == 0) m1 = fmax(m1, q);
+    if (x == 0 || x == xb - 1) m2 = fmax(m2, q);
+    if (y == 0 || y == yb - 1) m3 = fmax(m3, q);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    m0 = fmax(m0, __shfl_xor_sync(0xffffffffu, m0, o));
+    m1 = fmax(m1, __shfl_xor_sync(0xffffffffu, m1, o));
+    m2 = fmax(m2, __shfl_xor_sync(0xffffffffu, m2, o));
+    m3 = fmax(m3, __shfl_xor_sync(0xffffffffu, m3, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMax(&ctrl->box_max[0], (unsigned long long)__double_as_longlong(m0));
+    atomicMax(&ctrl->box_max[1], (unsigned long long)__double_as_longlong(m1));
+    atomicMax(&ctrl->box_max[2], (unsigned long long)__double_as_longlong(m2));
+    atomicMax(&ctrl->box_max[3], (unsigned long long)__double_as_longlong(m3));
   }
 }
 
@@ -161,7 +286,8 @@ __global__ void k_run_setup(Ctrl* ctrl, sgh_laser laser, const sgh_laser* table,
 // solvers/spectral.py:258-268) and the warm-start shift in pixels
 // (spectral_cpu_kernels.py:392-396); opens the Picard loop.
 __global__ void k_step_begin(const DevParams* __restrict__ P, Ctrl* ctrl,
-                             cudaGraphConditionalHandle h_picard, int in_graph) {
+                             cudaGraphConditionalHandle h_picard, cudaGraphConditionalHandle h_seed,
+                             int in_graph) {
   if (ctrl->table) ctrl->laser = ctrl->table[ctrl->step];
   const sgh_laser L = ctrl->laser;
   ctrl->I0 = L.is_on ? P->absorptivity * L.power / (P->area_factor * (P->r_x * P->r_y)) : 0.0;
@@ -172,6 +298,16 @@ __global__ void k_step_begin(const DevParams* __restrict__ P, Ctrl* ctrl,
   ctrl->status = SGH_STEP_CAPPED;
   ctrl->rel_err = nan("");
   if (in_graph) cudaGraphSetConditional(h_picard, P->max_iter > 0 ? 1u : 0u);
+  if (P->box) {
+    // window of this step and the history shift in fine pixels
+    // (physics/spectral_state.py:229-237, physics/spectral_ops.py:300-302)
+    ctrl->box_i0x = box_start(L.x, P->dxf, P->fx, P->xb);
+    ctrl->box_i0y = box_start(L.y, P->dyf, P->fy, P->yb);
+    ctrl->box_sx = -((L.vx * P->dt) / P->dxf);
+    ctrl->box_sy = -((L.vy * P->dt) / P->dyf);
+    for (int j = 0; j < 4; ++j) ctrl->box_max[j] = 0ull;
+    if (in_graph) cudaGraphSetConditional(h_seed, ctrl->have_tprev ? 0u : 1u);
+  }
 }
 
 // Face forcing of the initial guess: q_las, P_laser partials, and
@@ -210,7 +346,8 @@ k_zsum(const double* __restrict__ a, const double* __restrict__ w, int nz, int S
   A[i] = s;
 }
 
-// a <- K a; a_temp = aK + KK Ct[p] S_top [+ KK Q_prev]  (solvers/spectral.py:283, 320-334)
+// a <- K a; a_temp = aK + KK Ct[p] S_top [+ KK Q_prev]  (solvers/spectral.py:283, 320-334);
+// in box mode Q_prev is the projection of the shifted box history (:323-327).
 __global__ void __launch_bounds__(EW_THREADS)
 k_init_modes(const DevParams* __restrict__ P, const Ctrl* __restrict__ ctrl, double* a_it,
              const double* __restrict__ K, const double* __restrict__ KK, const double* __restrict__ Ct,
@@ -223,7 +360,7 @@ k_init_modes(const DevParams* __restrict__ P, const Ctrl* __restrict__ ctrl, dou
   aK[i] = ak;
   const double kk = KK[i];
   double t = ak + kk * Ct[z] * S_top[yx];
-  if (ctrl->have_qprev) t += kk * Qm[i];
+  if (ctrl->have_qprev || P->box) t += kk * Qm[i];
   a_it[i] = t;
 }
 
@@ -374,7 +511,19 @@ k_commit(const DevParams* __restrict__ P, Ctrl* ctrl, const double* __restrict__
     o.n_iter = ctrl->iter;
     o.converged = ctrl->status == SGH_STEP_CONVERGED ? 1 : 0;
     o.status = ctrl->status;
-    o.pad = 0;
+    int flags = 0;
+    if (P->box && ctrl->iter > 0) {
+      // truncation check (solvers/spectral.py:545-586): a face of the box whose
+      // source exceeds 1% of the peak; x and y only where the box is a window
+      const double peak = __longlong_as_double((long long)ctrl->box_max[0]);
+      if (peak > 0.0) {
+        const double thr = 1e-2 * peak;
+        if (__longlong_as_double((long long)ctrl->box_max[1]) > thr) flags |= SGH_STEP_FLAG_BOX_FLOOR;
+        if (P->xb < P->fx && __longlong_as_double((long long)ctrl->box_max[2]) > thr) flags |= SGH_STEP_FLAG_BOX_X;
+        if (P->yb < P->fy && __longlong_as_double((long long)ctrl->box_max[3]) > thr) flags |= SGH_STEP_FLAG_BOX_Y;
+      }
+    }
+    o.flags = flags;
     ctrl->out = o;
     if (ctrl->out_table) ctrl->out_table[ctrl->step] = o;
     if (P->grid_latent && P->max_iter > 0) ctrl->have_qprev = 1;
@@ -535,6 +684,11 @@ struct sgh_plan {
   bool face_space = false;
   int nparts_fs = 0, nparts_n1 = 0;
   size_t o_fsF = 0, o_fsW = 0, o_sigma = 0, o_beta = 0, o_Ab = 0, o_pn1 = 0;
+  // box mode: point-major x/y tables, z reconstruction (+ face row) and
+  // projection matrices, window bases, pass scratch, source and history
+  double box_z0 = 0.0;
+  size_t o_bx = 0, o_by = 0, o_bzi = 0, o_bzf = 0, o_wxi = 0, o_wxf = 0, o_wyi = 0, o_wyf = 0;
+  size_t o_bt1 = 0, o_bt2 = 0, o_Qbox = 0, o_Tpb = 0, o_Qpb = 0, o_Tsh = 0, o_Qsh = 0;
   size_t ws_need = 0;
   char* ws = nullptr;
   bool bound = false;
@@ -708,6 +862,50 @@ void volume_pass3(sgh_plan* p, const double* in, bool inverse, const Epi& epi, d
   axis(t2, mz, z_rows, h.nz, 1, h.S, epi, s);
 }
 
+// ---- box passes (order z, x, y for a reconstruction; y, x, z for a projection:
+// the contraction order of least work when the box is shallow in z) ----
+
+// z-pass of a box reconstruction of modes into bt1: rows 0..zb-1 of the box
+// bases, and with the face row (the top weights Ct) the z-summed input of the
+// top-surface temperature as slab zb (einsum 'p,pij->ij', spectral_ops.py:210-219).
+void box_zpass(sgh_plan* p, const double* modes, bool with_face, cudaStream_t s) {
+  const DevParams& h = p->hp;
+  axis(modes, p->d(p->o_bzi), h.zb + (with_face ? 1 : 0), h.nz, 1, h.S,
+       EpiStore{p->d(p->o_bt1), 1.0, nullptr}, s);
+}
+
+// x- and y-passes of a box reconstruction from bt1; epi receives T_box.
+template <class Epi>
+void box_xy(sgh_plan* p, const Epi& epi, cudaStream_t s) {
+  const DevParams& h = p->hp;
+  axis(p->d(p->o_bt1), p->d(p->o_wxi), h.xb, h.nx, h.zb * h.ny, 1, EpiStore{p->d(p->o_bt2), 1.0, nullptr}, s);
+  axis(p->d(p->o_bt2), p->d(p->o_wyi), h.yb, h.ny, h.zb, h.xb, epi, s);
+}
+
+// Projection of a box field onto the modes (project_box_to_modes,
+// physics/spectral_ops.py:53-74); epi receives the contraction before the
+// dV_fine scale.
+template <class Epi>
+void box_project(sgh_plan* p, const double* field, const Epi& epi, cudaStream_t s) {
+  const DevParams& h = p->hp;
+  axis(field, p->d(p->o_wyf), h.ny, h.yb, h.zb, h.xb, EpiStore{p->d(p->o_bt2), 1.0, nullptr}, s);
+  axis(p->d(p->o_bt2), p->d(p->o_wxf), h.nx, h.xb, h.zb * h.ny, 1, EpiStore{p->d(p->o_bt1), 1.0, nullptr}, s);
+  axis(p->d(p->o_bt1), p->d(p->o_bzf), h.nz, h.zb, 1, h.S, epi, s);
+}
+
+// First step of a run: seed T_prev = T_box(aK) and Q_prev = 0
+// (initialize_latent_heat_if_needed, physics/spectral_ops.py:182-194). Every
+// launch is guarded by the history flag, so eager calls may enqueue it each
+// step; the graph runs it under a conditional node.
+void enqueue_box_seed(sgh_plan* p, cudaStream_t s) {
+  const DevParams& h = p->hp;
+  k_box_seed<<<cdiv(h.V, EW_THREADS), EW_THREADS, 0, s>>>(p->P(), p->ctrl(), p->d(p->o_a), p->d(p->o_K),
+                                                          p->d(p->o_aK));
+  ++g_launches;
+  box_zpass(p, p->d(p->o_aK), false, s);
+  box_xy(p, EpiBoxInit{p->ctrl(), p->d(p->o_Tpb), p->d(p->o_Qpb), nullptr}, s);
+}
+
 void enqueue_pre_face_space(sgh_plan* p, cudaStream_t s) {
   const DevParams& h = p->hp;
   DevParams* P = p->P();
@@ -761,19 +959,44 @@ void enqueue_picard_face_space(sgh_plan* p, cudaStream_t s, cudaGraphConditional
   ++g_launches;
 }
 
-void enqueue_pre(sgh_plan* p, cudaStream_t s, cudaGraphConditionalHandle h_picard, int in_graph) {
+// Step opening: laser state, Picard switch, face forcing and (box mode) the
+// window of this step.
+void enqueue_pre_begin(sgh_plan* p, cudaStream_t s, cudaGraphConditionalHandle h_picard,
+                       cudaGraphConditionalHandle h_seed, int in_graph) {
   const DevParams& h = p->hp;
   DevParams* P = p->P();
   Ctrl* C = p->ctrl();
-  const int gV = cdiv(h.V, EW_THREADS), gS = cdiv(h.S, EW_THREADS);
-  k_step_begin<<<1, 1, 0, s>>>(P, C, h_picard, in_graph);
+  const int gS = cdiv(h.S, EW_THREADS);
+  k_step_begin<<<1, 1, 0, s>>>(P, C, h_picard, h_seed, in_graph);
   ++g_launches;
   k_face_begin<<<gS, EW_THREADS, 0, s>>>(P, C, p->d(p->o_xc), p->d(p->o_yc), p->d(p->o_qevold),
                                           p->d(p->o_qlas), p->d(p->o_qnet), p->d(p->o_plas));
   ++g_launches;
+  if (h.box) {
+    const long long n = (long long)h.xb * h.nx + (long long)h.yb * h.ny;
+    k_box_window<<<cdiv(n, EW_THREADS), EW_THREADS, 0, s>>>(P, C, p->d(p->o_bx), p->d(p->o_by), p->d(p->o_wxi),
+                                                            p->d(p->o_wxf), p->d(p->o_wyi), p->d(p->o_wyf));
+    ++g_launches;
+  }
+}
+
+// Rest of the step opening: (box mode) history shift and its projection,
+// initial guess and the convection guesses.
+void enqueue_pre_rest(sgh_plan* p, cudaStream_t s) {
+  const DevParams& h = p->hp;
+  DevParams* P = p->P();
+  Ctrl* C = p->ctrl();
+  const int gV = cdiv(h.V, EW_THREADS);
   if (p->face_space) {
     enqueue_pre_face_space(p, s);
     return;
+  }
+  if (h.box) {
+    k_box_shift<<<cdiv(h.Nb, EW_THREADS), EW_THREADS, 0, s>>>(P, C, p->d(p->o_Tpb), p->d(p->o_Qpb),
+                                                              p->d(p->o_Tsh), p->d(p->o_Qsh));
+    ++g_launches;
+    // warm start: the shifted source of the previous step, projected (solvers/spectral.py:323-327)
+    box_project(p, p->d(p->o_Qsh), EpiStore{p->d(p->o_Qm), h.dV_fine, nullptr}, s);
   }
   face_dct2(p, p->d(p->o_qnet), p->d(p->o_Stop), h.dct_scale, s);
   k_init_modes<<<gV, EW_THREADS, 0, s>>>(P, C, p->d(p->o_a), p->d(p->o_K), p->d(p->o_KK), p->d(p->o_ct),
@@ -797,6 +1020,12 @@ void enqueue_pre(sgh_plan* p, cudaStream_t s, cudaGraphConditionalHandle h_picar
   }
 }
 
+void enqueue_pre(sgh_plan* p, cudaStream_t s) {
+  enqueue_pre_begin(p, s, 0, 0, 0);
+  if (p->hp.box) enqueue_box_seed(p, s);
+  enqueue_pre_rest(p, s);
+}
+
 void enqueue_picard(sgh_plan* p, cudaStream_t s, cudaGraphConditionalHandle h_picard, int in_graph) {
   if (p->face_space) {
     enqueue_picard_face_space(p, s, h_picard, in_graph);
@@ -808,7 +1037,28 @@ void enqueue_picard(sgh_plan* p, cudaStream_t s, cudaGraphConditionalHandle h_pi
   const int gV = cdiv(h.V, EW_THREADS);
   double* S_bot = h.has_bottom_conv ? p->d(p->o_Sbot) : nullptr;
   int nparts = 0;
-  if (h.grid_latent) {
+  if (h.box) {
+    // box z-pass with the face row, top flux from the face row, the latent
+    // source on the box, and its projection into the trial modes
+    // (solvers/spectral.py:388-443 with the box branch :413-422)
+    box_zpass(p, p->d(p->o_a), true, s);
+    face_idct2_from(p, p->d(p->o_bt1) + (size_t)h.zb * h.S,
+                    EpiTopFlux{P, p->d(p->o_qlas), p->d(p->o_qev), p->d(p->o_qnet), h.prop_corr, nullptr}, s);
+    face_dct2(p, p->d(p->o_qnet), p->d(p->o_Stop), h.dct_scale, s);
+    box_xy(p, EpiBoxLatent{P, p->d(p->o_Tsh), p->d(p->o_Qbox), nullptr}, s);
+    if (h.prop_corr) {
+      box_project(p, p->d(p->o_Qbox),
+                  EpiTrial<false>{P, p->d(p->o_aK), p->d(p->o_KK), p->d(p->o_ct), p->d(p->o_cb), p->d(p->o_Stop),
+                                  1.0, h.dV_fine, S_bot, nullptr, p->d(p->o_trial), nullptr, nullptr},
+                  s);
+    } else {
+      box_project(p, p->d(p->o_Qbox),
+                  EpiTrial<true>{P, p->d(p->o_aK), p->d(p->o_KK), p->d(p->o_ct), p->d(p->o_cb), p->d(p->o_Stop),
+                                 1.0, h.dV_fine, S_bot, nullptr, nullptr, p->d(p->o_a), p->d(p->o_prelax)},
+                  s);
+      nparts = axis_blocks(h.nz, 1, h.S);
+    }
+  } else if (h.grid_latent) {
     // IDCT3(a_old) with the surface row: latent source in slabs 0..nz-1 and
     // the net top flux in slab nz of vol; then DCT3 over nz + 1 slabs turns
     // slab nz into DCT2(q_net), read by the trial epilogue as S_top.
@@ -820,13 +1070,13 @@ void enqueue_picard(sgh_plan* p, cudaStream_t s, cudaGraphConditionalHandle h_pi
     if (h.prop_corr) {
       volume_pass3(p, p->d(p->o_vol), false,
                    EpiTrial<false>{P, p->d(p->o_aK), p->d(p->o_KK), p->d(p->o_ct), p->d(p->o_cb),
-                                   S_top, h.dct_scale, S_bot, p->d(p->o_Qm), p->d(p->o_trial), nullptr,
-                                   nullptr},
+                                   S_top, h.dct_scale, h.sqrt_dV, S_bot, p->d(p->o_Qm), p->d(p->o_trial),
+                                   nullptr, nullptr},
                    p->d(p->o_t1), p->d(p->o_t2), s, h.nz + 1, h.nz);
     } else {
       volume_pass3(p, p->d(p->o_vol), false,
                    EpiTrial<true>{P, p->d(p->o_aK), p->d(p->o_KK), p->d(p->o_ct), p->d(p->o_cb),
-                                  S_top, h.dct_scale, S_bot, p->d(p->o_Qm), nullptr, p->d(p->o_a),
+                                  S_top, h.dct_scale, h.sqrt_dV, S_bot, p->d(p->o_Qm), nullptr, p->d(p->o_a),
                                   p->d(p->o_prelax)},
                    p->d(p->o_t1), p->d(p->o_t2), s, h.nz + 1, h.nz);
       nparts = axis_blocks(h.nz, 1, h.S);
@@ -837,11 +1087,11 @@ void enqueue_picard(sgh_plan* p, cudaStream_t s, cudaGraphConditionalHandle h_pi
                EpiTopFlux{P, p->d(p->o_qlas), p->d(p->o_qev), p->d(p->o_qnet), h.prop_corr, nullptr}, s);
     face_dct2(p, p->d(p->o_qnet), p->d(p->o_Stop), h.dct_scale, s);
   }
-  if (!h.grid_latent && h.prop_corr) {
+  if (!h.grid_latent && !h.box && h.prop_corr) {
     k_trial<<<gV, EW_THREADS, 0, s>>>(P, p->d(p->o_aK), p->d(p->o_KK), p->d(p->o_ct), p->d(p->o_cb),
                                        p->d(p->o_Stop), S_bot, p->d(p->o_trial));
     ++g_launches;
-  } else if (!h.grid_latent) {
+  } else if (!h.grid_latent && !h.box) {
     const int g = p->nparts_relax;
     k_trial_relax<<<g, EW_THREADS, 0, s>>>(P, p->d(p->o_aK), p->d(p->o_KK), p->d(p->o_ct), p->d(p->o_cb),
                                             p->d(p->o_Stop), S_bot, p->d(p->o_a), p->d(p->o_prelax));
@@ -867,7 +1117,28 @@ void enqueue_post(sgh_plan* p, cudaStream_t s, cudaGraphConditionalHandle h_step
   const DevParams& h = p->hp;
   DevParams* P = p->P();
   int n_surf;
-  if (p->face_space) {
+  if (h.box) {
+    // surface of the committed modes (from the box z-pass face row unless the
+    // property correction commits the full volume), then the box history:
+    // T_prev = T_box(a), Q_prev = the last source (solvers/spectral.py:502-533)
+    if (h.prop_corr) {
+      volume_pass3(p, p->d(p->o_a), true,
+                   EpiCommitVolume{P, p->d(p->o_Tprev), p->d(p->o_Tsurf), p->d(p->o_qev), p->d(p->o_qevold),
+                                   p->d(p->o_psurf)},
+                   p->d(p->o_t1), p->d(p->o_t2), s, h.nz, h.nz + 1);
+      n_surf = axis_blocks(h.nz + 1, 1, h.S);
+      box_zpass(p, p->d(p->o_a), false, s);
+    } else {
+      box_zpass(p, p->d(p->o_a), true, s);
+      face_idct2_from(p, p->d(p->o_bt1) + (size_t)h.zb * h.S,
+                      EpiCommitSurface{P, p->d(p->o_Tsurf), p->d(p->o_qev), p->d(p->o_qevold), p->d(p->o_psurf)},
+                      s);
+      n_surf = p->nparts_surf;
+    }
+    box_xy(p, EpiBoxCommit{p->ctrl(), p->d(p->o_Tpb), p->d(p->o_Qpb), p->d(p->o_Qbox), p->d(p->o_Qsh), nullptr}, s);
+    k_box_check<<<std::min(4 * 148, cdiv(h.Nb, EW_THREADS)), EW_THREADS, 0, s>>>(P, p->ctrl(), p->d(p->o_Qpb));
+    ++g_launches;
+  } else if (p->face_space) {
     face_idct2_from(p, p->d(p->o_A),
                     EpiCommitSurface{P, p->d(p->o_Tsurf), p->d(p->o_qev), p->d(p->o_qevold), p->d(p->o_psurf)},
                     s);
@@ -893,6 +1164,27 @@ void enqueue_post(sgh_plan* p, cudaStream_t s, cudaGraphConditionalHandle h_step
   ++g_launches;
 }
 
+// Adds a conditional node of the given type to the graph being captured on
+// cs (after the captured work so far) and returns its body graph.
+int add_conditional(cudaStream_t cs, cudaGraphConditionalHandle h, cudaGraphConditionalNodeType type,
+                    cudaGraph_t* body) {
+  cudaStreamCaptureStatus status;
+  cudaGraph_t cur;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t ndeps = 0;
+  SGH_CK(cudaStreamGetCaptureInfo(cs, &status, nullptr, &cur, &deps, &ndeps));
+  cudaGraphNodeParams np = {};
+  np.type = cudaGraphNodeTypeConditional;
+  np.conditional.handle = h;
+  np.conditional.type = type;
+  np.conditional.size = 1;
+  cudaGraphNode_t node;
+  SGH_CK(cudaGraphAddNode(&node, cur, deps, ndeps, &np));
+  SGH_CK(cudaStreamUpdateCaptureDependencies(cs, &node, 1, cudaStreamSetCaptureDependencies));
+  *body = np.conditional.phGraph_out[0];
+  return SGH_OK;
+}
+
 int capture(sgh_plan* p) {
   cudaGraph_t G;
   SGH_CK(cudaGraphCreate(&G, 0));
@@ -909,25 +1201,29 @@ int capture(sgh_plan* p) {
   cudaGraph_t body = outer.conditional.phGraph_out[0];
 
   SGH_CK(cudaStreamBeginCaptureToGraph(p->cs1, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-  cudaGraphConditionalHandle h_picard;
+  cudaGraphConditionalHandle h_picard, h_seed = 0;
   SGH_CK(cudaGraphConditionalHandleCreate(&h_picard, body, 0, 0));
+  if (p->hp.box) SGH_CK(cudaGraphConditionalHandleCreate(&h_seed, body, 0, 0));
   g_launches = 0;
-  enqueue_pre(p, p->cs1, h_picard, 1);
+  enqueue_pre_begin(p, p->cs1, h_picard, h_seed, 1);
+  if (p->hp.box) {
+    // history seeding, first step of a run only (not counted per step)
+    cudaGraph_t sbody;
+    const int rc = add_conditional(p->cs1, h_seed, cudaGraphCondTypeIf, &sbody);
+    if (rc) return rc;
+    const int saved = g_launches;
+    SGH_CK(cudaStreamBeginCaptureToGraph(p->cs2, sbody, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    enqueue_box_seed(p, p->cs2);
+    SGH_CK(cudaStreamEndCapture(p->cs2, &sbody));
+    g_launches = saved;
+  }
+  enqueue_pre_rest(p, p->cs1);
   p->n_pre = g_launches;
-  cudaStreamCaptureStatus status;
-  cudaGraph_t cur;
-  const cudaGraphNode_t* deps = nullptr;
-  size_t ndeps = 0;
-  SGH_CK(cudaStreamGetCaptureInfo(p->cs1, &status, nullptr, &cur, &deps, &ndeps));
-  cudaGraphNodeParams inner = {};
-  inner.type = cudaGraphNodeTypeConditional;
-  inner.conditional.handle = h_picard;
-  inner.conditional.type = cudaGraphCondTypeWhile;
-  inner.conditional.size = 1;
-  cudaGraphNode_t inner_node;
-  SGH_CK(cudaGraphAddNode(&inner_node, cur, deps, ndeps, &inner));
-  SGH_CK(cudaStreamUpdateCaptureDependencies(p->cs1, &inner_node, 1, cudaStreamSetCaptureDependencies));
-  cudaGraph_t ibody = inner.conditional.phGraph_out[0];
+  cudaGraph_t ibody;
+  {
+    const int rc = add_conditional(p->cs1, h_picard, cudaGraphCondTypeWhile, &ibody);
+    if (rc) return rc;
+  }
   SGH_CK(cudaStreamBeginCaptureToGraph(p->cs2, ibody, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
   g_launches = 0;
   enqueue_picard(p, p->cs2, h_picard, 1);
@@ -973,8 +1269,17 @@ int sgh_plan_create(const sgh_config* cfg, sgh_plan** out) {
     return fail(SGH_ERR_INVALID, "cell_integrated flux is only defined for the Gaussian (order 2)");
   const bool prop_corr = c.has_model && !c.model_constant;
   const bool latent = c.L_f > 0.0;
+  const bool box = c.box != 0;
   if (latent && !(c.has_model && !c.model_constant) && !(c.T_liquidus > c.T_solidus))
     return fail(SGH_ERR_INVALID, "latent heat with constant properties needs T_liquidus > T_solidus");
+  if (box) {
+    if (c.box_refinement < 1 || c.box_refinement > 64)
+      return fail(SGH_ERR_INVALID, "box_refinement must be in [1, 64]");
+    if (!(c.box_size[0] > 0 && c.box_size[1] > 0 && c.box_size[2] > 0))
+      return fail(SGH_ERR_INVALID, "box_size must be positive");
+    if (!prop_corr && !(c.T_liquidus > c.T_solidus))
+      return fail(SGH_ERR_INVALID, "box mode with constant properties needs T_liquidus > T_solidus");
+  }
   if (c.has_model) {
     const sgh_program* progs[6] = {&c.k_solid, &c.k_liquid, &c.rho_solid, &c.rho_liquid, &c.c_solid, &c.c_liquid};
     const char* names[6] = {"k_solid", "k_liquid", "rho_solid", "rho_liquid", "c_solid", "c_liquid"};
@@ -991,7 +1296,8 @@ int sgh_plan_create(const sgh_config* cfg, sgh_plan** out) {
   h.nx = c.nx; h.ny = c.ny; h.nz = c.nz;
   h.S = c.nx * c.ny;
   h.V = h.S * c.nz;
-  h.grid_latent = latent;
+  h.grid_latent = latent && !box;  // grid mode: no fine box (solvers/spectral.py:182-186)
+  h.box = box;
   h.prop_corr = prop_corr;
   h.latent_model = prop_corr;  // blended-rho source only for a non-constant model
   h.k_constant = c.k_constant;
@@ -1030,6 +1336,27 @@ int sgh_plan_create(const sgh_config* cfg, sgh_plan** out) {
   h.area_factor = c.area_factor;
   h.omega = c.omega;
   h.tol = c.tol;
+  if (box) {
+    // FineMeshState.__init__ (physics/spectral_state.py:189-227), in its operation order
+    const double r = (double)c.box_refinement;
+    h.dxf = h.dx / r; h.dyf = h.dy / r; h.dzf = h.dz / r;
+    const double fx = std::ceil(c.Lx / h.dxf), fy = std::ceil(c.Ly / h.dyf), fz = std::ceil(c.box_size[2] / h.dzf);
+    const double bx = std::ceil(c.box_size[0] / h.dxf), by = std::ceil(c.box_size[1] / h.dyf);
+    if (!(fx <= 65536 && fy <= 65536 && fz <= 65536))
+      return fail(SGH_ERR_INVALID, "fine box grid exceeds 65536 cells on an axis");
+    h.fx = (int)fx; h.fy = (int)fy; h.fz = (int)fz;
+    h.xb = std::min((int)bx, h.fx);
+    h.yb = std::min((int)by, h.fy);
+    h.zb = std::min((int)fz, h.fz);
+    h.dV_fine = h.dxf * h.dyf * h.dzf;
+    if (h.xb < 1 || h.yb < 1 || h.zb < 1) return fail(SGH_ERR_INVALID, "fine box is empty");
+    const long long nb = (long long)h.zb * h.yb * h.xb;
+    const long long lim = 1LL << 30;
+    if (nb > lim || (long long)(h.zb + 1) * h.S > lim || (long long)h.zb * h.ny * h.xb > lim ||
+        (long long)h.fx * h.nx > lim || (long long)h.fy * h.ny > lim)
+      return fail(SGH_ERR_INVALID, "fine box too large (a box array exceeds 2^30 elements)");
+    h.Nb = (int)nb;
+  }
   if (c.has_model) {
     h.prog[P_K_SOLID] = c.k_solid;
     h.prog[P_K_LIQUID] = c.k_liquid;
@@ -1085,7 +1412,26 @@ int sgh_plan_create(const sgh_config* cfg, sgh_plan** out) {
   p->o_prelax = L.take(sizeof(double) * 2 * std::max(p->nparts_relax, nparts_axis));
   p->o_plas = L.take(sizeof(double) * p->nparts_las);
   p->o_psurf = L.take(sizeof(double) * 2 * std::max(p->nparts_surf, axis_blocks(h.nz + 1, 1, h.S)));
-  p->face_space = !latent && !prop_corr;
+  p->face_space = !latent && !prop_corr && !box;
+  if (box) {
+    p->box_z0 = c.Lz - c.box_size[2];
+    const size_t B8 = sizeof(double) * (size_t)h.Nb;
+    p->o_bx = L.take(sizeof(double) * (size_t)h.fx * h.nx);
+    p->o_by = L.take(sizeof(double) * (size_t)h.fy * h.ny);
+    p->o_bzi = L.take(sizeof(double) * (size_t)(h.zb + 1) * h.nz);
+    p->o_bzf = L.take(sizeof(double) * (size_t)h.nz * h.zb);
+    p->o_wxi = L.take(sizeof(double) * (size_t)h.xb * h.nx);
+    p->o_wxf = L.take(sizeof(double) * (size_t)h.xb * h.nx);
+    p->o_wyi = L.take(sizeof(double) * (size_t)h.yb * h.ny);
+    p->o_wyf = L.take(sizeof(double) * (size_t)h.yb * h.ny);
+    p->o_bt1 = L.take(sizeof(double) * (size_t)(h.zb + 1) * h.S);
+    p->o_bt2 = L.take(sizeof(double) * (size_t)h.zb * h.ny * h.xb);
+    p->o_Qbox = L.take(B8);
+    p->o_Tpb = L.take(B8);
+    p->o_Qpb = L.take(B8);
+    p->o_Tsh = L.take(B8);
+    p->o_Qsh = L.take(B8);
+  }
   p->nparts_n1 = cdiv(h.S, EW_THREADS);
   p->nparts_fs = std::min(RELAX_BLOCKS_MAX, cdiv(h.S, EW_THREADS));
   p->o_fsF = L.take(S8 * 4);
@@ -1139,6 +1485,17 @@ int sgh_plan_bind(sgh_plan* p, void* workspace, uint64_t bytes, void* stream) {
   k_propagators<<<cdiv(h.V, EW_THREADS), EW_THREADS, 0, s>>>(p->P(), alpha, c.rho * c.cp, p->d(p->o_K),
                                                              p->d(p->o_KK));
   SGH_CK(cudaMemsetAsync(p->ws + p->o_Sbot, 0, sizeof(double) * h.S, s));
+  if (h.box) {
+    k_fine_basis<<<cdiv((long)h.fx * h.nx, EW_THREADS), EW_THREADS, 0, s>>>(h.nx, h.fx, c.Lx, h.dxf, 0.0,
+                                                                          p->d(p->o_bx), nullptr);
+    k_fine_basis<<<cdiv((long)h.fy * h.ny, EW_THREADS), EW_THREADS, 0, s>>>(h.ny, h.fy, c.Ly, h.dyf, 0.0,
+                                                                          p->d(p->o_by), nullptr);
+    k_fine_basis<<<cdiv((long)h.zb * h.nz, EW_THREADS), EW_THREADS, 0, s>>>(h.nz, h.zb, c.Lz, h.dzf, p->box_z0,
+                                                                          p->d(p->o_bzi), p->d(p->o_bzf));
+    // face row of the z reconstruction matrix: the top-surface weights
+    SGH_CK(cudaMemcpyAsync(p->d(p->o_bzi) + (size_t)h.zb * h.nz, p->d(p->o_ct), sizeof(double) * h.nz,
+                           cudaMemcpyDeviceToDevice, s));
+  }
   if (p->face_space)
     k_fs_weights<<<cdiv(h.S, EW_THREADS), EW_THREADS, 0, s>>>(p->P(), p->d(p->o_KK), p->d(p->o_ct),
                                                               p->d(p->o_cb), p->d(p->o_fsW));
@@ -1178,6 +1535,20 @@ int sgh_plan_buffer(const sgh_plan* p, int32_t which, void** ptr, uint64_t* byte
     case SGH_BUF_Q_MODES: off = p->o_Qm; n = V8; break;
     case SGH_BUF_SURFACE: off = p->o_Tsurf; n = S8; break;
     case SGH_BUF_SCRATCH: off = p->o_vol; n = V8; break;
+    case SGH_BUF_BOX_T_PREV:
+    case SGH_BUF_BOX_Q_PREV:
+    case SGH_BUF_BOX_BX:
+    case SGH_BUF_BOX_BY:
+    case SGH_BUF_BOX_BZ: {
+      const DevParams& h = p->hp;
+      if (!h.box) return fail(SGH_ERR_STATE, "box buffers exist in box mode only");
+      if (which == SGH_BUF_BOX_T_PREV) { off = p->o_Tpb; n = sizeof(double) * (size_t)h.Nb; }
+      else if (which == SGH_BUF_BOX_Q_PREV) { off = p->o_Qpb; n = sizeof(double) * (size_t)h.Nb; }
+      else if (which == SGH_BUF_BOX_BX) { off = p->o_bx; n = sizeof(double) * (size_t)h.fx * h.nx; }
+      else if (which == SGH_BUF_BOX_BY) { off = p->o_by; n = sizeof(double) * (size_t)h.fy * h.ny; }
+      else { off = p->o_bzi; n = sizeof(double) * (size_t)(h.zb + 1) * h.nz; }
+      break;
+    }
     default: return fail(SGH_ERR_INVALID, "unknown buffer id");
   }
   *ptr = p->ws + off;
@@ -1192,6 +1563,19 @@ int sgh_state_reset(sgh_plan* p, void* stream) {
   k_reset<<<cdiv(n, EW_THREADS), EW_THREADS, 0, s>>>(p->P(), p->ctrl(), p->d(p->o_a), p->d(p->o_Tprev),
                                                      p->d(p->o_qevold), p->d(p->o_qev), p->d(p->o_Qm));
   SGH_CK(cudaGetLastError());
+  if (p->hp.box) {
+    // no window yet: zero window bases (physics/spectral_state.py:221-225), no history
+    const DevParams& h = p->hp;
+    const size_t wx = sizeof(double) * (size_t)h.xb * h.nx, wy = sizeof(double) * (size_t)h.yb * h.ny;
+    const size_t B8 = sizeof(double) * (size_t)h.Nb;
+    SGH_CK(cudaMemsetAsync(p->ws + p->o_wxi, 0, wx, s));
+    SGH_CK(cudaMemsetAsync(p->ws + p->o_wxf, 0, wx, s));
+    SGH_CK(cudaMemsetAsync(p->ws + p->o_wyi, 0, wy, s));
+    SGH_CK(cudaMemsetAsync(p->ws + p->o_wyf, 0, wy, s));
+    SGH_CK(cudaMemsetAsync(p->ws + p->o_Tpb, 0, B8, s));
+    SGH_CK(cudaMemsetAsync(p->ws + p->o_Qpb, 0, B8, s));
+    SGH_CK(cudaMemsetAsync(p->ws + p->o_Qbox, 0, B8, s));
+  }
   return SGH_OK;
 }
 
@@ -1213,7 +1597,7 @@ int sgh_step_eager(sgh_plan* p, const sgh_laser* laser, sgh_step_out* out, void*
   if (!p->bound) return fail(SGH_ERR_STATE, "plan is not bound");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   k_run_setup<<<1, 1, 0, s>>>(p->ctrl(), *laser, nullptr, nullptr, 1);
-  enqueue_pre(p, s, 0, 0);
+  enqueue_pre(p, s);
   for (int it = 0; it < p->hp.max_iter; ++it) {
     enqueue_picard(p, s, 0, 0);
     int stop = 0;
@@ -1278,6 +1662,55 @@ int sgh_reconstruct_volume(sgh_plan* p, const double* modes, double* field, void
   if (!p->bound) return fail(SGH_ERR_STATE, "plan is not bound");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   volume_pass3(p, modes, true, EpiDiv{field, p->hp.sqrt_dV, nullptr}, p->d(p->o_t1), p->d(p->o_t2), s);
+  SGH_CK(cudaGetLastError());
+  return SGH_OK;
+}
+
+int sgh_box_geometry(const sgh_plan* p, sgh_box_geom* out) {
+  if (!p || !out) return fail(SGH_ERR_INVALID, "null argument");
+  const DevParams& h = p->hp;
+  if (!h.box) return fail(SGH_ERR_STATE, "plan is not in box mode");
+  out->n_box[0] = h.xb; out->n_box[1] = h.yb; out->n_box[2] = h.zb;
+  out->n_fine_total[0] = h.fx; out->n_fine_total[1] = h.fy; out->n_fine_total[2] = h.fz;
+  out->d_fine[0] = h.dxf; out->d_fine[1] = h.dyf; out->d_fine[2] = h.dzf;
+  out->dV_fine = h.dV_fine;
+  out->z0 = p->box_z0;
+  return SGH_OK;
+}
+
+int sgh_box_window(sgh_plan* p, int32_t* i0, void* stream) {
+  if (!p || !i0) return fail(SGH_ERR_INVALID, "null argument");
+  if (!p->bound) return fail(SGH_ERR_STATE, "plan is not bound");
+  if (!p->hp.box) return fail(SGH_ERR_STATE, "plan is not in box mode");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  int32_t w[2];
+  SGH_CK(cudaMemcpyAsync(&w[0], &p->ctrl()->box_i0x, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+  SGH_CK(cudaMemcpyAsync(&w[1], &p->ctrl()->box_i0y, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+  SGH_CK(cudaStreamSynchronize(s));
+  i0[0] = w[0];
+  i0[1] = w[1];
+  return SGH_OK;
+}
+
+int sgh_box_temperature(sgh_plan* p, const double* modes, double* out, void* stream) {
+  AxisPolicy policy(p ? p->cfg.axis_min_ctas : 0);
+  if (!p || !modes || !out) return fail(SGH_ERR_INVALID, "null argument");
+  if (!p->bound) return fail(SGH_ERR_STATE, "plan is not bound");
+  if (!p->hp.box) return fail(SGH_ERR_STATE, "plan is not in box mode");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  box_zpass(p, modes, false, s);
+  box_xy(p, EpiStore{out, 1.0, nullptr}, s);
+  SGH_CK(cudaGetLastError());
+  return SGH_OK;
+}
+
+int sgh_box_project(sgh_plan* p, const double* field_box, double* modes, void* stream) {
+  AxisPolicy policy(p ? p->cfg.axis_min_ctas : 0);
+  if (!p || !field_box || !modes) return fail(SGH_ERR_INVALID, "null argument");
+  if (!p->bound) return fail(SGH_ERR_STATE, "plan is not bound");
+  if (!p->hp.box) return fail(SGH_ERR_STATE, "plan is not in box mode");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  box_project(p, field_box, EpiStore{modes, p->hp.dV_fine, nullptr}, s);
   SGH_CK(cudaGetLastError());
   return SGH_OK;
 }

@@ -1068,7 +1068,7 @@ kb_commit(BView v, const double* part_las, const double* part_tile, int umma_til
     o.n_iter = st.iter;
     o.converged = st.status == SGH_STEP_CONVERGED ? 1 : 0;
     o.status = st.status;
-    o.pad = 0;
+    o.flags = 0;
     st.last = o;
     if (st.outs) st.outs[st.step] = o;
     st.iters += st.iter;
@@ -1329,6 +1329,8 @@ int sgh_batch_create(const sgh_config* cfgs, int32_t n, int32_t precision, sgh_b
       rc = bfail(SGH_ERR_INVALID, where + "max_iter must be in [0, 1e6]");
     else if (c.cell_integrated && c.order != 2.0)
       rc = bfail(SGH_ERR_INVALID, where + "cell_integrated flux is only defined for the Gaussian");
+    else if (c.box)
+      rc = bfail(SGH_ERR_UNSUPPORTED, where + "box mode (fine_mesh) runs on single-instance plans only");
     else if (c.L_f > 0.0 || (c.has_model && !c.model_constant) || c.h_top > 0.0 || c.h_bottom > 0.0)
       rc = bfail(SGH_ERR_UNSUPPORTED,
                  where + "batches step the face-space form only (no latent heat, no T-dependent model, "

@@ -20,6 +20,10 @@ struct DevParams {
   int grid_latent, prop_corr, latent_model, k_constant;
   int has_top_conv, has_bottom_conv, cell_integrated, max_iter;
   int degenerate_band;
+  // box mode (FineMeshState, physics/spectral_state.py:166-239): box extents
+  // xb, yb, zb (nx_box, ny_box, nz_box), fine-grid totals fx, fy, fz
+  // (n_fine_totals), Nb = zb yb xb
+  int box, xb, yb, zb, fx, fy, fz, Nb;
   int pad_i;
   double Lx, Ly, Lz, dx, dy, dz, inv_dx, inv_dy, inv_dz, dt, inv_dt;
   double dct_scale, recon_scale, sqrt_dV, n_elements;
@@ -30,6 +34,7 @@ struct DevParams {
   double L_f;
   double r_x, r_y, absorptivity, order, area_factor;
   double omega, tol;
+  double dxf, dyf, dzf, dV_fine;  // fine spacings and cell volume (box mode)
   int affine[P_COUNT];       // program reduces to aff_a + aff_b * T (host analysis)
   double aff_a[P_COUNT], aff_b[P_COUNT];
   sgh_program prog[P_COUNT];
@@ -46,6 +51,13 @@ struct Ctrl {
   double I0, shift_x, shift_y;  // peak intensity and warm-start shift (pixels)
   double rel_err;
   sgh_step_out out;         // metrics of the last step
+  // box mode: history present (FineMeshState.T_prev is not None), window
+  // start indices, history shift in fine pixels, and the magnitude maxima of
+  // the committed latent source (peak, floor, x edges, y edges) as the bit
+  // patterns of non-negative doubles (ordered like the values)
+  int have_tprev, box_i0x, box_i0y, pad_c;
+  double box_sx, box_sy;
+  unsigned long long box_max[4];
 };
 
 // ---------------------------------------------------------------------------

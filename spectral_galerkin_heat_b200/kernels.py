@@ -16,7 +16,11 @@ Functions with the reference kernel modules' names and meanings
   ``reconstruct_temperature_volume_at_points(a, num, geom, state, coords)``
   (:206-248) -> ``sgh_points_temperature``; ``save_temp_profiles(a, num, geom,
   state, laser_position, center, num_points)`` (:251-333) on top of them. The
-  results stay on the device (torch tensors); the reference returns NumPy.
+  results stay on the device (torch tensors); the reference returns NumPy;
+* box mode (``physics/spectral_ops.py``): ``reconstruct_temperature_box(a, state)``
+  (:173-179) -> ``sgh_box_temperature`` and ``project_box_to_modes(field_box,
+  state)`` (:53-74) -> ``sgh_box_project``, on the window of the last step;
+  both raise ``RuntimeError`` for a grid-mode state, as the reference does.
 
 ``state`` is the :class:`~spectral_galerkin_heat_b200.solver.B200State` returned
 by ``B200SpectralSolver.initialize``. The time step itself is not exposed
@@ -31,7 +35,7 @@ from . import _lib
 __all__ = ["DCT_II", "IDCT_II", "reconstruct_surface_temperature",
            "reconstruct_bottom_temperature", "reconstruct_volume", "project_volume",
            "reconstruct_temperature_DCT", "reconstruct_temperature_volume_at_points",
-           "save_temp_profiles"]
+           "save_temp_profiles", "reconstruct_temperature_box", "project_box_to_modes"]
 
 _scratch = {}
 
@@ -108,6 +112,41 @@ def project_volume(f, state):
     f = f.to(torch.float64).contiguous()
     out = torch.empty_like(f)
     _lib.check("sgh_project_volume", _lib.lib().sgh_project_volume(
+        state.plan, C.c_void_p(f.data_ptr()), C.c_void_p(out.data_ptr()),
+        C.c_void_p(state.stream.cuda_stream)))
+    return out
+
+
+def _fine_mesh(state):
+    fm = getattr(state, "fine_mesh", None)
+    if fm is None:
+        raise RuntimeError("Fine mesh not initialized.")
+    return fm
+
+
+def reconstruct_temperature_box(a, state):
+    """Temperature on the fine box at the current window, (nz_box, ny_box, nx_box)."""
+    import torch
+    fm = _fine_mesh(state)
+    a = a.to(torch.float64).contiguous()
+    if tuple(a.shape) != tuple(state.shape):
+        raise ValueError(f"modes shape {tuple(a.shape)} != {tuple(state.shape)}")
+    out = torch.empty(fm.box_shape, dtype=torch.float64, device=a.device)
+    _lib.check("sgh_box_temperature", _lib.lib().sgh_box_temperature(
+        state.plan, C.c_void_p(a.data_ptr()), C.c_void_p(out.data_ptr()),
+        C.c_void_p(state.stream.cuda_stream)))
+    return out
+
+
+def project_box_to_modes(field_box, state):
+    """Modes of a fine-box field: ``dV_fine`` times its contraction with the window bases."""
+    import torch
+    fm = _fine_mesh(state)
+    f = field_box.to(torch.float64).contiguous()
+    if tuple(f.shape) != fm.box_shape:
+        raise ValueError(f"box field shape {tuple(f.shape)} != {fm.box_shape}")
+    out = torch.empty(state.shape, dtype=torch.float64, device=f.device)
+    _lib.check("sgh_box_project", _lib.lib().sgh_box_project(
         state.plan, C.c_void_p(f.data_ptr()), C.c_void_p(out.data_ptr()),
         C.c_void_p(state.stream.cuda_stream)))
     return out

@@ -11,7 +11,10 @@ lifecycle (``solvers/base.py:31-91``):
 * Picard controls resolved as constructor argument > config > default
   (0.1 / 1e-4 / 30) (``solvers/spectral.py:107-123``); a one-time warning when
   a step hits the iteration cap (``:486-499``) and a one-time warning for the
-  grid-mode T-dependent configuration (``:210-216``).
+  grid-mode T-dependent configuration (``:210-216``);
+* grid mode (no ``fine_mesh``) and box mode (``fine_mesh``: latent heat on a
+  laser-following refined sub-box, ``state.fine_mesh`` mirroring
+  ``FineMeshState``), with the one-time box-truncation warning (``:545-586``).
 
 The whole step runs on the device (``libsgh_b200.so``): the host calls
 ``LaserPath.get_state(t, dt)``, hands the laser state to ``sgh_step`` and reads
@@ -37,7 +40,8 @@ from .properties import PropertyExpr
 
 logger = logging.getLogger(__name__)
 
-__all__ = ["HeatSolver", "B200SpectralSolver", "B200State", "make_config", "laser_struct"]
+__all__ = ["HeatSolver", "B200SpectralSolver", "B200State", "B200FineMesh", "make_config",
+           "laser_struct"]
 
 
 class HeatSolver(ABC):
@@ -111,6 +115,12 @@ def make_config(ctx, omega: float, tol: float, max_iter: int) -> _lib.SghConfig:
     c.cell_integrated = int(prof.cell_integrated)
     c.max_iter = int(max_iter)
     c.omega, c.tol = float(omega), float(tol)
+    fine = getattr(ctx, "fine", None)
+    if fine is not None:
+        c.box = 1
+        c.box_refinement = int(fine.refinement)
+        bs = fine.box_size
+        c.box_size[0], c.box_size[1], c.box_size[2] = float(bs[0]), float(bs[1]), float(bs[2])
     return c
 
 
@@ -142,6 +152,17 @@ class B200State:
         self.KK = self.buffer("KK")
         self.T_prev = self.buffer("T_prev")
         self.q_evap_old = self.buffer("q_evap_old")
+        self.fine_mesh = None
+
+    def raw_buffer(self, name):
+        """torch float64 1-D view of a named workspace buffer."""
+        torch = _torch()
+        ptr = C.c_void_p()
+        nbytes = C.c_uint64()
+        _lib.check("sgh_plan_buffer",
+                   _lib.lib().sgh_plan_buffer(self.plan, _lib.BUF[name], C.byref(ptr), C.byref(nbytes)))
+        off = ptr.value - self.workspace.data_ptr()
+        return self.workspace[off:off + nbytes.value].view(torch.float64)
 
     def buffer(self, name):
         """torch float64 view of a named workspace buffer."""
@@ -156,8 +177,58 @@ class B200State:
         return view.view(nz, ny, nx) if view.numel() == nz * ny * nx else view.view(ny, nx)
 
 
+class B200FineMesh:
+    """Fine box of a box-mode instance (``FineMeshState``, ``physics/spectral_state.py:166-239``).
+
+    Geometry attributes carry the reference's names and values; ``B_fine_full``
+    (cosine bases, modes x fine cells), ``T_prev`` and ``Q_prev`` are views of
+    the device workspace. The window follows the laser inside the step on the
+    device (``FineMeshState.update``); :meth:`window` reads its start indices.
+    ``T_prev`` and ``Q_prev`` are ``None`` until the first step, as in the
+    reference.
+    """
+
+    def __init__(self, state, fine):
+        g = _lib.SghBoxGeom()
+        _lib.check("sgh_box_geometry", _lib.lib().sgh_box_geometry(state.plan, C.byref(g)))
+        self._state = state
+        self.refinement = int(fine.refinement)
+        self.nx_box, self.ny_box, self.nz_box = (int(v) for v in g.n_box)
+        self.n_fine_totals = [int(v) for v in g.n_fine_total]
+        self.dx_fine, self.dy_fine, self.dz_fine = (float(v) for v in g.d_fine)
+        self.dV_fine = float(g.dV_fine)
+        self.z0 = float(g.z0)
+        self.box_shape = (self.nz_box, self.ny_box, self.nx_box)
+        self.coords_fine = [(np.arange(n) + 0.5) * d for n, d in
+                            zip(self.n_fine_totals, (self.dx_fine, self.dy_fine, self.dz_fine))]
+        nz, ny, nx = state.shape
+        fx, fy, _ = self.n_fine_totals
+        bx = state.raw_buffer("box_Bx").view(fx, nx)
+        by = state.raw_buffer("box_By").view(fy, ny)
+        bz = state.raw_buffer("box_Bz").view(self.nz_box + 1, nz)
+        self.B_fine_full = [bx.t(), by.t(), bz[:self.nz_box].t()]
+        self._T_prev = state.raw_buffer("box_T_prev").view(*self.box_shape)
+        self._Q_prev = state.raw_buffer("box_Q_prev").view(*self.box_shape)
+        self.primed = False
+
+    @property
+    def T_prev(self):
+        return self._T_prev if self.primed else None
+
+    @property
+    def Q_prev(self):
+        return self._Q_prev if self.primed else None
+
+    def window(self):
+        """``(i_start_x, i_start_y)`` of the last step's window; ``(-1, -1)`` before the first."""
+        w = (C.c_int32 * 2)()
+        _lib.check("sgh_box_window", _lib.lib().sgh_box_window(
+            self._state.plan, w, C.c_void_p(self._state.stream.cuda_stream)))
+        return int(w[0]), int(w[1])
+
+
 class B200SpectralSolver(HeatSolver):
-    """Spectral-Galerkin heat step on one B200 (FP64, grid mode)."""
+    """Spectral-Galerkin heat step on one B200 (FP64, grid or box mode)."""
 
     def __init__(self, backend=None, context=None, *, mixing_omega=None,
                  convergence_tol=None, max_picard_iter=None, device=None, axis_min_ctas=None):
@@ -175,6 +246,8 @@ class B200SpectralSolver(HeatSolver):
         self._picard_cap_warned = False
         self._property_correction = False
         self._grid_latent = False
+        self._latent_truncation_warned = False
+        self.last_flags = 0  # sgh_step_out.flags of the last step (box truncation bits)
 
     # ---- configuration -------------------------------------------------
     def _resolve_picard_params(self, dtype) -> None:
@@ -199,9 +272,6 @@ class B200SpectralSolver(HeatSolver):
             raise RuntimeError("SimulationContext must be provided either at construction "
                                "or in initialize().")
         ctx = self.context
-        if getattr(ctx, "fine", None) is not None:
-            raise NotImplementedError("box mode (fine_mesh) is not supported by the b200 "
-                                      "backend; remove the fine_mesh section (grid mode)")
         torch = _torch()
         if not torch.cuda.is_available():
             raise RuntimeError("the b200 backend needs a CUDA device (no CPU fallback)")
@@ -238,7 +308,11 @@ class B200SpectralSolver(HeatSolver):
         self._cfg = cfg
         model = getattr(ctx.mat, "model", None)
         self._property_correction = model is not None and not model.is_constant
-        self._grid_latent = float(getattr(ctx.mat, "L_f", 0.0)) > 0.0
+        fine = getattr(ctx, "fine", None)
+        self._grid_latent = fine is None and float(getattr(ctx.mat, "L_f", 0.0)) > 0.0
+        if fine is not None:
+            self.state.fine_mesh = B200FineMesh(self.state, fine)
+        self._latent_truncation_warned = False
         if self._property_correction and self._grid_latent:
             logger.warning(
                 "Temperature-dependent run in grid mode (no fine_mesh): the sharp latent-heat "
@@ -255,19 +329,47 @@ class B200SpectralSolver(HeatSolver):
         """One time step. ``eager=True`` launches the same kernels one by one with
         the Picard loop driven from the host (for profilers and debugging)."""
         self._require()
+        self._check_box_dt(dt)
         st = self.context.laser_path.get_state(t, dt)
         laser = laser_struct(st, dt, self._cfg.dt)
         out = _lib.SghStepOut()
         fn = "sgh_step_eager" if eager else "sgh_step"
         _lib.check(fn, getattr(_lib.lib(), fn)(self._plan, C.byref(laser), C.byref(out),
                                                C.c_void_p(self.state.stream.cuda_stream)))
+        if self.state.fine_mesh is not None:
+            self.state.fine_mesh.primed = True
         metrics = self._metrics(out, t)
         if self.track_picard_history:
             self.picard_history = [{"iter": metrics["n_evap_iter"] - 1, "rms_diff": None,
                                     "rho": None, "true_rel_err": metrics["picard_rel_err"]}]
         return self.state, metrics
 
+    def _check_box_dt(self, dt) -> None:
+        # The box history moves by v * num.dt (physics/spectral_ops.py:300-302)
+        # while the face warm start moves by v * dt; the library shifts both by
+        # v * dt of the plan, so box mode steps at the configured dt only.
+        if self.state.fine_mesh is not None and float(dt) != float(self._cfg.dt):
+            raise ValueError(f"box mode steps at the configured dt={self._cfg.dt!r} only "
+                             f"(got dt={dt!r})")
+
+    def _box_warning(self, flags) -> None:
+        """One-time truncation warning (``solvers/spectral.py:545-586``)."""
+        if not flags or self._latent_truncation_warned:
+            return
+        fm = self.state.fine_mesh
+        hit = [name for bit, name in sorted(_lib.STEP_FLAGS.items()) if flags & bit]
+        box_mm = (fm.nx_box * fm.dx_fine * 1e3, fm.ny_box * fm.dy_fine * 1e3,
+                  fm.nz_box * fm.dz_fine * 1e3)
+        logger.warning(
+            "Latent-heat source reaches the fine-mesh box boundary (%s): the melt pool extends "
+            "beyond the refined sub-box, so its latent heat is truncated. Enlarge "
+            "fine_mesh.box_size (currently %.3g x %.3g x %.3g mm) to enclose the pool.",
+            ", ".join(hit), *box_mm)
+        self._latent_truncation_warned = True
+
     def _metrics(self, out, t):
+        self.last_flags = int(out.flags)
+        self._box_warning(self.last_flags)
         conv = bool(out.converged)
         if not conv and out.n_iter > 0 and not self._picard_cap_warned:
             self._picard_cap_warned = True
@@ -291,6 +393,7 @@ class B200SpectralSolver(HeatSolver):
         self._require()
         torch = _torch()
         dt = self._cfg.dt if dt is None else dt
+        self._check_box_dt(dt)
         n = int(n_steps)
         if n <= 0:
             return []
@@ -324,6 +427,8 @@ class B200SpectralSolver(HeatSolver):
         lsz, osz = C.sizeof(_lib.SghLaser), C.sizeof(_lib.SghStepOut)
         if table.numel() < (start + n) * lsz or outs.numel() < (start + n) * osz:
             raise ValueError("laser or metrics table too short")
+        if self.state.fine_mesh is not None and n > 0:
+            self.state.fine_mesh.primed = True
         _lib.check("sgh_run", _lib.lib().sgh_run(
             self._plan, C.c_void_p(table.data_ptr() + start * lsz), int(n),
             C.c_void_p(outs.data_ptr() + start * osz), C.c_void_p(self.state.stream.cuda_stream)))
@@ -385,6 +490,9 @@ class B200SpectralSolver(HeatSolver):
         self._require()
         _lib.check("sgh_state_reset", _lib.lib().sgh_state_reset(
             self._plan, C.c_void_p(self.state.stream.cuda_stream)))
+        if self.state.fine_mesh is not None:
+            self.state.fine_mesh.primed = False
+        self._latent_truncation_warned = False
 
     def finalize(self) -> None:
         if self._plan is not None:

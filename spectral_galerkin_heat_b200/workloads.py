@@ -41,7 +41,7 @@ import numpy as np
 from .laser import RasterPath, StraightTrack
 
 __all__ = ["MATERIAL_316L", "straight_track", "nonlinear_raster", "precision_track",
-           "uneven_batch", "serving_stream", "serving_config", "scaled"]
+           "uneven_batch", "serving_stream", "serving_config", "scaled", "box_track"]
 
 MATERIAL_316L = {
     "name": "316L", "rho": 7900.0, "k": 20.0, "Cp": 500.0, "L_f": 0.0,
@@ -89,6 +89,27 @@ def nonlinear_raster(nx=128, ny=64, nz=32, steps=1000, dt=2e-6, seed=0,
     x_start = 0.5 * size[0] - 0.5 * line_length + jx
     y_start = 0.5 * size[1] - 0.5 * (n_lines - 1) * hatch + jy
     return cfg, RasterPath(x_start, y_start, line_length, hatch, n_lines, speed, power)
+
+
+def box_track(nx=80, ny=48, nz=120, steps=140, dt=5e-6, size=(0.6e-3, 0.4e-3, 0.15e-3),
+              refinement=2, box_size=(0.6e-3, 0.6e-3, 0.07e-3), x0=0.15e-3, y0=None,
+              speed=0.4, power=120.0):
+    """Box-mode single track with latent heat and bottom convection (the layout of
+    the reference's example 02, ``simulations/examples/02_single_track.yaml``):
+    constant 316L properties at 293 K, Picard at the reference defaults, latent
+    heat on a laser-following fine box; ``(cfg, path)``."""
+    cfg = {
+        "simulation": {"backend": "b200", "dtype": "float64", "dt": dt, "duration": steps * dt},
+        "domain": {"size": list(size), "mesh": [nx, ny, nz]},
+        "fine_mesh": {"refinement": refinement, "box_size": list(box_size)},
+        "material": {"name": "316L", "rho": 7957.5, "k": 13.851, "Cp": 497.89, "L_f": 2.677e5,
+                     "T_solidus": 1674.15, "T_liquidus": 1697.15, "T0": 293.0,
+                     "h_conv_bottom": 3000.0, "DeltaH_LV": 7.416e6, "R_v": 150.774,
+                     "Pa": 101325.0, "T_boil": 3090.0},
+        "laser": {"radius": 60e-6, "absorptivity": 0.30, "power_nominal": power},
+    }
+    y = size[1] / 2.0 if y0 is None else y0
+    return cfg, StraightTrack(x0, y, speed, 0.0, power)
 
 
 def precision_track(seed=0, nx=256, ny=128, nz=64, steps=500, dt=5e-6):

@@ -111,6 +111,32 @@ def cases():
     cfg, _ = W.straight_track(nx=8, ny=6, nz=4, steps=3)
     path = FixedLaser(1e-3, 0.5e-3, 200.0, is_on=False)
     out["laser_off_8x6x4"] = (cfg, path, 3, [3], None)
+    # box mode, constant properties: a window narrower than the domain in x and
+    # y, sliding diagonally (non-integer history shifts), partial depth
+    cfg, _ = W.straight_track(nx=24, ny=12, nz=8, steps=8, dt=2e-6,
+                              size=(0.6e-3, 0.3e-3, 0.15e-3))
+    cfg["material"]["L_f"] = 2.7e5
+    cfg["simulation"].update({"max_picard_iter": 400, "picard_omega": 0.1, "picard_tol": 1e-8})
+    cfg["fine_mesh"] = {"refinement": 2, "box_size": [0.2e-3, 0.15e-3, 0.05e-3]}
+    path = StraightTrack(0.2e-3, 0.13e-3, 2.0, 1.0, 220.0)
+    out["box_const_24x12x8"] = (cfg, path, 8, [1, 8], None)
+    # a box too shallow and narrow for the pool: the truncation warning fires
+    cfg = copy.deepcopy(cfg)
+    cfg["fine_mesh"] = {"refinement": 2, "box_size": [0.06e-3, 0.2e-3, 0.02e-3]}
+    cfg["simulation"]["duration"] = 5 * 2e-6
+    out["box_shallow_24x12x8"] = (cfg, path, 5, [5], None)
+    # box mode with the T-dependent model (property correction) and convection
+    cfg, path = W.nonlinear_raster(nx=16, ny=12, nz=8, size=(0.4e-3, 0.3e-3, 0.1e-3),
+                                   line_length=0.1e-3, hatch=25e-6, steps=6)
+    cfg["fine_mesh"] = {"refinement": 3, "box_size": [0.15e-3, 0.1e-3, 0.04e-3]}
+    out["box_tdep_16x12x8"] = (cfg, path, 6, [6], None)
+    # box mode at refinement 1 over the whole domain (the equivalence with grid
+    # mode that the reference tests), bottom convection, laser at rest
+    cfg, path = W.box_track(nx=20, ny=12, nz=30, steps=6, size=(0.6e-3, 0.4e-3, 0.15e-3),
+                            refinement=1, box_size=(0.6e-3, 0.4e-3, 0.15e-3),
+                            x0=0.3e-3, y0=0.2e-3, speed=0.0)
+    cfg["simulation"]["max_picard_iter"] = 80
+    out["box_full_r1_20x12x30"] = (cfg, path, 6, [6], None)
     return out
 
 
@@ -131,10 +157,12 @@ def run_case(name, spec, Ctx, Solver, Numpy):
     files = {}
     worst = 0.0
     t0 = time.time()
+    box_flags = []
     for i in range(steps):
         t = i * dt
         _, m = ref.step(t, dt)
         _, mo = orc.step(t, dt)
+        box_flags.append(orc.box_flags)
         for k in rec:
             rec[k].append(float(m[k]))
         a = np.array(ref.state.a, dtype=np.float64, copy=True)
@@ -150,6 +178,25 @@ def run_case(name, spec, Ctx, Solver, Numpy):
                 orc.surface_T(a, top=True), dtype=np.float64)
     for k, v in rec.items():
         files[f"metric_{k}"] = np.asarray(v)
+    fm = getattr(ref.state, "fine_mesh", None)
+    if fm is not None:
+        # box history and window bases after the last step
+        T_ref, Q_ref = np.asarray(fm.T_prev, np.float64), np.asarray(fm.Q_prev, np.float64)
+        relT = float(np.linalg.norm(orc.box.T_prev - T_ref) / np.linalg.norm(T_ref))
+        scaleQ = max(float(np.max(np.abs(Q_ref))), 1e-300)
+        errQ = float(np.max(np.abs(orc.box.Q_prev - Q_ref))) / scaleQ
+        for a in range(2):
+            assert np.array_equal(np.asarray(fm.B_fine[a]), orc.box.B_fine[a]), f"{name}: window {a}"
+        assert relT < 1e-12 and errQ < 1e-9, f"{name}: box history differs: {relT} {errQ}"
+        worst = max(worst, relT)
+        files["box_T_prev"] = T_ref
+        files["box_Q_prev"] = Q_ref
+        files["box_window"] = np.array(orc.box.window)
+        warned = bool(ref._latent_truncation_warned)
+        assert warned == any(box_flags), f"{name}: truncation check differs"
+        files["box_truncation_warned"] = np.array(warned)
+        files["box_flags"] = np.array(box_flags, dtype=np.int32)
+        files["box_shape"] = np.array(orc.box.shape)
     import numba
     import scipy
     files["meta"] = np.array(str({

@@ -28,7 +28,7 @@ def test_library_loads_and_exports_every_declared_symbol():
     for n in names:
         assert hasattr(L, n), n
     assert sorted(_lib.EXPORTED) == names
-    assert L.sgh_abi_version() == 2
+    assert L.sgh_abi_version() == _lib.ABI_VERSION == 3
 
 
 def test_struct_layout_matches_header():
@@ -36,6 +36,7 @@ def test_struct_layout_matches_header():
     structs = {
         "sgh_config": _lib.SghConfig, "sgh_laser": _lib.SghLaser,
         "sgh_step_out": _lib.SghStepOut, "sgh_program": _lib.SghProgram,
+        "sgh_box_geom": _lib.SghBoxGeom,
     }
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "sgh_b200.h"', "int main(void){"]
     for cname, py in structs.items():

@@ -11,8 +11,9 @@ from oracle.sgh_oracle import OracleSolver, dct2, dct3, dct_matrix
 # in library summation order, so the bound is a few ulps times the step count.
 TOL_ORACLE = 1e-12
 
+BOX_CASES = ["box_const_24x12x8", "box_shallow_24x12x8", "box_tdep_16x12x8", "box_full_r1_20x12x30"]
 CASES = ["track_64x32x16", "raster_32x16x8", "odd_13x10x6_conv", "latent_const_24x12x8",
-         "supergauss_20x18x5", "laser_off_8x6x4", "raster_128x64x32"]
+         "supergauss_20x18x5", "laser_off_8x6x4", "raster_128x64x32"] + BOX_CASES
 
 
 def _run_oracle(name, upto=None):
@@ -24,11 +25,15 @@ def _run_oracle(name, upto=None):
     n = steps if upto is None else upto
     metrics = []
     snap_modes = {}
+    flags = []
     for i in range(n):
         _, m = o.step(i * ctx.num.dt, ctx.num.dt)
         metrics.append(m)
+        flags.append(o.box_flags)
         if (i + 1) in snaps:
             snap_modes[i + 1] = o.a.copy()
+    if o.box is not None:
+        snap_modes["box"] = (o.box, flags)
     return g, metrics, snap_modes, block
 
 
@@ -36,6 +41,16 @@ def _run_oracle(name, upto=None):
 def test_oracle_matches_reference_fixture(name):
     upto = 60 if name == "track_64x32x16" else None
     g, metrics, snaps, block = _run_oracle(name, upto)
+    box = snaps.pop("box", None)
+    if box is not None:
+        fb, flags = box
+        # box history, window and truncation flags after the last step
+        assert tuple(g["box_shape"]) == fb.shape
+        assert tuple(g["box_window"]) == fb.window
+        assert rel_l2(fb.T_prev, g["box_T_prev"]) < TOL_ORACLE
+        assert np.max(np.abs(fb.Q_prev - g["box_Q_prev"])) <= 1e-9 * np.max(np.abs(g["box_Q_prev"]))
+        np.testing.assert_array_equal(flags, g["box_flags"])
+        assert bool(g["box_truncation_warned"]) == any(flags)
     for step, a in snaps.items():
         ref = g[f"modes_step{step}"]
         got = a if block is None else a[:block[0], :block[1], :block[2]]
