@@ -69,6 +69,9 @@ NCU_VOLUME_TRAFFIC_PER_MODE = 449.26e6 / 38993920
 # the raster workload's dominant kernel (k_axis) was captured on the same
 # 128x64x32 case: 2.14 MB for one contiguous-axis pass (field resident in L2)
 NCU_TRAFFIC_BYTES = 2.14e6
+# the box workload's box passes (one reconstruction + one projection) from an
+# ncu capture of the same case; None until captured
+NCU_BOX_TRAFFIC_BYTES = None
 
 
 def reduce_over_ranks(times_ms, counts, device="cpu"):
@@ -101,6 +104,14 @@ def _workload(name, seed):
                 "picard_omega": 0.1, "picard_cap": 400, "latent": "grid",
                 "properties": "k(T), c_p(T) linear", "surface": "evaporation + convection",
                 "path": "5-line raster, 0.4 mm lines, 100 um hatch, 1 m/s", "seed": seed}
+    elif name == "box":
+        cfg, path = workloads.box_track()
+        desc = {"workload": "box_track_fp64", "modes": [80, 48, 120],
+                "domain_mm": [0.6, 0.4, 0.15], "dt_s": 5e-6, "latent": "box",
+                "box": {"refinement": 2, "size_mm": [0.6, 0.6, 0.07], "cells": [160, 96, 112]},
+                "picard": "reference defaults (omega 0.1, tol 1e-4, cap 30)",
+                "properties": "constant 316L (293 K)", "surface": "evaporation + bottom convection",
+                "path": "straight, 0.4 m/s, 120 W"}
     elif name == "track":
         cfg, path = workloads.straight_track()
         desc = {"workload": "straight_track_fp64", "modes": [64, 32, 16],
@@ -289,7 +300,7 @@ def run_b200(args, rank, world, local_rank):
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
 
     # ---- device-resident throughput -----------------------------------------
-    s = B200SpectralSolver(None, _context(cfg, path))
+    s = B200SpectralSolver(None, _context(cfg, path), axis_cuda_cores=args.axis_cuda_cores)
     s.initialize()
     table = s.laser_table(0.0, W + K)
     osz = C.sizeof(_lib.SghStepOut)
@@ -319,33 +330,15 @@ def run_b200(args, rank, world, local_rank):
     launches = sum(pre + post + n * per_it for n in iters)
     statuses = sorted({_lib.STEP_STATUS.get(r.status, r.status) for r in recs})
 
-    # ---- dominant kernel, timed live: DCT axis passes of one 3-D transform ----
-    R = 20
-    src = torch.randn(s.state.shape, dtype=torch.float64, device=dev)
-    dst = torch.empty_like(src)
-    kev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-           for _ in range(R)]
-    for i in range(R + 2):
-        flush.fill_(i & 0xFF)
-        if i >= 2:
-            kev[i - 2][0].record(stream)
-        _lib.check("sgh_dct3d", _lib.lib().sgh_dct3d(
-            s._plan, 3, C.c_void_p(src.data_ptr()), C.c_void_p(dst.data_ptr()),
-            C.c_void_p(stream.cuda_stream)))
-        if i >= 2:
-            kev[i - 2][1].record(stream)
-    torch.cuda.synchronize()
-    per_transform_ms = sum(a.elapsed_time(b) for a, b in kev) / R
-    nz, ny, nx = s.state.shape
-    V = nx * ny * nz
-    # algorithmic bytes of one axis pass: read the field once, write it once (FP64)
-    bytes_per_pass = 2 * V * 8
-    achieved_gbs = bytes_per_pass / (per_transform_ms / 3 * 1e-3) / 1e9
-    peak, peak_kind = _peaks()
-    s.finalize()
+    if args.workload == "box":
+        roof = _box_roofline(s, flush, stream, dev)
+        s.finalize()
+    else:
+        roof = _axis_roofline(s, flush, stream, dev)
+        s.finalize()
 
     # ---- end to end through the public API ----------------------------------
-    e = B200SpectralSolver(None, _context(cfg, path))
+    e = B200SpectralSolver(None, _context(cfg, path), axis_cuda_cores=args.axis_cuda_cores)
     e.initialize()
     dt = e.context.num.dt
     for i in range(W):
@@ -376,6 +369,8 @@ def run_b200(args, rank, world, local_rank):
         "data": "synthetic (seeded laser path; no dataset)",
         "config": dict(desc, parallelism=f"replicas x{world}" if world > 1 else "single",
                        l2="flushed between timed steps (256 MB write)",
+                       axis_kernels="CUDA-core FP64" if args.axis_cuda_cores
+                       else "FP64 tensor cores (mma.sync .f64) where the pass is large enough",
                        picard_iters_mean=float(np.mean(iters)), step_status=statuses),
         "clocks": clocks,
         "gpu_launches": launches * world,
@@ -383,13 +378,7 @@ def run_b200(args, rank, world, local_rank):
                 "h2d_bytes_per_step": C.sizeof(_lib.SghLaser),
                 "d2h_bytes_per_step": C.sizeof(_lib.SghStepOut),
                 "api": "B200SpectralSolver.step(t, dt)"},
-        "roofline": {"kernel": "k_axis (DCT axis pass, FP64)", "bound": "hbm",
-                     "achieved": achieved_gbs, "peak": peak, "unit": "GB/s",
-                     "frac": achieved_gbs / peak, "peak_source": peak_kind,
-                     "traffic": NCU_TRAFFIC_BYTES,
-                     "algorithmic_bytes_per_launch": bytes_per_pass,
-                     "fp64_tflops": (2.0 * V * (nx + ny + nz) / 3)
-                     / (per_transform_ms / 3 * 1e-3) / 1e12},
+        "roofline": roof,
     }
     if world == 1 and not args.no_cpu_baseline:
         v, n, el = cpu_baseline(cfg, path, budget_s=args.cpu_budget)
@@ -398,6 +387,109 @@ def run_b200(args, rank, world, local_rank):
                                 "sample": f"{n} steps from t=dt of the same workload "
                                           f"({el:.1f} s), after 1 warm-up step"}
     return line
+
+
+def _fp64_peak(dev, n=4096, reps=10):
+    """Measured FP64 matrix peak of this GPU: cuBLAS DGEMM (torch.matmul on
+    float64) of n^3, best of ``reps``, CUDA events; TFLOP/s."""
+    import torch
+    a = torch.randn(n, n, dtype=torch.float64, device=dev)
+    b = torch.randn(n, n, dtype=torch.float64, device=dev)
+    c = torch.matmul(a, b)
+    best = float("inf")
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b, out=c)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    del a, b, c
+    return 2.0 * n ** 3 / (best * 1e-3) / 1e12
+
+
+def _box_roofline(s, flush, stream, dev):
+    """The box passes (reconstruction z, x, y and projection y, x, z of the
+    latent source; FP64 contractions, compute-bound) timed alone with CUDA
+    events at the window of the last step, against the measured DGEMM peak."""
+    import ctypes as C
+
+    import torch
+
+    from spectral_galerkin_heat_b200 import _lib
+    fm = s.state.fine_mesh
+    nz, ny, nx = s.state.shape
+    zb, yb, xb = fm.box_shape
+    S = nx * ny
+    # multiply-adds of one reconstruction in the pass order z, x, y (a projection
+    # is the same contraction in reverse)
+    fma = nz * S * zb + zb * ny * nx * xb + zb * ny * xb * yb
+    flops = 2.0 * 2 * fma
+    a = torch.randn(s.state.shape, dtype=torch.float64, device=dev)
+    box = torch.empty(fm.box_shape, dtype=torch.float64, device=dev)
+    modes = torch.empty_like(a)
+    R = 20
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(R)]
+    L = _lib.lib()
+    for i in range(R + 2):
+        flush.fill_(i & 0xFF)
+        if i >= 2:
+            ev[i - 2][0].record(stream)
+        _lib.check("sgh_box_temperature", L.sgh_box_temperature(
+            s._plan, C.c_void_p(a.data_ptr()), C.c_void_p(box.data_ptr()), C.c_void_p(stream.cuda_stream)))
+        _lib.check("sgh_box_project", L.sgh_box_project(
+            s._plan, C.c_void_p(box.data_ptr()), C.c_void_p(modes.data_ptr()), C.c_void_p(stream.cuda_stream)))
+        if i >= 2:
+            ev[i - 2][1].record(stream)
+    torch.cuda.synchronize()
+    ms = sum(x.elapsed_time(y) for x, y in ev) / R
+    achieved = flops / (ms * 1e-3) / 1e12
+    peak = _fp64_peak(dev)
+    return {"kernel": "k_axis box passes (reconstruction + projection, FP64)", "bound": "fp64",
+            "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+            "peak_source": "measured here: cuBLAS DGEMM 4096^3, best of 10",
+            "traffic": NCU_BOX_TRAFFIC_BYTES, "algorithmic_flops_per_launch": flops,
+            "launches": 6, "ms_per_pair": ms,
+            # bytes each pass reads and writes once, both directions
+            "hbm_gbs_algorithmic": 8.0 * 2 * (nz * S + 2 * zb * S + 2 * zb * ny * xb + zb * yb * xb)
+            / (ms * 1e-3) / 1e9}
+
+
+def _axis_roofline(s, flush, stream, dev):
+    """DCT axis passes of one 3-D transform, timed alone (HBM-bound)."""
+    import ctypes as C
+
+    import torch
+
+    from spectral_galerkin_heat_b200 import _lib
+    R = 20
+    src = torch.randn(s.state.shape, dtype=torch.float64, device=dev)
+    dst = torch.empty_like(src)
+    kev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(R)]
+    for i in range(R + 2):
+        flush.fill_(i & 0xFF)
+        if i >= 2:
+            kev[i - 2][0].record(stream)
+        _lib.check("sgh_dct3d", _lib.lib().sgh_dct3d(
+            s._plan, 3, C.c_void_p(src.data_ptr()), C.c_void_p(dst.data_ptr()),
+            C.c_void_p(stream.cuda_stream)))
+        if i >= 2:
+            kev[i - 2][1].record(stream)
+    torch.cuda.synchronize()
+    per_transform_ms = sum(a.elapsed_time(b) for a, b in kev) / R
+    nz, ny, nx = s.state.shape
+    V = nx * ny * nz
+    # algorithmic bytes of one axis pass: read the field once, write it once (FP64)
+    bytes_per_pass = 2 * V * 8
+    achieved_gbs = bytes_per_pass / (per_transform_ms / 3 * 1e-3) / 1e9
+    peak, peak_kind = _peaks()
+    return {"kernel": "k_axis (DCT axis pass, FP64)", "bound": "hbm",
+            "achieved": achieved_gbs, "peak": peak, "unit": "GB/s",
+            "frac": achieved_gbs / peak, "peak_source": peak_kind,
+            "traffic": NCU_TRAFFIC_BYTES,
+            "algorithmic_bytes_per_launch": bytes_per_pass,
+            "fp64_tflops": (2.0 * V * (nx + ny + nz) / 3) / (per_transform_ms / 3 * 1e-3) / 1e12}
 
 
 def _serving_desc(args):
@@ -631,9 +723,10 @@ def run_profile(args):
 
     ``serving-step``: the serving engine as in the benchmark (slots per class
     from --max-slots), every slot filled from the saturated stream, then
-    --steps eager batched steps and three volume passes. ``raster-step``: the
-    nonlinear raster workload through ``B200SpectralSolver.step(eager=True)``
-    for --warmup + --steps steps. Prints one line; no timing."""
+    --steps eager batched steps and three volume passes. ``raster-step`` /
+    ``box-step``: the nonlinear raster / box workload through
+    ``B200SpectralSolver.step(eager=True)`` for --warmup + --steps steps.
+    Prints one line; no timing."""
     import copy
 
     import torch
@@ -655,9 +748,9 @@ def run_profile(args):
         print(json.dumps({"profile": args.profile, "precision": args.precision, "slots": eng.memory["slots"],
                           "active_modes": eng.batch.active_modes(), "workspace_gb": eng.batch.workspace_bytes / 1e9}))
         eng.close()
-    elif args.profile == "raster-step":
+    elif args.profile in ("raster-step", "box-step"):
         from spectral_galerkin_heat_b200 import B200SpectralSolver
-        cfg, path, desc = _workload("raster", seed=0)
+        cfg, path, desc = _workload(args.profile.split("-")[0], seed=0)
         s = B200SpectralSolver(None, _context(cfg, path))
         s.initialize()
         dt = s.context.num.dt
@@ -901,8 +994,11 @@ def main():
                     help="timed steps (serving: batched steps, default 1000; otherwise 200)")
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
-    ap.add_argument("--workload", choices=["serving", "batch", "raster", "track", "outputs"], default="serving")
+    ap.add_argument("--workload", choices=["serving", "batch", "raster", "track", "box", "outputs"],
+                    default="serving")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--axis-cuda-cores", action="store_true",
+                    help="raster/track/box: FP64 axis passes on the CUDA-core kernels only")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--requests", type=int, default=600, help="serving: saturated stream length")
     ap.add_argument("--max-slots", type=int, default=16, help="serving: slots per grid class at most")
@@ -911,7 +1007,7 @@ def main():
     ap.add_argument("--plain-steps", type=int, default=300)
     ap.add_argument("--cpu-steps-per-request", type=int, default=20)
     ap.add_argument("--accuracy-steps", type=int, default=100)
-    ap.add_argument("--profile", choices=["serving-step", "raster-step"], default=None,
+    ap.add_argument("--profile", choices=["serving-step", "raster-step", "box-step"], default=None,
                     help="launch the step kernels one by one for a profiler and exit (no timing)")
     ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed", help="--profile serving-step")
     args = ap.parse_args()

@@ -100,7 +100,9 @@ typedef struct {
    * least this many CTAs, else 1 x 1 tiles; 0 = the built-in default (132).
    * Chosen per (nx, ny, nz) by the autotuner (autotune.py). Batches ignore it. */
   int32_t axis_min_ctas;
-  int32_t pad1;
+  /* 0: passes large enough run on the FP64 tensor cores (mma.sync .f64);
+   * 1: every pass runs on the CUDA-core FP64 kernels (for comparison). */
+  int32_t axis_cuda_cores;
   /* Laser-following refined sub-box (FineMeshParams, core/parameters.py:391-410;
    * FineMeshState, physics/spectral_state.py:166-239). box = 1 selects box
    * mode: the latent-heat source is evaluated on a fine box of

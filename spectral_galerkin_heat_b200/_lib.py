@@ -69,7 +69,7 @@ class SghConfig(C.Structure):
         ("order", C.c_double), ("area_factor", C.c_double),
         ("cell_integrated", C.c_int32), ("max_iter", C.c_int32),
         ("omega", C.c_double), ("tol", C.c_double),
-        ("axis_min_ctas", C.c_int32), ("pad1", C.c_int32),
+        ("axis_min_ctas", C.c_int32), ("axis_cuda_cores", C.c_int32),
         ("box", C.c_int32), ("box_refinement", C.c_int32), ("box_size", C.c_double * 3),
     ]
 

@@ -179,36 +179,288 @@ k_axis(const double* __restrict__ X, const double* __restrict__ Mat, int Nout, i
   }
 }
 
-// Launch shape of one pass: the 2 x 4 thread tile when it yields enough CTAs
-// to cover the SMs, else the 1 x 1 tile (small faces, short axes).
+// ---------------------------------------------------------------------------
+// FP64 tensor-core variant: mma.sync m16n8k8 .f64 (the FP64 MMA of sm_90+,
+// kept on sm_100a; tcgen05 has no FP64 kind). CTA tile AXM_BM (outputs along
+// the transformed axis) x BN (columns c), 8 warps as 2 x 4, warp tile 32 x BN/4
+// = 2 m16 x BN/32 n8 MMA tiles per k8 step. Mat and X tiles stream through an
+// AXM_STAGES-deep cp.async pipeline of AXM_BK slices. Shared layouts keep the
+// fragment reads and the cp.async writes free of bank conflicts: Mat tiles
+// k-major rows of AXM_BK + 4 doubles; X tiles column-major (rows of AXM_BK + 4)
+// when the contraction axis is the contiguous one (B == 1), else n-major rows
+// of BN + 4. Each thread's source columns are fixed across stages, so their
+// offsets are computed once.
+// ---------------------------------------------------------------------------
+constexpr int AXM_BM = 64;
+constexpr int AXM_BK = 16;
+constexpr int AXM_STAGES = 3;
+constexpr int AXM_LDK = AXM_BK + 4;  // rows of AXM_BK contraction slices
+
+template <bool CONTIG, int BN>
+constexpr int axm_stage_doubles() {
+  return AXM_BM * AXM_LDK + (CONTIG ? BN * AXM_LDK : AXM_BK * (BN + 4));
+}
+template <bool CONTIG, int BN>
+constexpr int axm_smem_bytes() {
+  return AXM_STAGES * axm_stage_doubles<CONTIG, BN>() * (int)sizeof(double);
+}
+
+__device__ __forceinline__ void mma_f64_m16n8k8(double (&d)[4], const double (&a)[4], const double (&b)[2]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+      : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
+}
+
+template <bool CONTIG, int BN, class Epi>
+__global__ void __launch_bounds__(AX_THREADS)
+k_axis_mma(const double* __restrict__ X, const double* __restrict__ Mat, int Nout, int N, int A, int B,
+           Epi epi) {
+  extern __shared__ __align__(16) double axm_sh[];
+  constexpr int STAGE = axm_stage_doubles<CONTIG, BN>();
+  constexpr int LDX = CONTIG ? AXM_LDK : BN + 4;
+  constexpr int NT = BN / 32;           // n8 tiles per warp
+  constexpr int XPT = BN * AXM_BK / AX_THREADS;  // X elements per thread per stage
+  __shared__ double red_sh[2 * (AX_THREADS / 32)];
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int wm = warp >> 2, wn = warp & 3;
+  const int ncol = A * B;
+  const int c0 = blockIdx.x * BN, k0 = blockIdx.y * AXM_BM;
+  const int nchunks = (N + AXM_BK - 1) / AXM_BK;
+
+  // Mat tile: AXM_BM rows x AXM_BK slices, 4 per thread, slices fastest
+  const int m_kk = tid & 15, m_r0 = tid >> 4;  // rows m_r0 + 16 j
+  // X tile: per-thread column bases (fixed over the stages)
+  int x_kk0, x_cr0;
+  size_t xbase[CONTIG ? XPT : 1];
+  bool xok[CONTIG ? XPT : 1];
+  if (CONTIG) {
+    x_kk0 = tid & 15;
+    x_cr0 = tid >> 4;  // columns x_cr0 + 16 j
+#pragma unroll
+    for (int j = 0; j < XPT; ++j) {
+      const int c = c0 + x_cr0 + 16 * j;
+      xok[j] = c < ncol;
+      xbase[j] = (size_t)(xok[j] ? c : 0) * N;
+    }
+  } else {
+    x_cr0 = tid % BN;
+    x_kk0 = tid / BN;  // slices x_kk0 + (AX_THREADS / BN) j
+    const int c = c0 + x_cr0;
+    xok[0] = c < ncol;
+    const int cc = xok[0] ? c : 0;
+    const int a = cc / B, b = cc - a * B;
+    xbase[0] = (size_t)a * N * B + b;
+  }
+
+  auto issue = [&](int stage, int n0) {
+    double* Ms = axm_sh + stage * STAGE;
+    double* Xs = Ms + AXM_BM * AXM_LDK;
+    {
+      const int n = n0 + m_kk;
+#pragma unroll
+      for (int j = 0; j < AXM_BM / 16; ++j) {
+        const int k = k0 + m_r0 + 16 * j;
+        const bool ok = k < Nout && n < N;
+        cp_async8(&Ms[(m_r0 + 16 * j) * AXM_LDK + m_kk], ok ? Mat + (size_t)k * N + n : Mat, ok ? 8 : 0);
+      }
+    }
+    if (CONTIG) {
+      const int n = n0 + x_kk0;
+#pragma unroll
+      for (int j = 0; j < XPT; ++j) {
+        const bool ok = xok[j] && n < N;
+        cp_async8(&Xs[(x_cr0 + 16 * j) * LDX + x_kk0], ok ? X + xbase[j] + n : X, ok ? 8 : 0);
+      }
+    } else {
+      constexpr int KSTEP = AX_THREADS / BN;
+#pragma unroll
+      for (int j = 0; j < XPT; ++j) {
+        const int kk = x_kk0 + KSTEP * j;
+        const int n = n0 + kk;
+        const bool ok = xok[0] && n < N;
+        cp_async8(&Xs[kk * LDX + x_cr0], ok ? X + xbase[0] + (size_t)n * B : X, ok ? 8 : 0);
+      }
+    }
+    cp_async_commit();
+  };
+
+  double acc[2][NT][4];
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < NT; ++j)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc[i][j][q] = 0.0;
+
+#pragma unroll
+  for (int st = 0; st < AXM_STAGES - 1; ++st) {
+    if (st < nchunks) issue(st, st * AXM_BK);
+    else cp_async_commit();
+  }
+  for (int ch = 0; ch < nchunks; ++ch) {
+    cp_async_wait<AXM_STAGES - 2>();
+    __syncthreads();
+    const int nxt = ch + AXM_STAGES - 1;
+    if (nxt < nchunks) issue(nxt % AXM_STAGES, nxt * AXM_BK);
+    else cp_async_commit();
+    const double* Ms = axm_sh + (ch % AXM_STAGES) * STAGE;
+    const double* Xs = Ms + AXM_BM * AXM_LDK;
+#pragma unroll
+    for (int k8 = 0; k8 < AXM_BK; k8 += 8) {
+      // A fragment (row-major 16 x 8): a0 (g, t), a1 (g + 8, t), a2 (g, t + 4), a3 (g + 8, t + 4)
+      double af[2][4];
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+        const double* r0 = Ms + (wm * 32 + i * 16 + g) * AXM_LDK + k8 + t;
+        const double* r1 = r0 + 8 * AXM_LDK;
+        af[i][0] = r0[0];
+        af[i][1] = r1[0];
+        af[i][2] = r0[4];
+        af[i][3] = r1[4];
+      }
+      // B fragment (col-major 8 x 8): b0 (k = t, n = g), b1 (k = t + 4, n = g)
+      double bf[NT][2];
+#pragma unroll
+      for (int j = 0; j < NT; ++j) {
+        const int col = wn * (BN / 4) + j * 8 + g;
+        if (CONTIG) {
+          bf[j][0] = Xs[col * LDX + k8 + t];
+          bf[j][1] = Xs[col * LDX + k8 + t + 4];
+        } else {
+          bf[j][0] = Xs[(k8 + t) * LDX + col];
+          bf[j][1] = Xs[(k8 + t + 4) * LDX + col];
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < NT; ++j) mma_f64_m16n8k8(acc[i][j], af[i], bf[j]);
+    }
+  }
+  cp_async_wait<0>();
+  __syncthreads();
+
+  // Epilogue through shared memory: the D fragments (16 x 8: d0, d1 at
+  // (g, 2t + {0, 1}), d2, d3 at (g + 8, 2t + {0, 1})) go to a BM x BN tile,
+  // then every thread hands consecutive outputs to epi, contiguous in memory
+  // (along k when B == 1, along c otherwise). Column offsets are computed
+  // once per column.
+  constexpr int LDT = BN + 1;
+  double* tile = axm_sh;                                  // AXM_BM x LDT (fits in the stages)
+  int* colbase = reinterpret_cast<int*>(tile + AXM_BM * LDT);  // BN: a * Nout * B + b
+  int* colb = colbase + BN;                                    // BN: b
+  static_assert((AXM_BM * (BN + 1)) * 8 + 2 * BN * 4 <= axm_smem_bytes<CONTIG, BN>(), "epilogue tile");
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < NT; ++j)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int row = wm * 32 + i * 16 + g + 8 * (q >> 1);
+        const int col = wn * (BN / 4) + j * 8 + 2 * t + (q & 1);
+        tile[row * LDT + col] = acc[i][j][q];
+      }
+  if (tid < BN) {
+    const int c = c0 + tid;
+    const int cc = c < ncol ? c : 0;
+    const int a = cc / B, b = cc - a * B;
+    colbase[tid] = a * Nout * B + b;
+    colb[tid] = b;
+  }
+  __syncthreads();
+  Red r;
+  const int kmax = min(AXM_BM, Nout - k0), cmax = min(BN, ncol - c0);
+  if (CONTIG) {
+    for (int e = tid; e < AXM_BM * BN; e += AX_THREADS) {
+      const int kr = e % AXM_BM, cr = e / AXM_BM;
+      if (kr < kmax && cr < cmax) {
+        const int k = k0 + kr;
+        epi(colbase[cr] + k, k, 0, tile[kr * LDT + cr], r);
+      }
+    }
+  } else {
+    for (int e = tid; e < AXM_BM * BN; e += AX_THREADS) {
+      const int cr = e % BN, kr = e / BN;
+      if (kr < kmax && cr < cmax) {
+        const int k = k0 + kr;
+        epi(colbase[cr] + k * B, k, colb[cr], tile[kr * LDT + cr], r);
+      }
+    }
+  }
+  if (Epi::kReduce) {
+    double p0, p1;
+    if (Epi::kReduce == 1) {
+      p0 = r.s0;
+      p1 = r.s1;
+      block_sum2<AX_THREADS>(p0, p1, red_sh);
+    } else {
+      p0 = r.mx;
+      p1 = r.s0;
+      block_max_sum<AX_THREADS>(p0, p1, red_sh);
+    }
+    if (threadIdx.x == 0) {
+      const int blk = blockIdx.y * gridDim.x + blockIdx.x;
+      epi.partials[2 * blk] = p0;
+      epi.partials[2 * blk + 1] = p1;
+    }
+  }
+}
+
+// Launch shape of one pass. kind 2 / 3: the FP64 tensor-core kernel with
+// BN = 128 / 64 columns per CTA, when the pass is large enough (see
+// axis_shape); kind 1: the 2 x 4 thread tile when it yields enough CTAs to
+// cover the SMs; kind 0: the 1 x 1 tile (small faces, short axes).
 struct AxisShape {
   bool big;
   dim3 grid;
+  int kind = 0;
 };
 constexpr int AX_MIN_CTAS = 132;
 // Tile policy of the calling thread: 2 x 4 tiles when that grid has at least
 // this many CTAs. Set for the duration of a plan's call by AxisPolicy, so the
 // captured graph, eager launches and the partial-buffer sizing agree.
 inline thread_local int g_axis_min_ctas = AX_MIN_CTAS;
+// Whether passes may use the FP64 tensor-core kernel (on by default; the
+// CUDA-core kernels remain for small passes and for comparison).
+inline thread_local bool g_axis_mma = true;
+constexpr int AXM_SMS = 148;          // CTAs of one full wave at one CTA per SM
+constexpr int AXM_MIN_CTAS = 16;      // smaller passes stay on the CUDA-core kernels
 
 struct AxisPolicy {
   int saved;
-  explicit AxisPolicy(int min_ctas) : saved(g_axis_min_ctas) {
+  bool saved_mma;
+  explicit AxisPolicy(int min_ctas, int cuda_cores_only = 0) : saved(g_axis_min_ctas), saved_mma(g_axis_mma) {
     g_axis_min_ctas = min_ctas > 0 ? min_ctas : AX_MIN_CTAS;
+    g_axis_mma = cuda_cores_only == 0;
   }
-  ~AxisPolicy() { g_axis_min_ctas = saved; }
+  ~AxisPolicy() {
+    g_axis_min_ctas = saved;
+    g_axis_mma = saved_mma;
+  }
 };
 
+// The choice depends on (Nout, A, B) only, so axis_blocks() sizes partial
+// buffers for exactly the kernel launch_axis() runs.
 inline AxisShape axis_shape(int Nout, int A, int B) {
   const int ncol = A * B;
+  if (g_axis_mma && Nout >= 16) {
+    const int gy = (Nout + AXM_BM - 1) / AXM_BM;
+    const long g128 = (long)((ncol + 127) / 128) * gy, g64 = (long)((ncol + 63) / 64) * gy;
+    if (g128 >= AXM_SMS) return {true, dim3((ncol + 127) / 128, gy), 2};
+    if (g64 >= AXM_MIN_CTAS) return {true, dim3((ncol + 63) / 64, gy), 3};
+  }
   auto grid_of = [&](int ti, int tj) {
     const int tk = (B == 1) ? 16 * tj : 16 * ti;
     const int tc = (B == 1) ? 16 * ti : 16 * tj;
     return dim3((ncol + tc - 1) / tc, (Nout + tk - 1) / tk);
   };
   const dim3 g = grid_of(2, 4);
-  if ((long)g.x * g.y >= g_axis_min_ctas) return {true, g};
-  return {false, grid_of(1, 1)};
+  if ((long)g.x * g.y >= g_axis_min_ctas) return {true, g, 1};
+  return {false, grid_of(1, 1), 0};
 }
 
 // Number of CTAs of one pass (the number of partials a reducing epilogue writes).
@@ -217,11 +469,35 @@ inline int axis_blocks(int Nout, int A, int B) {
   return (int)(sh.grid.x * sh.grid.y);
 }
 
+// Dynamic shared memory of the tensor-core kernel, raised past the 48 KB
+// default once per instantiation.
+template <bool CONTIG, int BN, class Epi>
+inline void launch_axis_mma(const double* X, const double* Mat, int Nout, int N, int A, int B, const Epi& epi,
+                            dim3 grid, cudaStream_t st) {
+  constexpr int bytes = axm_smem_bytes<CONTIG, BN>();
+  static const bool attr = [] {
+    cudaFuncSetAttribute(k_axis_mma<CONTIG, BN, Epi>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    return true;
+  }();
+  (void)attr;
+  k_axis_mma<CONTIG, BN, Epi><<<grid, AX_THREADS, bytes, st>>>(X, Mat, Nout, N, A, B, epi);
+}
+
 // One pass with Mat of Nout x N (N = contraction length).
 template <class Epi>
 inline void launch_axis(const double* X, const double* Mat, int Nout, int N, int A, int B,
                         const Epi& epi, cudaStream_t st) {
   const AxisShape sh = axis_shape(Nout, A, B);
+  if (sh.kind >= 2) {
+    if (B == 1) {
+      if (sh.kind == 2) launch_axis_mma<true, 128>(X, Mat, Nout, N, A, B, epi, sh.grid, st);
+      else launch_axis_mma<true, 64>(X, Mat, Nout, N, A, B, epi, sh.grid, st);
+    } else {
+      if (sh.kind == 2) launch_axis_mma<false, 128>(X, Mat, Nout, N, A, B, epi, sh.grid, st);
+      else launch_axis_mma<false, 64>(X, Mat, Nout, N, A, B, epi, sh.grid, st);
+    }
+    return;
+  }
   if (B == 1) {
     if (sh.big) k_axis<true, 2, 4, Epi><<<sh.grid, AX_THREADS, 0, st>>>(X, Mat, Nout, N, A, B, epi);
     else k_axis<true, 1, 1, Epi><<<sh.grid, AX_THREADS, 0, st>>>(X, Mat, Nout, N, A, B, epi);
@@ -313,8 +589,9 @@ struct EpiTrial {
   double* a_trial;       // written when !RELAX
   double* a_it;          // read and updated when RELAX
   double* partials;
+  int S;                 // ny nx (a copy of P->S, held by value: the stores above may not alias it)
+  double omega;          // P->omega, likewise
   __device__ __forceinline__ void operator()(int i, int, int, double v, Red& r) const {
-    const int S = P->S;
     const int z = i / S, yx = i - z * S;
     const double q = v * q_scale;
     if (Qm) Qm[i] = q;
@@ -325,7 +602,7 @@ struct EpiTrial {
     if (RELAX) {
       const double old = a_it[i];
       const double res = t - old;
-      a_it[i] = res * P->omega + old;
+      a_it[i] = res * omega + old;
       r.s0 = fma(res, res, r.s0);
       r.s1 = fma(old, old, r.s1);
     } else {
@@ -498,14 +775,27 @@ struct EpiBoxInit {
 
 // Picard iteration: the latent source on the box from the current iterate and
 // the shifted history (compute_latent_heat_source, physics/spectral_ops.py:234-267).
+// The constant-property source (spectral_cpu_kernels.py:115-140) uses the
+// scalars held by value; the blended-rho form (model != 0) reads P.
 struct EpiBoxLatent {
   static constexpr int kReduce = 0;
   const DevParams* P;
   const double* Tprev;
   double* Q;
   double* partials;
+  int model;             // P->latent_model
+  double T_solidus, band_inv, latent_factor;
   __device__ __forceinline__ void operator()(int i, int, int, double v, Red&) const {
-    Q[i] = latent_source(*P, v, Tprev[i]);
+    const double tp = Tprev[i];
+    if (model) {
+      Q[i] = latent_source(*P, v, tp);
+      return;
+    }
+    double fc = (v - T_solidus) * band_inv;
+    fc = fc < 0.0 ? 0.0 : (fc > 1.0 ? 1.0 : fc);
+    double fp = (tp - T_solidus) * band_inv;
+    fp = fp < 0.0 ? 0.0 : (fp > 1.0 ? 1.0 : fp);
+    Q[i] = latent_factor * (fc - fp);
   }
 };
 

@@ -1045,16 +1045,19 @@ void enqueue_picard(sgh_plan* p, cudaStream_t s, cudaGraphConditionalHandle h_pi
     face_idct2_from(p, p->d(p->o_bt1) + (size_t)h.zb * h.S,
                     EpiTopFlux{P, p->d(p->o_qlas), p->d(p->o_qev), p->d(p->o_qnet), h.prop_corr, nullptr}, s);
     face_dct2(p, p->d(p->o_qnet), p->d(p->o_Stop), h.dct_scale, s);
-    box_xy(p, EpiBoxLatent{P, p->d(p->o_Tsh), p->d(p->o_Qbox), nullptr}, s);
+    box_xy(p, EpiBoxLatent{P, p->d(p->o_Tsh), p->d(p->o_Qbox), nullptr, h.latent_model, h.T_solidus, h.band_inv,
+                           h.latent_factor},
+           s);
     if (h.prop_corr) {
       box_project(p, p->d(p->o_Qbox),
                   EpiTrial<false>{P, p->d(p->o_aK), p->d(p->o_KK), p->d(p->o_ct), p->d(p->o_cb), p->d(p->o_Stop),
-                                  1.0, h.dV_fine, S_bot, nullptr, p->d(p->o_trial), nullptr, nullptr},
+                                  1.0, h.dV_fine, S_bot, nullptr, p->d(p->o_trial), nullptr, nullptr, h.S, h.omega},
                   s);
     } else {
       box_project(p, p->d(p->o_Qbox),
                   EpiTrial<true>{P, p->d(p->o_aK), p->d(p->o_KK), p->d(p->o_ct), p->d(p->o_cb), p->d(p->o_Stop),
-                                 1.0, h.dV_fine, S_bot, nullptr, nullptr, p->d(p->o_a), p->d(p->o_prelax)},
+                                 1.0, h.dV_fine, S_bot, nullptr, nullptr, p->d(p->o_a), p->d(p->o_prelax), h.S,
+                                 h.omega},
                   s);
       nparts = axis_blocks(h.nz, 1, h.S);
     }
@@ -1071,13 +1074,13 @@ void enqueue_picard(sgh_plan* p, cudaStream_t s, cudaGraphConditionalHandle h_pi
       volume_pass3(p, p->d(p->o_vol), false,
                    EpiTrial<false>{P, p->d(p->o_aK), p->d(p->o_KK), p->d(p->o_ct), p->d(p->o_cb),
                                    S_top, h.dct_scale, h.sqrt_dV, S_bot, p->d(p->o_Qm), p->d(p->o_trial),
-                                   nullptr, nullptr},
+                                   nullptr, nullptr, h.S, h.omega},
                    p->d(p->o_t1), p->d(p->o_t2), s, h.nz + 1, h.nz);
     } else {
       volume_pass3(p, p->d(p->o_vol), false,
                    EpiTrial<true>{P, p->d(p->o_aK), p->d(p->o_KK), p->d(p->o_ct), p->d(p->o_cb),
                                   S_top, h.dct_scale, h.sqrt_dV, S_bot, p->d(p->o_Qm), nullptr, p->d(p->o_a),
-                                  p->d(p->o_prelax)},
+                                  p->d(p->o_prelax), h.S, h.omega},
                    p->d(p->o_t1), p->d(p->o_t2), s, h.nz + 1, h.nz);
       nparts = axis_blocks(h.nz, 1, h.S);
     }
@@ -1254,7 +1257,8 @@ int sgh_plan_create(const sgh_config* cfg, sgh_plan** out) {
   *out = nullptr;
   const sgh_config& c = *cfg;
   if (c.axis_min_ctas < 0) return fail(SGH_ERR_INVALID, "axis_min_ctas must be >= 0");
-  AxisPolicy policy(c.axis_min_ctas);
+  if (c.axis_cuda_cores != 0 && c.axis_cuda_cores != 1) return fail(SGH_ERR_INVALID, "axis_cuda_cores must be 0 or 1");
+  AxisPolicy policy(c.axis_min_ctas, c.axis_cuda_cores);
   if (c.nx < 2 || c.ny < 2 || c.nz < 2) return fail(SGH_ERR_INVALID, "every axis needs at least 2 modes");
   if (c.nx > 4096 || c.ny > 4096 || c.nz > 4096) return fail(SGH_ERR_INVALID, "an axis exceeds 4096 modes");
   if ((long long)c.nx * c.ny * c.nz > (1LL << 28)) return fail(SGH_ERR_INVALID, "grid exceeds 2^28 modes");
@@ -1462,7 +1466,7 @@ int sgh_plan_workspace_bytes(const sgh_plan* p, uint64_t* bytes) {
 }
 
 int sgh_plan_bind(sgh_plan* p, void* workspace, uint64_t bytes, void* stream) {
-  AxisPolicy policy(p ? p->cfg.axis_min_ctas : 0);
+  AxisPolicy policy(p ? p->cfg.axis_min_ctas : 0, p ? p->cfg.axis_cuda_cores : 0);
   if (!p || !workspace) return fail(SGH_ERR_INVALID, "null argument");
   if (p->bound) return fail(SGH_ERR_STATE, "plan is already bound");
   if (bytes < p->ws_need) return fail(SGH_ERR_WORKSPACE, "workspace is smaller than sgh_plan_workspace_bytes()");
@@ -1592,7 +1596,7 @@ int sgh_step(sgh_plan* p, const sgh_laser* laser, sgh_step_out* out, void* strea
 }
 
 int sgh_step_eager(sgh_plan* p, const sgh_laser* laser, sgh_step_out* out, void* stream) {
-  AxisPolicy policy(p ? p->cfg.axis_min_ctas : 0);
+  AxisPolicy policy(p ? p->cfg.axis_min_ctas : 0, p ? p->cfg.axis_cuda_cores : 0);
   if (!p || !laser) return fail(SGH_ERR_INVALID, "null argument");
   if (!p->bound) return fail(SGH_ERR_STATE, "plan is not bound");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -1626,7 +1630,7 @@ int sgh_run(sgh_plan* p, const sgh_laser* lasers_dev, int32_t n_steps, sgh_step_
 }
 
 int sgh_dct3d(sgh_plan* p, int32_t kind, const double* in, double* out, void* stream) {
-  AxisPolicy policy(p ? p->cfg.axis_min_ctas : 0);
+  AxisPolicy policy(p ? p->cfg.axis_min_ctas : 0, p ? p->cfg.axis_cuda_cores : 0);
   if (!p || !in || !out) return fail(SGH_ERR_INVALID, "null argument");
   if (!p->bound) return fail(SGH_ERR_STATE, "plan is not bound");
   if (kind != 2 && kind != 3) return fail(SGH_ERR_INVALID, "kind must be 2 (DCT_II) or 3 (IDCT_II)");
@@ -1637,7 +1641,7 @@ int sgh_dct3d(sgh_plan* p, int32_t kind, const double* in, double* out, void* st
 }
 
 int sgh_surface_temperature(sgh_plan* p, const double* modes, int32_t top, double* out, void* stream) {
-  AxisPolicy policy(p ? p->cfg.axis_min_ctas : 0);
+  AxisPolicy policy(p ? p->cfg.axis_min_ctas : 0, p ? p->cfg.axis_cuda_cores : 0);
   if (!p || !modes || !out) return fail(SGH_ERR_INVALID, "null argument");
   if (!p->bound) return fail(SGH_ERR_STATE, "plan is not bound");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -1647,7 +1651,7 @@ int sgh_surface_temperature(sgh_plan* p, const double* modes, int32_t top, doubl
 }
 
 int sgh_project_volume(sgh_plan* p, const double* field, double* modes, void* stream) {
-  AxisPolicy policy(p ? p->cfg.axis_min_ctas : 0);
+  AxisPolicy policy(p ? p->cfg.axis_min_ctas : 0, p ? p->cfg.axis_cuda_cores : 0);
   if (!p || !field || !modes) return fail(SGH_ERR_INVALID, "null argument");
   if (!p->bound) return fail(SGH_ERR_STATE, "plan is not bound");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -1657,7 +1661,7 @@ int sgh_project_volume(sgh_plan* p, const double* field, double* modes, void* st
 }
 
 int sgh_reconstruct_volume(sgh_plan* p, const double* modes, double* field, void* stream) {
-  AxisPolicy policy(p ? p->cfg.axis_min_ctas : 0);
+  AxisPolicy policy(p ? p->cfg.axis_min_ctas : 0, p ? p->cfg.axis_cuda_cores : 0);
   if (!p || !field || !modes) return fail(SGH_ERR_INVALID, "null argument");
   if (!p->bound) return fail(SGH_ERR_STATE, "plan is not bound");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -1693,7 +1697,7 @@ int sgh_box_window(sgh_plan* p, int32_t* i0, void* stream) {
 }
 
 int sgh_box_temperature(sgh_plan* p, const double* modes, double* out, void* stream) {
-  AxisPolicy policy(p ? p->cfg.axis_min_ctas : 0);
+  AxisPolicy policy(p ? p->cfg.axis_min_ctas : 0, p ? p->cfg.axis_cuda_cores : 0);
   if (!p || !modes || !out) return fail(SGH_ERR_INVALID, "null argument");
   if (!p->bound) return fail(SGH_ERR_STATE, "plan is not bound");
   if (!p->hp.box) return fail(SGH_ERR_STATE, "plan is not in box mode");
@@ -1705,7 +1709,7 @@ int sgh_box_temperature(sgh_plan* p, const double* modes, double* out, void* str
 }
 
 int sgh_box_project(sgh_plan* p, const double* field_box, double* modes, void* stream) {
-  AxisPolicy policy(p ? p->cfg.axis_min_ctas : 0);
+  AxisPolicy policy(p ? p->cfg.axis_min_ctas : 0, p ? p->cfg.axis_cuda_cores : 0);
   if (!p || !field_box || !modes) return fail(SGH_ERR_INVALID, "null argument");
   if (!p->bound) return fail(SGH_ERR_STATE, "plan is not bound");
   if (!p->hp.box) return fail(SGH_ERR_STATE, "plan is not in box mode");

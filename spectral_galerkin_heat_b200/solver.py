@@ -231,11 +231,14 @@ class B200SpectralSolver(HeatSolver):
     """Spectral-Galerkin heat step on one B200 (FP64, grid or box mode)."""
 
     def __init__(self, backend=None, context=None, *, mixing_omega=None,
-                 convergence_tol=None, max_picard_iter=None, device=None, axis_min_ctas=None):
+                 convergence_tol=None, max_picard_iter=None, device=None, axis_min_ctas=None,
+                 axis_cuda_cores=False):
         self.backend = backend
         self.context = context
         # tile policy of the axis passes: explicit, else the autotuner's table, else default
         self.axis_min_ctas = axis_min_ctas
+        # True: every FP64 axis pass on the CUDA-core kernels (no FP64 tensor cores)
+        self.axis_cuda_cores = bool(axis_cuda_cores)
         self.state: Optional[B200State] = None
         self.device = device
         self._req = (mixing_omega, convergence_tol, max_picard_iter)
@@ -285,6 +288,7 @@ class B200SpectralSolver(HeatSolver):
             from .autotune import lookup
             policy = lookup(cfg)
         cfg.axis_min_ctas = int(policy or 0)
+        cfg.axis_cuda_cores = 1 if self.axis_cuda_cores else 0
         self.tile_policy = int(cfg.axis_min_ctas)
         plan = C.c_void_p()
         _lib.check("sgh_plan_create", L.sgh_plan_create(C.byref(cfg), C.byref(plan)))
