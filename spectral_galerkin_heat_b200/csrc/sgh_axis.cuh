@@ -37,6 +37,10 @@ __device__ __forceinline__ void cp_async8(void* smem, const void* gmem, int src_
   const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(smem));
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(gmem), "r"(src_bytes));
 }
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, int src_bytes) {
+  const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(gmem), "r"(src_bytes));
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
@@ -181,9 +185,9 @@ k_axis(const double* __restrict__ X, const double* __restrict__ Mat, int Nout, i
 
 // ---------------------------------------------------------------------------
 // FP64 tensor-core variant: mma.sync m16n8k8 .f64 (the FP64 MMA of sm_90+,
-// kept on sm_100a; tcgen05 has no FP64 kind). CTA tile AXM_BM (outputs along
-// the transformed axis) x BN (columns c), 8 warps as 2 x 4, warp tile 32 x BN/4
-// = 2 m16 x BN/32 n8 MMA tiles per k8 step. Mat and X tiles stream through an
+// kept on sm_100a; tcgen05 has no FP64 kind). CTA tile BM (outputs along the
+// transformed axis) x BN (columns c), 8 warps as 2 x 4, warp tile BM/2 x BN/4
+// = BM/32 m16 x BN/32 n8 MMA tiles per k8 step. Mat and X tiles stream through an
 // AXM_STAGES-deep cp.async pipeline of AXM_BK slices. Shared layouts keep the
 // fragment reads and the cp.async writes free of bank conflicts: Mat tiles
 // k-major rows of AXM_BK + 4 doubles; X tiles column-major (rows of AXM_BK + 4)
@@ -191,18 +195,17 @@ k_axis(const double* __restrict__ X, const double* __restrict__ Mat, int Nout, i
 // of BN + 4. Each thread's source columns are fixed across stages, so their
 // offsets are computed once.
 // ---------------------------------------------------------------------------
-constexpr int AXM_BM = 64;
 constexpr int AXM_BK = 16;
 constexpr int AXM_STAGES = 3;
 constexpr int AXM_LDK = AXM_BK + 4;  // rows of AXM_BK contraction slices
 
-template <bool CONTIG, int BN>
+template <bool CONTIG, int BM, int BN>
 constexpr int axm_stage_doubles() {
-  return AXM_BM * AXM_LDK + (CONTIG ? BN * AXM_LDK : AXM_BK * (BN + 4));
+  return BM * AXM_LDK + (CONTIG ? BN * AXM_LDK : AXM_BK * (BN + 4));
 }
-template <bool CONTIG, int BN>
+template <bool CONTIG, int BM, int BN>
 constexpr int axm_smem_bytes() {
-  return AXM_STAGES * axm_stage_doubles<CONTIG, BN>() * (int)sizeof(double);
+  return AXM_STAGES * axm_stage_doubles<CONTIG, BM, BN>() * (int)sizeof(double);
 }
 
 __device__ __forceinline__ void mma_f64_m16n8k8(double (&d)[4], const double (&a)[4], const double (&b)[2]) {
@@ -213,13 +216,16 @@ __device__ __forceinline__ void mma_f64_m16n8k8(double (&d)[4], const double (&a
       : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
 }
 
-template <bool CONTIG, int BN, class Epi>
+template <bool CONTIG, int BM, int BN, class Epi>
 __global__ void __launch_bounds__(AX_THREADS)
 k_axis_mma(const double* __restrict__ X, const double* __restrict__ Mat, int Nout, int N, int A, int B,
            Epi epi) {
+  static_assert(BM == 32 || BM == 64, "BM");
+  static_assert(BN == 64 || BN == 128, "BN");
   extern __shared__ __align__(16) double axm_sh[];
-  constexpr int STAGE = axm_stage_doubles<CONTIG, BN>();
+  constexpr int STAGE = axm_stage_doubles<CONTIG, BM, BN>();
   constexpr int LDX = CONTIG ? AXM_LDK : BN + 4;
+  constexpr int MT = BM / 32;           // m16 tiles per warp (warp rows BM / 2)
   constexpr int NT = BN / 32;           // n8 tiles per warp
   constexpr int XPT = BN * AXM_BK / AX_THREADS;  // X elements per thread per stage
   __shared__ double red_sh[2 * (AX_THREADS / 32)];
@@ -228,15 +234,30 @@ k_axis_mma(const double* __restrict__ X, const double* __restrict__ Mat, int Nou
   const int g = lane >> 2, t = lane & 3;
   const int wm = warp >> 2, wn = warp & 3;
   const int ncol = A * B;
-  const int c0 = blockIdx.x * BN, k0 = blockIdx.y * AXM_BM;
+  const int c0 = blockIdx.x * BN, k0 = blockIdx.y * BM;
   const int nchunks = (N + AXM_BK - 1) / AXM_BK;
 
-  // Mat tile: AXM_BM rows x AXM_BK slices, 4 per thread, slices fastest
-  const int m_kk = tid & 15, m_r0 = tid >> 4;  // rows m_r0 + 16 j
+  // 16-byte copies of element pairs where every pair is aligned and lies
+  // wholly inside or outside the array: along n for Mat (and X when B == 1)
+  // when N is even, along c for X when B is even. Uniform per launch.
+  const bool vecM = (N % 2 == 0) && (reinterpret_cast<uintptr_t>(Mat) % 16 == 0);
+  const bool vecX = (CONTIG ? (N % 2 == 0) : (B % 2 == 0)) && (reinterpret_cast<uintptr_t>(X) % 16 == 0);
+
+  // Mat tile: BM rows x AXM_BK slices, slices fastest. Scalar: BM / 16 per
+  // thread, rows m_r0 + 16 j, slice m_kk. Pairs: BM / 32 per thread, rows
+  // mp_r0 + 32 j, slices 2 mp_p, 2 mp_p + 1.
+  const int m_kk = tid & 15, m_r0 = tid >> 4;
+  const int mp_p = tid & 7, mp_r0 = tid >> 3;
   // X tile: per-thread column bases (fixed over the stages)
   int x_kk0, x_cr0;
   size_t xbase[CONTIG ? XPT : 1];
   bool xok[CONTIG ? XPT : 1];
+  // pairs: CONTIG: pair xp_p (slices 2 xp_p, +1) of columns xp_c0 + 32 j;
+  // otherwise columns 2 xp_c, 2 xp_c + 1 of slices xp_k0 + (2 AX_THREADS / BN) j
+  const int xp_p = tid & 7, xp_c0 = tid >> 3;
+  const int xp_c = tid % (BN / 2), xp_k0 = tid / (BN / 2);
+  size_t xpbase = 0;
+  bool xpok = false;
   if (CONTIG) {
     x_kk0 = tid & 15;
     x_cr0 = tid >> 4;  // columns x_cr0 + 16 j
@@ -254,43 +275,79 @@ k_axis_mma(const double* __restrict__ X, const double* __restrict__ Mat, int Nou
     const int cc = xok[0] ? c : 0;
     const int a = cc / B, b = cc - a * B;
     xbase[0] = (size_t)a * N * B + b;
+    // pair base: column c0 + 2 xp_c (even, so b is even when B is even)
+    const int cp = c0 + 2 * xp_c;
+    xpok = cp < ncol;
+    const int cq = xpok ? cp : 0;
+    const int ap = cq / B, bp = cq - ap * B;
+    xpbase = (size_t)ap * N * B + bp;
   }
 
   auto issue = [&](int stage, int n0) {
     double* Ms = axm_sh + stage * STAGE;
-    double* Xs = Ms + AXM_BM * AXM_LDK;
-    {
+    double* Xs = Ms + BM * AXM_LDK;
+    if (vecM) {
+      const int n = n0 + 2 * mp_p;
+#pragma unroll
+      for (int j = 0; j < BM / 32; ++j) {
+        const int k = k0 + mp_r0 + 32 * j;
+        const bool ok = k < Nout && n < N;
+        cp_async16(&Ms[(mp_r0 + 32 * j) * AXM_LDK + 2 * mp_p], ok ? Mat + (size_t)k * N + n : Mat, ok ? 16 : 0);
+      }
+    } else {
       const int n = n0 + m_kk;
 #pragma unroll
-      for (int j = 0; j < AXM_BM / 16; ++j) {
+      for (int j = 0; j < BM / 16; ++j) {
         const int k = k0 + m_r0 + 16 * j;
         const bool ok = k < Nout && n < N;
         cp_async8(&Ms[(m_r0 + 16 * j) * AXM_LDK + m_kk], ok ? Mat + (size_t)k * N + n : Mat, ok ? 8 : 0);
       }
     }
     if (CONTIG) {
-      const int n = n0 + x_kk0;
+      if (vecX) {
+        const int n = n0 + 2 * xp_p;
 #pragma unroll
-      for (int j = 0; j < XPT; ++j) {
-        const bool ok = xok[j] && n < N;
-        cp_async8(&Xs[(x_cr0 + 16 * j) * LDX + x_kk0], ok ? X + xbase[j] + n : X, ok ? 8 : 0);
+        for (int j = 0; j < XPT / 2; ++j) {
+          const int cr = xp_c0 + 32 * j;
+          const int c = c0 + cr;
+          const bool ok = c < ncol && n < N;
+          cp_async16(&Xs[cr * LDX + 2 * xp_p], ok ? X + (size_t)c * N + n : X, ok ? 16 : 0);
+        }
+      } else {
+        const int n = n0 + x_kk0;
+#pragma unroll
+        for (int j = 0; j < XPT; ++j) {
+          const bool ok = xok[j] && n < N;
+          cp_async8(&Xs[(x_cr0 + 16 * j) * LDX + x_kk0], ok ? X + xbase[j] + n : X, ok ? 8 : 0);
+        }
       }
     } else {
-      constexpr int KSTEP = AX_THREADS / BN;
+      if (vecX) {
+        constexpr int KSTEP2 = 2 * AX_THREADS / BN;
 #pragma unroll
-      for (int j = 0; j < XPT; ++j) {
-        const int kk = x_kk0 + KSTEP * j;
-        const int n = n0 + kk;
-        const bool ok = xok[0] && n < N;
-        cp_async8(&Xs[kk * LDX + x_cr0], ok ? X + xbase[0] + (size_t)n * B : X, ok ? 8 : 0);
+        for (int j = 0; j < XPT / 2; ++j) {
+          const int kk = xp_k0 + KSTEP2 * j;
+          const int n = n0 + kk;
+          const bool ok = xpok && n < N;
+          cp_async16(&Xs[kk * LDX + 2 * xp_c], ok ? X + xpbase + (size_t)n * B : X, ok ? 16 : 0);
+        }
+      } else {
+        constexpr int KSTEP = AX_THREADS / BN;
+#pragma unroll
+        for (int j = 0; j < XPT; ++j) {
+          const int kk = x_kk0 + KSTEP * j;
+          const int n = n0 + kk;
+          const bool ok = xok[0] && n < N;
+          cp_async8(&Xs[kk * LDX + x_cr0], ok ? X + xbase[0] + (size_t)n * B : X, ok ? 8 : 0);
+        }
       }
     }
     cp_async_commit();
   };
 
-  double acc[2][NT][4];
+  double acc[MT][NT][4];
 #pragma unroll
-  for (int i = 0; i < 2; ++i)
+  for (int i = 0; i < MT; ++i)
 #pragma unroll
     for (int j = 0; j < NT; ++j)
 #pragma unroll
@@ -308,14 +365,14 @@ k_axis_mma(const double* __restrict__ X, const double* __restrict__ Mat, int Nou
     if (nxt < nchunks) issue(nxt % AXM_STAGES, nxt * AXM_BK);
     else cp_async_commit();
     const double* Ms = axm_sh + (ch % AXM_STAGES) * STAGE;
-    const double* Xs = Ms + AXM_BM * AXM_LDK;
+    const double* Xs = Ms + BM * AXM_LDK;
 #pragma unroll
     for (int k8 = 0; k8 < AXM_BK; k8 += 8) {
       // A fragment (row-major 16 x 8): a0 (g, t), a1 (g + 8, t), a2 (g, t + 4), a3 (g + 8, t + 4)
-      double af[2][4];
+      double af[MT][4];
 #pragma unroll
-      for (int i = 0; i < 2; ++i) {
-        const double* r0 = Ms + (wm * 32 + i * 16 + g) * AXM_LDK + k8 + t;
+      for (int i = 0; i < MT; ++i) {
+        const double* r0 = Ms + (wm * (BM / 2) + i * 16 + g) * AXM_LDK + k8 + t;
         const double* r1 = r0 + 8 * AXM_LDK;
         af[i][0] = r0[0];
         af[i][1] = r1[0];
@@ -336,7 +393,7 @@ k_axis_mma(const double* __restrict__ X, const double* __restrict__ Mat, int Nou
         }
       }
 #pragma unroll
-      for (int i = 0; i < 2; ++i)
+      for (int i = 0; i < MT; ++i)
 #pragma unroll
         for (int j = 0; j < NT; ++j) mma_f64_m16n8k8(acc[i][j], af[i], bf[j]);
     }
@@ -350,17 +407,17 @@ k_axis_mma(const double* __restrict__ X, const double* __restrict__ Mat, int Nou
   // (along k when B == 1, along c otherwise). Column offsets are computed
   // once per column.
   constexpr int LDT = BN + 1;
-  double* tile = axm_sh;                                  // AXM_BM x LDT (fits in the stages)
-  int* colbase = reinterpret_cast<int*>(tile + AXM_BM * LDT);  // BN: a * Nout * B + b
+  double* tile = axm_sh;                                  // BM x LDT (fits in the stages)
+  int* colbase = reinterpret_cast<int*>(tile + BM * LDT);      // BN: a * Nout * B + b
   int* colb = colbase + BN;                                    // BN: b
-  static_assert((AXM_BM * (BN + 1)) * 8 + 2 * BN * 4 <= axm_smem_bytes<CONTIG, BN>(), "epilogue tile");
+  static_assert((BM * (BN + 1)) * 8 + 2 * BN * 4 <= axm_smem_bytes<CONTIG, BM, BN>(), "epilogue tile");
 #pragma unroll
-  for (int i = 0; i < 2; ++i)
+  for (int i = 0; i < MT; ++i)
 #pragma unroll
     for (int j = 0; j < NT; ++j)
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
-        const int row = wm * 32 + i * 16 + g + 8 * (q >> 1);
+        const int row = wm * (BM / 2) + i * 16 + g + 8 * (q >> 1);
         const int col = wn * (BN / 4) + j * 8 + 2 * t + (q & 1);
         tile[row * LDT + col] = acc[i][j][q];
       }
@@ -373,17 +430,17 @@ k_axis_mma(const double* __restrict__ X, const double* __restrict__ Mat, int Nou
   }
   __syncthreads();
   Red r;
-  const int kmax = min(AXM_BM, Nout - k0), cmax = min(BN, ncol - c0);
+  const int kmax = min(BM, Nout - k0), cmax = min(BN, ncol - c0);
   if (CONTIG) {
-    for (int e = tid; e < AXM_BM * BN; e += AX_THREADS) {
-      const int kr = e % AXM_BM, cr = e / AXM_BM;
+    for (int e = tid; e < BM * BN; e += AX_THREADS) {
+      const int kr = e % BM, cr = e / BM;
       if (kr < kmax && cr < cmax) {
         const int k = k0 + kr;
         epi(colbase[cr] + k, k, 0, tile[kr * LDT + cr], r);
       }
     }
   } else {
-    for (int e = tid; e < AXM_BM * BN; e += AX_THREADS) {
+    for (int e = tid; e < BM * BN; e += AX_THREADS) {
       const int cr = e % BN, kr = e / BN;
       if (kr < kmax && cr < cmax) {
         const int k = k0 + kr;
@@ -410,10 +467,10 @@ k_axis_mma(const double* __restrict__ X, const double* __restrict__ Mat, int Nou
   }
 }
 
-// Launch shape of one pass. kind 2 / 3: the FP64 tensor-core kernel with
-// BN = 128 / 64 columns per CTA, when the pass is large enough (see
-// axis_shape); kind 1: the 2 x 4 thread tile when it yields enough CTAs to
-// cover the SMs; kind 0: the 1 x 1 tile (small faces, short axes).
+// Launch shape of one pass. kind 2..5: the FP64 tensor-core kernel with a
+// BM x BN tile of 64 x 128, 64 x 64, 32 x 128, 32 x 64, when the pass is large
+// enough (see axis_shape); kind 1: the 2 x 4 thread tile when it yields
+// enough CTAs to cover the SMs; kind 0: the 1 x 1 tile (small faces, short axes).
 struct AxisShape {
   bool big;
   dim3 grid;
@@ -448,10 +505,14 @@ struct AxisPolicy {
 inline AxisShape axis_shape(int Nout, int A, int B) {
   const int ncol = A * B;
   if (g_axis_mma && Nout >= 16) {
-    const int gy = (Nout + AXM_BM - 1) / AXM_BM;
-    const long g128 = (long)((ncol + 127) / 128) * gy, g64 = (long)((ncol + 63) / 64) * gy;
-    if (g128 >= AXM_SMS) return {true, dim3((ncol + 127) / 128, gy), 2};
-    if (g64 >= AXM_MIN_CTAS) return {true, dim3((ncol + 63) / 64, gy), 3};
+    // the largest tile that fills one wave (a CTA per SM); else the smallest
+    const int tiles[4][2] = {{64, 128}, {64, 64}, {32, 128}, {32, 64}};
+    for (int q = 0; q < 4; ++q) {
+      const int bm = tiles[q][0], bn = tiles[q][1];
+      const dim3 gq((ncol + bn - 1) / bn, (Nout + bm - 1) / bm);
+      const long n = (long)gq.x * gq.y;
+      if (n >= AXM_SMS || (q == 3 && n >= AXM_MIN_CTAS)) return {true, gq, 2 + q};
+    }
   }
   auto grid_of = [&](int ti, int tj) {
     const int tk = (B == 1) ? 16 * tj : 16 * ti;
@@ -471,16 +532,27 @@ inline int axis_blocks(int Nout, int A, int B) {
 
 // Dynamic shared memory of the tensor-core kernel, raised past the 48 KB
 // default once per instantiation.
-template <bool CONTIG, int BN, class Epi>
+template <bool CONTIG, int BM, int BN, class Epi>
 inline void launch_axis_mma(const double* X, const double* Mat, int Nout, int N, int A, int B, const Epi& epi,
                             dim3 grid, cudaStream_t st) {
-  constexpr int bytes = axm_smem_bytes<CONTIG, BN>();
+  constexpr int bytes = axm_smem_bytes<CONTIG, BM, BN>();
   static const bool attr = [] {
-    cudaFuncSetAttribute(k_axis_mma<CONTIG, BN, Epi>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    cudaFuncSetAttribute(k_axis_mma<CONTIG, BM, BN, Epi>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     return true;
   }();
   (void)attr;
-  k_axis_mma<CONTIG, BN, Epi><<<grid, AX_THREADS, bytes, st>>>(X, Mat, Nout, N, A, B, epi);
+  k_axis_mma<CONTIG, BM, BN, Epi><<<grid, AX_THREADS, bytes, st>>>(X, Mat, Nout, N, A, B, epi);
+}
+
+template <bool CONTIG, class Epi>
+inline void launch_axis_mma_kind(int kind, const double* X, const double* Mat, int Nout, int N, int A, int B,
+                                 const Epi& epi, dim3 grid, cudaStream_t st) {
+  switch (kind) {
+    case 2: launch_axis_mma<CONTIG, 64, 128>(X, Mat, Nout, N, A, B, epi, grid, st); break;
+    case 3: launch_axis_mma<CONTIG, 64, 64>(X, Mat, Nout, N, A, B, epi, grid, st); break;
+    case 4: launch_axis_mma<CONTIG, 32, 128>(X, Mat, Nout, N, A, B, epi, grid, st); break;
+    default: launch_axis_mma<CONTIG, 32, 64>(X, Mat, Nout, N, A, B, epi, grid, st); break;
+  }
 }
 
 // One pass with Mat of Nout x N (N = contraction length).
@@ -489,13 +561,8 @@ inline void launch_axis(const double* X, const double* Mat, int Nout, int N, int
                         const Epi& epi, cudaStream_t st) {
   const AxisShape sh = axis_shape(Nout, A, B);
   if (sh.kind >= 2) {
-    if (B == 1) {
-      if (sh.kind == 2) launch_axis_mma<true, 128>(X, Mat, Nout, N, A, B, epi, sh.grid, st);
-      else launch_axis_mma<true, 64>(X, Mat, Nout, N, A, B, epi, sh.grid, st);
-    } else {
-      if (sh.kind == 2) launch_axis_mma<false, 128>(X, Mat, Nout, N, A, B, epi, sh.grid, st);
-      else launch_axis_mma<false, 64>(X, Mat, Nout, N, A, B, epi, sh.grid, st);
-    }
+    if (B == 1) launch_axis_mma_kind<true>(sh.kind, X, Mat, Nout, N, A, B, epi, sh.grid, st);
+    else launch_axis_mma_kind<false>(sh.kind, X, Mat, Nout, N, A, B, epi, sh.grid, st);
     return;
   }
   if (B == 1) {
