@@ -609,13 +609,13 @@ struct EpiDiv {
 // T = IDCT(a)/sqrt_dV; Q = latent(T, T_prev) (spectral_ops.py:270-289).
 struct EpiLatent {
   static constexpr int kReduce = 0;
-  const DevParams* P;
+  PointPhys P;
   const double* Tprev;
   double* Q;
   double* partials;
   __device__ __forceinline__ void operator()(int i, int, int, double v, Red&) const {
-    const double T = v / P->sqrt_dV;
-    Q[i] = latent_source(*P, T, Tprev[i]);
+    const double T = v / P.sqrt_dV;
+    Q[i] = latent_source(P, T, ld_in(Tprev + i));
   }
 };
 
@@ -623,14 +623,14 @@ struct EpiLatent {
 // (spectral_ops.py:142-148).
 struct EpiTemperatureKp {
   static constexpr int kReduce = 0;
-  const DevParams* P;
+  PointPhys P;
   double* T;
   double* kp;
   double* partials;
   __device__ __forceinline__ void operator()(int i, int, int, double v, Red&) const {
-    const double t = v / P->sqrt_dV;
+    const double t = v / P.sqrt_dV;
     T[i] = t;
-    kp[i] = k_prime(*P, t);
+    kp[i] = k_prime(P, t);
   }
 };
 
@@ -643,7 +643,7 @@ struct EpiTemperatureKp {
 template <bool RELAX>
 struct EpiTrial {
   static constexpr int kReduce = RELAX ? 1 : 0;
-  const DevParams* P;
+  PointPhys P;
   const double* aK;
   const double* KK;
   const double* Ct;
@@ -656,16 +656,16 @@ struct EpiTrial {
   double* a_trial;       // written when !RELAX
   double* a_it;          // read and updated when RELAX
   double* partials;
-  int S;                 // ny nx (a copy of P->S, held by value: the stores above may not alias it)
-  double omega;          // P->omega, likewise
+  int S;                 // ny nx
+  double omega;
   __device__ __forceinline__ void operator()(int i, int, int, double v, Red& r) const {
     const int z = i / S, yx = i - z * S;
     const double q = v * q_scale;
     if (Qm) Qm[i] = q;
-    const double kk = KK[i];
-    double t = aK[i] + kk * Ct[z] * (s_top_scale * S_top[yx]);
+    const double kk = ld_in(KK + i);
+    double t = ld_in(aK + i) + kk * ld_in(Ct + z) * (s_top_scale * ld_in(S_top + yx));
     t += kk * q;
-    if (S_bot) t += kk * Cb[z] * S_bot[yx];
+    if (S_bot) t += kk * ld_in(Cb + z) * ld_in(S_bot + yx);
     if (RELAX) {
       const double old = a_it[i];
       const double res = t - old;
@@ -683,17 +683,17 @@ struct EpiTrial {
 //   a = res*omega + a_old; partial sums of res^2 and a_old^2.
 struct EpiRelax {
   static constexpr int kReduce = 1;
-  const DevParams* P;
+  PointPhys P;
   const double* a_trial;
   const double* KK;
   double* a_it;
   double* partials;
   __device__ __forceinline__ void operator()(int i, int, int, double v, Red& r) const {
-    const double c = v * P->sqrt_dV;
-    const double raw = a_trial[i] + KK[i] * c;
+    const double c = v * P.sqrt_dV;
+    const double raw = ld_in(a_trial + i) + ld_in(KK + i) * c;
     const double old = a_it[i];
     const double res = raw - old;
-    a_it[i] = res * P->omega + old;
+    a_it[i] = res * P.omega + old;
     r.s0 = fma(res, res, r.s0);
     r.s1 = fma(old, old, r.s1);
   }
@@ -703,19 +703,19 @@ struct EpiRelax {
 // optional k_bar/k(T_s) rescale of the net top flux (solvers/spectral.py:388-407).
 struct EpiTopFlux {
   static constexpr int kReduce = 0;
-  const DevParams* P;
+  PointPhys P;
   const double* q_las;
   double* q_evap;
   double* q_net;
   int rescale;
   double* partials;
   __device__ __forceinline__ void operator()(int i, int, int, double v, Red&) const {
-    const double Ts = P->recon_scale * v;
-    const double qe = evaporation(*P, Ts);
+    const double Ts = P.recon_scale * v;
+    const double qe = evaporation(P, Ts);
     q_evap[i] = qe;
-    const double qc = P->has_top_conv ? P->h_top * (Ts - P->T0) : 0.0;
-    double q = q_las[i] - qe - qc;
-    if (rescale) q = q * (P->kbar / k_blended(*P, Ts));
+    const double qc = P.has_top_conv ? P.h_top * (Ts - P.T0) : 0.0;
+    double q = ld_in(q_las + i) - qe - qc;
+    if (rescale) q = q * (P.kbar / k_blended(P, Ts));
     q_net[i] = q;
   }
 };
@@ -724,15 +724,15 @@ struct EpiTopFlux {
 // optionally rescaled by k_bar/k(T) (solvers/spectral.py:335-379).
 struct EpiConvFace {
   static constexpr int kReduce = 0;
-  const DevParams* P;
+  PointPhys P;
   double h;
   int rescale;
   double* q;
   double* partials;
   __device__ __forceinline__ void operator()(int i, int, int, double v, Red&) const {
-    const double T = P->recon_scale * v;
-    double qc = -h * (T - P->T0);
-    if (rescale) qc = qc * (P->kbar / k_blended(*P, T));
+    const double T = P.recon_scale * v;
+    double qc = -h * (T - P.T0);
+    if (rescale) qc = qc * (P.kbar / k_blended(P, T));
     q[i] = qc;
   }
 };
@@ -740,11 +740,11 @@ struct EpiConvFace {
 // Face: plain reconstruction T = recon_scale * IDCT2(A) into out.
 struct EpiFaceTemperature {
   static constexpr int kReduce = 0;
-  const DevParams* P;
+  PointPhys P;
   double* out;
   double* partials;
   __device__ __forceinline__ void operator()(int i, int, int, double v, Red&) const {
-    out[i] = P->recon_scale * v;
+    out[i] = P.recon_scale * v;
   }
 };
 
@@ -752,13 +752,13 @@ struct EpiFaceTemperature {
 // (solvers/spectral.py:502, 537) and the q_evap_old <- q_evap copy (:512).
 struct EpiCommitSurface {
   static constexpr int kReduce = 2;
-  const DevParams* P;
+  PointPhys P;
   double* T_surf;
   const double* q_evap;
   double* q_evap_old;
   double* partials;
   __device__ __forceinline__ void operator()(int i, int, int, double v, Red& r) const {
-    const double T = P->recon_scale * v;
+    const double T = P.recon_scale * v;
     T_surf[i] = T;
     q_evap_old[i] = q_evap[i];
     r.mx = fmax(r.mx, T);
@@ -775,7 +775,7 @@ struct EpiCommitSurface {
 // following DCT3(Q) x- and y-passes also produce DCT2(q_net).
 struct EpiLatentSurface {
   static constexpr int kReduce = 0;
-  const DevParams* P;
+  PointPhys P;
   const double* Tprev;
   double* Q;             // (nz + 1) slabs
   const double* q_las;
@@ -783,15 +783,15 @@ struct EpiLatentSurface {
   int rescale;
   double* partials;
   __device__ __forceinline__ void operator()(int i, int k, int b, double v, Red&) const {
-    if (k < P->nz) {
-      Q[i] = latent_source(*P, v / P->sqrt_dV, Tprev[i]);
+    if (k < P.nz) {
+      Q[i] = latent_source(P, v / P.sqrt_dV, ld_in(Tprev + i));
     } else {
       const double Ts = v;
-      const double qe = evaporation(*P, Ts);
+      const double qe = evaporation(P, Ts);
       q_evap[b] = qe;
-      const double qc = P->has_top_conv ? P->h_top * (Ts - P->T0) : 0.0;
-      double q = q_las[b] - qe - qc;
-      if (rescale) q = q * (P->kbar / k_blended(*P, Ts));
+      const double qc = P.has_top_conv ? P.h_top * (Ts - P.T0) : 0.0;
+      double q = ld_in(q_las + b) - qe - qc;
+      if (rescale) q = q * (P.kbar / k_blended(P, Ts));
       Q[i] = q;
     }
   }
@@ -803,15 +803,15 @@ struct EpiLatentSurface {
 // the q_evap_old <- q_evap copy (:512).
 struct EpiCommitVolume {
   static constexpr int kReduce = 2;
-  const DevParams* P;
+  PointPhys P;
   double* Tprev;
   double* T_surf;
   const double* q_evap;
   double* q_evap_old;
   double* partials;
   __device__ __forceinline__ void operator()(int i, int k, int b, double v, Red& r) const {
-    if (k < P->nz) {
-      Tprev[i] = v / P->sqrt_dV;
+    if (k < P.nz) {
+      Tprev[i] = v / P.sqrt_dV;
     } else {
       T_surf[b] = v;
       q_evap_old[b] = q_evap[b];
@@ -846,16 +846,16 @@ struct EpiBoxInit {
 // scalars held by value; the blended-rho form (model != 0) reads P.
 struct EpiBoxLatent {
   static constexpr int kReduce = 0;
-  const DevParams* P;
+  PointPhys P;
   const double* Tprev;
   double* Q;
   double* partials;
-  int model;             // P->latent_model
+  int model;             // P.latent_model
   double T_solidus, band_inv, latent_factor;
   __device__ __forceinline__ void operator()(int i, int, int, double v, Red&) const {
-    const double tp = Tprev[i];
+    const double tp = ld_in(Tprev + i);
     if (model) {
-      Q[i] = latent_source(*P, v, tp);
+      Q[i] = latent_source(P, v, tp);
       return;
     }
     double fc = (v - T_solidus) * band_inv;
@@ -879,7 +879,7 @@ struct EpiBoxCommit {
   double* partials;
   __device__ __forceinline__ void operator()(int i, int, int, double v, Red&) const {
     Tprev[i] = v;
-    Qprev[i] = ctrl->iter > 0 ? Qlast[i] : Qshift[i];
+    Qprev[i] = ld_in((ctrl->iter > 0 ? Qlast : Qshift) + i);
   }
 };
 

@@ -909,6 +909,7 @@ void enqueue_box_seed(sgh_plan* p, cudaStream_t s) {
 void enqueue_pre_face_space(sgh_plan* p, cudaStream_t s) {
   const DevParams& h = p->hp;
   DevParams* P = p->P();
+  const PointPhys PP = point_phys(p->hp, P);
   const int gS = cdiv(h.S, EW_THREADS);
   double* F = p->d(p->o_fsF);
   double* W = p->d(p->o_fsW);
@@ -924,18 +925,18 @@ void enqueue_pre_face_space(sgh_plan* p, cudaStream_t s) {
   if (h.has_top_conv) {
     k_fs_assemble<<<gS, EW_THREADS, 0, s>>>(P, F, W, sg, bt, At, nullptr);
     ++g_launches;
-    face_idct2_from(p, At, EpiConvFace{P, h.h_top, 0, p->d(p->o_f2), nullptr}, s);
+    face_idct2_from(p, At, EpiConvFace{PP, h.h_top, 0, p->d(p->o_f2), nullptr}, s);
     face_dct2_epi(p, p->d(p->o_f2), EpiAdd{sg, h.dct_scale, nullptr}, s);
   }
   if (h.has_bottom_conv) {
     k_fs_assemble<<<gS, EW_THREADS, 0, s>>>(P, F, W, sg, bt, At, Ab);
     ++g_launches;
-    face_idct2_from(p, Ab, EpiConvFace{P, h.h_bottom, 0, p->d(p->o_f2), nullptr}, s);
+    face_idct2_from(p, Ab, EpiConvFace{PP, h.h_bottom, 0, p->d(p->o_f2), nullptr}, s);
     face_dct2_epi(p, p->d(p->o_f2), EpiAdd{bt, h.dct_scale, nullptr}, s);
     // S_bot_raw, held fixed through the Picard loop (solvers/spectral.py:373-379)
     k_fs_assemble<<<gS, EW_THREADS, 0, s>>>(P, F, W, sg, bt, At, Ab);
     ++g_launches;
-    face_idct2_from(p, Ab, EpiConvFace{P, h.h_bottom, 0, p->d(p->o_f2), nullptr}, s);
+    face_idct2_from(p, Ab, EpiConvFace{PP, h.h_bottom, 0, p->d(p->o_f2), nullptr}, s);
     face_dct2(p, p->d(p->o_f2), p->d(p->o_Sbot), h.dct_scale, s);
   }
   k_fs_assemble<<<gS, EW_THREADS, 0, s>>>(P, F, W, sg, bt, At, nullptr);
@@ -946,8 +947,9 @@ void enqueue_picard_face_space(sgh_plan* p, cudaStream_t s, cudaGraphConditional
                                int in_graph) {
   const DevParams& h = p->hp;
   DevParams* P = p->P();
+  const PointPhys PP = point_phys(p->hp, P);
   face_idct2_from(p, p->d(p->o_A),
-                  EpiTopFlux{P, p->d(p->o_qlas), p->d(p->o_qev), p->d(p->o_qnet), 0, nullptr}, s);
+                  EpiTopFlux{PP, p->d(p->o_qlas), p->d(p->o_qev), p->d(p->o_qnet), 0, nullptr}, s);
   face_dct2(p, p->d(p->o_qnet), p->d(p->o_Stop), h.dct_scale, s);
   k_fs_relax<<<p->nparts_fs, EW_THREADS, 0, s>>>(P, p->d(p->o_fsF), p->d(p->o_fsW), p->d(p->o_Stop),
                                                  h.has_bottom_conv ? p->d(p->o_Sbot) : nullptr,
@@ -965,6 +967,7 @@ void enqueue_pre_begin(sgh_plan* p, cudaStream_t s, cudaGraphConditionalHandle h
                        cudaGraphConditionalHandle h_seed, int in_graph) {
   const DevParams& h = p->hp;
   DevParams* P = p->P();
+  const PointPhys PP = point_phys(p->hp, P);
   Ctrl* C = p->ctrl();
   const int gS = cdiv(h.S, EW_THREADS);
   k_step_begin<<<1, 1, 0, s>>>(P, C, h_picard, h_seed, in_graph);
@@ -985,6 +988,7 @@ void enqueue_pre_begin(sgh_plan* p, cudaStream_t s, cudaGraphConditionalHandle h
 void enqueue_pre_rest(sgh_plan* p, cudaStream_t s) {
   const DevParams& h = p->hp;
   DevParams* P = p->P();
+  const PointPhys PP = point_phys(p->hp, P);
   Ctrl* C = p->ctrl();
   const int gV = cdiv(h.V, EW_THREADS);
   if (p->face_space) {
@@ -1003,19 +1007,19 @@ void enqueue_pre_rest(sgh_plan* p, cudaStream_t s) {
                                           p->d(p->o_Stop), p->d(p->o_Qm), p->d(p->o_aK));
   ++g_launches;
   if (h.has_top_conv) {
-    face_idct2(p, p->d(p->o_a), p->d(p->o_ct), EpiConvFace{P, h.h_top, 0, p->d(p->o_f2), nullptr}, s);
+    face_idct2(p, p->d(p->o_a), p->d(p->o_ct), EpiConvFace{PP, h.h_top, 0, p->d(p->o_f2), nullptr}, s);
     face_dct2(p, p->d(p->o_f2), p->d(p->o_Stop), h.dct_scale, s);
     k_add_face<<<gV, EW_THREADS, 0, s>>>(P, p->d(p->o_a), p->d(p->o_KK), p->d(p->o_ct), p->d(p->o_Stop));
   ++g_launches;
   }
   if (h.has_bottom_conv) {
-    face_idct2(p, p->d(p->o_a), p->d(p->o_cb), EpiConvFace{P, h.h_bottom, 0, p->d(p->o_f2), nullptr}, s);
+    face_idct2(p, p->d(p->o_a), p->d(p->o_cb), EpiConvFace{PP, h.h_bottom, 0, p->d(p->o_f2), nullptr}, s);
     face_dct2(p, p->d(p->o_f2), p->d(p->o_Sbot), h.dct_scale, s);
     k_add_face<<<gV, EW_THREADS, 0, s>>>(P, p->d(p->o_a), p->d(p->o_KK), p->d(p->o_cb), p->d(p->o_Sbot));
   ++g_launches;
     // S_bot_raw, held fixed through the Picard loop (solvers/spectral.py:373-379)
     face_idct2(p, p->d(p->o_a), p->d(p->o_cb),
-               EpiConvFace{P, h.h_bottom, h.prop_corr, p->d(p->o_f2), nullptr}, s);
+               EpiConvFace{PP, h.h_bottom, h.prop_corr, p->d(p->o_f2), nullptr}, s);
     face_dct2(p, p->d(p->o_f2), p->d(p->o_Sbot), h.dct_scale, s);
   }
 }
@@ -1033,6 +1037,7 @@ void enqueue_picard(sgh_plan* p, cudaStream_t s, cudaGraphConditionalHandle h_pi
   }
   const DevParams& h = p->hp;
   DevParams* P = p->P();
+  const PointPhys PP = point_phys(p->hp, P);
   Ctrl* C = p->ctrl();
   const int gV = cdiv(h.V, EW_THREADS);
   double* S_bot = h.has_bottom_conv ? p->d(p->o_Sbot) : nullptr;
@@ -1043,19 +1048,19 @@ void enqueue_picard(sgh_plan* p, cudaStream_t s, cudaGraphConditionalHandle h_pi
     // (solvers/spectral.py:388-443 with the box branch :413-422)
     box_zpass(p, p->d(p->o_a), true, s);
     face_idct2_from(p, p->d(p->o_bt1) + (size_t)h.zb * h.S,
-                    EpiTopFlux{P, p->d(p->o_qlas), p->d(p->o_qev), p->d(p->o_qnet), h.prop_corr, nullptr}, s);
+                    EpiTopFlux{PP, p->d(p->o_qlas), p->d(p->o_qev), p->d(p->o_qnet), h.prop_corr, nullptr}, s);
     face_dct2(p, p->d(p->o_qnet), p->d(p->o_Stop), h.dct_scale, s);
-    box_xy(p, EpiBoxLatent{P, p->d(p->o_Tsh), p->d(p->o_Qbox), nullptr, h.latent_model, h.T_solidus, h.band_inv,
+    box_xy(p, EpiBoxLatent{PP, p->d(p->o_Tsh), p->d(p->o_Qbox), nullptr, h.latent_model, h.T_solidus, h.band_inv,
                            h.latent_factor},
            s);
     if (h.prop_corr) {
       box_project(p, p->d(p->o_Qbox),
-                  EpiTrial<false>{P, p->d(p->o_aK), p->d(p->o_KK), p->d(p->o_ct), p->d(p->o_cb), p->d(p->o_Stop),
+                  EpiTrial<false>{PP, p->d(p->o_aK), p->d(p->o_KK), p->d(p->o_ct), p->d(p->o_cb), p->d(p->o_Stop),
                                   1.0, h.dV_fine, S_bot, nullptr, p->d(p->o_trial), nullptr, nullptr, h.S, h.omega},
                   s);
     } else {
       box_project(p, p->d(p->o_Qbox),
-                  EpiTrial<true>{P, p->d(p->o_aK), p->d(p->o_KK), p->d(p->o_ct), p->d(p->o_cb), p->d(p->o_Stop),
+                  EpiTrial<true>{PP, p->d(p->o_aK), p->d(p->o_KK), p->d(p->o_ct), p->d(p->o_cb), p->d(p->o_Stop),
                                  1.0, h.dV_fine, S_bot, nullptr, nullptr, p->d(p->o_a), p->d(p->o_prelax), h.S,
                                  h.omega},
                   s);
@@ -1066,19 +1071,19 @@ void enqueue_picard(sgh_plan* p, cudaStream_t s, cudaGraphConditionalHandle h_pi
     // the net top flux in slab nz of vol; then DCT3 over nz + 1 slabs turns
     // slab nz into DCT2(q_net), read by the trial epilogue as S_top.
     volume_pass3(p, p->d(p->o_a), true,
-                 EpiLatentSurface{P, p->d(p->o_Tprev), p->d(p->o_vol), p->d(p->o_qlas), p->d(p->o_qev),
+                 EpiLatentSurface{PP, p->d(p->o_Tprev), p->d(p->o_vol), p->d(p->o_qlas), p->d(p->o_qev),
                                   h.prop_corr, nullptr},
                  p->d(p->o_t1), p->d(p->o_t2), s, h.nz, h.nz + 1);
     const double* S_top = p->d(p->o_t2) + (size_t)h.nz * h.S;
     if (h.prop_corr) {
       volume_pass3(p, p->d(p->o_vol), false,
-                   EpiTrial<false>{P, p->d(p->o_aK), p->d(p->o_KK), p->d(p->o_ct), p->d(p->o_cb),
+                   EpiTrial<false>{PP, p->d(p->o_aK), p->d(p->o_KK), p->d(p->o_ct), p->d(p->o_cb),
                                    S_top, h.dct_scale, h.sqrt_dV, S_bot, p->d(p->o_Qm), p->d(p->o_trial),
                                    nullptr, nullptr, h.S, h.omega},
                    p->d(p->o_t1), p->d(p->o_t2), s, h.nz + 1, h.nz);
     } else {
       volume_pass3(p, p->d(p->o_vol), false,
-                   EpiTrial<true>{P, p->d(p->o_aK), p->d(p->o_KK), p->d(p->o_ct), p->d(p->o_cb),
+                   EpiTrial<true>{PP, p->d(p->o_aK), p->d(p->o_KK), p->d(p->o_ct), p->d(p->o_cb),
                                   S_top, h.dct_scale, h.sqrt_dV, S_bot, p->d(p->o_Qm), nullptr, p->d(p->o_a),
                                   p->d(p->o_prelax), h.S, h.omega},
                    p->d(p->o_t1), p->d(p->o_t2), s, h.nz + 1, h.nz);
@@ -1087,7 +1092,7 @@ void enqueue_picard(sgh_plan* p, cudaStream_t s, cudaGraphConditionalHandle h_pi
   } else {
     // top face: T_s, evaporation, convection, rescale -> S_top
     face_idct2(p, p->d(p->o_a), p->d(p->o_ct),
-               EpiTopFlux{P, p->d(p->o_qlas), p->d(p->o_qev), p->d(p->o_qnet), h.prop_corr, nullptr}, s);
+               EpiTopFlux{PP, p->d(p->o_qlas), p->d(p->o_qev), p->d(p->o_qnet), h.prop_corr, nullptr}, s);
     face_dct2(p, p->d(p->o_qnet), p->d(p->o_Stop), h.dct_scale, s);
   }
   if (!h.grid_latent && !h.box && h.prop_corr) {
@@ -1103,12 +1108,12 @@ void enqueue_picard(sgh_plan* p, cudaStream_t s, cudaGraphConditionalHandle h_pi
   }
   if (h.prop_corr) {
     volume_pass3(p, p->d(p->o_trial), true,
-                 EpiTemperatureKp{P, p->d(p->o_vol), p->d(p->o_kp), nullptr}, p->d(p->o_t1),
+                 EpiTemperatureKp{PP, p->d(p->o_vol), p->d(p->o_kp), nullptr}, p->d(p->o_t1),
                  p->d(p->o_t2), s);
     k_stencil<<<gV, EW_THREADS, 0, s>>>(P, p->d(p->o_vol), p->d(p->o_kp), p->d(p->o_Tprev), p->d(p->o_t1));
     ++g_launches;
     volume_pass3(p, p->d(p->o_t1), false,
-                 EpiRelax{P, p->d(p->o_trial), p->d(p->o_KK), p->d(p->o_a), p->d(p->o_prelax)},
+                 EpiRelax{PP, p->d(p->o_trial), p->d(p->o_KK), p->d(p->o_a), p->d(p->o_prelax)},
                  p->d(p->o_t2), p->d(p->o_vol), s);
     nparts = axis_blocks(h.nz, 1, h.S);
   }
@@ -1119,6 +1124,7 @@ void enqueue_picard(sgh_plan* p, cudaStream_t s, cudaGraphConditionalHandle h_pi
 void enqueue_post(sgh_plan* p, cudaStream_t s, cudaGraphConditionalHandle h_steps, int in_graph) {
   const DevParams& h = p->hp;
   DevParams* P = p->P();
+  const PointPhys PP = point_phys(p->hp, P);
   int n_surf;
   if (h.box) {
     // surface of the committed modes (from the box z-pass face row unless the
@@ -1126,7 +1132,7 @@ void enqueue_post(sgh_plan* p, cudaStream_t s, cudaGraphConditionalHandle h_step
     // T_prev = T_box(a), Q_prev = the last source (solvers/spectral.py:502-533)
     if (h.prop_corr) {
       volume_pass3(p, p->d(p->o_a), true,
-                   EpiCommitVolume{P, p->d(p->o_Tprev), p->d(p->o_Tsurf), p->d(p->o_qev), p->d(p->o_qevold),
+                   EpiCommitVolume{PP, p->d(p->o_Tprev), p->d(p->o_Tsurf), p->d(p->o_qev), p->d(p->o_qevold),
                                    p->d(p->o_psurf)},
                    p->d(p->o_t1), p->d(p->o_t2), s, h.nz, h.nz + 1);
       n_surf = axis_blocks(h.nz + 1, 1, h.S);
@@ -1134,7 +1140,7 @@ void enqueue_post(sgh_plan* p, cudaStream_t s, cudaGraphConditionalHandle h_step
     } else {
       box_zpass(p, p->d(p->o_a), true, s);
       face_idct2_from(p, p->d(p->o_bt1) + (size_t)h.zb * h.S,
-                      EpiCommitSurface{P, p->d(p->o_Tsurf), p->d(p->o_qev), p->d(p->o_qevold), p->d(p->o_psurf)},
+                      EpiCommitSurface{PP, p->d(p->o_Tsurf), p->d(p->o_qev), p->d(p->o_qevold), p->d(p->o_psurf)},
                       s);
       n_surf = p->nparts_surf;
     }
@@ -1143,7 +1149,7 @@ void enqueue_post(sgh_plan* p, cudaStream_t s, cudaGraphConditionalHandle h_step
     ++g_launches;
   } else if (p->face_space) {
     face_idct2_from(p, p->d(p->o_A),
-                    EpiCommitSurface{P, p->d(p->o_Tsurf), p->d(p->o_qev), p->d(p->o_qevold), p->d(p->o_psurf)},
+                    EpiCommitSurface{PP, p->d(p->o_Tsurf), p->d(p->o_qev), p->d(p->o_qevold), p->d(p->o_psurf)},
                     s);
     k_fs_commit_modes<<<cdiv(h.V, EW_THREADS), EW_THREADS, 0, s>>>(
         P, p->d(p->o_a), p->d(p->o_K), p->d(p->o_KK), p->d(p->o_ct), p->d(p->o_cb), p->d(p->o_sigma),
@@ -1153,13 +1159,13 @@ void enqueue_post(sgh_plan* p, cudaStream_t s, cudaGraphConditionalHandle h_step
   } else if (h.grid_latent || h.prop_corr) {
     // T_prev and the surface temperature from one IDCT3 with the surface row
     volume_pass3(p, p->d(p->o_a), true,
-                 EpiCommitVolume{P, p->d(p->o_Tprev), p->d(p->o_Tsurf), p->d(p->o_qev), p->d(p->o_qevold),
+                 EpiCommitVolume{PP, p->d(p->o_Tprev), p->d(p->o_Tsurf), p->d(p->o_qev), p->d(p->o_qevold),
                                  p->d(p->o_psurf)},
                  p->d(p->o_t1), p->d(p->o_t2), s, h.nz, h.nz + 1);
     n_surf = axis_blocks(h.nz + 1, 1, h.S);
   } else {
     face_idct2(p, p->d(p->o_a), p->d(p->o_ct),
-               EpiCommitSurface{P, p->d(p->o_Tsurf), p->d(p->o_qev), p->d(p->o_qevold), p->d(p->o_psurf)}, s);
+               EpiCommitSurface{PP, p->d(p->o_Tsurf), p->d(p->o_qev), p->d(p->o_qevold), p->d(p->o_psurf)}, s);
     n_surf = p->nparts_surf;
   }
   k_commit<<<1, EW_THREADS, 0, s>>>(P, p->ctrl(), p->d(p->o_plas), p->nparts_las, p->d(p->o_psurf),
@@ -1645,7 +1651,7 @@ int sgh_surface_temperature(sgh_plan* p, const double* modes, int32_t top, doubl
   if (!p || !modes || !out) return fail(SGH_ERR_INVALID, "null argument");
   if (!p->bound) return fail(SGH_ERR_STATE, "plan is not bound");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  face_idct2(p, modes, p->d(top ? p->o_ct : p->o_cb), EpiFaceTemperature{p->P(), out, nullptr}, s);
+  face_idct2(p, modes, p->d(top ? p->o_ct : p->o_cb), EpiFaceTemperature{point_phys(p->hp, p->P()), out, nullptr}, s);
   SGH_CK(cudaGetLastError());
   return SGH_OK;
 }

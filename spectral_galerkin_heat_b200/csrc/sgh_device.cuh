@@ -63,7 +63,10 @@ struct Ctrl {
 // ---------------------------------------------------------------------------
 // property programs (core/property_expr.py grammar; postfix, FP64)
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ double eval_program(const sgh_program& p, double T) {
+// Kept out of line: inlined into every epilogue, the interpreter's switch
+// (every math function of the grammar) evicts the hot loop from the
+// instruction cache, although affine programs never reach it.
+static __device__ __noinline__ double eval_program(const sgh_program& p, double T) {
   double st[SGH_MAX_STACK];
   int sp = 0;
   const int n = p.n_ops;
@@ -108,16 +111,65 @@ __device__ __forceinline__ double eval_program(const sgh_program& p, double T) {
   return sp > 0 ? st[0] : nan("");
 }
 
+// Load of an epilogue input that no thread writes during the kernel, through
+// the read-only path. Written as non-volatile inline asm without a memory
+// clobber, so the compiler may issue it ahead of earlier stores to other
+// arrays (with a plain load it must assume they alias and serialise). Only
+// for arrays that stay unwritten for the whole kernel; a load guarded by a
+// bounds test stays behind the test (inline asm is not speculated).
+__device__ __forceinline__ double ld_in(const double* p) {
+  double v;
+  asm("ld.global.nc.f64 %0, [%1];" : "=d"(v) : "l"(p));
+  return v;
+}
+
+// Pointwise constants of the step, held by value inside the axis-pass
+// epilogues: kernel parameters, which the epilogues' global stores cannot
+// alias, so the compiler keeps them in registers instead of reloading
+// DevParams after every store. Non-affine property programs are read
+// through `full`.
+struct PointPhys {
+  int nz, S, latent_model, degenerate_band, k_constant, has_top_conv;
+  int affine[P_COUNT];
+  double sqrt_dV, omega, T_solidus, T_liquidus, band_inv, latent_factor, L_f, inv_dt;
+  double kbar, abar, T0, h_top, T_boil, evap_f1, evap_f2, recon_scale;
+  double aff_a[P_COUNT], aff_b[P_COUNT];
+  const DevParams* full;
+};
+
+// Built on the host from the host copy of the parameters and the device copy.
+inline PointPhys point_phys(const DevParams& h, const DevParams* dev) {
+  PointPhys q;
+  q.nz = h.nz; q.S = h.S; q.latent_model = h.latent_model; q.degenerate_band = h.degenerate_band;
+  q.k_constant = h.k_constant; q.has_top_conv = h.has_top_conv;
+  for (int i = 0; i < P_COUNT; ++i) {
+    q.affine[i] = h.affine[i];
+    q.aff_a[i] = h.aff_a[i];
+    q.aff_b[i] = h.aff_b[i];
+  }
+  q.sqrt_dV = h.sqrt_dV; q.omega = h.omega; q.T_solidus = h.T_solidus; q.T_liquidus = h.T_liquidus;
+  q.band_inv = h.band_inv; q.latent_factor = h.latent_factor; q.L_f = h.L_f; q.inv_dt = h.inv_dt;
+  q.kbar = h.kbar; q.abar = h.abar; q.T0 = h.T0; q.h_top = h.h_top; q.T_boil = h.T_boil;
+  q.evap_f1 = h.evap_f1; q.evap_f2 = h.evap_f2; q.recon_scale = h.recon_scale;
+  q.full = dev;
+  return q;
+}
+
+__device__ __forceinline__ const sgh_program& prog_of(const DevParams& P, int slot) { return P.prog[slot]; }
+__device__ __forceinline__ const sgh_program& prog_of(const PointPhys& P, int slot) { return P.full->prog[slot]; }
+
 // One property branch: affine programs (the common piecewise-linear tables)
 // take one FMA; anything else runs the postfix interpreter.
-__device__ __forceinline__ double prop(const DevParams& P, int slot, double T) {
+template <class PP>
+__device__ __forceinline__ double prop(const PP& P, int slot, double T) {
   if (P.affine[slot]) return fma(P.aff_b[slot], T, P.aff_a[slot]);
-  return eval_program(P.prog[slot], T);
+  return eval_program(prog_of(P, slot), T);
 }
 
 // Liquid fraction as the fused kernels compute it: clip((T - T_s) * inv, 0, 1),
 // a step at T_s for a degenerate band (core/properties.py:175-183, 218-229).
-__device__ __forceinline__ double fl_kernel(const DevParams& P, double T) {
+template <class PP>
+__device__ __forceinline__ double fl_kernel(const PP& P, double T) {
   if (P.degenerate_band) return T >= P.T_solidus ? 1.0 : 0.0;
   double f = (T - P.T_solidus) * P.band_inv;
   return f < 0.0 ? 0.0 : (f > 1.0 ? 1.0 : f);
@@ -125,7 +177,8 @@ __device__ __forceinline__ double fl_kernel(const DevParams& P, double T) {
 
 // k(T) as TempProperty.__call__ evaluates it (core/properties.py:96-103,
 // liquid_fraction :61-77 by division).
-__device__ __forceinline__ double k_blended(const DevParams& P, double T) {
+template <class PP>
+__device__ __forceinline__ double k_blended(const PP& P, double T) {
   const double ks = prop(P, P_K_SOLID, T);
   if (P.k_constant) return ks;
   const double kl = prop(P, P_K_LIQUID, T);
@@ -140,7 +193,8 @@ __device__ __forceinline__ double k_blended(const DevParams& P, double T) {
 }
 
 // k'(T) = k(T) - kbar of the fused kernel (core/properties.py:185-191).
-__device__ __forceinline__ double k_prime(const DevParams& P, double T) {
+template <class PP>
+__device__ __forceinline__ double k_prime(const PP& P, double T) {
   const double fl = fl_kernel(P, T);
   const double om = 1.0 - fl;
   const double kv = om * prop(P, P_K_SOLID, T) + fl * prop(P, P_K_LIQUID, T);
@@ -148,7 +202,8 @@ __device__ __forceinline__ double k_prime(const DevParams& P, double T) {
 }
 
 // a'(T) = rho(T) c(T) - abar (core/properties.py:188-192).
-__device__ __forceinline__ double a_prime(const DevParams& P, double T) {
+template <class PP>
+__device__ __forceinline__ double a_prime(const PP& P, double T) {
   const double fl = fl_kernel(P, T);
   const double om = 1.0 - fl;
   const double rv = om * prop(P, P_RHO_SOLID, T) + fl * prop(P, P_RHO_LIQUID, T);
@@ -159,7 +214,8 @@ __device__ __forceinline__ double a_prime(const DevParams& P, double T) {
 // Latent sink Q = -rho(T) L_f (f_l(T) - f_l(T_prev)) / dt: blended-rho form
 // (core/properties.py:212-236) or constant form
 // (physics/spectral_cpu_kernels.py:115-140).
-__device__ __forceinline__ double latent_source(const DevParams& P, double T, double Tp) {
+template <class PP>
+__device__ __forceinline__ double latent_source(const PP& P, double T, double Tp) {
   if (P.latent_model) {
     const double flc = fl_kernel(P, T);
     const double flp = fl_kernel(P, Tp);
