@@ -240,6 +240,17 @@ int sgh_project_volume(sgh_plan* plan, const double* field, double* modes, void*
  * (physics/spectral_ops.py:83-91). Async. */
 int sgh_reconstruct_volume(sgh_plan* plan, const double* modes, double* field, void* stream);
 
+/* Warm-start flags of the instance state, for checkpoints: bit 0 = the
+ * latent modes of the previous step are present (grid mode,
+ * SpectralSolver._Q_latent_modes_prev is not None, solvers/spectral.py:328),
+ * bit 1 = the box history is present (FineMeshState.T_prev is not None,
+ * physics/spectral_ops.py:182-194). sgh_state_flags copies them to the host
+ * and synchronises the stream; sgh_state_set_flags writes them (async). */
+#define SGH_STATE_HAVE_Q_MODES   1
+#define SGH_STATE_HAVE_BOX       2
+int sgh_state_flags(sgh_plan* plan, int32_t* flags, void* stream);
+int sgh_state_set_flags(sgh_plan* plan, int32_t flags, void* stream);
+
 /* Box mode. Geometry of the fine box (host values, no device work);
  * SGH_ERR_STATE for a grid-mode plan. */
 int sgh_box_geometry(const sgh_plan* plan, sgh_box_geom* out);

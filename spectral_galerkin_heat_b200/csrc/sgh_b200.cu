@@ -147,6 +147,12 @@ __global__ void k_reset(const DevParams* __restrict__ P, Ctrl* ctrl, double* a, 
   }
 }
 
+// Warm-start flags of a restored state (sgh_state_set_flags).
+__global__ void k_set_flags(Ctrl* ctrl, int flags) {
+  ctrl->have_qprev = (flags & SGH_STATE_HAVE_Q_MODES) ? 1 : 0;
+  ctrl->have_tprev = (flags & SGH_STATE_HAVE_BOX) ? 1 : 0;
+}
+
 // ---------------------------------------------------------------------------
 // box mode: tables, window, history
 // ---------------------------------------------------------------------------
@@ -1672,6 +1678,28 @@ int sgh_reconstruct_volume(sgh_plan* p, const double* modes, double* field, void
   if (!p->bound) return fail(SGH_ERR_STATE, "plan is not bound");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   volume_pass3(p, modes, true, EpiDiv{field, p->hp.sqrt_dV, nullptr}, p->d(p->o_t1), p->d(p->o_t2), s);
+  SGH_CK(cudaGetLastError());
+  return SGH_OK;
+}
+
+int sgh_state_flags(sgh_plan* p, int32_t* flags, void* stream) {
+  if (!p || !flags) return fail(SGH_ERR_INVALID, "null argument");
+  if (!p->bound) return fail(SGH_ERR_STATE, "plan is not bound");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  int32_t v[2];
+  SGH_CK(cudaMemcpyAsync(&v[0], &p->ctrl()->have_qprev, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+  SGH_CK(cudaMemcpyAsync(&v[1], &p->ctrl()->have_tprev, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+  SGH_CK(cudaStreamSynchronize(s));
+  *flags = (v[0] ? SGH_STATE_HAVE_Q_MODES : 0) | (v[1] ? SGH_STATE_HAVE_BOX : 0);
+  return SGH_OK;
+}
+
+int sgh_state_set_flags(sgh_plan* p, int32_t flags, void* stream) {
+  if (!p) return fail(SGH_ERR_INVALID, "null argument");
+  if (!p->bound) return fail(SGH_ERR_STATE, "plan is not bound");
+  if (flags & ~(SGH_STATE_HAVE_Q_MODES | SGH_STATE_HAVE_BOX)) return fail(SGH_ERR_INVALID, "unknown flag bits");
+  if ((flags & SGH_STATE_HAVE_BOX) && !p->hp.box) return fail(SGH_ERR_INVALID, "box history flag on a grid-mode plan");
+  k_set_flags<<<1, 1, 0, static_cast<cudaStream_t>(stream)>>>(p->ctrl(), flags);
   SGH_CK(cudaGetLastError());
   return SGH_OK;
 }

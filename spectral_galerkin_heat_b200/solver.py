@@ -489,6 +489,99 @@ class B200SpectralSolver(HeatSolver):
             C.c_void_p(self.state.stream.cuda_stream)))
         return out
 
+    # ---- checkpoints ------------------------------------------------------
+    CHECKPOINT_FORMAT = "sgh_b200 modal checkpoint 1"
+
+    def _config_digest(self) -> str:
+        import hashlib
+        c = _lib.SghConfig.from_buffer_copy(bytes(self._cfg))
+        c.axis_min_ctas = 0
+        c.axis_cuda_cores = 0
+        return hashlib.sha256(bytes(c)).hexdigest()
+
+    def checkpoint(self, t: float = 0.0, step: int = 0) -> dict:
+        """Host copy of everything a later step reads, for an exact resume.
+
+        ``modes`` / ``time`` / ``step`` follow the datasets of the reference's
+        ``modes.h5`` (``io_utils/spectral_fs_io.py:207-241``): modes as
+        ``(1, nz, ny, nx)``. The rest is the warm start the reference keeps in
+        memory between steps: the previous evaporation flux
+        (``buffers.q_evap_old``), the previous converged field
+        (``_T_prev_full``), the previous latent modes (``_Q_latent_modes_prev``,
+        grid mode) and the box history (``fine_mesh.T_prev`` / ``Q_prev``).
+        """
+        self._require()
+        st = self.state
+        flags = C.c_int32()
+        _lib.check("sgh_state_flags", _lib.lib().sgh_state_flags(
+            self._plan, C.byref(flags), C.c_void_p(st.stream.cuda_stream)))
+        ck = {
+            "format": np.array(self.CHECKPOINT_FORMAT),
+            "config_digest": np.array(self._config_digest()),
+            "modes": st.a.cpu().numpy()[None].copy(),
+            "time": np.array([float(t)], dtype=np.float64),
+            "step": np.array([int(step)], dtype=np.int64),
+            "q_evap_old": st.q_evap_old.cpu().numpy().copy(),
+            "T_prev_full": st.T_prev.cpu().numpy().copy(),
+            "Q_latent_modes_prev": st.buffer("Q_modes").cpu().numpy().copy(),
+            "flags": np.array(int(flags.value), dtype=np.int32),
+        }
+        fm = st.fine_mesh
+        if fm is not None:
+            ck["fine_T_prev"] = fm._T_prev.cpu().numpy().copy()
+            ck["fine_Q_prev"] = fm._Q_prev.cpu().numpy().copy()
+        return ck
+
+    def restore(self, ck: dict) -> tuple:
+        """Load a :meth:`checkpoint` into this instance (same configuration);
+        returns ``(time, step)`` of the checkpoint."""
+        self._require()
+        torch = _torch()
+        if str(ck["format"]) != self.CHECKPOINT_FORMAT:
+            raise ValueError(f"not a {self.CHECKPOINT_FORMAT!r} checkpoint")
+        if str(ck["config_digest"]) != self._config_digest():
+            raise ValueError("checkpoint was written by an instance with another configuration")
+        st = self.state
+        modes = np.asarray(ck["modes"])
+        if modes.shape != (1, *st.shape):
+            raise ValueError(f"checkpoint modes {modes.shape} do not match {(1, *st.shape)}")
+        flags = int(ck["flags"])
+        fm = st.fine_mesh
+        if (fm is not None) != ("fine_T_prev" in ck):
+            raise ValueError("checkpoint and instance disagree on box mode")
+
+        def put(dst, arr):
+            dst.copy_(torch.as_tensor(np.ascontiguousarray(arr, dtype=np.float64)).reshape(dst.shape))
+
+        with torch.cuda.stream(st.stream):
+            put(st.a, modes[0])
+            put(st.q_evap_old, ck["q_evap_old"])
+            put(st.T_prev, ck["T_prev_full"])
+            put(st.buffer("Q_modes"), ck["Q_latent_modes_prev"])
+            if fm is not None:
+                put(fm._T_prev, ck["fine_T_prev"])
+                put(fm._Q_prev, ck["fine_Q_prev"])
+        _lib.check("sgh_state_set_flags", _lib.lib().sgh_state_set_flags(
+            self._plan, flags, C.c_void_p(st.stream.cuda_stream)))
+        st.stream.synchronize()
+        if fm is not None:
+            fm.primed = bool(flags & 2)
+        return float(ck["time"][0]), int(ck["step"][0])
+
+    def save_checkpoint(self, path: str, t: float = 0.0, step: int = 0) -> str:
+        """:meth:`checkpoint` written as ``.npz`` (dataset names as above)."""
+        ck = self.checkpoint(t, step)
+        path = str(path)
+        if not path.endswith(".npz"):
+            path += ".npz"
+        np.savez(path, **ck)
+        return path
+
+    def load_checkpoint(self, path: str) -> tuple:
+        """:meth:`restore` from a file written by :meth:`save_checkpoint`."""
+        with np.load(str(path)) as f:
+            return self.restore({k: f[k] for k in f.files})
+
     def reset(self) -> None:
         """Back to the initial condition (keeps the plan and its graph)."""
         self._require()
