@@ -188,7 +188,9 @@ k_axis(const double* __restrict__ X, const double* __restrict__ Mat, int Nout, i
 // kept on sm_100a; tcgen05 has no FP64 kind). CTA tile BM (outputs along the
 // transformed axis) x BN (columns c), 8 warps as 2 x 4, warp tile BM/2 x BN/4
 // = BM/32 m16 x BN/32 n8 MMA tiles per k8 step. Mat and X tiles stream through an
-// AXM_STAGES-deep cp.async pipeline of AXM_BK slices. Shared layouts keep the
+// cp.async pipeline of AXM_BK-slice stages, as deep as about 96 KB of shared
+// memory allows (3 to 6 stages: small tiles compute little per stage, so
+// more stages stay in flight to cover the L2 latency). Shared layouts keep the
 // fragment reads and the cp.async writes free of bank conflicts: Mat tiles
 // k-major rows of AXM_BK + 4 doubles; X tiles column-major (rows of AXM_BK + 4)
 // when the contraction axis is the contiguous one (B == 1), else n-major rows
@@ -196,7 +198,7 @@ k_axis(const double* __restrict__ X, const double* __restrict__ Mat, int Nout, i
 // offsets are computed once.
 // ---------------------------------------------------------------------------
 constexpr int AXM_BK = 16;
-constexpr int AXM_STAGES = 3;
+constexpr int AXM_SMEM_TARGET = 96 * 1024;
 constexpr int AXM_LDK = AXM_BK + 4;  // rows of AXM_BK contraction slices
 
 template <bool CONTIG, int BM, int BN>
@@ -204,8 +206,13 @@ constexpr int axm_stage_doubles() {
   return BM * AXM_LDK + (CONTIG ? BN * AXM_LDK : AXM_BK * (BN + 4));
 }
 template <bool CONTIG, int BM, int BN>
+constexpr int axm_stages() {
+  constexpr int n = AXM_SMEM_TARGET / (axm_stage_doubles<CONTIG, BM, BN>() * (int)sizeof(double));
+  return n < 3 ? 3 : (n > 6 ? 6 : n);
+}
+template <bool CONTIG, int BM, int BN>
 constexpr int axm_smem_bytes() {
-  return AXM_STAGES * axm_stage_doubles<CONTIG, BM, BN>() * (int)sizeof(double);
+  return axm_stages<CONTIG, BM, BN>() * axm_stage_doubles<CONTIG, BM, BN>() * (int)sizeof(double);
 }
 
 __device__ __forceinline__ void mma_f64_m16n8k8(double (&d)[4], const double (&a)[4], const double (&b)[2]) {
@@ -354,17 +361,18 @@ k_axis_mma(const double* __restrict__ X, const double* __restrict__ Mat, int Nou
       for (int q = 0; q < 4; ++q) acc[i][j][q] = 0.0;
 
 #pragma unroll
-  for (int st = 0; st < AXM_STAGES - 1; ++st) {
+  constexpr int STAGES = axm_stages<CONTIG, BM, BN>();
+  for (int st = 0; st < STAGES - 1; ++st) {
     if (st < nchunks) issue(st, st * AXM_BK);
     else cp_async_commit();
   }
   for (int ch = 0; ch < nchunks; ++ch) {
-    cp_async_wait<AXM_STAGES - 2>();
+    cp_async_wait<STAGES - 2>();
     __syncthreads();
-    const int nxt = ch + AXM_STAGES - 1;
-    if (nxt < nchunks) issue(nxt % AXM_STAGES, nxt * AXM_BK);
+    const int nxt = ch + STAGES - 1;
+    if (nxt < nchunks) issue(nxt % STAGES, nxt * AXM_BK);
     else cp_async_commit();
-    const double* Ms = axm_sh + (ch % AXM_STAGES) * STAGE;
+    const double* Ms = axm_sh + (ch % STAGES) * STAGE;
     const double* Xs = Ms + BM * AXM_LDK;
 #pragma unroll
     for (int k8 = 0; k8 < AXM_BK; k8 += 8) {
