@@ -237,6 +237,11 @@ k_axis_mma(const double* __restrict__ X, const double* __restrict__ Mat, int Nou
   constexpr int XPT = BN * AXM_BK / AX_THREADS;  // X elements per thread per stage
   __shared__ double red_sh[2 * (AX_THREADS / 32)];
 
+  // Launched with programmatic stream serialisation: wait for the previous
+  // kernel of the stream (complete, memory visible) before the first global
+  // access of any kind, so neither its outputs nor the buffers it still reads
+  // are touched early. Only the launch and this prologue overlap its tail.
+  asm volatile("griddepcontrol.wait;\n" ::: "memory");
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int g = lane >> 2, t = lane & 3;
   const int wm = warp >> 2, wn = warp & 3;
@@ -549,7 +554,17 @@ inline void launch_axis_mma(const double* X, const double* Mat, int Nout, int N,
     return true;
   }();
   (void)attr;
-  k_axis_mma<CONTIG, BM, BN, Epi><<<grid, AX_THREADS, bytes, st>>>(X, Mat, Nout, N, A, B, epi);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = dim3(AX_THREADS);
+  cfg.dynamicSmemBytes = bytes;
+  cfg.stream = st;
+  cudaLaunchAttribute la[1];
+  la[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  la[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = la;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, k_axis_mma<CONTIG, BM, BN, Epi>, X, Mat, Nout, N, A, B, epi);
 }
 
 template <bool CONTIG, class Epi>
