@@ -21,6 +21,8 @@
 // value) and may accumulate two partial sums or a max that are reduced per CTA
 // and written to a partials array (deterministic order).
 #pragma once
+#include <utility>
+
 #include "sgh_device.cuh"
 
 namespace sgh {
@@ -162,6 +164,8 @@ k_axis(const double* __restrict__ X, const double* __restrict__ Mat, int Nout, i
   constexpr int TK = CONTIG ? 16 * TJ : 16 * TI;
   constexpr int TC = CONTIG ? 16 * TI : 16 * TJ;
   __shared__ double red_sh[2 * (AX_THREADS / 32)];
+  // programmatic stream serialisation: nothing global before the previous kernel completes
+  asm volatile("griddepcontrol.wait;\n" ::: "memory");
   Red r;
   axis_tile<CONTIG, TI, TJ>(X, Mat, Nout, N, A, B, blockIdx.x * TC, blockIdx.y * TK, epi, r);
   if (Epi::kReduce) {
@@ -480,6 +484,26 @@ k_axis_mma(const double* __restrict__ X, const double* __restrict__ Mat, int Nou
   }
 }
 
+// Launch with programmatic stream serialisation: the kernel may be scheduled
+// while the previous kernel of the stream finishes, and must execute
+// griddepcontrol.wait before its first global access (every kernel launched
+// here does, in all CTAs).
+template <class... KArgs, class... Args>
+inline void launch_pdl(void (*kernel)(KArgs...), dim3 grid, int threads, int smem, cudaStream_t st,
+                       Args&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = dim3(threads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute la[1];
+  la[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  la[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = la;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
+
 // Launch shape of one pass. kind 2..5: the FP64 tensor-core kernel with a
 // BM x BN tile of 64 x 128, 64 x 64, 32 x 128, 32 x 64, when the pass is large
 // enough (see axis_shape); kind 1: the 2 x 4 thread tile when it yields
@@ -554,17 +578,7 @@ inline void launch_axis_mma(const double* X, const double* Mat, int Nout, int N,
     return true;
   }();
   (void)attr;
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = grid;
-  cfg.blockDim = dim3(AX_THREADS);
-  cfg.dynamicSmemBytes = bytes;
-  cfg.stream = st;
-  cudaLaunchAttribute la[1];
-  la[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  la[0].val.programmaticStreamSerializationAllowed = 1;
-  cfg.attrs = la;
-  cfg.numAttrs = 1;
-  cudaLaunchKernelEx(&cfg, k_axis_mma<CONTIG, BM, BN, Epi>, X, Mat, Nout, N, A, B, epi);
+  launch_pdl(k_axis_mma<CONTIG, BM, BN, Epi>, grid, AX_THREADS, bytes, st, X, Mat, Nout, N, A, B, epi);
 }
 
 template <bool CONTIG, class Epi>
@@ -589,11 +603,11 @@ inline void launch_axis(const double* X, const double* Mat, int Nout, int N, int
     return;
   }
   if (B == 1) {
-    if (sh.big) k_axis<true, 2, 4, Epi><<<sh.grid, AX_THREADS, 0, st>>>(X, Mat, Nout, N, A, B, epi);
-    else k_axis<true, 1, 1, Epi><<<sh.grid, AX_THREADS, 0, st>>>(X, Mat, Nout, N, A, B, epi);
+    if (sh.big) launch_pdl(k_axis<true, 2, 4, Epi>, sh.grid, AX_THREADS, 0, st, X, Mat, Nout, N, A, B, epi);
+    else launch_pdl(k_axis<true, 1, 1, Epi>, sh.grid, AX_THREADS, 0, st, X, Mat, Nout, N, A, B, epi);
   } else {
-    if (sh.big) k_axis<false, 2, 4, Epi><<<sh.grid, AX_THREADS, 0, st>>>(X, Mat, Nout, N, A, B, epi);
-    else k_axis<false, 1, 1, Epi><<<sh.grid, AX_THREADS, 0, st>>>(X, Mat, Nout, N, A, B, epi);
+    if (sh.big) launch_pdl(k_axis<false, 2, 4, Epi>, sh.grid, AX_THREADS, 0, st, X, Mat, Nout, N, A, B, epi);
+    else launch_pdl(k_axis<false, 1, 1, Epi>, sh.grid, AX_THREADS, 0, st, X, Mat, Nout, N, A, B, epi);
   }
 }
 
