@@ -913,7 +913,8 @@ def run_batch(args, rank, world, local_rank):
 def run_outputs(args, rank, world, local_rank):
     """--workload outputs: output reconstruction of a modal field -- the
     node-centred volume field of a full-volume output (sgh_nodal_temperature)
-    and 3 x 1000 profile points (sgh_points_temperature) -- at 128 x 64 x 32
+    and 3 x 1000 profile points, as arbitrary points (sgh_points_temperature)
+    and as three profile lines (sgh_line_temperature) -- at 128 x 64 x 32
     and at the serving maximum 512 x 256 x 64, against the reference's host
     algorithm (weighted DCT-I, all host threads) on the same modes."""
     from types import SimpleNamespace
@@ -951,6 +952,9 @@ def run_outputs(args, rank, world, local_rank):
             return sum(x.elapsed_time(y) for x, y in ev) / K
         nodal_ms = timed(lambda: Kn.reconstruct_temperature_DCT(ad, st))
         points_ms = timed(lambda: Kn.reconstruct_temperature_volume_at_points(ad, None, geom, st, ptd))
+        # the same 3 x 1000 points as three profile lines (each reduced once)
+        profiles_ms = timed(lambda: Kn.save_temp_profiles(ad, None, geom, st, (L[0] / 2, L[1] / 2),
+                                                          center="laser", num_points=1000))
         # e2e: modes from host memory in, the node field back to host memory
         host_a = torch.as_tensor(a).pin_memory()
 
@@ -969,6 +973,7 @@ def run_outputs(args, rank, world, local_rank):
         cpu_ms = (time.perf_counter() - t0) * 1e3 / n_cpu
         rows[f"{nx}x{ny}x{nz}"] = {
             "nodal_ms": nodal_ms, "nodal_e2e_ms": e2e_ms, "points_3000_ms": points_ms,
+            "profiles_3x1000_ms": profiles_ms,
             "nodal_cpu_reference_algorithm_ms": cpu_ms, "cpu_over_gpu": cpu_ms / nodal_ms,
             "nodal_gbs_min_traffic": nodal_bytes / (nodal_ms * 1e-3) / 1e9,
             "nodal_fp64_tflops": nodal_flop / (nodal_ms * 1e-3) / 1e12}

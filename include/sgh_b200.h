@@ -400,6 +400,18 @@ int sgh_nodal_temperature(int32_t nx, int32_t ny, int32_t nz, double Lx, double 
  * reconstruct_temperature_volume_at_points (physics/spectral_helpers.py:206-248),
  * the point evaluation behind save_temp_profiles (:251-333). coords and out
  * are device arrays; workspace: sgh_points_workspace_bytes() bytes. Async. */
+/* Temperature along a line parallel to axis (0 = x, 1 = y, 2 = z) at the fixed
+ * position (x, y, z) of the other two axes (the axis's own entry is ignored),
+ * at n_points positions coords (device, along the axis); every coordinate is
+ * clipped to the domain. The same values as sgh_points_temperature on those
+ * points, as the profiles of save_temp_profiles (physics/spectral_helpers.py:251-333)
+ * need them, but the modes are reduced once per line (two one-row axis passes)
+ * instead of once per point. out (n_points). Async. */
+int sgh_line_workspace_bytes(int32_t nx, int32_t ny, int32_t nz, uint64_t* bytes);
+int sgh_line_temperature(int32_t nx, int32_t ny, int32_t nz, double Lx, double Ly, double Lz,
+                         const double* modes, int32_t axis, double x, double y, double z, int32_t n_points,
+                         const double* coords, double* out, void* workspace, uint64_t bytes, void* stream);
+
 int sgh_points_workspace_bytes(int32_t nx, int32_t ny, int32_t nz, int32_t n_points, uint64_t* bytes);
 int sgh_points_temperature(int32_t nx, int32_t ny, int32_t nz, double Lx, double Ly, double Lz,
                            const double* modes, int32_t n_points, const double* coords, double* out,

@@ -39,7 +39,8 @@ EXPORTED = (
     "sgh_reconstruct_volume", "sgh_dctn_workspace_bytes", "sgh_dctn", "sgh_dctn_noalloc",
     "sgh_nodal_workspace_bytes", "sgh_nodal_temperature", "sgh_points_workspace_bytes",
     "sgh_points_temperature", "sgh_box_geometry", "sgh_box_window", "sgh_box_temperature",
-    "sgh_box_project", "sgh_state_flags", "sgh_state_set_flags",
+    "sgh_box_project", "sgh_state_flags", "sgh_state_set_flags", "sgh_line_workspace_bytes",
+    "sgh_line_temperature",
     "sgh_batch_create", "sgh_batch_destroy", "sgh_batch_workspace_bytes", "sgh_batch_bind",
     "sgh_batch_slot_start", "sgh_batch_slot_stop", "sgh_batch_step", "sgh_batch_step_eager",
     "sgh_batch_status",
@@ -166,6 +167,10 @@ def lib() -> C.CDLL:
             "sgh_box_temperature": ([vp, vp, vp, vp], C.c_int),
             "sgh_box_project": ([vp, vp, vp, vp], C.c_int),
             "sgh_state_flags": ([vp, C.POINTER(i32), vp], C.c_int),
+            "sgh_line_workspace_bytes": ([i32, i32, i32, u64p], C.c_int),
+            "sgh_line_temperature": ([i32, i32, i32, C.c_double, C.c_double, C.c_double, vp, i32,
+                                      C.c_double, C.c_double, C.c_double, i32, vp, vp, vp, C.c_uint64, vp],
+                                     C.c_int),
             "sgh_state_set_flags": ([vp, i32, vp], C.c_int),
         }
         for name, (args, res) in sig.items():

@@ -21,6 +21,7 @@
 // entry points check; nothing waits.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 
 #include "sgh_b200.h"
@@ -80,7 +81,37 @@ __global__ void __launch_bounds__(T) k_points(int nx, int ny, int nz, const doub
   }
 }
 
+// w[m] = C_m cos(pi m u / L), u = clip(pos, 0, L): the basis of one axis at
+// one position (a fixed coordinate of a profile line).
+__global__ void k_axis_weights(int n_modes, double L, double pos, double* w) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= n_modes) return;
+  const double u = fmin(fmax(pos, 0.0), L);
+  const double c = (m == 0) ? sqrt(1.0 / L) : sqrt(2.0 / L);
+  w[m] = c * cos(M_PI * (double)m * u / L);
+}
+
+// T_i = sum_k A[k] C_k cos(pi k x_i / L) for points x_i (clipped) along one
+// axis: the cosine series of the line, one point per thread.
+__global__ void k_line_eval(int n_modes, double L, const double* A, int n, const double* x, double* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double u = fmin(fmax(x[i], 0.0), L);
+  double t = 0.0;
+  for (int k = 0; k < n_modes; ++k) {
+    const double c = (k == 0) ? sqrt(1.0 / L) : sqrt(2.0 / L);
+    t = fma(A[k], c * cos(M_PI * (double)k * u / L), t);
+  }
+  out[i] = t;
+}
+
 inline int blocks(long long n) { return (int)((n + T - 1) / T); }
+
+size_t line_bytes(int nx, int ny, int nz) {
+  const size_t w = (size_t)nx + ny + nz;
+  const size_t t = std::max((size_t)nx * ny, (size_t)nz * ny);
+  return sizeof(double) * (w + t + (size_t)std::max(nx, std::max(ny, nz)));
+}
 
 inline bool axes_ok(int nx, int ny, int nz) {
   return nx >= 1 && ny >= 1 && nz >= 1 && nx <= 4096 && ny <= 4096 && nz <= 4096;
@@ -170,6 +201,57 @@ int sgh_points_temperature(int32_t nx, int32_t ny, int32_t nz, double Lx, double
   outputs::k_point_basis<<<outputs::blocks((long long)ny * n_points), outputs::T, 0, s>>>(ny, Ly, n_points, coords, 1, By);
   outputs::k_point_basis<<<outputs::blocks((long long)nz * n_points), outputs::T, 0, s>>>(nz, Lz, n_points, coords, 2, Bz);
   outputs::k_points<<<(n_points + 31) / 32, outputs::T, 0, s>>>(nx, ny, nz, modes, n_points, Bx, By, Bz, out);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return set_error(SGH_ERR_CUDA, cudaGetErrorString(e));
+  return SGH_OK;
+}
+
+int sgh_line_workspace_bytes(int32_t nx, int32_t ny, int32_t nz, uint64_t* bytes) {
+  if (!bytes) return set_error(SGH_ERR_INVALID, "null argument");
+  if (!outputs::axes_ok(nx, ny, nz)) return set_error(SGH_ERR_INVALID, "axis lengths must be in [1, 4096]");
+  *bytes = outputs::line_bytes(nx, ny, nz);
+  return SGH_OK;
+}
+
+int sgh_line_temperature(int32_t nx, int32_t ny, int32_t nz, double Lx, double Ly, double Lz,
+                         const double* modes, int32_t axis, double x, double y, double z, int32_t n_points,
+                         const double* coords, double* out, void* workspace, uint64_t bytes, void* stream) {
+  const int rc = outputs::check_shape(nx, ny, nz, Lx, Ly, Lz);
+  if (rc) return rc;
+  if (axis < 0 || axis > 2) return set_error(SGH_ERR_INVALID, "axis must be 0 (x), 1 (y) or 2 (z)");
+  if (n_points < 0) return set_error(SGH_ERR_INVALID, "n_points must be >= 0");
+  if (n_points == 0) return SGH_OK;
+  if (!modes || !coords || !out || !workspace) return set_error(SGH_ERR_INVALID, "null pointer");
+  if (bytes < outputs::line_bytes(nx, ny, nz))
+    return set_error(SGH_ERR_WORKSPACE, "workspace smaller than sgh_line_workspace_bytes()");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  double* wx = static_cast<double*>(workspace);
+  double* wy = wx + nx;
+  double* wz = wy + ny;
+  double* t1 = wz + nz;
+  double* A = t1 + std::max((size_t)nx * ny, (size_t)nz * ny);
+  const int S = nx * ny;
+  // weights of the two fixed axes, then two one-row axis passes that reduce
+  // the modes to the series of the line (largest reduction first)
+  if (axis == 0) {
+    outputs::k_axis_weights<<<outputs::blocks(ny), outputs::T, 0, s>>>(ny, Ly, y, wy);
+    outputs::k_axis_weights<<<outputs::blocks(nz), outputs::T, 0, s>>>(nz, Lz, z, wz);
+    launch_axis(modes, wz, 1, nz, 1, S, EpiStore{t1, 1.0, nullptr}, s);   // (ny, nx)
+    launch_axis(t1, wy, 1, ny, 1, nx, EpiStore{A, 1.0, nullptr}, s);      // (nx)
+    outputs::k_line_eval<<<outputs::blocks(n_points), outputs::T, 0, s>>>(nx, Lx, A, n_points, coords, out);
+  } else if (axis == 1) {
+    outputs::k_axis_weights<<<outputs::blocks(nx), outputs::T, 0, s>>>(nx, Lx, x, wx);
+    outputs::k_axis_weights<<<outputs::blocks(nz), outputs::T, 0, s>>>(nz, Lz, z, wz);
+    launch_axis(modes, wz, 1, nz, 1, S, EpiStore{t1, 1.0, nullptr}, s);   // (ny, nx)
+    launch_axis(t1, wx, 1, nx, ny, 1, EpiStore{A, 1.0, nullptr}, s);      // (ny)
+    outputs::k_line_eval<<<outputs::blocks(n_points), outputs::T, 0, s>>>(ny, Ly, A, n_points, coords, out);
+  } else {
+    outputs::k_axis_weights<<<outputs::blocks(nx), outputs::T, 0, s>>>(nx, Lx, x, wx);
+    outputs::k_axis_weights<<<outputs::blocks(ny), outputs::T, 0, s>>>(ny, Ly, y, wy);
+    launch_axis(modes, wx, 1, nx, nz * ny, 1, EpiStore{t1, 1.0, nullptr}, s);  // (nz, ny)
+    launch_axis(t1, wy, 1, ny, nz, 1, EpiStore{A, 1.0, nullptr}, s);           // (nz)
+    outputs::k_line_eval<<<outputs::blocks(n_points), outputs::T, 0, s>>>(nz, Lz, A, n_points, coords, out);
+  }
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return set_error(SGH_ERR_CUDA, cudaGetErrorString(e));
   return SGH_OK;

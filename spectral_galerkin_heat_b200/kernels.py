@@ -15,7 +15,8 @@ Functions with the reference kernel modules' names and meanings
   (node-centred field, :146-204) -> ``sgh_nodal_temperature``;
   ``reconstruct_temperature_volume_at_points(a, num, geom, state, coords)``
   (:206-248) -> ``sgh_points_temperature``; ``save_temp_profiles(a, num, geom,
-  state, laser_position, center, num_points)`` (:251-333) on top of them. The
+  state, laser_position, center, num_points)`` (:251-333), each line reduced
+  once (``sgh_line_temperature``) and evaluated at its points. The
   results stay on the device (torch tensors); the reference returns NumPy;
 * box mode (``physics/spectral_ops.py``): ``reconstruct_temperature_box(a, state)``
   (:173-179) -> ``sgh_box_temperature`` and ``project_box_to_modes(field_box,
@@ -246,13 +247,27 @@ def save_temp_profiles(a, num, geom, state, laser_position, center="laser", num_
         raise ValueError(f"Unknown center method: {center}")
     x_center = float(np.clip(x_center, 0.0, Lx))
     y_center = float(np.clip(y_center, 0.0, Ly))
-    axes_cfg = [("x", Lx, (None, y_center, z_top)), ("y", Ly, (x_center, None, z_top)),
-                ("z", Lz, (x_center, y_center, None))]
+    axes_cfg = [("x", Lx, (0.0, y_center, z_top)), ("y", Ly, (x_center, 0.0, z_top)),
+                ("z", Lz, (x_center, y_center, 0.0))]
+    if not (isinstance(a, torch.Tensor) and a.is_cuda):
+        raise TypeError("b200 kernels take CUDA tensors")
+    a = a.to(torch.float64).contiguous()
+    L = _lib.lib()
+    nbytes = C.c_uint64()
+    _lib.check("sgh_line_workspace_bytes", L.sgh_line_workspace_bytes(nx, ny, nz, C.byref(nbytes)))
+    ws = _workspace("line", nbytes.value, a.device)
+    stream = C.c_void_p(torch.cuda.current_stream(a.device).cuda_stream)
     profiles = {}
-    for key, L_axis, fixed in axes_cfg:
+    for axis, (key, L_axis, fixed) in enumerate(axes_cfg):
         coords = np.linspace(0.0, L_axis, num_points, dtype=np.float64)
-        pts = np.empty((num_points, 3), dtype=np.float64)
-        for col, v in enumerate(fixed):
-            pts[:, col] = coords if v is None else v
-        profiles[key] = (coords, reconstruct_temperature_volume_at_points(a, num, geom, state, pts))
+        out = torch.empty(num_points, dtype=torch.float64, device=a.device)
+        if num_points > 0:
+            xs = torch.as_tensor(coords, device=a.device)
+            # the modes reduced once along the line, then its cosine series at the points
+            _lib.check("sgh_line_temperature", L.sgh_line_temperature(
+                nx, ny, nz, Lx, Ly, Lz, C.c_void_p(a.data_ptr()), axis, float(fixed[0]), float(fixed[1]),
+                float(fixed[2]), num_points, C.c_void_p(xs.data_ptr()), C.c_void_p(out.data_ptr()),
+                C.c_void_p(ws.data_ptr()), ws.numel(), stream))
+            torch.cuda.current_stream(a.device).synchronize()
+        profiles[key] = (coords, out)
     return profiles
