@@ -300,7 +300,7 @@ def run_b200(args, rank, world, local_rank):
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
 
     # ---- device-resident throughput -----------------------------------------
-    s = B200SpectralSolver(None, _context(cfg, path), axis_cuda_cores=args.axis_cuda_cores)
+    s = B200SpectralSolver(None, _context(cfg, path), axis_cuda_cores=True if args.axis_cuda_cores else None)
     s.initialize()
     table = s.laser_table(0.0, W + K)
     osz = C.sizeof(_lib.SghStepOut)
@@ -338,7 +338,7 @@ def run_b200(args, rank, world, local_rank):
         s.finalize()
 
     # ---- end to end through the public API ----------------------------------
-    e = B200SpectralSolver(None, _context(cfg, path), axis_cuda_cores=args.axis_cuda_cores)
+    e = B200SpectralSolver(None, _context(cfg, path), axis_cuda_cores=True if args.axis_cuda_cores else None)
     e.initialize()
     dt = e.context.num.dt
     for i in range(W):
@@ -370,7 +370,8 @@ def run_b200(args, rank, world, local_rank):
         "config": dict(desc, parallelism=f"replicas x{world}" if world > 1 else "single",
                        l2="flushed between timed steps (256 MB write)",
                        axis_kernels="CUDA-core FP64" if args.axis_cuda_cores
-                       else "FP64 tensor cores (mma.sync .f64) where the pass is large enough",
+                       else "autotuner table per shape: FP64 tensor cores (mma.sync .f64) where the "
+                            "pass is large enough, or CUDA cores",
                        picard_iters_mean=float(np.mean(iters)), step_status=statuses),
         "clocks": clocks,
         "gpu_launches": launches * world,

@@ -232,13 +232,14 @@ class B200SpectralSolver(HeatSolver):
 
     def __init__(self, backend=None, context=None, *, mixing_omega=None,
                  convergence_tol=None, max_picard_iter=None, device=None, axis_min_ctas=None,
-                 axis_cuda_cores=False):
+                 axis_cuda_cores=None):
         self.backend = backend
         self.context = context
         # tile policy of the axis passes: explicit, else the autotuner's table, else default
         self.axis_min_ctas = axis_min_ctas
-        # True: every FP64 axis pass on the CUDA-core kernels (no FP64 tensor cores)
-        self.axis_cuda_cores = bool(axis_cuda_cores)
+        # True: every FP64 axis pass on the CUDA-core kernels (no FP64 tensor cores);
+        # None: the autotuner's table, else False
+        self.axis_cuda_cores = axis_cuda_cores
         self.state: Optional[B200State] = None
         self.device = device
         self._req = (mixing_omega, convergence_tol, max_picard_iter)
@@ -288,7 +289,12 @@ class B200SpectralSolver(HeatSolver):
             from .autotune import lookup
             policy = lookup(cfg)
         cfg.axis_min_ctas = int(policy or 0)
-        cfg.axis_cuda_cores = 1 if self.axis_cuda_cores else 0
+        cores = self.axis_cuda_cores
+        if cores is None:
+            from .autotune import lookup_kernel
+            cores = lookup_kernel(cfg)
+        cfg.axis_cuda_cores = 1 if cores else 0
+        self.kernel_policy = int(cfg.axis_cuda_cores)
         self.tile_policy = int(cfg.axis_min_ctas)
         plan = C.c_void_p()
         _lib.check("sgh_plan_create", L.sgh_plan_create(C.byref(cfg), C.byref(plan)))

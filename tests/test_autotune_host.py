@@ -23,3 +23,19 @@ def test_keys_and_lookup(tmp_path, monkeypatch):
     assert autotune.lookup(_cfg(40, 20, 6)) == 264
     assert autotune.lookup(_cfg(40, 20, 7)) is None  # in neither table: built-in default
     autotune._cache.clear()
+
+
+def test_kernel_choice_and_box_form(tmp_path, monkeypatch):
+    c = _cfg(80, 48, 120, latent=True)
+    c.box = 1
+    assert autotune.key_of(c) == "80x48x120:box"
+    table = tmp_path / "t.json"
+    table.write_text(json.dumps({"entries": {
+        "80x48x120:box": {"axis_min_ctas": 132, "axis_cuda_cores": 1},
+        "40x20x6:face": {"axis_min_ctas": 264}}}))
+    monkeypatch.setenv("SGH_TUNE_TABLE", str(table))
+    autotune._cache.clear()
+    assert autotune.lookup_kernel(c) == 1
+    assert autotune.lookup_kernel(_cfg(40, 20, 6)) is None   # entries without a kernel choice
+    assert autotune.lookup_kernel(_cfg(41, 20, 6)) is None   # no entry
+    autotune._cache.clear()
