@@ -1005,7 +1005,7 @@ kb_volume(BView v, R* a, const R* K, const R* KK, const double* sigma, double* Z
       zt[c] = 0.0;
       yt[c] = 0.0;
     }
-#pragma unroll 2
+#pragma unroll 4
     for (int p = 0; p < sl.nz; ++p) {
       const long long j0 = sl.vol + (long long)p * sl.S + i0;
       R av[VEC], kkv[VEC], kvv[VEC];
