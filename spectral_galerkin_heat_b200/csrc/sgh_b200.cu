@@ -247,7 +247,9 @@ k_box_shift(const DevParams* __restrict__ P, Ctrl* ctrl, const double* __restric
 // Magnitude maxima of the committed latent source over the box, its floor
 // (z = 0) and its x and y edge columns, for the truncation check
 // (SpectralSolver._check_latent_box_truncation, solvers/spectral.py:545-586).
-// Skipped when no Picard iteration ran (no source of this step).
+// Skipped when no Picard iteration ran (no source of this step). fmax drops
+// NaN sources, where the reference's max would return NaN and flag nothing;
+// such a step already reports SGH_STEP_NONFINITE.
 __global__ void __launch_bounds__(EW_THREADS)
 k_box_check(const DevParams* __restrict__ P, Ctrl* ctrl, const double* __restrict__ Q) {
   if (ctrl->iter <= 0) return;
