@@ -127,3 +127,18 @@ def test_box_functions_require_fine_mesh():
         kernels.project_box_to_modes(None, _GridState())
     with pytest.raises(RuntimeError):
         kernels.reconstruct_temperature_box(None, _GridState())
+
+
+def test_checkpoint_digest_ignores_tile_policy_only():
+    """A checkpoint names the configuration it belongs to by a digest of the
+    plan config with the tile-policy fields zeroed: a plan with other tiles may
+    restore it, a plan with other physics may not (no device needed)."""
+    from spectral_galerkin_heat_b200.solver import B200SpectralSolver
+    cfg, path, *_ = golden_case("box_const_24x12x8")
+    s = B200SpectralSolver(None, make_context(cfg, path))
+    s._cfg = make_config(s.context, 0.1, 1e-8, 10)
+    d0 = s._config_digest()
+    s._cfg.axis_min_ctas, s._cfg.axis_cuda_cores = 264, 1
+    assert s._config_digest() == d0
+    s._cfg.dt *= 2.0
+    assert s._config_digest() != d0
