@@ -117,8 +117,16 @@ typedef struct {
 typedef struct {
   double x, y, power, vx, vy;
   int32_t is_on;
-  int32_t pad;
+  int32_t flags;              /* SGH_LASER_* bits; 0 for float64 states      */
 } sgh_laser;
+
+/* x, y, vx and vy are float32 values, as a G-code path reports them
+ * (io_utils/gcode_path.py:91-119). The reference then forms the warm-start
+ * shift v*dt/dx, the box-history shift and the box window position x/dx in
+ * float32 arithmetic (solvers/spectral.py:303-305, physics/spectral_ops.py:
+ * 300-302, physics/spectral_helpers.py:74); with this bit the library does the
+ * same, so G-code-driven steps match it to rounding. */
+#define SGH_LASER_F32 1
 
 /* Metrics of one step (solvers/spectral.py:536-542), written on the device. */
 typedef struct {
@@ -369,9 +377,10 @@ int sgh_dct2_bf16x3(int32_t kind, int32_t ny, int32_t nx, const double* in, doub
  * sgh_dctn_workspace_bytes() exceeds that size is rejected with
  * SGH_ERR_WORKSPACE (about 10^6 elements for a 3-D array).
  *
- * The first call on a device looks up the scratch's device address
- * (cudaGetSymbolAddress) and caches it; make that first call before any
- * stream capture. All calls share the one scratch array: calls that overlap
+ * Every call looks up the scratch's device address on the current device
+ * (cudaGetSymbolAddress, which allocates nothing) and runs sgh_dctn on it; the
+ * first call on a device may load the library's device module there, so make
+ * that first call before any stream capture. All calls share the one scratch array: calls that overlap
  * on the GPU (different streams, or several threads) race and must be
  * serialised by the caller. The scratch keeps the previous call's contents;
  * this transform writes every scratch element it reads, so none needs

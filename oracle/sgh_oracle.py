@@ -531,7 +531,9 @@ class OracleSolver:
         mat, lp = ctx.mat, ctx.laser
         st = ctx.laser_path.get_state(t, dt)
         vx, vy = st.v
-        I0 = (float(lp.absorptivity) * st.power / (self.area_factor * float(lp.ref_area))
+        # the absorptivity is a float64 scalar in the reference, so a float32
+        # power (G-code paths) is widened before the product (core/laser.py:110-112)
+        I0 = (float(lp.absorptivity) * float(st.power) / (self.area_factor * float(lp.ref_area))
               if st.is_on else 0.0)
         q_las = self.laser_flux(st.x, st.y, I0)
         P_laser = float(np.sum(q_las) * self.dx * self.dy)

@@ -77,7 +77,7 @@ class SghConfig(C.Structure):
 
 class SghLaser(C.Structure):
     _fields_ = [("x", C.c_double), ("y", C.c_double), ("power", C.c_double),
-                ("vx", C.c_double), ("vy", C.c_double), ("is_on", C.c_int32), ("pad", C.c_int32)]
+                ("vx", C.c_double), ("vy", C.c_double), ("is_on", C.c_int32), ("flags", C.c_int32)]
 
 
 class SghStepOut(C.Structure):

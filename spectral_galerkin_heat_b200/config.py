@@ -23,13 +23,14 @@ The solver only reads these objects by attribute, so the reference's own
 """
 from __future__ import annotations
 
+import os
 from dataclasses import dataclass, field
 from typing import Any, Optional
 
 import numpy as np
 
-from .laser import LaserPath, LaserState  # noqa: F401  (re-exported)
-from .properties import MaterialModel
+from .laser import GCodeLaserPath, LaserPath, LaserState  # noqa: F401  (re-exported)
+from .properties import MaterialModel, TempProperty
 
 __all__ = [
     "Vec3", "NumParams", "MaterialParams", "GeomParams", "LaserParams",
@@ -172,19 +173,61 @@ class FineMeshParams:
     box_size: Vec3 = Vec3(0.9e-3, 0.9e-3, 0.04e-3)
 
 
-_SECTION_KEYS = {
-    "simulation": {"name", "backend", "dtype", "dt", "duration", "update_interval",
-                   "max_picard_iter", "picard_tol", "picard_omega"},
-    "domain": {"size", "mesh"},
-    "material": {"name", "rho", "k", "Cp", "L_f", "T_solidus", "T_liquidus", "T0",
-                 "Pa", "R_v", "T_boil", "DeltaH_LV", "h_conv_top", "h_conv_bottom"},
-    "laser": {"radius", "absorptivity", "power_nominal", "profile", "r_x", "r_y",
-              "super_gaussian_order", "cell_integrated", "path"},
-    "fine_mesh": {"refinement", "box_size"},
-}
-_PASSTHROUGH = {"io", "post_processing"}
+# ---------------------------------------------------------------------------
+# Schema. Each section maps its keys to a reader: how the raw value is turned
+# into a number (``kind``), the SI unit a ``{value, unit}`` mapping must carry
+# (``unit``) and the default of an absent key (``_NEED`` = the key is
+# required). The keys and defaults are the reference's schema
+# (``core/parameters.py:415-437, 514-682``); the reading machinery is this
+# module's own. Readers of kind "real" round to the configured precision.
+# ---------------------------------------------------------------------------
 
-# SI unit spellings accepted in a {value, unit} mapping, per target quantity.
+_NEED = object()
+
+
+@dataclass(frozen=True)
+class _Key:
+    kind: str                 # real | float | int | opt_int | opt_float | vec | ivec | str | bool | raw
+    unit: Optional[str] = None
+    default: Any = _NEED
+
+
+_SCHEMA: dict[str, dict[str, _Key]] = {
+    "simulation": {
+        "name": _Key("raw", default=None), "backend": _Key("str", default="b200"),
+        "dtype": _Key("raw", default="float32"), "dt": _Key("float", "s"),
+        "duration": _Key("float", "s", 0.01), "update_interval": _Key("float", "s", 1e-3),
+        "max_picard_iter": _Key("opt_int", default=None),
+        "picard_tol": _Key("opt_float", default=None),
+        "picard_omega": _Key("opt_float", default=None),
+    },
+    "domain": {"size": _Key("vec", "m"), "mesh": _Key("ivec")},
+    "material": {
+        "name": _Key("raw", default="Material"),
+        # k / rho / Cp may carry solid and liquid branches: _property_constants()
+        "rho": _Key("raw"), "k": _Key("raw"), "Cp": _Key("raw"),
+        "L_f": _Key("real", "J/kg", 0.0), "T_solidus": _Key("real", "K", 0.0),
+        "T_liquidus": _Key("real", "K", 0.0), "T0": _Key("real", "K", 0.0),
+        "Pa": _Key("real", "Pa", 0.0), "R_v": _Key("real", "J/kgK", 0.0),
+        "T_boil": _Key("real", "K", 0.0), "DeltaH_LV": _Key("real", "J/kg", 0.0),
+        "h_conv_top": _Key("real", "W/m2K", 0.0), "h_conv_bottom": _Key("real", "W/m2K", 0.0),
+    },
+    "laser": {
+        "radius": _Key("real", "m"), "absorptivity": _Key("real"),
+        "power_nominal": _Key("real", "W"), "profile": _Key("str", default="gaussian"),
+        "r_x": _Key("real", "m", 0.0), "r_y": _Key("real", "m", 0.0),
+        "super_gaussian_order": _Key("float", default=2.0),
+        "cell_integrated": _Key("bool", default=False), "path": _Key("raw", default=None),
+    },
+    "fine_mesh": {"refinement": _Key("int", default=4),
+                  "box_size": _Key("vec", "m", (0.9e-3, 0.9e-3, 0.04e-3))},
+    "laser.path": {"type": _Key("str", default=""), "file": _Key("raw", default=None),
+                   "initial_position": _Key("raw", default=(0.0, 0.0))},
+}
+# Sections carried through unread.
+_UNREAD = ("io", "post_processing")
+
+# SI spellings accepted in a {value, unit} mapping, per unit family.
 _SI_SPELLINGS = {
     "m": {"m"}, "s": {"s"}, "K": {"K", "kelvin"}, "W": {"W"}, "Pa": {"Pa"},
     "kg/m3": {"kg/m3", "kg/m**3", "kg / m**3", "kg/m^3"},
@@ -193,46 +236,122 @@ _SI_SPELLINGS = {
     "J/kg": {"J/kg", "J / kg"},
     "W/m2K": {"W/(m2.K)", "W/(m**2*K)", "W / (m**2 * K)", "W/m2/K", "W/(m^2.K)"},
 }
+_PROPERTY_UNITS = {"k": "W/mK", "rho": "kg/m3", "Cp": "J/kgK"}
 
 
-def _scalar(raw, si=None) -> float:
-    if isinstance(raw, dict):
-        unit = raw.get("unit")
-        if unit and si is not None and unit.strip() not in _SI_SPELLINGS[si]:
-            raise ValueError(
-                f"Unit {unit!r} is not the SI unit {si!r}; this backend reads SI values only.")
-        return float(raw["value"])
-    if isinstance(raw, bool) or not isinstance(raw, (int, float, np.floating, np.integer)):
-        raise TypeError(f"Cannot extract a value from type {type(raw)}")
-    return float(raw)
+def _unwrap(raw, unit):
+    """The payload of a ``{value, unit}`` mapping (checked to be SI), or ``raw``."""
+    if not isinstance(raw, dict):
+        return raw
+    given = (raw.get("unit") or "").strip()
+    if given and unit is not None and given not in _SI_SPELLINGS[unit]:
+        raise ValueError(f"unit {given!r} given where {unit!r} is expected: this backend "
+                         "reads SI values only (no unit conversion)")
+    return raw["value"]
 
 
-def _vector(raw, si=None) -> list:
-    if isinstance(raw, dict):
-        unit = raw.get("unit")
-        if unit and si is not None and unit.strip() not in _SI_SPELLINGS[si]:
-            raise ValueError(
-                f"Unit {unit!r} is not the SI unit {si!r}; this backend reads SI values only.")
-        return [float(v) for v in raw["value"]]
-    if isinstance(raw, (list, tuple)):
-        return [_scalar(v, si) for v in raw]
-    raise TypeError(f"Cannot extract a vector from type {type(raw)}")
+def _number(raw, unit=None) -> float:
+    v = _unwrap(raw, unit)
+    if isinstance(v, bool) or not isinstance(v, (int, float, np.floating, np.integer)):
+        raise TypeError(f"expected a number, got {type(v).__name__}")
+    return float(v)
 
 
-def _validate(cfg: dict) -> None:
-    known = set(_SECTION_KEYS) | _PASSTHROUGH
-    for section in cfg:
-        if section not in known:
-            raise ValueError(f"Unknown config section {section!r}. "
-                             f"Valid sections: {', '.join(sorted(known))}.")
-    for section, allowed in _SECTION_KEYS.items():
-        body = cfg.get(section)
-        if isinstance(body, dict):
-            for key in body:
-                if key not in allowed:
-                    raise ValueError(
-                        f"Unknown key {key!r} in the {section!r} config section. "
-                        f"Valid keys: {', '.join(sorted(allowed))}.")
+_READERS = {
+    "raw": lambda raw, unit, real: raw,
+    "str": lambda raw, unit, real: str(raw),
+    "bool": lambda raw, unit, real: bool(raw),
+    "float": lambda raw, unit, real: _number(raw, unit),
+    "real": lambda raw, unit, real: real(_number(raw, unit)),
+    "int": lambda raw, unit, real: int(_number(raw, unit)),
+    "opt_int": lambda raw, unit, real: None if raw is None else int(raw),
+    "opt_float": lambda raw, unit, real: None if raw is None else float(raw),
+    "vec": lambda raw, unit, real: [_number(v, unit) for v in _sequence(raw, unit)],
+    "ivec": lambda raw, unit, real: [int(_number(v)) for v in _sequence(raw, unit)],
+}
+
+
+def _sequence(raw, unit):
+    seq = _unwrap(raw, unit)
+    if not isinstance(seq, (list, tuple)):
+        raise TypeError(f"expected a sequence of numbers, got {type(seq).__name__}")
+    return seq
+
+
+def _check_keys(cfg: dict) -> None:
+    """Refuse unknown sections and keys before anything is read."""
+    for name in cfg:
+        if name not in _SCHEMA and name not in _UNREAD:
+            known = sorted(set(_SCHEMA) - {"laser.path"} | set(_UNREAD))
+            raise ValueError(f"config section {name!r} is not part of the schema "
+                             f"(sections: {', '.join(known)})")
+    bodies = {name: cfg.get(name) for name in _SCHEMA}
+    laser = cfg.get("laser")
+    bodies["laser.path"] = laser.get("path") if isinstance(laser, dict) else None
+    for name, body in bodies.items():
+        if not isinstance(body, dict):
+            continue
+        extra = sorted(set(body) - set(_SCHEMA[name]))
+        if extra:
+            raise ValueError(f"key {extra[0]!r} is not part of config section {name!r} "
+                             f"(keys: {', '.join(sorted(_SCHEMA[name]))})")
+
+
+def _read(cfg: dict, section: str, real) -> dict:
+    """Every key of ``section`` read through its schema entry."""
+    body = cfg.get(section) or {}
+    out = {}
+    for key, spec in _SCHEMA[section].items():
+        if key in body:
+            out[key] = _READERS[spec.kind](body[key], spec.unit, real)
+        elif spec.default is _NEED:
+            raise KeyError(f"config section {section!r} needs the key {key!r}")
+        else:
+            out[key] = spec.default
+    return out
+
+
+def _gcode_path(cfg: dict, config_dir: Optional[str]):
+    """The G-code laser path a ``laser.path`` section names, or None."""
+    laser = cfg.get("laser") or {}
+    if not isinstance(laser.get("path"), dict):
+        return None
+    path = _read({"laser.path": laser["path"]}, "laser.path", float)
+    if path["type"].lower() != "gcode" or path["file"] is None:
+        return None
+    name = str(path["file"])
+    if not os.path.isabs(name):
+        base = (os.path.join(config_dir, "paths") if config_dir is not None
+                else os.path.join(os.getcwd(), "simulations", "examples", "paths"))
+        name = os.path.abspath(os.path.join(base, name))
+        laser["path"]["file"] = name          # the reference writes the resolved name back
+    return GCodeLaserPath(name, initial_position=tuple(path["initial_position"]))
+
+
+def _property_constants(m: dict, raw: dict, model: Optional[MaterialModel], real) -> dict:
+    """The constant ``k`` / ``rho`` / ``Cp`` of the ETD1 propagators.
+
+    Without a model they are the section's numbers. With one, a property that
+    varies with T takes its ``reference:`` value (required), and a constant
+    one its value at T0 (``core/parameters.py:593-630``)."""
+    if model is None:
+        return {key: real(_number(raw[key], unit)) for key, unit in _PROPERTY_UNITS.items()}
+    varying = [key for key in _PROPERTY_UNITS
+               if TempProperty._branches(raw[key]) is not None
+               and not model.by_config_key(key).is_constant]
+    lacking = [key for key in varying if "reference" not in raw[key]]
+    if lacking:
+        rec = dict(zip(("k", "rho", "Cp"),
+                       model.recommended_references(float(m["T0"]), float(m["T_boil"]))))
+        hint = ", ".join(f"{key}.reference={rec[key]:g}" for key in lacking)
+        raise ValueError(
+            f"temperature-dependent {lacking} lack the 'reference:' constant that splits "
+            f"each property into its implicit and explicit parts; a value in the middle of "
+            f"the working range converges best (midpoints of the extrema over [T0, T_boil]: "
+            f"{hint})")
+    return {key: real(_number(raw[key]["reference"], unit)) if key in varying
+            else real(float(model.by_config_key(key)(float(m["T0"]))))
+            for key, unit in _PROPERTY_UNITS.items()}
 
 
 @dataclass
@@ -252,101 +371,49 @@ class SimulationContext:
     def from_dict(cls, cfg: dict, config_dir: Optional[str] = None) -> "SimulationContext":
         """Parse a config dict with the reference's schema.
 
-        The laser path is left ``None`` unless the config names a G-code file,
-        which this backend does not parse: set ``ctx.laser_path`` to a
-        :class:`LaserPath` instead.
+        A ``laser.path`` of type ``gcode`` is read with :class:`GCodeLaserPath`;
+        a relative file name is looked up in ``<config_dir>/paths`` (or
+        ``./simulations/examples/paths`` without a ``config_dir``), as the
+        reference does. Other paths leave ``laser_path`` ``None``: assign a
+        :class:`LaserPath` to it.
         """
-        _validate(cfg)
-        sim = cfg.get("simulation", {})
-        real_t = resolve_dtype(sim.get("dtype", "float32"))
-        dom = cfg.get("domain", {})
-        Lx, Ly, Lz = _vector(dom["size"], "m")
-        nx, ny, nz = _vector(dom["mesh"])
-        t_end = _scalar(sim.get("duration", 0.01), "s")
-        dt_nominal = float(real_t(_scalar(sim["dt"], "s")))
-        n_steps = round(t_end / dt_nominal)
-        dt = t_end / n_steps
+        _check_keys(cfg)
+        real = resolve_dtype((cfg.get("simulation") or {}).get("dtype", "float32"))
+        sim = _read(cfg, "simulation", real)
+        dom = _read(cfg, "domain", real)
+        m = _read(cfg, "material", real)
+        las = _read(cfg, "laser", real)
+
+        # the step is re-derived so that n_steps * dt == t_end exactly
+        dt_nominal = float(real(sim["dt"]))
+        n_steps = round(sim["duration"] / dt_nominal)
+        mesh = [int(v) for v in dom["mesh"]]
         num = NumParams(
-            dt=dt, nx=int(nx), ny=int(ny), nz=int(nz), t_end=t_end, n_steps=n_steps,
-            dt_nominal=dt_nominal,
-            update_interval=_scalar(sim.get("update_interval", 1e-3), "s"),
-            max_picard_iter=(int(sim["max_picard_iter"])
-                             if sim.get("max_picard_iter") is not None else None),
-            picard_tol=(float(sim["picard_tol"]) if sim.get("picard_tol") is not None else None),
-            picard_omega=(float(sim["picard_omega"])
-                          if sim.get("picard_omega") is not None else None),
-            dtype=real_t,
-        )
-        geom = GeomParams(size=Vec3(Lx, Ly, Lz), n=Vec3(int(nx), int(ny), int(nz)))
+            dt=sim["duration"] / n_steps, nx=mesh[0], ny=mesh[1], nz=mesh[2],
+            t_end=sim["duration"], n_steps=n_steps, dt_nominal=dt_nominal,
+            update_interval=sim["update_interval"], max_picard_iter=sim["max_picard_iter"],
+            picard_tol=sim["picard_tol"], picard_omega=sim["picard_omega"], dtype=real)
+        geom = GeomParams(size=Vec3(*dom["size"]), n=Vec3(*mesh))
 
-        fine_cfg = cfg.get("fine_mesh")
         fine = None
-        if fine_cfg is not None:
-            box = fine_cfg.get("box_size", (0.9e-3, 0.9e-3, 0.04e-3))
-            bx = [_scalar(v, "m") for v in box]
-            fine = FineMeshParams(refinement=int(_scalar(fine_cfg.get("refinement", 4))),
-                                  box_size=Vec3(*bx))
+        if cfg.get("fine_mesh") is not None:
+            fm = _read(cfg, "fine_mesh", real)
+            fine = FineMeshParams(refinement=fm["refinement"], box_size=Vec3(*fm["box_size"]))
 
-        m = cfg.get("material", {})
-        T_sol = real_t(_scalar(m.get("T_solidus", 0.0), "K"))
-        T_liq = real_t(_scalar(m.get("T_liquidus", 0.0), "K"))
-        T0 = real_t(_scalar(m.get("T0", 0.0), "K"))
-        T_boil = real_t(_scalar(m.get("T_boil", 0.0), "K"))
-        model = MaterialModel.from_config(m, float(T_sol), float(T_liq))
-        units = {"k": "W/mK", "rho": "kg/m3", "Cp": "J/kgK"}
-        if model is None:
-            rho = real_t(_scalar(m["rho"], "kg/m3"))
-            k = real_t(_scalar(m["k"], "W/mK"))
-            cp = real_t(_scalar(m["Cp"], "J/kgK"))
-        else:
-            refs, missing = {}, []
-            for key, prop in (("k", model.k), ("rho", model.rho), ("Cp", model.c)):
-                spec = m.get(key)
-                branched = isinstance(spec, dict) and ("solid" in spec or "liquid" in spec)
-                if branched and not prop.is_constant:
-                    if "reference" not in spec:
-                        missing.append(key)
-                        continue
-                    refs[key] = real_t(_scalar(spec["reference"], units[key]))
-                else:
-                    refs[key] = real_t(float(prop(float(T0))))
-            if missing:
-                rec = dict(zip(("k", "rho", "Cp"),
-                               model.recommended_references(float(T0), float(T_boil))))
-                hint = ", ".join(f"{k}.reference={rec[k]:g}" for k in missing)
-                raise ValueError(
-                    f"Temperature-dependent material property {missing} needs an explicit "
-                    f"'reference:' key inside its block. Recommended values: {hint}.")
-            k, rho, cp = refs["k"], refs["rho"], refs["Cp"]
+        raw_props = {key: m[key] for key in _PROPERTY_UNITS}
+        model = MaterialModel.from_config(raw_props, float(m["T_solidus"]),
+                                          float(m["T_liquidus"]))
+        consts = _property_constants(m, raw_props, model, real)
         mat = MaterialParams(
-            name=m.get("name", "Material"), rho=rho, k=k, Cp=cp,
-            L_f=real_t(_scalar(m.get("L_f", 0.0), "J/kg")),
-            T_solidus=T_sol, T_liquidus=T_liq,
-            Pa=real_t(_scalar(m.get("Pa", 0.0), "Pa")),
-            R_v=real_t(_scalar(m.get("R_v", 0.0), "J/kgK")),
-            T_boil=T_boil,
-            DeltaH_LV=real_t(_scalar(m.get("DeltaH_LV", 0.0), "J/kg")),
-            T0=T0,
-            h_conv_top=real_t(_scalar(m.get("h_conv_top", 0.0), "W/m2K")),
-            h_conv_bottom=real_t(_scalar(m.get("h_conv_bottom", 0.0), "W/m2K")),
-            model=model,
-        )
-        lc = cfg.get("laser", {})
+            name=m["name"], rho=consts["rho"], k=consts["k"], Cp=consts["Cp"], model=model,
+            **{key: m[key] for key in ("L_f", "T_solidus", "T_liquidus", "Pa", "R_v", "T_boil",
+                                       "DeltaH_LV", "T0", "h_conv_top", "h_conv_bottom")})
         laser = LaserParams(
-            radius=real_t(_scalar(lc["radius"], "m")),
-            absorptivity=real_t(_scalar(lc["absorptivity"])),
-            power=real_t(_scalar(lc["power_nominal"], "W")),
-            profile=str(lc.get("profile", "gaussian")),
-            r_x=real_t(_scalar(lc.get("r_x", 0.0), "m")),
-            r_y=real_t(_scalar(lc.get("r_y", 0.0), "m")),
-            super_gaussian_order=_scalar(lc.get("super_gaussian_order", 2.0)),
-            cell_integrated=bool(lc.get("cell_integrated", False)),
-        )
-        path_cfg = lc.get("path", {}) or {}
-        if str(path_cfg.get("type", "")).lower() == "gcode":
-            raise ValueError("G-code laser paths are not parsed by this backend; "
-                             "assign a LaserPath to context.laser_path instead.")
-        return cls(num=num, mat=mat, geom=geom, laser=laser, laser_path=None,
-                   io=cfg.get("io", {}), backend=str(sim.get("backend", "b200")).lower(),
-                   fine=fine)
-
+            radius=las["radius"], absorptivity=las["absorptivity"], power=las["power_nominal"],
+            profile=las["profile"],
+            r_x=las["r_x"], r_y=las["r_y"],
+            super_gaussian_order=las["super_gaussian_order"],
+            cell_integrated=las["cell_integrated"])
+        return cls(num=num, mat=mat, geom=geom, laser=laser,
+                   laser_path=_gcode_path(cfg, config_dir), io=cfg.get("io", {}),
+                   backend=sim["backend"].lower(), fine=fine)

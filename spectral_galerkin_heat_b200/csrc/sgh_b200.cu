@@ -23,7 +23,6 @@
 
 #include <algorithm>
 #include <cmath>
-#include <mutex>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -177,8 +176,8 @@ __global__ void k_fine_basis(int n_modes, int n_pts, double L, double d, double 
 // Start of the window of n_box fine cells centred on pos, clamped to the fine
 // grid (_calculate_subgrid_indices, physics/spectral_helpers.py:49-85).
 // Python's round() rounds half to even, as rint() does.
-__device__ int box_start(double pos, double d, int n_total, int n_box) {
-  const double g = rint(fmax(0.0, fmin(pos / d, (double)(n_total - 1))));
+__device__ int box_start(double q, int n_total, int n_box) {
+  const double g = rint(fmax(0.0, fmin(q, (double)(n_total - 1))));
   long long st = (long long)g - n_box / 2;
   const long long max_start = n_total > n_box ? n_total - n_box : 0;
   if (st > max_start) st = max_start;
@@ -299,8 +298,9 @@ __global__ void k_step_begin(const DevParams* __restrict__ P, Ctrl* ctrl,
   if (ctrl->table) ctrl->laser = ctrl->table[ctrl->step];
   const sgh_laser L = ctrl->laser;
   ctrl->I0 = L.is_on ? P->absorptivity * L.power / (P->area_factor * (P->r_x * P->r_y)) : 0.0;
-  ctrl->shift_x = (L.vx * P->dt) / P->dx;
-  ctrl->shift_y = (L.vy * P->dt) / P->dy;
+  const bool f32 = (L.flags & SGH_LASER_F32) != 0;
+  ctrl->shift_x = laser_shift(L.vx, P->dt, P->dx, f32);
+  ctrl->shift_y = laser_shift(L.vy, P->dt, P->dy, f32);
   ctrl->iter = 0;
   ctrl->stop = 0;
   ctrl->status = SGH_STEP_CAPPED;
@@ -309,10 +309,10 @@ __global__ void k_step_begin(const DevParams* __restrict__ P, Ctrl* ctrl,
   if (P->box) {
     // window of this step and the history shift in fine pixels
     // (physics/spectral_state.py:229-237, physics/spectral_ops.py:300-302)
-    ctrl->box_i0x = box_start(L.x, P->dxf, P->fx, P->xb);
-    ctrl->box_i0y = box_start(L.y, P->dyf, P->fy, P->yb);
-    ctrl->box_sx = -((L.vx * P->dt) / P->dxf);
-    ctrl->box_sy = -((L.vy * P->dt) / P->dyf);
+    ctrl->box_i0x = box_start(laser_cells(L.x, P->dxf, f32), P->fx, P->xb);
+    ctrl->box_i0y = box_start(laser_cells(L.y, P->dyf, f32), P->fy, P->yb);
+    ctrl->box_sx = -laser_shift(L.vx, P->dt, P->dxf, f32);
+    ctrl->box_sy = -laser_shift(L.vy, P->dt, P->dyf, f32);
     for (int j = 0; j < 4; ++j) ctrl->box_max[j] = 0ull;
     if (in_graph) cudaGraphSetConditional(h_seed, ctrl->have_tprev ? 0u : 1u);
   }
@@ -1843,29 +1843,6 @@ int sgh_dctn(int32_t kind, int32_t ndim, const int32_t* shape, const double* in,
 // is not a device address in host code.
 static __device__ __align__(256) double g_noalloc_scratch[SGH_NOALLOC_SCRATCH_BYTES / sizeof(double)];
 
-namespace {
-constexpr int kMaxNoallocDevices = 64;
-std::mutex g_noalloc_mutex;
-void* g_noalloc_ptr[kMaxNoallocDevices] = {};
-
-// Device address of g_noalloc_scratch on the current device, looked up once per
-// device (first call on that device) and cached.
-int noalloc_scratch(void** out) {
-  int dev = -1;
-  SGH_CK(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= kMaxNoallocDevices) return fail(SGH_ERR_UNSUPPORTED, "device ordinal out of range");
-  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-  if (!g_noalloc_ptr[dev]) {
-    void* ptr = nullptr;
-    SGH_CK(cudaGetSymbolAddress(&ptr, g_noalloc_scratch));
-    if (!ptr) return fail(SGH_ERR_CUDA, "cudaGetSymbolAddress returned a null scratch address");
-    g_noalloc_ptr[dev] = ptr;
-  }
-  *out = g_noalloc_ptr[dev];
-  return SGH_OK;
-}
-}  // namespace
-
 int sgh_dctn_noalloc(int32_t kind, int32_t ndim, const int32_t* shape, const double* in, double* out,
                      void* stream) {
   if (!in || !out) return fail(SGH_ERR_INVALID, "null argument");
@@ -1878,39 +1855,13 @@ int sgh_dctn_noalloc(int32_t kind, int32_t ndim, const int32_t* shape, const dou
                 "array too large for sgh_dctn_noalloc: needs " + std::to_string(L.total) +
                     " bytes of scratch, the built-in scratch holds " +
                     std::to_string((unsigned long long)SGH_NOALLOC_SCRATCH_BYTES) + "; use sgh_dctn");
+  // The device address of the scratch on the current device, looked up on
+  // every call (no allocation, and nothing cached that a context reset could
+  // leave stale).
   void* scratch = nullptr;
-  const int rs = noalloc_scratch(&scratch);
-  if (rs) return rs;
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
-  char* ws = static_cast<char*>(scratch);
-  const double* mats[3];
-  for (int a = 0; a < 3; ++a) {
-    const int N = L.n[a];
-    double* M = reinterpret_cast<double*>(ws + L.o_mat[a]);
-    k_dct_matrix<<<cdiv((long)N * N, EW_THREADS), EW_THREADS, 0, s>>>(N, M, M + (size_t)N * N);
-    mats[a] = (kind == 2) ? M : M + (size_t)N * N;
-  }
-  double* t1 = reinterpret_cast<double*>(ws + L.o_t1);
-  double* t2 = reinterpret_cast<double*>(ws + L.o_t2);
-  const int n0 = L.n[0], n1 = L.n[1], n2 = L.n[2];
-  const int first = 3 - L.ndim;
-  const double* src = in;
-  double* bufs[2] = {t1, t2};
-  int nb = 0;
-  if (L.ndim == 1 && in == out) {
-    SGH_CK(cudaMemcpyAsync(t2, in, sizeof(double) * (size_t)n2, cudaMemcpyDeviceToDevice, s));
-    src = t2;
-  }
-  for (int a = 2; a >= first; --a) {
-    double* dst = (a == first) ? out : bufs[nb++ & 1];
-    const int N = L.n[a];
-    const int A = (a == 2) ? n0 * n1 : (a == 1 ? n0 : 1);
-    const int B = (a == 2) ? 1 : (a == 1 ? n2 : n1 * n2);
-    launch_axis(src, mats[a], N, N, A, B, EpiStore{dst, 1.0, nullptr}, s);
-    src = dst;
-  }
-  SGH_CK(cudaGetLastError());
-  return SGH_OK;
+  SGH_CK(cudaGetSymbolAddress(&scratch, g_noalloc_scratch));
+  if (!scratch) return fail(SGH_ERR_CUDA, "cudaGetSymbolAddress returned a null scratch address");
+  return sgh_dctn(kind, ndim, shape, in, out, scratch, SGH_NOALLOC_SCRATCH_BYTES, stream);
 }
 
 }  // extern "C"

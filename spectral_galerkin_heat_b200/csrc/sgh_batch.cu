@@ -280,8 +280,9 @@ __global__ void __launch_bounds__(CT) kb_begin(BView v, cudaGraphConditionalHand
     st.laser = st.table[st.step];
     const sgh_laser L = st.laser;
     st.I0 = L.is_on ? sl.absorptivity * L.power / (sl.area_factor * (sl.r_x * sl.r_y)) : 0.0;
-    st.shift_x = (L.vx * sl.dt) / sl.dx;
-    st.shift_y = (L.vy * sl.dt) / sl.dy;
+    const bool f32 = (L.flags & SGH_LASER_F32) != 0;
+    st.shift_x = laser_shift(L.vx, sl.dt, sl.dx, f32);
+    st.shift_y = laser_shift(L.vy, sl.dt, sl.dy, f32);
     st.iter = 0;
     st.status = SGH_STEP_CAPPED;
     st.rel_err = nan("");

@@ -265,6 +265,22 @@ __device__ __forceinline__ double laser_flux(const PP& P, double I0, double x0, 
   return I0 * shape;
 }
 
+// Shift v*dt/d in cells of size d. A float32 laser state (SGH_LASER_F32,
+// G-code paths) has the reference form it in float32: the product with a
+// Python float dt and the quotient by a Python float d both round to float32
+// (solvers/spectral.py:303-305, physics/spectral_cpu_kernels.py:392-396).
+__device__ __forceinline__ double laser_shift(double v, double dt, double d, bool f32) {
+  if (f32) return (double)__fdiv_rn(__fmul_rn((float)v, (float)dt), (float)d);
+  return (v * dt) / d;
+}
+
+// Position in cells, x/d (physics/spectral_helpers.py:74), float32 for a
+// float32 laser state.
+__device__ __forceinline__ double laser_cells(double x, double d, bool f32) {
+  if (f32) return (double)__fdiv_rn((float)x, (float)d);
+  return x / d;
+}
+
 // Order-1 shift table entry for output index o (physics/spectral_cpu_kernels.py:305-325).
 struct ShiftTap {
   int i0, i1;

@@ -23,7 +23,7 @@ import numpy as np
 __all__ = [
     "LaserState", "LaserPath", "LaserProfile", "build_laser_profile",
     "super_gaussian_area_factor", "StraightTrack", "RasterPath", "FixedLaser",
-    "LASER_DTYPE", "laser_table",
+    "GCodeLaserPath", "LASER_DTYPE", "LASER_F32", "laser_table",
 ]
 
 
@@ -141,9 +141,137 @@ class RasterPath(LaserPath):
         return LaserState(x=x, y=y, power=self.power if on else 0.0, is_on=on, v=(vx, 0.0))
 
 
-# One ``sgh_laser`` record (include/sgh_b200.h): x, y, power, vx, vy, is_on, pad.
+_F32 = np.float32
+
+# Segment table of a G-code path: start and end point, start and end time and
+# power, all single precision (the reference quantises them so), and laser on.
+_SEGMENT_DTYPE = np.dtype([("x0", "<f4"), ("y0", "<f4"), ("x1", "<f4"), ("y1", "<f4"),
+                           ("t0", "<f4"), ("t1", "<f4"), ("power", "<f4"), ("on", "?")])
+
+
+class GCodeLaserPath(LaserPath):
+    """Laser path read from a G-code file (``io_utils/gcode_path.py:25-119``).
+
+    Understood: ``G21`` (millimetres) and ``G20`` (inches) set the unit, metres
+    otherwise; ``G0``/``G1`` move to ``X``/``Y`` at feed ``F`` (unit per
+    minute); ``M3 S<W>`` switches the beam on at that power and ``M5`` off. A
+    move made while the beam is on becomes a timed segment; moves with the beam
+    off relocate it without taking time. Text after ``;`` is a comment.
+
+    Positions, times and powers are kept in single precision, and ``get_state``
+    interpolates them in single precision, because the reference does so: the
+    states it returns (numpy float32 scalars) are the reference's bit for bit,
+    and the solver forms the quantities it derives from them (warm-start shift,
+    box window) in single precision too (``LASER_F32``).
+    """
+
+    def __init__(self, gcode_file, initial_position=(0.0, 0.0)):
+        self.file = str(gcode_file)
+        with open(self.file) as fh:
+            self.segments, self.unit_scale = self.parse(fh.read().splitlines())
+        self.initial_position = (_F32(initial_position[0]) * _F32(self.unit_scale),
+                                 _F32(initial_position[1]) * _F32(self.unit_scale))
+
+    @staticmethod
+    def parse(lines):
+        """``(segment table, unit scale)`` of G-code text lines."""
+        scale, power, on, feed = 1.0, 0.0, False, 0.0
+        pos = [0.0, 0.0]
+        last = None
+        clock = 0.0
+        rows = []
+        for raw in lines:
+            line = raw.split(";", 1)[0].strip()
+            if not line:
+                continue
+            if line.startswith("G21"):
+                scale = 1.0 / 1000.0
+            elif line.startswith("G20"):
+                scale = 25.4 / 1000.0
+            elif line.startswith(("G0", "G1")):
+                for word in line.split()[1:]:
+                    axis, val = word[0], word[1:]
+                    if axis in "XY" and val:
+                        pos["XY".index(axis)] = float(_F32(float(val) * scale))
+                    elif axis == "F" and val:
+                        feed = _F32(float(val) * scale)
+                if last is not None and on:
+                    length = float(np.sqrt((pos[0] - last[0]) ** 2 + (pos[1] - last[1]) ** 2))
+                    speed = float(feed) / 60.0 if feed > 0 else 1.0
+                    end = float(clock + (length / speed if speed > 0 else 0.0))
+                    rows.append((last[0], last[1], pos[0], pos[1], clock, end, power, True))
+                    clock = end
+                last = list(pos)
+            elif line.startswith("M3"):
+                for word in line.split()[1:]:
+                    if word.startswith("S"):
+                        power = float(word[1:])
+                on = True
+            elif line.startswith("M5"):
+                on, power = False, 0.0
+        return np.array(rows, dtype=_SEGMENT_DTYPE), scale
+
+    def get_state(self, time, dt):
+        tab = self.table(np.array([float(time)]), float(dt))[0]
+        return LaserState(x=_F32(tab["x"]), y=_F32(tab["y"]), power=_F32(tab["power"]),
+                          is_on=bool(tab["is_on"]), v=(_F32(tab["vx"]), _F32(tab["vy"])))
+
+    def table(self, times, dt: float) -> np.ndarray:
+        """States at float64 ``times`` (each the value of a Python float time
+        ``t``; the step ``dt`` a Python float) as ``sgh_laser`` records, with
+        the reference's single-precision arithmetic: a Python float meets a
+        float32 scalar in float32, and the velocity is a float64 difference
+        quotient rounded to float32."""
+        times = np.asarray(times, dtype=np.float64)
+        out = np.zeros(times.shape, dtype=LASER_DTYPE)
+        out["flags"] = LASER_F32
+        t32 = times.astype(_F32)
+        seg = self.segments
+        hit = np.full(times.shape, -1, dtype=np.int64)
+        for i in range(len(seg) - 1, -1, -1):            # first matching segment wins
+            inside = (seg["t0"][i] <= t32) & (t32 <= seg["t1"][i])
+            hit = np.where(inside, i, hit)
+        found = hit >= 0
+        if found.any():
+            s = seg[hit[found]]
+            tf = t32[found]
+            span = s["t1"] - s["t0"]
+            frac = np.where(s["t1"] > s["t0"], (tf - s["t0"]) / np.where(span > 0, span, _F32(1)),
+                            _F32(0))
+            x = (s["x0"] + frac * (s["x1"] - s["x0"])).astype(_F32)
+            y = (s["y0"] + frac * (s["y1"] - s["y0"])).astype(_F32)
+            moving = (tf > s["t0"]) & (dt > 0.0)
+            tp = (times[found] - dt).astype(_F32)
+            use = (tp >= s["t0"]) & (span > 0)
+            pfrac = np.where(use, (tp - s["t0"]) / np.where(span > 0, span, _F32(1)), _F32(0))
+            px = (s["x0"] + pfrac * (s["x1"] - s["x0"])).astype(_F32)
+            py = (s["y0"] + pfrac * (s["y1"] - s["y0"])).astype(_F32)
+            with np.errstate(all="ignore"):
+                vx = ((x.astype(np.float64) - px.astype(np.float64)) / dt).astype(_F32)
+                vy = ((y.astype(np.float64) - py.astype(np.float64)) / dt).astype(_F32)
+            out["x"][found], out["y"][found] = x, y
+            out["power"][found] = s["power"]
+            out["is_on"][found] = s["on"].astype(np.int32)
+            out["vx"][found] = np.where(moving, vx, _F32(0))
+            out["vy"][found] = np.where(moving, vy, _F32(0))
+        rest = ~found
+        if rest.any():
+            after = rest & (len(seg) > 0) & (t32 > (seg["t1"][-1] if len(seg) else _F32(0)))
+            if after.any():
+                out["x"][after], out["y"][after] = seg["x1"][-1], seg["y1"][-1]
+            before = rest & ~after
+            out["x"][before], out["y"][before] = self.initial_position
+        return out
+
+
+# Flag of an ``sgh_laser`` record whose position and velocity are float32
+# values (G-code paths): the library then forms the warm-start shift and the
+# box window from them in float32 arithmetic, as the reference does.
+LASER_F32 = 1
+
+# One ``sgh_laser`` record (include/sgh_b200.h): x, y, power, vx, vy, is_on, flags.
 LASER_DTYPE = np.dtype([("x", "<f8"), ("y", "<f8"), ("power", "<f8"), ("vx", "<f8"),
-                        ("vy", "<f8"), ("is_on", "<i4"), ("pad", "<i4")])
+                        ("vy", "<f8"), ("is_on", "<i4"), ("flags", "<i4")])
 
 
 def laser_table(path: LaserPath, t0: float, dt: float, n: int) -> np.ndarray:
@@ -175,7 +303,11 @@ def laser_table(path: LaserPath, t0: float, dt: float, n: int) -> np.ndarray:
         out["vx"] = np.where(even, path.speed, -path.speed)
         out["is_on"] = np.where(off, 0, 1)
         return out
+    if isinstance(path, GCodeLaserPath):
+        return path.table(times, float(dt))
     for i, t in enumerate(times):
         st = path.get_state(float(t), dt)
-        out[i] = (st.x, st.y, st.power, st.v[0], st.v[1], 1 if st.is_on else 0, 0)
+        single = isinstance(st.x, np.float32) and isinstance(st.v[0], np.float32)
+        out[i] = (st.x, st.y, st.power, st.v[0], st.v[1], 1 if st.is_on else 0,
+                  LASER_F32 if single else 0)
     return out

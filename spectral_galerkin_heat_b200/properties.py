@@ -1,30 +1,35 @@
-"""Temperature-dependent material properties and their device bytecode.
+"""Temperature-dependent material properties, compiled to device bytecode.
 
-Mirrors the reference's property model: the whitelisted expression grammar of
-``core/property_expr.py`` (:53-157, names ``T``, ``pi``, ``e``; ``+ - * / **``;
-unary ``+``/``-``; the function list of ``_NUMPY_FUNC_NAME`` :68-76),
-``liquid_fraction`` / ``TempProperty`` / ``MaterialModel`` of
-``core/properties.py`` (:61-150, :242-479).
+The configuration language is the reference's (``core/property_expr.py:53-157``
+defines the grammar; ``core/properties.py:61-150, 242-479`` the solid/liquid
+model): a property branch is a number or an expression of ``T`` built from
+numeric literals, the names ``T``, ``pi`` and ``e``, the operators
+``+ - * / **``, unary ``+``/``-`` and calls of a fixed list of one-argument
+math functions (two for ``atan2``). Config files written for the reference
+therefore parse to the same properties here.
 
-The reference turns each expression into generated CUDA-C compiled at run
-time. Here every expression is compiled once, on the host, into a short
-postfix program (``SGH_OP_*`` opcodes of ``include/sgh_b200.h``) that the
-kernels interpret per cell. All threads of a launch run the same program, so
-the interpreter loop is warp-uniform; operations are applied in the same order
-as the Python evaluation of the tree, which keeps FP64 results equal to the
-host evaluation up to the last-ulp differences of the transcendental functions.
+The implementation is this library's own. An expression is lowered in one
+pass, straight from Python's syntax tree, into the postfix program that the
+CUDA kernels interpret per cell (``SGH_OP_*`` opcodes of
+``include/sgh_b200.h``, ``eval_program`` in ``csrc/sgh_device.cuh``). Every
+node kind has one lowering rule in a dispatch table; a node kind with no rule,
+or a rule that refuses its node, is a ``ValueError`` raised while lowering, so
+validation and compilation are the same walk. Host-side values
+(``PropertyExpr.__call__``, the reference constants, the recommended
+references) come from :class:`Program.run`, a NumPy stack machine that executes
+the very program the device runs, in the same operation order.
 """
 from __future__ import annotations
 
 import ast
 import math
 from dataclasses import dataclass
-from typing import Any, Optional
+from typing import Any, Callable, Optional
 
 import numpy as np
 
-__all__ = ["PropertyExpr", "TempProperty", "MaterialModel", "liquid_fraction",
-           "OPCODES", "MAX_PROGRAM", "MAX_STACK"]
+__all__ = ["PropertyExpr", "TempProperty", "MaterialModel", "Program", "liquid_fraction",
+           "compile_expression", "OPCODES", "MAX_PROGRAM", "MAX_STACK"]
 
 # Opcode numbers; must match the SGH_OP_* enum in include/sgh_b200.h.
 OPCODES = {
@@ -34,189 +39,232 @@ OPCODES = {
     "asinh": 30, "acosh": 31, "atanh": 32, "fabs": 33, "ceil": 34, "floor": 35,
     "trunc": 36, "log1p": 37, "expm1": 38, "atan2": 48,
 }
-MAX_PROGRAM = 64   # instructions per expression (SGH_MAX_PROGRAM)
+MAX_PROGRAM = 64   # instruction slots per expression (SGH_MAX_PROGRAM)
 MAX_STACK = 16     # evaluation stack depth (SGH_MAX_STACK)
 
-_NUMPY_NAME = {
-    "sqrt": "sqrt", "exp": "exp", "log": "log", "log2": "log2", "log10": "log10",
-    "sin": "sin", "cos": "cos", "tan": "tan", "asin": "arcsin", "acos": "arccos",
-    "atan": "arctan", "atan2": "arctan2", "sinh": "sinh", "cosh": "cosh", "tanh": "tanh",
-    "asinh": "arcsinh", "acosh": "arccosh", "atanh": "arctanh", "fabs": "abs",
-    "ceil": "ceil", "floor": "floor", "trunc": "trunc", "log1p": "log1p", "expm1": "expm1",
+# Host semantics of every opcode: (arity, numpy implementation).
+_HOST_OP: dict[int, tuple[int, Callable]] = {
+    OPCODES["add"]: (2, np.add), OPCODES["sub"]: (2, np.subtract),
+    OPCODES["mul"]: (2, np.multiply), OPCODES["div"]: (2, np.true_divide),
+    OPCODES["pow"]: (2, np.power), OPCODES["atan2"]: (2, np.arctan2),
+    OPCODES["neg"]: (1, np.negative),
+    OPCODES["sqrt"]: (1, np.sqrt), OPCODES["exp"]: (1, np.exp), OPCODES["log"]: (1, np.log),
+    OPCODES["log2"]: (1, np.log2), OPCODES["log10"]: (1, np.log10),
+    OPCODES["sin"]: (1, np.sin), OPCODES["cos"]: (1, np.cos), OPCODES["tan"]: (1, np.tan),
+    OPCODES["asin"]: (1, np.arcsin), OPCODES["acos"]: (1, np.arccos),
+    OPCODES["atan"]: (1, np.arctan), OPCODES["sinh"]: (1, np.sinh),
+    OPCODES["cosh"]: (1, np.cosh), OPCODES["tanh"]: (1, np.tanh),
+    OPCODES["asinh"]: (1, np.arcsinh), OPCODES["acosh"]: (1, np.arccosh),
+    OPCODES["atanh"]: (1, np.arctanh), OPCODES["fabs"]: (1, np.abs),
+    OPCODES["ceil"]: (1, np.ceil), OPCODES["floor"]: (1, np.floor),
+    OPCODES["trunc"]: (1, np.trunc), OPCODES["log1p"]: (1, np.log1p),
+    OPCODES["expm1"]: (1, np.expm1),
 }
-_CONSTANTS = {"pi": math.pi, "e": math.e}
+# Callable names of the grammar -> opcode; the operand count is in _HOST_OP.
+_CALLS = {name: OPCODES[name] for name in (
+    "sqrt", "exp", "log", "log2", "log10", "sin", "cos", "tan", "asin", "acos", "atan",
+    "atan2", "sinh", "cosh", "tanh", "asinh", "acosh", "atanh", "fabs", "ceil", "floor",
+    "trunc", "log1p", "expm1")}
+_NAMED_CONSTANTS = {"pi": math.pi, "e": math.e}
+_BINARY = {ast.Add: "add", ast.Sub: "sub", ast.Mult: "mul", ast.Div: "div", ast.Pow: "pow"}
 
 
-def _check(node) -> None:
-    if isinstance(node, ast.Constant):
-        if isinstance(node.value, bool) or not isinstance(node.value, (int, float)):
-            raise ValueError(f"Only numeric literals are allowed, got {node.value!r}.")
-    elif isinstance(node, ast.Name):
-        if node.id != "T" and node.id not in _CONSTANTS:
-            raise ValueError(f"Unknown name {node.id!r} in property expression "
-                             f"(only 'T' and {sorted(_CONSTANTS)} are allowed).")
-    elif isinstance(node, ast.BinOp):
-        if not isinstance(node.op, (ast.Add, ast.Sub, ast.Mult, ast.Div, ast.Pow)):
-            raise ValueError(f"Operator {type(node.op).__name__} is not allowed.")
-        _check(node.left)
-        _check(node.right)
-    elif isinstance(node, ast.UnaryOp):
-        if not isinstance(node.op, (ast.UAdd, ast.USub)):
-            raise ValueError(f"Unary operator {type(node.op).__name__} is not allowed.")
-        _check(node.operand)
-    elif isinstance(node, ast.Call):
-        if (not isinstance(node.func, ast.Name) or node.func.id not in _NUMPY_NAME
-                or node.keywords or not node.args):
-            raise ValueError(f"Function {getattr(node.func, 'id', '<expr>')!r} is not "
-                             "allowed in a property expression.")
-        want = 2 if node.func.id == "atan2" else 1
-        if len(node.args) != want:
-            raise ValueError(f"{node.func.id} takes {want} argument(s).")
-        for a in node.args:
-            _check(a)
-    else:
-        raise ValueError(f"{type(node).__name__} is not allowed in a property expression.")
+@dataclass(frozen=True)
+class Program:
+    """A postfix program: ``ops`` holds opcode numbers, and every ``const``
+    opcode is followed by the index of its value in ``consts``."""
+
+    ops: tuple
+    consts: tuple
+
+    @property
+    def max_depth(self) -> int:
+        """Deepest evaluation stack the program needs."""
+        depth = peak = 0
+        for op, _ in self._decode():
+            if op in (OPCODES["const"], OPCODES["T"]):
+                depth += 1
+            else:
+                depth -= _HOST_OP[op][0] - 1
+            peak = max(peak, depth)
+        return peak
+
+    def _decode(self):
+        i = 0
+        while i < len(self.ops):
+            op = self.ops[i]
+            if op == OPCODES["const"]:
+                yield op, self.consts[self.ops[i + 1]]
+                i += 2
+            else:
+                yield op, None
+                i += 1
+
+    def run(self, T):
+        """Execute on a scalar or an array of temperatures (float64)."""
+        T = np.asarray(T, dtype=np.float64) if not np.isscalar(T) else float(T)
+        stack: list = []
+        for op, value in self._decode():
+            if op == OPCODES["const"]:
+                stack.append(value)
+            elif op == OPCODES["T"]:
+                stack.append(T)
+            else:
+                arity, fn = _HOST_OP[op]
+                args = stack[-arity:]
+                del stack[-arity:]
+                stack.append(fn(*args))
+        (out,) = stack
+        # a program without T still yields one value per temperature
+        return out + np.zeros_like(T) if np.ndim(T) else out
+
+
+class _Lowering:
+    """One expression's lowering into a :class:`Program` (single use)."""
+
+    def __init__(self, source: str):
+        self.source = source
+        self.ops: list[int] = []
+        self.consts: list[float] = []
+
+    def fail(self, what: str):
+        raise ValueError(f"property expression {self.source!r}: {what}")
+
+    def emit_const(self, value: float):
+        self.ops += [OPCODES["const"], len(self.consts)]
+        self.consts.append(float(value))
+
+    def lower(self, node):
+        rule = self.RULES.get(type(node))
+        if rule is None:
+            self.fail(f"{type(node).__name__} nodes are outside the property grammar")
+        rule(self, node)
+
+    def _constant(self, node):
+        v = node.value
+        if isinstance(v, bool) or not isinstance(v, (int, float)):
+            self.fail(f"literal {v!r} is not a real number")
+        self.emit_const(v)
+
+    def _name(self, node):
+        if node.id == "T":
+            self.ops.append(OPCODES["T"])
+        elif node.id in _NAMED_CONSTANTS:
+            self.emit_const(_NAMED_CONSTANTS[node.id])
+        else:
+            self.fail(f"name {node.id!r} is undefined; the variable is 'T' and the "
+                      f"constants are {sorted(_NAMED_CONSTANTS)}")
+
+    def _binary(self, node):
+        op = _BINARY.get(type(node.op))
+        if op is None:
+            self.fail(f"operator {type(node.op).__name__} is outside the property grammar")
+        self.lower(node.left)
+        self.lower(node.right)
+        self.ops.append(OPCODES[op])
+
+    def _unary(self, node):
+        if isinstance(node.op, ast.UAdd):
+            self.lower(node.operand)
+        elif isinstance(node.op, ast.USub):
+            self.lower(node.operand)
+            self.ops.append(OPCODES["neg"])
+        else:
+            self.fail(f"unary operator {type(node.op).__name__} is outside the property grammar")
+
+    def _call(self, node):
+        name = node.func.id if isinstance(node.func, ast.Name) else None
+        if name not in _CALLS:
+            self.fail(f"call of {ast.unparse(node.func)!r} is outside the property grammar")
+        if node.keywords:
+            self.fail(f"{name}() takes positional arguments only")
+        arity = _HOST_OP[_CALLS[name]][0]
+        if len(node.args) != arity:
+            self.fail(f"{name}() takes {arity} argument(s), got {len(node.args)}")
+        for arg in node.args:
+            self.lower(arg)
+        self.ops.append(_CALLS[name])
+
+    RULES = {ast.Constant: _constant, ast.Name: _name, ast.BinOp: _binary,
+             ast.UnaryOp: _unary, ast.Call: _call}
+
+
+def compile_expression(source) -> Program:
+    """Lower a property expression (or a bare number) to a device :class:`Program`."""
+    text = str(source).strip()
+    low = _Lowering(text)
+    try:
+        low.emit_const(float(text))
+    except ValueError:
+        try:
+            tree = ast.parse(text, mode="eval")
+        except SyntaxError as exc:
+            raise ValueError(f"property expression {text!r} does not parse: {exc.msg}") from None
+        low.lower(tree.body)
+    prog = Program(tuple(low.ops), tuple(low.consts))
+    if len(prog.ops) > MAX_PROGRAM:
+        raise ValueError(f"property expression {text!r} needs {len(prog.ops)} program slots; "
+                         f"the device interpreter holds {MAX_PROGRAM}")
+    if prog.max_depth > MAX_STACK:
+        raise ValueError(f"property expression {text!r} nests deeper than the device "
+                         f"stack ({MAX_STACK})")
+    return prog
 
 
 class PropertyExpr:
-    """A validated expression of ``T`` (or a bare constant)."""
+    """A property branch: a number or an expression of ``T``, held as its program."""
 
-    __slots__ = ("source", "_const", "_tree")
+    __slots__ = ("source", "_prog", "_number")
 
     def __init__(self, expr):
         self.source = str(expr).strip()
+        self._prog = compile_expression(self.source)
         try:
-            self._const = float(self.source)
-            self._tree = None
-            return
+            self._number = float(self.source)
         except ValueError:
-            pass
-        try:
-            tree = ast.parse(self.source, mode="eval").body
-        except SyntaxError as exc:
-            raise ValueError(f"Invalid property expression {self.source!r}: {exc}") from None
-        _check(tree)
-        self._const, self._tree = None, tree
+            self._number = None
 
     @property
     def is_constant(self) -> bool:
-        return self._const is not None
+        """True for a bare number (an expression without ``T`` still counts as
+        an expression, as in the reference)."""
+        return self._number is not None
 
     @property
     def constant_value(self) -> float:
-        if self._const is None:
-            raise ValueError(f"{self.source!r} is not a constant expression.")
-        return self._const
+        if self._number is None:
+            raise ValueError(f"{self.source!r} is an expression, not a number")
+        return self._number
 
     def __call__(self, T):
-        if self._const is not None:
-            return T * 0.0 + self._const
-        return _evaluate(self._tree, T)
+        return self._prog.run(T)
 
     def program(self) -> tuple[list[int], list[float]]:
-        """Postfix program ``(ops, consts)``: ``ops`` holds opcode numbers, and
-        each ``const`` opcode is followed by the index of its value in ``consts``."""
-        ops: list[int] = []
-        consts: list[float] = []
-        if self._const is not None:
-            ops += [OPCODES["const"], 0]
-            consts.append(self._const)
-        else:
-            _emit(self._tree, ops, consts)
-        if len(ops) > MAX_PROGRAM:
-            raise ValueError(f"Property expression {self.source!r} is too long for the "
-                             f"device interpreter ({len(ops)} > {MAX_PROGRAM} slots).")
-        if _stack_depth(ops) > MAX_STACK:
-            raise ValueError(f"Property expression {self.source!r} nests too deeply.")
-        return ops, consts
+        """``(ops, consts)`` of the device program."""
+        return list(self._prog.ops), list(self._prog.consts)
 
     def __repr__(self):
         return f"PropertyExpr({self.source!r})"
 
 
-def _evaluate(node, T):
-    if isinstance(node, ast.Constant):
-        return node.value
-    if isinstance(node, ast.Name):
-        return T if node.id == "T" else _CONSTANTS[node.id]
-    if isinstance(node, ast.BinOp):
-        a, b = _evaluate(node.left, T), _evaluate(node.right, T)
-        op = type(node.op)
-        if op is ast.Add:
-            return a + b
-        if op is ast.Sub:
-            return a - b
-        if op is ast.Mult:
-            return a * b
-        if op is ast.Div:
-            return a / b
-        return a ** b
-    if isinstance(node, ast.UnaryOp):
-        v = _evaluate(node.operand, T)
-        return -v if isinstance(node.op, ast.USub) else v
-    fn = getattr(np, _NUMPY_NAME[node.func.id])
-    return fn(*(_evaluate(a, T) for a in node.args))
-
-
-def _emit(node, ops, consts) -> None:
-    if isinstance(node, ast.Constant):
-        ops += [OPCODES["const"], len(consts)]
-        consts.append(float(node.value))
-    elif isinstance(node, ast.Name):
-        if node.id == "T":
-            ops.append(OPCODES["T"])
-        else:
-            ops += [OPCODES["const"], len(consts)]
-            consts.append(_CONSTANTS[node.id])
-    elif isinstance(node, ast.BinOp):
-        _emit(node.left, ops, consts)
-        _emit(node.right, ops, consts)
-        ops.append(OPCODES[{ast.Add: "add", ast.Sub: "sub", ast.Mult: "mul",
-                            ast.Div: "div", ast.Pow: "pow"}[type(node.op)]])
-    elif isinstance(node, ast.UnaryOp):
-        _emit(node.operand, ops, consts)
-        if isinstance(node.op, ast.USub):
-            ops.append(OPCODES["neg"])
-    else:
-        for a in node.args:
-            _emit(a, ops, consts)
-        ops.append(OPCODES[node.func.id])
-
-
-def _stack_depth(ops) -> int:
-    depth = peak = 0
-    i = 0
-    while i < len(ops):
-        op = ops[i]
-        if op == OPCODES["const"]:
-            depth += 1
-            i += 2
-            peak = max(peak, depth)
-            continue
-        if op == OPCODES["T"]:
-            depth += 1
-        elif op in (3, 4, 5, 6, 7, OPCODES["atan2"]):
-            depth -= 1
-        peak = max(peak, depth)
-        i += 1
-    return peak
-
-
 def liquid_fraction(T, T_solidus, T_liquidus):
-    """``clip((T - T_s)/(T_l - T_s), 0, 1)``; a step at ``T_s`` when ``T_l <= T_s``."""
-    if T_liquidus <= T_solidus:
-        if hasattr(T, "shape"):
-            return np.where(np.asarray(T) >= T_solidus, 1.0, 0.0).astype(T.dtype)
-        return 1.0 if T >= T_solidus else 0.0
-    f = (T - T_solidus) / (T_liquidus - T_solidus)
-    if hasattr(f, "clip"):
-        return f.clip(0.0, 1.0)
-    return min(max(f, 0.0), 1.0)
+    """Liquid fraction: a linear ramp from 0 at the solidus to 1 at the liquidus,
+    or a step at the solidus when the band is empty (``T_liquidus <= T_solidus``).
+    Arrays keep their dtype; scalars give a float."""
+    Ts, Tl = float(T_solidus), float(T_liquidus)
+    arr = np.asarray(T)
+    if Tl > Ts:
+        f = np.clip((arr - Ts) / (Tl - Ts), 0.0, 1.0)
+    else:
+        f = (arr >= Ts).astype(arr.dtype if arr.dtype.kind == "f" else np.float64)
+    return f if np.ndim(T) else float(f)
 
 
 @dataclass
 class TempProperty:
-    """One property with solid and liquid branches blended by the liquid fraction."""
+    """One property: solid and liquid branches blended by the liquid fraction,
+    ``p(T) = (1 - f_l) p_solid(T) + f_l p_liquid(T)``. ``is_constant`` marks a
+    property whose branches are the same number (the constant-coefficient path)."""
 
     solid: PropertyExpr
     liquid: PropertyExpr
@@ -227,20 +275,36 @@ class TempProperty:
     def __call__(self, T):
         if self.is_constant:
             return self.solid(T)
-        fl = liquid_fraction(T, self.T_solidus, self.T_liquidus)
-        return (1.0 - fl) * self.solid(T) + fl * self.liquid(T)
+        f = liquid_fraction(T, self.T_solidus, self.T_liquidus)
+        return (1.0 - f) * self.solid(T) + f * self.liquid(T)
+
+    @staticmethod
+    def _branches(spec) -> Optional[tuple]:
+        """``(solid, liquid)`` sources of a branch mapping (one missing branch
+        takes the other), or None for a scalar spec."""
+        if not isinstance(spec, dict):
+            return None
+        present = [spec[k] for k in ("solid", "liquid") if k in spec]
+        if not present:
+            return None
+        return spec.get("solid", present[0]), spec.get("liquid", present[0])
 
     @classmethod
     def from_config(cls, spec: Any, T_solidus: float, T_liquidus: float) -> "TempProperty":
-        if isinstance(spec, dict) and ("solid" in spec or "liquid" in spec):
-            solid = PropertyExpr(spec.get("solid", spec.get("liquid")))
-            liquid = PropertyExpr(spec.get("liquid", spec.get("solid")))
-            const = (solid.is_constant and liquid.is_constant
-                     and solid.constant_value == liquid.constant_value)
-            return cls(solid, liquid, float(T_solidus), float(T_liquidus), const)
-        value = spec["value"] if isinstance(spec, dict) else spec
-        c = PropertyExpr(value)
-        return cls(c, c, float(T_solidus), float(T_liquidus), True)
+        """From a number, a ``{value, unit}`` mapping or a ``{solid, liquid}``
+        mapping (whose ``reference``/``unit`` keys the config parser reads)."""
+        band = (float(T_solidus), float(T_liquidus))
+        branches = cls._branches(spec)
+        if branches is None:
+            c = PropertyExpr(spec["value"] if isinstance(spec, dict) else spec)
+            return cls(c, c, *band, is_constant=True)
+        s, l = PropertyExpr(branches[0]), PropertyExpr(branches[1])
+        same = s.is_constant and l.is_constant and s.constant_value == l.constant_value
+        return cls(s, l, *band, is_constant=same)
+
+
+# config key -> MaterialModel field
+_MODEL_FIELDS = (("k", "k"), ("rho", "rho"), ("Cp", "c"))
 
 
 @dataclass
@@ -256,27 +320,28 @@ class MaterialModel:
 
     @property
     def is_constant(self) -> bool:
-        return self.k.is_constant and self.rho.is_constant and self.c.is_constant
+        return all(getattr(self, f).is_constant for _, f in _MODEL_FIELDS)
+
+    def by_config_key(self, key: str) -> TempProperty:
+        """The property of config key ``k`` / ``rho`` / ``Cp``."""
+        return getattr(self, dict(_MODEL_FIELDS)[key])
 
     def recommended_references(self, T_lo: float, T_hi: float, n_samples: int = 512):
-        """Midpoint of each property's extrema over ``[T_lo, T_hi]`` -> ``(k, rho, Cp)``."""
+        """``(k, rho, Cp)`` reference constants: for each property the midpoint of
+        its smallest and largest value on ``n_samples`` points of ``[T_lo, T_hi]``."""
         T = np.linspace(float(T_lo), float(T_hi), int(n_samples))
-
-        def mid(p):
-            v = np.asarray(p(T), dtype=np.float64)
-            return 0.5 * (float(v.min()) + float(v.max()))
-
-        return mid(self.k), mid(self.rho), mid(self.c)
+        out = []
+        for _, f in _MODEL_FIELDS:
+            v = np.asarray(getattr(self, f)(T), dtype=np.float64)
+            out.append(0.5 * (float(v.min()) + float(v.max())))
+        return tuple(out)
 
     @classmethod
     def from_config(cls, mat_cfg: dict, T_solidus: float, T_liquidus: float
                     ) -> Optional["MaterialModel"]:
-        def branched(s):
-            return isinstance(s, dict) and ("solid" in s or "liquid" in s)
-
-        specs = {"k": mat_cfg.get("k"), "rho": mat_cfg.get("rho"), "c": mat_cfg.get("Cp")}
-        if not any(branched(s) for s in specs.values()):
+        """The model of a material section, or None when no property has branches."""
+        specs = {key: mat_cfg.get(key) for key, _ in _MODEL_FIELDS}
+        if all(TempProperty._branches(s) is None for s in specs.values()):
             return None
-        return cls(k=TempProperty.from_config(specs["k"], T_solidus, T_liquidus),
-                   rho=TempProperty.from_config(specs["rho"], T_solidus, T_liquidus),
-                   c=TempProperty.from_config(specs["c"], T_solidus, T_liquidus))
+        return cls(**{f: TempProperty.from_config(specs[key], T_solidus, T_liquidus)
+                      for key, f in _MODEL_FIELDS})

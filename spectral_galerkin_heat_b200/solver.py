@@ -35,7 +35,7 @@ from typing import Any, Optional
 import numpy as np
 
 from . import _lib
-from .laser import build_laser_profile
+from .laser import LASER_F32, build_laser_profile
 from .properties import PropertyExpr
 
 logger = logging.getLogger(__name__)
@@ -134,6 +134,9 @@ def laser_struct(state, dt: float, plan_dt: float) -> _lib.SghLaser:
         vx, vy = vx * dt / plan_dt, vy * dt / plan_dt
     L.vx, L.vy = float(vx), float(vy)
     L.is_on = 1 if state.is_on else 0
+    # float32 states (G-code paths): shifts and the box window in float32
+    single = isinstance(state.x, np.float32) and isinstance(state.v[0], np.float32)
+    L.flags = LASER_F32 if single and dt == plan_dt else 0
     return L
 
 

@@ -41,7 +41,8 @@ import numpy as np
 from .laser import RasterPath, StraightTrack
 
 __all__ = ["MATERIAL_316L", "straight_track", "nonlinear_raster", "precision_track",
-           "uneven_batch", "serving_stream", "serving_config", "scaled", "box_track"]
+           "uneven_batch", "serving_stream", "serving_config", "scaled", "box_track",
+           "example03", "MATERIAL_316L_TDEP"]
 
 MATERIAL_316L = {
     "name": "316L", "rho": 7900.0, "k": 20.0, "Cp": 500.0, "L_f": 0.0,
@@ -110,6 +111,41 @@ def box_track(nx=80, ny=48, nz=120, steps=140, dt=5e-6, size=(0.6e-3, 0.4e-3, 0.
     }
     y = size[1] / 2.0 if y0 is None else y0
     return cfg, StraightTrack(x0, y, speed, 0.0, power)
+
+
+# Temperature-dependent 316L of the reference's example 03
+# (``simulations/examples/03_nonlinear_tdep.yaml:54-96``): distinct solid and
+# liquid branches blended by the liquid fraction, a quadratic rho(T), a liquid
+# Cp given as a constant string, and the reference constants of that file.
+MATERIAL_316L_TDEP = {
+    "name": "316L",
+    "k": {"solid": "9.248 + 0.01571 * T", "liquid": "12.41 + 0.003279 * T",
+          "reference": 24.5075},
+    "rho": {"solid": "8084.2 - 0.42086 * T - 3.8942e-5 * T**2",
+            "liquid": "7432.7 + 0.039338 * T - 1.8007e-4 * T**2", "reference": 6896.2365},
+    "Cp": {"solid": "458.98 + 0.1328 * T", "liquid": "769.86", "reference": 633.8752},
+    "L_f": 2.677e5, "T_solidus": 1674.15, "T_liquidus": 1697.15, "T0": 293.0,
+    "h_conv_bottom": 3000.0, "DeltaH_LV": 7.416e6, "R_v": 150.774, "Pa": 101325.0,
+    "T_boil": 3090.0,
+}
+
+
+def example03(nx=100, ny=60, nz=96, steps=50, dt=4e-6, box=False, power=24.0):
+    """The reference's example-03 layout: 0.5 x 0.3 x 0.12 mm box, the T-dependent
+    316L block above, Picard capped at 80 with omega 0.31 (tolerance at the
+    default), a 30 um / A = 0.3 beam moving along +x at 0.15 m/s from
+    (0.2, 0.15) mm; ``box`` adds the example's refinement-2 fine box
+    (0.2 x 0.15 x 0.04 mm). ``(cfg, path)``."""
+    cfg = {
+        "simulation": {"backend": "b200", "dtype": "float64", "dt": dt, "duration": steps * dt,
+                       "max_picard_iter": 80, "picard_omega": 0.31},
+        "domain": {"size": [0.5e-3, 0.3e-3, 0.12e-3], "mesh": [nx, ny, nz]},
+        "material": copy.deepcopy(MATERIAL_316L_TDEP),
+        "laser": {"radius": 30e-6, "absorptivity": 0.30, "power_nominal": power},
+    }
+    if box:
+        cfg["fine_mesh"] = {"refinement": 2, "box_size": [0.2e-3, 0.15e-3, 0.04e-3]}
+    return cfg, StraightTrack(0.2e-3, 0.15e-3, 0.15, 0.0, power)
 
 
 def precision_track(seed=0, nx=256, ny=128, nz=64, steps=500, dt=5e-6):

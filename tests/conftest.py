@@ -34,7 +34,8 @@ def make_context(cfg, path):
     from spectral_galerkin_heat_b200 import SimulationContext
     import copy
     ctx = SimulationContext.from_dict(copy.deepcopy(cfg))
-    ctx.laser_path = path
+    if path is not None:          # None: the path the config names (G-code)
+        ctx.laser_path = path
     return ctx
 
 

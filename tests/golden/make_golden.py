@@ -1,9 +1,10 @@
 """Generate the golden fixtures under ``tests/golden/`` from the reference itself.
 
-Run in a container where the reference checkout exists (read-only) at
-``/root/reference`` (override with ``SGH_REFERENCE``)::
+Run where a checkout of the reference exists, naming its root (the directory
+holding ``src/spectral_galerkin_heat``) with ``--reference`` or the
+``SGH_REFERENCE`` environment variable::
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py --reference <checkout> [case ...]
 
 The reference is the pure-Python package ``spectral_galerkin_heat``. Its module
 imports pull in ``pint``, ``h5py``, ``matplotlib`` and ``pyfftw``, which are
@@ -38,10 +39,29 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 REPO = HERE.parent.parent
-REF = Path(os.environ.get("SGH_REFERENCE", "/root/reference"))
+REF = None
 
 
-def import_reference():
+def reference_root(argv=()):
+    """The reference checkout named by ``--reference PATH`` or ``SGH_REFERENCE``."""
+    argv = list(argv)
+    if "--reference" in argv:
+        i = argv.index("--reference")
+        root = argv[i + 1]
+        del argv[i:i + 2]
+    else:
+        root = os.environ.get("SGH_REFERENCE")
+    if not root:
+        raise SystemExit("name the reference checkout with --reference PATH or SGH_REFERENCE")
+    root = Path(root)
+    if not (root / "src" / "spectral_galerkin_heat").is_dir():
+        raise SystemExit(f"{root} holds no src/spectral_galerkin_heat")
+    return root, argv
+
+
+def import_reference(root=None):
+    global REF
+    REF = Path(root) if root is not None else reference_root()[0]
     os.environ.setdefault("NUMBA_CACHE_DIR", tempfile.mkdtemp(prefix="sgh_numba_"))
     sys.dont_write_bytecode = True
     for name in ("pint", "h5py", "matplotlib", "matplotlib.pyplot", "pyfftw"):
@@ -79,9 +99,9 @@ def cases():
     cfg, path = W.nonlinear_raster(nx=32, ny=16, nz=8, size=(0.5e-3, 0.25e-3, 0.125e-3),
                                    line_length=0.1e-3, hatch=25e-6, steps=40)
     out["raster_32x16x8"] = (cfg, path, 40, [1, 10, 40], None)
-    # nonlinear raster at the full mode count, first steps; low-index block stored
-    cfg, path = W.nonlinear_raster(steps=3)
-    out["raster_128x64x32"] = (cfg, path, 3, [3], (8, 16, 32))
+    # nonlinear raster at the full mode count (the C2 grid), 20 steps, every mode stored
+    cfg, path = W.nonlinear_raster(steps=20)
+    out["raster_128x64x32"] = (cfg, path, 20, [20], None)
     # odd sizes, bottom + top convection, cell-integrated beam, T-dependent k only
     cfg, _ = W.nonlinear_raster(nx=13, ny=10, nz=6, size=(0.4e-3, 0.3e-3, 0.1e-3), steps=6,
                                 tol=1e-9, omega=0.2, cap=200)
@@ -137,6 +157,30 @@ def cases():
                             x0=0.3e-3, y0=0.2e-3, speed=0.0)
     cfg["simulation"]["max_picard_iter"] = 80
     out["box_full_r1_20x12x30"] = (cfg, path, 6, [6], None)
+    # the material block of the reference's example 03 (distinct solid and
+    # liquid polynomials, quadratic rho(T), a constant-string liquid Cp) on a
+    # reduced grid of its 0.5 x 0.3 x 0.12 mm box, omega 0.31, in grid mode and
+    # in box mode; the track melts from the fourth step on
+    cfg, path = W.example03(nx=25, ny=15, nz=24, steps=10)
+    out["tdep03_grid_25x15x24"] = (cfg, path, 10, [5, 10], None)
+    cfg, path = W.example03(nx=25, ny=15, nz=24, steps=10, box=True)
+    out["tdep03_box_25x15x24"] = (cfg, path, 10, [5, 10], None)
+    # G-code laser paths (float32 positions and velocities): the path is read
+    # from the config (path None here), so each side uses its own G-code
+    # reader on the same file. One-pass track in grid mode, and box mode.
+    gcode = {"type": "gcode", "file": str(HERE / "scan_two_segments.gcode"),
+             "initial_position": [0.1, 0.2]}
+    cfg, _ = W.straight_track(nx=30, ny=16, nz=8, steps=40, dt=2e-6,
+                              size=(0.6e-3, 0.3e-3, 0.15e-3))
+    cfg["laser"]["path"] = dict(gcode)
+    out["gcode_track_30x16x8"] = (cfg, None, 40, [20, 40], None)
+    cfg, _ = W.straight_track(nx=24, ny=12, nz=8, steps=12, dt=2e-6,
+                              size=(0.6e-3, 0.3e-3, 0.15e-3))
+    cfg["material"]["L_f"] = 2.7e5
+    cfg["simulation"].update({"max_picard_iter": 400, "picard_omega": 0.1, "picard_tol": 1e-8})
+    cfg["fine_mesh"] = {"refinement": 2, "box_size": [0.2e-3, 0.15e-3, 0.05e-3]}
+    cfg["laser"]["path"] = dict(gcode)
+    out["gcode_box_24x12x8"] = (cfg, None, 12, [6, 12], None)
     return out
 
 
@@ -146,7 +190,8 @@ def run_case(name, spec, Ctx, Solver, Numpy):
 
     cfg, path, steps, snaps, block = spec
     ctx = Ctx.from_dict(copy.deepcopy(cfg))
-    ctx.laser_path = path
+    if path is not None:
+        ctx.laser_path = path
     ref = Solver(Numpy(), ctx)
     ref.initialize()
     orc = OracleSolver(ctx)
@@ -272,9 +317,34 @@ def run_outputs(name, case, steps, Ctx, Solver, Numpy):
     print(f"{name}: outputs of {case} after {steps} steps, oracle vs reference worst rel L2 {worst:.2e}")
 
 
+def run_gcode_states(name="gcode_states"):
+    """The reference's own G-code reader (``io_utils/gcode_path.py``) on
+    ``scan_two_segments.gcode``: laser states at ``t = i*dt`` over every
+    segment, the jump with the beam off and the time after the last segment,
+    for two step sizes and ``dt = 0``."""
+    from spectral_galerkin_heat.io_utils.gcode_path import GCodeLaserPath as RefGCode
+    path = RefGCode(str(HERE / "scan_two_segments.gcode"), initial_position=(0.1, 0.2))
+    files = {}
+    for tag, dt, n in (("dt2", 2e-6, 300), ("dt37", 3.7e-6, 170), ("dt0", 0.0, 50)):
+        times = [i * (dt if dt else 1.3e-5) for i in range(n)]
+        recs = [path.get_state(t, dt) for t in times]
+        assert all(isinstance(r.x, np.float32) and isinstance(r.v[0], np.float32) for r in recs)
+        files[f"{tag}_times"] = np.array(times)
+        files[f"{tag}_xy"] = np.array([(r.x, r.y) for r in recs], dtype=np.float32)
+        files[f"{tag}_v"] = np.array([r.v for r in recs], dtype=np.float32)
+        files[f"{tag}_power"] = np.array([r.power for r in recs], dtype=np.float32)
+        files[f"{tag}_on"] = np.array([r.is_on for r in recs])
+        files[f"{tag}_dt"] = np.array(dt)
+    files["meta"] = np.array(str({"gcode": "scan_two_segments.gcode", "initial_position": (0.1, 0.2),
+                                  "numpy": np.__version__}))
+    np.savez_compressed(HERE / f"{name}.npz", **files)
+    print(f"{name}: reference G-code states stored")
+
+
 def main(argv):
     warnings.simplefilter("ignore")
-    Ctx, Solver, Numpy = import_reference()
+    root, argv = reference_root(argv)
+    Ctx, Solver, Numpy = import_reference(root)
     sel = set(argv[1:])
     for name, spec in cases().items():
         if sel and name not in sel:
@@ -284,6 +354,8 @@ def main(argv):
         if sel and name not in sel:
             continue
         run_outputs(name, case, steps, Ctx, Solver, Numpy)
+    if not sel or "gcode_states" in sel:
+        run_gcode_states()
 
 
 if __name__ == "__main__":

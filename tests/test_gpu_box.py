@@ -16,7 +16,8 @@ from conftest import golden_case, load_golden, make_context, rel_l2
 pytestmark = pytest.mark.gpu
 
 TOL = 1e-10
-BOX_CASES = ["box_const_24x12x8", "box_shallow_24x12x8", "box_tdep_16x12x8", "box_full_r1_20x12x30"]
+BOX_CASES = ["box_const_24x12x8", "box_shallow_24x12x8", "box_tdep_16x12x8", "box_full_r1_20x12x30",
+             "tdep03_box_25x15x24", "gcode_box_24x12x8"]
 
 
 def _solver(cfg, path, **kw):
@@ -61,7 +62,7 @@ def test_box_matches_reference_fixture(name):
     s.finalize()
 
 
-@pytest.mark.parametrize("name", ["box_const_24x12x8", "box_tdep_16x12x8"])
+@pytest.mark.parametrize("name", ["box_const_24x12x8", "box_tdep_16x12x8", "gcode_box_24x12x8"])
 def test_box_run_eager_and_graph_agree(name):
     """The device-graph run (``run``), graph steps and eager steps give the same
     field and metrics (same kernels, same order)."""

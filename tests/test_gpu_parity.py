@@ -16,7 +16,8 @@ pytestmark = pytest.mark.gpu
 TOL = 1e-10
 
 GOLDEN = ["track_64x32x16", "raster_32x16x8", "odd_13x10x6_conv", "latent_const_24x12x8",
-          "supergauss_20x18x5", "laser_off_8x6x4", "raster_128x64x32"]
+          "supergauss_20x18x5", "laser_off_8x6x4", "raster_128x64x32", "tdep03_grid_25x15x24",
+          "gcode_track_30x16x8"]
 
 
 def _solver(cfg, path):
@@ -157,3 +158,36 @@ def test_dctn_alias_in_place():
                       C.c_void_p(ws.data_ptr()), n.value, None) == 0
     torch.cuda.synchronize()
     assert rel_l2(x.cpu().numpy(), ref) < 1e-14
+
+
+@pytest.mark.parametrize("which", ["precision_256x128x64", "serving_512x256x64"])
+def test_large_grid_matches_live_oracle(which):
+    """The largest grids the benchmarks step, in FP64, against the oracle run now:
+    the 256x128x64 precision-study track (4 x 2 x 1 mm, seeded power and speed)
+    and the largest serving class, 512x256x64 on the 2 x 1 x 0.5 mm cuboid with
+    a serving raster. One forcing pass per step; 10 steps stay well inside the
+    range over which this explicit scheme is not chaotic (about 60 steps)."""
+    from oracle.sgh_oracle import OracleSolver
+    from spectral_galerkin_heat_b200 import workloads
+    from spectral_galerkin_heat_b200.laser import RasterPath
+    steps = 10
+    if which.startswith("precision"):
+        cfg, path = workloads.precision_track(seed=0, steps=steps)
+    else:
+        cfg = workloads.serving_config(512, 256, 64)
+        cfg["simulation"]["duration"] = steps * cfg["simulation"]["dt"]
+        path = RasterPath(0.25e-3, 0.2e-3, 1.5e-3, 50e-6, 2, 1.3, 350.0)
+    s = _solver(cfg, path)
+    o = OracleSolver(make_context(cfg, path))
+    o.initialize()
+    dt = s.context.num.dt
+    for i in range(steps):
+        _, m = s.step(i * dt, dt)
+        _, mo = o.step(i * dt, dt)
+        assert m["n_evap_iter"] == mo["n_evap_iter"]
+        assert m["T_surface_max"] == pytest.approx(mo["T_surface_max"], rel=TOL)
+        assert m["P_laser"] == pytest.approx(mo["P_laser"], rel=1e-12)
+    assert mo["T_surface_max"] > 1000.0          # the beam has heated the surface
+    assert rel_l2(s.state.a.cpu().numpy(), o.a) < TOL
+    assert rel_l2(s.surface_temperature().cpu().numpy(), o.surface_T(o.a, top=True)) < TOL
+    s.finalize()

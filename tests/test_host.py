@@ -50,12 +50,21 @@ EXPRS = ["15 + 20*(T - 300)/2700", "450 + 350*(T - 300)/2700", "7900", "9.248 + 
          "log(T) * e - +3", "tanh((T-1700)/50)*2 + floor(T/100)"]
 
 
+_NUMPY_NS = {"sqrt": np.sqrt, "exp": np.exp, "log": np.log, "atan2": np.arctan2,
+             "fabs": np.abs, "tanh": np.tanh, "floor": np.floor, "pi": math.pi, "e": math.e}
+
+
 @pytest.mark.parametrize("src", EXPRS)
 def test_program_matches_expression(src):
+    """The device program (run by the test's own interpreter and by the host
+    stack machine) gives the values of the expression evaluated directly by
+    Python on NumPy arrays."""
     T = np.linspace(300.0, 4000.0, 37)
     e = PropertyExpr(src)
     ops, consts = e.program()
-    np.testing.assert_array_equal(run_program(ops, consts, T), e(T) + 0 * T)
+    direct = eval(src, {"__builtins__": {}}, dict(_NUMPY_NS, T=T)) + 0 * T
+    np.testing.assert_array_equal(run_program(ops, consts, T), direct)
+    np.testing.assert_array_equal(e(T), direct)
 
 
 @pytest.mark.parametrize("bad", ["T.real", "T[0]", "foo(T)", "T < 3", "import os", "x + 1",
@@ -181,3 +190,53 @@ def test_box_mode_is_rejected():
     s = B200SpectralSolver(None, make_context(cfg, path))
     with pytest.raises((NotImplementedError, RuntimeError)):
         s.initialize()
+
+
+@pytest.mark.parametrize("tag", ["dt2", "dt37", "dt0"])
+def test_gcode_path_matches_reference_states(tag):
+    """The G-code reader gives the reference reader's laser states bit for bit
+    (float32 positions, velocities and powers; fixture from the reference's
+    ``GCodeLaserPath``), one call at a time and as a vectorised step table."""
+    import os
+    from conftest import GOLDEN, load_golden
+    from spectral_galerkin_heat_b200.laser import LASER_F32, GCodeLaserPath, laser_table
+    g = load_golden("gcode_states")
+    path = GCodeLaserPath(os.path.join(GOLDEN, "scan_two_segments.gcode"),
+                          initial_position=(0.1, 0.2))
+    dt = float(g[f"{tag}_dt"])
+    times = g[f"{tag}_times"]
+    for i, t in enumerate(times):
+        st = path.get_state(float(t), dt)
+        assert isinstance(st.x, np.float32) and isinstance(st.v[1], np.float32)
+        assert (st.x, st.y) == tuple(g[f"{tag}_xy"][i])
+        assert st.v == tuple(g[f"{tag}_v"][i])
+        assert st.power == g[f"{tag}_power"][i] and st.is_on == bool(g[f"{tag}_on"][i])
+    if dt > 0:
+        tab = laser_table(path, 0.0, dt, len(times))
+        np.testing.assert_array_equal(tab["x"], g[f"{tag}_xy"][:, 0])
+        np.testing.assert_array_equal(tab["vy"], g[f"{tag}_v"][:, 1])
+        np.testing.assert_array_equal(tab["power"], g[f"{tag}_power"])
+        np.testing.assert_array_equal(tab["is_on"], g[f"{tag}_on"].astype(np.int32))
+        assert np.all(tab["flags"] == LASER_F32)
+
+
+def test_gcode_path_from_config():
+    """A ``laser.path`` of type gcode is read into a GCodeLaserPath; a relative
+    file name resolves under ``<config_dir>/paths`` as in the reference."""
+    import os
+    import shutil
+    import tempfile
+    from conftest import GOLDEN
+    from spectral_galerkin_heat_b200.laser import GCodeLaserPath
+    cfg, _ = workloads.straight_track()
+    with tempfile.TemporaryDirectory() as d:
+        os.makedirs(os.path.join(d, "paths"))
+        shutil.copy(os.path.join(GOLDEN, "scan_two_segments.gcode"), os.path.join(d, "paths"))
+        cfg["laser"]["path"] = {"type": "gcode", "file": "scan_two_segments.gcode"}
+        ctx = SimulationContext.from_dict(cfg, config_dir=d)
+        assert isinstance(ctx.laser_path, GCodeLaserPath)
+        assert len(ctx.laser_path.segments) == 3
+        assert cfg["laser"]["path"]["file"] == os.path.join(d, "paths", "scan_two_segments.gcode")
+    cfg["laser"]["path"] = {"type": "gcode", "file": "x.gcode", "bogus": 1}
+    with pytest.raises(ValueError):
+        SimulationContext.from_dict(cfg)

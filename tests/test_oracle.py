@@ -11,9 +11,11 @@ from oracle.sgh_oracle import OracleSolver, dct2, dct3, dct_matrix
 # in library summation order, so the bound is a few ulps times the step count.
 TOL_ORACLE = 1e-12
 
-BOX_CASES = ["box_const_24x12x8", "box_shallow_24x12x8", "box_tdep_16x12x8", "box_full_r1_20x12x30"]
+BOX_CASES = ["box_const_24x12x8", "box_shallow_24x12x8", "box_tdep_16x12x8", "box_full_r1_20x12x30",
+             "tdep03_box_25x15x24", "gcode_box_24x12x8"]
 CASES = ["track_64x32x16", "raster_32x16x8", "odd_13x10x6_conv", "latent_const_24x12x8",
-         "supergauss_20x18x5", "laser_off_8x6x4", "raster_128x64x32"] + BOX_CASES
+         "supergauss_20x18x5", "laser_off_8x6x4", "raster_128x64x32",
+         "tdep03_grid_25x15x24", "gcode_track_30x16x8"] + BOX_CASES
 
 
 def _run_oracle(name, upto=None):
