@@ -22,6 +22,20 @@ alone and in the mix.
 Latency is completion minus arrival on the host clock; throughput is the
 timesteps of all completed requests divided by the span from the first
 arrival to the last completion.
+
+Failure handling (the host side of what the reference does with a warning or
+an exception, ``solvers/spectral.py:486-499``):
+
+* a request of a grid class the engine holds no slots for is refused with a
+  ``ValueError`` before anything runs;
+* ``cancel(request)`` stops a queued or running request at the next chunk
+  boundary and frees its slot (``status = "cancelled"``);
+* a request with a ``deadline`` (seconds after its arrival) that has not
+  finished by then is stopped the same way (``status = "timed_out"``);
+* after every chunk the batch's tensor-core error flag is read: if a bounded
+  wait of a tensor-core face pass ran out, every request in flight is marked
+  ``"failed"`` (its slot results are not trusted) and ``run`` raises
+  ``RuntimeError``.
 """
 from __future__ import annotations
 
@@ -51,10 +65,12 @@ class Request:
     steps: int
     arrival: float = 0.0
     table: object = None
+    deadline: Optional[float] = None   # seconds after arrival; None = no limit
     # filled in by the engine
     admitted: float = float("nan")
     finished: float = float("nan")
     slot: int = -1
+    status: str = "new"   # queued | running | done | cancelled | timed_out | failed
     last: Optional[dict] = None
     modes: object = None
     surface: object = None
@@ -80,6 +96,9 @@ class _Stats:
     admitted: int = 0
     completed: int = 0
     slot_steps: int = 0
+    class_steps: dict = field(default_factory=dict)   # slot-steps per class key
+    cancelled: int = 0
+    timed_out: int = 0
     busy_s: float = 0.0
     launches: int = 0
     extra: dict = field(default_factory=dict)
@@ -141,6 +160,7 @@ class ServingEngine:
         self.stats = _Stats()
         self._active: Dict[int, Request] = {}
         self._done_steps: Dict[int, int] = {}
+        self._cancel: set = set()
         self.memory = {"free_bytes_at_start": int(free), "total_bytes": int(total),
                        "budget_bytes": self.budget, "workspace_bytes": self.batch.workspace_bytes,
                        "slots": len(contexts)}
@@ -162,7 +182,7 @@ class ServingEngine:
         slot = fr.popleft()
         table = self._device_table(req)
         self.batch.start(slot, req.steps, table=table, record=False)
-        req.slot, req.admitted = slot, now
+        req.slot, req.admitted, req.status = slot, now, "running"
         req._dev_table = table  # keep the device table alive while the slot runs
         self.stats.admitted += 1
         return True
@@ -177,8 +197,34 @@ class ServingEngine:
         if self.keep_modes:
             req.modes = self.batch.snapshot(req.slot, "modes")  # device copy
         req._dev_table = None
+        req.status = "done"
         self.free[req.key].append(req.slot)
         self.stats.completed += 1
+
+    def cancel(self, req: Request) -> None:
+        """Stop ``req`` (queued or running) at the next chunk boundary of
+        :meth:`run`; its slot is freed and ``req.status`` becomes "cancelled"."""
+        self._cancel.add(id(req))
+
+    def _stop(self, req: Request, status: str, now: float) -> None:
+        """Stop a running request: free its slot, no result."""
+        self.batch.stop(req.slot)
+        self.free[req.key].append(req.slot)
+        req._dev_table = None
+        req.status, req.finished = status, now
+        self._active.pop(req.slot, None)
+        self._done_steps.pop(req.slot, None)
+
+    def _expired(self, req: Request, now: float) -> bool:
+        return req.deadline is not None and now > req.arrival + req.deadline
+
+    def _check_classes(self, requests: Sequence[Request]) -> None:
+        for r in requests:
+            if r.key not in self.free:
+                declared = ", ".join(map(str, self.keys))
+                raise ValueError(f"request {r.id} is of class {r.key!r}, for which this engine holds "
+                                 f"no slots (declared classes: {declared}); create the engine with "
+                                 f"that class")
 
     # ---- the loop ------------------------------------------------------------
     def run(self, requests: Sequence[Request], realtime: bool = True, max_steps: Optional[int] = None,
@@ -192,10 +238,13 @@ class ServingEngine:
         flight then stay in their slots until :meth:`reset`. Returns the
         requests with their timings and results filled in.
         """
+        self._check_classes(requests)
         pending = deque(sorted(requests, key=lambda r: r.arrival))
         if not realtime:
             for r in pending:
                 r.arrival = 0.0
+        for r in pending:
+            r.status = "queued"
         queue: List[Request] = []
         active, done_steps = self._active, self._done_steps
         pre, per_it, post = self.batch.launch_counts()
@@ -206,6 +255,28 @@ class ServingEngine:
             now = clock() - t0
             while pending and pending[0].arrival <= now:
                 queue.append(pending.popleft())
+            # cancellations and deadlines, at chunk boundaries only
+            for s, r in list(active.items()):
+                if id(r) in self._cancel:
+                    self._cancel.discard(id(r))
+                    self._stop(r, "cancelled", now)
+                    self.stats.cancelled += 1
+                elif self._expired(r, now):
+                    self._stop(r, "timed_out", now)
+                    self.stats.timed_out += 1
+            if queue:
+                kept = []
+                for r in queue:
+                    if id(r) in self._cancel:
+                        self._cancel.discard(id(r))
+                        r.status, r.finished = "cancelled", now
+                        self.stats.cancelled += 1
+                    elif self._expired(r, now):
+                        r.status, r.finished = "timed_out", now
+                        self.stats.timed_out += 1
+                    else:
+                        kept.append(r)
+                queue = kept
             if queue:
                 still = []
                 for r in queue:
@@ -231,6 +302,13 @@ class ServingEngine:
             c0 = clock()
             self.batch.step(chunk)
             info = self.batch.status()  # synchronises
+            if self.batch.tensor_core_error():
+                now = clock() - t0
+                for r in active.values():
+                    r.status, r.finished = "failed", now
+                raise RuntimeError("a bounded tensor-core wait ran out in the batch's face "
+                                   "transforms; the results of the requests in flight are not "
+                                   "trusted (marked failed)")
             dt_chunk = clock() - c0
             self.stats.busy_s += dt_chunk
             self.stats.d2h_bytes += len(info) * 64
@@ -245,6 +323,8 @@ class ServingEngine:
             for s in list(active):
                 st = info[s]
                 self.stats.slot_steps += st.step - done_steps[s]
+                key = active[s].key
+                self.stats.class_steps[key] = self.stats.class_steps.get(key, 0) + st.step - done_steps[s]
                 iters = max(iters, st.last.n_iter)
                 done_steps[s] = st.step
                 if not st.active:

@@ -19,6 +19,11 @@ class FakeBatch:
                                                         converged=1, picard_rel_err=0.0))
                    for _ in range(self.n)]
         self.starts, self.chunks = [], []
+        self.umma_err = 0
+        self.fail_after_chunks = None
+
+    def tensor_core_error(self):
+        return self.umma_err
 
     def launch_counts(self):
         return 5, 3, 4
@@ -33,6 +38,8 @@ class FakeBatch:
 
     def step(self, k):
         self.chunks.append(k)
+        if self.fail_after_chunks is not None and len(self.chunks) > self.fail_after_chunks:
+            self.umma_err = 1
         for s in self.st:
             if s.active:
                 s.step = min(s.n_steps, s.step + k)
@@ -135,3 +142,44 @@ def test_vectorised_laser_tables_equal_get_state_bitwise():
     for i in range(40):
         s = track.get_state(1e-5 + i * 2e-6, 2e-6)
         assert tuple(tab[i])[:6] == (s.x, s.y, s.power, s.v[0], s.v[1], 1)
+
+
+def test_unknown_class_is_refused_before_anything_runs():
+    eng = _engine({"a": 1, "b": 1})
+    reqs = _reqs([("a", 5), ("c", 5)])
+    with pytest.raises(ValueError, match="no slots"):
+        eng.run(reqs, realtime=False)
+    assert eng.batch.starts == [] and eng.stats.admitted == 0
+
+
+def test_cancel_running_and_queued_requests():
+    eng = _engine({"a": 1, "b": 1}, max_chunk=4)
+    reqs = _reqs([("a", 40), ("a", 10), ("b", 12)])
+    eng.cancel(reqs[0])            # running once admitted: stopped at the first boundary
+    eng.cancel(reqs[1])            # still queued behind it: never runs
+    eng.run(reqs, realtime=False)
+    a0, a1, b0 = reqs
+    assert a0.status == "cancelled" and a0.last is None
+    assert a1.status in ("cancelled", "done")
+    assert b0.status == "done" and b0.last["T_surface_max"] == 12
+    assert eng.stats.cancelled >= 1 and len(eng.free["a"]) == 1 and eng.in_flight == 0
+
+
+def test_deadline_stops_a_request_and_frees_its_slot():
+    clock = iter(float(i) for i in range(10_000))
+    eng = _engine({"a": 1, "b": 1}, max_chunk=2)
+    reqs = _reqs([("a", 100), ("a", 4), ("b", 6)])
+    reqs[0].deadline = 3.0          # host seconds after arrival (the fake clock ticks 1 per call)
+    eng.run(reqs, realtime=False, clock=lambda: next(clock))
+    assert reqs[0].status == "timed_out" and np.isfinite(reqs[0].finished)
+    assert reqs[1].status == "done" and reqs[2].status == "done"
+    assert eng.stats.timed_out == 1 and eng.in_flight == 0
+
+
+def test_tensor_core_error_fails_requests_in_flight():
+    eng = _engine({"a": 1, "b": 1})
+    eng.batch.fail_after_chunks = 1
+    reqs = _reqs([("a", 30), ("b", 50)])
+    with pytest.raises(RuntimeError, match="tensor-core"):
+        eng.run(reqs, realtime=False)
+    assert {r.status for r in reqs} <= {"failed", "done"} and any(r.status == "failed" for r in reqs)
