@@ -270,6 +270,16 @@ int sgh_box_geometry(const sgh_plan* plan, sgh_box_geom* out);
  * step, when the window bases are still zero as in the reference. */
 int sgh_box_window(sgh_plan* plan, int32_t* i0, void* stream);
 
+/* Picard history of the plan's last step (the per-iteration record of
+ * SpectralSolver.step with track_picard_history, solvers/spectral.py:470-481):
+ * out[2 k] = rms of the residual a_raw - a_old and out[2 k + 1] = the relative
+ * residual of iteration k, for k < min(*n_iter, cap, SGH_PICARD_HISTORY_MAX);
+ * *n_iter = the step's iteration count. The record is written on the device by
+ * the convergence test; this call copies it to the host array out (2 cap
+ * doubles) and returns after the stream has drained. */
+#define SGH_PICARD_HISTORY_MAX 4096
+int sgh_picard_history(sgh_plan* plan, double* out, int32_t cap, int32_t* n_iter, void* stream);
+
 /* out (nz_box, ny_box, nx_box) = the temperature of modes on the fine box at
  * the current window: reconstruct_temperature_box
  * (physics/spectral_ops.py:173-179). Async. */
@@ -317,6 +327,17 @@ typedef struct {
 } sgh_batch_slot_info;
 
 int sgh_batch_create(const sgh_config* cfgs, int32_t n, int32_t precision, sgh_batch** out);
+
+/* Tile policy of a batch's kernels (no reference counterpart: the reference
+ * steps one instance with library transforms). vol_unroll: z-planes whose
+ * loads one round of the volume pass issues before their arithmetic (2, 4 or
+ * 8; 0 = 4). The other fields are reserved and must be 0. Chosen per grid
+ * mix by the autotuner; set before sgh_batch_bind. */
+typedef struct {
+  int32_t vol_unroll;
+  int32_t reserved[7];
+} sgh_batch_policy;
+int sgh_batch_set_policy(sgh_batch* batch, const sgh_batch_policy* policy);
 int sgh_batch_destroy(sgh_batch* batch);
 int sgh_batch_workspace_bytes(const sgh_batch* batch, uint64_t* bytes);
 /* Bind workspace, build per-slot tables, capture the batch step graph. All
@@ -341,6 +362,16 @@ int sgh_batch_buffer(const sgh_batch* batch, int32_t slot, int32_t which, void**
 /* *err = nonzero once a tensor-core wait of a mixed-precision batch expired
  * (the affected face pass wrote no results). Synchronises the stream. */
 int sgh_batch_error(const sgh_batch* batch, int32_t* err, void* stream);
+/* Bound of the tensor-core data waits of the batch's face transforms: at most
+ * `polls` mbarrier polls (0 = the default, 2^22) before the CTA records the
+ * error flag, waits for its copies and MMAs in flight (always with the
+ * default bound), frees its tensor memory and returns without results.
+ * stall_test = 1 makes every face-transform CTA first wait, with that bound,
+ * on a barrier that nothing completes -- a wait that can only run out -- so a
+ * test can drive the error path without a fault (needs polls > 0); 0 for
+ * normal stepping. No reference counterpart: the reference has no bounded
+ * device waits. Synchronises the stream. */
+int sgh_batch_set_wait_limit(sgh_batch* batch, uint32_t polls, int32_t stall_test, void* stream);
 /* Kernels per batch step: *pre + n_iter * *per_iter + *post, n_iter = the
  * largest iteration count over the active slots. */
 int sgh_batch_launch_counts(const sgh_batch* batch, int32_t* pre, int32_t* per_iter, int32_t* post);

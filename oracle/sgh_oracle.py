@@ -614,7 +614,11 @@ class OracleSolver:
             rms_o = math.sqrt(float(np.vdot(a_old, a_old)) / n_el)
             rel = rms_d / max(rms_o, 1e-9)
             if self.track_picard_history:
-                self.picard_history.append({"iter": it, "rms_diff": rms_d, "true_rel_err": rel})
+                # contraction ratio to the previous iteration (solvers/spectral.py:470-481)
+                prev = self.picard_history[-1]["rms_diff"] if self.picard_history else 0.0
+                rho = rms_d / prev if it > 0 and prev > 0 else None
+                self.picard_history.append({"iter": it, "rms_diff": rms_d, "rho": rho,
+                                            "true_rel_err": rel})
             self.q_evap = q_ev
             if rel < self.tol:
                 converged = True

@@ -20,6 +20,7 @@ LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libsgh_b200
 
 MAX_PROGRAM = 64
 MAX_CONSTS = 32
+PICARD_HISTORY_MAX = 4096  # SGH_PICARD_HISTORY_MAX
 
 ERRORS = {-1: "SGH_ERR_INVALID", -2: "SGH_ERR_CUDA", -3: "SGH_ERR_STATE",
           -4: "SGH_ERR_UNSUPPORTED", -5: "SGH_ERR_WORKSPACE"}
@@ -40,11 +41,12 @@ EXPORTED = (
     "sgh_nodal_workspace_bytes", "sgh_nodal_temperature", "sgh_points_workspace_bytes",
     "sgh_points_temperature", "sgh_box_geometry", "sgh_box_window", "sgh_box_temperature",
     "sgh_box_project", "sgh_state_flags", "sgh_state_set_flags", "sgh_line_workspace_bytes",
-    "sgh_line_temperature",
+    "sgh_line_temperature", "sgh_picard_history",
     "sgh_batch_create", "sgh_batch_destroy", "sgh_batch_workspace_bytes", "sgh_batch_bind",
     "sgh_batch_slot_start", "sgh_batch_slot_stop", "sgh_batch_step", "sgh_batch_step_eager",
     "sgh_batch_status",
-    "sgh_batch_buffer", "sgh_batch_launch_counts", "sgh_batch_volume_pass", "sgh_batch_error", "sgh_dct2_bf16x3_workspace_bytes",
+    "sgh_batch_buffer", "sgh_batch_launch_counts", "sgh_batch_volume_pass", "sgh_batch_error",
+    "sgh_batch_set_wait_limit", "sgh_batch_set_policy", "sgh_dct2_bf16x3_workspace_bytes",
     "sgh_dct2_bf16x3",
 )
 
@@ -78,6 +80,10 @@ class SghConfig(C.Structure):
 class SghLaser(C.Structure):
     _fields_ = [("x", C.c_double), ("y", C.c_double), ("power", C.c_double),
                 ("vx", C.c_double), ("vy", C.c_double), ("is_on", C.c_int32), ("flags", C.c_int32)]
+
+
+class SghBatchPolicy(C.Structure):
+    _fields_ = [("vol_unroll", C.c_int32), ("reserved", C.c_int32 * 7)]
 
 
 class SghStepOut(C.Structure):
@@ -160,6 +166,8 @@ def lib() -> C.CDLL:
             "sgh_batch_status": ([vp, C.POINTER(SghBatchSlotInfo), vp], C.c_int),
             "sgh_batch_buffer": ([vp, i32, i32, C.POINTER(vp), u64p], C.c_int),
             "sgh_batch_error": ([vp, C.POINTER(i32), vp], C.c_int),
+            "sgh_batch_set_wait_limit": ([vp, C.c_uint32, i32, vp], C.c_int),
+            "sgh_batch_set_policy": ([vp, C.POINTER(SghBatchPolicy)], C.c_int),
             "sgh_batch_launch_counts": ([vp, C.POINTER(i32), C.POINTER(i32), C.POINTER(i32)], C.c_int),
             "sgh_batch_volume_pass": ([vp, vp], C.c_int),
             "sgh_box_geometry": ([vp, C.POINTER(SghBoxGeom)], C.c_int),
@@ -172,6 +180,7 @@ def lib() -> C.CDLL:
                                       C.c_double, C.c_double, C.c_double, i32, vp, vp, vp, C.c_uint64, vp],
                                      C.c_int),
             "sgh_state_set_flags": ([vp, i32, vp], C.c_int),
+            "sgh_picard_history": ([vp, C.POINTER(C.c_double), i32, C.POINTER(i32), vp], C.c_int),
         }
         for name, (args, res) in sig.items():
             fn = getattr(L, name)

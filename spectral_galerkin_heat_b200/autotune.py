@@ -33,7 +33,8 @@ import os
 import time
 from typing import Dict, Iterable, Optional
 
-__all__ = ["CANDIDATES", "KERNELS", "key_of", "lookup", "lookup_kernel", "tune", "tune_table"]
+__all__ = ["CANDIDATES", "KERNELS", "key_of", "lookup", "lookup_kernel", "tune", "tune_table",
+           "BATCH_CANDIDATES", "batch_key", "lookup_batch", "tune_batch"]
 
 # always 2 x 4, three switch points, never 2 x 4
 CANDIDATES = (1, 66, 132, 264, 1 << 30)
@@ -56,14 +57,14 @@ def key_of(cfg) -> str:
     return f"{int(cfg.nx)}x{int(cfg.ny)}x{int(cfg.nz)}:{_form(cfg)}"
 
 
-def _load(path: str) -> Dict:
-    if path not in _cache:
+def _load(path: str, section: str = "entries") -> Dict:
+    if (path, section) not in _cache:
         try:
             with open(path) as f:
-                _cache[path] = json.load(f).get("entries", {})
+                _cache[(path, section)] = json.load(f).get(section, {})
         except (OSError, ValueError):
-            _cache[path] = {}
-    return _cache[path]
+            _cache[(path, section)] = {}
+    return _cache[(path, section)]
 
 
 def _entry(cfg) -> Optional[Dict]:
@@ -146,10 +147,130 @@ def tune_table(contexts: Dict[str, object], out: Optional[str] = None, **kw) -> 
                      "shape and step form, timed on the step graph",
              "entries": entries}
     if out:
+        try:
+            with open(out) as f:
+                table["batch_entries"] = json.load(f).get("batch_entries", {})
+        except (OSError, ValueError):
+            pass
         with open(out, "w") as f:
             json.dump(table, f, indent=1, sort_keys=True)
-        _cache.pop(out, None)
+        for k in list(_cache):
+            if k[0] == out:
+                _cache.pop(k)
     return table
+
+
+# ---------------------------------------------------------------------------
+# batched engine: the tile policy of its kernels per grid mix
+# ---------------------------------------------------------------------------
+# vol_unroll: z-planes whose loads one round of the volume pass (the
+# bandwidth-bound modal commit) issues before their arithmetic. More planes
+# keep more bytes in flight per thread; fewer keep registers, and so warps
+# per SM, up. The best trade depends on nz and on the mix of slot shapes.
+BATCH_CANDIDATES = ({"vol_unroll": 2}, {"vol_unroll": 4}, {"vol_unroll": 8})
+
+
+def batch_key(cfgs, precision: str) -> str:
+    """Table key of a batch: its precision and grid mix (shape and form of
+    every slot class, with the slot count)."""
+    counts: Dict[str, int] = {}
+    for c in cfgs:
+        k = key_of(c)
+        counts[k] = counts.get(k, 0) + 1
+    return f"{precision}|" + "+".join(f"{n}*{k}" for k, n in sorted(counts.items()))
+
+
+def lookup_batch(cfgs, precision: str) -> Optional[Dict]:
+    """Tuned policy for this batch's precision and grid mix, or None."""
+    k = batch_key(cfgs, precision)
+    for path in (os.environ.get("SGH_TUNE_TABLE"), SHIPPED):
+        if path:
+            e = _load(path, "batch_entries").get(k)
+            if e is not None:
+                return dict(e["policy"])
+    return None
+
+
+def tune_batch(contexts, precision: str = "mixed", steps: int = 20, warmup: int = 5,
+               candidates=BATCH_CANDIDATES) -> Dict:
+    """Time every candidate policy on a batch of ``contexts`` with all slots
+    active: ms per batched step (step graph, CUDA events after warm-up) and
+    ms of the volume pass alone; keeps the fastest step."""
+    import torch
+
+    from .batch import BatchSolver
+    res = {}
+    for pol in candidates:
+        b = BatchSolver(contexts, precision, policy=pol)
+        for i in range(b.n):
+            b.start(i, warmup + steps + 2, record=False)
+        b.step(warmup)
+        torch.cuda.synchronize()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        ev[0].record(b.stream)
+        b.step(steps)
+        ev[1].record(b.stream)
+        ev[2].record(b.stream)
+        for _ in range(5):
+            b.volume_pass()
+        ev[3].record(b.stream)
+        torch.cuda.synchronize()
+        if b.tensor_core_error():
+            raise RuntimeError("a tensor-core wait ran out while tuning")
+        res[json.dumps(pol, sort_keys=True)] = {"ms_per_step": ev[0].elapsed_time(ev[1]) / steps,
+                                                 "volume_pass_ms": ev[2].elapsed_time(ev[3]) / 5}
+        b.close()
+    best = min(res, key=lambda k: res[k]["ms_per_step"])
+    return {"policy": json.loads(best), "candidates": res}
+
+
+def tune_batch_table(mixes: Dict[str, tuple], out: Optional[str] = None, **kw) -> Dict:
+    """Tune every named (contexts, precision) mix and merge the entries into
+    the table's ``batch_entries``."""
+    from .solver import make_config
+    from .batch import _picard
+    entries = {}
+    for name, (ctxs, prec) in mixes.items():
+        cfgs = [make_config(c, *_picard(c)) for c in ctxs]
+        t0 = time.perf_counter()
+        r = tune_batch(ctxs, prec, **kw)
+        r["workload"] = name
+        r["tuning_s"] = time.perf_counter() - t0
+        entries[batch_key(cfgs, prec)] = r
+    table = {"note": "", "entries": {}}
+    if out:
+        try:
+            with open(out) as f:
+                table = json.load(f)
+        except (OSError, ValueError):
+            pass
+        table.setdefault("batch_entries", {}).update(entries)
+        with open(out, "w") as f:
+            json.dump(table, f, indent=1, sort_keys=True)
+        for k in list(_cache):
+            if k[0] == out:
+                _cache.pop(k)
+    return entries
+
+
+def batch_mixes() -> Dict[str, tuple]:
+    """The batched engine's benchmark mixes: the serving engine's slot classes
+    (16 slots per class, mixed and FP64) and the 64 uneven instances."""
+    from . import workloads
+    from .config import SimulationContext
+
+    def ctx(cfg, path=None):
+        c = SimulationContext.from_dict(copy.deepcopy(cfg))
+        c.laser_path = path
+        return c
+    stream = workloads.serving_stream(n_requests=1000, seed=0)
+    serving = []
+    for m in sorted({r["mesh"] for r in stream}):
+        paths = [r["path"] for r in stream if r["mesh"] == m]
+        serving += [ctx(workloads.serving_config(*m), paths[i % len(paths)]) for i in range(16)]
+    uneven = [ctx(cfg, path) for cfg, path in workloads.uneven_batch()]
+    return {"serving_mixed": (serving, "mixed"), "serving_fp64": (serving, "fp64"),
+            "uneven_mixed": (uneven, "mixed"), "uneven_fp64": (uneven, "fp64")}
 
 
 def main(argv=None):
@@ -158,12 +279,21 @@ def main(argv=None):
     ap = argparse.ArgumentParser(description="tune the axis-pass tiles for the benchmark shapes")
     ap.add_argument("--out", default=SHIPPED)
     ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--batch-only", action="store_true", help="tune only the batched engine's mixes")
     args = ap.parse_args(argv)
 
     def ctx(cfg, path):
         c = SimulationContext.from_dict(copy.deepcopy(cfg))
         c.laser_path = path
         return c
+    mixes = batch_mixes()
+    entries = tune_batch_table(mixes, out=args.out)
+    for k, e in sorted(entries.items()):
+        print(f"{e['workload']:24s} -> {e['policy']}  " + "  ".join(
+            f"{pk}: {v['ms_per_step']:.3f} ms/step, volume {v['volume_pass_ms']:.3f} ms"
+            for pk, v in e["candidates"].items()))
+    if args.batch_only:
+        return
     contexts = {}
     cfg, path = workloads.nonlinear_raster()
     contexts["nonlinear_raster"] = ctx(cfg, path)

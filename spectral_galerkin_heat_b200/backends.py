@@ -73,13 +73,22 @@ class B200Backend(MathBackend):
 
 
 def install_into_reference() -> bool:
-    """Register ``"b200"`` in the reference's backend registry if it is importable."""
+    """Plug the B200 backend into the reference package when it is importable:
+    ``"b200"`` goes into its backend registry (``backends/_registry.py:45-110``),
+    so ``spectral_galerkin_heat.backends.get_backend("b200")`` builds a
+    :class:`B200Backend`, and :class:`B200SpectralSolver` is registered as a
+    virtual subclass of its ``HeatSolver`` ABC (``solvers/base.py:31-91``), so
+    ``isinstance(solver, HeatSolver)`` holds in code written for the reference.
+    Returns False when the reference is not importable."""
     try:
         from spectral_galerkin_heat.backends import _registry as ref_registry  # type: ignore
+        from spectral_galerkin_heat.solvers.base import HeatSolver as RefHeatSolver  # type: ignore
     except Exception:
         return False
     if "b200" not in ref_registry._BACKEND_FACTORIES:
         ref_registry._BACKEND_FACTORIES["b200"] = B200Backend
+    from .solver import B200SpectralSolver
+    RefHeatSolver.register(B200SpectralSolver)
     return True
 
 

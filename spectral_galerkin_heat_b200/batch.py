@@ -41,7 +41,11 @@ def _picard(ctx, omega=None, tol=None, max_iter=None):
 class BatchSolver:
     """A bound batch of slots on one device."""
 
-    def __init__(self, contexts: Sequence, precision: str = "fp64", device=None):
+    def __init__(self, contexts: Sequence, precision: str = "fp64", device=None,
+                 policy: Optional[dict] = None):
+        """``policy``: the kernels' tile policy, ``{"vol_unroll": 2 | 4 | 8}``;
+        None takes the autotuner's entry for this grid mix (``tuned.json`` or
+        ``SGH_TUNE_TABLE``) and the built-in default without one."""
         import torch
         if precision not in _lib.PRECISION:
             raise ValueError(f"precision must be one of {sorted(_lib.PRECISION)}")
@@ -61,6 +65,13 @@ class BatchSolver:
         _lib.check("sgh_batch_create", L.sgh_batch_create(cfgs, self.n, _lib.PRECISION[precision],
                                                           C.byref(h)))
         self._h = h
+        if policy is None:
+            from .autotune import lookup_batch
+            policy = lookup_batch(cfgs, precision) or {}
+        self.policy = {"vol_unroll": int(policy.get("vol_unroll", 4))}
+        pol = _lib.SghBatchPolicy()
+        pol.vol_unroll = self.policy["vol_unroll"]
+        _lib.check("sgh_batch_set_policy", L.sgh_batch_set_policy(h, C.byref(pol)))
         nbytes = C.c_uint64()
         _lib.check("sgh_batch_workspace_bytes", L.sgh_batch_workspace_bytes(h, C.byref(nbytes)))
         self.device = torch.device("cuda", torch.cuda.current_device()) if device is None \
@@ -204,6 +215,13 @@ class BatchSolver:
         e = C.c_int32()
         _lib.check("sgh_batch_error", _lib.lib().sgh_batch_error(self._h, C.byref(e), self._s()))
         return e.value
+
+    def set_wait_limit(self, polls: int = 0, stall_test: bool = False) -> None:
+        """Bound the tensor-core data waits to ``polls`` polls (0: the default);
+        ``stall_test`` makes the face transforms wait on a barrier nothing
+        completes, so the bounded-wait error path runs (tests only)."""
+        _lib.check("sgh_batch_set_wait_limit", _lib.lib().sgh_batch_set_wait_limit(
+            self._h, int(polls), 1 if stall_test else 0, self._s()))
 
     def launch_counts(self):
         a, b, c = C.c_int32(), C.c_int32(), C.c_int32()

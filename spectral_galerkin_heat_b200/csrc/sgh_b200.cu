@@ -482,6 +482,10 @@ k_converge(const DevParams* __restrict__ P, Ctrl* ctrl, const double* __restrict
     const int it = ctrl->iter + 1;
     ctrl->iter = it;
     ctrl->rel_err = rel;
+    if (ctrl->hist && it <= ctrl->hist_cap) {
+      ctrl->hist[2 * (it - 1)] = rms_d;
+      ctrl->hist[2 * (it - 1) + 1] = rel;
+    }
     int stop = 0;
     if (rel < P->tol) {
       ctrl->status = SGH_STEP_CONVERGED;
@@ -496,6 +500,12 @@ k_converge(const DevParams* __restrict__ P, Ctrl* ctrl, const double* __restrict
     ctrl->stop = stop;
     if (in_graph) cudaGraphSetConditional(h_picard, stop ? 0u : 1u);
   }
+}
+
+// Where k_converge records the Picard history of a step.
+__global__ void k_ctrl_history(Ctrl* ctrl, double* hist, int cap) {
+  ctrl->hist = hist;
+  ctrl->hist_cap = cap;
 }
 
 // Metrics and history of the committed step (solvers/spectral.py:502-542);
@@ -687,7 +697,8 @@ struct sgh_plan {
   size_t o_params, o_ctrl, o_mx, o_mxt, o_my, o_myt, o_mz, o_mzt, o_xc, o_yc, o_ct, o_cb;
   size_t o_K, o_KK, o_a, o_aK, o_trial, o_Tprev, o_Qm, o_t1, o_t2, o_vol, o_kp;
   size_t o_qlas, o_qnet, o_qev, o_qevold, o_Stop, o_Sbot, o_f1, o_f2, o_Tsurf, o_A;
-  size_t o_prelax, o_plas, o_psurf;
+  size_t o_prelax, o_plas, o_psurf, o_hist;
+  int hist_cap = 0;
   // face-space Picard state: F (Zt, Zb, Yt, Yb), W (6 weights), sigma, beta, Ab, n1 partials
   bool face_space = false;
   int nparts_fs = 0, nparts_n1 = 0;
@@ -1430,6 +1441,8 @@ int sgh_plan_create(const sgh_config* cfg, sgh_plan** out) {
   p->o_prelax = L.take(sizeof(double) * 2 * std::max(p->nparts_relax, nparts_axis));
   p->o_plas = L.take(sizeof(double) * p->nparts_las);
   p->o_psurf = L.take(sizeof(double) * 2 * std::max(p->nparts_surf, axis_blocks(h.nz + 1, 1, h.S)));
+  p->hist_cap = std::max(1, std::min(c.max_iter, SGH_PICARD_HISTORY_MAX));
+  p->o_hist = L.take(sizeof(double) * 2 * p->hist_cap);
   p->face_space = !latent && !prop_corr && !box;
   if (box) {
     p->box_z0 = c.Lz - c.box_size[2];
@@ -1491,6 +1504,7 @@ int sgh_plan_bind(sgh_plan* p, void* workspace, uint64_t bytes, void* stream) {
   const DevParams& h = p->hp;
   SGH_CK(cudaMemcpyAsync(p->P(), &h, sizeof(DevParams), cudaMemcpyHostToDevice, s));
   SGH_CK(cudaMemsetAsync(p->ctrl(), 0, sizeof(Ctrl), s));
+  k_ctrl_history<<<1, 1, 0, s>>>(p->ctrl(), p->d(p->o_hist), p->hist_cap);
   struct { int n; size_t m, mt; } mats[3] = {{h.nx, p->o_mx, p->o_mxt}, {h.ny, p->o_my, p->o_myt},
                                              {h.nz, p->o_mz, p->o_mzt}};
   for (auto& m : mats)
@@ -1715,6 +1729,22 @@ int sgh_box_geometry(const sgh_plan* p, sgh_box_geom* out) {
   out->d_fine[0] = h.dxf; out->d_fine[1] = h.dyf; out->d_fine[2] = h.dzf;
   out->dV_fine = h.dV_fine;
   out->z0 = p->box_z0;
+  return SGH_OK;
+}
+
+int sgh_picard_history(sgh_plan* p, double* out, int32_t cap, int32_t* n_iter, void* stream) {
+  if (!p || !out || !n_iter || cap < 0) return fail(SGH_ERR_INVALID, "null argument or negative cap");
+  if (!p->bound) return fail(SGH_ERR_STATE, "plan is not bound");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  int32_t it = 0;
+  SGH_CK(cudaMemcpyAsync(&it, &p->ctrl()->iter, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+  SGH_CK(cudaStreamSynchronize(s));
+  const int n = std::min(std::min(it, p->hist_cap), (int)cap);
+  if (n > 0) {
+    SGH_CK(cudaMemcpyAsync(out, p->ws + p->o_hist, sizeof(double) * 2 * n, cudaMemcpyDeviceToHost, s));
+    SGH_CK(cudaStreamSynchronize(s));
+  }
+  *n_iter = it;
   return SGH_OK;
 }
 

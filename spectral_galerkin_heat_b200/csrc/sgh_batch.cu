@@ -27,6 +27,7 @@
 #include <cstring>
 #include <map>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "sgh_b200.h"
@@ -49,7 +50,8 @@ struct BSlot {
   long long vol;   // element offset of this slot in the volume arenas
   long long face;  // element offset in the face arenas
   int zoff;        // offset in the Ct table
-  int eoff;        // offset of the slot's 1-D decay tables Ex (nx), Ey (ny), Ez (nz)
+  int eoff;        // offset of the slot's 1-D tables, each over x (nx), y (ny), z (nz):
+                   // decay E = exp(-alpha dt k^2), D = 1 - E, L = kbar k^2
   int mx, my;      // element offsets of the x / y DCT matrices (M, then M^T)
   int blk0, nblk;  // element / column blocks
   int rblk0, nrblk;  // relaxation blocks (RB elements)
@@ -86,6 +88,8 @@ struct BGlobal {
   int picard_any;   // some slot is still iterating (read by the eager step)
   unsigned slots_done;   // slots finished in the current kb_relax launch (back to 0 after it)
   int n_iter_slots;      // slots iterating in the current Picard iteration
+  unsigned wait_limit;   // polls of the tensor-core data waits (0: umma::WAIT_LIMIT)
+  int stall_test;        // 1: every face-transform CTA first waits on a barrier nothing completes
   int pad;
 };
 
@@ -167,11 +171,28 @@ __global__ void kb_matrix_planes(int N, const double* M, int inv, char* plane) {
   umma::pair_put<R>(plane, r, k, (N + umma::KC - 1) / umma::KC, val);
 }
 
+// KK of one mode in the mixed-precision form, from per-axis tables (FP32):
+// KK = (1 - Ex Ey Ez) / (kbar (qx^2 + qy^2 + qz^2)), and dt / (rho c) for the
+// zero mode (precompute_K_KK, physics/spectral_state.py:405-413, with
+// alpha rho c = kbar). The numerator is formed without cancellation as
+// (1 - Ex Ey) + Ex Ey (1 - Ez), each 1 - E_axis an accurate -expm1 table
+// entry, so the low modes (1 - K ~ 1e-4) keep full FP32 accuracy; the
+// quotient is a fast FP32 division. Relative error a few 1e-7, the order of
+// the FP32 rounding of a stored KK, at a handful of FP32 instructions per mode
+// instead of 4 bytes of HBM traffic.
+__device__ __forceinline__ double mode_kk(float dxy, float exy, float dz, float lxy, float lz,
+                                          double dt_rc) {
+  const float num = fmaf(exy, dz, dxy);
+  const float den = lxy + lz;
+  return den > 0.0f ? (double)__fdividef(num, den) : dt_rc;
+}
+
 // K, KK of every slot exactly as precompute_K_KK (physics/spectral_state.py:374-421),
-// in FP64, stored as R (K only when K is given); Ct tables; and the 1-D decay
-// tables E_axis[i] = exp(-alpha dt k_i^2). K = exp(-alpha dt (kx^2 + ky^2 +
-// kz^2)) is exactly separable, so K = Ex[x] Ey[y] Ez[z]: the mixed-precision
-// form evaluates it in FP64 from these tables instead of storing it.
+// in FP64, stored as R (K and KK only when given); Ct tables; and per axis the
+// 1-D tables E[i] = exp(-alpha dt k_i^2), D[i] = 1 - E[i] (as -expm1) and
+// L[i] = kbar k_i^2. K = exp(-alpha dt (kx^2 + ky^2 + kz^2)) is exactly
+// separable, K = Ex[x] Ey[y] Ez[z] (FP64), and KK follows from D, E and L
+// (mode_kk): the mixed-precision form stores neither.
 template <class R>
 __global__ void __launch_bounds__(BT) kb_tables(BView v, R* K, R* KK, double* Ct, double* E) {
   const int b = blockIdx.x;
@@ -190,19 +211,19 @@ __global__ void __launch_bounds__(BT) kb_tables(BView v, R* K, R* KK, double* Ct
     const double lam = alpha * (kz * kz + ky * ky + kx * kx);
     const double k = exp(-lam * sl.dt);
     if (K) K[sl.vol + i] = (R)k;
-    if (i < sl.nx) {
-      const double q = M_PI * (double)i / sl.Lx;
-      E[sl.eoff + i] = exp(-(alpha * (q * q)) * sl.dt);
+    const int nsum = sl.nx + sl.ny + sl.nz;
+    const int axis_n[3] = {sl.nx, sl.ny, sl.nz};
+    const double axis_L[3] = {sl.Lx, sl.Ly, sl.Lz};
+    for (int ax = 0, base = 0; ax < 3; base += axis_n[ax], ++ax) {
+      if (i < axis_n[ax]) {
+        const double q = M_PI * (double)i / axis_L[ax];
+        const double e = -(alpha * (q * q)) * sl.dt;
+        E[sl.eoff + base + i] = exp(e);
+        E[sl.eoff + nsum + base + i] = -expm1(e);
+        E[sl.eoff + 2 * nsum + base + i] = sl.k * (q * q);
+      }
     }
-    if (i < sl.ny) {
-      const double q = M_PI * (double)i / sl.Ly;
-      E[sl.eoff + sl.nx + i] = exp(-(alpha * (q * q)) * sl.dt);
-    }
-    if (i < sl.nz) {
-      const double q = M_PI * (double)i / sl.Lz;
-      E[sl.eoff + sl.nx + sl.ny + i] = exp(-(alpha * (q * q)) * sl.dt);
-    }
-    KK[sl.vol + i] = (R)((i == 0) ? sl.dt / rho_cp : ((k - 1.0) / (-lam)) / rho_cp);
+    if (KK) KK[sl.vol + i] = (R)((i == 0) ? sl.dt / rho_cp : ((k - 1.0) / (-lam)) / rho_cp);
     if (i < sl.nz) {
       const double c = (i == 0) ? sqrt(1.0 / sl.Lz) : sqrt(2.0 / sl.Lz);
       Ct[sl.zoff + i] = (i & 1) ? -c : c;
@@ -218,9 +239,19 @@ __global__ void __launch_bounds__(BT) kb_weights(BView v, const R* KK, double* W
   const BSlot& sl = v.slot[s];
   const int i = (b - sl.blk0) * BT + threadIdx.x;
   if (i >= sl.S) return;
+  const int nsum = sl.nx + sl.ny + sl.nz;
+  const double* E = v.E + sl.eoff;
+  const double* D = E + nsum;
+  const double* Lt = E + 2 * nsum;
+  const int ix = i % sl.nx, iy = sl.nx + i / sl.nx, z0 = sl.nx + sl.ny;
+  const float exy = (float)(E[ix] * E[iy]);
+  const float dxy = (float)(D[ix] + E[ix] * D[iy]);
+  const float lxy = (float)(Lt[ix] + Lt[iy]);
+  const double dt_rc = sl.dt / (sl.rho * sl.cp);
   double w = 0.0, q = 0.0;
   for (int p = 0; p < sl.nz; ++p) {
-    const double kk = (double)KK[sl.vol + (long long)p * sl.S + i];
+    const double kk = KK ? (double)KK[sl.vol + (long long)p * sl.S + i]
+                         : mode_kk(dxy, exy, (float)D[z0 + p], lxy, (float)Lt[z0 + p], dt_rc);
     const double ct = v.Ct[sl.zoff + p];
     w += ct * ct * kk;
     q += (kk * ct) * (kk * ct);
@@ -521,6 +552,7 @@ kb_face2d(BView v, F2Args args, double* part_tile, int n_stages, int bop_max) {
   uint64_t* done = full + f2::MAX_STAGES;
   uint32_t* tslot = reinterpret_cast<uint32_t*>(done + f2::MAX_STAGES);
   volatile int* okflag = reinterpret_cast<volatile int*>(tslot + 1);
+  uint64_t* stall = done + f2::MAX_STAGES + 1;  // never arrived on (wait test)
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   // TMEM: the x-pass keeps hi*hi, hi*lo and lo*hi in three accumulators
   // (columns 0, 64, 128: three independent MMA chains); y-pass row tile rt
@@ -551,10 +583,14 @@ kb_face2d(BView v, F2Args args, double* part_tile, int n_stages, int bop_max) {
       bulk_g2s(stg, v.mp + (size_t)myo + (size_t)(rt * nky + kc) * 2 * CA, 2 * CA, bar);
     }
   };
-  auto wait_full = [&](int g) { return mbar_wait_bounded(&full[g % S], (uint32_t)((g / S) & 1)); };
-  auto wait_done = [&](int g) { return mbar_wait_bounded(&done[g % S], (uint32_t)((g / S) & 1)); };
+  // data waits poll at most `lim` times (the batch's setting); the drain after
+  // a failed wait always keeps the full bound, so no copy or MMA is left in
+  // flight when the CTA exits
+  const unsigned lim = v.g->wait_limit ? v.g->wait_limit : WAIT_LIMIT;
+  auto wait_full = [&](int g, unsigned l) { return mbar_wait_bounded(&full[g % S], (uint32_t)((g / S) & 1), l); };
+  auto wait_done = [&](int g, unsigned l) { return mbar_wait_bounded(&done[g % S], (uint32_t)((g / S) & 1), l); };
   auto step = [&](int g) -> bool {
-    if (!wait_full(g)) return false;
+    if (!wait_full(g, lim)) return false;
     tc_fence_after();
     const uint32_t s0 = smem_u32(ring + (g % S) * f2::STAGE);
     uint32_t ah, al, bh, bl, d0, d1, d2;
@@ -586,7 +622,7 @@ kb_face2d(BView v, F2Args args, double* part_tile, int n_stages, int bop_max) {
     committed = g + 1;
     const int nxt = g - 1 + S;  // the stage of chunk g - 1 takes chunk g - 1 + S
     if (g >= 1 && nxt < total && nxt >= issued) {
-      if (!wait_done(g - 1)) return false;
+      if (!wait_done(g - 1, lim)) return false;
       load(nxt);
       issued = nxt + 1;
     }
@@ -595,8 +631,8 @@ kb_face2d(BView v, F2Args args, double* part_tile, int n_stages, int bop_max) {
   auto fail = [&]() {  // thread 0: record, then wait (bounded) for in-flight copies and MMAs
     atomicExch(&v.g->umma_err, 1);
     *okflag = 0;
-    for (int g = issued - S < 0 ? 0 : issued - S; g < issued; ++g) wait_full(g);
-    for (int g = committed - S < 0 ? 0 : committed - S; g < committed; ++g) wait_done(g);
+    for (int g = issued - S < 0 ? 0 : issued - S; g < issued; ++g) wait_full(g, WAIT_LIMIT);
+    for (int g = committed - S < 0 ? 0 : committed - S; g < committed; ++g) wait_done(g, WAIT_LIMIT);
   };
 
   // the first copies go out before the tensor memory is allocated
@@ -605,6 +641,7 @@ kb_face2d(BView v, F2Args args, double* part_tile, int n_stages, int bop_max) {
       mbar_init(&full[i], 1);
       mbar_init(&done[i], 1);
     }
+    mbar_init(stall, 1);
     *okflag = 1;
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     const int pre = total < S ? total : S;
@@ -620,9 +657,10 @@ kb_face2d(BView v, F2Args args, double* part_tile, int n_stages, int bop_max) {
   const int q = warp & 3, half = warp >> 2;  // TMEM lane quarter, column half
   for (int rt = 0; rt < nrt; ++rt) {
     if (tid == 0 && *okflag) {
-      bool ok = true;
+      // the wait test: a wait that can only run out, with copies in flight
+      bool ok = !(rt == 0 && v.g->stall_test) || mbar_wait_bounded(stall, 0u, lim);
       for (int kc = 0; kc < nkx && ok; ++kc) ok = step(rt * nkx + kc);
-      if (ok) ok = wait_done(rt * nkx + nkx - 1);
+      if (ok) ok = wait_done(rt * nkx + nkx - 1, lim);
       if (!ok) fail();
     }
     __syncthreads();
@@ -665,7 +703,7 @@ kb_face2d(BView v, F2Args args, double* part_tile, int n_stages, int bop_max) {
     tc_fence_after();
     bool ok = true;
     for (int g = n_x; g < total && ok; ++g) ok = step(g);
-    if (ok) ok = wait_done(total - 1);
+    if (ok) ok = wait_done(total - 1, lim);
     if (!ok) fail();
   }
   __syncthreads();
@@ -981,10 +1019,13 @@ __device__ __forceinline__ void vstore(R* p, const R (&o)[VEC]) {
   *reinterpret_cast<T*>(p) = t;
 }
 
-template <class R, int VEC, bool COMMIT>
+template <class R, int VEC, bool COMMIT, int U>
 __global__ void __launch_bounds__(BT / VEC)
 kb_volume(BView v, R* a, const R* K, const R* KK, const double* sigma, double* Zt, double* Yt,
           double* part_n1) {
+  // FP32 modes (mixed precision): K and KK formed from the 1-D tables; FP64
+  // modes: K and KK read from the volume arenas
+  constexpr bool TAB = sizeof(R) == 4;
   constexpr int NT = BT / VEC;
   __shared__ double sh[2 * (NT / 32)];
   const int b = blockIdx.x;
@@ -996,35 +1037,61 @@ kb_volume(BView v, R* a, const R* K, const R* KK, const double* sigma, double* Z
   double n1 = 0.0, dummy = 0.0;
   if (i0 < sl.S) {
     const double* ct = v.Ct + sl.zoff;
-    const double* ez = v.E + sl.eoff + sl.nx + sl.ny;
+    const int nsum = sl.nx + sl.ny + sl.nz;
+    const double* E = v.E + sl.eoff;
+    const double* ez = E + sl.nx + sl.ny;
+    const double* dz = ez + nsum;
+    const double* lz = ez + 2 * nsum;
+    const double dt_rc = sl.dt / (sl.rho * sl.cp);
     double sg[VEC], exy[VEC], zt[VEC], yt[VEC];
+    float exy32[VEC], dxy32[VEC], lxy32[VEC];
 #pragma unroll
     for (int c = 0; c < VEC; ++c) {
       const int i = i0 + c;
+      const int ix = i % sl.nx, iy = sl.nx + i / sl.nx;
       sg[c] = COMMIT ? sigma[sl.face + i] : 0.0;
-      exy[c] = K ? 0.0 : v.E[sl.eoff + i % sl.nx] * v.E[sl.eoff + sl.nx + i / sl.nx];
+      exy[c] = TAB ? E[ix] * E[iy] : 0.0;
+      exy32[c] = (float)exy[c];
+      dxy32[c] = TAB ? (float)(E[nsum + ix] + E[ix] * E[nsum + iy]) : 0.0f;
+      lxy32[c] = TAB ? (float)(E[2 * nsum + ix] + E[2 * nsum + iy]) : 0.0f;
       zt[c] = 0.0;
       yt[c] = 0.0;
     }
-#pragma unroll 4
-    for (int p = 0; p < sl.nz; ++p) {
-      const long long j0 = sl.vol + (long long)p * sl.S + i0;
-      R av[VEC], kkv[VEC], kvv[VEC];
-      vload<R, VEC>(a + j0, av);
-      vload<R, VEC>(KK + j0, kkv);
-      if (K) vload<R, VEC>(K + j0, kvv);
-      const double cp = ct[p];
+    // U planes per round: every load of the round is issued before its
+    // arithmetic, so U x VEC values per thread are in flight
+    for (int p0 = 0; p0 < sl.nz; p0 += U) {
+      R av[U][VEC], kkv[U][VEC], kvv[U][VEC];
 #pragma unroll
-      for (int c = 0; c < VEC; ++c) {
-        const double kv = K ? (double)kvv[c] : exy[c] * ez[p];
-        const double kk = (double)kkv[c];
-        if (COMMIT) av[c] = (R)((double)av[c] * kv + kk * (cp * sg[c]));
-        const double ak = (double)av[c] * kv;
-        zt[c] = fma(cp, ak, zt[c]);
-        yt[c] = fma(ak * kk, cp, yt[c]);
-        n1 = fma(ak, ak, n1);
+      for (int u = 0; u < U; ++u) {
+        if (p0 + u < sl.nz) {
+          const long long j0 = sl.vol + (long long)(p0 + u) * sl.S + i0;
+          vload<R, VEC>(a + j0, av[u]);
+          if (!TAB) {
+            vload<R, VEC>(KK + j0, kkv[u]);
+            vload<R, VEC>(K + j0, kvv[u]);
+          }
+        }
       }
-      if (COMMIT) vstore<R, VEC>(a + j0, av);
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int p = p0 + u;
+        if (p < sl.nz) {
+          const double cp = ct[p];
+          const double ezp = TAB ? ez[p] : 0.0;
+          const float dzp = TAB ? (float)dz[p] : 0.0f, lzp = TAB ? (float)lz[p] : 0.0f;
+#pragma unroll
+          for (int c = 0; c < VEC; ++c) {
+            const double kv = TAB ? exy[c] * ezp : (double)kvv[u][c];
+            const double kk = TAB ? mode_kk(dxy32[c], exy32[c], dzp, lxy32[c], lzp, dt_rc) : (double)kkv[u][c];
+            if (COMMIT) av[u][c] = (R)((double)av[u][c] * kv + kk * (cp * sg[c]));
+            const double ak = (double)av[u][c] * kv;
+            zt[c] = fma(cp, ak, zt[c]);
+            yt[c] = fma(ak * kk, cp, yt[c]);
+            n1 = fma(ak, ak, n1);
+          }
+          if (COMMIT) vstore<R, VEC>(a + sl.vol + (long long)p * sl.S + i0, av[u]);
+        }
+      }
     }
 #pragma unroll
     for (int c = 0; c < VEC; ++c) {
@@ -1111,6 +1178,7 @@ struct sgh_batch {
   size_t xa_bytes = 0, mp_bytes = 0;
   int f2_stages = 0, f2_bop = 0, f2_smem = 0;  // fused face transform: ring stages, operand bytes, smem
   int vec = 1;  // columns per thread of the volume passes
+  int vol_unroll = 4;  // z-planes per load round of the volume passes (2, 4 or 8)
   std::vector<std::pair<int, long long>> mplane_list;  // (N, byte offset of the forward plane)
   size_t ws_need = 0;
   char* ws = nullptr;
@@ -1184,10 +1252,22 @@ void launch_volume(sgh_batch* B, cudaStream_t s, R* a, const R* K, const R* KK) 
   const BView v = B->view();
   double *sg = B->d(B->o_sigma), *zt = B->d(B->o_Zt), *yt = B->d(B->o_Yt), *pn = B->d(B->o_pn1);
   constexpr int VW = sizeof(R) == 4 ? 4 : 2;
-  if (B->vec == VW)
-    kb_volume<R, VW, COMMIT><<<B->tot_blk, BT / VW, 0, s>>>(v, a, K, KK, sg, zt, yt, pn);
-  else
-    kb_volume<R, 1, COMMIT><<<B->tot_blk, BT, 0, s>>>(v, a, K, KK, sg, zt, yt, pn);
+  auto go = [&](auto vec, auto u) {
+    constexpr int V_ = decltype(vec)::value, U_ = decltype(u)::value;
+    kb_volume<R, V_, COMMIT, U_><<<B->tot_blk, BT / V_, 0, s>>>(v, a, K, KK, sg, zt, yt, pn);
+  };
+  using I1 = std::integral_constant<int, 1>;
+  using IV = std::integral_constant<int, VW>;
+  const int u = B->vol_unroll;
+  if (B->vec == VW) {
+    if (u == 2) go(IV{}, std::integral_constant<int, 2>{});
+    else if (u == 8) go(IV{}, std::integral_constant<int, 8>{});
+    else go(IV{}, std::integral_constant<int, 4>{});
+  } else {
+    if (u == 2) go(I1{}, std::integral_constant<int, 2>{});
+    else if (u == 8) go(I1{}, std::integral_constant<int, 8>{});
+    else go(I1{}, std::integral_constant<int, 4>{});
+  }
 }
 
 template <class R>
@@ -1195,7 +1275,7 @@ void enqueue_pre(sgh_batch* B, cudaStream_t s, cudaGraphConditionalHandle h, int
   const BView v = B->view();
   R* a = reinterpret_cast<R*>(B->ws + B->o_a);
   R* K = B->precision == SGH_PRECISION_MIXED ? nullptr : reinterpret_cast<R*>(B->ws + B->o_K);
-  R* KK = reinterpret_cast<R*>(B->ws + B->o_KK);
+  R* KK = B->precision == SGH_PRECISION_MIXED ? nullptr : reinterpret_cast<R*>(B->ws + B->o_KK);
   kb_begin<<<1, CT, 0, s>>>(v, h, in_graph);
   kb_face_begin<<<B->tot_rblk, BT, 0, s>>>(v, B->d(B->o_qlas), B->d(B->o_qnet), B->d(B->o_qevold), B->d(B->o_plas));
   launch_volume<R, false>(B, s, a, K, KK);
@@ -1232,7 +1312,7 @@ void enqueue_post(sgh_batch* B, cudaStream_t s, cudaGraphConditionalHandle h, in
   const BView v = B->view();
   R* a = reinterpret_cast<R*>(B->ws + B->o_a);
   R* K = B->precision == SGH_PRECISION_MIXED ? nullptr : reinterpret_cast<R*>(B->ws + B->o_K);
-  R* KK = reinterpret_cast<R*>(B->ws + B->o_KK);
+  R* KK = B->precision == SGH_PRECISION_MIXED ? nullptr : reinterpret_cast<R*>(B->ws + B->o_KK);
   face2d<true, false, F2_COMMIT>(B, s, B->d(B->o_A),
                                  EB_CommitSurface{B->d(B->o_Tsurf), B->d(B->o_qev), B->d(B->o_qevold)},
                                  F2Args{B->d(B->o_Tsurf), B->d(B->o_qevold), B->d(B->o_qev), 0}, B->d(B->o_ptile));
@@ -1421,7 +1501,7 @@ int sgh_batch_create(const sgh_config* cfgs, int32_t n, int32_t precision, sgh_b
     B->tot_vol = sl.vol + sl.V;
     B->tot_face += sl.S;
     B->tot_z += c.nz;
-    B->tot_e += c.nx + c.ny + c.nz;
+    B->tot_e += 3 * (c.nx + c.ny + c.nz);  // E, 1 - E and kbar k^2 per axis
     B->tot_blk += sl.nblk;
     B->tot_rblk += sl.nrblk;
     B->tot_tile += sl.ntile;
@@ -1454,7 +1534,7 @@ int sgh_batch_create(const sgh_config* cfgs, int32_t n, int32_t precision, sgh_b
   B->o_ct = L.take(sizeof(double) * (size_t)B->tot_z);
   B->o_a = L.take(VE);
   B->o_K = L.take(precision == SGH_PRECISION_MIXED ? 0 : VE);  // mixed: K from the decay tables
-  B->o_KK = L.take(VE);
+  B->o_KK = L.take(precision == SGH_PRECISION_MIXED ? 0 : VE);  // mixed: KK from the 1-D tables
   B->o_E = L.take(sizeof(double) * (size_t)B->tot_e);
   B->o_qlas = L.take(F8);
   B->o_qnet = L.take(F8);
@@ -1497,6 +1577,15 @@ int sgh_batch_destroy(sgh_batch* B) {
   if (B->cs1) cudaStreamDestroy(B->cs1);
   if (B->cs2) cudaStreamDestroy(B->cs2);
   delete B;
+  return SGH_OK;
+}
+
+int sgh_batch_set_policy(sgh_batch* B, const sgh_batch_policy* pol) {
+  if (!B || !pol) return bfail(SGH_ERR_INVALID, "null argument");
+  if (B->bound) return bfail(SGH_ERR_STATE, "set the policy before sgh_batch_bind (the graphs are captured there)");
+  const int u = pol->vol_unroll ? pol->vol_unroll : 4;
+  if (u != 2 && u != 4 && u != 8) return bfail(SGH_ERR_INVALID, "vol_unroll must be 2, 4 or 8");
+  B->vol_unroll = u;
   return SGH_OK;
 }
 
@@ -1549,9 +1638,8 @@ int sgh_batch_bind(sgh_batch* B, void* workspace, uint64_t bytes, void* stream) 
         kb_matrix_planes<f2::NB><<<g, BT, 0, s>>>(N, B->d(B->o_mats) + moff, inv, pl(2 * pb + inv * pn));
       }
     }
-    float* KK = reinterpret_cast<float*>(B->ws + B->o_KK);
-    kb_tables<float><<<B->tot_vblk, BT, 0, s>>>(v, nullptr, KK, B->d(B->o_ct), B->d(B->o_E));
-    kb_weights<float><<<B->tot_blk, BT, 0, s>>>(v, KK, B->d(B->o_Wtt), B->d(B->o_Qtt));
+    kb_tables<float><<<B->tot_vblk, BT, 0, s>>>(v, nullptr, nullptr, B->d(B->o_ct), B->d(B->o_E));
+    kb_weights<float><<<B->tot_blk, BT, 0, s>>>(v, nullptr, B->d(B->o_Wtt), B->d(B->o_Qtt));
   } else {
     double* K = B->d(B->o_K);
     double* KK = B->d(B->o_KK);
@@ -1658,7 +1746,12 @@ int sgh_batch_buffer(const sgh_batch* B, int32_t slot, int32_t which, void** ptr
       off = B->o_K + e * sl.vol;
       nb = e * sl.V;
       break;
-    case SGH_BUF_KK: off = B->o_KK + e * sl.vol; nb = e * sl.V; break;
+    case SGH_BUF_KK:
+      if (B->precision == SGH_PRECISION_MIXED)
+        return bfail(SGH_ERR_INVALID, "mixed-precision batches do not store KK (it is formed from 1-D tables)");
+      off = B->o_KK + e * sl.vol;
+      nb = e * sl.V;
+      break;
     case SGH_BUF_Q_EVAP_OLD: off = B->o_qevold + sizeof(double) * sl.face; nb = sizeof(double) * sl.S; break;
     case SGH_BUF_SURFACE: off = B->o_Tsurf + sizeof(double) * sl.face; nb = sizeof(double) * sl.S; break;
     default: return bfail(SGH_ERR_INVALID, "buffer id not available for batch slots");
@@ -1678,12 +1771,24 @@ int sgh_batch_error(const sgh_batch* B, int32_t* err, void* stream) {
   return SGH_OK;
 }
 
+int sgh_batch_set_wait_limit(sgh_batch* B, uint32_t polls, int32_t stall_test, void* stream) {
+  if (!B || !B->bound) return bfail(SGH_ERR_STATE, "batch is not bound");
+  if (stall_test && polls == 0) return bfail(SGH_ERR_INVALID, "the wait test needs an explicit poll bound");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const unsigned v[2] = {polls, stall_test ? 1u : 0u};
+  static_assert(offsetof(BGlobal, stall_test) == offsetof(BGlobal, wait_limit) + sizeof(unsigned),
+                "wait_limit and stall_test are adjacent");
+  SGB_CK(cudaMemcpyAsync(B->ws + B->o_g + offsetof(BGlobal, wait_limit), v, sizeof(v),
+                         cudaMemcpyHostToDevice, s));
+  SGB_CK(cudaStreamSynchronize(s));
+  return SGH_OK;
+}
+
 int sgh_batch_volume_pass(sgh_batch* B, void* stream) {
   if (!B || !B->bound) return bfail(SGH_ERR_STATE, "batch is not bound");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   if (B->precision == SGH_PRECISION_MIXED)
-    launch_volume<float, true>(B, s, reinterpret_cast<float*>(B->ws + B->o_a), nullptr,
-                               reinterpret_cast<const float*>(B->ws + B->o_KK));
+    launch_volume<float, true>(B, s, reinterpret_cast<float*>(B->ws + B->o_a), nullptr, nullptr);
   else
     launch_volume<double, true>(B, s, B->d(B->o_a), B->d(B->o_K), B->d(B->o_KK));
   SGB_CK(cudaGetLastError());

@@ -58,6 +58,10 @@ struct Ctrl {
   int have_tprev, box_i0x, box_i0y, pad_c;
   double box_sx, box_sy;
   unsigned long long box_max[4];
+  // Picard history of the current step: (rms of the residual, relative
+  // residual) per iteration, the first hist_cap iterations
+  double* hist;
+  int hist_cap, pad_h;
 };
 
 // ---------------------------------------------------------------------------

@@ -11,15 +11,25 @@ For one configuration and laser path this runs, side by side on the device:
   one part in 1e12. Where this run already parts from ``fp64``, the problem
   is ill-conditioned and a difference between precisions there is not a
   precision error.
+* ``fp64_fp32_rounded``: the FP64 solver again, with its modes rounded to
+  FP32 once, after the first step. A random perturbation of the whole volume
+  mostly lands in fast-decaying modes; this one has the structure of the
+  rounding that an FP32 modal state undergoes every step, so it shows how far
+  a single such rounding carries on this problem (the floor of any form that
+  stores the state in FP32).
 
 At each checkpoint step the report gives, against ``fp64``:
 
 * ``rel_l2``: ||T - T_fp64|| / ||T_fp64|| over the cell-centred volume field
   (the transform is orthonormal, so this is also the relative L2 of the modes);
 * ``peak_T``: the maximum of the volume field, and its difference in K;
-* ``melt_pool``: length (x), width (y) and depth (from the top face z = Lz) of
-  the cells at or above the liquidus, in metres (cell extents), and their
-  differences.
+* ``melt_pool``: length (x) and width (y) of the region at or above the
+  liquidus on the top face, and its depth below the top face (z = Lz), on the
+  node-centred field (the reference's ``reconstruct_temperature_DCT``,
+  evaluated on the device), each end located where the linear interpolation
+  between neighbouring nodes crosses the liquidus; and their differences.
+  ``melt_pool_cells`` gives the same extents in whole cells of the
+  cell-centred field.
 
 Run it with ``python -m spectral_galerkin_heat_b200.precision`` (see --help);
 the default is the 256 x 128 x 64 straight-track study with seeded power and
@@ -31,11 +41,12 @@ from __future__ import annotations
 import argparse
 import copy
 import json
+from types import SimpleNamespace
 from typing import Dict, List, Optional, Sequence
 
 import numpy as np
 
-__all__ = ["melt_pool", "compare_fields", "run_study"]
+__all__ = ["melt_pool", "melt_pool_nodal", "compare_fields", "run_study"]
 
 
 def melt_pool(T: np.ndarray, dx: float, dy: float, dz: float, T_melt: float) -> Dict[str, float]:
@@ -51,17 +62,67 @@ def melt_pool(T: np.ndarray, dx: float, dy: float, dz: float, T_melt: float) -> 
             "depth": float((nz - zs.min()) * dz), "cells": int(m.sum())}
 
 
-def compare_fields(T: np.ndarray, T_ref: np.ndarray, cell, T_melt: float) -> Dict[str, object]:
-    """Error report of ``T`` against ``T_ref`` (both (nz, ny, nx), FP64)."""
+def _crossings(T_line: np.ndarray, x: np.ndarray, T_melt: float):
+    """Ends of the region T >= T_melt along one node line: (lo, hi) positions
+    with the outer crossings interpolated linearly between nodes, or None."""
+    hot = np.nonzero(T_line >= T_melt)[0]
+    if hot.size == 0:
+        return None
+    i0, i1 = int(hot[0]), int(hot[-1])
+
+    def cross(a, b):  # node a is hot, node b is not
+        ta, tb = T_line[a], T_line[b]
+        return x[a] + (x[b] - x[a]) * (ta - T_melt) / (ta - tb)
+    lo = x[i0] if i0 == 0 else cross(i0, i0 - 1)
+    hi = x[i1] if i1 == len(x) - 1 else cross(i1, i1 + 1)
+    return lo, hi
+
+
+def melt_pool_nodal(T_nodes: np.ndarray, lengths, T_melt: float) -> Dict[str, float]:
+    """Melt-pool extents on a node-centred field ``T_nodes`` of shape
+    (nx+1, ny+1, nz+1) at nodes (j Lx/nx, k Ly/ny, l Lz/nz), as
+    ``reconstruct_temperature_DCT`` returns it: length along x and width along
+    y of the region T >= T_melt on the top face z = Lz, and depth of that
+    region below the top face; the ends are interpolated linearly to the
+    isotherm (zero when no node melts)."""
+    T = np.asarray(T_nodes, dtype=np.float64)
+    nx, ny, nz = (n - 1 for n in T.shape)
+    Lx, Ly, Lz = (float(v) for v in lengths)
+    xs, ys, zs = (np.linspace(0.0, L, n + 1) for L, n in ((Lx, nx), (Ly, ny), (Lz, nz)))
+    top = T[:, :, nz]
+    out = {"length": 0.0, "width": 0.0, "depth": 0.0}
+    spans = [c for c in (_crossings(top[:, k], xs, T_melt) for k in range(ny + 1)) if c]
+    if not spans:
+        return out
+    out["length"] = float(max(h for _, h in spans) - min(lo for lo, _ in spans))
+    spans = [c for c in (_crossings(top[j, :], ys, T_melt) for j in range(nx + 1)) if c]
+    out["width"] = float(max(h for _, h in spans) - min(lo for lo, _ in spans))
+    depth = 0.0
+    for j, k in zip(*np.nonzero(top >= T_melt)):
+        col = T[j, k, ::-1]                       # from the top face down
+        c = _crossings(col, Lz - zs[::-1], T_melt)
+        depth = max(depth, c[1])
+    out["depth"] = float(depth)
+    return out
+
+
+def compare_fields(T: np.ndarray, T_ref: np.ndarray, cell, T_melt: float,
+                   nodes=None, nodes_ref=None, lengths=None) -> Dict[str, object]:
+    """Error report of ``T`` against ``T_ref`` (both (nz, ny, nx), FP64), with
+    the nodal melt pool when the node-centred fields are given."""
     dx, dy, dz = cell
     mp, mp_ref = melt_pool(T, dx, dy, dz, T_melt), melt_pool(T_ref, dx, dy, dz, T_melt)
-    return {
+    rep = {
         "rel_l2": float(np.linalg.norm(T - T_ref) / np.linalg.norm(T_ref)),
         "peak_T": float(T.max()), "peak_T_ref": float(T_ref.max()),
         "peak_T_err_K": float(T.max() - T_ref.max()),
-        "melt_pool": mp, "melt_pool_ref": mp_ref,
-        "melt_pool_err_m": {k: mp[k] - mp_ref[k] for k in ("length", "width", "depth")},
+        "melt_pool_cells": mp, "melt_pool_cells_ref": mp_ref,
     }
+    if nodes is not None:
+        mn, mn_ref = melt_pool_nodal(nodes, lengths, T_melt), melt_pool_nodal(nodes_ref, lengths, T_melt)
+        rep.update(melt_pool=mn, melt_pool_ref=mn_ref,
+                   melt_pool_err_m={k: mn[k] - mn_ref[k] for k in ("length", "width", "depth")})
+    return rep
 
 
 def run_study(cfg: dict, path, checkpoints: Sequence[int], picard: Optional[dict] = None,
@@ -69,6 +130,7 @@ def run_study(cfg: dict, path, checkpoints: Sequence[int], picard: Optional[dict
     """Step the three runs to each checkpoint and compare (see the module doc)."""
     import torch
 
+    from . import kernels
     from .batch import BatchSolver
     from .config import SimulationContext
     from .solver import B200SpectralSolver
@@ -81,6 +143,8 @@ def run_study(cfg: dict, path, checkpoints: Sequence[int], picard: Optional[dict
     dt = float(num.dt)
     Lx, Ly, Lz = cfg["domain"]["size"]
     cell = (Lx / num.nx, Ly / num.ny, Lz / num.nz)
+    lengths = (Lx, Ly, Lz)
+    geo = SimpleNamespace(size=lengths)
     T_melt = float(cfg["material"]["T_liquidus"])
     total = int(max(checkpoints))
 
@@ -91,6 +155,10 @@ def run_study(cfg: dict, path, checkpoints: Sequence[int], picard: Optional[dict
     T0 = per.volume_temperature().cpu().numpy()
     rng = np.random.default_rng(seed)
     per.set_state(T0 * (1.0 + perturb * rng.standard_normal(T0.shape)))
+    rnd = B200SpectralSolver(None, copy.copy(ctx))
+    rnd.initialize()
+    rnd.run(0.0, 1)
+    rnd.state.a.copy_(rnd.state.a.to(torch.float32).to(torch.float64))
     mix = BatchSolver([copy.copy(ctx)], "mixed")
     mix.start(0, total, record=True)
 
@@ -99,22 +167,32 @@ def run_study(cfg: dict, path, checkpoints: Sequence[int], picard: Optional[dict
         n = cp - done
         ref_m = ref.run(done * dt, n)
         per.run(done * dt, n)
+        rnd.run(max(done, 1) * dt, cp - max(done, 1))
         mix.step(n)
         done = cp
         T_ref = ref.volume_temperature().cpu().numpy()
         T_per = per.volume_temperature().cpu().numpy()
-        T_mix = ref.volume_temperature(mix.modes(0).to(torch.float64).contiguous()).cpu().numpy()
+        T_rnd = rnd.volume_temperature().cpu().numpy()
+        a_mix = mix.modes(0).to(torch.float64).contiguous()
+        T_mix = ref.volume_temperature(a_mix).cpu().numpy()
+        nodes = {name: kernels.reconstruct_temperature_DCT(a, geo).cpu().numpy()
+                 for name, a in (("ref", ref.state.a), ("per", per.state.a), ("rnd", rnd.state.a),
+                                 ("mix", a_mix))}
         mm = mix.metrics(0)[-1]
         out.append({
             "step": cp,
             "picard_iters_fp64_last": ref_m[-1]["n_evap_iter"], "picard_iters_mixed_last": mm["n_evap_iter"],
             "T_surface_max_fp64": ref_m[-1]["T_surface_max"], "T_surface_max_mixed": mm["T_surface_max"],
-            "mixed": compare_fields(T_mix, T_ref, cell, T_melt),
-            "fp64_perturbed": compare_fields(T_per, T_ref, cell, T_melt),
+            "mixed": compare_fields(T_mix, T_ref, cell, T_melt, nodes["mix"], nodes["ref"], lengths),
+            "fp64_perturbed": compare_fields(T_per, T_ref, cell, T_melt, nodes["per"], nodes["ref"],
+                                             lengths),
+            "fp64_fp32_rounded": compare_fields(T_rnd, T_ref, cell, T_melt, nodes["rnd"], nodes["ref"],
+                                                lengths),
             "tensor_core_error": mix.tensor_core_error(),
         })
     ref.finalize()
     per.finalize()
+    rnd.finalize()
     mix.close()
     return out
 

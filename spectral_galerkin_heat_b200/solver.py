@@ -255,6 +255,7 @@ class B200SpectralSolver(HeatSolver):
         self._grid_latent = False
         self._latent_truncation_warned = False
         self.last_flags = 0  # sgh_step_out.flags of the last step (box truncation bits)
+        self.last_status = None  # Picard outcome of the last step
 
     # ---- configuration -------------------------------------------------
     def _resolve_picard_params(self, dtype) -> None:
@@ -353,9 +354,29 @@ class B200SpectralSolver(HeatSolver):
             self.state.fine_mesh.primed = True
         metrics = self._metrics(out, t)
         if self.track_picard_history:
-            self.picard_history = [{"iter": metrics["n_evap_iter"] - 1, "rms_diff": None,
-                                    "rho": None, "true_rel_err": metrics["picard_rel_err"]}]
+            self.picard_history = self.read_picard_history()
         return self.state, metrics
+
+    def read_picard_history(self):
+        """Per-iteration record of the last step, as the reference keeps it with
+        ``track_picard_history`` (``solvers/spectral.py:470-481``): ``iter``,
+        ``rms_diff`` (rms of the residual), ``rho`` (its ratio to the previous
+        iteration's) and ``true_rel_err``; written on the device by the
+        convergence test, read in one copy (the first SGH_PICARD_HISTORY_MAX
+        iterations)."""
+        self._require()
+        cap = _lib.PICARD_HISTORY_MAX
+        buf = (C.c_double * (2 * cap))()
+        n = C.c_int32()
+        _lib.check("sgh_picard_history", _lib.lib().sgh_picard_history(
+            self._plan, buf, cap, C.byref(n), C.c_void_p(self.state.stream.cuda_stream)))
+        hist = []
+        for k in range(min(n.value, cap)):
+            rms, rel = buf[2 * k], buf[2 * k + 1]
+            prev = hist[-1]["rms_diff"] if hist else 0.0
+            hist.append({"iter": k, "rms_diff": rms, "rho": rms / prev if k > 0 and prev > 0 else None,
+                         "true_rel_err": rel})
+        return hist
 
     def _check_box_dt(self, dt) -> None:
         # The box history moves by v * num.dt (physics/spectral_ops.py:300-302)
@@ -382,6 +403,10 @@ class B200SpectralSolver(HeatSolver):
 
     def _metrics(self, out, t):
         self.last_flags = int(out.flags)
+        # "converged" | "capped" | "nonfinite" (the Picard loop stops on a
+        # non-finite residual, as the reference's comparison with the
+        # tolerance would never succeed on one)
+        self.last_status = _lib.STEP_STATUS.get(int(out.status), int(out.status))
         self._box_warning(self.last_flags)
         conv = bool(out.converged)
         if not conv and out.n_iter > 0 and not self._picard_cap_warned:

@@ -168,3 +168,35 @@ def test_mixed_batch_rejects_tall_faces():
     from spectral_galerkin_heat_b200.batch import BatchSolver
     with pytest.raises(Exception, match="ny <= 256"):
         BatchSolver([_ctx(64, 300, 8, seed=1, steps=2)], "mixed")
+
+
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_every_tile_policy_gives_the_same_result(precision):
+    """The autotuner's candidate policies change only how the volume pass
+    issues its loads, not the arithmetic: every candidate gives the same bits,
+    and the result matches the oracle (FP64 to 1e-10, mixed to 1e-4)."""
+    from oracle.sgh_oracle import OracleSolver
+    from spectral_galerkin_heat_b200.autotune import BATCH_CANDIDATES
+    from spectral_galerkin_heat_b200.batch import BatchSolver
+    steps = 6
+    ctxs = [_ctx(*sh, seed=10 + i, steps=steps) for i, sh in enumerate(SHAPES)]
+    modes = []
+    for pol in BATCH_CANDIDATES:
+        b = BatchSolver(ctxs, precision, policy=pol)
+        assert b.policy == pol
+        for i in range(len(ctxs)):
+            b.start(i, steps)
+        b.step(steps)
+        assert b.tensor_core_error() == 0
+        modes.append([b.modes(i).double().cpu().numpy() for i in range(len(ctxs))])
+        b.close()
+    for other in modes[1:]:
+        for x, y in zip(modes[0], other):
+            assert np.array_equal(x, y)
+    tol = 1e-10 if precision == "fp64" else 1e-4
+    for i, ctx in enumerate(ctxs):
+        o = OracleSolver(ctx)
+        o.initialize()
+        for k in range(steps):
+            o.step(k * ctx.num.dt, ctx.num.dt)
+        assert rel_l2(modes[0][i], o.a) < tol

@@ -18,5 +18,9 @@ def test_precision_report_small_case():
         assert r["fp64_perturbed"]["rel_l2"] < 1e-9
         assert abs(r["mixed"]["peak_T_err_K"]) < 1.0
     last = rep[-1]["mixed"]
-    assert last["melt_pool"]["cells"] > 0
-    assert all(abs(v) <= 62.5e-6 + 1e-12 for v in last["melt_pool_err_m"].values())  # one cell
+    assert last["melt_pool_cells"]["cells"] > 0
+    # nodal extents with interpolated isotherm crossings: a relative field
+    # error of 1e-6 moves the liquidus by far less than a micrometre
+    assert last["melt_pool"]["length"] > 0 and last["melt_pool"]["depth"] > 0
+    assert all(abs(v) <= 1e-6 for v in last["melt_pool_err_m"].values())
+    assert rep[-1]["fp64_fp32_rounded"]["rel_l2"] < 1e-5

@@ -43,3 +43,24 @@ def test_two_replicas_aggregate_max_time_and_summed_work():
     for rank, times, counts in out:
         assert times == [11.0, 10.0]     # max over ranks of each interval
         assert counts == [300, 14]       # sum over ranks of each count
+
+
+@pytest.mark.timeout(300)
+def test_bench_gpus_two_starts_two_ranks():
+    """``bench.py --gpus 2`` without a launcher starts two ranks itself (one
+    process per GPU) and reports the aggregate with n_gpus from the world size;
+    a host-only stand-in workload keeps the test off the GPU."""
+    import json
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = {k: v for k, v in os.environ.items() if k not in ("WORLD_SIZE", "RANK", "LOCAL_RANK")}
+    out = subprocess.run([sys.executable, os.path.join(root, "bench.py"), "--gpus", "2",
+                          "--workload", "replica-selftest", "--steps", "50", "--warmup", "3"],
+                         capture_output=True, text=True, timeout=240, env=env, cwd=root)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = [json.loads(x) for x in out.stdout.splitlines() if x.startswith("{")]
+    assert len(lines) == 1                      # rank 0 alone prints
+    line = lines[0]
+    assert line["n_gpus"] == 2 and line["config"]["ranks"] == 2
+    assert line["steps"] == 50 and line["value"] > 0
