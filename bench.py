@@ -378,6 +378,10 @@ def run_b200(args, rank, world, local_rank):
                 "api": "B200SpectralSolver.step(t, dt)"},
         "roofline": roof,
     }
+    if args.workload in ("raster", "box") and not args.no_mixed:
+        mixed = _mixed_volume_comparison(args, cfg, path, dev, flush)
+        mixed["mixed_over_fp64"] = mixed["mixed_tol"]["value"] / line["value"]
+        line["comparisons"] = {"mixed_precision": mixed}
     if world == 1 and not args.no_cpu_baseline:
         v, n, el = cpu_baseline(cfg, path, budget_s=args.cpu_budget)
         line["cpu_baseline"] = {"value": v, "unit": "steps/s", "cores": os.cpu_count(),
@@ -385,6 +389,72 @@ def run_b200(args, rank, world, local_rank):
                                 "sample": f"{n} steps from t=dt of the same workload "
                                           f"({el:.1f} s), after 1 warm-up step"}
     return line
+
+
+def _mixed_volume_comparison(args, cfg, path, dev, flush):
+    """The mixed-precision form of the same single-instance step (split-BF16
+    tcgen05 contractions, FP32 modal iterates, FP64 latent source, property
+    correction, fluxes and norms) beside the FP64 plan: throughput from the
+    step graph (L2 flushed between steps, as for ``value``) at the mixed
+    Picard tolerance and, for a few steps, at the FP64 one; and the error of
+    its fields against FP64 after ``--mixed-error-steps`` steps (relative L2
+    of the volume field, peak temperature, nodal melt-pool extents)."""
+    import copy
+    import ctypes as C
+
+    import torch
+
+    from spectral_galerkin_heat_b200 import B200SpectralSolver, _lib, kernels
+    from spectral_galerkin_heat_b200.precision import compare_fields
+    stream = torch.cuda.current_stream(dev)
+
+    def timed(tol, steps):
+        s = B200SpectralSolver(None, _context(cfg, path), precision="mixed", convergence_tol=tol)
+        s.initialize()
+        W = args.warmup
+        table = s.laser_table(0.0, W + steps)
+        outs = torch.zeros((W + steps) * C.sizeof(_lib.SghStepOut), dtype=torch.uint8, device=dev)
+        s.run_table(table, outs, W, start=0)
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(steps)]
+        torch.cuda.synchronize()
+        for i in range(steps):
+            flush.fill_(i & 0xFF)
+            ev[i][0].record(stream)
+            s.run_table(table, outs, 1, start=W + i)
+            ev[i][1].record(stream)
+        torch.cuda.synchronize()
+        ms = sum(a.elapsed_time(b) for a, b in ev)
+        recs = s.decode_outs(outs.cpu().numpy().tobytes(), W + steps)[W:]
+        s.finalize()
+        st = sorted({_lib.STEP_STATUS.get(r.status, r.status) for r in recs})
+        return {"value": steps / (ms * 1e-3), "unit": "steps/s", "steps": steps, "picard_tol": tol,
+                "picard_iters_mean": float(np.mean([r.n_iter for r in recs])), "step_status": st}
+
+    out = {"mixed_tol": timed(args.mixed_tol, args.steps),
+           "fp64_tol": timed(float(cfg["simulation"].get("picard_tol", 1e-4)), min(args.steps, 3))}
+    n = args.mixed_error_steps
+    f64 = B200SpectralSolver(None, _context(cfg, path))
+    f64.initialize()
+    mix = B200SpectralSolver(None, _context(cfg, path), precision="mixed", convergence_tol=args.mixed_tol)
+    mix.initialize()
+    f64.run(0.0, n)
+    mm = mix.run(0.0, n)
+    T64 = f64.volume_temperature().cpu().numpy()
+    Tmx = f64.volume_temperature(mix.state.a).cpu().numpy()   # FP64 reconstruction of the mixed modes
+    g = f64.context.geom
+    lengths = (float(g.size.x), float(g.size.y), float(g.size.z))
+    geo = type("G", (), {"size": lengths})
+    n64 = kernels.reconstruct_temperature_DCT(f64.state.a, geo).cpu().numpy()
+    nmx = kernels.reconstruct_temperature_DCT(mix.state.a.clone(), geo).cpu().numpy()
+    cell = tuple(L / m for L, m in zip(lengths, (g.n.x, g.n.y, g.n.z)))
+    rep = compare_fields(Tmx, T64, cell, float(f64.context.mat.T_liquidus), nmx, n64, lengths)
+    out["error_vs_fp64"] = dict(rep, steps=n, mixed_picard_tol=args.mixed_tol,
+                                mixed_status_last=mix.last_status,
+                                mixed_picard_iters_last=int(mm[-1]["n_evap_iter"]))
+    f64.finalize()
+    mix.finalize()
+    return out
 
 
 def _fp64_peak(dev, n=4096, reps=10):
@@ -1164,6 +1234,11 @@ def main():
     ap.add_argument("--requests", type=int, default=1000, help="serving: saturated stream length")
     ap.add_argument("--stagger-steps", type=int, default=1100,
                     help="serving: untimed batched steps before the timed region (steady state)")
+    ap.add_argument("--mixed-tol", type=float, default=1e-5,
+                    help="raster/box: Picard tolerance of the mixed-precision comparison")
+    ap.add_argument("--mixed-error-steps", type=int, default=20,
+                    help="raster/box: steps of the mixed-vs-FP64 error report")
+    ap.add_argument("--no-mixed", action="store_true", help="raster/box: skip the mixed-precision comparison")
     ap.add_argument("--horizon-steps", type=int, default=40,
                     help="serving: steps of the one-pass accuracy check")
     ap.add_argument("--max-slots", type=int, default=16, help="serving: slots per grid class at most")

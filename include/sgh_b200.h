@@ -40,6 +40,8 @@ extern "C" {
 #define SGH_STEP_CONVERGED   0   /* Picard residual fell below the tolerance */
 #define SGH_STEP_CAPPED      1   /* hit max_picard_iter                      */
 #define SGH_STEP_NONFINITE   2   /* residual became NaN/Inf; loop stopped    */
+#define SGH_STEP_TC_TIMEOUT  3   /* mixed plan: a bounded tensor-core wait ran
+                                    out; the step's results are not trusted  */
 
 /* property-expression opcodes (postfix program, see sgh_program) */
 enum {
@@ -73,7 +75,13 @@ typedef struct {
  * (solvers/spectral.py:125-217). */
 typedef struct {
   int32_t nx, ny, nz;
-  int32_t precision;          /* SGH_PRECISION_FP64                          */
+  /* SGH_PRECISION_FP64, or SGH_PRECISION_MIXED: every DCT contraction of the
+   * step as split-BF16 products on the tensor cores (hi/lo operands, three
+   * products, FP32 accumulation) and the modal iterates rounded to FP32 at
+   * every write; the latent source across the solidus-liquidus band, the
+   * property correction, the face fluxes, the Picard norms and the
+   * coefficient tables stay FP64. */
+  int32_t precision;
   double Lx, Ly, Lz;          /* domain size, m                              */
   double dt;                  /* corrected step, s                           */
   /* material: reference constants of the propagators (MaterialParams)      */
@@ -331,11 +339,14 @@ int sgh_batch_create(const sgh_config* cfgs, int32_t n, int32_t precision, sgh_b
 /* Tile policy of a batch's kernels (no reference counterpart: the reference
  * steps one instance with library transforms). vol_unroll: z-planes whose
  * loads one round of the volume pass issues before their arithmetic (2, 4 or
- * 8; 0 = 4). The other fields are reserved and must be 0. Chosen per grid
- * mix by the autotuner; set before sgh_batch_bind. */
+ * 8; 0 = 4). vol_vec: columns per thread of the volume pass (1, 2, or 4 with
+ * FP32 modes; 0 = the widest; a width that does not divide every slot's face
+ * falls back to 1). The reserved fields must be 0. Chosen per grid mix by the
+ * autotuner; set before sgh_batch_bind. */
 typedef struct {
   int32_t vol_unroll;
-  int32_t reserved[7];
+  int32_t vol_vec;
+  int32_t reserved[6];
 } sgh_batch_policy;
 int sgh_batch_set_policy(sgh_batch* batch, const sgh_batch_policy* policy);
 int sgh_batch_destroy(sgh_batch* batch);

@@ -24,7 +24,7 @@ PICARD_HISTORY_MAX = 4096  # SGH_PICARD_HISTORY_MAX
 
 ERRORS = {-1: "SGH_ERR_INVALID", -2: "SGH_ERR_CUDA", -3: "SGH_ERR_STATE",
           -4: "SGH_ERR_UNSUPPORTED", -5: "SGH_ERR_WORKSPACE"}
-STEP_STATUS = {0: "converged", 1: "capped", 2: "nonfinite"}
+STEP_STATUS = {0: "converged", 1: "capped", 2: "nonfinite", 3: "tensor_core_timeout"}
 PRECISION = {"fp64": 0, "mixed": 1}
 BUF = {"modes": 0, "K": 1, "KK": 2, "T_prev": 3, "q_evap_old": 4, "Q_modes": 5,
        "surface": 6, "scratch": 7, "box_T_prev": 8, "box_Q_prev": 9, "box_Bx": 10,
@@ -83,7 +83,7 @@ class SghLaser(C.Structure):
 
 
 class SghBatchPolicy(C.Structure):
-    _fields_ = [("vol_unroll", C.c_int32), ("reserved", C.c_int32 * 7)]
+    _fields_ = [("vol_unroll", C.c_int32), ("vol_vec", C.c_int32), ("reserved", C.c_int32 * 6)]
 
 
 class SghStepOut(C.Structure):

@@ -164,10 +164,11 @@ def tune_table(contexts: Dict[str, object], out: Optional[str] = None, **kw) -> 
 # batched engine: the tile policy of its kernels per grid mix
 # ---------------------------------------------------------------------------
 # vol_unroll: z-planes whose loads one round of the volume pass (the
-# bandwidth-bound modal commit) issues before their arithmetic. More planes
-# keep more bytes in flight per thread; fewer keep registers, and so warps
-# per SM, up. The best trade depends on nz and on the mix of slot shapes.
-BATCH_CANDIDATES = ({"vol_unroll": 2}, {"vol_unroll": 4}, {"vol_unroll": 8})
+# bandwidth-bound modal commit) issues before their arithmetic; vol_vec:
+# columns per thread (vector width of its loads). More planes and wider
+# vectors keep more bytes in flight per thread; fewer keep registers, and so
+# warps per SM, up. The best trade depends on nz and on the mix of slot shapes.
+BATCH_CANDIDATES = tuple({"vol_unroll": u, "vol_vec": v} for v in (2, 4) for u in (2, 4, 8))
 
 
 def batch_key(cfgs, precision: str) -> str:
@@ -201,6 +202,8 @@ def tune_batch(contexts, precision: str = "mixed", steps: int = 20, warmup: int 
     from .batch import BatchSolver
     res = {}
     for pol in candidates:
+        if precision != "mixed" and pol.get("vol_vec", 0) > 2:
+            continue  # 4-wide vectors need FP32 modes
         b = BatchSolver(contexts, precision, policy=pol)
         for i in range(b.n):
             b.start(i, warmup + steps + 2, record=False)

@@ -43,7 +43,8 @@ class BatchSolver:
 
     def __init__(self, contexts: Sequence, precision: str = "fp64", device=None,
                  policy: Optional[dict] = None):
-        """``policy``: the kernels' tile policy, ``{"vol_unroll": 2 | 4 | 8}``;
+        """``policy``: the kernels' tile policy, ``{"vol_unroll": 2 | 4 | 8,
+        "vol_vec": 0 | 1 | 2 | 4}`` (0: the widest vector);
         None takes the autotuner's entry for this grid mix (``tuned.json`` or
         ``SGH_TUNE_TABLE``) and the built-in default without one."""
         import torch
@@ -68,9 +69,11 @@ class BatchSolver:
         if policy is None:
             from .autotune import lookup_batch
             policy = lookup_batch(cfgs, precision) or {}
-        self.policy = {"vol_unroll": int(policy.get("vol_unroll", 4))}
+        self.policy = {"vol_unroll": int(policy.get("vol_unroll", 4)),
+                       "vol_vec": int(policy.get("vol_vec", 0))}
         pol = _lib.SghBatchPolicy()
         pol.vol_unroll = self.policy["vol_unroll"]
+        pol.vol_vec = self.policy["vol_vec"]
         _lib.check("sgh_batch_set_policy", L.sgh_batch_set_policy(h, C.byref(pol)))
         nbytes = C.c_uint64()
         _lib.check("sgh_batch_workspace_bytes", L.sgh_batch_workspace_bytes(h, C.byref(nbytes)))

@@ -24,6 +24,7 @@
 #include <utility>
 
 #include "sgh_device.cuh"
+#include "sgh_umma.cuh"
 
 namespace sgh {
 
@@ -504,6 +505,229 @@ inline void launch_pdl(void (*kernel)(KArgs...), dim3 grid, int threads, int sme
   cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
 }
 
+// ---------------------------------------------------------------------------
+// Split-BF16 tensor-core variant (tcgen05, the mixed-precision plans). One CTA
+// of 128 threads computes out[c][k] for 128 columns c (the MMA's M; TMEM lane
+// = column) and NT outputs k of the transformed axis (the MMA's N; TMEM column
+// = output): D[c][k] = sum_n X(c, n) Mat[k][n]. Both operands are split into
+// BF16 hi + lo while the threads stage them into shared memory (K-major, no
+// swizzle, 8 x 8 core matrices), two stages deep over 32-slice chunks; per
+// 16-slice step one thread issues the three products hi.hi, hi.lo, lo.hi,
+// accumulating in FP32 in tensor memory. The epilogue reads each thread's
+// column from tensor memory and hands the values to the same epilogue
+// functors as the FP64 kernels. Every mbarrier wait is bounded: on expiry
+// the CTA sets *err, waits (bounded) for its MMAs, writes NaN partials so
+// the Picard test stops, frees its tensor memory and returns without results.
+// ---------------------------------------------------------------------------
+constexpr int AXU_THREADS = 128;
+constexpr int AXU_M = 128;  // columns per CTA
+constexpr int AXU_KC = 32;  // contraction slices per stage
+// Whether passes run on the split-BF16 tensor-core kernel (mixed-precision
+// plans), and where that kernel records an expired wait.
+inline thread_local bool g_axis_umma = false;
+inline thread_local int* g_umma_err = nullptr;
+
+template <int NT>
+__host__ __device__ constexpr int axu_stage_bytes() { return 2 * AXU_M * AXU_KC * 2 + 2 * NT * AXU_KC * 2; }
+template <int NT>
+__host__ __device__ constexpr int axu_smem_bytes() { return 2 * axu_stage_bytes<NT>() + 64; }
+// Output tile NT of a pass: the smallest of 32..256 covering Nout, narrowed
+// (more CTAs, each re-staging its columns' operands) until the pass fills the
+// SMs or NT reaches 32.
+inline int axu_nt(int Nout, int ncol) {
+  int nt = Nout <= 32 ? 32 : (Nout <= 64 ? 64 : (Nout <= 128 ? 128 : 256));
+  constexpr long kSms = 148;  // one wave at one CTA per SM
+  const long col_tiles = (ncol + AXU_M - 1) / AXU_M;
+  while (nt > 32 && col_tiles * ((Nout + nt - 1) / nt) < kSms) nt /= 2;
+  return nt;
+}
+
+template <bool CONTIG, int NT, class Epi>
+__global__ void __launch_bounds__(AXU_THREADS)
+k_axis_umma(const double* __restrict__ X, const double* __restrict__ Mat, int Nout, int N, int A, int B,
+            Epi epi, int* err) {
+  using namespace umma;
+  extern __shared__ __align__(128) char axu_sh[];
+  __shared__ double red_sh[2 * (AXU_THREADS / 32)];
+  constexpr int XB = AXU_M * AXU_KC * 2, MB = NT * AXU_KC * 2, STAGE = 2 * XB + 2 * MB;
+  constexpr uint32_t NCOLS = NT;  // 32, 64, 128 or 256 FP32 accumulator columns
+  asm volatile("griddepcontrol.wait;\n" ::: "memory");
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int ncol = A * B;
+  const int c0 = blockIdx.x * AXU_M, k0 = blockIdx.y * NT;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(axu_sh + 2 * STAGE);
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(axu_sh + 2 * STAGE + 16);
+  volatile int* okflag = reinterpret_cast<volatile int*>(axu_sh + 2 * STAGE + 32);
+  const uint32_t idesc = idesc_bf16_f32(AXU_M, NT);
+  if (warp == 0) tmem_alloc(tslot, NCOLS);
+  if (tid == 0) {
+    mbar_init(&bars[0], 1);
+    mbar_init(&bars[1], 1);
+    *okflag = 1;
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tslot;
+
+  // this thread's staged X column: CONTIG, rows warp + 4 j at slice lane;
+  // otherwise column tid at every slice of the chunk
+  size_t xcol = 0;
+  bool xok = false;
+  if (!CONTIG) {
+    const int c = c0 + tid;
+    xok = c < ncol;
+    const int cc = xok ? c : 0;
+    const int a = cc / B, b = cc - a * B;
+    xcol = (size_t)a * N * B + b;
+  }
+  const int nchunks = (N + AXU_KC - 1) / AXU_KC;
+  uint32_t phase[2] = {0u, 0u};
+  bool ok = true;
+  for (int ch = 0; ch < nchunks; ++ch) {
+    const int s = ch & 1;
+    if (ch >= 2) {  // stage s was read by the MMAs of chunk ch - 2
+      if (tid == 0 && !mbar_wait_bounded(&bars[s], phase[s])) *okflag = 0;
+      phase[s] ^= 1u;
+      __syncthreads();
+      if (!*okflag) {
+        ok = false;
+        break;
+      }
+    }
+    char* st = axu_sh + s * STAGE;
+    const int n0 = ch * AXU_KC;
+    if (CONTIG) {
+#pragma unroll 4
+      for (int j = 0; j < AXU_M / 4; ++j) {
+        const int r = warp + 4 * j, c = c0 + r, n = n0 + lane;
+        const double x = (c < ncol && n < N) ? X[(size_t)c * N + n] : 0.0;
+        __nv_bfloat16 h, l;
+        split_bf16(x, h, l);
+        const uint32_t o = core_off(r, lane, AXU_M);
+        *reinterpret_cast<__nv_bfloat16*>(st + o) = h;
+        *reinterpret_cast<__nv_bfloat16*>(st + XB + o) = l;
+      }
+    } else {
+#pragma unroll 4
+      for (int k = 0; k < AXU_KC; ++k) {
+        const int n = n0 + k;
+        const double x = (xok && n < N) ? X[xcol + (size_t)n * B] : 0.0;
+        __nv_bfloat16 h, l;
+        split_bf16(x, h, l);
+        const uint32_t o = core_off(tid, k, AXU_M);
+        *reinterpret_cast<__nv_bfloat16*>(st + o) = h;
+        *reinterpret_cast<__nv_bfloat16*>(st + XB + o) = l;
+      }
+    }
+    for (int e = tid; e < NT * AXU_KC; e += AXU_THREADS) {  // Mat rows k, slices n (n fastest)
+      const int r = e / AXU_KC, kk = e % AXU_KC;
+      const int k = k0 + r, n = n0 + kk;
+      const double x = (k < Nout && n < N) ? Mat[(size_t)k * N + n] : 0.0;
+      __nv_bfloat16 h, l;
+      split_bf16(x, h, l);
+      const uint32_t o = core_off(r, kk, NT);
+      *reinterpret_cast<__nv_bfloat16*>(st + 2 * XB + o) = h;
+      *reinterpret_cast<__nv_bfloat16*>(st + 2 * XB + MB + o) = l;
+    }
+    fence_proxy_async();
+    __syncthreads();
+    if (tid == 0) {
+      tc_fence_after();
+      const uint32_t xh = smem_u32(st), xl = xh + XB, mh = xh + 2 * XB, ml = mh + MB;
+#pragma unroll
+      for (int q = 0; q < AXU_KC / 16; ++q) {
+        const uint32_t ao = (uint32_t)(2 * q * (AXU_M / 8) * 128), bo = (uint32_t)(2 * q * (NT / 8) * 128);
+        const uint64_t dxh = smem_desc(xh + ao, (AXU_M / 8) * 128, 128);
+        const uint64_t dxl = smem_desc(xl + ao, (AXU_M / 8) * 128, 128);
+        const uint64_t dmh = smem_desc(mh + bo, (NT / 8) * 128, 128);
+        const uint64_t dml = smem_desc(ml + bo, (NT / 8) * 128, 128);
+        const uint32_t acc = (ch > 0 || q > 0) ? 1u : 0u;
+        mma_bf16(tmem, dxh, dmh, idesc, acc);
+        mma_bf16(tmem, dxh, dml, idesc, 1u);
+        mma_bf16(tmem, dxl, dmh, idesc, 1u);
+      }
+      mma_commit(&bars[s]);
+    }
+  }
+  if (ok && nchunks > 0) {  // the last commit covers every MMA before it
+    const int s = (nchunks - 1) & 1;
+    if (tid == 0 && !mbar_wait_bounded(&bars[s], phase[s])) *okflag = 0;
+    __syncthreads();
+    ok = *okflag != 0;
+  }
+  Red r;
+  if (!ok) {
+    if (tid == 0) {
+      if (err) atomicExch(err, 1);
+      for (int s = 0; s < 2; ++s) mbar_wait_bounded(&bars[s], phase[s]);  // drain, bounded
+    }
+  } else {
+    tc_fence_after();
+    const int c = c0 + warp * 32 + lane;
+    const bool cin = c < ncol;
+    const int cc = cin ? c : 0;
+    const int a = cc / B, b = cc - a * B;
+    const int base = CONTIG ? cc * Nout : a * Nout * B + b;
+#pragma unroll 1
+    for (int j0 = 0; j0 < NT; j0 += 16) {
+      float v[16];
+      tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)j0, v);
+      if (cin) {
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+          const int k = k0 + j0 + i;
+          if (k < Nout) epi(CONTIG ? base + k : base + k * B, k, b, (double)v[i], r);
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tmem_dealloc(tmem, NCOLS);
+  if (Epi::kReduce) {
+    double p0, p1;
+    if (Epi::kReduce == 1) {
+      p0 = r.s0;
+      p1 = r.s1;
+      block_sum2<AXU_THREADS>(p0, p1, red_sh);
+    } else {
+      p0 = r.mx;
+      p1 = r.s0;
+      block_max_sum<AXU_THREADS>(p0, p1, red_sh);
+    }
+    if (threadIdx.x == 0) {
+      const int blk = blockIdx.y * gridDim.x + blockIdx.x;
+      epi.partials[2 * blk] = ok ? p0 : nan("");
+      epi.partials[2 * blk + 1] = ok ? p1 : nan("");
+    }
+  }
+}
+
+template <bool CONTIG, int NT, class Epi>
+inline void launch_axis_umma_nt(const double* X, const double* Mat, int Nout, int N, int A, int B, const Epi& epi,
+                                dim3 grid, cudaStream_t st) {
+  constexpr int bytes = axu_smem_bytes<NT>();
+  static const bool attr = [] {
+    cudaFuncSetAttribute(k_axis_umma<CONTIG, NT, Epi>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    return true;
+  }();
+  (void)attr;
+  launch_pdl(k_axis_umma<CONTIG, NT, Epi>, grid, AXU_THREADS, bytes, st, X, Mat, Nout, N, A, B, epi, g_umma_err);
+}
+
+template <bool CONTIG, class Epi>
+inline void launch_axis_umma(const double* X, const double* Mat, int Nout, int N, int A, int B, const Epi& epi,
+                             dim3 grid, cudaStream_t st) {
+  switch (axu_nt(Nout, A * B)) {
+    case 32: launch_axis_umma_nt<CONTIG, 32>(X, Mat, Nout, N, A, B, epi, grid, st); break;
+    case 64: launch_axis_umma_nt<CONTIG, 64>(X, Mat, Nout, N, A, B, epi, grid, st); break;
+    case 128: launch_axis_umma_nt<CONTIG, 128>(X, Mat, Nout, N, A, B, epi, grid, st); break;
+    default: launch_axis_umma_nt<CONTIG, 256>(X, Mat, Nout, N, A, B, epi, grid, st); break;
+  }
+}
+
 // Launch shape of one pass. kind 2..5: the FP64 tensor-core kernel with a
 // BM x BN tile of 64 x 128, 64 x 64, 32 x 128, 32 x 64, when the pass is large
 // enough (see axis_shape); kind 1: the 2 x 4 thread tile when it yields
@@ -526,14 +750,23 @@ constexpr int AXM_MIN_CTAS = 16;      // smaller passes stay on the CUDA-core ke
 
 struct AxisPolicy {
   int saved;
-  bool saved_mma;
-  explicit AxisPolicy(int min_ctas, int cuda_cores_only = 0) : saved(g_axis_min_ctas), saved_mma(g_axis_mma) {
+  bool saved_mma, saved_umma;
+  int* saved_err;
+  // umma: every pass on the split-BF16 tensor-core kernel (mixed-precision
+  // plans); err: where that kernel records an expired wait (null while only
+  // sizing buffers)
+  explicit AxisPolicy(int min_ctas, int cuda_cores_only = 0, bool umma = false, int* err = nullptr)
+      : saved(g_axis_min_ctas), saved_mma(g_axis_mma), saved_umma(g_axis_umma), saved_err(g_umma_err) {
     g_axis_min_ctas = min_ctas > 0 ? min_ctas : AX_MIN_CTAS;
     g_axis_mma = cuda_cores_only == 0;
+    g_axis_umma = umma;
+    g_umma_err = err;
   }
   ~AxisPolicy() {
     g_axis_min_ctas = saved;
     g_axis_mma = saved_mma;
+    g_axis_umma = saved_umma;
+    g_umma_err = saved_err;
   }
 };
 
@@ -541,6 +774,10 @@ struct AxisPolicy {
 // buffers for exactly the kernel launch_axis() runs.
 inline AxisShape axis_shape(int Nout, int A, int B) {
   const int ncol = A * B;
+  if (g_axis_umma) {
+    const int nt = axu_nt(Nout, ncol);
+    return {true, dim3((ncol + AXU_M - 1) / AXU_M, (Nout + nt - 1) / nt), 6};
+  }
   if (g_axis_mma && Nout >= 16) {
     // the largest tile that fills one wave (a CTA per SM); else the smallest
     const int tiles[4][2] = {{64, 128}, {64, 64}, {32, 128}, {32, 64}};
@@ -597,6 +834,11 @@ template <class Epi>
 inline void launch_axis(const double* X, const double* Mat, int Nout, int N, int A, int B,
                         const Epi& epi, cudaStream_t st) {
   const AxisShape sh = axis_shape(Nout, A, B);
+  if (sh.kind == 6) {
+    if (B == 1) launch_axis_umma<true>(X, Mat, Nout, N, A, B, epi, sh.grid, st);
+    else launch_axis_umma<false>(X, Mat, Nout, N, A, B, epi, sh.grid, st);
+    return;
+  }
   if (sh.kind >= 2) {
     if (B == 1) launch_axis_mma_kind<true>(sh.kind, X, Mat, Nout, N, A, B, epi, sh.grid, st);
     else launch_axis_mma_kind<false>(sh.kind, X, Mat, Nout, N, A, B, epi, sh.grid, st);
@@ -706,11 +948,11 @@ struct EpiTrial {
     if (RELAX) {
       const double old = a_it[i];
       const double res = t - old;
-      a_it[i] = res * omega + old;
+      a_it[i] = st_mode(res * omega + old, P.round32);
       r.s0 = fma(res, res, r.s0);
       r.s1 = fma(old, old, r.s1);
     } else {
-      a_trial[i] = t;
+      a_trial[i] = st_mode(t, P.round32);
     }
   }
 };
@@ -730,7 +972,7 @@ struct EpiRelax {
     const double raw = ld_in(a_trial + i) + ld_in(KK + i) * c;
     const double old = a_it[i];
     const double res = raw - old;
-    a_it[i] = res * P.omega + old;
+    a_it[i] = st_mode(res * P.omega + old, P.round32);
     r.s0 = fma(res, res, r.s0);
     r.s1 = fma(old, old, r.s1);
   }

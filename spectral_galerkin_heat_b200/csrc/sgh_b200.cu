@@ -364,12 +364,12 @@ k_init_modes(const DevParams* __restrict__ P, const Ctrl* __restrict__ ctrl, dou
   if (i >= P->V) return;
   const int S = P->S;
   const int z = i / S, yx = i - z * S;
-  const double ak = a_it[i] * K[i];
+  const double ak = st_mode(a_it[i] * K[i], P->round32);
   aK[i] = ak;
   const double kk = KK[i];
   double t = ak + kk * Ct[z] * S_top[yx];
   if (ctrl->have_qprev || P->box) t += kk * Qm[i];
-  a_it[i] = t;
+  a_it[i] = st_mode(t, P->round32);
 }
 
 // a += KK w[p] S[y,x]  (add_bottom_surface_source, spectral_cpu_kernels.py:105-113)
@@ -380,7 +380,7 @@ k_add_face(const DevParams* __restrict__ P, double* a, const double* __restrict_
   if (i >= P->V) return;
   const int S = P->S;
   const int z = i / S, yx = i - z * S;
-  a[i] += KK[i] * w[z] * Sf[yx];
+  a[i] = st_mode(a[i] + KK[i] * w[z] * Sf[yx], P->round32);
 }
 
 // Trial modes without latent heat (property correction follows).
@@ -395,7 +395,7 @@ k_trial(const DevParams* __restrict__ P, const double* __restrict__ aK, const do
   const double kk = KK[i];
   double t = aK[i] + kk * Ct[z] * S_top[yx];
   if (S_bot) t += kk * Cb[z] * S_bot[yx];
-  a_trial[i] = t;
+  a_trial[i] = st_mode(t, P->round32);
 }
 
 // Trial modes and relaxation in one pass when there is neither latent heat nor
@@ -417,7 +417,7 @@ k_trial_relax(const DevParams* __restrict__ P, const double* __restrict__ aK,
     if (S_bot) t += kk * Cb[z] * S_bot[yx];
     const double old = a_it[i];
     const double res = t - old;
-    a_it[i] = res * om + old;
+    a_it[i] = st_mode(res * om + old, P->round32);
     s0 = fma(res, res, s0);
     s1 = fma(old, old, s1);
   }
@@ -528,7 +528,7 @@ k_commit(const DevParams* __restrict__ P, Ctrl* ctrl, const double* __restrict__
     o.picard_rel_err = ctrl->rel_err;
     o.n_iter = ctrl->iter;
     o.converged = ctrl->status == SGH_STEP_CONVERGED ? 1 : 0;
-    o.status = ctrl->status;
+    o.status = ctrl->umma_err ? SGH_STEP_TC_TIMEOUT : ctrl->status;
     int flags = 0;
     if (P->box && ctrl->iter > 0) {
       // truncation check (solvers/spectral.py:545-586): a face of the box whose
@@ -723,6 +723,11 @@ struct sgh_plan {
 };
 
 namespace {
+
+// Mixed-precision plan: every contraction on the split-BF16 tensor-core
+// kernel, modal iterates rounded to FP32.
+bool plan_mixed(const sgh_plan* p) { return p && p->cfg.precision == SGH_PRECISION_MIXED; }
+int* umma_err_of(const sgh_plan* p) { return (p && p->ws) ? &p->ctrl()->umma_err : nullptr; }
 
 int check_program(const sgh_program& p, const char* name) {
   if (p.n_ops < 1 || p.n_ops > SGH_MAX_PROGRAM || p.n_consts < 0 || p.n_consts > SGH_MAX_CONSTS)
@@ -1283,11 +1288,12 @@ int sgh_plan_create(const sgh_config* cfg, sgh_plan** out) {
   const sgh_config& c = *cfg;
   if (c.axis_min_ctas < 0) return fail(SGH_ERR_INVALID, "axis_min_ctas must be >= 0");
   if (c.axis_cuda_cores != 0 && c.axis_cuda_cores != 1) return fail(SGH_ERR_INVALID, "axis_cuda_cores must be 0 or 1");
-  AxisPolicy policy(c.axis_min_ctas, c.axis_cuda_cores);
+  AxisPolicy policy(c.axis_min_ctas, c.axis_cuda_cores, c.precision == SGH_PRECISION_MIXED);
   if (c.nx < 2 || c.ny < 2 || c.nz < 2) return fail(SGH_ERR_INVALID, "every axis needs at least 2 modes");
   if (c.nx > 4096 || c.ny > 4096 || c.nz > 4096) return fail(SGH_ERR_INVALID, "an axis exceeds 4096 modes");
   if ((long long)c.nx * c.ny * c.nz > (1LL << 28)) return fail(SGH_ERR_INVALID, "grid exceeds 2^28 modes");
-  if (c.precision != SGH_PRECISION_FP64) return fail(SGH_ERR_UNSUPPORTED, "only SGH_PRECISION_FP64 is built");
+  if (c.precision != SGH_PRECISION_FP64 && c.precision != SGH_PRECISION_MIXED)
+    return fail(SGH_ERR_INVALID, "precision must be SGH_PRECISION_FP64 or SGH_PRECISION_MIXED");
   if (!(c.Lx > 0 && c.Ly > 0 && c.Lz > 0 && c.dt > 0))
     return fail(SGH_ERR_INVALID, "domain size and dt must be positive");
   if (!(c.r_x > 0 && c.r_y > 0 && c.area_factor > 0 && c.order > 0))
@@ -1322,6 +1328,7 @@ int sgh_plan_create(const sgh_config* cfg, sgh_plan** out) {
   p->cfg = c;
   DevParams& h = p->hp;
   std::memset(&h, 0, sizeof(h));
+  h.round32 = c.precision == SGH_PRECISION_MIXED ? 1 : 0;
   h.nx = c.nx; h.ny = c.ny; h.nz = c.nz;
   h.S = c.nx * c.ny;
   h.V = h.S * c.nz;
@@ -1493,7 +1500,7 @@ int sgh_plan_workspace_bytes(const sgh_plan* p, uint64_t* bytes) {
 }
 
 int sgh_plan_bind(sgh_plan* p, void* workspace, uint64_t bytes, void* stream) {
-  AxisPolicy policy(p ? p->cfg.axis_min_ctas : 0, p ? p->cfg.axis_cuda_cores : 0);
+  AxisPolicy policy(p ? p->cfg.axis_min_ctas : 0, p ? p->cfg.axis_cuda_cores : 0, plan_mixed(p), umma_err_of(p));
   if (!p || !workspace) return fail(SGH_ERR_INVALID, "null argument");
   if (p->bound) return fail(SGH_ERR_STATE, "plan is already bound");
   if (bytes < p->ws_need) return fail(SGH_ERR_WORKSPACE, "workspace is smaller than sgh_plan_workspace_bytes()");
@@ -1501,6 +1508,7 @@ int sgh_plan_bind(sgh_plan* p, void* workspace, uint64_t bytes, void* stream) {
     return fail(SGH_ERR_WORKSPACE, "workspace must be 256-byte aligned");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   p->ws = static_cast<char*>(workspace);
+  g_umma_err = umma_err_of(p);  // the policy above was made before the workspace existed
   const DevParams& h = p->hp;
   SGH_CK(cudaMemcpyAsync(p->P(), &h, sizeof(DevParams), cudaMemcpyHostToDevice, s));
   SGH_CK(cudaMemsetAsync(p->ctrl(), 0, sizeof(Ctrl), s));
@@ -1624,7 +1632,7 @@ int sgh_step(sgh_plan* p, const sgh_laser* laser, sgh_step_out* out, void* strea
 }
 
 int sgh_step_eager(sgh_plan* p, const sgh_laser* laser, sgh_step_out* out, void* stream) {
-  AxisPolicy policy(p ? p->cfg.axis_min_ctas : 0, p ? p->cfg.axis_cuda_cores : 0);
+  AxisPolicy policy(p ? p->cfg.axis_min_ctas : 0, p ? p->cfg.axis_cuda_cores : 0, plan_mixed(p), umma_err_of(p));
   if (!p || !laser) return fail(SGH_ERR_INVALID, "null argument");
   if (!p->bound) return fail(SGH_ERR_STATE, "plan is not bound");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -1658,7 +1666,7 @@ int sgh_run(sgh_plan* p, const sgh_laser* lasers_dev, int32_t n_steps, sgh_step_
 }
 
 int sgh_dct3d(sgh_plan* p, int32_t kind, const double* in, double* out, void* stream) {
-  AxisPolicy policy(p ? p->cfg.axis_min_ctas : 0, p ? p->cfg.axis_cuda_cores : 0);
+  AxisPolicy policy(p ? p->cfg.axis_min_ctas : 0, p ? p->cfg.axis_cuda_cores : 0, plan_mixed(p), umma_err_of(p));
   if (!p || !in || !out) return fail(SGH_ERR_INVALID, "null argument");
   if (!p->bound) return fail(SGH_ERR_STATE, "plan is not bound");
   if (kind != 2 && kind != 3) return fail(SGH_ERR_INVALID, "kind must be 2 (DCT_II) or 3 (IDCT_II)");
@@ -1669,7 +1677,7 @@ int sgh_dct3d(sgh_plan* p, int32_t kind, const double* in, double* out, void* st
 }
 
 int sgh_surface_temperature(sgh_plan* p, const double* modes, int32_t top, double* out, void* stream) {
-  AxisPolicy policy(p ? p->cfg.axis_min_ctas : 0, p ? p->cfg.axis_cuda_cores : 0);
+  AxisPolicy policy(p ? p->cfg.axis_min_ctas : 0, p ? p->cfg.axis_cuda_cores : 0, plan_mixed(p), umma_err_of(p));
   if (!p || !modes || !out) return fail(SGH_ERR_INVALID, "null argument");
   if (!p->bound) return fail(SGH_ERR_STATE, "plan is not bound");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -1679,7 +1687,7 @@ int sgh_surface_temperature(sgh_plan* p, const double* modes, int32_t top, doubl
 }
 
 int sgh_project_volume(sgh_plan* p, const double* field, double* modes, void* stream) {
-  AxisPolicy policy(p ? p->cfg.axis_min_ctas : 0, p ? p->cfg.axis_cuda_cores : 0);
+  AxisPolicy policy(p ? p->cfg.axis_min_ctas : 0, p ? p->cfg.axis_cuda_cores : 0, plan_mixed(p), umma_err_of(p));
   if (!p || !field || !modes) return fail(SGH_ERR_INVALID, "null argument");
   if (!p->bound) return fail(SGH_ERR_STATE, "plan is not bound");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -1689,7 +1697,7 @@ int sgh_project_volume(sgh_plan* p, const double* field, double* modes, void* st
 }
 
 int sgh_reconstruct_volume(sgh_plan* p, const double* modes, double* field, void* stream) {
-  AxisPolicy policy(p ? p->cfg.axis_min_ctas : 0, p ? p->cfg.axis_cuda_cores : 0);
+  AxisPolicy policy(p ? p->cfg.axis_min_ctas : 0, p ? p->cfg.axis_cuda_cores : 0, plan_mixed(p), umma_err_of(p));
   if (!p || !field || !modes) return fail(SGH_ERR_INVALID, "null argument");
   if (!p->bound) return fail(SGH_ERR_STATE, "plan is not bound");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -1763,7 +1771,7 @@ int sgh_box_window(sgh_plan* p, int32_t* i0, void* stream) {
 }
 
 int sgh_box_temperature(sgh_plan* p, const double* modes, double* out, void* stream) {
-  AxisPolicy policy(p ? p->cfg.axis_min_ctas : 0, p ? p->cfg.axis_cuda_cores : 0);
+  AxisPolicy policy(p ? p->cfg.axis_min_ctas : 0, p ? p->cfg.axis_cuda_cores : 0, plan_mixed(p), umma_err_of(p));
   if (!p || !modes || !out) return fail(SGH_ERR_INVALID, "null argument");
   if (!p->bound) return fail(SGH_ERR_STATE, "plan is not bound");
   if (!p->hp.box) return fail(SGH_ERR_STATE, "plan is not in box mode");
@@ -1775,7 +1783,7 @@ int sgh_box_temperature(sgh_plan* p, const double* modes, double* out, void* str
 }
 
 int sgh_box_project(sgh_plan* p, const double* field_box, double* modes, void* stream) {
-  AxisPolicy policy(p ? p->cfg.axis_min_ctas : 0, p ? p->cfg.axis_cuda_cores : 0);
+  AxisPolicy policy(p ? p->cfg.axis_min_ctas : 0, p ? p->cfg.axis_cuda_cores : 0, plan_mixed(p), umma_err_of(p));
   if (!p || !field_box || !modes) return fail(SGH_ERR_INVALID, "null argument");
   if (!p->bound) return fail(SGH_ERR_STATE, "plan is not bound");
   if (!p->hp.box) return fail(SGH_ERR_STATE, "plan is not in box mode");

@@ -331,12 +331,22 @@ __global__ void __launch_bounds__(CT) kb_begin(BView v, cudaGraphConditionalHand
 }
 
 // q_las, P_laser partials and q_net = q_las - shift(q_evap_old) per slot
-// (solvers/spectral.py:273-306).
+// (solvers/spectral.py:273-306). The Gaussian beam factorises,
+// exp(-2 (ux^2 + uy^2)) = exp(-2 ux^2) exp(-2 uy^2), so a block first tabulates
+// the column factors of its slot and the row factors of the rows it covers in
+// shared memory (one exp per column and per row instead of one per element;
+// a few ulps from the unfactorised form); other profiles evaluate the flux
+// per element.
+constexpr int FB_MAX_COLS = 1024;  // column factors tabulated (wider faces: per element)
+constexpr int FB_MAX_ROWS = 160;   // row factors of one block (RB / 16 + 2 rows at nx >= 16)
+
 __global__ void __launch_bounds__(BT)
 kb_face_begin(BView v, double* q_las, double* q_net, const double* q_evold, double* part_las) {
   // RB elements per block (RPT per thread, consecutive across the block per
   // round); the four shift taps of U elements are gathered before their use
   __shared__ double sh[2 * (BT / 32)];
+  __shared__ double fx[FB_MAX_COLS];
+  __shared__ double fy[FB_MAX_ROWS];
   const int b = blockIdx.x;
   const int s = v.rblk_slot[b];
   const BSlot& sl = v.slot[s];
@@ -346,17 +356,34 @@ kb_face_begin(BView v, double* q_las, double* q_net, const double* q_evold, doub
   const double* f = q_evold + sl.face;
   const double I0 = st.I0, lx = st.laser.x, ly = st.laser.y, sx = st.shift_x, sy = st.shift_y;
   const int i0 = (b - sl.rblk0) * RB;
+  const int y_lo = i0 / nx, y_hi = min(ny - 1, (i0 + RB - 1) / nx);
+  const bool table = !sl.cell_integrated && sl.order == 2.0 && nx <= FB_MAX_COLS &&
+                     (y_hi - y_lo + 1) <= FB_MAX_ROWS;
+  if (table) {
+    for (int x = threadIdx.x; x < nx; x += BT) {
+      const double ux = (((double)x + 0.5) * sl.dx - lx) / sl.r_x;
+      fx[x] = exp(-2.0 * (ux * ux));
+    }
+    for (int y = y_lo + (int)threadIdx.x; y <= y_hi; y += BT) {
+      const double uy = (((double)y + 0.5) * sl.dy - ly) / sl.r_y;
+      fy[y - y_lo] = exp(-2.0 * (uy * uy));
+    }
+    __syncthreads();
+  }
   double sum = 0.0, dummy = 0.0;
   constexpr int U = 4;
 #pragma unroll 1
   for (int u0 = 0; u0 < RPT; u0 += U) {
     double g[U][4], wy0[U], wy1[U], wx0[U], wx1[U];
+    int xs[U], ys[U];
     bool ok[U], in[U];
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       const int i = i0 + (u0 + u) * BT + threadIdx.x;
       ok[u] = i < sl.S;
       const int y = ok[u] ? i / nx : 0, x = ok[u] ? i - y * nx : 0;
+      xs[u] = x;
+      ys[u] = y;
       const ShiftTap ty = shift_tap(y, ny, sy);
       const ShiftTap tx = shift_tap(x, nx, sx);
       in[u] = ok[u] && ty.in && tx.in;
@@ -371,9 +398,14 @@ kb_face_begin(BView v, double* q_las, double* q_net, const double* q_evold, doub
       const int i = i0 + (u0 + u) * BT + threadIdx.x;
       double qn = 0.0;
       if (ok[u]) {
-        const int y = i / nx, x = i - y * nx;
-        const double xc = ((double)x + 0.5) * sl.dx, yc = ((double)y + 0.5) * sl.dy;
-        const double q = laser_flux(sl, I0, lx, ly, xc, yc);
+        const int y = ys[u], x = xs[u];
+        double q;
+        if (table) {
+          q = I0 * (fx[x] * fy[y - y_lo]);
+        } else {
+          const double xc = ((double)x + 0.5) * sl.dx, yc = ((double)y + 0.5) * sl.dy;
+          q = laser_flux(sl, I0, lx, ly, xc, yc);
+        }
         q_las[sl.face + i] = q;
         sum += q;
         // the bilinear shift (spectral_cpu_kernels.py:328-371), zero outside the grid
@@ -1001,11 +1033,14 @@ struct VecOf { using T = R; };
 template <>
 struct VecOf<float, 4> { using T = float4; };
 template <>
+struct VecOf<float, 2> { using T = float2; };
+template <>
 struct VecOf<double, 2> { using T = double2; };
 
 template <class R, int VEC>
 __device__ __forceinline__ void vload(const R* p, R (&o)[VEC]) {
   using T = typename VecOf<R, VEC>::T;
+  static_assert(sizeof(T) == VEC * sizeof(R), "no vector type of this width");
   const T t = *reinterpret_cast<const T*>(p);
 #pragma unroll
   for (int c = 0; c < VEC; ++c) o[c] = reinterpret_cast<const R*>(&t)[c];
@@ -1013,18 +1048,26 @@ __device__ __forceinline__ void vload(const R* p, R (&o)[VEC]) {
 template <class R, int VEC>
 __device__ __forceinline__ void vstore(R* p, const R (&o)[VEC]) {
   using T = typename VecOf<R, VEC>::T;
+  static_assert(sizeof(T) == VEC * sizeof(R), "no vector type of this width");
   T t;
 #pragma unroll
   for (int c = 0; c < VEC; ++c) reinterpret_cast<R*>(&t)[c] = o[c];
   *reinterpret_cast<T*>(p) = t;
 }
 
+// Mixed precision (FP32 modes): the volume pass works in FP32 registers,
+// except the face sums and the norm. Per mode: K = Ex Ey Ez and KK (mode_kk)
+// in FP32 from the FP64-derived 1-D tables, a <- K a + KK Ct sigma as two
+// FP32 products and a fused add (relative rounding a few 1e-7, the order of
+// the FP32 storage of a), and the face sums Zt, Yt and the norm partial
+// accumulated in FP64. No FP64 arithmetic or conversion sits on the per-mode
+// path except the three accumulations and the widening of their two FP32
+// inputs, so the pass stays close to its 8 bytes per mode of HBM traffic.
+// FP64 modes: K and KK read from the volume arenas, everything in FP64.
 template <class R, int VEC, bool COMMIT, int U>
-__global__ void __launch_bounds__(BT / VEC)
+__global__ void __launch_bounds__(BT / VEC, (sizeof(R) == 4 ? 3 : 2) * VEC)
 kb_volume(BView v, R* a, const R* K, const R* KK, const double* sigma, double* Zt, double* Yt,
           double* part_n1) {
-  // FP32 modes (mixed precision): K and KK formed from the 1-D tables; FP64
-  // modes: K and KK read from the volume arenas
   constexpr bool TAB = sizeof(R) == 4;
   constexpr int NT = BT / VEC;
   __shared__ double sh[2 * (NT / 32)];
@@ -1043,15 +1086,15 @@ kb_volume(BView v, R* a, const R* K, const R* KK, const double* sigma, double* Z
     const double* dz = ez + nsum;
     const double* lz = ez + 2 * nsum;
     const double dt_rc = sl.dt / (sl.rho * sl.cp);
-    double sg[VEC], exy[VEC], zt[VEC], yt[VEC];
-    float exy32[VEC], dxy32[VEC], lxy32[VEC];
+    double zt[VEC], yt[VEC], sg[VEC];
+    float sg32[VEC], exy32[VEC], dxy32[VEC], lxy32[VEC];
 #pragma unroll
     for (int c = 0; c < VEC; ++c) {
       const int i = i0 + c;
       const int ix = i % sl.nx, iy = sl.nx + i / sl.nx;
       sg[c] = COMMIT ? sigma[sl.face + i] : 0.0;
-      exy[c] = TAB ? E[ix] * E[iy] : 0.0;
-      exy32[c] = (float)exy[c];
+      sg32[c] = (float)sg[c];
+      exy32[c] = TAB ? (float)(E[ix] * E[iy]) : 0.0f;
       dxy32[c] = TAB ? (float)(E[nsum + ix] + E[ix] * E[nsum + iy]) : 0.0f;
       lxy32[c] = TAB ? (float)(E[2 * nsum + ix] + E[2 * nsum + iy]) : 0.0f;
       zt[c] = 0.0;
@@ -1077,17 +1120,35 @@ kb_volume(BView v, R* a, const R* K, const R* KK, const double* sigma, double* Z
         const int p = p0 + u;
         if (p < sl.nz) {
           const double cp = ct[p];
-          const double ezp = TAB ? ez[p] : 0.0;
-          const float dzp = TAB ? (float)dz[p] : 0.0f, lzp = TAB ? (float)lz[p] : 0.0f;
+          if (TAB) {
+            const float cp32 = (float)cp, ez32 = (float)ez[p];
+            const float dz32 = (float)dz[p], lz32 = (float)lz[p];
 #pragma unroll
-          for (int c = 0; c < VEC; ++c) {
-            const double kv = TAB ? exy[c] * ezp : (double)kvv[u][c];
-            const double kk = TAB ? mode_kk(dxy32[c], exy32[c], dzp, lxy32[c], lzp, dt_rc) : (double)kkv[u][c];
-            if (COMMIT) av[u][c] = (R)((double)av[u][c] * kv + kk * (cp * sg[c]));
-            const double ak = (double)av[u][c] * kv;
-            zt[c] = fma(cp, ak, zt[c]);
-            yt[c] = fma(ak * kk, cp, yt[c]);
-            n1 = fma(ak, ak, n1);
+            for (int c = 0; c < VEC; ++c) {
+              const float kv = exy32[c] * ez32;
+              const float num = fmaf(exy32[c], dz32, dxy32[c]);
+              const float den = lxy32[c] + lz32;
+              const float kk = den > 0.0f ? __fdividef(num, den) : (float)dt_rc;
+              float x = (float)av[u][c];
+              if (COMMIT) x = fmaf(x, kv, kk * (cp32 * sg32[c]));
+              av[u][c] = (R)x;
+              const float ak = x * kv;
+              const double ak64 = (double)ak, akk64 = (double)(ak * kk);
+              zt[c] = fma(cp, ak64, zt[c]);
+              yt[c] = fma(akk64, cp, yt[c]);
+              n1 = fma(ak64, ak64, n1);
+            }
+          } else {
+#pragma unroll
+            for (int c = 0; c < VEC; ++c) {
+              const double kv = (double)kvv[u][c];
+              const double kk = (double)kkv[u][c];
+              if (COMMIT) av[u][c] = (R)((double)av[u][c] * kv + kk * (cp * sg[c]));
+              const double ak = (double)av[u][c] * kv;
+              zt[c] = fma(cp, ak, zt[c]);
+              yt[c] = fma(ak * kk, cp, yt[c]);
+              n1 = fma(ak, ak, n1);
+            }
           }
           if (COMMIT) vstore<R, VEC>(a + sl.vol + (long long)p * sl.S + i0, av[u]);
         }
@@ -1251,23 +1312,24 @@ template <class R, bool COMMIT>
 void launch_volume(sgh_batch* B, cudaStream_t s, R* a, const R* K, const R* KK) {
   const BView v = B->view();
   double *sg = B->d(B->o_sigma), *zt = B->d(B->o_Zt), *yt = B->d(B->o_Yt), *pn = B->d(B->o_pn1);
-  constexpr int VW = sizeof(R) == 4 ? 4 : 2;
   auto go = [&](auto vec, auto u) {
     constexpr int V_ = decltype(vec)::value, U_ = decltype(u)::value;
     kb_volume<R, V_, COMMIT, U_><<<B->tot_blk, BT / V_, 0, s>>>(v, a, K, KK, sg, zt, yt, pn);
   };
-  using I1 = std::integral_constant<int, 1>;
-  using IV = std::integral_constant<int, VW>;
-  const int u = B->vol_unroll;
-  if (B->vec == VW) {
-    if (u == 2) go(IV{}, std::integral_constant<int, 2>{});
-    else if (u == 8) go(IV{}, std::integral_constant<int, 8>{});
-    else go(IV{}, std::integral_constant<int, 4>{});
-  } else {
-    if (u == 2) go(I1{}, std::integral_constant<int, 2>{});
-    else if (u == 8) go(I1{}, std::integral_constant<int, 8>{});
-    else go(I1{}, std::integral_constant<int, 4>{});
+  auto with_u = [&](auto vec) {
+    const int u = B->vol_unroll;
+    if (u == 2) go(vec, std::integral_constant<int, 2>{});
+    else if (u == 8) go(vec, std::integral_constant<int, 8>{});
+    else go(vec, std::integral_constant<int, 4>{});
+  };
+  if constexpr (sizeof(R) == 4) {
+    if (B->vec == 4) {
+      with_u(std::integral_constant<int, 4>{});
+      return;
+    }
   }
+  if (B->vec == 2) with_u(std::integral_constant<int, 2>{});
+  else with_u(std::integral_constant<int, 1>{});
 }
 
 template <class R>
@@ -1585,7 +1647,16 @@ int sgh_batch_set_policy(sgh_batch* B, const sgh_batch_policy* pol) {
   if (B->bound) return bfail(SGH_ERR_STATE, "set the policy before sgh_batch_bind (the graphs are captured there)");
   const int u = pol->vol_unroll ? pol->vol_unroll : 4;
   if (u != 2 && u != 4 && u != 8) return bfail(SGH_ERR_INVALID, "vol_unroll must be 2, 4 or 8");
+  const int vmax = B->precision == SGH_PRECISION_MIXED ? 4 : 2;
+  const int vw = pol->vol_vec ? pol->vol_vec : vmax;
+  if (vw != 1 && vw != 2 && vw != 4) return bfail(SGH_ERR_INVALID, "vol_vec must be 1, 2 or 4");
+  if (vw > vmax) return bfail(SGH_ERR_INVALID, "vol_vec 4 needs FP32 modes (mixed precision)");
+  for (int i = 0; i < 6; ++i)
+    if (pol->reserved[i]) return bfail(SGH_ERR_INVALID, "reserved policy fields must be 0");
+  bool ok = true;  // every slot's face a multiple of the vector width (offsets are padded to 4)
+  for (const BSlot& sl : B->slots) ok = ok && (sl.S % vw == 0);
   B->vol_unroll = u;
+  B->vec = ok ? vw : 1;
   return SGH_OK;
 }
 

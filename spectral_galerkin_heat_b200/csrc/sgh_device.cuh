@@ -24,7 +24,7 @@ struct DevParams {
   // xb, yb, zb (nx_box, ny_box, nz_box), fine-grid totals fx, fy, fz
   // (n_fine_totals), Nb = zb yb xb
   int box, xb, yb, zb, fx, fy, fz, Nb;
-  int pad_i;
+  int round32;  // mixed-precision plan: modal iterates rounded to FP32 at every write
   double Lx, Ly, Lz, dx, dy, dz, inv_dx, inv_dy, inv_dz, dt, inv_dt;
   double dct_scale, recon_scale, sqrt_dV, n_elements;
   double kbar, abar, T0, h_top, h_bottom;
@@ -61,7 +61,8 @@ struct Ctrl {
   // Picard history of the current step: (rms of the residual, relative
   // residual) per iteration, the first hist_cap iterations
   double* hist;
-  int hist_cap, pad_h;
+  int hist_cap;
+  int umma_err;  // a split-BF16 tensor-core wait ran out (mixed-precision plans)
 };
 
 // ---------------------------------------------------------------------------
@@ -132,8 +133,12 @@ __device__ __forceinline__ double ld_in(const double* p) {
 // alias, so the compiler keeps them in registers instead of reloading
 // DevParams after every store. Non-affine property programs are read
 // through `full`.
+// A modal value as a plan stores it: FP64, or rounded to FP32 in
+// mixed-precision plans (the FP32 modal state of the mixed form).
+__device__ __forceinline__ double st_mode(double x, int round32) { return round32 ? (double)(float)x : x; }
+
 struct PointPhys {
-  int nz, S, latent_model, degenerate_band, k_constant, has_top_conv;
+  int nz, S, latent_model, degenerate_band, k_constant, has_top_conv, round32;
   int affine[P_COUNT];
   double sqrt_dV, omega, T_solidus, T_liquidus, band_inv, latent_factor, L_f, inv_dt;
   double kbar, abar, T0, h_top, T_boil, evap_f1, evap_f2, recon_scale;
@@ -145,7 +150,7 @@ struct PointPhys {
 inline PointPhys point_phys(const DevParams& h, const DevParams* dev) {
   PointPhys q;
   q.nz = h.nz; q.S = h.S; q.latent_model = h.latent_model; q.degenerate_band = h.degenerate_band;
-  q.k_constant = h.k_constant; q.has_top_conv = h.has_top_conv;
+  q.k_constant = h.k_constant; q.has_top_conv = h.has_top_conv; q.round32 = h.round32;
   for (int i = 0; i < P_COUNT; ++i) {
     q.affine[i] = h.affine[i];
     q.aff_a[i] = h.aff_a[i];

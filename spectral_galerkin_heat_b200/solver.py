@@ -231,11 +231,21 @@ class B200FineMesh:
 
 
 class B200SpectralSolver(HeatSolver):
-    """Spectral-Galerkin heat step on one B200 (FP64, grid or box mode)."""
+    """Spectral-Galerkin heat step on one B200 (grid or box mode).
+
+    ``precision="fp64"`` (default) is the plain form, FP64 throughout.
+    ``precision="mixed"`` runs every DCT contraction of the step as split-BF16
+    products on the tensor cores (tcgen05, FP32 accumulation) and keeps the
+    modal iterates rounded to FP32; the latent source across the
+    solidus-liquidus band, the property correction, the face fluxes, the
+    Picard norms and the coefficient tables stay FP64."""
 
     def __init__(self, backend=None, context=None, *, mixing_omega=None,
                  convergence_tol=None, max_picard_iter=None, device=None, axis_min_ctas=None,
-                 axis_cuda_cores=None):
+                 axis_cuda_cores=None, precision: str = "fp64"):
+        if precision not in _lib.PRECISION:
+            raise ValueError(f"precision must be one of {sorted(_lib.PRECISION)}")
+        self.precision = precision
         self.backend = backend
         self.context = context
         # tile policy of the axis passes: explicit, else the autotuner's table, else default
@@ -288,6 +298,7 @@ class B200SpectralSolver(HeatSolver):
         self._resolve_picard_params(np.float64)
         cfg = make_config(ctx, float(self.mixing_omega), float(self.convergence_tol),
                           self.max_picard_iter)
+        cfg.precision = _lib.PRECISION[self.precision]
         policy = self.axis_min_ctas
         if policy is None:
             from .autotune import lookup
@@ -520,6 +531,21 @@ class B200SpectralSolver(HeatSolver):
         out = torch.empty(self.state.shape, dtype=torch.float64, device=self.state.workspace.device)
         _lib.check("sgh_reconstruct_volume", _lib.lib().sgh_reconstruct_volume(
             self._plan, C.c_void_p(a.data_ptr()), C.c_void_p(out.data_ptr()),
+            C.c_void_p(self.state.stream.cuda_stream)))
+        return out
+
+    def dct3d(self, x, kind: int = 2):
+        """Orthonormal 3-D DCT-II (``kind=2``) or DCT-III (``kind=3``) of a
+        field of the plan's shape with the plan's own contractions (FP64, or
+        split-BF16 on the tensor cores in a mixed plan); a new tensor."""
+        self._require()
+        torch = _torch()
+        x = torch.as_tensor(x, dtype=torch.float64, device=self.state.workspace.device).contiguous()
+        if tuple(x.shape) != self.state.shape:
+            raise ValueError(f"field shape {tuple(x.shape)} != plan shape {self.state.shape}")
+        out = torch.empty_like(x)
+        _lib.check("sgh_dct3d", _lib.lib().sgh_dct3d(
+            self._plan, int(kind), C.c_void_p(x.data_ptr()), C.c_void_p(out.data_ptr()),
             C.c_void_p(self.state.stream.cuda_stream)))
         return out
 

@@ -182,6 +182,8 @@ def test_every_tile_policy_gives_the_same_result(precision):
     ctxs = [_ctx(*sh, seed=10 + i, steps=steps) for i, sh in enumerate(SHAPES)]
     modes = []
     for pol in BATCH_CANDIDATES:
+        if precision == "fp64" and pol["vol_vec"] > 2:
+            continue  # 4-wide vectors need FP32 modes
         b = BatchSolver(ctxs, precision, policy=pol)
         assert b.policy == pol
         for i in range(len(ctxs)):
