@@ -931,10 +931,12 @@ def run_profile(args):
         print(json.dumps({"profile": args.profile, "precision": args.precision, "slots": eng.memory["slots"],
                           "active_modes": eng.batch.active_modes(), "workspace_gb": eng.batch.workspace_bytes / 1e9}))
         eng.close()
-    elif args.profile in ("raster-step", "box-step"):
+    elif args.profile in ("raster-step", "box-step", "raster-step-mixed"):
         from spectral_galerkin_heat_b200 import B200SpectralSolver
         cfg, path, desc = _workload(args.profile.split("-")[0], seed=0)
-        s = B200SpectralSolver(None, _context(cfg, path))
+        mixed = args.profile.endswith("-mixed")
+        s = B200SpectralSolver(None, _context(cfg, path), precision="mixed" if mixed else "fp64",
+                               convergence_tol=args.mixed_tol if mixed else None)
         s.initialize()
         dt = s.context.num.dt
         for i in range(args.warmup + args.steps):
@@ -1246,7 +1248,8 @@ def main():
     ap.add_argument("--plain-steps", type=int, default=300)
     ap.add_argument("--cpu-steps-per-request", type=int, default=20)
     ap.add_argument("--accuracy-steps", type=int, default=100)
-    ap.add_argument("--profile", choices=["serving-step", "raster-step", "box-step"], default=None,
+    ap.add_argument("--profile", choices=["serving-step", "raster-step", "box-step", "raster-step-mixed"],
+                    default=None,
                     help="launch the step kernels one by one for a profiler and exit (no timing)")
     ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed", help="--profile serving-step")
     args = ap.parse_args()

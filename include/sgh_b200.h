@@ -69,6 +69,10 @@ typedef struct {
 } sgh_program;
 
 #define SGH_PRECISION_FP64  0
+/* Single-instance plans only: every contraction in FP32 arithmetic on the CUDA
+ * cores (operands rounded to FP32, FP32 products and sums) and the modal
+ * iterates rounded to FP32 -- the FP32 arm of a precision study. */
+#define SGH_PRECISION_FP32  2
 
 /* Everything one instance needs; mirrors SimulationContext
  * (core/parameters.py:482-682) as consumed by SpectralSolver.initialize
@@ -80,7 +84,8 @@ typedef struct {
    * products, FP32 accumulation) and the modal iterates rounded to FP32 at
    * every write; the latent source across the solidus-liquidus band, the
    * property correction, the face fluxes, the Picard norms and the
-   * coefficient tables stay FP64. */
+   * coefficient tables stay FP64. SGH_PRECISION_FP32: the same with FP32
+   * contractions on the CUDA cores instead. */
   int32_t precision;
   double Lx, Ly, Lz;          /* domain size, m                              */
   double dt;                  /* corrected step, s                           */
@@ -360,6 +365,17 @@ int sgh_batch_slot_start(sgh_batch* batch, int32_t slot, const sgh_laser* lasers
                          sgh_step_out* outs_dev, void* stream);
 /* Stop a slot (it is skipped by later steps). Async. */
 int sgh_batch_slot_stop(sgh_batch* batch, int32_t slot, void* stream);
+/* Resume a slot from state the caller has written into its buffers
+ * (SGH_BUF_MODES and SGH_BUF_Q_EVAP_OLD of sgh_batch_buffer, e.g. copied out
+ * of a slot of the same configuration in this or another batch after a step):
+ * it continues at entry `step` of its laser table (n_steps entries, device)
+ * with the same results as if it had never stopped. This is the per-request
+ * state the reference keeps between steps (modes and the evaporation warm
+ * start, solvers/spectral.py:502-512; its modes.h5 layout,
+ * io_utils/spectral_fs_io.py:207-241), used for preemption and to move
+ * requests between batches. Async. */
+int sgh_batch_slot_resume(sgh_batch* batch, int32_t slot, const sgh_laser* lasers_dev, int32_t n_steps,
+                          int32_t step, sgh_step_out* outs_dev, void* stream);
 /* n_steps batch steps (each active slot advances until its table ends). Async. */
 int sgh_batch_step(sgh_batch* batch, int32_t n_steps, void* stream);
 /* One batch step with the same kernels launched one by one and the Picard

@@ -25,7 +25,8 @@ PICARD_HISTORY_MAX = 4096  # SGH_PICARD_HISTORY_MAX
 ERRORS = {-1: "SGH_ERR_INVALID", -2: "SGH_ERR_CUDA", -3: "SGH_ERR_STATE",
           -4: "SGH_ERR_UNSUPPORTED", -5: "SGH_ERR_WORKSPACE"}
 STEP_STATUS = {0: "converged", 1: "capped", 2: "nonfinite", 3: "tensor_core_timeout"}
-PRECISION = {"fp64": 0, "mixed": 1}
+PRECISION = {"fp64": 0, "mixed": 1}          # batches and plans
+PLAN_PRECISION = {"fp64": 0, "mixed": 1, "fp32": 2}   # single-instance plans
 BUF = {"modes": 0, "K": 1, "KK": 2, "T_prev": 3, "q_evap_old": 4, "Q_modes": 5,
        "surface": 6, "scratch": 7, "box_T_prev": 8, "box_Q_prev": 9, "box_Bx": 10,
        "box_By": 11, "box_Bz": 12}
@@ -43,7 +44,7 @@ EXPORTED = (
     "sgh_box_project", "sgh_state_flags", "sgh_state_set_flags", "sgh_line_workspace_bytes",
     "sgh_line_temperature", "sgh_picard_history",
     "sgh_batch_create", "sgh_batch_destroy", "sgh_batch_workspace_bytes", "sgh_batch_bind",
-    "sgh_batch_slot_start", "sgh_batch_slot_stop", "sgh_batch_step", "sgh_batch_step_eager",
+    "sgh_batch_slot_start", "sgh_batch_slot_stop", "sgh_batch_slot_resume", "sgh_batch_step", "sgh_batch_step_eager",
     "sgh_batch_status",
     "sgh_batch_buffer", "sgh_batch_launch_counts", "sgh_batch_volume_pass", "sgh_batch_error",
     "sgh_batch_set_wait_limit", "sgh_batch_set_policy", "sgh_dct2_bf16x3_workspace_bytes",
@@ -161,6 +162,7 @@ def lib() -> C.CDLL:
             "sgh_batch_bind": ([vp, vp, C.c_uint64, vp], C.c_int),
             "sgh_batch_slot_start": ([vp, i32, vp, i32, vp, vp], C.c_int),
             "sgh_batch_slot_stop": ([vp, i32, vp], C.c_int),
+            "sgh_batch_slot_resume": ([vp, i32, vp, i32, i32, vp, vp], C.c_int),
             "sgh_batch_step": ([vp, i32, vp], C.c_int),
             "sgh_batch_step_eager": ([vp, vp], C.c_int),
             "sgh_batch_status": ([vp, C.POINTER(SghBatchSlotInfo), vp], C.c_int),

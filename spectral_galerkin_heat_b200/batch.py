@@ -25,6 +25,11 @@ from .solver import laser_struct, make_config
 __all__ = ["BatchSolver"]
 
 
+def _torch_stream(stream):
+    import torch
+    return torch.cuda.stream(stream)
+
+
 def _picard(ctx, omega=None, tol=None, max_iter=None):
     num = ctx.num
 
@@ -135,6 +140,35 @@ class BatchSolver:
         _lib.check("sgh_batch_slot_start", _lib.lib().sgh_batch_slot_start(
             self._h, int(slot), C.c_void_p(table.data_ptr()), int(n_steps),
             C.c_void_p(outs.data_ptr()) if outs is not None else None, self._s()))
+
+    def export_slot(self, slot: int) -> dict:
+        """The state a slot carries between steps, as device copies: its modes
+        (FP64 or FP32), its evaporation warm start ``q_evap_old`` and its
+        progress (``step`` of ``n_steps``). The slot keeps running unless it is
+        stopped; a checkpoint of a request in flight (preemption)."""
+        info = self.status()[slot]
+        return {"modes": self.snapshot(slot, "modes"), "q_evap_old": self.snapshot(slot, "q_evap_old"),
+                "step": int(info.step), "n_steps": int(info.n_steps), "precision": self.precision,
+                "shape": tuple(self.buffer(slot, "modes").shape)}
+
+    def import_slot(self, slot: int, state: dict, table) -> None:
+        """Continue an exported request in ``slot`` (same grid, physics and
+        precision) with its laser ``table`` (all of the request's steps): it
+        resumes at the exported step and gives the same bits as if it had run
+        on uninterrupted."""
+        if state["precision"] != self.precision:
+            raise ValueError("a slot state moves between batches of the same precision only")
+        dst = self.buffer(slot, "modes")
+        if tuple(dst.shape) != tuple(state["shape"]):
+            raise ValueError(f"slot {slot} has modes {tuple(dst.shape)}, the state {state['shape']}")
+        with _torch_stream(self.stream):
+            dst.copy_(state["modes"])
+            self.buffer(slot, "q_evap_old").copy_(state["q_evap_old"])
+        self._tables[slot] = table
+        self._outs[slot] = None
+        _lib.check("sgh_batch_slot_resume", _lib.lib().sgh_batch_slot_resume(
+            self._h, int(slot), C.c_void_p(table.data_ptr()), int(state["n_steps"]), int(state["step"]),
+            None, self._s()))
 
     def stop(self, slot: int) -> None:
         _lib.check("sgh_batch_slot_stop", _lib.lib().sgh_batch_slot_stop(self._h, int(slot), self._s()))

@@ -54,10 +54,12 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 // cp.async pipeline of AX_BK-slice stages (out-of-range elements zero-filled).
 // Computes the output tile at (c0, k0) and hands every element to epi; the
 // caller reduces r over the block.
-template <bool CONTIG, int TI, int TJ, class Epi>
+template <bool CONTIG, int TI, int TJ, class Epi, class T = double>
 __device__ __forceinline__ void axis_tile(const double* __restrict__ X, const double* __restrict__ Mat,
                                           int Nout, int N, int A, int B, int c0, int k0, const Epi& epi,
                                           Red& r) {
+  // T: the arithmetic of the contraction -- double, or float for the FP32
+  // plans (operands rounded to FP32 as they are read, FP32 products and sums)
   constexpr int TK = CONTIG ? 16 * TJ : 16 * TI;  // outputs along the transformed axis per tile
   constexpr int TC = CONTIG ? 16 * TI : 16 * TJ;  // outputs along c per tile
   __shared__ double Ms[AX_STAGES][AX_BK][TK + 1];
@@ -99,11 +101,11 @@ __device__ __forceinline__ void axis_tile(const double* __restrict__ X, const do
     cp_async_commit();
   };
 
-  double acc[TI][TJ];
+  T acc[TI][TJ];
 #pragma unroll
   for (int i = 0; i < TI; ++i)
 #pragma unroll
-    for (int j = 0; j < TJ; ++j) acc[i][j] = 0.0;
+    for (int j = 0; j < TJ; ++j) acc[i][j] = T(0);
 
 #pragma unroll
   for (int st = 0; st < AX_STAGES - 1; ++st) {
@@ -119,21 +121,21 @@ __device__ __forceinline__ void axis_tile(const double* __restrict__ X, const do
     const int stg = ch % AX_STAGES;
 #pragma unroll
     for (int kk = 0; kk < AX_BK; ++kk) {
-      double m[CONTIG ? TJ : TI], x[CONTIG ? TI : TJ];
+      T m[CONTIG ? TJ : TI], x[CONTIG ? TI : TJ];
       if (CONTIG) {
 #pragma unroll
-        for (int j = 0; j < TJ; ++j) m[j] = Ms[stg][kk][f + 16 * j];
+        for (int j = 0; j < TJ; ++j) m[j] = (T)Ms[stg][kk][f + 16 * j];
 #pragma unroll
-        for (int i = 0; i < TI; ++i) x[i] = Xs[stg][kk][TI * s + i];
+        for (int i = 0; i < TI; ++i) x[i] = (T)Xs[stg][kk][TI * s + i];
 #pragma unroll
         for (int i = 0; i < TI; ++i)
 #pragma unroll
           for (int j = 0; j < TJ; ++j) acc[i][j] = fma(m[j], x[i], acc[i][j]);
       } else {
 #pragma unroll
-        for (int i = 0; i < TI; ++i) m[i] = Ms[stg][kk][TI * s + i];
+        for (int i = 0; i < TI; ++i) m[i] = (T)Ms[stg][kk][TI * s + i];
 #pragma unroll
-        for (int j = 0; j < TJ; ++j) x[j] = Xs[stg][kk][f + 16 * j];
+        for (int j = 0; j < TJ; ++j) x[j] = (T)Xs[stg][kk][f + 16 * j];
 #pragma unroll
         for (int i = 0; i < TI; ++i)
 #pragma unroll
@@ -152,13 +154,13 @@ __device__ __forceinline__ void axis_tile(const double* __restrict__ X, const do
       if (k < Nout && c < ncol) {
         const int a = c / B, b = c - a * B;
         const int idx = (a * Nout + k) * B + b;
-        epi(idx, k, b, acc[i][j], r);
+        epi(idx, k, b, (double)acc[i][j], r);
       }
     }
   }
 }
 
-template <bool CONTIG, int TI, int TJ, class Epi>
+template <bool CONTIG, int TI, int TJ, class Epi, class T = double>
 __global__ void __launch_bounds__(AX_THREADS)
 k_axis(const double* __restrict__ X, const double* __restrict__ Mat, int Nout, int N, int A, int B,
        Epi epi) {
@@ -168,7 +170,7 @@ k_axis(const double* __restrict__ X, const double* __restrict__ Mat, int Nout, i
   // programmatic stream serialisation: nothing global before the previous kernel completes
   asm volatile("griddepcontrol.wait;\n" ::: "memory");
   Red r;
-  axis_tile<CONTIG, TI, TJ>(X, Mat, Nout, N, A, B, blockIdx.x * TC, blockIdx.y * TK, epi, r);
+  axis_tile<CONTIG, TI, TJ, Epi, T>(X, Mat, Nout, N, A, B, blockIdx.x * TC, blockIdx.y * TK, epi, r);
   if (Epi::kReduce) {
     double p0, p1;
     if (Epi::kReduce == 1) {
@@ -526,6 +528,8 @@ constexpr int AXU_KC = 32;  // contraction slices per stage
 // plans), and where that kernel records an expired wait.
 inline thread_local bool g_axis_umma = false;
 inline thread_local int* g_umma_err = nullptr;
+// Whether passes run the CUDA-core kernel in FP32 arithmetic (FP32 plans).
+inline thread_local bool g_axis_fp32 = false;
 
 template <int NT>
 __host__ __device__ constexpr int axu_stage_bytes() { return 2 * AXU_M * AXU_KC * 2 + 2 * NT * AXU_KC * 2; }
@@ -598,38 +602,51 @@ k_axis_umma(const double* __restrict__ X, const double* __restrict__ Mat, int No
     }
     char* st = axu_sh + s * STAGE;
     const int n0 = ch * AXU_KC;
-    if (CONTIG) {
-#pragma unroll 4
-      for (int j = 0; j < AXU_M / 4; ++j) {
-        const int r = warp + 4 * j, c = c0 + r, n = n0 + lane;
-        const double x = (c < ncol && n < N) ? X[(size_t)c * N + n] : 0.0;
-        __nv_bfloat16 h, l;
-        split_bf16(x, h, l);
-        const uint32_t o = core_off(r, lane, AXU_M);
-        *reinterpret_cast<__nv_bfloat16*>(st + o) = h;
-        *reinterpret_cast<__nv_bfloat16*>(st + XB + o) = l;
+    // every load of a group is issued before the first split, so a thread
+    // keeps 16 operand values in flight
+    constexpr int G = 16;
+#pragma unroll
+    for (int j0 = 0; j0 < AXU_KC; j0 += G) {  // X: 32 values per thread
+      double xv[G];
+#pragma unroll
+      for (int j = 0; j < G; ++j) {
+        if (CONTIG) {
+          const int r = warp + 4 * (j0 + j), c = c0 + r, n = n0 + lane;
+          xv[j] = (c < ncol && n < N) ? __ldg(X + (size_t)c * N + n) : 0.0;
+        } else {
+          const int n = n0 + j0 + j;
+          xv[j] = (xok && n < N) ? __ldg(X + xcol + (size_t)n * B) : 0.0;
+        }
       }
-    } else {
-#pragma unroll 4
-      for (int k = 0; k < AXU_KC; ++k) {
-        const int n = n0 + k;
-        const double x = (xok && n < N) ? X[xcol + (size_t)n * B] : 0.0;
+#pragma unroll
+      for (int j = 0; j < G; ++j) {
         __nv_bfloat16 h, l;
-        split_bf16(x, h, l);
-        const uint32_t o = core_off(tid, k, AXU_M);
+        split_bf16(xv[j], h, l);
+        const uint32_t o = CONTIG ? core_off(warp + 4 * (j0 + j), lane, AXU_M) : core_off(tid, j0 + j, AXU_M);
         *reinterpret_cast<__nv_bfloat16*>(st + o) = h;
         *reinterpret_cast<__nv_bfloat16*>(st + XB + o) = l;
       }
     }
-    for (int e = tid; e < NT * AXU_KC; e += AXU_THREADS) {  // Mat rows k, slices n (n fastest)
-      const int r = e / AXU_KC, kk = e % AXU_KC;
-      const int k = k0 + r, n = n0 + kk;
-      const double x = (k < Nout && n < N) ? Mat[(size_t)k * N + n] : 0.0;
-      __nv_bfloat16 h, l;
-      split_bf16(x, h, l);
-      const uint32_t o = core_off(r, kk, NT);
-      *reinterpret_cast<__nv_bfloat16*>(st + 2 * XB + o) = h;
-      *reinterpret_cast<__nv_bfloat16*>(st + 2 * XB + MB + o) = l;
+    constexpr int MPT = NT * AXU_KC / AXU_THREADS;  // Mat values per thread: 8 .. 64
+    constexpr int MG = MPT < G ? MPT : G;
+#pragma unroll
+    for (int j0 = 0; j0 < MPT; j0 += MG) {  // Mat rows k, slices n (n fastest)
+      double mv[MG];
+#pragma unroll
+      for (int j = 0; j < MG; ++j) {
+        const int e = tid + (j0 + j) * AXU_THREADS;
+        const int k = k0 + e / AXU_KC, n = n0 + e % AXU_KC;
+        mv[j] = (k < Nout && n < N) ? __ldg(Mat + (size_t)k * N + n) : 0.0;
+      }
+#pragma unroll
+      for (int j = 0; j < MG; ++j) {
+        const int e = tid + (j0 + j) * AXU_THREADS;
+        __nv_bfloat16 h, l;
+        split_bf16(mv[j], h, l);
+        const uint32_t o = core_off(e / AXU_KC, e % AXU_KC, NT);
+        *reinterpret_cast<__nv_bfloat16*>(st + 2 * XB + o) = h;
+        *reinterpret_cast<__nv_bfloat16*>(st + 2 * XB + MB + o) = l;
+      }
     }
     fence_proxy_async();
     __syncthreads();
@@ -750,22 +767,27 @@ constexpr int AXM_MIN_CTAS = 16;      // smaller passes stay on the CUDA-core ke
 
 struct AxisPolicy {
   int saved;
-  bool saved_mma, saved_umma;
+  bool saved_mma, saved_umma, saved_fp32;
   int* saved_err;
   // umma: every pass on the split-BF16 tensor-core kernel (mixed-precision
   // plans); err: where that kernel records an expired wait (null while only
   // sizing buffers)
-  explicit AxisPolicy(int min_ctas, int cuda_cores_only = 0, bool umma = false, int* err = nullptr)
-      : saved(g_axis_min_ctas), saved_mma(g_axis_mma), saved_umma(g_axis_umma), saved_err(g_umma_err) {
+  // fp32: every pass on the CUDA-core kernel in FP32 arithmetic (FP32 plans)
+  explicit AxisPolicy(int min_ctas, int cuda_cores_only = 0, bool umma = false, int* err = nullptr,
+                      bool fp32 = false)
+      : saved(g_axis_min_ctas), saved_mma(g_axis_mma), saved_umma(g_axis_umma), saved_fp32(g_axis_fp32),
+        saved_err(g_umma_err) {
     g_axis_min_ctas = min_ctas > 0 ? min_ctas : AX_MIN_CTAS;
-    g_axis_mma = cuda_cores_only == 0;
+    g_axis_mma = cuda_cores_only == 0 && !fp32;
     g_axis_umma = umma;
+    g_axis_fp32 = fp32;
     g_umma_err = err;
   }
   ~AxisPolicy() {
     g_axis_min_ctas = saved;
     g_axis_mma = saved_mma;
     g_axis_umma = saved_umma;
+    g_axis_fp32 = saved_fp32;
     g_umma_err = saved_err;
   }
 };
@@ -842,6 +864,16 @@ inline void launch_axis(const double* X, const double* Mat, int Nout, int N, int
   if (sh.kind >= 2) {
     if (B == 1) launch_axis_mma_kind<true>(sh.kind, X, Mat, Nout, N, A, B, epi, sh.grid, st);
     else launch_axis_mma_kind<false>(sh.kind, X, Mat, Nout, N, A, B, epi, sh.grid, st);
+    return;
+  }
+  if (g_axis_fp32) {
+    if (B == 1) {
+      if (sh.big) launch_pdl(k_axis<true, 2, 4, Epi, float>, sh.grid, AX_THREADS, 0, st, X, Mat, Nout, N, A, B, epi);
+      else launch_pdl(k_axis<true, 1, 1, Epi, float>, sh.grid, AX_THREADS, 0, st, X, Mat, Nout, N, A, B, epi);
+    } else {
+      if (sh.big) launch_pdl(k_axis<false, 2, 4, Epi, float>, sh.grid, AX_THREADS, 0, st, X, Mat, Nout, N, A, B, epi);
+      else launch_pdl(k_axis<false, 1, 1, Epi, float>, sh.grid, AX_THREADS, 0, st, X, Mat, Nout, N, A, B, epi);
+    }
     return;
   }
   if (B == 1) {

@@ -727,6 +727,9 @@ namespace {
 // Mixed-precision plan: every contraction on the split-BF16 tensor-core
 // kernel, modal iterates rounded to FP32.
 bool plan_mixed(const sgh_plan* p) { return p && p->cfg.precision == SGH_PRECISION_MIXED; }
+// FP32 plan: every contraction in FP32 arithmetic on the CUDA cores, modal
+// iterates rounded to FP32 (the FP32 arm of the precision study).
+bool plan_fp32(const sgh_plan* p) { return p && p->cfg.precision == SGH_PRECISION_FP32; }
 int* umma_err_of(const sgh_plan* p) { return (p && p->ws) ? &p->ctrl()->umma_err : nullptr; }
 
 int check_program(const sgh_program& p, const char* name) {
@@ -1288,12 +1291,14 @@ int sgh_plan_create(const sgh_config* cfg, sgh_plan** out) {
   const sgh_config& c = *cfg;
   if (c.axis_min_ctas < 0) return fail(SGH_ERR_INVALID, "axis_min_ctas must be >= 0");
   if (c.axis_cuda_cores != 0 && c.axis_cuda_cores != 1) return fail(SGH_ERR_INVALID, "axis_cuda_cores must be 0 or 1");
-  AxisPolicy policy(c.axis_min_ctas, c.axis_cuda_cores, c.precision == SGH_PRECISION_MIXED);
+  AxisPolicy policy(c.axis_min_ctas, c.axis_cuda_cores, c.precision == SGH_PRECISION_MIXED, nullptr,
+                    c.precision == SGH_PRECISION_FP32);
   if (c.nx < 2 || c.ny < 2 || c.nz < 2) return fail(SGH_ERR_INVALID, "every axis needs at least 2 modes");
   if (c.nx > 4096 || c.ny > 4096 || c.nz > 4096) return fail(SGH_ERR_INVALID, "an axis exceeds 4096 modes");
   if ((long long)c.nx * c.ny * c.nz > (1LL << 28)) return fail(SGH_ERR_INVALID, "grid exceeds 2^28 modes");
-  if (c.precision != SGH_PRECISION_FP64 && c.precision != SGH_PRECISION_MIXED)
-    return fail(SGH_ERR_INVALID, "precision must be SGH_PRECISION_FP64 or SGH_PRECISION_MIXED");
+  if (c.precision != SGH_PRECISION_FP64 && c.precision != SGH_PRECISION_MIXED &&
+      c.precision != SGH_PRECISION_FP32)
+    return fail(SGH_ERR_INVALID, "precision must be SGH_PRECISION_FP64, _MIXED or _FP32");
   if (!(c.Lx > 0 && c.Ly > 0 && c.Lz > 0 && c.dt > 0))
     return fail(SGH_ERR_INVALID, "domain size and dt must be positive");
   if (!(c.r_x > 0 && c.r_y > 0 && c.area_factor > 0 && c.order > 0))
@@ -1328,7 +1333,7 @@ int sgh_plan_create(const sgh_config* cfg, sgh_plan** out) {
   p->cfg = c;
   DevParams& h = p->hp;
   std::memset(&h, 0, sizeof(h));
-  h.round32 = c.precision == SGH_PRECISION_MIXED ? 1 : 0;
+  h.round32 = c.precision != SGH_PRECISION_FP64 ? 1 : 0;
   h.nx = c.nx; h.ny = c.ny; h.nz = c.nz;
   h.S = c.nx * c.ny;
   h.V = h.S * c.nz;
@@ -1500,7 +1505,8 @@ int sgh_plan_workspace_bytes(const sgh_plan* p, uint64_t* bytes) {
 }
 
 int sgh_plan_bind(sgh_plan* p, void* workspace, uint64_t bytes, void* stream) {
-  AxisPolicy policy(p ? p->cfg.axis_min_ctas : 0, p ? p->cfg.axis_cuda_cores : 0, plan_mixed(p), umma_err_of(p));
+  AxisPolicy policy(p ? p->cfg.axis_min_ctas : 0, p ? p->cfg.axis_cuda_cores : 0, plan_mixed(p), umma_err_of(p),
+                    plan_fp32(p));
   if (!p || !workspace) return fail(SGH_ERR_INVALID, "null argument");
   if (p->bound) return fail(SGH_ERR_STATE, "plan is already bound");
   if (bytes < p->ws_need) return fail(SGH_ERR_WORKSPACE, "workspace is smaller than sgh_plan_workspace_bytes()");
@@ -1632,7 +1638,8 @@ int sgh_step(sgh_plan* p, const sgh_laser* laser, sgh_step_out* out, void* strea
 }
 
 int sgh_step_eager(sgh_plan* p, const sgh_laser* laser, sgh_step_out* out, void* stream) {
-  AxisPolicy policy(p ? p->cfg.axis_min_ctas : 0, p ? p->cfg.axis_cuda_cores : 0, plan_mixed(p), umma_err_of(p));
+  AxisPolicy policy(p ? p->cfg.axis_min_ctas : 0, p ? p->cfg.axis_cuda_cores : 0, plan_mixed(p), umma_err_of(p),
+                    plan_fp32(p));
   if (!p || !laser) return fail(SGH_ERR_INVALID, "null argument");
   if (!p->bound) return fail(SGH_ERR_STATE, "plan is not bound");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -1666,7 +1673,8 @@ int sgh_run(sgh_plan* p, const sgh_laser* lasers_dev, int32_t n_steps, sgh_step_
 }
 
 int sgh_dct3d(sgh_plan* p, int32_t kind, const double* in, double* out, void* stream) {
-  AxisPolicy policy(p ? p->cfg.axis_min_ctas : 0, p ? p->cfg.axis_cuda_cores : 0, plan_mixed(p), umma_err_of(p));
+  AxisPolicy policy(p ? p->cfg.axis_min_ctas : 0, p ? p->cfg.axis_cuda_cores : 0, plan_mixed(p), umma_err_of(p),
+                    plan_fp32(p));
   if (!p || !in || !out) return fail(SGH_ERR_INVALID, "null argument");
   if (!p->bound) return fail(SGH_ERR_STATE, "plan is not bound");
   if (kind != 2 && kind != 3) return fail(SGH_ERR_INVALID, "kind must be 2 (DCT_II) or 3 (IDCT_II)");
@@ -1677,7 +1685,8 @@ int sgh_dct3d(sgh_plan* p, int32_t kind, const double* in, double* out, void* st
 }
 
 int sgh_surface_temperature(sgh_plan* p, const double* modes, int32_t top, double* out, void* stream) {
-  AxisPolicy policy(p ? p->cfg.axis_min_ctas : 0, p ? p->cfg.axis_cuda_cores : 0, plan_mixed(p), umma_err_of(p));
+  AxisPolicy policy(p ? p->cfg.axis_min_ctas : 0, p ? p->cfg.axis_cuda_cores : 0, plan_mixed(p), umma_err_of(p),
+                    plan_fp32(p));
   if (!p || !modes || !out) return fail(SGH_ERR_INVALID, "null argument");
   if (!p->bound) return fail(SGH_ERR_STATE, "plan is not bound");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -1687,7 +1696,8 @@ int sgh_surface_temperature(sgh_plan* p, const double* modes, int32_t top, doubl
 }
 
 int sgh_project_volume(sgh_plan* p, const double* field, double* modes, void* stream) {
-  AxisPolicy policy(p ? p->cfg.axis_min_ctas : 0, p ? p->cfg.axis_cuda_cores : 0, plan_mixed(p), umma_err_of(p));
+  AxisPolicy policy(p ? p->cfg.axis_min_ctas : 0, p ? p->cfg.axis_cuda_cores : 0, plan_mixed(p), umma_err_of(p),
+                    plan_fp32(p));
   if (!p || !field || !modes) return fail(SGH_ERR_INVALID, "null argument");
   if (!p->bound) return fail(SGH_ERR_STATE, "plan is not bound");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -1697,7 +1707,8 @@ int sgh_project_volume(sgh_plan* p, const double* field, double* modes, void* st
 }
 
 int sgh_reconstruct_volume(sgh_plan* p, const double* modes, double* field, void* stream) {
-  AxisPolicy policy(p ? p->cfg.axis_min_ctas : 0, p ? p->cfg.axis_cuda_cores : 0, plan_mixed(p), umma_err_of(p));
+  AxisPolicy policy(p ? p->cfg.axis_min_ctas : 0, p ? p->cfg.axis_cuda_cores : 0, plan_mixed(p), umma_err_of(p),
+                    plan_fp32(p));
   if (!p || !field || !modes) return fail(SGH_ERR_INVALID, "null argument");
   if (!p->bound) return fail(SGH_ERR_STATE, "plan is not bound");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -1771,7 +1782,8 @@ int sgh_box_window(sgh_plan* p, int32_t* i0, void* stream) {
 }
 
 int sgh_box_temperature(sgh_plan* p, const double* modes, double* out, void* stream) {
-  AxisPolicy policy(p ? p->cfg.axis_min_ctas : 0, p ? p->cfg.axis_cuda_cores : 0, plan_mixed(p), umma_err_of(p));
+  AxisPolicy policy(p ? p->cfg.axis_min_ctas : 0, p ? p->cfg.axis_cuda_cores : 0, plan_mixed(p), umma_err_of(p),
+                    plan_fp32(p));
   if (!p || !modes || !out) return fail(SGH_ERR_INVALID, "null argument");
   if (!p->bound) return fail(SGH_ERR_STATE, "plan is not bound");
   if (!p->hp.box) return fail(SGH_ERR_STATE, "plan is not in box mode");
@@ -1783,7 +1795,8 @@ int sgh_box_temperature(sgh_plan* p, const double* modes, double* out, void* str
 }
 
 int sgh_box_project(sgh_plan* p, const double* field_box, double* modes, void* stream) {
-  AxisPolicy policy(p ? p->cfg.axis_min_ctas : 0, p ? p->cfg.axis_cuda_cores : 0, plan_mixed(p), umma_err_of(p));
+  AxisPolicy policy(p ? p->cfg.axis_min_ctas : 0, p ? p->cfg.axis_cuda_cores : 0, plan_mixed(p), umma_err_of(p),
+                    plan_fp32(p));
   if (!p || !field_box || !modes) return fail(SGH_ERR_INVALID, "null argument");
   if (!p->bound) return fail(SGH_ERR_STATE, "plan is not bound");
   if (!p->hp.box) return fail(SGH_ERR_STATE, "plan is not in box mode");

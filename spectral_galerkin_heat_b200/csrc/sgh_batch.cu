@@ -289,6 +289,24 @@ kb_slot_start(BView v, int s, R* a, double* q_evold, double* q_ev, double* sigma
 
 __global__ void kb_slot_stop(BView v, int s) { v.st[s].active = 0; }
 
+// Resume one slot from state already written into its buffers (modes and
+// q_evap_old, exported from another slot or batch): it continues at step
+// `step` of its laser table. The next step forms its face sums from the
+// stored modes (pass1_ready = 0), exactly as the commit would have.
+__global__ void kb_slot_resume(BView v, int s, const sgh_laser* table, int n_steps, int step,
+                               sgh_step_out* outs) {
+  BState& st = v.st[s];
+  st.table = table;
+  st.outs = outs;
+  st.n_steps = n_steps;
+  st.step = step;
+  st.active = step < n_steps ? 1 : 0;
+  st.iters = 0;
+  st.done = 1;
+  st.iter = 0;
+  st.pass1_ready = 0;
+}
+
 // ---------------------------------------------------------------------------
 // step
 // ---------------------------------------------------------------------------
@@ -332,11 +350,11 @@ __global__ void __launch_bounds__(CT) kb_begin(BView v, cudaGraphConditionalHand
 
 // q_las, P_laser partials and q_net = q_las - shift(q_evap_old) per slot
 // (solvers/spectral.py:273-306). The Gaussian beam factorises,
-// exp(-2 (ux^2 + uy^2)) = exp(-2 ux^2) exp(-2 uy^2), so a block first tabulates
-// the column factors of its slot and the row factors of the rows it covers in
-// shared memory (one exp per column and per row instead of one per element;
-// a few ulps from the unfactorised form); other profiles evaluate the flux
-// per element.
+// exp(-2 (ux^2 + uy^2)) = exp(-2 ux^2) exp(-2 uy^2), so in mixed-precision
+// batches a block first tabulates the column factors of its slot and the row
+// factors of the rows it covers in shared memory (one exp per column and per
+// row instead of one per element; a few ulps from the unfactorised form);
+// FP64 batches and other profiles evaluate the flux per element.
 constexpr int FB_MAX_COLS = 1024;  // column factors tabulated (wider faces: per element)
 constexpr int FB_MAX_ROWS = 160;   // row factors of one block (RB / 16 + 2 rows at nx >= 16)
 
@@ -357,7 +375,9 @@ kb_face_begin(BView v, double* q_las, double* q_net, const double* q_evold, doub
   const double I0 = st.I0, lx = st.laser.x, ly = st.laser.y, sx = st.shift_x, sy = st.shift_y;
   const int i0 = (b - sl.rblk0) * RB;
   const int y_lo = i0 / nx, y_hi = min(ny - 1, (i0 + RB - 1) / nx);
-  const bool table = !sl.cell_integrated && sl.order == 2.0 && nx <= FB_MAX_COLS &&
+  // mixed precision only: FP64 batches keep the unfactorised exponential, so
+  // they stay equal to the single-instance plan to rounding
+  const bool table = v.xq != nullptr && !sl.cell_integrated && sl.order == 2.0 && nx <= FB_MAX_COLS &&
                      (y_hi - y_lo + 1) <= FB_MAX_ROWS;
   if (table) {
     for (int x = threadIdx.x; x < nx; x += BT) {
@@ -1742,6 +1762,18 @@ int sgh_batch_slot_start(sgh_batch* B, int32_t slot, const sgh_laser* lasers_dev
   else
     kb_slot_start<double><<<g, BT, 0, s>>>(B->view(), slot, B->d(B->o_a), B->d(B->o_qevold), B->d(B->o_qev),
                                            B->d(B->o_sigma), lasers_dev, n_steps, outs_dev);
+  SGB_CK(cudaGetLastError());
+  return SGH_OK;
+}
+
+int sgh_batch_slot_resume(sgh_batch* B, int32_t slot, const sgh_laser* lasers_dev, int32_t n_steps,
+                          int32_t step, sgh_step_out* outs_dev, void* stream) {
+  if (!B || !B->bound) return bfail(SGH_ERR_STATE, "batch is not bound");
+  if (slot < 0 || slot >= B->n) return bfail(SGH_ERR_INVALID, "slot out of range");
+  if (n_steps < 0 || (n_steps > 0 && !lasers_dev)) return bfail(SGH_ERR_INVALID, "bad laser table");
+  if (step < 0 || step > n_steps) return bfail(SGH_ERR_INVALID, "step must be in [0, n_steps]");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  kb_slot_resume<<<1, 1, 0, s>>>(B->view(), slot, lasers_dev, n_steps, step, outs_dev);
   SGB_CK(cudaGetLastError());
   return SGH_OK;
 }

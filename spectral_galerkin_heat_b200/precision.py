@@ -7,6 +7,10 @@ For one configuration and laser path this runs, side by side on the device:
 * ``mixed``: the mixed-precision form (a batch of one slot: FP32 modal state,
   split-BF16 tensor-core face transforms with FP32 accumulation, FP64 faces,
   norms and coefficient tables);
+* ``fp32``: the single-instance plan with every contraction in FP32
+  arithmetic on the CUDA cores and the modal iterates in FP32 (FP64 faces,
+  norms and tables), the plain FP32 arm against which the split-BF16
+  contractions are judged;
 * ``fp64_perturbed``: the FP64 solver again, from an initial field changed by
   one part in 1e12. Where this run already parts from ``fp64``, the problem
   is ill-conditioned and a difference between precisions there is not a
@@ -155,6 +159,8 @@ def run_study(cfg: dict, path, checkpoints: Sequence[int], picard: Optional[dict
     T0 = per.volume_temperature().cpu().numpy()
     rng = np.random.default_rng(seed)
     per.set_state(T0 * (1.0 + perturb * rng.standard_normal(T0.shape)))
+    f32 = B200SpectralSolver(None, copy.copy(ctx), precision="fp32")
+    f32.initialize()
     rnd = B200SpectralSolver(None, copy.copy(ctx))
     rnd.initialize()
     rnd.run(0.0, 1)
@@ -168,6 +174,7 @@ def run_study(cfg: dict, path, checkpoints: Sequence[int], picard: Optional[dict
         ref_m = ref.run(done * dt, n)
         per.run(done * dt, n)
         rnd.run(max(done, 1) * dt, cp - max(done, 1))
+        f32_m = f32.run(done * dt, n)
         mix.step(n)
         done = cp
         T_ref = ref.volume_temperature().cpu().numpy()
@@ -175,15 +182,18 @@ def run_study(cfg: dict, path, checkpoints: Sequence[int], picard: Optional[dict
         T_rnd = rnd.volume_temperature().cpu().numpy()
         a_mix = mix.modes(0).to(torch.float64).contiguous()
         T_mix = ref.volume_temperature(a_mix).cpu().numpy()
+        T_f32 = ref.volume_temperature(f32.state.a).cpu().numpy()
         nodes = {name: kernels.reconstruct_temperature_DCT(a, geo).cpu().numpy()
                  for name, a in (("ref", ref.state.a), ("per", per.state.a), ("rnd", rnd.state.a),
-                                 ("mix", a_mix))}
+                                 ("mix", a_mix), ("f32", f32.state.a.clone()))}
         mm = mix.metrics(0)[-1]
         out.append({
             "step": cp,
             "picard_iters_fp64_last": ref_m[-1]["n_evap_iter"], "picard_iters_mixed_last": mm["n_evap_iter"],
             "T_surface_max_fp64": ref_m[-1]["T_surface_max"], "T_surface_max_mixed": mm["T_surface_max"],
             "mixed": compare_fields(T_mix, T_ref, cell, T_melt, nodes["mix"], nodes["ref"], lengths),
+            "fp32": compare_fields(T_f32, T_ref, cell, T_melt, nodes["f32"], nodes["ref"], lengths),
+            "picard_iters_fp32_last": f32_m[-1]["n_evap_iter"],
             "fp64_perturbed": compare_fields(T_per, T_ref, cell, T_melt, nodes["per"], nodes["ref"],
                                              lengths),
             "fp64_fp32_rounded": compare_fields(T_rnd, T_ref, cell, T_melt, nodes["rnd"], nodes["ref"],
@@ -193,6 +203,7 @@ def run_study(cfg: dict, path, checkpoints: Sequence[int], picard: Optional[dict
     ref.finalize()
     per.finalize()
     rnd.finalize()
+    f32.finalize()
     mix.close()
     return out
 
@@ -212,9 +223,7 @@ def main(argv=None):
         "picard_converged": {"max_picard_iter": 400, "picard_omega": 0.1, "picard_tol": 1e-8},
     }
     report = {"config": {"mesh": [nx, ny, nz], "domain_m": cfg["domain"]["size"], "seed": args.seed,
-                         "power_W": path.power, "speed_m_s": path.vx,
-                         "fp32_contraction_variant": "not built: the mixed form's contractions are "
-                                                     "split-BF16 on the tensor cores"},
+                         "power_W": path.power, "speed_m_s": path.vx},
               "forms": {}}
     for name, picard in forms.items():
         report["forms"][name] = run_study(cfg, path, args.checkpoints, picard=picard, seed=args.seed)

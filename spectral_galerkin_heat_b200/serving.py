@@ -36,6 +36,20 @@ an exception, ``solvers/spectral.py:486-499``):
   wait of a tensor-core face pass ran out, every request in flight is marked
   ``"failed"`` (its slot results are not trusted) and ``run`` raises
   ``RuntimeError``.
+
+Preemption and adaptive capacity. A slot's state between steps is its modes
+and its evaporation warm start (``BatchSolver.export_slot``); a request moved
+with that state resumes bit for bit (``import_slot``). ``preempt(request)``
+takes a running request out of its slot at the next chunk boundary and queues
+it again with its state, to resume when a slot of its class frees. With
+``adaptive=True`` the engine also re-plans its capacity by free HBM while it
+runs: when queued requests find no free slot of their class -- a class it has
+never seen included -- it re-divides the memory budget (a fraction of the free
+device memory plus its own workspace) among the classes in proportion to
+their demand (requests running and waiting), builds the new batch, and moves
+every request in flight into it with its state. Freed slot bytes of one class
+thus go to another, and admission follows free memory rather than a fixed
+class plan.
 """
 from __future__ import annotations
 
@@ -120,50 +134,132 @@ class ServingEngine:
                  weights: Optional[Dict[Tuple, float]] = None, slots: Optional[Dict[Tuple, int]] = None,
                  keep_modes: bool = False, max_chunk: int = 64,
                  batch_factory: Optional[Callable] = None, mem_info: Optional[Callable] = None,
-                 slot_bytes: Optional[Callable] = None):
+                 slot_bytes: Optional[Callable] = None, adaptive: bool = False,
+                 rebalance_interval: float = 1.0):
         if batch_factory is None:
             import torch
             if not torch.cuda.is_available():
                 raise RuntimeError("ServingEngine needs a CUDA device (no CPU fallback)")
             batch_factory = BatchSolver
             mem_info = mem_info or torch.cuda.mem_get_info
-        slot_bytes = slot_bytes or (lambda ctx: BatchSolver.workspace_bytes_for([ctx], precision))
+        self._slot_bytes_fn = slot_bytes or (lambda ctx: BatchSolver.workspace_bytes_for([ctx], precision))
+        self._batch_factory = batch_factory
+        self._mem_info = mem_info
         self.precision = precision
+        self.memory_fraction = float(memory_fraction)
+        self.max_slots = int(max_slots)
+        self.adaptive = bool(adaptive)
+        self.rebalance_interval = float(rebalance_interval)
         self.keys = list(classes)
         self.templates = {k: classes[k] for k in self.keys}
         self.keep_modes = keep_modes
         self.max_chunk = int(max_chunk)
+        self._per_slot: Dict[Tuple, int] = {}
         free, total = mem_info()
-        self.budget = int(memory_fraction * free)
-        per_slot = {k: int(slot_bytes(self.templates[k])) for k in self.keys}
+        self.budget = int(self.memory_fraction * free)
         if slots is None:
             w = {k: float((weights or {}).get(k, 1.0)) for k in self.keys}
-            slots = {k: 1 for k in self.keys}
-            used = sum(per_slot[k] for k in self.keys)
-            if used > self.budget:
-                raise RuntimeError(f"one slot per class needs {used} bytes; the budget is {self.budget}")
-            while True:
-                cand = [k for k in self.keys if slots[k] < max_slots and used + per_slot[k] <= self.budget]
-                if not cand:
-                    break
-                k = min(cand, key=lambda c: slots[c] / max(w[c], 1e-12))
-                slots[k] += 1
-                used += per_slot[k]
-        self.slots_per_class = dict(slots)
-        contexts, self.slot_key = [], []
-        for k in self.keys:
-            for _ in range(slots[k]):
-                contexts.append(self.templates[k])
-                self.slot_key.append(k)
-        self.batch = batch_factory(contexts, precision)
-        self.free = {k: deque(i for i, kk in enumerate(self.slot_key) if kk == k) for k in self.keys}
+            slots = self._allocate(w, {}, self.budget)
         self.stats = _Stats()
         self._active: Dict[int, Request] = {}
         self._done_steps: Dict[int, int] = {}
         self._cancel: set = set()
+        self._preempt: set = set()
+        self._last_rebalance = -float("inf")
+        self.rebalances = 0
+        self._build(slots)
         self.memory = {"free_bytes_at_start": int(free), "total_bytes": int(total),
                        "budget_bytes": self.budget, "workspace_bytes": self.batch.workspace_bytes,
-                       "slots": len(contexts)}
+                       "slots": len(self.slot_key)}
+
+    # ---- capacity ------------------------------------------------------------
+    def slot_bytes(self, key) -> int:
+        """Device bytes one slot of class ``key`` adds to the batch workspace."""
+        if key not in self._per_slot:
+            self._per_slot[key] = int(self._slot_bytes_fn(self.templates[key]))
+        return self._per_slot[key]
+
+    def _allocate(self, weights: Dict[Tuple, float], floor: Dict[Tuple, int], budget: int) -> Dict[Tuple, int]:
+        """Slots per class: ``floor`` (at least one per weighted class), then one
+        at a time to the class with the fewest slots per unit of weight, while
+        the workspace fits in ``budget`` and a class holds at most max_slots."""
+        keys = [k for k in self.keys if weights.get(k, 0.0) > 0 or floor.get(k, 0) > 0]
+        slots = {k: max(1, floor.get(k, 0)) for k in keys}
+        used = sum(self.slot_bytes(k) * n for k, n in slots.items())
+        if used > budget:
+            raise RuntimeError(f"the classes in use need {used} bytes; the budget is {budget}")
+        while True:
+            cand = [k for k in keys if slots[k] < self.max_slots and used + self.slot_bytes(k) <= budget]
+            if not cand:
+                break
+            k = min(cand, key=lambda c: slots[c] / max(weights.get(c, 0.0), 1e-12))
+            slots[k] += 1
+            used += self.slot_bytes(k)
+        return slots
+
+    def _build(self, slots: Dict[Tuple, int]) -> None:
+        """A new batch holding ``slots[k]`` slots of each class (empty)."""
+        self.slots_per_class = {k: n for k, n in slots.items() if n > 0}
+        contexts, self.slot_key = [], []
+        for k in self.keys:
+            for _ in range(self.slots_per_class.get(k, 0)):
+                contexts.append(self.templates[k])
+                self.slot_key.append(k)
+        self.batch = self._batch_factory(contexts, self.precision)
+        self.free = {k: deque(i for i, kk in enumerate(self.slot_key) if kk == k) for k in self.keys}
+
+    def _rebalance(self, queue: List[Request], now: float) -> bool:
+        """Re-divide the memory budget among the classes by demand and move
+        every request in flight into the new batch with its state."""
+        demand = {k: 0.0 for k in self.keys}
+        active_n = {k: 0 for k in self.keys}
+        for r in self._active.values():
+            demand[r.key] += 1.0
+            active_n[r.key] += 1
+        for r in queue:
+            demand[r.key] += 1.0
+        free, _ = self._mem_info()
+        budget = int(self.memory_fraction * (free + self.batch.workspace_bytes))
+        try:
+            slots = self._allocate(demand, active_n, budget)
+        except RuntimeError:
+            return False
+        if slots == self.slots_per_class:
+            return False
+        states = {}
+        for s, r in list(self._active.items()):
+            states[id(r)] = (r, self.batch.export_slot(s), self._done_steps[s])
+        self.batch.synchronize()
+        self.batch.close()
+        self._build(slots)
+        self._active, self._done_steps = {}, {}
+        for r, st, done in states.values():
+            slot = self.free[r.key].popleft()
+            self.batch.import_slot(slot, st, r._dev_table)
+            r.slot = slot
+            self._active[slot] = r
+            self._done_steps[slot] = done
+        self.budget = budget
+        self.memory.update(budget_bytes=budget, workspace_bytes=self.batch.workspace_bytes,
+                           slots=len(self.slot_key))
+        self.rebalances += 1
+        return True
+
+    def _short_of_slots(self, queue: List[Request]) -> bool:
+        """Some class has more requests waiting than free slots."""
+        need: Dict[Tuple, int] = {}
+        for r in queue:
+            need[r.key] = need.get(r.key, 0) + 1
+        return any(n > len(self.free[k]) for k, n in need.items())
+
+    def _add_class(self, req: Request) -> None:
+        """Adaptive mode: a request of a new class brings its class (its
+        context, without the laser path, is the template)."""
+        tpl = copy.copy(req.context)
+        tpl.laser_path = None
+        self.keys.append(req.key)
+        self.templates[req.key] = tpl
+        self.free[req.key] = deque()
 
     # ---- one request -------------------------------------------------------
     def _device_table(self, req: Request):
@@ -181,7 +277,14 @@ class ServingEngine:
             return False
         slot = fr.popleft()
         table = self._device_table(req)
-        self.batch.start(slot, req.steps, table=table, record=False)
+        resume = getattr(req, "_resume", None)
+        if resume is not None:  # a preempted request continues where it stopped
+            self.batch.import_slot(slot, resume, table)
+            req._resume = None
+            self._done_steps_pending = resume["step"]
+        else:
+            self.batch.start(slot, req.steps, table=table, record=False)
+            self._done_steps_pending = 0
         req.slot, req.admitted, req.status = slot, now, "running"
         req._dev_table = table  # keep the device table alive while the slot runs
         self.stats.admitted += 1
@@ -200,6 +303,12 @@ class ServingEngine:
         req.status = "done"
         self.free[req.key].append(req.slot)
         self.stats.completed += 1
+
+    def preempt(self, req: Request) -> None:
+        """Take ``req`` out of its slot at the next chunk boundary of
+        :meth:`run` and queue it again with its state (modes and warm start);
+        it resumes, bit for bit, when a slot of its class is free."""
+        self._preempt.add(id(req))
 
     def cancel(self, req: Request) -> None:
         """Stop ``req`` (queued or running) at the next chunk boundary of
@@ -220,7 +329,9 @@ class ServingEngine:
 
     def _check_classes(self, requests: Sequence[Request]) -> None:
         for r in requests:
-            if r.key not in self.free:
+            if r.key not in self.free and self.adaptive:
+                self._add_class(r)
+            elif r.key not in self.free:
                 declared = ", ".join(map(str, self.keys))
                 raise ValueError(f"request {r.id} is of class {r.key!r}, for which this engine holds "
                                  f"no slots (declared classes: {declared}); create the engine with "
@@ -277,12 +388,29 @@ class ServingEngine:
                     else:
                         kept.append(r)
                 queue = kept
+            # preemption: export the state, free the slot, queue again
+            for s, r in list(active.items()):
+                if id(r) in self._preempt:
+                    self._preempt.discard(id(r))
+                    r._resume = self.batch.export_slot(s)
+                    self.batch.stop(s)
+                    self.free[r.key].append(s)
+                    active.pop(s)
+                    done_steps.pop(s)
+                    r.status = "queued"
+                    r.preempted = getattr(r, "preempted", 0) + 1
+                    queue.insert(0, r)
+            if (self.adaptive and queue and now - self._last_rebalance >= self.rebalance_interval
+                    and self._short_of_slots(queue)):
+                self._last_rebalance = now
+                if self._rebalance(queue, now):
+                    active, done_steps = self._active, self._done_steps
             if queue:
                 still = []
                 for r in queue:
                     if self._admit(r, now):
                         active[r.slot] = r
-                        done_steps[r.slot] = 0
+                        done_steps[r.slot] = self._done_steps_pending
                     else:
                         still.append(r)
                 queue = still

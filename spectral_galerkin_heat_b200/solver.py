@@ -238,13 +238,15 @@ class B200SpectralSolver(HeatSolver):
     products on the tensor cores (tcgen05, FP32 accumulation) and keeps the
     modal iterates rounded to FP32; the latent source across the
     solidus-liquidus band, the property correction, the face fluxes, the
-    Picard norms and the coefficient tables stay FP64."""
+    Picard norms and the coefficient tables stay FP64. ``precision="fp32"``
+    is the same with FP32 contractions on the CUDA cores (the FP32 arm of the
+    precision study)."""
 
     def __init__(self, backend=None, context=None, *, mixing_omega=None,
                  convergence_tol=None, max_picard_iter=None, device=None, axis_min_ctas=None,
                  axis_cuda_cores=None, precision: str = "fp64"):
-        if precision not in _lib.PRECISION:
-            raise ValueError(f"precision must be one of {sorted(_lib.PRECISION)}")
+        if precision not in _lib.PLAN_PRECISION:
+            raise ValueError(f"precision must be one of {sorted(_lib.PLAN_PRECISION)}")
         self.precision = precision
         self.backend = backend
         self.context = context
@@ -298,7 +300,7 @@ class B200SpectralSolver(HeatSolver):
         self._resolve_picard_params(np.float64)
         cfg = make_config(ctx, float(self.mixing_omega), float(self.convergence_tol),
                           self.max_picard_iter)
-        cfg.precision = _lib.PRECISION[self.precision]
+        cfg.precision = _lib.PLAN_PRECISION[self.precision]
         policy = self.axis_min_ctas
         if policy is None:
             from .autotune import lookup

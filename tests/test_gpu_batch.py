@@ -202,3 +202,35 @@ def test_every_tile_policy_gives_the_same_result(precision):
         for k in range(steps):
             o.step(k * ctx.num.dt, ctx.num.dt)
         assert rel_l2(modes[0][i], o.a) < tol
+
+
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_slot_export_import_resumes_bit_for_bit(precision):
+    """A request exported after some steps and resumed in another batch (a
+    different slot, another slot mix) ends with the same bits as the same
+    request run through without a stop."""
+    from spectral_galerkin_heat_b200.batch import BatchSolver
+    steps, cut = 10, 4
+    ctx = _ctx(48, 24, 16, seed=3, steps=steps)
+    other = _ctx(32, 16, 8, seed=4, steps=steps)
+    ref = BatchSolver([ctx], precision)
+    ref.start(0, steps)
+    ref.step(steps)
+    want = ref.modes(0).double().cpu().numpy()
+    a = BatchSolver([other, ctx], precision)
+    a.start(1, steps)
+    a.step(cut)
+    state = a.export_slot(1)
+    assert state["step"] == cut and state["n_steps"] == steps
+    table = a._tables[1]
+    a.close()
+    b = BatchSolver([ctx, other, ctx], precision)
+    b.start(1, steps)                 # a neighbour running alongside
+    b.import_slot(2, state, table)
+    b.step(steps - cut)
+    info = b.status()[2]
+    assert info.step == steps and not info.active
+    assert np.array_equal(b.modes(2).double().cpu().numpy(), want)
+    assert b.tensor_core_error() == 0
+    b.close()
+    ref.close()

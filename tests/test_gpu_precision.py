@@ -24,3 +24,7 @@ def test_precision_report_small_case():
     assert last["melt_pool"]["length"] > 0 and last["melt_pool"]["depth"] > 0
     assert all(abs(v) <= 1e-6 for v in last["melt_pool_err_m"].values())
     assert rep[-1]["fp64_fp32_rounded"]["rel_l2"] < 1e-5
+    # the FP32 arm (FP32 CUDA-core contractions, FP32 modal iterates)
+    for r in rep:
+        assert r["fp32"]["rel_l2"] < 1e-4
+        assert abs(r["fp32"]["peak_T_err_K"]) < 1.0

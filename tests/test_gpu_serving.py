@@ -109,3 +109,41 @@ def test_mixed_serving_error_vs_fp64_oracle():
             o.step(k * dt, dt)
         assert rel_l2(r.modes.double().cpu().numpy(), o.a) < 1e-4
     eng.close()
+
+
+def test_preempted_request_resumes_bit_for_bit():
+    """A request taken out of its slot and queued again (its modes and warm
+    start exported to the device and imported into the next free slot) ends
+    with the same bits as run alone without a stop."""
+    from spectral_galerkin_heat_b200.serving import ServingEngine
+    stream = _stream(n=4, seed=11)
+    eng = ServingEngine(_classes(stream), precision="mixed", slots={m: 1 for m in MESHES},
+                        keep_modes=True, max_chunk=5)
+    reqs = _requests(stream)
+    eng.preempt(reqs[0])
+    eng.run(reqs, realtime=False)
+    assert reqs[0].preempted == 1 and all(r.status == "done" for r in reqs)
+    for r in reqs:
+        assert np.array_equal(r.modes.cpu().numpy(), _alone(r, "mixed").cpu().numpy()), r.id
+    eng.close()
+
+
+def test_adaptive_engine_plans_capacity_by_free_memory():
+    """An adaptive engine declared with one class only: requests of the other
+    classes bring their classes, the engine re-plans its slots by demand
+    within its memory budget and moves requests in flight into the new batch
+    with their state; every result is the same as alone."""
+    from spectral_galerkin_heat_b200.serving import ServingEngine
+    stream = _stream(n=9, seed=12)
+    first = MESHES[0]
+    eng = ServingEngine({first: _classes(stream)[first]}, precision="mixed", slots={first: 1},
+                        keep_modes=True, adaptive=True, rebalance_interval=0.0, max_slots=3,
+                        max_chunk=7)
+    reqs = _requests(stream)
+    eng.run(reqs, realtime=False)
+    assert all(r.status == "done" for r in reqs)
+    assert eng.rebalances >= 1 and set(eng.slots_per_class) >= set(MESHES)
+    assert eng.batch.tensor_core_error() == 0
+    for r in reqs:
+        assert np.array_equal(r.modes.cpu().numpy(), _alone(r, "mixed").cpu().numpy()), r.id
+    eng.close()

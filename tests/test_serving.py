@@ -53,6 +53,17 @@ class FakeBatch:
     def stop(self, slot):
         self.st[slot].active = 0
 
+    def export_slot(self, slot):
+        st = self.st[slot]
+        return {"step": st.step, "n_steps": st.n_steps, "value": st.last.T_surface_max}
+
+    def import_slot(self, slot, state, table):
+        assert not self.st[slot].active, "slot reused while active"
+        st = self.st[slot]
+        st.active, st.step, st.n_steps = 1, state["step"], state["n_steps"]
+        st.last.T_surface_max = state["value"]
+        self.imports = getattr(self, "imports", 0) + 1
+
     def fetch(self, slot, name):
         return np.zeros(4)
 
@@ -183,3 +194,53 @@ def test_tensor_core_error_fails_requests_in_flight():
     with pytest.raises(RuntimeError, match="tensor-core"):
         eng.run(reqs, realtime=False)
     assert {r.status for r in reqs} <= {"failed", "done"} and any(r.status == "failed" for r in reqs)
+
+
+def test_preempted_request_resumes_and_completes_its_steps():
+    eng = _engine({"a": 1, "b": 1}, max_chunk=4)
+    reqs = _reqs([("a", 20), ("a", 6), ("b", 9)])
+    eng.preempt(reqs[0])          # taken out at the first chunk boundary, queued again
+    eng.run(reqs, realtime=False)
+    a0, a1, b0 = reqs
+    assert a0.status == "done" and a0.preempted == 1
+    assert a0.last["T_surface_max"] == 20          # the fake slot's step counter went on
+    assert eng.stats.slot_steps == 35 and eng.batch.imports >= 1
+    assert all(r.status == "done" for r in reqs)
+
+
+def _adaptive(slots, budget_slots, **kw):
+    """An adaptive engine on a fake device whose free memory is 2 x budget_slots
+    slots' worth minus what the engine's batch holds (the budget is half)."""
+    holder = {}
+
+    def mem_info():
+        used = holder["eng"].batch.workspace_bytes if "eng" in holder else 0
+        return 1000 * budget_slots * 2 - used, 10**9
+    eng = ServingEngine({k: object() for k in slots}, precision="mixed", slots=slots,
+                        batch_factory=FakeBatch, mem_info=mem_info,
+                        slot_bytes=lambda ctx: 1000, adaptive=True, rebalance_interval=0.0,
+                        memory_fraction=0.5, max_slots=8, **kw)
+    holder["eng"] = eng
+    return eng
+
+
+def test_adaptive_engine_admits_a_new_class_by_free_memory():
+    from types import SimpleNamespace
+    eng = _adaptive({"a": 2}, budget_slots=6)
+    reqs = _reqs([("a", 12), ("c", 7), ("c", 5), ("c", 9)])
+    for r in reqs:
+        r.context = SimpleNamespace(laser_path=None)
+    eng.run(reqs, realtime=False)
+    assert all(r.status == "done" for r in reqs)
+    assert "c" in eng.slots_per_class and eng.rebalances >= 1
+    assert sum(eng.slots_per_class.values()) <= 6 + 1   # budget: half of free + own workspace
+    assert eng.stats.slot_steps == 12 + 7 + 5 + 9
+
+
+def test_adaptive_engine_moves_idle_capacity_to_the_busy_class():
+    eng = _adaptive({"a": 4, "b": 1}, budget_slots=5)
+    reqs = _reqs([("a", 30)] + [("b", 10)] * 6)
+    eng.run(reqs, realtime=False)
+    assert all(r.status == "done" for r in reqs)
+    assert eng.rebalances >= 1 and eng.slots_per_class.get("b", 0) > 1
+    assert eng.stats.slot_steps == 30 + 60
