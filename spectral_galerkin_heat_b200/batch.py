@@ -22,7 +22,7 @@ import numpy as np
 from . import _lib
 from .solver import laser_struct, make_config
 
-__all__ = ["BatchSolver"]
+__all__ = ["BatchSolver", "LaneBatch"]
 
 
 def _torch_stream(stream):
@@ -47,11 +47,13 @@ class BatchSolver:
     """A bound batch of slots on one device."""
 
     def __init__(self, contexts: Sequence, precision: str = "fp64", device=None,
-                 policy: Optional[dict] = None):
+                 policy: Optional[dict] = None, stream=None):
         """``policy``: the kernels' tile policy, ``{"vol_unroll": 2 | 4 | 8,
         "vol_vec": 0 | 1 | 2 | 4}`` (0: the widest vector);
         None takes the autotuner's entry for this grid mix (``tuned.json`` or
-        ``SGH_TUNE_TABLE``) and the built-in default without one."""
+        ``SGH_TUNE_TABLE``) and the built-in default without one. ``stream``:
+        the CUDA stream of every launch and copy of this batch (default: the
+        device's current stream)."""
         import torch
         if precision not in _lib.PRECISION:
             raise ValueError(f"precision must be one of {sorted(_lib.PRECISION)}")
@@ -85,7 +87,7 @@ class BatchSolver:
         self.device = torch.device("cuda", torch.cuda.current_device()) if device is None \
             else torch.device(device)
         self.workspace = torch.empty(int(nbytes.value), dtype=torch.uint8, device=self.device)
-        self.stream = torch.cuda.current_stream(self.device)
+        self.stream = torch.cuda.current_stream(self.device) if stream is None else stream
         _lib.check("sgh_batch_bind", L.sgh_batch_bind(h, C.c_void_p(self.workspace.data_ptr()),
                                                       nbytes.value, self._s()))
         self._tables = [None] * self.n
@@ -277,3 +279,150 @@ class BatchSolver:
             self.close()
         except Exception:
             pass
+
+
+class LaneBatch:
+    """Several batches ("lanes") driven as one, each on its own CUDA stream.
+
+    The slots are dealt to the lanes class by class, so every lane holds a
+    share of each grid class. A step launches every lane's step graph on its
+    own stream before any is waited for, so the lanes run concurrently: while
+    one lane is in its latency-bound face transforms, another streams its
+    volume pass from HBM. Results do not depend on the lane count (each slot's
+    arithmetic is its own). The interface is BatchSolver's, with global slot
+    numbers."""
+
+    def __init__(self, contexts: Sequence, precision: str = "fp64", lanes: int = 2, device=None,
+                 policy: Optional[dict] = None):
+        import torch
+        self.contexts = list(contexts)
+        self.precision = precision
+        self.n = len(self.contexts)
+        lanes = max(1, min(int(lanes), self.n))
+        # deal the slots of each class round-robin over the lanes
+        by_key = {}
+        for i, c in enumerate(self.contexts):
+            key = (int(c.num.nx), int(c.num.ny), int(c.num.nz))
+            by_key.setdefault(key, []).append(i)
+        members = [[] for _ in range(lanes)]
+        turn = 0
+        for key in sorted(by_key):
+            for i in by_key[key]:
+                members[turn % lanes].append(i)
+                turn += 1
+        members = [m for m in members if m]
+        dev = torch.device("cuda", torch.cuda.current_device()) if device is None else torch.device(device)
+        self.lanes = []
+        self.where = [None] * self.n   # global slot -> (lane, local slot)
+        for li, m in enumerate(members):
+            st = torch.cuda.Stream(dev)
+            self.lanes.append(BatchSolver([self.contexts[i] for i in m], precision, device=dev,
+                                          policy=policy, stream=st))
+            for local, g in enumerate(m):
+                self.where[g] = (li, local)
+        self.policy = self.lanes[0].policy
+        self.stream = torch.cuda.current_stream(dev)
+        self.device = dev
+
+    def _l(self, slot):
+        li, local = self.where[slot]
+        return self.lanes[li], local
+
+    @property
+    def workspace_bytes(self) -> int:
+        return sum(b.workspace_bytes for b in self.lanes)
+
+    @property
+    def _cfgs(self):
+        out = [None] * self.n
+        for g, (li, local) in enumerate(self.where):
+            out[g] = self.lanes[li]._cfgs[local]
+        return out
+
+    def upload_table(self, records):
+        import torch
+        host = torch.from_numpy(np.ascontiguousarray(records).view(np.uint8)).pin_memory()
+        return host.to(self.device, non_blocking=True)
+
+    def start(self, slot, n_steps, t0=0.0, record=True, table=None):
+        b, local = self._l(slot)
+        b.stream.wait_stream(self.stream)   # the table was uploaded on the engine's stream
+        b.start(local, n_steps, t0=t0, record=record, table=table)
+
+    def stop(self, slot):
+        b, local = self._l(slot)
+        b.stop(local)
+
+    def step(self, n_steps: int = 1) -> None:
+        for b in self.lanes:               # every lane's graph is in flight before any wait
+            b.step(n_steps)
+
+    def step_eager(self) -> None:
+        for b in self.lanes:
+            b.step_eager()
+
+    def status(self):
+        infos = [b.status() for b in self.lanes]
+        return [infos[li][local] for li, local in self.where]
+
+    def buffer(self, slot, name):
+        b, local = self._l(slot)
+        return b.buffer(local, name)
+
+    def modes(self, slot):
+        return self.buffer(slot, "modes")
+
+    def fetch(self, slot, name):
+        b, local = self._l(slot)
+        self.stream.wait_stream(b.stream)
+        return b.fetch(local, name)
+
+    def snapshot(self, slot, name):
+        b, local = self._l(slot)
+        out = b.snapshot(local, name)
+        self.stream.wait_stream(b.stream)
+        return out
+
+    def export_slot(self, slot):
+        b, local = self._l(slot)
+        state = b.export_slot(local)
+        self.stream.wait_stream(b.stream)
+        return state
+
+    def import_slot(self, slot, state, table):
+        b, local = self._l(slot)
+        b.stream.wait_stream(self.stream)
+        b.import_slot(local, state, table)
+
+    def volume_pass(self):
+        # bracketed by the engine's stream, so events on it time every lane
+        for b in self.lanes:
+            b.stream.wait_stream(self.stream)
+        for b in self.lanes:
+            b.volume_pass()
+        for b in self.lanes:
+            self.stream.wait_stream(b.stream)
+
+    def active_modes(self) -> int:
+        return sum(b.active_modes() for b in self.lanes)
+
+    def synchronize(self):
+        for b in self.lanes:
+            b.synchronize()
+        self.stream.synchronize()
+
+    def tensor_core_error(self) -> int:
+        return max(b.tensor_core_error() for b in self.lanes)
+
+    def launch_counts(self):
+        pre, it, post = self.lanes[0].launch_counts()
+        k = len(self.lanes)
+        return pre * k, it * k, post * k
+
+    def metrics(self, slot):
+        b, local = self._l(slot)
+        return b.metrics(local)
+
+    def close(self):
+        for b in self.lanes:
+            b.close()

@@ -349,22 +349,12 @@ __global__ void __launch_bounds__(CT) kb_begin(BView v, cudaGraphConditionalHand
 }
 
 // q_las, P_laser partials and q_net = q_las - shift(q_evap_old) per slot
-// (solvers/spectral.py:273-306). The Gaussian beam factorises,
-// exp(-2 (ux^2 + uy^2)) = exp(-2 ux^2) exp(-2 uy^2), so in mixed-precision
-// batches a block first tabulates the column factors of its slot and the row
-// factors of the rows it covers in shared memory (one exp per column and per
-// row instead of one per element; a few ulps from the unfactorised form);
-// FP64 batches and other profiles evaluate the flux per element.
-constexpr int FB_MAX_COLS = 1024;  // column factors tabulated (wider faces: per element)
-constexpr int FB_MAX_ROWS = 160;   // row factors of one block (RB / 16 + 2 rows at nx >= 16)
-
+// (solvers/spectral.py:273-306).
 __global__ void __launch_bounds__(BT)
 kb_face_begin(BView v, double* q_las, double* q_net, const double* q_evold, double* part_las) {
   // RB elements per block (RPT per thread, consecutive across the block per
   // round); the four shift taps of U elements are gathered before their use
   __shared__ double sh[2 * (BT / 32)];
-  __shared__ double fx[FB_MAX_COLS];
-  __shared__ double fy[FB_MAX_ROWS];
   const int b = blockIdx.x;
   const int s = v.rblk_slot[b];
   const BSlot& sl = v.slot[s];
@@ -374,36 +364,17 @@ kb_face_begin(BView v, double* q_las, double* q_net, const double* q_evold, doub
   const double* f = q_evold + sl.face;
   const double I0 = st.I0, lx = st.laser.x, ly = st.laser.y, sx = st.shift_x, sy = st.shift_y;
   const int i0 = (b - sl.rblk0) * RB;
-  const int y_lo = i0 / nx, y_hi = min(ny - 1, (i0 + RB - 1) / nx);
-  // mixed precision only: FP64 batches keep the unfactorised exponential, so
-  // they stay equal to the single-instance plan to rounding
-  const bool table = v.xq != nullptr && !sl.cell_integrated && sl.order == 2.0 && nx <= FB_MAX_COLS &&
-                     (y_hi - y_lo + 1) <= FB_MAX_ROWS;
-  if (table) {
-    for (int x = threadIdx.x; x < nx; x += BT) {
-      const double ux = (((double)x + 0.5) * sl.dx - lx) / sl.r_x;
-      fx[x] = exp(-2.0 * (ux * ux));
-    }
-    for (int y = y_lo + (int)threadIdx.x; y <= y_hi; y += BT) {
-      const double uy = (((double)y + 0.5) * sl.dy - ly) / sl.r_y;
-      fy[y - y_lo] = exp(-2.0 * (uy * uy));
-    }
-    __syncthreads();
-  }
   double sum = 0.0, dummy = 0.0;
   constexpr int U = 4;
 #pragma unroll 1
   for (int u0 = 0; u0 < RPT; u0 += U) {
     double g[U][4], wy0[U], wy1[U], wx0[U], wx1[U];
-    int xs[U], ys[U];
     bool ok[U], in[U];
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       const int i = i0 + (u0 + u) * BT + threadIdx.x;
       ok[u] = i < sl.S;
       const int y = ok[u] ? i / nx : 0, x = ok[u] ? i - y * nx : 0;
-      xs[u] = x;
-      ys[u] = y;
       const ShiftTap ty = shift_tap(y, ny, sy);
       const ShiftTap tx = shift_tap(x, nx, sx);
       in[u] = ok[u] && ty.in && tx.in;
@@ -418,14 +389,9 @@ kb_face_begin(BView v, double* q_las, double* q_net, const double* q_evold, doub
       const int i = i0 + (u0 + u) * BT + threadIdx.x;
       double qn = 0.0;
       if (ok[u]) {
-        const int y = ys[u], x = xs[u];
-        double q;
-        if (table) {
-          q = I0 * (fx[x] * fy[y - y_lo]);
-        } else {
-          const double xc = ((double)x + 0.5) * sl.dx, yc = ((double)y + 0.5) * sl.dy;
-          q = laser_flux(sl, I0, lx, ly, xc, yc);
-        }
+        const int y = i / nx, x = i - y * nx;
+        const double xc = ((double)x + 0.5) * sl.dx, yc = ((double)y + 0.5) * sl.dy;
+        const double q = laser_flux(sl, I0, lx, ly, xc, yc);
         q_las[sl.face + i] = q;
         sum += q;
         // the bilinear shift (spectral_cpu_kernels.py:328-371), zero outside the grid

@@ -54,6 +54,7 @@ class plan.
 from __future__ import annotations
 
 import copy
+import functools
 import time
 from collections import deque
 from dataclasses import dataclass, field
@@ -61,7 +62,7 @@ from typing import Callable, Dict, List, Optional, Sequence, Tuple
 
 import numpy as np
 
-from .batch import BatchSolver
+from .batch import BatchSolver, LaneBatch
 from .laser import laser_table
 
 __all__ = ["Request", "ServingEngine", "latency_percentiles"]
@@ -123,7 +124,10 @@ class ServingEngine:
 
     ``classes`` maps a class key to a template context (its laser path is not
     used) and ``weights`` gives each class's expected share of the device
-    memory demand (default: equal). Slot capacity: starting from one slot per
+    memory demand (default: equal). ``lanes`` > 1 splits the slots over that
+    many batches on their own CUDA streams, stepped concurrently
+    (:class:`LaneBatch`), so one lane's latency-bound face transforms overlap
+    another's bandwidth-bound volume pass. Slot capacity: starting from one slot per
     class, slots go to the class with the lowest slots/weight ratio while the
     batch workspace fits in ``memory_fraction`` of the free device memory and
     stays within ``max_slots`` slots per class.
@@ -135,12 +139,15 @@ class ServingEngine:
                  keep_modes: bool = False, max_chunk: int = 64,
                  batch_factory: Optional[Callable] = None, mem_info: Optional[Callable] = None,
                  slot_bytes: Optional[Callable] = None, adaptive: bool = False,
-                 rebalance_interval: float = 1.0):
+                 rebalance_interval: float = 1.0, lanes: int = 1):
         if batch_factory is None:
             import torch
             if not torch.cuda.is_available():
                 raise RuntimeError("ServingEngine needs a CUDA device (no CPU fallback)")
-            batch_factory = BatchSolver
+            if int(lanes) > 1:
+                batch_factory = functools.partial(LaneBatch, lanes=int(lanes))
+            else:
+                batch_factory = BatchSolver
             mem_info = mem_info or torch.cuda.mem_get_info
         self._slot_bytes_fn = slot_bytes or (lambda ctx: BatchSolver.workspace_bytes_for([ctx], precision))
         self._batch_factory = batch_factory

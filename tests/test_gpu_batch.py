@@ -234,3 +234,26 @@ def test_slot_export_import_resumes_bit_for_bit(precision):
     assert b.tensor_core_error() == 0
     b.close()
     ref.close()
+
+
+def test_lanes_give_the_same_bits_as_one_batch():
+    """Slots dealt to two batches on their own streams and stepped
+    concurrently end with the same bits as in one batch."""
+    from spectral_galerkin_heat_b200.batch import BatchSolver, LaneBatch
+    steps = 7
+    ctxs = [_ctx(*sh, seed=20 + i, steps=steps) for i, sh in enumerate(SHAPES + SHAPES)]
+    one = BatchSolver(ctxs, "mixed")
+    two = LaneBatch(ctxs, "mixed", lanes=2)
+    assert len(two.lanes) == 2
+    for b in (one, two):
+        for i in range(len(ctxs)):
+            b.start(i, steps, record=False)
+        b.step(3)
+        b.step(steps - 3)
+        assert b.tensor_core_error() == 0
+    info = two.status()
+    assert all(x.step == steps and not x.active for x in info)
+    for i in range(len(ctxs)):
+        assert np.array_equal(one.modes(i).cpu().numpy(), two.modes(i).cpu().numpy())
+    one.close()
+    two.close()

@@ -147,3 +147,18 @@ def test_adaptive_engine_plans_capacity_by_free_memory():
     for r in reqs:
         assert np.array_equal(r.modes.cpu().numpy(), _alone(r, "mixed").cpu().numpy()), r.id
     eng.close()
+
+
+def test_serving_lanes_same_result_as_alone():
+    """A two-lane engine (two batches on their own streams, stepped
+    concurrently) serves every request with the bits it has alone."""
+    from spectral_galerkin_heat_b200.serving import ServingEngine
+    stream = _stream(n=8, seed=13)
+    eng = ServingEngine(_classes(stream), precision="mixed", slots={m: 2 for m in MESHES},
+                        keep_modes=True, lanes=2)
+    reqs = _requests(stream)
+    eng.run(reqs, realtime=False)
+    assert all(r.status == "done" for r in reqs)
+    for r in reqs:
+        assert np.array_equal(r.modes.cpu().numpy(), _alone(r, "mixed").cpu().numpy()), r.id
+    eng.close()
