@@ -509,21 +509,28 @@ inline void launch_pdl(void (*kernel)(KArgs...), dim3 grid, int threads, int sme
 
 // ---------------------------------------------------------------------------
 // Split-BF16 tensor-core variant (tcgen05, the mixed-precision plans). One CTA
-// of 128 threads computes out[c][k] for 128 columns c (the MMA's M; TMEM lane
-// = column) and NT outputs k of the transformed axis (the MMA's N; TMEM column
-// = output): D[c][k] = sum_n X(c, n) Mat[k][n]. Both operands are split into
-// BF16 hi + lo while the threads stage them into shared memory (K-major, no
-// swizzle, 8 x 8 core matrices), two stages deep over 32-slice chunks; per
-// 16-slice step one thread issues the three products hi.hi, hi.lo, lo.hi,
-// accumulating in FP32 in tensor memory. The epilogue reads each thread's
-// column from tensor memory and hands the values to the same epilogue
-// functors as the FP64 kernels. Every mbarrier wait is bounded: on expiry
-// the CTA sets *err, waits (bounded) for its MMAs, writes NaN partials so
-// the Picard test stops, frees its tensor memory and returns without results.
+// of 128 threads computes D[k][c] = sum_n Mat[k][n] X(c, n) for 128 outputs k
+// of the transformed axis (the MMA's M; TMEM lane = output) and NC columns c
+// (the MMA's N; TMEM column = column), so every column is read once per
+// 128 outputs. The matrix operand arrives split into BF16 hi + lo: from the
+// plan's pair plane of that matrix (one 16 KB bulk copy per 32-slice chunk,
+// completing on the stage's mbarrier), or, for a matrix without a plane,
+// split by the threads. The column operand is copied raw (FP64) by cp.async
+// into a ring of S stages -- every thread copies and later splits the same
+// elements -- and split into the MMA stage of the same index. Per 16-slice
+// step one thread issues hi.hi, hi.lo, lo.hi, accumulating in FP32 in tensor
+// memory. Contiguous passes (B == 1) hand each thread's output row to the
+// epilogue straight from tensor memory (lanes = consecutive outputs of one
+// column, so stores coalesce); strided passes transpose through shared memory
+// so that consecutive threads take consecutive columns. Every mbarrier wait
+// is bounded: on expiry the CTA sets *err, waits (bounded) for its bulk
+// copies and MMAs in flight, writes NaN partials so the Picard test stops,
+// frees its tensor memory and returns without results.
 // ---------------------------------------------------------------------------
 constexpr int AXU_THREADS = 128;
-constexpr int AXU_M = 128;  // columns per CTA
-constexpr int AXU_KC = 32;  // contraction slices per stage
+constexpr int AXU_M = 128;                            // outputs per CTA
+constexpr int AXU_KC = 32;                            // contraction slices per stage
+constexpr int AXU_ABYTES = 2 * AXU_M * AXU_KC * 2;    // matrix hi + lo of one stage (16 KB)
 // Whether passes run on the split-BF16 tensor-core kernel (mixed-precision
 // plans), and where that kernel records an expired wait.
 inline thread_local bool g_axis_umma = false;
@@ -531,42 +538,83 @@ inline thread_local int* g_umma_err = nullptr;
 // Whether passes run the CUDA-core kernel in FP32 arithmetic (FP32 plans).
 inline thread_local bool g_axis_fp32 = false;
 
-template <int NT>
-__host__ __device__ constexpr int axu_stage_bytes() { return 2 * AXU_M * AXU_KC * 2 + 2 * NT * AXU_KC * 2; }
-template <int NT>
-__host__ __device__ constexpr int axu_smem_bytes() { return 2 * axu_stage_bytes<NT>() + 64; }
-// Output tile NT of a pass: the smallest of 32..256 covering Nout, narrowed
-// (more CTAs, each re-staging its columns' operands) until the pass fills the
-// SMs or NT reaches 32.
-inline int axu_nt(int Nout, int ncol) {
-  int nt = Nout <= 32 ? 32 : (Nout <= 64 ? 64 : (Nout <= 128 ? 128 : 256));
-  constexpr long kSms = 148;  // one wave at one CTA per SM
-  const long col_tiles = (ncol + AXU_M - 1) / AXU_M;
-  while (nt > 32 && col_tiles * ((Nout + nt - 1) / nt) < kSms) nt /= 2;
-  return nt;
+// A matrix of a plan with its BF16 pair plane (umma::pair_off<128> layout,
+// rows and slices beyond the matrix zero): passes whose Mat is listed here
+// with the same contraction length and no more outputs than rows stream
+// the matrix operand from the plane.
+struct UmmaPlane {
+  const double* mat;
+  const char* pair;
+  int rows, k;
+};
+inline thread_local const UmmaPlane* g_umma_planes = nullptr;
+inline thread_local int g_umma_nplanes = 0;
+inline const char* umma_plane_for(const double* Mat, int Nout, int N) {
+  for (int i = 0; i < g_umma_nplanes; ++i) {
+    const UmmaPlane& q = g_umma_planes[i];
+    if (q.mat == Mat && q.k == N && Nout <= q.rows) return q.pair;
+  }
+  return nullptr;
 }
 
-template <bool CONTIG, int NT, class Epi>
+template <int NC>
+__host__ __device__ constexpr int axu_stages() { return NC >= 64 ? 3 : 4; }
+template <int NC>
+__host__ __device__ constexpr int axu_bbytes() { return 2 * NC * AXU_KC * 2; }  // column operand hi + lo
+template <int NC>
+__host__ __device__ constexpr int axu_rbytes() { return NC * AXU_KC * 8; }      // raw FP64 columns
+template <int NC>
+__host__ __device__ constexpr int axu_stage_bytes() { return AXU_ABYTES + axu_bbytes<NC>() + axu_rbytes<NC>(); }
+template <int NC>
+__host__ __device__ constexpr int axu_smem_bytes() { return axu_stages<NC>() * axu_stage_bytes<NC>() + 128; }
+// Column tile NC of a pass: the widest of 64, 32, 16 that still gives one
+// wave of CTAs (one per SM), else 16.
+inline int axu_nc(int Nout, int ncol) {
+  constexpr long kSms = 148;
+  const long mt = (Nout + AXU_M - 1) / AXU_M;
+  int nc = 64;
+  while (nc > 16 && mt * ((ncol + nc - 1) / nc) < kSms) nc /= 2;
+  return nc;
+}
+
+// Builds the pair plane of an rows x k matrix (row-major, Mat[r * k + n]).
+static __global__ void k_pair_plane(const double* __restrict__ M, int rows, int k, char* __restrict__ pair) {
+  const int nkc = (k + AXU_KC - 1) / AXU_KC, kpad = nkc * AXU_KC;
+  const long n = (long)((rows + AXU_M - 1) / AXU_M) * AXU_M * kpad;
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < n; e += (long)gridDim.x * blockDim.x) {
+    const int r = (int)(e / kpad), kk = (int)(e % kpad);
+    const double x = (r < rows && kk < k) ? M[(size_t)r * k + kk] : 0.0;
+    umma::pair_put<AXU_M>(pair, r, kk, nkc, x);
+  }
+}
+
+template <bool CONTIG, int NC, class Epi>
 __global__ void __launch_bounds__(AXU_THREADS)
-k_axis_umma(const double* __restrict__ X, const double* __restrict__ Mat, int Nout, int N, int A, int B,
-            Epi epi, int* err) {
+k_axis_umma(const double* __restrict__ X, const double* __restrict__ Mat, const char* __restrict__ pair,
+            int Nout, int N, int A, int B, Epi epi, int* err) {
   using namespace umma;
   extern __shared__ __align__(128) char axu_sh[];
   __shared__ double red_sh[2 * (AXU_THREADS / 32)];
-  constexpr int XB = AXU_M * AXU_KC * 2, MB = NT * AXU_KC * 2, STAGE = 2 * XB + 2 * MB;
-  constexpr uint32_t NCOLS = NT;  // 32, 64, 128 or 256 FP32 accumulator columns
+  constexpr int S = axu_stages<NC>(), BH = NC * AXU_KC * 2, STAGE = axu_stage_bytes<NC>();
+  constexpr int PER = NC * AXU_KC / AXU_THREADS;  // column values per thread and chunk: 4 .. 16
+  constexpr uint32_t NCOLS = NC < 32 ? 32 : NC;
   asm volatile("griddepcontrol.wait;\n" ::: "memory");
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int ncol = A * B;
-  const int c0 = blockIdx.x * AXU_M, k0 = blockIdx.y * NT;
-  uint64_t* bars = reinterpret_cast<uint64_t*>(axu_sh + 2 * STAGE);
-  uint32_t* tslot = reinterpret_cast<uint32_t*>(axu_sh + 2 * STAGE + 16);
-  volatile int* okflag = reinterpret_cast<volatile int*>(axu_sh + 2 * STAGE + 32);
-  const uint32_t idesc = idesc_bf16_f32(AXU_M, NT);
+  const int c0 = blockIdx.x * NC, k0 = blockIdx.y * AXU_M;
+  uint64_t* full = reinterpret_cast<uint64_t*>(axu_sh + S * STAGE);
+  uint64_t* empty = full + S;
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(axu_sh + S * STAGE + 64);
+  volatile int* okflag = reinterpret_cast<volatile int*>(axu_sh + S * STAGE + 72);
+  const uint32_t idesc = idesc_bf16_f32(AXU_M, NC);
+  const int nchunks = (N + AXU_KC - 1) / AXU_KC;
+  const bool planed = pair != nullptr;
   if (warp == 0) tmem_alloc(tslot, NCOLS);
   if (tid == 0) {
-    mbar_init(&bars[0], 1);
-    mbar_init(&bars[1], 1);
+    for (int s = 0; s < S; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
     *okflag = 1;
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
@@ -575,102 +623,137 @@ k_axis_umma(const double* __restrict__ X, const double* __restrict__ Mat, int No
   tc_fence_after();
   const uint32_t tmem = *tslot;
 
-  // this thread's staged X column: CONTIG, rows warp + 4 j at slice lane;
-  // otherwise column tid at every slice of the chunk
-  size_t xcol = 0;
-  bool xok = false;
-  if (!CONTIG) {
-    const int c = c0 + tid;
-    xok = c < ncol;
-    const int cc = xok ? c : 0;
-    const int a = cc / B, b = cc - a * B;
-    xcol = (size_t)a * N * B + b;
-  }
-  const int nchunks = (N + AXU_KC - 1) / AXU_KC;
-  uint32_t phase[2] = {0u, 0u};
+  // element e = tid + i * 128 of a chunk: column j, slice nl; the raw ring
+  // holds it at 8 e (contiguous passes: [column][slice], a warp copies 32
+  // consecutive slices of a column; strided: [slice][column], consecutive
+  // threads copy consecutive columns)
+  auto elem = [&](int e, int& j, int& nl) {
+    if (CONTIG) {
+      j = e / AXU_KC;
+      nl = e % AXU_KC;
+    } else {
+      nl = e / NC;
+      j = e % NC;
+    }
+  };
+  auto issue_raw = [&](int ch) {  // one commit group per chunk (empty past the end)
+    if (ch < nchunks) {
+      char* raw = axu_sh + (ch % S) * STAGE + AXU_ABYTES + 2 * BH;
+      const int n0 = ch * AXU_KC;
+#pragma unroll
+      for (int i = 0; i < PER; ++i) {
+        const int e = tid + i * AXU_THREADS;
+        int j, nl;
+        elem(e, j, nl);
+        const int c = c0 + j, n = n0 + nl;
+        const bool in = c < ncol && n < N;
+        size_t off = 0;
+        if (in) {
+          if (CONTIG) {
+            off = (size_t)c * N + n;
+          } else {
+            const int a = c / B, b = c - a * B;
+            off = (size_t)a * N * B + (size_t)n * B + b;
+          }
+        }
+        cp_async8(raw + 8 * e, X + off, in ? 8 : 0);
+      }
+    }
+    cp_async_commit();
+  };
+  auto issue_a = [&](int ch) {  // thread 0: the matrix chunk ch from the plane
+    const int s = ch % S;
+    mbar_expect_tx(&full[s], AXU_ABYTES);
+    bulk_g2s(axu_sh + s * STAGE, pair + ((size_t)blockIdx.y * nchunks + ch) * AXU_ABYTES, AXU_ABYTES, &full[s]);
+  };
+
+  // thread 0's bookkeeping: matrix chunks copied (a_next) and consumed
+  // (a_done), and the last chunk whose MMAs were committed
+  int a_next = 0, a_done = 0, last_commit = -1;
+  for (int ch = 0; ch < S; ++ch) issue_raw(ch);
+  if (planed && tid == 0)
+    for (; a_next < S && a_next < nchunks; ++a_next) issue_a(a_next);
   bool ok = true;
   for (int ch = 0; ch < nchunks; ++ch) {
-    const int s = ch & 1;
-    if (ch >= 2) {  // stage s was read by the MMAs of chunk ch - 2
-      if (tid == 0 && !mbar_wait_bounded(&bars[s], phase[s])) *okflag = 0;
-      phase[s] ^= 1u;
-      __syncthreads();
-      if (!*okflag) {
-        ok = false;
-        break;
-      }
-    }
+    const int s = ch % S;
     char* st = axu_sh + s * STAGE;
+    cp_async_wait<S - 1>();  // this thread's copies of chunk ch have landed
+    __syncthreads();         // thread 0 saw the MMAs of chunk ch - S complete
+    if (!*okflag) {
+      ok = false;
+      break;
+    }
     const int n0 = ch * AXU_KC;
-    // every load of a group is issued before the first split, so a thread
-    // keeps 16 operand values in flight
-    constexpr int G = 16;
-#pragma unroll
-    for (int j0 = 0; j0 < AXU_KC; j0 += G) {  // X: 32 values per thread
-      double xv[G];
-#pragma unroll
-      for (int j = 0; j < G; ++j) {
-        if (CONTIG) {
-          const int r = warp + 4 * (j0 + j), c = c0 + r, n = n0 + lane;
-          xv[j] = (c < ncol && n < N) ? __ldg(X + (size_t)c * N + n) : 0.0;
-        } else {
-          const int n = n0 + j0 + j;
-          xv[j] = (xok && n < N) ? __ldg(X + xcol + (size_t)n * B) : 0.0;
-        }
-      }
-#pragma unroll
-      for (int j = 0; j < G; ++j) {
+    if (!planed) {  // matrix rows k0.. of slices n0..: 32 values per thread
+#pragma unroll 8
+      for (int i = 0; i < AXU_M * AXU_KC / AXU_THREADS; ++i) {
+        const int e = tid + i * AXU_THREADS, r = e / AXU_KC, kl = e % AXU_KC;
+        const int k = k0 + r, n = n0 + kl;
+        const double x = (k < Nout && n < N) ? __ldg(Mat + (size_t)k * N + n) : 0.0;
         __nv_bfloat16 h, l;
-        split_bf16(xv[j], h, l);
-        const uint32_t o = CONTIG ? core_off(warp + 4 * (j0 + j), lane, AXU_M) : core_off(tid, j0 + j, AXU_M);
+        split_bf16(x, h, l);
+        const uint32_t o = core_off(r, kl, AXU_M);
         *reinterpret_cast<__nv_bfloat16*>(st + o) = h;
-        *reinterpret_cast<__nv_bfloat16*>(st + XB + o) = l;
+        *reinterpret_cast<__nv_bfloat16*>(st + AXU_ABYTES / 2 + o) = l;
       }
     }
-    constexpr int MPT = NT * AXU_KC / AXU_THREADS;  // Mat values per thread: 8 .. 64
-    constexpr int MG = MPT < G ? MPT : G;
+    {
+      const double* raw = reinterpret_cast<const double*>(st + AXU_ABYTES + 2 * BH);
+      double xv[PER];
 #pragma unroll
-    for (int j0 = 0; j0 < MPT; j0 += MG) {  // Mat rows k, slices n (n fastest)
-      double mv[MG];
+      for (int i = 0; i < PER; ++i) xv[i] = raw[tid + i * AXU_THREADS];
 #pragma unroll
-      for (int j = 0; j < MG; ++j) {
-        const int e = tid + (j0 + j) * AXU_THREADS;
-        const int k = k0 + e / AXU_KC, n = n0 + e % AXU_KC;
-        mv[j] = (k < Nout && n < N) ? __ldg(Mat + (size_t)k * N + n) : 0.0;
-      }
-#pragma unroll
-      for (int j = 0; j < MG; ++j) {
-        const int e = tid + (j0 + j) * AXU_THREADS;
+      for (int i = 0; i < PER; ++i) {
+        int j, nl;
+        elem(tid + i * AXU_THREADS, j, nl);
         __nv_bfloat16 h, l;
-        split_bf16(mv[j], h, l);
-        const uint32_t o = core_off(e / AXU_KC, e % AXU_KC, NT);
-        *reinterpret_cast<__nv_bfloat16*>(st + 2 * XB + o) = h;
-        *reinterpret_cast<__nv_bfloat16*>(st + 2 * XB + MB + o) = l;
+        split_bf16(xv[i], h, l);
+        const uint32_t o = core_off(j, nl, NC);
+        *reinterpret_cast<__nv_bfloat16*>(st + AXU_ABYTES + o) = h;
+        *reinterpret_cast<__nv_bfloat16*>(st + AXU_ABYTES + BH + o) = l;
       }
     }
+    issue_raw(ch + S);  // into the slot this thread just read
     fence_proxy_async();
     __syncthreads();
     if (tid == 0) {
-      tc_fence_after();
-      const uint32_t xh = smem_u32(st), xl = xh + XB, mh = xh + 2 * XB, ml = mh + MB;
-#pragma unroll
-      for (int q = 0; q < AXU_KC / 16; ++q) {
-        const uint32_t ao = (uint32_t)(2 * q * (AXU_M / 8) * 128), bo = (uint32_t)(2 * q * (NT / 8) * 128);
-        const uint64_t dxh = smem_desc(xh + ao, (AXU_M / 8) * 128, 128);
-        const uint64_t dxl = smem_desc(xl + ao, (AXU_M / 8) * 128, 128);
-        const uint64_t dmh = smem_desc(mh + bo, (NT / 8) * 128, 128);
-        const uint64_t dml = smem_desc(ml + bo, (NT / 8) * 128, 128);
-        const uint32_t acc = (ch > 0 || q > 0) ? 1u : 0u;
-        mma_bf16(tmem, dxh, dmh, idesc, acc);
-        mma_bf16(tmem, dxh, dml, idesc, 1u);
-        mma_bf16(tmem, dxl, dmh, idesc, 1u);
+      bool good = true;
+      if (planed) {
+        good = mbar_wait_bounded(&full[s], (uint32_t)((ch / S) & 1));
+        if (good) a_done = ch + 1;
       }
-      mma_commit(&bars[s]);
+      if (good) {
+        tc_fence_after();
+        const uint32_t ah = smem_u32(st), al = ah + AXU_ABYTES / 2, bh = ah + AXU_ABYTES, bl = bh + BH;
+#pragma unroll
+        for (int q = 0; q < AXU_KC / 16; ++q) {
+          const uint32_t ao = (uint32_t)(2 * q * (AXU_M / 8) * 128), bo = (uint32_t)(2 * q * (NC / 8) * 128);
+          const uint64_t dah = smem_desc(ah + ao, (AXU_M / 8) * 128, 128);
+          const uint64_t dal = smem_desc(al + ao, (AXU_M / 8) * 128, 128);
+          const uint64_t dbh = smem_desc(bh + bo, (NC / 8) * 128, 128);
+          const uint64_t dbl = smem_desc(bl + bo, (NC / 8) * 128, 128);
+          const uint32_t acc = (ch > 0 || q > 0) ? 1u : 0u;
+          mma_bf16(tmem, dah, dbh, idesc, acc);
+          mma_bf16(tmem, dah, dbl, idesc, 1u);
+          mma_bf16(tmem, dal, dbh, idesc, 1u);
+        }
+        mma_commit(&empty[s]);
+        last_commit = ch;
+        // stage (ch - 1) % S is reused by chunk ch - 1 + S: wait for the MMAs
+        // of chunk ch - 1 (issued an iteration ago), then refill its matrix
+        const int prev = ch - 1, next = ch - 1 + S;
+        if (prev >= 0 && next < nchunks) {
+          good = mbar_wait_bounded(&empty[prev % S], (uint32_t)((prev / S) & 1));
+          if (good && planed) issue_a(a_next++);
+        }
+      }
+      if (!good) *okflag = 0;
     }
   }
+  cp_async_wait<0>();
   if (ok && nchunks > 0) {  // the last commit covers every MMA before it
-    const int s = (nchunks - 1) & 1;
-    if (tid == 0 && !mbar_wait_bounded(&bars[s], phase[s])) *okflag = 0;
+    if (tid == 0 && !mbar_wait_bounded(&empty[(nchunks - 1) % S], (uint32_t)(((nchunks - 1) / S) & 1)))
+      *okflag = 0;
     __syncthreads();
     ok = *okflag != 0;
   }
@@ -678,24 +761,47 @@ k_axis_umma(const double* __restrict__ X, const double* __restrict__ Mat, int No
   if (!ok) {
     if (tid == 0) {
       if (err) atomicExch(err, 1);
-      for (int s = 0; s < 2; ++s) mbar_wait_bounded(&bars[s], phase[s]);  // drain, bounded
+      for (int c = a_done; c < a_next; ++c) mbar_wait_bounded(&full[c % S], (uint32_t)((c / S) & 1));
+      if (last_commit >= 0) mbar_wait_bounded(&empty[last_commit % S], (uint32_t)((last_commit / S) & 1));
     }
   } else {
     tc_fence_after();
-    const int c = c0 + warp * 32 + lane;
-    const bool cin = c < ncol;
-    const int cc = cin ? c : 0;
-    const int a = cc / B, b = cc - a * B;
-    const int base = CONTIG ? cc * Nout : a * Nout * B + b;
+    fence_proxy_async();
+    const int kl = warp * 32 + lane, k = k0 + kl;
+    const bool live = k0 + warp * 32 < Nout;  // warp-uniform
+    if (CONTIG) {
+      if (live) {
 #pragma unroll 1
-    for (int j0 = 0; j0 < NT; j0 += 16) {
-      float v[16];
-      tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)j0, v);
-      if (cin) {
+        for (int j0 = 0; j0 < NC; j0 += 16) {
+          float v[16];
+          tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)j0, v);
+          if (k < Nout) {
 #pragma unroll
-        for (int i = 0; i < 16; ++i) {
-          const int k = k0 + j0 + i;
-          if (k < Nout) epi(CONTIG ? base + k : base + k * B, k, b, (double)v[i], r);
+            for (int i = 0; i < 16; ++i) {
+              const int c = c0 + j0 + i;
+              if (c < ncol) epi(c * Nout + k, k, 0, (double)v[i], r);
+            }
+          }
+        }
+      }
+    } else {
+      float* T = reinterpret_cast<float*>(axu_sh);  // [128 outputs][NC + 1]
+      if (live) {
+#pragma unroll 1
+        for (int j0 = 0; j0 < NC; j0 += 16) {
+          float v[16];
+          tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)j0, v);
+#pragma unroll
+          for (int i = 0; i < 16; ++i) T[kl * (NC + 1) + j0 + i] = v[i];
+        }
+      }
+      __syncthreads();
+      const int rows = min(AXU_M, Nout - k0);
+      for (int e = tid; e < rows * NC; e += AXU_THREADS) {
+        const int kk = e / NC, j = e - kk * NC, c = c0 + j;
+        if (c < ncol) {
+          const int a = c / B, b = c - a * B, kq = k0 + kk;
+          epi(a * Nout * B + kq * B + b, kq, b, (double)T[kk * (NC + 1) + j], r);
         }
       }
     }
@@ -722,26 +828,27 @@ k_axis_umma(const double* __restrict__ X, const double* __restrict__ Mat, int No
   }
 }
 
-template <bool CONTIG, int NT, class Epi>
-inline void launch_axis_umma_nt(const double* X, const double* Mat, int Nout, int N, int A, int B, const Epi& epi,
-                                dim3 grid, cudaStream_t st) {
-  constexpr int bytes = axu_smem_bytes<NT>();
+template <bool CONTIG, int NC, class Epi>
+inline void launch_axis_umma_nc(const double* X, const double* Mat, const char* pair, int Nout, int N, int A,
+                                int B, const Epi& epi, dim3 grid, cudaStream_t st) {
+  constexpr int bytes = axu_smem_bytes<NC>();
   static const bool attr = [] {
-    cudaFuncSetAttribute(k_axis_umma<CONTIG, NT, Epi>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    cudaFuncSetAttribute(k_axis_umma<CONTIG, NC, Epi>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     return true;
   }();
   (void)attr;
-  launch_pdl(k_axis_umma<CONTIG, NT, Epi>, grid, AXU_THREADS, bytes, st, X, Mat, Nout, N, A, B, epi, g_umma_err);
+  launch_pdl(k_axis_umma<CONTIG, NC, Epi>, grid, AXU_THREADS, bytes, st, X, Mat, pair, Nout, N, A, B, epi,
+             g_umma_err);
 }
 
 template <bool CONTIG, class Epi>
 inline void launch_axis_umma(const double* X, const double* Mat, int Nout, int N, int A, int B, const Epi& epi,
                              dim3 grid, cudaStream_t st) {
-  switch (axu_nt(Nout, A * B)) {
-    case 32: launch_axis_umma_nt<CONTIG, 32>(X, Mat, Nout, N, A, B, epi, grid, st); break;
-    case 64: launch_axis_umma_nt<CONTIG, 64>(X, Mat, Nout, N, A, B, epi, grid, st); break;
-    case 128: launch_axis_umma_nt<CONTIG, 128>(X, Mat, Nout, N, A, B, epi, grid, st); break;
-    default: launch_axis_umma_nt<CONTIG, 256>(X, Mat, Nout, N, A, B, epi, grid, st); break;
+  const char* pair = umma_plane_for(Mat, Nout, N);
+  switch (axu_nc(Nout, A * B)) {
+    case 16: launch_axis_umma_nc<CONTIG, 16>(X, Mat, pair, Nout, N, A, B, epi, grid, st); break;
+    case 32: launch_axis_umma_nc<CONTIG, 32>(X, Mat, pair, Nout, N, A, B, epi, grid, st); break;
+    default: launch_axis_umma_nc<CONTIG, 64>(X, Mat, pair, Nout, N, A, B, epi, grid, st); break;
   }
 }
 
@@ -769,19 +876,23 @@ struct AxisPolicy {
   int saved;
   bool saved_mma, saved_umma, saved_fp32;
   int* saved_err;
+  const UmmaPlane* saved_planes;
+  int saved_nplanes;
   // umma: every pass on the split-BF16 tensor-core kernel (mixed-precision
   // plans); err: where that kernel records an expired wait (null while only
-  // sizing buffers)
+  // sizing buffers); planes: the plan's matrices with their BF16 pair planes
   // fp32: every pass on the CUDA-core kernel in FP32 arithmetic (FP32 plans)
   explicit AxisPolicy(int min_ctas, int cuda_cores_only = 0, bool umma = false, int* err = nullptr,
-                      bool fp32 = false)
+                      bool fp32 = false, const UmmaPlane* planes = nullptr, int nplanes = 0)
       : saved(g_axis_min_ctas), saved_mma(g_axis_mma), saved_umma(g_axis_umma), saved_fp32(g_axis_fp32),
-        saved_err(g_umma_err) {
+        saved_err(g_umma_err), saved_planes(g_umma_planes), saved_nplanes(g_umma_nplanes) {
     g_axis_min_ctas = min_ctas > 0 ? min_ctas : AX_MIN_CTAS;
     g_axis_mma = cuda_cores_only == 0 && !fp32;
     g_axis_umma = umma;
     g_axis_fp32 = fp32;
     g_umma_err = err;
+    g_umma_planes = planes;
+    g_umma_nplanes = planes ? nplanes : 0;
   }
   ~AxisPolicy() {
     g_axis_min_ctas = saved;
@@ -789,6 +900,8 @@ struct AxisPolicy {
     g_axis_umma = saved_umma;
     g_axis_fp32 = saved_fp32;
     g_umma_err = saved_err;
+    g_umma_planes = saved_planes;
+    g_umma_nplanes = saved_nplanes;
   }
 };
 
@@ -797,8 +910,8 @@ struct AxisPolicy {
 inline AxisShape axis_shape(int Nout, int A, int B) {
   const int ncol = A * B;
   if (g_axis_umma) {
-    const int nt = axu_nt(Nout, ncol);
-    return {true, dim3((ncol + AXU_M - 1) / AXU_M, (Nout + nt - 1) / nt), 6};
+    const int nc = axu_nc(Nout, ncol);
+    return {true, dim3((ncol + nc - 1) / nc, (Nout + AXU_M - 1) / AXU_M), 6};
   }
   if (g_axis_mma && Nout >= 16) {
     // the largest tile that fills one wave (a CTA per SM); else the smallest

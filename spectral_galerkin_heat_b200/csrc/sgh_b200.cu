@@ -708,6 +708,17 @@ struct sgh_plan {
   double box_z0 = 0.0;
   size_t o_bx = 0, o_by = 0, o_bzi = 0, o_bzf = 0, o_wxi = 0, o_wxf = 0, o_wyi = 0, o_wyf = 0;
   size_t o_bt1 = 0, o_bt2 = 0, o_Qbox = 0, o_Tpb = 0, o_Qpb = 0, o_Tsh = 0, o_Qsh = 0;
+  // mixed plans: BF16 pair planes of the transform and box matrices
+  // (matrix offset, rows, contraction length, plane offset)
+  struct PlaneSpec {
+    size_t mat;
+    int rows, k;
+    size_t off;
+    bool per_step;  // a window basis, rebuilt with the window every step
+  };
+  std::vector<PlaneSpec> plane_specs;
+  std::vector<UmmaPlane> planes;
+  bool bound_planes = false;
   size_t ws_need = 0;
   char* ws = nullptr;
   bool bound = false;
@@ -731,6 +742,9 @@ bool plan_mixed(const sgh_plan* p) { return p && p->cfg.precision == SGH_PRECISI
 // iterates rounded to FP32 (the FP32 arm of the precision study).
 bool plan_fp32(const sgh_plan* p) { return p && p->cfg.precision == SGH_PRECISION_FP32; }
 int* umma_err_of(const sgh_plan* p) { return (p && p->ws) ? &p->ctrl()->umma_err : nullptr; }
+// The plan's matrices with BF16 pair planes (mixed plans, once bound).
+const UmmaPlane* planes_of(const sgh_plan* p) { return (p && p->bound_planes) ? p->planes.data() : nullptr; }
+int nplanes_of(const sgh_plan* p) { return (p && p->bound_planes) ? (int)p->planes.size() : 0; }
 
 int check_program(const sgh_program& p, const char* name) {
   if (p.n_ops < 1 || p.n_ops > SGH_MAX_PROGRAM || p.n_consts < 0 || p.n_consts > SGH_MAX_CONSTS)
@@ -988,6 +1002,12 @@ void enqueue_picard_face_space(sgh_plan* p, cudaStream_t s, cudaGraphConditional
   ++g_launches;
 }
 
+// BF16 pair plane of one matrix of a mixed plan.
+void build_plane(sgh_plan* p, const sgh_plan::PlaneSpec& q, cudaStream_t s) {
+  const long n = (long)cdiv(q.rows, AXU_M) * AXU_M * (long)cdiv(q.k, AXU_KC) * AXU_KC;
+  k_pair_plane<<<std::min(cdiv(n, EW_THREADS), 1184), EW_THREADS, 0, s>>>(p->d(q.mat), q.rows, q.k, p->ws + q.off);
+}
+
 // Step opening: laser state, Picard switch, face forcing and (box mode) the
 // window of this step.
 void enqueue_pre_begin(sgh_plan* p, cudaStream_t s, cudaGraphConditionalHandle h_picard,
@@ -1007,6 +1027,11 @@ void enqueue_pre_begin(sgh_plan* p, cudaStream_t s, cudaGraphConditionalHandle h
     k_box_window<<<cdiv(n, EW_THREADS), EW_THREADS, 0, s>>>(P, C, p->d(p->o_bx), p->d(p->o_by), p->d(p->o_wxi),
                                                             p->d(p->o_wxf), p->d(p->o_wyi), p->d(p->o_wyf));
     ++g_launches;
+    for (const auto& q : p->plane_specs)
+      if (q.per_step) {
+        build_plane(p, q, s);
+        ++g_launches;
+      }
   }
 }
 
@@ -1483,6 +1508,26 @@ int sgh_plan_create(const sgh_config* cfg, sgh_plan** out) {
   p->o_beta = L.take(S8);
   p->o_Ab = L.take(S8);
   p->o_pn1 = L.take(sizeof(double) * p->nparts_n1);
+  if (c.precision == SGH_PRECISION_MIXED) {
+    // each matrix with the largest (rows, contraction length) its passes use
+    auto plane = [&](size_t mat, int rows, int k, bool per_step = false) {
+      p->plane_specs.push_back({mat, rows, k, L.take(umma::pair_bytes<AXU_M>(rows, k)), per_step});
+    };
+    plane(p->o_mx, h.nx, h.nx);
+    plane(p->o_mxt, h.nx, h.nx);
+    plane(p->o_my, h.ny, h.ny);
+    plane(p->o_myt, h.ny, h.ny);
+    plane(p->o_mz, h.nz, h.nz);
+    plane(p->o_mzt, h.nz + 2, h.nz);
+    if (box) {
+      plane(p->o_bzi, h.zb + 1, h.nz);
+      plane(p->o_wxi, h.xb, h.nx, true);
+      plane(p->o_wyi, h.yb, h.ny, true);
+      plane(p->o_wyf, h.ny, h.yb, true);
+      plane(p->o_wxf, h.nx, h.xb, true);
+      plane(p->o_bzf, h.nz, h.zb);
+    }
+  }
   p->ws_need = L.off;
   *out = p;
   return SGH_OK;
@@ -1506,7 +1551,7 @@ int sgh_plan_workspace_bytes(const sgh_plan* p, uint64_t* bytes) {
 
 int sgh_plan_bind(sgh_plan* p, void* workspace, uint64_t bytes, void* stream) {
   AxisPolicy policy(p ? p->cfg.axis_min_ctas : 0, p ? p->cfg.axis_cuda_cores : 0, plan_mixed(p), umma_err_of(p),
-                    plan_fp32(p));
+                    plan_fp32(p), planes_of(p), nplanes_of(p));
   if (!p || !workspace) return fail(SGH_ERR_INVALID, "null argument");
   if (p->bound) return fail(SGH_ERR_STATE, "plan is already bound");
   if (bytes < p->ws_need) return fail(SGH_ERR_WORKSPACE, "workspace is smaller than sgh_plan_workspace_bytes()");
@@ -1545,6 +1590,16 @@ int sgh_plan_bind(sgh_plan* p, void* workspace, uint64_t bytes, void* stream) {
   if (p->face_space)
     k_fs_weights<<<cdiv(h.S, EW_THREADS), EW_THREADS, 0, s>>>(p->P(), p->d(p->o_KK), p->d(p->o_ct),
                                                               p->d(p->o_cb), p->d(p->o_fsW));
+  // BF16 pair planes of the matrices (mixed plans), once the matrices exist
+  // (the window bases' planes are rebuilt with the window every step)
+  p->planes.clear();
+  for (const auto& q : p->plane_specs) {
+    if (!q.per_step) build_plane(p, q, s);
+    p->planes.push_back({p->d(q.mat), p->ws + q.off, q.rows, q.k});
+  }
+  p->bound_planes = true;
+  g_umma_planes = planes_of(p);
+  g_umma_nplanes = nplanes_of(p);
   SGH_CK(cudaGetLastError());
   SGH_CK(cudaStreamSynchronize(s));
   SGH_CK(cudaStreamCreateWithFlags(&p->cs1, cudaStreamNonBlocking));
@@ -1639,7 +1694,7 @@ int sgh_step(sgh_plan* p, const sgh_laser* laser, sgh_step_out* out, void* strea
 
 int sgh_step_eager(sgh_plan* p, const sgh_laser* laser, sgh_step_out* out, void* stream) {
   AxisPolicy policy(p ? p->cfg.axis_min_ctas : 0, p ? p->cfg.axis_cuda_cores : 0, plan_mixed(p), umma_err_of(p),
-                    plan_fp32(p));
+                    plan_fp32(p), planes_of(p), nplanes_of(p));
   if (!p || !laser) return fail(SGH_ERR_INVALID, "null argument");
   if (!p->bound) return fail(SGH_ERR_STATE, "plan is not bound");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -1674,7 +1729,7 @@ int sgh_run(sgh_plan* p, const sgh_laser* lasers_dev, int32_t n_steps, sgh_step_
 
 int sgh_dct3d(sgh_plan* p, int32_t kind, const double* in, double* out, void* stream) {
   AxisPolicy policy(p ? p->cfg.axis_min_ctas : 0, p ? p->cfg.axis_cuda_cores : 0, plan_mixed(p), umma_err_of(p),
-                    plan_fp32(p));
+                    plan_fp32(p), planes_of(p), nplanes_of(p));
   if (!p || !in || !out) return fail(SGH_ERR_INVALID, "null argument");
   if (!p->bound) return fail(SGH_ERR_STATE, "plan is not bound");
   if (kind != 2 && kind != 3) return fail(SGH_ERR_INVALID, "kind must be 2 (DCT_II) or 3 (IDCT_II)");
@@ -1686,7 +1741,7 @@ int sgh_dct3d(sgh_plan* p, int32_t kind, const double* in, double* out, void* st
 
 int sgh_surface_temperature(sgh_plan* p, const double* modes, int32_t top, double* out, void* stream) {
   AxisPolicy policy(p ? p->cfg.axis_min_ctas : 0, p ? p->cfg.axis_cuda_cores : 0, plan_mixed(p), umma_err_of(p),
-                    plan_fp32(p));
+                    plan_fp32(p), planes_of(p), nplanes_of(p));
   if (!p || !modes || !out) return fail(SGH_ERR_INVALID, "null argument");
   if (!p->bound) return fail(SGH_ERR_STATE, "plan is not bound");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -1697,7 +1752,7 @@ int sgh_surface_temperature(sgh_plan* p, const double* modes, int32_t top, doubl
 
 int sgh_project_volume(sgh_plan* p, const double* field, double* modes, void* stream) {
   AxisPolicy policy(p ? p->cfg.axis_min_ctas : 0, p ? p->cfg.axis_cuda_cores : 0, plan_mixed(p), umma_err_of(p),
-                    plan_fp32(p));
+                    plan_fp32(p), planes_of(p), nplanes_of(p));
   if (!p || !field || !modes) return fail(SGH_ERR_INVALID, "null argument");
   if (!p->bound) return fail(SGH_ERR_STATE, "plan is not bound");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -1708,7 +1763,7 @@ int sgh_project_volume(sgh_plan* p, const double* field, double* modes, void* st
 
 int sgh_reconstruct_volume(sgh_plan* p, const double* modes, double* field, void* stream) {
   AxisPolicy policy(p ? p->cfg.axis_min_ctas : 0, p ? p->cfg.axis_cuda_cores : 0, plan_mixed(p), umma_err_of(p),
-                    plan_fp32(p));
+                    plan_fp32(p), planes_of(p), nplanes_of(p));
   if (!p || !field || !modes) return fail(SGH_ERR_INVALID, "null argument");
   if (!p->bound) return fail(SGH_ERR_STATE, "plan is not bound");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -1783,7 +1838,7 @@ int sgh_box_window(sgh_plan* p, int32_t* i0, void* stream) {
 
 int sgh_box_temperature(sgh_plan* p, const double* modes, double* out, void* stream) {
   AxisPolicy policy(p ? p->cfg.axis_min_ctas : 0, p ? p->cfg.axis_cuda_cores : 0, plan_mixed(p), umma_err_of(p),
-                    plan_fp32(p));
+                    plan_fp32(p), planes_of(p), nplanes_of(p));
   if (!p || !modes || !out) return fail(SGH_ERR_INVALID, "null argument");
   if (!p->bound) return fail(SGH_ERR_STATE, "plan is not bound");
   if (!p->hp.box) return fail(SGH_ERR_STATE, "plan is not in box mode");
@@ -1796,7 +1851,7 @@ int sgh_box_temperature(sgh_plan* p, const double* modes, double* out, void* str
 
 int sgh_box_project(sgh_plan* p, const double* field_box, double* modes, void* stream) {
   AxisPolicy policy(p ? p->cfg.axis_min_ctas : 0, p ? p->cfg.axis_cuda_cores : 0, plan_mixed(p), umma_err_of(p),
-                    plan_fp32(p));
+                    plan_fp32(p), planes_of(p), nplanes_of(p));
   if (!p || !field_box || !modes) return fail(SGH_ERR_INVALID, "null argument");
   if (!p->bound) return fail(SGH_ERR_STATE, "plan is not bound");
   if (!p->hp.box) return fail(SGH_ERR_STATE, "plan is not in box mode");

@@ -37,6 +37,26 @@ def test_mixed_dct3d_matches_scipy():
     s.finalize()
 
 
+@pytest.mark.parametrize("mesh", [(300, 40, 20), (128, 80, 100), (33, 17, 129)])
+def test_mixed_dct3d_tiles_and_ring(mesh):
+    """Shapes that reach every tile path of the split-BF16 pass: 300 outputs
+    (three 128-row tiles, a ragged last one), contraction lengths of 100 to
+    300 slices (more 32-slice chunks than ring stages, so stages are refilled
+    while MMAs run), 16-, 32- and 64-column tiles, and ragged columns."""
+    import copy
+    import torch
+    cfg, path, *_ = golden_case("raster_32x16x8")
+    cfg = copy.deepcopy(cfg)
+    cfg["domain"]["mesh"] = list(mesh)
+    s = _solver(cfg, path, "mixed")
+    x = np.random.default_rng(sum(mesh)).standard_normal(s.state.shape)
+    for kind in (2, 3):
+        got = s.dct3d(torch.as_tensor(x, device="cuda"), kind).cpu().numpy()
+        ref = scipy.fft.dctn(x, type=kind, norm="ortho")
+        assert rel_l2(got, ref) < 2e-5, (mesh, kind, rel_l2(got, ref))
+    s.finalize()
+
+
 @pytest.mark.parametrize("name", ["raster_32x16x8", "tdep03_grid_25x15x24", "box_tdep_16x12x8",
                                   "tdep03_box_25x15x24"])
 def test_mixed_volume_form_matches_reference(name):
@@ -54,7 +74,9 @@ def test_mixed_volume_form_matches_reference(name):
             assert rel_l2(got, ref) < TOL, (name, i + 1, rel_l2(got, ref))
             # the modal state is FP32
             assert np.array_equal(a, a.astype(np.float32).astype(np.float64))
-    np.testing.assert_allclose([m["T_surface_max"]], [g["metric_T_surface_max"][steps - 1]], rtol=1e-4)
+    # a pointwise peak: held to the mixed forms' peak-temperature bound (1 K),
+    # not to the L2 bound of the modes
+    assert abs(m["T_surface_max"] - g["metric_T_surface_max"][steps - 1]) < 1.0
     s.finalize()
 
 
