@@ -61,6 +61,7 @@ struct BSlot {
   long long xa;        // byte offset of the slot's face planes (rows y, k = x) in the xa / xq arenas
   long long mpx, mpy;  // byte offsets of the forward x / y matrix planes (inverse at + mp_inv)
   long long mpx_inv, mpy_inv;
+  long long x1;        // byte offset of the slot's x1 plane (x-pass result, y-pass B operand)
   double dx, dy, dt, Lx, Ly, Lz;
   double dct_scale, recon_scale, n_elements;
   double T0, evap_f1, evap_f2, T_boil, T_liquidus;
@@ -89,7 +90,7 @@ struct BGlobal {
   unsigned slots_done;   // slots finished in the current kb_relax launch (back to 0 after it)
   int n_iter_slots;      // slots iterating in the current Picard iteration
   unsigned wait_limit;   // polls of the tensor-core data waits (0: umma::WAIT_LIMIT)
-  int stall_test;        // 1: every face-transform CTA first waits on a barrier nothing completes
+  int stall_test;        // 1: every face y-pass CTA first waits on a barrier nothing completes
   int pad;
 };
 
@@ -102,9 +103,10 @@ struct BView {
   const int* rblk_slot;   // slot of each relaxation block
   const int* tile_slot;   // slot of each FP64 face-transform tile
   const int* vblk_slot;   // slot of each volume block
-  const int* utile_slot;  // slot of each tensor-core column block
+  const int* utile_slot;  // slot of each tensor-core face tile
   char* xa;               // operand pair planes (mixed precision; null otherwise):
   char* xq;               //   xa = A = Zt + W_tt sigma (inverse transform input), xq = q_net (forward)
+  char* x1;               //   x1 = the x-pass result of the face transform in flight
   const char* mp;         // DCT matrix pair planes
   const double* mats;
   const double* Ct;
@@ -478,44 +480,43 @@ __global__ void __launch_bounds__(AX_THREADS) kb_face_axis(BView v, const double
   }
 }
 
-// ---- fused 2-D face transform on the tensor cores (mixed precision) -------
-// One CTA transforms one NB-column block of a slot's face along both axes:
-//   x-pass  X1[y][c] = sum_x P[y][x] Mx[c][x]    (P: the slot's xa or xq plane)
-//   y-pass  G[r][c]  = sum_y My[r][y] X1[y][c]
-// for every row y < ny (ny <= 256: one or two 128-row tiles). Each x-pass row
-// tile accumulates in tensor memory (M = 128, N = NB), is split into BF16
-// hi/lo and written to shared memory as the K-major B operand of the y-pass;
-// the y-pass row tiles accumulate in tensor memory and reach the epilogue
-// through a shared-memory tile. Separability makes the column blocks
-// independent: a slot's transform needs no exchange between CTAs. One thread
-// streams every operand chunk (the x-pass P and Mx chunks, then the My
-// chunks) through one ring of bulk-copy stages and issues the MMAs, so the My
-// copies are in flight while the x-pass result is converted. Operands are
-// split-BF16 (three MMAs per k-step, FP32 accumulation), as in tile_bf16x3.
-// Shared memory is sized for two CTAs per SM, so one CTA's epilogue overlaps
-// another's copies and MMAs.
+// ---- batched face transform on the tensor cores (mixed precision) ---------
+// A 2-D transform of every slot's top face is two launches:
+//   kb_fx   X1[y][c] = sum_x P[y][x] Mx[c][x]    (P: the slot's xa or xq plane)
+//   kb_fy   G[r][c]  = sum_y My[r][y] X1[y][c], then the epilogue KIND
+// Each CTA computes one 128-row x NB-column tile of one slot (MMA M = 128,
+// N = NB). One thread streams the tile's operand chunks -- BF16 hi + lo, one
+// bulk copy per operand and 32-slice chunk -- through a ring of f2::STAGES
+// stages and issues three split-BF16 MMAs per 16-slice step (hi.hi, hi.lo,
+// lo.hi, each its own FP32 accumulator chain in tensor memory, summed when
+// read out); the ring is primed before the tensor memory is allocated.
+// kb_fx writes X1, split into BF16 hi + lo, to the slot's x1 plane, chunked
+// and laid out exactly as the B operand chunks of kb_fy, which streams it
+// like any other operand. Separability makes the tiles independent. Shared
+// memory (4 stages of 24 KB) and tensor memory (256 columns) allow two CTAs
+// per SM, so one CTA's epilogue overlaps another's copies and MMAs.
 namespace f2 {
 constexpr int THREADS = 256;
 constexpr int NB = 64;                       // column block (MMA N)
 constexpr int CA = umma::CHUNK_BYTES;        // 128 x 32 BF16 chunk of an A operand (8 KB)
 constexpr int CBN = NB * umma::KC * 2;       // NB x 32 BF16 chunk of a B operand (4 KB)
-constexpr int STAGE = 2 * CA + 2 * CBN;      // 24 KB: P hi/lo + Mx hi/lo, or My hi/lo
-constexpr int MAX_STAGES = 4;
-constexpr int SMEM_PER_CTA = 233472 / 2 - 1024;  // two CTAs per SM
-constexpr int TAIL = 256;                    // barriers, TMEM address, status flag
-constexpr int STATIC = 512;                  // static shared memory of the kernel (upper bound)
-constexpr int MAX_NY = 256;
-inline int bop_bytes(int max_ny) { return ((max_ny + 31) / 32) * 2 * CBN; }
-inline int stages(int max_ny) {
-  const int s = (SMEM_PER_CTA - STATIC - TAIL - bop_bytes(max_ny)) / STAGE;
-  return s < MAX_STAGES ? s : MAX_STAGES;
-}
-inline int smem_bytes(int max_ny) { return bop_bytes(max_ny) + stages(max_ny) * STAGE + TAIL; }
+constexpr int STAGE = 2 * CA + 2 * CBN;      // 24 KB: A hi/lo + B hi/lo
+constexpr int STAGES = 4;
+constexpr int TAIL = 128;                    // barriers, TMEM address, status flag
+constexpr int SMEM = STAGES * STAGE + TAIL;  // 98,432 bytes: two CTAs per SM
+constexpr uint32_t TCOLS = 256;              // three NB-column accumulators
 }  // namespace f2
 
-inline __host__ __device__ int face_utiles(int nx, int) { return (nx + f2::NB - 1) / f2::NB; }
+// Tensor-core face tiles of a slot: 128-row tiles x NB-column blocks.
+inline __host__ __device__ int face_utiles(int nx, int ny) {
+  return ((nx + f2::NB - 1) / f2::NB) * ((ny + umma::TM - 1) / umma::TM);
+}
+// Bytes of a slot's x1 plane: NB-column blocks x 32-row chunks of {hi, lo}.
+inline __host__ __device__ long long x1_bytes(int nx, int ny) {
+  return (long long)((nx + f2::NB - 1) / f2::NB) * ((ny + umma::KC - 1) / umma::KC) * 2 * f2::CBN;
+}
 
-// Epilogue of the fused transform, on output element (r, c) of the slot's face:
+// Epilogue of the transform, on output element (r, c) of the slot's face:
 //   F2_STORE    FP64 face array (x dct_scale if scaled)
 //   F2_TOPFLUX  T_s -> evaporation -> q_evap (FP64), q_net -> xq plane
 //   F2_COMMIT   T_temp, its block max, q_evap_old <- q_evap
@@ -542,9 +543,181 @@ struct F2Args {
 // copy, a row stays conflict-free for the epilogue.
 __device__ __forceinline__ float f2_tile(const float* t, int m, int n) { return t[m * f2::NB + (n ^ (m & 31))]; }
 
+// Shared-memory layout of both kernels: the ring, then full[STAGES],
+// done[STAGES], the never-completed wait-test barrier, the TMEM address and
+// the status flag.
+struct F2Smem {
+  char* ring;
+  uint64_t *full, *done, *stall;
+  uint32_t* tslot;
+  volatile int* okflag;
+  __device__ explicit F2Smem(char* sm)
+      : ring(sm),
+        full(reinterpret_cast<uint64_t*>(sm + f2::STAGES * f2::STAGE)),
+        done(full + f2::STAGES),
+        stall(done + f2::STAGES),
+        tslot(reinterpret_cast<uint32_t*>(stall + 1)),
+        okflag(reinterpret_cast<volatile int*>(tslot + 1)) {}
+};
+
+// Thread 0: initialise the barriers and issue the first min(n, STAGES)
+// chunks; returns how many were issued.
+template <class Load>
+__device__ __forceinline__ int f2_prime(const F2Smem& m, int n, const Load& load) {
+  using namespace umma;
+  for (int i = 0; i < f2::STAGES; ++i) {
+    mbar_init(&m.full[i], 1);
+    mbar_init(&m.done[i], 1);
+  }
+  mbar_init(m.stall, 1);
+  *m.okflag = 1;
+  asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  const int pre = n < f2::STAGES ? n : f2::STAGES;
+  for (int g = 0; g < pre; ++g) load(g);
+  return pre;
+}
+
+// Thread 0: chunks 0..n-1 of the tile (chunk g in stage g % STAGES; each
+// barrier completes one phase per use of its stage, so chunk g waits for
+// parity (g / STAGES) & 1), MMAs into the accumulators at tmem, tmem + NB
+// and tmem + 2 NB, then the wait for the last MMAs. A wait that expires
+// (after `lim` polls) records the error, clears the status flag and drains,
+// with the full bound, every copy and MMA in flight; returns false then.
+// stall: first wait on a barrier that nothing completes (the wait test).
+template <class Load>
+__device__ bool f2_run(const F2Smem& m, int n, int issued, const Load& load, uint32_t tmem, unsigned lim,
+                       bool stall, int* err) {
+  using namespace umma;
+  constexpr int S = f2::STAGES, NB = f2::NB;
+  const uint32_t idesc = idesc_bf16_f32(TM, NB);
+  int committed = 0;
+  bool ok = !stall || mbar_wait_bounded(m.stall, 0u, lim);
+  for (int g = 0; g < n && ok; ++g) {
+    if (!mbar_wait_bounded(&m.full[g % S], (uint32_t)((g / S) & 1), lim)) {
+      ok = false;
+      break;
+    }
+    tc_fence_after();
+    const uint32_t ah = smem_u32(m.ring + (g % S) * f2::STAGE), al = ah + f2::CA;
+    const uint32_t bh = ah + 2 * f2::CA, bl = bh + f2::CBN;
+#pragma unroll
+    for (int k = 0; k < KC / 16; ++k) {
+      const uint32_t oa = (uint32_t)(2 * k * (TM / 8) * 128), ob = (uint32_t)(2 * k * (NB / 8) * 128);
+      const uint64_t dah = smem_desc(ah + oa, (TM / 8) * 128, 128);
+      const uint64_t dal = smem_desc(al + oa, (TM / 8) * 128, 128);
+      const uint64_t dbh = smem_desc(bh + ob, (NB / 8) * 128, 128);
+      const uint64_t dbl = smem_desc(bl + ob, (NB / 8) * 128, 128);
+      const uint32_t acc = (g > 0 || k > 0) ? 1u : 0u;
+      mma_bf16(tmem, dah, dbh, idesc, acc);
+      mma_bf16(tmem + NB, dah, dbl, idesc, acc);
+      mma_bf16(tmem + 2 * NB, dal, dbh, idesc, acc);
+    }
+    mma_commit(&m.done[g % S]);
+    committed = g + 1;
+    const int nxt = g - 1 + S;  // the stage of chunk g - 1 takes chunk g - 1 + S
+    if (g >= 1 && nxt < n && nxt >= issued) {
+      if (!mbar_wait_bounded(&m.done[(g - 1) % S], (uint32_t)(((g - 1) / S) & 1), lim)) {
+        ok = false;
+        break;
+      }
+      load(nxt);
+      issued = nxt + 1;
+    }
+  }
+  if (ok && n > 0) ok = mbar_wait_bounded(&m.done[(n - 1) % S], (uint32_t)(((n - 1) / S) & 1), lim);
+  if (!ok) {
+    atomicExch(err, 1);
+    *m.okflag = 0;
+    for (int g = issued - S < 0 ? 0 : issued - S; g < issued; ++g)
+      mbar_wait_bounded(&m.full[g % S], (uint32_t)((g / S) & 1), WAIT_LIMIT);
+    for (int g = committed - S < 0 ? 0 : committed - S; g < committed; ++g)
+      mbar_wait_bounded(&m.done[g % S], (uint32_t)((g / S) & 1), WAIT_LIMIT);
+  }
+  return ok;
+}
+
+// 32 x 16 accumulator values of this warp's lane quarter: the three parts summed.
+__device__ __forceinline__ void f2_read16(uint32_t ta, float (&x)[16]) {
+  float p1[16], p2[16];
+  umma::tmem_ld16(ta, x);
+  umma::tmem_ld16(ta + f2::NB, p1);
+  umma::tmem_ld16(ta + 2 * f2::NB, p2);
+#pragma unroll
+  for (int i = 0; i < 16; ++i) x[i] = x[i] + (p1[i] + p2[i]);
+}
+
+template <bool INV, bool SKIP_DONE>
+__global__ void __launch_bounds__(f2::THREADS, 2) kb_fx(BView v) {
+  using namespace umma;
+  constexpr int CA = f2::CA, CBN = f2::CBN, NB = f2::NB;
+  extern __shared__ __align__(128) char sm[];
+  const int b = blockIdx.x;
+  const int s = v.utile_slot[b];
+  const BSlot& sl = v.slot[s];
+  const BState& st = v.st[s];
+  if (!st.active || (SKIP_DONE && st.done)) return;
+  const int nx = sl.nx, ny = sl.ny;
+  const int ncb = (nx + NB - 1) / NB, t = b - sl.utile0, rt = t / ncb, cb = t - rt * ncb;
+  const int nkx = (nx + KC - 1) / KC, nky = (ny + KC - 1) / KC;
+  const F2Smem m(sm);
+  const char* pp = (INV ? v.xa : v.xq) + sl.xa + (size_t)rt * nkx * 2 * CA;       // 128-row pair chunks
+  const char* mx = v.mp + (INV ? sl.mpx_inv : sl.mpx) + (size_t)cb * nkx * 2 * CBN;  // NB-row pair chunks
+  auto load = [&](int g) {  // P chunk (rt, g) and Mx chunk (cb, g)
+    char* stg = m.ring + (g % f2::STAGES) * f2::STAGE;
+    uint64_t* bar = &m.full[g % f2::STAGES];
+    mbar_expect_tx(bar, f2::STAGE);
+    bulk_g2s(stg, pp + (size_t)g * 2 * CA, 2 * CA, bar);
+    bulk_g2s(stg + 2 * CA, mx + (size_t)g * 2 * CBN, 2 * CBN, bar);
+  };
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  int issued = 0;
+  if (tid == 0) issued = f2_prime(m, nkx, load);
+  __syncwarp();
+  if (warp == 0) tmem_alloc(m.tslot, f2::TCOLS);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *m.tslot;
+  if (tid == 0) {
+    const unsigned lim = v.g->wait_limit ? v.g->wait_limit : WAIT_LIMIT;
+    f2_run(m, nkx, issued, load, tmem, lim, false, &v.g->umma_err);
+  }
+  __syncthreads();
+  if (*m.okflag) {
+    // X1 row y = TMEM lane -> x1 plane element (row c, k = y); rows y and
+    // y + 1 (lanes l, l + 1) go out as one 32-bit store per part
+    tc_fence_after();
+    const int q = warp & 3, half = warp >> 2;  // TMEM lane quarter, column half
+    const int y = rt * TM + q * 32 + lane;
+    const bool keep = y < nky * KC;
+    const int c = half * 32;
+    char* x1 = v.x1 + sl.x1 + (size_t)cb * nky * 2 * CBN + (size_t)(y >> 5) * 2 * CBN;
+#pragma unroll
+    for (int cc = 0; cc < 32; cc += 16) {
+      float x16[16];
+      f2_read16(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(c + cc), x16);
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        __nv_bfloat16 h, l;
+        split_bf16((double)x16[i], h, l);
+        const uint32_t hv = __bfloat16_as_ushort(h), lv = __bfloat16_as_ushort(l);
+        const uint32_t hn = __shfl_down_sync(0xffffffffu, hv, 1);
+        const uint32_t ln = __shfl_down_sync(0xffffffffu, lv, 1);
+        if ((lane & 1) == 0 && keep) {
+          const uint32_t o = core_off(c + cc + i, y & 31, NB);
+          *reinterpret_cast<uint32_t*>(x1 + o) = hv | (hn << 16);
+          *reinterpret_cast<uint32_t*>(x1 + CBN + o) = lv | (ln << 16);
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tmem_dealloc(tmem, f2::TCOLS);
+}
+
 template <bool INV, bool SKIP_DONE, int KIND>
-__global__ void __launch_bounds__(f2::THREADS, 2)
-kb_face2d(BView v, F2Args args, double* part_tile, int n_stages, int bop_max) {
+__global__ void __launch_bounds__(f2::THREADS, 2) kb_fy(BView v, F2Args args, double* part_tile) {
   using namespace umma;
   constexpr int CA = f2::CA, CBN = f2::CBN, NB = f2::NB;
   extern __shared__ __align__(128) char sm[];
@@ -559,285 +732,141 @@ kb_face2d(BView v, F2Args args, double* part_tile, int n_stages, int bop_max) {
   fp.recon_scale = sl.recon_scale; fp.dct_scale = sl.dct_scale; fp.T_liquidus = sl.T_liquidus;
   fp.T_boil = sl.T_boil; fp.evap_f1 = sl.evap_f1; fp.evap_f2 = sl.evap_f2;
   const int nx = fp.nx, ny = fp.ny;
-  const int ct = b - sl.utile0;
+  const int ncb = (nx + NB - 1) / NB, t = b - sl.utile0, rt = t / ncb, cb = t - rt * ncb;
   const int nkx = (nx + KC - 1) / KC, nky = (ny + KC - 1) / KC;
-  const int nrt = (ny + TM - 1) / TM;
-  const int S = n_stages;
-  const int n_x = nrt * nkx, total = n_x + nrt * nky;
-  char* bop = sm;                // y-pass B operand: nky chunks of {hi, lo}
-  char* ring = sm + bop_max;     // S stages; later the epilogue tile
-  uint64_t* full = reinterpret_cast<uint64_t*>(ring + S * f2::STAGE);
-  uint64_t* done = full + f2::MAX_STAGES;
-  uint32_t* tslot = reinterpret_cast<uint32_t*>(done + f2::MAX_STAGES);
-  volatile int* okflag = reinterpret_cast<volatile int*>(tslot + 1);
-  uint64_t* stall = done + f2::MAX_STAGES + 1;  // never arrived on (wait test)
+  const F2Smem m(sm);
+  const char* my = v.mp + (INV ? sl.mpy_inv : sl.mpy) + (size_t)rt * nky * 2 * CA;  // 128-row pair chunks
+  const char* x1 = v.x1 + sl.x1 + (size_t)cb * nky * 2 * CBN;                       // NB-row pair chunks
+  auto load = [&](int g) {  // My chunk (rt, g) and x1 chunk (cb, g)
+    char* stg = m.ring + (g % f2::STAGES) * f2::STAGE;
+    uint64_t* bar = &m.full[g % f2::STAGES];
+    mbar_expect_tx(bar, f2::STAGE);
+    bulk_g2s(stg, my + (size_t)g * 2 * CA, 2 * CA, bar);
+    bulk_g2s(stg + 2 * CA, x1 + (size_t)g * 2 * CBN, 2 * CBN, bar);
+  };
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  // TMEM: the x-pass keeps hi*hi, hi*lo and lo*hi in three accumulators
-  // (columns 0, 64, 128: three independent MMA chains); y-pass row tile rt
-  // keeps hi*hi and hi*lo + lo*hi in two (columns 128 rt and 128 rt + 64).
-  // The parts are summed when read out.
-  constexpr uint32_t ncols = 256u;
-  const char* pp = (INV ? v.xa : v.xq) + fp.xa;                                        // pair chunks of 2 CA
-  const long long mxo = (INV ? sl.mpx_inv : sl.mpx) + (long long)ct * nkx * 2 * CBN;  // NB-row pairs
-  const long long myo = INV ? sl.mpy_inv : sl.mpy;                                     // 128-row pairs
-  const uint32_t idesc = idesc_bf16_f32(TM, NB);
-
-  uint32_t tmem = 0;  // tensor-memory base, set once allocated
-  // Thread 0's ring: chunk g lives in stage g % S; each barrier completes one
-  // phase per use of its stage, so chunk g waits for parity (g / S) & 1.
-  // Chunks: x-pass (rt, kc) = P hi/lo + Mx hi/lo; then y-pass (rt, kc) = My hi/lo.
-  int issued = 0, committed = 0;
-  auto load = [&](int g) {
-    char* stg = ring + (g % S) * f2::STAGE;
-    uint64_t* bar = &full[g % S];
-    if (g < n_x) {  // one copy of P's hi + lo chunk, one of Mx's
-      const int rt = g / nkx, kc = g - rt * nkx;
-      mbar_expect_tx(bar, 2 * CA + 2 * CBN);
-      bulk_g2s(stg, pp + (size_t)(rt * nkx + kc) * 2 * CA, 2 * CA, bar);
-      bulk_g2s(stg + 2 * CA, v.mp + mxo + (size_t)kc * 2 * CBN, 2 * CBN, bar);
-    } else {        // one copy of My's hi + lo chunk
-      const int gy = g - n_x, rt = gy / nky, kc = gy - rt * nky;
-      mbar_expect_tx(bar, 2 * CA);
-      bulk_g2s(stg, v.mp + (size_t)myo + (size_t)(rt * nky + kc) * 2 * CA, 2 * CA, bar);
-    }
-  };
-  // data waits poll at most `lim` times (the batch's setting); the drain after
-  // a failed wait always keeps the full bound, so no copy or MMA is left in
-  // flight when the CTA exits
-  const unsigned lim = v.g->wait_limit ? v.g->wait_limit : WAIT_LIMIT;
-  auto wait_full = [&](int g, unsigned l) { return mbar_wait_bounded(&full[g % S], (uint32_t)((g / S) & 1), l); };
-  auto wait_done = [&](int g, unsigned l) { return mbar_wait_bounded(&done[g % S], (uint32_t)((g / S) & 1), l); };
-  auto step = [&](int g) -> bool {
-    if (!wait_full(g, lim)) return false;
-    tc_fence_after();
-    const uint32_t s0 = smem_u32(ring + (g % S) * f2::STAGE);
-    uint32_t ah, al, bh, bl, d0, d1, d2;
-    int kc;
-    if (g < n_x) {
-      kc = g % nkx;
-      ah = s0; al = s0 + CA; bh = s0 + 2 * CA; bl = s0 + 2 * CA + CBN;
-      d0 = tmem; d1 = tmem + NB; d2 = tmem + 2 * NB;
-    } else {
-      const int gy = g - n_x, rt = gy / nky;
-      kc = gy - rt * nky;
-      ah = s0; al = s0 + CA;
-      bh = smem_u32(bop + kc * 2 * CBN); bl = bh + CBN;
-      d0 = tmem + (uint32_t)(rt * 2 * NB); d1 = d0 + NB; d2 = d1;
-    }
-#pragma unroll
-    for (int k = 0; k < KC / 16; ++k) {
-      const uint32_t oa = (uint32_t)(2 * k * (TM / 8) * 128), ob = (uint32_t)(2 * k * (NB / 8) * 128);
-      const uint64_t dah = smem_desc(ah + oa, (TM / 8) * 128, 128);
-      const uint64_t dal = smem_desc(al + oa, (TM / 8) * 128, 128);
-      const uint64_t dbh = smem_desc(bh + ob, (NB / 8) * 128, 128);
-      const uint64_t dbl = smem_desc(bl + ob, (NB / 8) * 128, 128);
-      const uint32_t acc = (kc > 0 || k > 0) ? 1u : 0u;
-      mma_bf16(d0, dah, dbh, idesc, acc);
-      mma_bf16(d1, dah, dbl, idesc, acc);
-      mma_bf16(d2, dal, dbh, idesc, (d2 == d1) ? 1u : acc);
-    }
-    mma_commit(&done[g % S]);
-    committed = g + 1;
-    const int nxt = g - 1 + S;  // the stage of chunk g - 1 takes chunk g - 1 + S
-    if (g >= 1 && nxt < total && nxt >= issued) {
-      if (!wait_done(g - 1, lim)) return false;
-      load(nxt);
-      issued = nxt + 1;
-    }
-    return true;
-  };
-  auto fail = [&]() {  // thread 0: record, then wait (bounded) for in-flight copies and MMAs
-    atomicExch(&v.g->umma_err, 1);
-    *okflag = 0;
-    for (int g = issued - S < 0 ? 0 : issued - S; g < issued; ++g) wait_full(g, WAIT_LIMIT);
-    for (int g = committed - S < 0 ? 0 : committed - S; g < committed; ++g) wait_done(g, WAIT_LIMIT);
-  };
-
-  // the first copies go out before the tensor memory is allocated
-  if (tid == 0) {
-    for (int i = 0; i < S; ++i) {
-      mbar_init(&full[i], 1);
-      mbar_init(&done[i], 1);
-    }
-    mbar_init(stall, 1);
-    *okflag = 1;
-    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
-    const int pre = total < S ? total : S;
-    for (int g = 0; g < pre; ++g) load(g);
-    issued = pre;
-  }
+  int issued = 0;
+  if (tid == 0) issued = f2_prime(m, nky, load);
   __syncwarp();
-  if (warp == 0) tmem_alloc(tslot, ncols);
+  if (warp == 0) tmem_alloc(m.tslot, f2::TCOLS);
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
-  tmem = *tslot;
-  const int q = warp & 3, half = warp >> 2;  // TMEM lane quarter, column half
-  for (int rt = 0; rt < nrt; ++rt) {
-    if (tid == 0 && *okflag) {
-      // the wait test: a wait that can only run out, with copies in flight
-      bool ok = !(rt == 0 && v.g->stall_test) || mbar_wait_bounded(stall, 0u, lim);
-      for (int kc = 0; kc < nkx && ok; ++kc) ok = step(rt * nkx + kc);
-      if (ok) ok = wait_done(rt * nkx + nkx - 1, lim);
-      if (!ok) fail();
-    }
-    __syncthreads();
-    if (*okflag) {
-      // X1 row y = TMEM lane -> B operand element (row c, k = y); rows y and
-      // y + 1 (lanes l, l + 1) go out as one 32-bit store per part
-      tc_fence_after();
-      const int y = rt * TM + q * 32 + lane;
-      const bool keep = y < nky * KC;
-      const int c = half * 32;
-#pragma unroll
-      for (int cc = 0; cc < 32; cc += 16) {
-        float x16[16], p1[16], p2[16];
-        const uint32_t ta = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(c + cc);
-        tmem_ld16(ta, x16);
-        tmem_ld16(ta + NB, p1);
-        tmem_ld16(ta + 2 * NB, p2);
-#pragma unroll
-        for (int i = 0; i < 16; ++i) x16[i] = x16[i] + (p1[i] + p2[i]);
-#pragma unroll
-        for (int i = 0; i < 16; ++i) {
-          __nv_bfloat16 h, l;
-          split_bf16((double)x16[i], h, l);
-          const uint32_t hv = __bfloat16_as_ushort(h), lv = __bfloat16_as_ushort(l);
-          const uint32_t hn = __shfl_down_sync(0xffffffffu, hv, 1);
-          const uint32_t ln = __shfl_down_sync(0xffffffffu, lv, 1);
-          if ((lane & 1) == 0 && keep) {
-            const uint32_t o = (uint32_t)((y >> 5) * 2 * CBN) + core_off(c + cc + i, y & 31, NB);
-            *reinterpret_cast<uint32_t*>(bop + o) = hv | (hn << 16);
-            *reinterpret_cast<uint32_t*>(bop + CBN + o) = lv | (ln << 16);
-          }
-        }
-      }
-      fence_proxy_async();
-    }
-    tc_fence_before();
-    __syncthreads();
-  }
-  if (tid == 0 && *okflag) {
-    tc_fence_after();
-    bool ok = true;
-    for (int g = n_x; g < total && ok; ++g) ok = step(g);
-    if (ok) ok = wait_done(total - 1, lim);
-    if (!ok) fail();
+  const uint32_t tmem = *m.tslot;
+  if (tid == 0) {
+    // the wait test: a wait that can only run out, with copies in flight
+    const unsigned lim = v.g->wait_limit ? v.g->wait_limit : WAIT_LIMIT;
+    f2_run(m, nky, issued, load, tmem, lim, v.g->stall_test != 0, &v.g->umma_err);
   }
   __syncthreads();
 
   constexpr int ITEMS = TM * NB / f2::THREADS;  // tile elements per thread
   double mx = -INFINITY;
-  const int c0 = ct * NB;
-  float* tile = reinterpret_cast<float*>(ring);
-  for (int rt = 0; rt < nrt; ++rt) {
-    const bool good = *okflag != 0;
-    if (good) {
-      tc_fence_after();
-      const int m = q * 32 + lane;
-      const int c = half * 32;
+  const int c0 = cb * NB, r0 = rt * TM;
+  float* tile = reinterpret_cast<float*>(m.ring);
+  const bool good = *m.okflag != 0;
+  if (good) {
+    tc_fence_after();
+    const int q = warp & 3, half = warp >> 2;
+    const int mrow = q * 32 + lane;
+    const int c = half * 32;
 #pragma unroll
-      for (int cc = 0; cc < 32; cc += 16) {
-        float x16[16], p1[16];
-        const uint32_t ta = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(rt * 2 * NB + c + cc);
-        tmem_ld16(ta, x16);
-        tmem_ld16(ta + NB, p1);
+    for (int cc = 0; cc < 32; cc += 16) {
+      float x16[16];
+      f2_read16(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(c + cc), x16);
 #pragma unroll
-        for (int i = 0; i < 16; ++i) tile[m * NB + ((c + cc + i) ^ (m & 31))] = x16[i] + p1[i];
-      }
+      for (int i = 0; i < 16; ++i) tile[mrow * NB + ((c + cc + i) ^ (mrow & 31))] = x16[i];
     }
-    __syncthreads();
-    if (good) {
-      const int r0 = rt * TM;
-      if (KIND == F2_TOPFLUX) {
-        // a warp covers 32 consecutive x of one row (coalesced FP64 traffic);
-        // the loads of U elements are issued ahead of their stores
-        constexpr int U = 8;
-        for (int it0 = 0; it0 < ITEMS; it0 += U) {
-          double ql[U];
+  }
+  __syncthreads();
+  if (good) {
+    if (KIND == F2_TOPFLUX) {
+      // a warp covers 32 consecutive x of one row (coalesced FP64 traffic);
+      // the loads of U elements are issued ahead of their stores
+      constexpr int U = 8;
+      for (int it0 = 0; it0 < ITEMS; it0 += U) {
+        double ql[U];
 #pragma unroll
-          for (int u = 0; u < U; ++u) {
-            const int e = tid + (it0 + u) * f2::THREADS;
-            const int y = r0 + e / NB, x = c0 + e % NB;
-            ql[u] = (y < ny && x < nx) ? __ldg(args.in2 + fp.face + (long long)y * nx + x) : 0.0;
-          }
-#pragma unroll
-          for (int u = 0; u < U; ++u) {
-            const int e = tid + (it0 + u) * f2::THREADS;
-            const int m = e / NB, n = e % NB;
-            const int y = r0 + m, x = c0 + n;
-            const bool in = y < ny && x < nx;
-            double qn = 0.0;
-            if (in) {
-              const double qe = evaporation(fp, fp.recon_scale * (double)f2_tile(tile, m, n));
-              args.out[fp.face + (long long)y * nx + x] = qe;
-              qn = ql[u] - qe;
-            }
-            plane_put8_warp(v.xq + fp.xa, y, x, nkx, qn, in);
-          }
+        for (int u = 0; u < U; ++u) {
+          const int e = tid + (it0 + u) * f2::THREADS;
+          const int y = r0 + e / NB, x = c0 + e % NB;
+          ql[u] = (y < ny && x < nx) ? __ldg(args.in2 + fp.face + (long long)y * nx + x) : 0.0;
         }
-      } else if (KIND == F2_SIGMA) {
-        constexpr int U = 8;
-        for (int it0 = 0; it0 < ITEMS; it0 += U) {
-          double zt[U], wt[U];
 #pragma unroll
-          for (int u = 0; u < U; ++u) {
-            const int e = tid + (it0 + u) * f2::THREADS;
-            const int y = r0 + e / NB, x = c0 + e % NB;
-            const bool in = y < ny && x < nx;
-            const long long j = fp.face + (long long)y * nx + x;
-            zt[u] = in ? __ldg(args.in2 + j) : 0.0;
-            wt[u] = in ? __ldg(args.in3 + j) : 0.0;
+        for (int u = 0; u < U; ++u) {
+          const int e = tid + (it0 + u) * f2::THREADS;
+          const int mm = e / NB, n = e % NB;
+          const int y = r0 + mm, x = c0 + n;
+          const bool in = y < ny && x < nx;
+          double qn = 0.0;
+          if (in) {
+            const double qe = evaporation(fp, fp.recon_scale * (double)f2_tile(tile, mm, n));
+            args.out[fp.face + (long long)y * nx + x] = qe;
+            qn = ql[u] - qe;
           }
-#pragma unroll
-          for (int u = 0; u < U; ++u) {
-            const int e = tid + (it0 + u) * f2::THREADS;
-            const int m = e / NB, n = e % NB;
-            const int y = r0 + m, x = c0 + n;
-            const bool in = y < ny && x < nx;
-            double a = 0.0;
-            if (in) {
-              const double sg = fp.dct_scale * (double)f2_tile(tile, m, n);
-              args.out[fp.face + (long long)y * nx + x] = sg;
-              a = zt[u] + wt[u] * sg;
-            }
-            plane_put8_warp(v.xa + fp.xa, y, x, nkx, a, in);
-          }
+          plane_put8_warp(v.xq + fp.xa, y, x, nkx, qn, in);
         }
-      } else {
-        constexpr int U = 4;
-        for (int it0 = 0; it0 < ITEMS; it0 += U) {
-          long long idx[U];
-          double src[U];
+      }
+    } else if (KIND == F2_SIGMA) {
+      constexpr int U = 8;
+      for (int it0 = 0; it0 < ITEMS; it0 += U) {
+        double zt[U], wt[U];
 #pragma unroll
-          for (int u = 0; u < U; ++u) {
-            const int e = tid + (it0 + u) * f2::THREADS;
-            const int y = r0 + e / NB, x = c0 + e % NB;
-            idx[u] = (y < ny && x < nx) ? fp.face + (long long)y * nx + x : -1;
-            src[u] = (KIND == F2_COMMIT && idx[u] >= 0) ? __ldg(args.in2 + idx[u]) : 0.0;
+        for (int u = 0; u < U; ++u) {
+          const int e = tid + (it0 + u) * f2::THREADS;
+          const int y = r0 + e / NB, x = c0 + e % NB;
+          const bool in = y < ny && x < nx;
+          const long long j = fp.face + (long long)y * nx + x;
+          zt[u] = in ? __ldg(args.in2 + j) : 0.0;
+          wt[u] = in ? __ldg(args.in3 + j) : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          const int e = tid + (it0 + u) * f2::THREADS;
+          const int mm = e / NB, n = e % NB;
+          const int y = r0 + mm, x = c0 + n;
+          const bool in = y < ny && x < nx;
+          double a = 0.0;
+          if (in) {
+            const double sg = fp.dct_scale * (double)f2_tile(tile, mm, n);
+            args.out[fp.face + (long long)y * nx + x] = sg;
+            a = zt[u] + wt[u] * sg;
           }
+          plane_put8_warp(v.xa + fp.xa, y, x, nkx, a, in);
+        }
+      }
+    } else {
+      constexpr int U = 4;
+      for (int it0 = 0; it0 < ITEMS; it0 += U) {
+        long long idx[U];
+        double src[U];
 #pragma unroll
-          for (int u = 0; u < U; ++u) {
-            if (idx[u] < 0) continue;
-            const int e = tid + (it0 + u) * f2::THREADS;
-            const double val = (double)f2_tile(tile, e / NB, e % NB);
-            if (KIND == F2_STORE) {
-              args.out[idx[u]] = args.scaled ? val * fp.dct_scale : val;
-            } else {  // F2_COMMIT
-              const double T = fp.recon_scale * val;
-              args.out[idx[u]] = T;
-              args.out2[idx[u]] = src[u];
-              mx = fmax(mx, T);
-            }
+        for (int u = 0; u < U; ++u) {
+          const int e = tid + (it0 + u) * f2::THREADS;
+          const int y = r0 + e / NB, x = c0 + e % NB;
+          idx[u] = (y < ny && x < nx) ? fp.face + (long long)y * nx + x : -1;
+          src[u] = (KIND == F2_COMMIT && idx[u] >= 0) ? __ldg(args.in2 + idx[u]) : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          if (idx[u] < 0) continue;
+          const int e = tid + (it0 + u) * f2::THREADS;
+          const double val = (double)f2_tile(tile, e / NB, e % NB);
+          if (KIND == F2_STORE) {
+            args.out[idx[u]] = args.scaled ? val * fp.dct_scale : val;
+          } else {  // F2_COMMIT
+            const double T = fp.recon_scale * val;
+            args.out[idx[u]] = T;
+            args.out2[idx[u]] = src[u];
+            mx = fmax(mx, T);
           }
         }
       }
     }
-    __syncthreads();
   }
   tc_fence_before();
   __syncthreads();
-  if (warp == 0) tmem_dealloc(tmem, ncols);
+  if (warp == 0) tmem_dealloc(tmem, f2::TCOLS);
   if (KIND == F2_COMMIT) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_down_sync(0xffffffffu, mx, o));
@@ -1221,9 +1250,8 @@ struct sgh_batch {
   long long tot_e = 0;
   size_t o_qlas, o_qnet, o_qev, o_qevold, o_Stop, o_f1, o_sigma, o_A, o_Tsurf, o_Zt, o_Yt, o_Wtt, o_Qtt;
   size_t o_plas, o_pn1, o_prelax, o_ptile;
-  size_t o_xa = 0, o_xq = 0, o_mp = 0;  // operand pair planes (mixed)
-  size_t xa_bytes = 0, mp_bytes = 0;
-  int f2_stages = 0, f2_bop = 0, f2_smem = 0;  // fused face transform: ring stages, operand bytes, smem
+  size_t o_xa = 0, o_xq = 0, o_mp = 0, o_x1 = 0;  // operand pair planes (mixed)
+  size_t xa_bytes = 0, mp_bytes = 0, x1_bytes = 0;
   int vec = 1;  // columns per thread of the volume passes
   int vol_unroll = 4;  // z-planes per load round of the volume passes (2, 4 or 8)
   std::vector<std::pair<int, long long>> mplane_list;  // (N, byte offset of the forward plane)
@@ -1250,6 +1278,7 @@ struct sgh_batch {
     const bool mixed = precision == SGH_PRECISION_MIXED;
     v.xa = mixed ? ws + o_xa : nullptr;
     v.xq = mixed ? ws + o_xq : nullptr;
+    v.x1 = mixed ? ws + o_x1 : nullptr;
     v.mp = mixed ? ws + o_mp : nullptr;
     v.mats = d(o_mats);
     v.Ct = d(o_ct);
@@ -1275,16 +1304,17 @@ thread_local int g_blaunch = 0;
 
 // One 2-D transform of the top faces of all slots: the FP64 register-tiled
 // contraction as an x-pass (in -> f1) and a y-pass (f1 -> epilogue ef), or,
-// in mixed precision, one fused tensor-core launch with epilogue KIND
-// reading the xa (inverse) or xq (forward) operand plane.
+// in mixed precision, the tensor-core x-pass of the xa (inverse) or xq
+// (forward) operand plane into the x1 planes and the y-pass with epilogue KIND.
 template <bool INV, bool SKIP, int KIND, class EpiF>
 void face2d(sgh_batch* B, cudaStream_t s, const double* in, const EpiF& ef, const F2Args& fa, double* part) {
   const BView v = B->view();
   if (B->precision == SGH_PRECISION_MIXED) {
-    (void)cudaFuncSetAttribute(kb_face2d<INV, SKIP, KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               B->f2_smem);
-    kb_face2d<INV, SKIP, KIND><<<B->tot_utile, f2::THREADS, B->f2_smem, s>>>(v, fa, part, B->f2_stages, B->f2_bop);
-    ++g_blaunch;
+    (void)cudaFuncSetAttribute(kb_fx<INV, SKIP>, cudaFuncAttributeMaxDynamicSharedMemorySize, f2::SMEM);
+    (void)cudaFuncSetAttribute(kb_fy<INV, SKIP, KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize, f2::SMEM);
+    kb_fx<INV, SKIP><<<B->tot_utile, f2::THREADS, f2::SMEM, s>>>(v);
+    kb_fy<INV, SKIP, KIND><<<B->tot_utile, f2::THREADS, f2::SMEM, s>>>(v, fa, part);
+    g_blaunch += 2;
   } else {
     kb_face_axis<0, INV, SKIP, EB_Store><<<B->tot_tile, AX_THREADS, 0, s>>>(v, in, EB_Store{B->d(B->o_f1), 0},
                                                                             nullptr);
@@ -1464,8 +1494,6 @@ int sgh_batch_create(const sgh_config* cfgs, int32_t n, int32_t precision, sgh_b
       rc = bfail(SGH_ERR_UNSUPPORTED,
                  where + "batches step the face-space form only (no latent heat, no T-dependent model, "
                          "no convection); use a single-instance plan");
-    else if (precision == SGH_PRECISION_MIXED && c.ny > f2::MAX_NY)
-      rc = bfail(SGH_ERR_UNSUPPORTED, where + "mixed-precision batches need ny <= 256");
     if (rc) {
       delete B;
       return rc;
@@ -1520,6 +1548,8 @@ int sgh_batch_create(const sgh_config* cfgs, int32_t n, int32_t precision, sgh_b
     if (precision == SGH_PRECISION_MIXED) {
       sl.xa = (long long)B->xa_bytes;
       B->xa_bytes += umma::pair_bytes<128>(c.ny, c.nx);
+      sl.x1 = (long long)B->x1_bytes;
+      B->x1_bytes += x1_bytes(c.nx, c.ny);
       sl.mpx = mplane[c.nx] + 2LL * (long long)umma::pair_bytes<128>(c.nx, c.nx);
       sl.mpx_inv = sl.mpx + (long long)umma::pair_bytes<f2::NB>(c.nx, c.nx);
       sl.mpy = mplane[c.ny];
@@ -1605,13 +1635,7 @@ int sgh_batch_create(const sgh_config* cfgs, int32_t n, int32_t precision, sgh_b
     B->o_xa = L.take(B->xa_bytes);
     B->o_xq = L.take(B->xa_bytes);
     B->o_mp = L.take(B->mp_bytes);
-  }
-  if (precision == SGH_PRECISION_MIXED) {
-    int max_ny = 0;
-    for (int i = 0; i < n; ++i) max_ny = std::max(max_ny, cfgs[i].ny);
-    B->f2_bop = f2::bop_bytes(max_ny);
-    B->f2_stages = f2::stages(max_ny);
-    B->f2_smem = f2::smem_bytes(max_ny);
+    B->o_x1 = L.take(B->x1_bytes);
   }
   B->ws_need = L.off;
   *out = B;

@@ -164,10 +164,23 @@ def test_odd_shapes_mixed_batch_vs_oracle_and_alone():
     mix.close()
 
 
-def test_mixed_batch_rejects_tall_faces():
+def test_mixed_batch_tall_faces_vs_oracle():
+    """ny = 300 and nx = 72: three 128-row tiles per column block, the last
+    one ragged, and a ragged second column block, in both face passes."""
+    from oracle.sgh_oracle import OracleSolver
     from spectral_galerkin_heat_b200.batch import BatchSolver
-    with pytest.raises(Exception, match="ny <= 256"):
-        BatchSolver([_ctx(64, 300, 8, seed=1, steps=2)], "mixed")
+    steps = 4
+    ctx = _ctx(72, 300, 8, seed=1, steps=steps)
+    mix = BatchSolver([ctx], "mixed")
+    mix.start(0, steps)
+    mix.step(steps)
+    assert mix.tensor_core_error() == 0
+    o = OracleSolver(ctx)
+    o.initialize()
+    for k in range(steps):
+        o.step(k * ctx.num.dt, ctx.num.dt)
+    assert rel_l2(mix.modes(0).double().cpu().numpy(), o.a) < 1e-4
+    mix.close()
 
 
 @pytest.mark.parametrize("precision", ["mixed", "fp64"])

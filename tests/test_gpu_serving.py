@@ -162,3 +162,27 @@ def test_serving_lanes_same_result_as_alone():
     for r in reqs:
         assert np.array_equal(r.modes.cpu().numpy(), _alone(r, "mixed").cpu().numpy()), r.id
     eng.close()
+
+
+@pytest.mark.parametrize("mesh", [(512, 256, 16), (256, 128, 16)])
+def test_mixed_largest_classes_first_steps_vs_fp64(mesh):
+    """The largest serving classes in the benchmarked one-pass form (eight and
+    four 64-column blocks, two and one 128-row tiles per face transform),
+    two steps from the start, before the evaporation feedback can amplify
+    rounding: the mixed batch stays within 1e-4 of the FP64 solver."""
+    from spectral_galerkin_heat_b200 import B200SpectralSolver, workloads
+    from spectral_galerkin_heat_b200.batch import BatchSolver
+    from spectral_galerkin_heat_b200.laser import StraightTrack
+    steps = 2
+    cfg = workloads.serving_config(*mesh)
+    ctx = make_context(cfg, StraightTrack(0.3e-3, 0.5e-3, 1.0, 0.0, 300.0))
+    mix = BatchSolver([ctx], "mixed")
+    mix.start(0, steps)
+    mix.step(steps)
+    assert mix.tensor_core_error() == 0
+    s = B200SpectralSolver(None, copy.copy(ctx))
+    s.initialize()
+    s.run(0.0, steps)
+    assert rel_l2(mix.modes(0).double().cpu().numpy(), s.state.a.cpu().numpy()) < 1e-4
+    s.finalize()
+    mix.close()
