@@ -381,6 +381,7 @@ def run_b200(args, rank, world, local_rank):
     if args.workload in ("raster", "box") and not args.no_mixed:
         mixed = _mixed_volume_comparison(args, cfg, path, dev, flush)
         mixed["mixed_over_fp64"] = mixed["mixed_tol"]["value"] / line["value"]
+        mixed["mixed_over_fp64_same_tol"] = mixed["mixed_tol"]["value"] / mixed["fp64_at_mixed_tol"]["value"]
         line["comparisons"] = {"mixed_precision": mixed}
     if world == 1 and not args.no_cpu_baseline:
         v, n, el = cpu_baseline(cfg, path, budget_s=args.cpu_budget)
@@ -408,8 +409,8 @@ def _mixed_volume_comparison(args, cfg, path, dev, flush):
     from spectral_galerkin_heat_b200.precision import compare_fields
     stream = torch.cuda.current_stream(dev)
 
-    def timed(tol, steps):
-        s = B200SpectralSolver(None, _context(cfg, path), precision="mixed", convergence_tol=tol)
+    def timed(tol, steps, precision="mixed"):
+        s = B200SpectralSolver(None, _context(cfg, path), precision=precision, convergence_tol=tol)
         s.initialize()
         W = args.warmup
         table = s.laser_table(0.0, W + steps)
@@ -431,8 +432,13 @@ def _mixed_volume_comparison(args, cfg, path, dev, flush):
         return {"value": steps / (ms * 1e-3), "unit": "steps/s", "steps": steps, "picard_tol": tol,
                 "picard_iters_mean": float(np.mean([r.n_iter for r in recs])), "step_status": st}
 
+    # the mixed plan at its tolerance and at the FP64 one, and the FP64 plan at
+    # the mixed tolerance (the like-for-like rate: most of the mixed error
+    # against FP64 at 1e-8 is the looser tolerance, which FP64 at that
+    # tolerance shares)
     out = {"mixed_tol": timed(args.mixed_tol, args.steps),
-           "fp64_tol": timed(float(cfg["simulation"].get("picard_tol", 1e-4)), min(args.steps, 3))}
+           "fp64_tol": timed(float(cfg["simulation"].get("picard_tol", 1e-4)), min(args.steps, 3)),
+           "fp64_at_mixed_tol": timed(args.mixed_tol, args.steps, precision="fp64")}
     n = args.mixed_error_steps
     f64 = B200SpectralSolver(None, _context(cfg, path))
     f64.initialize()
@@ -804,21 +810,26 @@ def run_serving(args, rank, world, local_rank):
     # the evaporation solved to its Picard fixed point, where the problem is
     # well conditioned over any horizon
     acc_one, acc_conv = [], []
+    horizons = sorted({h for h in (5, 10, 20, args.horizon_steps) if h <= args.horizon_steps})
     for m in [(512, 256, 64), (256, 128, 32), (128, 64, 16), (64, 32, 16)]:
         r = next(q for q in sat if q["mesh"] == m)
         cfg = workloads.serving_config(*m)
-        rep = run_study(cfg, r["path"], [args.horizon_steps])[-1]
-        acc_one.append({"mesh": list(m), "steps": args.horizon_steps,
-                        "rel_l2": rep["mixed"]["rel_l2"], "peak_T_err_K": rep["mixed"]["peak_T_err_K"],
-                        "fp64_perturbed_rel_l2": rep["fp64_perturbed"]["rel_l2"],
-                        "fp64_fp32_rounded_rel_l2": rep["fp64_fp32_rounded"]["rel_l2"],
-                        "tensor_core_error": rep["tensor_core_error"]})
+        reps = run_study(cfg, r["path"], horizons)
+        curve = [{"steps": q["step"], "rel_l2": q["mixed"]["rel_l2"], "peak_T_err_K": q["mixed"]["peak_T_err_K"],
+                  "fp64_perturbed_rel_l2": q["fp64_perturbed"]["rel_l2"],
+                  "fp64_fp32_every_step_rel_l2": q["fp64_fp32_every_step"]["rel_l2"],
+                  "fp64_fp32_rounded_once_rel_l2": q["fp64_fp32_rounded"]["rel_l2"]} for q in reps]
+        # the last horizon at which the mixed error is within the bound
+        ok = [c for c in curve if c["rel_l2"] <= 1e-4]
+        acc_one.append({"mesh": list(m), "curve": curve,
+                        "steps_within_bound": ok[-1]["steps"] if ok else 0,
+                        "tensor_core_error": max(q["tensor_core_error"] for q in reps)})
         rep = run_study(cfg, r["path"], [min(r["steps"], args.accuracy_steps)],
                         picard={"max_picard_iter": 400, "picard_omega": 0.1, "picard_tol": 1e-8})[-1]
         acc_conv.append({"mesh": list(m), "steps": min(r["steps"], args.accuracy_steps),
                          "rel_l2": rep["mixed"]["rel_l2"], "peak_T_err_K": rep["mixed"]["peak_T_err_K"],
                          "fp64_perturbed_rel_l2": rep["fp64_perturbed"]["rel_l2"],
-                         "fp64_fp32_rounded_rel_l2": rep["fp64_fp32_rounded"]["rel_l2"],
+                         "fp64_fp32_every_step_rel_l2": rep["fp64_fp32_every_step"]["rel_l2"],
                          "tensor_core_error": rep["tensor_core_error"]})
     if any(a["tensor_core_error"] for a in acc_one + acc_conv):
         raise RuntimeError("a tensor-core wait ran out in the accuracy runs")
@@ -870,12 +881,18 @@ def run_serving(args, rank, world, local_rank):
             "mixed_over_plain_fp64": value / plain, "mixed_over_batched_fp64": value / fb},
         "accuracy": {"vs": "FP64 single-instance solver (matches the reference to 1e-10)",
                      "physics": "the benchmarked serving physics: one forcing pass per step",
-                     "steps": args.horizon_steps,
-                     "note": "fp64_perturbed_rel_l2: distance of an FP64 run started one part in "
-                             "1e12 away; fp64_fp32_rounded_rel_l2: distance of an FP64 run whose modes "
-                             "were rounded to FP32 once after the first step (the floor of any FP32 "
-                             "modal state). Where the latter is large the one-pass form is "
-                             "ill-conditioned at that grid and no precision can do better",
+                     "horizons": horizons,
+                     "note": "per grid, the mixed error against FP64 after 5..40 steps beside three "
+                             "FP64 references: fp64_perturbed (started one part in 1e12 away: its "
+                             "growth is the amplification of the explicit evaporation feedback), "
+                             "fp64_fp32_every_step (modes rounded to FP32 after every step, all else "
+                             "FP64) and fp64_fp32_rounded_once. The split-BF16 operands carry about "
+                             "17 significant bits (x = hi + lo to 2^-17), so the mixed form starts "
+                             "near 1e-6..1e-5 per step, above an FP32 state alone; where the feedback "
+                             "amplifies (fp64_perturbed growing ~1000x from 20 to 40 steps at 512x256 "
+                             "and 256x128) that error leaves the bound after steps_within_bound steps. "
+                             "accuracy_picard_converged holds the same grids with the feedback solved "
+                             "to its fixed point",
                      "runs": acc_one, "bound": 1e-4},
         "accuracy_picard_converged": {
             "physics": "the same requests with the evaporation solved to its Picard fixed point "

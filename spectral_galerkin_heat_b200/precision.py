@@ -19,8 +19,11 @@ For one configuration and laser path this runs, side by side on the device:
   FP32 once, after the first step. A random perturbation of the whole volume
   mostly lands in fast-decaying modes; this one has the structure of the
   rounding that an FP32 modal state undergoes every step, so it shows how far
-  a single such rounding carries on this problem (the floor of any form that
-  stores the state in FP32).
+  a single such rounding carries on this problem.
+* ``fp64_fp32_every_step``: the FP64 solver with its modes rounded to FP32
+  after every step -- the error of an FP32 modal state alone, with every
+  contraction and all physics in FP64: the floor of any form that keeps the
+  state in FP32, as the mixed form does.
 
 At each checkpoint step the report gives, against ``fp64``:
 
@@ -50,7 +53,7 @@ from typing import Dict, List, Optional, Sequence
 
 import numpy as np
 
-__all__ = ["melt_pool", "melt_pool_nodal", "compare_fields", "run_study"]
+__all__ = ["melt_pool", "melt_pool_nodal", "compare_fields", "run_study", "run_volume_study"]
 
 
 def melt_pool(T: np.ndarray, dx: float, dy: float, dz: float, T_melt: float) -> Dict[str, float]:
@@ -131,7 +134,7 @@ def compare_fields(T: np.ndarray, T_ref: np.ndarray, cell, T_melt: float,
 
 def run_study(cfg: dict, path, checkpoints: Sequence[int], picard: Optional[dict] = None,
               perturb: float = 1e-12, seed: int = 0) -> List[Dict[str, object]]:
-    """Step the three runs to each checkpoint and compare (see the module doc)."""
+    """Step the runs to each checkpoint and compare (see the module doc)."""
     import torch
 
     from . import kernels
@@ -165,6 +168,8 @@ def run_study(cfg: dict, path, checkpoints: Sequence[int], picard: Optional[dict
     rnd.initialize()
     rnd.run(0.0, 1)
     rnd.state.a.copy_(rnd.state.a.to(torch.float32).to(torch.float64))
+    ev = B200SpectralSolver(None, copy.copy(ctx))
+    ev.initialize()
     mix = BatchSolver([copy.copy(ctx)], "mixed")
     mix.start(0, total, record=True)
 
@@ -175,16 +180,21 @@ def run_study(cfg: dict, path, checkpoints: Sequence[int], picard: Optional[dict
         per.run(done * dt, n)
         rnd.run(max(done, 1) * dt, cp - max(done, 1))
         f32_m = f32.run(done * dt, n)
+        for i in range(done, cp):
+            ev.run(i * dt, 1)
+            ev.state.a.copy_(ev.state.a.to(torch.float32).to(torch.float64))
         mix.step(n)
         done = cp
         T_ref = ref.volume_temperature().cpu().numpy()
         T_per = per.volume_temperature().cpu().numpy()
         T_rnd = rnd.volume_temperature().cpu().numpy()
+        T_ev = ev.volume_temperature().cpu().numpy()
         a_mix = mix.modes(0).to(torch.float64).contiguous()
         T_mix = ref.volume_temperature(a_mix).cpu().numpy()
         T_f32 = ref.volume_temperature(f32.state.a).cpu().numpy()
         nodes = {name: kernels.reconstruct_temperature_DCT(a, geo).cpu().numpy()
                  for name, a in (("ref", ref.state.a), ("per", per.state.a), ("rnd", rnd.state.a),
+                                 ("ev", ev.state.a),
                                  ("mix", a_mix), ("f32", f32.state.a.clone()))}
         mm = mix.metrics(0)[-1]
         out.append({
@@ -198,13 +208,99 @@ def run_study(cfg: dict, path, checkpoints: Sequence[int], picard: Optional[dict
                                              lengths),
             "fp64_fp32_rounded": compare_fields(T_rnd, T_ref, cell, T_melt, nodes["rnd"], nodes["ref"],
                                                 lengths),
+            "fp64_fp32_every_step": compare_fields(T_ev, T_ref, cell, T_melt, nodes["ev"], nodes["ref"],
+                                                   lengths),
             "tensor_core_error": mix.tensor_core_error(),
         })
     ref.finalize()
     per.finalize()
     rnd.finalize()
+    ev.finalize()
     f32.finalize()
     mix.close()
+    return out
+
+
+def run_volume_study(cfg: dict, path, checkpoints: Sequence[int], mixed_tol: float = 1e-5,
+                     perturb: float = 1e-12, seed: int = 0) -> List[Dict[str, object]]:
+    """The nonlinear volume step (latent heat, T-dependent properties,
+    evaporation, convection) in its single-instance plans: ``fp64`` at the
+    configuration's Picard tolerance, ``mixed`` (split-BF16 tensor-core
+    contractions, FP32 modal iterates, FP64 latent source, correction, fluxes
+    and norms) and ``fp32`` (FP32 CUDA-core contractions) at ``mixed_tol``,
+    ``fp64_mixed_tol`` (the FP64 plan at ``mixed_tol``: the part of the error
+    that the looser Picard tolerance alone causes) and ``fp64_perturbed``
+    (the FP64 plan from an initial field changed by ``perturb`` relative),
+    compared at each checkpoint step as in
+    :func:`run_study`. Each form's device time (CUDA events around its
+    table-driven runs), mean Picard iterations and step statuses are reported
+    beside the errors."""
+    import ctypes as C
+
+    import torch
+
+    from . import _lib, kernels
+    from .config import SimulationContext
+    from .solver import B200SpectralSolver
+    ctx = SimulationContext.from_dict(copy.deepcopy(cfg))
+    ctx.laser_path = path
+    Lx, Ly, Lz = cfg["domain"]["size"]
+    cell = (Lx / ctx.num.nx, Ly / ctx.num.ny, Lz / ctx.num.nz)
+    lengths = (Lx, Ly, Lz)
+    geo = SimpleNamespace(size=lengths)
+    T_melt = float(cfg["material"]["T_liquidus"])
+    forms = {
+        "fp64": B200SpectralSolver(None, copy.copy(ctx)),
+        "fp64_perturbed": B200SpectralSolver(None, copy.copy(ctx)),
+        "mixed": B200SpectralSolver(None, copy.copy(ctx), precision="mixed", convergence_tol=mixed_tol),
+        "fp32": B200SpectralSolver(None, copy.copy(ctx), precision="fp32", convergence_tol=mixed_tol),
+        "fp64_mixed_tol": B200SpectralSolver(None, copy.copy(ctx), convergence_tol=mixed_tol),
+    }
+    for s in forms.values():
+        s.initialize()
+    per = forms["fp64_perturbed"]
+    T0 = per.volume_temperature().cpu().numpy()
+    per.set_state(T0 * (1.0 + perturb * np.random.default_rng(seed).standard_normal(T0.shape)))
+    total = int(max(checkpoints))
+    osz = C.sizeof(_lib.SghStepOut)
+    tables = {k: s.laser_table(0.0, total) for k, s in forms.items()}
+    outs = {k: torch.zeros(total * osz, dtype=torch.uint8, device=s.state.workspace.device)
+            for k, s in forms.items()}
+    ms = {k: 0.0 for k in forms}
+    out, done = [], 0
+    for cp in sorted(set(int(c) for c in checkpoints)):
+        n = cp - done
+        for name, s in forms.items():
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(s.state.stream)
+            s.run_table(tables[name], outs[name], n, start=done)
+            e1.record(s.state.stream)
+            torch.cuda.synchronize()
+            ms[name] += e0.elapsed_time(e1)
+        done = cp
+        ref = forms["fp64"]
+        T_ref = ref.volume_temperature().cpu().numpy()
+        n_ref = kernels.reconstruct_temperature_DCT(ref.state.a, geo).cpu().numpy()
+        row = {"step": cp}
+        for name in ("mixed", "fp32", "fp64_mixed_tol", "fp64_perturbed"):
+            a = forms[name].state.a.clone()
+            row[name] = compare_fields(ref.volume_temperature(a).cpu().numpy(), T_ref, cell, T_melt,
+                                       kernels.reconstruct_temperature_DCT(a, geo).cpu().numpy(), n_ref,
+                                       lengths)
+        timing = {}
+        for k, s in forms.items():
+            recs = s.decode_outs(outs[k][:done * osz].cpu().numpy().tobytes(), done)
+            st = {}
+            for r in recs:
+                key = _lib.STEP_STATUS.get(r.status, str(r.status))
+                st[key] = st.get(key, 0) + 1
+            timing[k] = {"steps_per_s": done / (ms[k] * 1e-3),
+                         "picard_iters_mean": float(np.mean([r.n_iter for r in recs])), "step_status": st}
+        row["timing"] = timing
+        out.append(row)
+    for s in forms.values():
+        s.finalize()
     return out
 
 
@@ -212,11 +308,34 @@ def main(argv=None):
     from . import workloads
     ap = argparse.ArgumentParser(description="mixed-precision vs FP64 error report")
     ap.add_argument("--seed", type=int, default=0)
-    ap.add_argument("--mesh", type=int, nargs=3, default=[256, 128, 64])
-    ap.add_argument("--checkpoints", type=int, nargs="+", default=[20, 100, 500])
+    ap.add_argument("--mesh", type=int, nargs=3, default=None,
+                    help="grid (default 256 128 64; with --volume 128 64 32)")
+    ap.add_argument("--checkpoints", type=int, nargs="+", default=None,
+                    help="steps to compare at (default 20 100 500; with --volume 20 100 250 500 1000)")
+    ap.add_argument("--volume", action="store_true",
+                    help="the nonlinear raster (latent heat, T-dependent k and c_p, evaporation, "
+                         "convection; Picard to 1e-8 in FP64) in the single-instance plans")
+    ap.add_argument("--mixed-tol", type=float, default=1e-5, help="--volume: Picard tolerance of mixed/fp32")
     ap.add_argument("--out", default=None, help="write the JSON report here")
     args = ap.parse_args(argv)
-    nx, ny, nz = args.mesh
+    if args.volume:
+        nx, ny, nz = args.mesh or (128, 64, 32)
+        cps = args.checkpoints or [20, 100, 250, 500, 1000]
+        cfg, path = workloads.nonlinear_raster(seed=args.seed, nx=nx, ny=ny, nz=nz, steps=max(cps))
+        report = {"config": {"workload": "nonlinear raster", "mesh": [nx, ny, nz],
+                             "domain_m": cfg["domain"]["size"], "seed": args.seed,
+                             "dt_s": cfg["simulation"]["dt"],
+                             "fp64_picard_tol": cfg["simulation"]["picard_tol"],
+                             "mixed_picard_tol": args.mixed_tol},
+                  "checkpoints": run_volume_study(cfg, path, cps, mixed_tol=args.mixed_tol, seed=args.seed)}
+        text = json.dumps(report, indent=1)
+        if args.out:
+            with open(args.out, "w") as f:
+                f.write(text)
+        print(text)
+        return
+    nx, ny, nz = args.mesh or (256, 128, 64)
+    args.checkpoints = args.checkpoints or [20, 100, 500]
     cfg, path = workloads.precision_track(seed=args.seed, nx=nx, ny=ny, nz=nz)
     forms = {
         "one_pass": None,
