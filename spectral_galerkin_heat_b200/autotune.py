@@ -181,13 +181,25 @@ def batch_key(cfgs, precision: str) -> str:
     return f"{precision}|" + "+".join(f"{n}*{k}" for k, n in sorted(counts.items()))
 
 
+def _classes_of(key: str):
+    """(precision, set of slot classes) of a batch key, slot counts dropped."""
+    prec, _, mix = key.partition("|")
+    return prec, frozenset(part.split("*", 1)[1] for part in mix.split("+") if "*" in part)
+
+
 def lookup_batch(cfgs, precision: str) -> Optional[Dict]:
-    """Tuned policy for this batch's precision and grid mix, or None."""
+    """Tuned policy for this batch's precision and grid mix, or None. A mix
+    tuned with other slot counts of the same classes (a serving batch dealt
+    over lanes holds a share of every class) takes that entry's policy."""
     k = batch_key(cfgs, precision)
-    for path in (os.environ.get("SGH_TUNE_TABLE"), SHIPPED):
-        if path:
-            e = _load(path, "batch_entries").get(k)
-            if e is not None:
+    tables = [_load(p, "batch_entries") for p in (os.environ.get("SGH_TUNE_TABLE"), SHIPPED) if p]
+    for t in tables:
+        if k in t:
+            return dict(t[k]["policy"])
+    want = _classes_of(k)
+    for t in tables:
+        for kk, e in sorted(t.items()):
+            if _classes_of(kk) == want:
                 return dict(e["policy"])
     return None
 

@@ -39,3 +39,22 @@ def test_kernel_choice_and_box_form(tmp_path, monkeypatch):
     assert autotune.lookup_kernel(_cfg(40, 20, 6)) is None   # entries without a kernel choice
     assert autotune.lookup_kernel(_cfg(41, 20, 6)) is None   # no entry
     autotune._cache.clear()
+
+
+def test_batch_lookup_exact_then_same_classes(tmp_path, monkeypatch):
+    """A batch mix is looked up by its exact key first; a batch that holds
+    other slot counts of the same classes (a serving batch dealt over lanes)
+    takes the entry of that class set; another class set finds nothing."""
+    full = [_cfg(64, 32, 16)] * 4 + [_cfg(128, 64, 16)] * 4
+    half = [_cfg(64, 32, 16)] * 2 + [_cfg(128, 64, 16)] * 2
+    other = [_cfg(64, 32, 16)] * 2
+    table = tmp_path / "t.json"
+    table.write_text(json.dumps({"batch_entries": {
+        autotune.batch_key(full, "mixed"): {"policy": {"vol_unroll": 8, "vol_vec": 2}}}}))
+    monkeypatch.setenv("SGH_TUNE_TABLE", str(table))
+    autotune._cache.clear()
+    assert autotune.lookup_batch(full, "mixed") == {"vol_unroll": 8, "vol_vec": 2}
+    assert autotune.lookup_batch(half, "mixed") == {"vol_unroll": 8, "vol_vec": 2}
+    assert autotune.lookup_batch(other, "mixed") is None
+    assert autotune.lookup_batch(half, "fp64") is None
+    autotune._cache.clear()
