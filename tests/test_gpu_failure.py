@@ -58,7 +58,7 @@ def _mixed_batch(n_steps):
 
 
 def test_tensor_core_wait_runs_out_records_the_flag_and_returns():
-    """Every face-transform CTA first waits, with a bound of 2000 polls, on a
+    """Every face y-pass CTA first waits, with a bound of 2000 polls, on a
     barrier that nothing completes; each records the batch's error flag,
     waits for its bulk copies in flight (full bound), frees its tensor memory
     and returns. The host reads the flag; the context and a fresh batch still
