@@ -137,6 +137,14 @@ __device__ __forceinline__ void plane_put8_warp(char* plane, int r, int k0, int 
 // arena, null in FP64 batches), written by a whole block of consecutive i (one
 // slot per block). When nx % 8 == 0 every aligned group of 8 lanes is 8
 // consecutive x of one row and goes out as one 16-byte store per part.
+__device__ __forceinline__ void plane_put_yx(char* plane, const BSlot& sl, int y, int x, double val, bool valid) {
+  if (!plane) return;
+  const int nkc = (sl.nx + umma::KC - 1) / umma::KC;
+  if ((sl.nx & 7) == 0)
+    plane_put8_warp(plane + sl.xa, y, x, nkc, valid ? val : 0.0, valid);
+  else if (valid)
+    umma::pair_put<umma::TM>(plane + sl.xa, y, x, nkc, val);
+}
 __device__ __forceinline__ void plane_put_block(char* plane, const BSlot& sl, int i, double val, bool valid) {
   if (!plane) return;
   const int nkc = (sl.nx + umma::KC - 1) / umma::KC;
@@ -352,7 +360,15 @@ __global__ void __launch_bounds__(CT) kb_begin(BView v, cudaGraphConditionalHand
 
 // q_las, P_laser partials and q_net = q_las - shift(q_evap_old) per slot
 // (solvers/spectral.py:273-306).
-__global__ void __launch_bounds__(BT)
+//
+// Each element's (y, x) is formed once and serves the flux, the shift and the
+// operand plane. In mixed precision the point-sampled beam multiplies by the
+// radii's reciprocals; the FP64 batch divides, in the reference's operation
+// order, so that it tracks the single-instance plan to rounding. The register
+// cap keeps
+// three blocks per SM, so the FP64 arithmetic's fixed latencies are hidden by
+// more warps.
+__global__ void __launch_bounds__(BT, 3)
 kb_face_begin(BView v, double* q_las, double* q_net, const double* q_evold, double* part_las) {
   // RB elements per block (RPT per thread, consecutive across the block per
   // round); the four shift taps of U elements are gathered before their use
@@ -365,18 +381,23 @@ kb_face_begin(BView v, double* q_las, double* q_net, const double* q_evold, doub
   const int nx = sl.nx, ny = sl.ny;
   const double* f = q_evold + sl.face;
   const double I0 = st.I0, lx = st.laser.x, ly = st.laser.y, sx = st.shift_x, sy = st.shift_y;
+  const double dx = sl.dx, dy = sl.dy, irx = 1.0 / sl.r_x, iry = 1.0 / sl.r_y, order = sl.order;
+  const bool cell = sl.cell_integrated != 0, rcp = v.xq != nullptr;
   const int i0 = (b - sl.rblk0) * RB;
   double sum = 0.0, dummy = 0.0;
-  constexpr int U = 4;
+  constexpr int U = 2;
 #pragma unroll 1
   for (int u0 = 0; u0 < RPT; u0 += U) {
     double g[U][4], wy0[U], wy1[U], wx0[U], wx1[U];
     bool ok[U], in[U];
+    int ys[U], xs[U];
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       const int i = i0 + (u0 + u) * BT + threadIdx.x;
       ok[u] = i < sl.S;
       const int y = ok[u] ? i / nx : 0, x = ok[u] ? i - y * nx : 0;
+      ys[u] = y;
+      xs[u] = x;
       const ShiftTap ty = shift_tap(y, ny, sy);
       const ShiftTap tx = shift_tap(x, nx, sx);
       in[u] = ok[u] && ty.in && tx.in;
@@ -391,9 +412,16 @@ kb_face_begin(BView v, double* q_las, double* q_net, const double* q_evold, doub
       const int i = i0 + (u0 + u) * BT + threadIdx.x;
       double qn = 0.0;
       if (ok[u]) {
-        const int y = i / nx, x = i - y * nx;
-        const double xc = ((double)x + 0.5) * sl.dx, yc = ((double)y + 0.5) * sl.dy;
-        const double q = laser_flux(sl, I0, lx, ly, xc, yc);
+        const double xc = ((double)xs[u] + 0.5) * dx, yc = ((double)ys[u] + 0.5) * dy;
+        double q;
+        if (cell) {
+          q = laser_flux(sl, I0, lx, ly, xc, yc);
+        } else {  // point-sampled (super-)Gaussian (core/laser.py:42-53)
+          const double ux = rcp ? (xc - lx) * irx : (xc - lx) / sl.r_x;
+          const double uy = rcp ? (yc - ly) * iry : (yc - ly) / sl.r_y;
+          const double r2 = ux * ux + uy * uy;
+          q = I0 * ((order == 2.0) ? exp(-2.0 * r2) : exp(-2.0 * pow(r2, order / 2.0)));
+        }
         q_las[sl.face + i] = q;
         sum += q;
         // the bilinear shift (spectral_cpu_kernels.py:328-371), zero outside the grid
@@ -402,7 +430,7 @@ kb_face_begin(BView v, double* q_las, double* q_net, const double* q_evold, doub
         qn = q - val;
         q_net[sl.face + i] = qn;
       }
-      plane_put_block(v.xq, sl, i, qn, ok[u]);
+      plane_put_yx(v.xq, sl, ys[u], xs[u], qn, ok[u]);
     }
   }
   block_sum2<BT>(sum, dummy, sh);
