@@ -608,7 +608,8 @@ __device__ __forceinline__ int f2_prime(const F2Smem& m, int n, const Load& load
 // Thread 0: chunks 0..n-1 of the tile (chunk g in stage g % STAGES; each
 // barrier completes one phase per use of its stage, so chunk g waits for
 // parity (g / STAGES) & 1), MMAs into the accumulators at tmem, tmem + NB
-// and tmem + 2 NB, then the wait for the last MMAs. A wait that expires
+// and tmem + 2 NB, each stage refilled once its MMAs have drained, then the
+// wait for the last MMAs. A wait that expires
 // (after `lim` polls) records the error, clears the status flag and drains,
 // with the full bound, every copy and MMA in flight; returns false then.
 // stall: first wait on a barrier that nothing completes (the wait test).
@@ -642,9 +643,12 @@ __device__ bool f2_run(const F2Smem& m, int n, int issued, const Load& load, uin
     }
     mma_commit(&m.done[g % S]);
     committed = g + 1;
-    const int nxt = g - 1 + S;  // the stage of chunk g - 1 takes chunk g - 1 + S
-    if (g >= 1 && nxt < n && nxt >= issued) {
-      if (!mbar_wait_bounded(&m.done[(g - 1) % S], (uint32_t)(((g - 1) / S) & 1), lim)) {
+    // this stage takes chunk g + S as soon as its MMAs have drained (a few
+    // hundred cycles, against the L2 latency of a chunk), so every stage of
+    // the ring stays in flight
+    const int nxt = g + S;
+    if (nxt < n) {
+      if (!mbar_wait_bounded(&m.done[g % S], (uint32_t)((g / S) & 1), lim)) {
         ok = false;
         break;
       }
