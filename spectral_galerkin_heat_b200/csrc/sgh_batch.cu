@@ -1214,6 +1214,124 @@ kb_volume(BView v, R* a, const R* K, const R* KK, const double* sigma, double* Z
   }
 }
 
+// Mixed-precision volume pass with a shared-memory ring. The block's BT face
+// columns of each z-plane (FP32 modes: 1 KB, contiguous) arrive by one bulk
+// copy per plane, completing on that stage's mbarrier, RING planes ahead of
+// the arithmetic. The bytes in flight then come from shared memory, not from
+// registers. Arithmetic and outputs are those of kb_volume's FP32 path. A copy
+// wait that expires sets the batch's error flag; the block then waits (with
+// the full bound) for its copies in flight, writes a NaN norm partial so the
+// Picard test stops, and leaves its face sums unwritten.
+template <bool COMMIT, int RING>
+__global__ void __launch_bounds__(BT / 4, 16)
+kb_volume_ring(BView v, float* a, const double* sigma, double* Zt, double* Yt, double* part_n1) {
+  constexpr int VEC = 4, NT = BT / VEC;
+  __shared__ __align__(128) float ring[RING][BT];
+  __shared__ uint64_t full[RING];
+  __shared__ double sh[2 * (NT / 32)];
+  __shared__ int bad;
+  const int b = blockIdx.x;
+  const int s = v.blk_slot[b];
+  const BSlot& sl = v.slot[s];
+  BState& st = v.st[s];
+  if (!st.active || (!COMMIT && st.pass1_ready)) return;
+  const int base = (b - sl.blk0) * BT;  // first face column of the block
+  const int i0 = base + VEC * threadIdx.x;
+  const int ncol = min(BT, sl.S - base);  // positive; a multiple of 4 (S is)
+  const uint32_t bytes = (uint32_t)ncol * 4u;
+  const int nz = sl.nz;
+  float* col = a + sl.vol + base;  // plane p of the block at col + p * S (16-byte aligned)
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < RING; ++k) umma::mbar_init(&full[k], 1);
+    bad = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    for (int p = 0; p < RING && p < nz; ++p) {
+      umma::mbar_expect_tx(&full[p], bytes);
+      umma::bulk_g2s(ring[p], col + (size_t)p * sl.S, bytes, &full[p]);
+    }
+  }
+  __syncthreads();
+  const bool live = i0 < sl.S;
+  const double* ct = v.Ct + sl.zoff;
+  const int nsum = sl.nx + sl.ny + sl.nz;
+  const double* E = v.E + sl.eoff;
+  const double* ez = E + sl.nx + sl.ny;
+  const double* dz = ez + nsum;
+  const double* lz = ez + 2 * nsum;
+  const float dt_rc = (float)(sl.dt / (sl.rho * sl.cp));
+  double zt[VEC], yt[VEC], n1 = 0.0, dummy = 0.0;
+  float sg32[VEC], exy32[VEC], dxy32[VEC], lxy32[VEC];
+#pragma unroll
+  for (int c = 0; c < VEC; ++c) {
+    const int i = live ? i0 + c : 0;
+    const int ix = i % sl.nx, iy = sl.nx + i / sl.nx;
+    sg32[c] = (COMMIT && live) ? (float)sigma[sl.face + i] : 0.0f;
+    exy32[c] = (float)(E[ix] * E[iy]);
+    dxy32[c] = (float)(E[nsum + ix] + E[ix] * E[nsum + iy]);
+    lxy32[c] = (float)(E[2 * nsum + ix] + E[2 * nsum + iy]);
+    zt[c] = 0.0;
+    yt[c] = 0.0;
+  }
+  const unsigned lim = v.g->wait_limit ? v.g->wait_limit : umma::WAIT_LIMIT;
+  int p = 0;
+  for (; p < nz; ++p) {
+    const int k = p % RING;
+    const bool arrived = umma::mbar_wait_bounded(&full[k], (uint32_t)((p / RING) & 1), lim);
+    if (!arrived) bad = 1;
+    if (arrived && live) {
+      const double cp = ct[p];
+      const float cp32 = (float)cp, ez32 = (float)ez[p], dz32 = (float)dz[p], lz32 = (float)lz[p];
+      float4 x4 = *reinterpret_cast<const float4*>(&ring[k][VEC * threadIdx.x]);
+      float av[VEC] = {x4.x, x4.y, x4.z, x4.w};
+#pragma unroll
+      for (int c = 0; c < VEC; ++c) {
+        const float kv = exy32[c] * ez32;
+        const float num = fmaf(exy32[c], dz32, dxy32[c]);
+        const float den = lxy32[c] + lz32;
+        const float kk = den > 0.0f ? __fdividef(num, den) : dt_rc;
+        float x = av[c];
+        if (COMMIT) x = fmaf(x, kv, kk * (cp32 * sg32[c]));
+        av[c] = x;
+        const float ak = x * kv;
+        const double ak64 = (double)ak, akk64 = (double)(ak * kk);
+        zt[c] = fma(cp, ak64, zt[c]);
+        yt[c] = fma(akk64, cp, yt[c]);
+        n1 = fma(ak64, ak64, n1);
+      }
+      if (COMMIT) *reinterpret_cast<float4*>(col + (size_t)p * sl.S + VEC * threadIdx.x) =
+          make_float4(av[0], av[1], av[2], av[3]);
+    }
+    __syncthreads();  // stage k is consumed by every thread; `bad` is visible
+    if (bad) break;
+    if (threadIdx.x == 0 && p + RING < nz) {
+      umma::fence_proxy_async();
+      umma::mbar_expect_tx(&full[k], bytes);
+      umma::bulk_g2s(ring[k], col + (size_t)(p + RING) * sl.S, bytes, &full[k]);
+    }
+  }
+  if (bad) {  // planes p .. min(nz, p + RING) - 1 were issued and not all consumed
+    if (threadIdx.x == 0) {
+      atomicExch(&v.g->umma_err, 1);
+      for (int q = p; q < nz && q < p + RING; ++q)
+        umma::mbar_wait_bounded(&full[q % RING], (uint32_t)((q / RING) & 1), umma::WAIT_LIMIT);
+      part_n1[b] = nan("");
+    }
+    return;
+  }
+  if (live) {
+#pragma unroll
+    for (int c = 0; c < VEC; ++c) {
+      Zt[sl.face + i0 + c] = zt[c];
+      Yt[sl.face + i0 + c] = yt[c];
+    }
+  }
+  block_sum2<NT>(n1, dummy, sh);
+  if (threadIdx.x == 0) {
+    part_n1[b] = n1;
+    if (COMMIT) st.pass1_ready = 1;
+  }
+}
+
 // Metrics of every active slot (solvers/spectral.py:536-542), one warp per
 // slot; advances the step counters and decides whether the step loop goes on.
 __global__ void __launch_bounds__(CT)
@@ -1371,8 +1489,12 @@ void launch_volume(sgh_batch* B, cudaStream_t s, R* a, const R* K, const R* KK) 
     else go(vec, std::integral_constant<int, 4>{});
   };
   if constexpr (sizeof(R) == 4) {
-    if (B->vec == 4) {
-      with_u(std::integral_constant<int, 4>{});
+    if (B->vec == 4) {  // the ring form: 2 U planes of each block in flight
+      float* af = reinterpret_cast<float*>(a);
+      const int u = B->vol_unroll;
+      if (u == 2) kb_volume_ring<COMMIT, 4><<<B->tot_blk, BT / 4, 0, s>>>(v, af, sg, zt, yt, pn);
+      else if (u == 8) kb_volume_ring<COMMIT, 16><<<B->tot_blk, BT / 4, 0, s>>>(v, af, sg, zt, yt, pn);
+      else kb_volume_ring<COMMIT, 8><<<B->tot_blk, BT / 4, 0, s>>>(v, af, sg, zt, yt, pn);
       return;
     }
   }
