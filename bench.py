@@ -63,9 +63,10 @@ METRIC = "timesteps/s"
 L2_FLUSH_BYTES = 256 << 20
 # dram__bytes_read.sum + dram__bytes_write.sum of the dominant kernel from ncu
 # captures (ncu --set full, one launch): the serving volume pass on the 24-slot
-# case (2 slots per class) moved 277.75 MB for 38,993,920 modes; the benchmark's
-# 192-slot case has the same class mix, so traffic scales with the modes.
-NCU_VOLUME_TRAFFIC_PER_MODE = 277.75e6 / 38993920
+# case (2 slots per class) moved 277.1 MB for 38,993,920 modes
+# (dram__bytes.sum.per_second x gpu__time_duration.sum); the benchmark's case
+# has the same class mix, so traffic scales with the modes.
+NCU_VOLUME_TRAFFIC_PER_MODE = 277.1e6 / 38993920
 # the raster workload's dominant kernel (k_axis) was captured on the same
 # 128x64x32 case: 2.14 MB for one contiguous-axis pass (field resident in L2)
 NCU_TRAFFIC_BYTES = 2.14e6
@@ -903,7 +904,7 @@ def run_serving(args, rank, world, local_rank):
                 "h2d_bytes_per_step": e2e["h2d"] / K, "d2h_bytes_per_step": e2e["d2h"] / K,
                 "completed_in_timed_region": e2e["completed"],
                 "api": "ServingEngine.run (host laser tables in, result surfaces out)"},
-        "roofline": {"kernel": "kb_volume<float,4,commit> (modal commit fused with the next step face sums)", "bound": "hbm",
+        "roofline": {"kernel": "kb_volume_ring<commit> (modal commit fused with the next step face sums, planes staged by bulk copies)", "bound": "hbm",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_source": peak_kind,
                      "traffic": (NCU_VOLUME_TRAFFIC_PER_MODE * modes
@@ -1096,7 +1097,7 @@ def run_batch(args, rank, world, local_rank):
         "e2e": {"value": e2e["slot_steps"] * world / (t[1] * 1e-3), "unit": "timesteps/s",
                 "h2d_bytes_per_step": 0, "d2h_bytes_per_step": e2e["d2h"] / K,
                 "api": "BatchSolver.step + status per step (laser tables resident from start)"},
-        "roofline": {"kernel": "kb_volume<float,4,commit>", "bound": "hbm", "achieved": achieved, "peak": peak,
+        "roofline": {"kernel": "kb_volume_ring<commit>", "bound": "hbm", "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
                      "traffic": NCU_VOLUME_TRAFFIC_PER_MODE * mixed["modes"],
                      "algorithmic_bytes_per_launch": mixed["vp_bytes"]},
