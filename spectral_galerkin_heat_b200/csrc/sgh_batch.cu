@@ -529,10 +529,10 @@ constexpr int NB = 64;                       // column block (MMA N)
 constexpr int CA = umma::CHUNK_BYTES;        // 128 x 32 BF16 chunk of an A operand (8 KB)
 constexpr int CBN = NB * umma::KC * 2;       // NB x 32 BF16 chunk of a B operand (4 KB)
 constexpr int STAGE = 2 * CA + 2 * CBN;      // 24 KB: A hi/lo + B hi/lo
-constexpr int STAGES = 4;
+constexpr int STAGES = 3;
 constexpr int TAIL = 128;                    // barriers, TMEM address, status flag
-constexpr int SMEM = STAGES * STAGE + TAIL;  // 98,432 bytes: two CTAs per SM
-constexpr uint32_t TCOLS = 256;              // three NB-column accumulators
+constexpr int SMEM = STAGES * STAGE + TAIL;  // 73,856 bytes: three CTAs per SM
+constexpr uint32_t TCOLS = 128;              // two NB-column accumulators
 }  // namespace f2
 
 // Tensor-core face tiles of a slot: 128-row tiles x NB-column blocks.
@@ -639,7 +639,7 @@ __device__ bool f2_run(const F2Smem& m, int n, int issued, const Load& load, uin
       const uint32_t acc = (g > 0 || k > 0) ? 1u : 0u;
       mma_bf16(tmem, dah, dbh, idesc, acc);
       mma_bf16(tmem + NB, dah, dbl, idesc, acc);
-      mma_bf16(tmem + 2 * NB, dal, dbh, idesc, acc);
+      mma_bf16(tmem + NB, dal, dbh, idesc, 1u);
     }
     mma_commit(&m.done[g % S]);
     committed = g + 1;
@@ -668,18 +668,17 @@ __device__ bool f2_run(const F2Smem& m, int n, int issued, const Load& load, uin
   return ok;
 }
 
-// 32 x 16 accumulator values of this warp's lane quarter: the three parts summed.
+// 32 x 16 accumulator values of this warp's lane quarter: the parts summed.
 __device__ __forceinline__ void f2_read16(uint32_t ta, float (&x)[16]) {
-  float p1[16], p2[16];
+  float p1[16];
   umma::tmem_ld16(ta, x);
   umma::tmem_ld16(ta + f2::NB, p1);
-  umma::tmem_ld16(ta + 2 * f2::NB, p2);
 #pragma unroll
-  for (int i = 0; i < 16; ++i) x[i] = x[i] + (p1[i] + p2[i]);
+  for (int i = 0; i < 16; ++i) x[i] = x[i] + p1[i];
 }
 
 template <bool INV, bool SKIP_DONE>
-__global__ void __launch_bounds__(f2::THREADS, 2) kb_fx(BView v) {
+__global__ void __launch_bounds__(f2::THREADS, 3) kb_fx(BView v) {
   using namespace umma;
   constexpr int CA = f2::CA, CBN = f2::CBN, NB = f2::NB;
   extern __shared__ __align__(128) char sm[];
@@ -749,7 +748,7 @@ __global__ void __launch_bounds__(f2::THREADS, 2) kb_fx(BView v) {
 }
 
 template <bool INV, bool SKIP_DONE, int KIND>
-__global__ void __launch_bounds__(f2::THREADS, 2) kb_fy(BView v, F2Args args, double* part_tile) {
+__global__ void __launch_bounds__(f2::THREADS, 3) kb_fy(BView v, F2Args args, double* part_tile) {
   using namespace umma;
   constexpr int CA = f2::CA, CBN = f2::CBN, NB = f2::NB;
   extern __shared__ __align__(128) char sm[];
