@@ -529,9 +529,9 @@ constexpr int NB = 64;                       // column block (MMA N)
 constexpr int CA = umma::CHUNK_BYTES;        // 128 x 32 BF16 chunk of an A operand (8 KB)
 constexpr int CBN = NB * umma::KC * 2;       // NB x 32 BF16 chunk of a B operand (4 KB)
 constexpr int STAGE = 2 * CA + 2 * CBN;      // 24 KB: A hi/lo + B hi/lo
-constexpr int STAGES = 3;
+constexpr int STAGES = 2;
 constexpr int TAIL = 128;                    // barriers, TMEM address, status flag
-constexpr int SMEM = STAGES * STAGE + TAIL;  // 73,856 bytes: three CTAs per SM
+constexpr int SMEM = STAGES * STAGE + TAIL;  // 49,280 bytes: four CTAs per SM
 constexpr uint32_t TCOLS = 128;              // two NB-column accumulators
 }  // namespace f2
 
@@ -678,7 +678,7 @@ __device__ __forceinline__ void f2_read16(uint32_t ta, float (&x)[16]) {
 }
 
 template <bool INV, bool SKIP_DONE>
-__global__ void __launch_bounds__(f2::THREADS, 3) kb_fx(BView v) {
+__global__ void __launch_bounds__(f2::THREADS, 4) kb_fx(BView v) {
   using namespace umma;
   constexpr int CA = f2::CA, CBN = f2::CBN, NB = f2::NB;
   extern __shared__ __align__(128) char sm[];
@@ -748,7 +748,7 @@ __global__ void __launch_bounds__(f2::THREADS, 3) kb_fx(BView v) {
 }
 
 template <bool INV, bool SKIP_DONE, int KIND>
-__global__ void __launch_bounds__(f2::THREADS, 3) kb_fy(BView v, F2Args args, double* part_tile) {
+__global__ void __launch_bounds__(f2::THREADS, 4) kb_fy(BView v, F2Args args, double* part_tile) {
   using namespace umma;
   constexpr int CA = f2::CA, CBN = f2::CBN, NB = f2::NB;
   extern __shared__ __align__(128) char sm[];
