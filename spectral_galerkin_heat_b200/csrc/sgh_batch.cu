@@ -515,14 +515,17 @@ __global__ void __launch_bounds__(AX_THREADS) kb_face_axis(BView v, const double
 // Each CTA computes one 128-row x NB-column tile of one slot (MMA M = 128,
 // N = NB). One thread streams the tile's operand chunks -- BF16 hi + lo, one
 // bulk copy per operand and 32-slice chunk -- through a ring of f2::STAGES
-// stages and issues three split-BF16 MMAs per 16-slice step (hi.hi, hi.lo,
-// lo.hi, each its own FP32 accumulator chain in tensor memory, summed when
-// read out); the ring is primed before the tensor memory is allocated.
+// stages and issues three split-BF16 MMAs per 16-slice step (hi.hi into one
+// FP32 accumulator in tensor memory, hi.lo and lo.hi into a second; the two
+// are summed when read out); the ring is primed before the tensor memory is
+// allocated.
 // kb_fx writes X1, split into BF16 hi + lo, to the slot's x1 plane, chunked
 // and laid out exactly as the B operand chunks of kb_fy, which streams it
-// like any other operand. Separability makes the tiles independent. Shared
-// memory (4 stages of 24 KB) and tensor memory (256 columns) allow two CTAs
-// per SM, so one CTA's epilogue overlaps another's copies and MMAs.
+// like any other operand. Separability makes the tiles independent. A tile
+// is a latency chain of nx/32 or ny/32 chunks, so concurrency decides the
+// rate: shared memory (2 stages of 24 KB) and tensor memory (128 columns)
+// allow four CTAs per SM, whose copies, MMAs and epilogues overlap (measured
+// against 2 CTAs x 4 stages and 3 x 3: 4 x 2 is the fastest).
 namespace f2 {
 constexpr int THREADS = 256;
 constexpr int NB = 64;                       // column block (MMA N)
@@ -607,9 +610,9 @@ __device__ __forceinline__ int f2_prime(const F2Smem& m, int n, const Load& load
 
 // Thread 0: chunks 0..n-1 of the tile (chunk g in stage g % STAGES; each
 // barrier completes one phase per use of its stage, so chunk g waits for
-// parity (g / STAGES) & 1), MMAs into the accumulators at tmem, tmem + NB
-// and tmem + 2 NB, each stage refilled once its MMAs have drained, then the
-// wait for the last MMAs. A wait that expires
+// parity (g / STAGES) & 1), MMAs into the accumulators at tmem (hi.hi) and
+// tmem + NB (hi.lo, lo.hi), each stage refilled once its MMAs have drained,
+// then the wait for the last MMAs. A wait that expires
 // (after `lim` polls) records the error, clears the status flag and drains,
 // with the full bound, every copy and MMA in flight; returns false then.
 // stall: first wait on a barrier that nothing completes (the wait test).
