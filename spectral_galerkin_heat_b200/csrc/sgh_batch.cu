@@ -1227,8 +1227,9 @@ kb_volume(BView v, R* a, const R* K, const R* KK, const double* sigma, double* Z
 template <bool COMMIT, int RING>
 __global__ void __launch_bounds__(BT / 4, 16)
 kb_volume_ring(BView v, float* a, const double* sigma, double* Zt, double* Yt, double* part_n1) {
-  constexpr int VEC = 4, NT = BT / VEC;
+  constexpr int VEC = 4, NT = BT / VEC, TABMAX = 256;
   __shared__ __align__(128) float ring[RING][BT];
+  __shared__ float ztab[4][TABMAX];  // Ct, Ez, 1 - Ez, L_z of each plane in FP32 (nz <= TABMAX)
   __shared__ uint64_t full[RING];
   __shared__ double sh[2 * (NT / 32)];
   __shared__ int bad;
@@ -1243,6 +1244,20 @@ kb_volume_ring(BView v, float* a, const double* sigma, double* Zt, double* Yt, d
   const uint32_t bytes = (uint32_t)ncol * 4u;
   const int nz = sl.nz;
   float* col = a + sl.vol + base;  // plane p of the block at col + p * S (16-byte aligned)
+  const double* ct = v.Ct + sl.zoff;
+  const int nsum = sl.nx + sl.ny + sl.nz;
+  const double* E = v.E + sl.eoff;
+  const double* ez = E + sl.nx + sl.ny;
+  const double* dz = ez + nsum;
+  const double* lz = ez + 2 * nsum;
+  const bool tabbed = nz <= TABMAX;  // the per-plane constants converted once per block
+  if (tabbed)
+    for (int p = threadIdx.x; p < nz; p += NT) {
+      ztab[0][p] = (float)ct[p];
+      ztab[1][p] = (float)ez[p];
+      ztab[2][p] = (float)dz[p];
+      ztab[3][p] = (float)lz[p];
+    }
   if (threadIdx.x == 0) {
     for (int k = 0; k < RING; ++k) umma::mbar_init(&full[k], 1);
     bad = 0;
@@ -1254,12 +1269,6 @@ kb_volume_ring(BView v, float* a, const double* sigma, double* Zt, double* Yt, d
   }
   __syncthreads();
   const bool live = i0 < sl.S;
-  const double* ct = v.Ct + sl.zoff;
-  const int nsum = sl.nx + sl.ny + sl.nz;
-  const double* E = v.E + sl.eoff;
-  const double* ez = E + sl.nx + sl.ny;
-  const double* dz = ez + nsum;
-  const double* lz = ez + 2 * nsum;
   const float dt_rc = (float)(sl.dt / (sl.rho * sl.cp));
   double zt[VEC], yt[VEC], n1 = 0.0, dummy = 0.0;
   float sg32[VEC], exy32[VEC], dxy32[VEC], lxy32[VEC];
@@ -1282,7 +1291,8 @@ kb_volume_ring(BView v, float* a, const double* sigma, double* Zt, double* Yt, d
     if (!arrived) bad = 1;
     if (arrived && live) {
       const double cp = ct[p];
-      const float cp32 = (float)cp, ez32 = (float)ez[p], dz32 = (float)dz[p], lz32 = (float)lz[p];
+      const float cp32 = tabbed ? ztab[0][p] : (float)cp, ez32 = tabbed ? ztab[1][p] : (float)ez[p];
+      const float dz32 = tabbed ? ztab[2][p] : (float)dz[p], lz32 = tabbed ? ztab[3][p] : (float)lz[p];
       float4 x4 = *reinterpret_cast<const float4*>(&ring[k][VEC * threadIdx.x]);
       float av[VEC] = {x4.x, x4.y, x4.z, x4.w};
 #pragma unroll
