@@ -515,27 +515,28 @@ __global__ void __launch_bounds__(AX_THREADS) kb_face_axis(BView v, const double
 // Each CTA computes one 128-row x NB-column tile of one slot (MMA M = 128,
 // N = NB). One thread streams the tile's operand chunks -- BF16 hi + lo, one
 // bulk copy per operand and 32-slice chunk -- through a ring of f2::STAGES
-// stages and issues three split-BF16 MMAs per 16-slice step (hi.hi into one
-// FP32 accumulator in tensor memory, hi.lo and lo.hi into a second; the two
-// are summed when read out); the ring is primed before the tensor memory is
-// allocated.
+// stages and issues three split-BF16 MMAs per 16-slice step (hi.hi, hi.lo,
+// lo.hi) into one FP32 accumulator in tensor memory; the ring is primed
+// before the tensor memory is allocated.
 // kb_fx writes X1, split into BF16 hi + lo, to the slot's x1 plane, chunked
 // and laid out exactly as the B operand chunks of kb_fy, which streams it
 // like any other operand. Separability makes the tiles independent. A tile
-// is a latency chain of nx/32 or ny/32 chunks, so concurrency decides the
-// rate: shared memory (2 stages of 24 KB) and tensor memory (128 columns)
-// allow four CTAs per SM, whose copies, MMAs and epilogues overlap (measured
-// against 2 CTAs x 4 stages and 3 x 3: 4 x 2 is the fastest).
+// is a latency chain of nx/32 or ny/32 chunks, so the bytes the SM holds in
+// flight decide the rate. Tiles of 128 columns take 32 KB per chunk where two
+// 64-column tiles took 48 KB. Shared memory (2 stages of 32 KB) and tensor
+// memory (one 128-column accumulator) allow three CTAs per SM, whose copies,
+// MMAs and epilogues overlap. Measured against 64-column tiles at 2 x 4,
+// 3 x 3 and 4 x 2 CTAs x stages, this is the fastest.
 namespace f2 {
 constexpr int THREADS = 256;
-constexpr int NB = 64;                       // column block (MMA N)
+constexpr int NB = 128;                      // column block (MMA N)
 constexpr int CA = umma::CHUNK_BYTES;        // 128 x 32 BF16 chunk of an A operand (8 KB)
-constexpr int CBN = NB * umma::KC * 2;       // NB x 32 BF16 chunk of a B operand (4 KB)
-constexpr int STAGE = 2 * CA + 2 * CBN;      // 24 KB: A hi/lo + B hi/lo
+constexpr int CBN = NB * umma::KC * 2;       // NB x 32 BF16 chunk of a B operand (8 KB)
+constexpr int STAGE = 2 * CA + 2 * CBN;      // 32 KB: A hi/lo + B hi/lo
 constexpr int STAGES = 2;
 constexpr int TAIL = 128;                    // barriers, TMEM address, status flag
-constexpr int SMEM = STAGES * STAGE + TAIL;  // 49,280 bytes: four CTAs per SM
-constexpr uint32_t TCOLS = 128;              // two NB-column accumulators
+constexpr int SMEM = STAGES * STAGE + TAIL;  // 65,664 bytes: three CTAs per SM
+constexpr uint32_t TCOLS = 128;              // one NB-column accumulator
 }  // namespace f2
 
 // Tensor-core face tiles of a slot: 128-row tiles x NB-column blocks.
@@ -610,9 +611,8 @@ __device__ __forceinline__ int f2_prime(const F2Smem& m, int n, const Load& load
 
 // Thread 0: chunks 0..n-1 of the tile (chunk g in stage g % STAGES; each
 // barrier completes one phase per use of its stage, so chunk g waits for
-// parity (g / STAGES) & 1), MMAs into the accumulators at tmem (hi.hi) and
-// tmem + NB (hi.lo, lo.hi), each stage refilled once its MMAs have drained,
-// then the wait for the last MMAs. A wait that expires
+// parity (g / STAGES) & 1), MMAs into the accumulator at tmem, each stage
+// refilled once its MMAs have drained, then the wait for the last MMAs. A wait that expires
 // (after `lim` polls) records the error, clears the status flag and drains,
 // with the full bound, every copy and MMA in flight; returns false then.
 // stall: first wait on a barrier that nothing completes (the wait test).
@@ -641,8 +641,8 @@ __device__ bool f2_run(const F2Smem& m, int n, int issued, const Load& load, uin
       const uint64_t dbl = smem_desc(bl + ob, (NB / 8) * 128, 128);
       const uint32_t acc = (g > 0 || k > 0) ? 1u : 0u;
       mma_bf16(tmem, dah, dbh, idesc, acc);
-      mma_bf16(tmem + NB, dah, dbl, idesc, acc);
-      mma_bf16(tmem + NB, dal, dbh, idesc, 1u);
+      mma_bf16(tmem, dah, dbl, idesc, 1u);
+      mma_bf16(tmem, dal, dbh, idesc, 1u);
     }
     mma_commit(&m.done[g % S]);
     committed = g + 1;
@@ -671,17 +671,11 @@ __device__ bool f2_run(const F2Smem& m, int n, int issued, const Load& load, uin
   return ok;
 }
 
-// 32 x 16 accumulator values of this warp's lane quarter: the parts summed.
-__device__ __forceinline__ void f2_read16(uint32_t ta, float (&x)[16]) {
-  float p1[16];
-  umma::tmem_ld16(ta, x);
-  umma::tmem_ld16(ta + f2::NB, p1);
-#pragma unroll
-  for (int i = 0; i < 16; ++i) x[i] = x[i] + p1[i];
-}
+// 32 x 16 accumulator values of this warp's lane quarter.
+__device__ __forceinline__ void f2_read16(uint32_t ta, float (&x)[16]) { umma::tmem_ld16(ta, x); }
 
 template <bool INV, bool SKIP_DONE>
-__global__ void __launch_bounds__(f2::THREADS, 4) kb_fx(BView v) {
+__global__ void __launch_bounds__(f2::THREADS, 3) kb_fx(BView v) {
   using namespace umma;
   constexpr int CA = f2::CA, CBN = f2::CBN, NB = f2::NB;
   extern __shared__ __align__(128) char sm[];
@@ -695,7 +689,7 @@ __global__ void __launch_bounds__(f2::THREADS, 4) kb_fx(BView v) {
   const int nkx = (nx + KC - 1) / KC, nky = (ny + KC - 1) / KC;
   const F2Smem m(sm);
   const char* pp = (INV ? v.xa : v.xq) + sl.xa + (size_t)rt * nkx * 2 * CA;       // 128-row pair chunks
-  const char* mx = v.mp + (INV ? sl.mpx_inv : sl.mpx) + (size_t)cb * nkx * 2 * CBN;  // NB-row pair chunks
+  const char* mx = v.mp + (INV ? sl.mpx_inv : sl.mpx) + (size_t)cb * nkx * 2 * CBN;  // 128-row pair chunks
   auto load = [&](int g) {  // P chunk (rt, g) and Mx chunk (cb, g)
     char* stg = m.ring + (g % f2::STAGES) * f2::STAGE;
     uint64_t* bar = &m.full[g % f2::STAGES];
@@ -724,10 +718,10 @@ __global__ void __launch_bounds__(f2::THREADS, 4) kb_fx(BView v) {
     const int q = warp & 3, half = warp >> 2;  // TMEM lane quarter, column half
     const int y = rt * TM + q * 32 + lane;
     const bool keep = y < nky * KC;
-    const int c = half * 32;
+    const int c = half * (NB / 2);
     char* x1 = v.x1 + sl.x1 + (size_t)cb * nky * 2 * CBN + (size_t)(y >> 5) * 2 * CBN;
-#pragma unroll
-    for (int cc = 0; cc < 32; cc += 16) {
+#pragma unroll 1
+    for (int cc = 0; cc < NB / 2; cc += 16) {
       float x16[16];
       f2_read16(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(c + cc), x16);
 #pragma unroll
@@ -751,7 +745,7 @@ __global__ void __launch_bounds__(f2::THREADS, 4) kb_fx(BView v) {
 }
 
 template <bool INV, bool SKIP_DONE, int KIND>
-__global__ void __launch_bounds__(f2::THREADS, 4) kb_fy(BView v, F2Args args, double* part_tile) {
+__global__ void __launch_bounds__(f2::THREADS, 3) kb_fy(BView v, F2Args args, double* part_tile) {
   using namespace umma;
   constexpr int CA = f2::CA, CBN = f2::CBN, NB = f2::NB;
   extern __shared__ __align__(128) char sm[];
@@ -803,9 +797,9 @@ __global__ void __launch_bounds__(f2::THREADS, 4) kb_fy(BView v, F2Args args, do
     tc_fence_after();
     const int q = warp & 3, half = warp >> 2;
     const int mrow = q * 32 + lane;
-    const int c = half * 32;
-#pragma unroll
-    for (int cc = 0; cc < 32; cc += 16) {
+    const int c = half * (NB / 2);
+#pragma unroll 1
+    for (int cc = 0; cc < NB / 2; cc += 16) {
       float x16[16];
       f2_read16(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(c + cc), x16);
 #pragma unroll
@@ -1678,11 +1672,11 @@ int sgh_batch_create(const sgh_config* cfgs, int32_t n, int32_t precision, sgh_b
   if (precision == SGH_PRECISION_MIXED) {
     long long po = 0;
     for (auto& kv : mats) {
-      // per N: forward, inverse in 128-row chunks; forward, inverse in NB-row chunks
+      // per N: forward, inverse in 128-row chunks (the A operand of the
+      // y-pass and the B operand of the x-pass alike)
       mplane[kv.first] = po;
       B->mplane_list.push_back({kv.first, po});
-      po += 2LL * (long long)(umma::pair_bytes<128>(kv.first, kv.first) +
-                              umma::pair_bytes<f2::NB>(kv.first, kv.first));
+      po += 2LL * (long long)umma::pair_bytes<128>(kv.first, kv.first);
     }
     B->mp_bytes = (size_t)po;
   }
@@ -1716,8 +1710,8 @@ int sgh_batch_create(const sgh_config* cfgs, int32_t n, int32_t precision, sgh_b
       B->xa_bytes += umma::pair_bytes<128>(c.ny, c.nx);
       sl.x1 = (long long)B->x1_bytes;
       B->x1_bytes += x1_bytes(c.nx, c.ny);
-      sl.mpx = mplane[c.nx] + 2LL * (long long)umma::pair_bytes<128>(c.nx, c.nx);
-      sl.mpx_inv = sl.mpx + (long long)umma::pair_bytes<f2::NB>(c.nx, c.nx);
+      sl.mpx = mplane[c.nx];
+      sl.mpx_inv = sl.mpx + (long long)umma::pair_bytes<128>(c.nx, c.nx);
       sl.mpy = mplane[c.ny];
       sl.mpy_inv = sl.mpy + (long long)umma::pair_bytes<128>(c.ny, c.ny);
     }
@@ -1877,12 +1871,11 @@ int sgh_batch_bind(sgh_batch* B, void* workspace, uint64_t bytes, void* stream) 
       long long moff = -1;
       for (auto& m : B->mat_list)
         if (m.first == N) moff = m.second;
-      const size_t pb = umma::pair_bytes<128>(N, N), pn = umma::pair_bytes<f2::NB>(N, N);
+      const size_t pb = umma::pair_bytes<128>(N, N);
       auto pl = [&](size_t o) { return B->ws + B->o_mp + po + o; };
       const int g = cdivl((long long)N * N, BT);
       for (int inv = 0; inv < 2; ++inv) {
         kb_matrix_planes<128><<<g, BT, 0, s>>>(N, B->d(B->o_mats) + moff, inv, pl(inv * pb));
-        kb_matrix_planes<f2::NB><<<g, BT, 0, s>>>(N, B->d(B->o_mats) + moff, inv, pl(2 * pb + inv * pn));
       }
     }
     kb_tables<float><<<B->tot_vblk, BT, 0, s>>>(v, nullptr, nullptr, B->d(B->o_ct), B->d(B->o_E));
