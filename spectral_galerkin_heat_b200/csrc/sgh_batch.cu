@@ -3,8 +3,8 @@
 // Every stage of the time step runs as ONE launch over all slots of a batch.
 // Work is decomposed per slot: element/column kernels give each slot
 // ceil(S_i / 256) blocks, face transforms give each slot its tiles (FP64) or
-// 64-column blocks (mixed); a block reads its slot from a block -> slot
-// table. Per-slot reductions (P_laser, Picard norms, surface max) are
+// 128-row x 128-column tiles (mixed); a block reads its slot from a block ->
+// slot table. Per-slot reductions (P_laser, Picard norms, surface max) are
 // per-block partials summed slot by slot in a fixed order.
 //
 // The physics is the face-space Picard form (see sgh_b200.cu): every iterate
@@ -16,10 +16,11 @@
 // still iterating; converged (or inactive) slots skip every kernel of the
 // body, so a slot's result does not depend on what else is in the batch.
 //
-// Volume state (modes a, K, KK) is FP64 (plain) or FP32 (mixed: K/KK computed
-// in FP64 and rounded once; all arithmetic on them in FP64 registers). Faces,
-// face sums and norms are FP64 in both; in mixed precision the face
-// transforms run on the tensor cores from split-BF16 operand planes.
+// Volume state is FP64 modes with stored K and KK (plain), or FP32 modes only
+// (mixed: K and KK formed in registers from per-axis FP64 tables, the mode
+// update in FP32). Faces, face sums and norms are FP64 in both; in mixed
+// precision the face transforms run on the tensor cores from split-BF16
+// operand planes.
 #include <cuda_runtime.h>
 
 #include <algorithm>
