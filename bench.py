@@ -62,11 +62,11 @@ import numpy as np  # noqa: E402
 METRIC = "timesteps/s"
 L2_FLUSH_BYTES = 256 << 20
 # dram__bytes_read.sum + dram__bytes_write.sum of the dominant kernel from ncu
-# captures (ncu --set full, one launch): the serving volume pass on the 24-slot
-# case (2 slots per class) moved 277.1 MB for 38,993,920 modes
-# (dram__bytes.sum.per_second x gpu__time_duration.sum); the benchmark's case
-# has the same class mix, so traffic scales with the modes.
-NCU_VOLUME_TRAFFIC_PER_MODE = 277.1e6 / 38993920
+# captures (one launch): the serving volume pass at the benchmark's size (288
+# slots, 467,927,040 active modes) moved 4.034 GB (dram__bytes.sum.per_second
+# 5.963 TB/s x gpu__time_duration.sum 676.6 us, --cache-control none); traffic
+# scales with the modes of the same class mix.
+NCU_VOLUME_TRAFFIC_PER_MODE = 4.034e9 / 467927040
 # the raster workload's dominant kernel (k_axis) was captured on the same
 # 128x64x32 case: 2.14 MB for one contiguous-axis pass (field resident in L2)
 NCU_TRAFFIC_BYTES = 2.14e6
@@ -909,7 +909,7 @@ def run_serving(args, rank, world, local_rank):
                      "peak_source": peak_kind,
                      "traffic": (NCU_VOLUME_TRAFFIC_PER_MODE * modes
                                  if NCU_VOLUME_TRAFFIC_PER_MODE is not None else None),
-                     "traffic_note": "ncu capture of the 24-slot case scaled by active modes",
+                     "traffic_note": "ncu capture of the 288-slot case, scaled by active modes",
                      "algorithmic_bytes_per_launch": vp_bytes, "modes": modes},
     }
     if world == 1 and not args.no_cpu_baseline:

@@ -43,6 +43,8 @@ constexpr int BT = 256;   // threads of element / column / face kernels
 constexpr int CT = 1024;  // threads of the per-slot control kernels
 constexpr int RPT = 8;    // elements per thread of the relaxation
 constexpr int RB = RPT * BT;
+constexpr int VOL_FLUSH = 8;  // z-planes per FP32 partial sum of the mixed volume passes
+constexpr int RING_TABMAX = 256;  // largest nz of the ring-staged volume pass (its per-plane table)
 
 struct BSlot {
   int nx, ny, nz, S;
@@ -274,14 +276,13 @@ __global__ void __launch_bounds__(BT) kb_weights(BView v, const R* KK, double* W
 // (Re)start one slot at the initial condition (solvers/spectral.py:176-180).
 template <class R>
 __global__ void __launch_bounds__(BT)
-kb_slot_start(BView v, int s, R* a, double* q_evold, double* q_ev, double* sigma, const sgh_laser* table,
+kb_slot_start(BView v, int s, R* a, double* q_evold, double* sigma, const sgh_laser* table,
               int n_steps, sgh_step_out* outs) {
   const BSlot& sl = v.slot[s];
   const long long i = (long long)blockIdx.x * BT + threadIdx.x;
   if (i < sl.V) a[sl.vol + i] = (R)((i == 0) ? sl.T0 * sqrt(sl.Lx * sl.Ly * sl.Lz) : 0.0);
   if (i < sl.S) {
     q_evold[sl.face + i] = 0.0;
-    q_ev[sl.face + i] = 0.0;
     sigma[sl.face + i] = 0.0;
   }
   if (i == 0) {
@@ -360,7 +361,8 @@ __global__ void __launch_bounds__(CT) kb_begin(BView v, cudaGraphConditionalHand
 }
 
 // q_las, P_laser partials and q_net = q_las - shift(q_evap_old) per slot
-// (solvers/spectral.py:273-306).
+// (solvers/spectral.py:273-306); q_net goes to the FP64 array (FP64 batches,
+// q_net non-null) or to the xq operand plane (mixed precision).
 //
 // Each element's (y, x) is formed once and serves the flux, the shift and the
 // operand plane. In mixed precision the point-sampled beam multiplies by the
@@ -429,7 +431,7 @@ kb_face_begin(BView v, double* q_las, double* q_net, const double* q_evold, doub
         double val = wy0[u] * (wx0[u] * g[u][0] + wx1[u] * g[u][1]) + wy1[u] * (wx0[u] * g[u][2] + wx1[u] * g[u][3]);
         if (!in[u]) val = 0.0;
         qn = q - val;
-        q_net[sl.face + i] = qn;
+        if (q_net) q_net[sl.face + i] = qn;
       }
       plane_put_yx(v.xq, sl, ys[u], xs[u], qn, ok[u]);
     }
@@ -509,6 +511,80 @@ __global__ void __launch_bounds__(AX_THREADS) kb_face_axis(BView v, const double
   }
 }
 
+// End of a Picard iteration's relaxation block (kb_relax, or kb_fy with the
+// relaxation epilogue): publish the block's residual / iterate norm partials
+// at part[2 p], part[2 p + 1] (p: the block's partial index; slot s has the
+// np partials p0 .. p0 + np - 1) and take a ticket. The block drawing the slot's
+// last ticket sums that slot's partials in a fixed order (so a slot's result
+// does not depend on the rest of the batch) and runs its convergence test
+// (solvers/spectral.py:464-499); the finisher of the last iterating slot sets
+// the Picard loop condition and the number of slots that iterate next. No
+// block waits on another. Called by every thread of the block.
+template <int NT>
+__device__ void relax_finish(const BView& v, int s, int p, int p0, int np, double r2, double o2, double* part,
+                             const double* part_n1, cudaGraphConditionalHandle h_picard, int in_graph,
+                             double* sh) {
+  __shared__ unsigned ticket;
+  __shared__ int last, count;
+  const BSlot& sl = v.slot[s];
+  BState& st = v.st[s];
+  block_sum2<NT>(r2, o2, sh);
+  if (threadIdx.x == 0) {
+    part[2 * p] = r2;
+    part[2 * p + 1] = o2;
+    __threadfence();
+    ticket = atomicAdd(&st.tickets, 1u);
+  }
+  __syncthreads();
+  if (ticket != (unsigned)np - 1u) return;
+  // this block finishes the slot
+  __threadfence();
+  double rs = 0.0, os = 0.0;
+  for (int k = threadIdx.x; k < np; k += NT) {
+    rs += __ldcg(part + 2 * (p0 + k));
+    os += __ldcg(part + 2 * (p0 + k) + 1);
+  }
+  for (int k = threadIdx.x; k < sl.nblk; k += NT) os += __ldcg(part_n1 + sl.blk0 + k);
+  block_sum2<NT>(rs, os, sh);
+  if (threadIdx.x == 0) {
+    const double n = sl.n_elements;
+    const double rel = sqrt(rs / n) / fmax(sqrt(os / n), 1e-9);
+    const int it = st.iter + 1;
+    st.iter = it;
+    st.rel_err = rel;
+    if (rel < sl.tol) {
+      st.status = SGH_STEP_CONVERGED;
+      st.done = 1;
+    } else if (!isfinite(rel)) {
+      st.status = SGH_STEP_NONFINITE;
+      st.done = 1;
+    } else if (it >= sl.max_iter) {
+      st.status = SGH_STEP_CAPPED;
+      st.done = 1;
+    }
+    st.tickets = 0u;
+    const int expect = __ldcg(&v.g->n_iter_slots);  // read before the ticket: the last finisher rewrites it
+    __threadfence();
+    last = atomicAdd(&v.g->slots_done, 1u) == (unsigned)expect - 1u;
+    count = 0;
+  }
+  __syncthreads();
+  if (!last) return;
+  // the last finisher: slots iterating next, loop condition
+  __threadfence();
+  int c = 0;
+  for (int k = threadIdx.x; k < v.n; k += NT)
+    if (__ldcg(&v.st[k].active) && !__ldcg(&v.st[k].done)) ++c;
+  if (c) atomicAdd(&count, c);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    v.g->slots_done = 0u;
+    v.g->n_iter_slots = count;
+    v.g->picard_any = count > 0;
+    if (in_graph) cudaGraphSetConditional(h_picard, count > 0 ? 1u : 0u);
+  }
+}
+
 // ---- batched face transform on the tensor cores (mixed precision) ---------
 // A 2-D transform of every slot's top face is two launches:
 //   kb_fx   X1[y][c] = sum_x P[y][x] Mx[c][x]    (P: the slot's xa or xq plane)
@@ -533,16 +609,26 @@ constexpr int THREADS = 256;
 constexpr int NB = 128;                      // column block (MMA N)
 constexpr int CA = umma::CHUNK_BYTES;        // 128 x 32 BF16 chunk of an A operand (8 KB)
 constexpr int CBN = NB * umma::KC * 2;       // NB x 32 BF16 chunk of a B operand (8 KB)
-constexpr int STAGE = 2 * CA + 2 * CBN;      // 32 KB: A hi/lo + B hi/lo
+// Column blocks per CTA: one A chunk could serve CB B chunks (CB = 2: 48 KB
+// stages, two CTAs per SM), but at 288 serving slots that measured 3% slower
+// than one block per CTA at three CTAs per SM (161.7K against 167.3K
+// timesteps/s), so CB = 1.
+constexpr int CB = 1;
+constexpr int STAGE = 2 * CA + CB * 2 * CBN; // 32 KB: A hi/lo + CB x B hi/lo
 constexpr int STAGES = 2;
 constexpr int TAIL = 128;                    // barriers, TMEM address, status flag
 constexpr int SMEM = STAGES * STAGE + TAIL;  // 65,664 bytes: three CTAs per SM
-constexpr uint32_t TCOLS = 128;              // one NB-column accumulator
+constexpr int CTAS = 3;                      // CTAs per SM (shared memory; CTAS x TCOLS <= 512)
+constexpr uint32_t TCOLS = CB * NB;          // CB NB-column accumulators
+static_assert(umma::TM * NB * 4 <= STAGES * STAGE, "the epilogue's FP32 tile fits in the drained ring");
+static_assert(CTAS * TCOLS <= 512, "tensor memory of CTAS resident CTAs");
+static_assert(CTAS * (SMEM + 1024) <= 228 * 1024, "shared memory of CTAS resident CTAs");
 }  // namespace f2
 
-// Tensor-core face tiles of a slot: 128-row tiles x NB-column blocks.
+// Tensor-core face tiles of a slot: 128-row tiles x groups of CB NB-column blocks.
 inline __host__ __device__ int face_utiles(int nx, int ny) {
-  return ((nx + f2::NB - 1) / f2::NB) * ((ny + umma::TM - 1) / umma::TM);
+  const int ncb = (nx + f2::NB - 1) / f2::NB;
+  return ((ncb + f2::CB - 1) / f2::CB) * ((ny + umma::TM - 1) / umma::TM);
 }
 // Bytes of a slot's x1 plane: NB-column blocks x 32-row chunks of {hi, lo}.
 inline __host__ __device__ long long x1_bytes(int nx, int ny) {
@@ -551,11 +637,15 @@ inline __host__ __device__ long long x1_bytes(int nx, int ny) {
 
 // Epilogue of the transform, on output element (r, c) of the slot's face:
 //   F2_STORE    FP64 face array (x dct_scale if scaled)
-//   F2_TOPFLUX  T_s -> evaporation -> q_evap (FP64), q_net -> xq plane
-//   F2_COMMIT   T_temp, its block max, q_evap_old <- q_evap
+//   F2_TOPFLUX  T_s -> evaporation -> q_evap (FP64, into the q_evap_old array), q_net -> xq plane
+//   F2_COMMIT   T_temp and its block max
 //   F2_SIGMA    sigma = dct_scale * G (FP64) and the first iterate's
 //               A = Zt + W_tt sigma into the xa plane (replaces kb_assemble)
-enum { F2_STORE = 0, F2_TOPFLUX = 1, F2_COMMIT = 2, F2_SIGMA = 3 };
+//   F2_RELAX    S_top = dct_scale * G straight into the Picard relaxation
+//               (kb_relax's arithmetic: residual and iterate norms, sigma,
+//               A = Zt + W_tt sigma into the xa plane), then the per-slot
+//               convergence test (relax_finish); S_top is never stored
+enum { F2_STORE = 0, F2_TOPFLUX = 1, F2_COMMIT = 2, F2_SIGMA = 3, F2_RELAX = 4 };
 
 struct FaceParams {  // per-slot constants held in registers by the epilogues
   long long face, xa;
@@ -564,11 +654,19 @@ struct FaceParams {  // per-slot constants held in registers by the epilogues
 };
 
 struct F2Args {
-  double* out;        // F2_STORE target, F2_TOPFLUX q_evap, F2_COMMIT T_surf, F2_SIGMA sigma
-  double* out2;       // F2_COMMIT q_evap_old
-  const double* in2;  // F2_TOPFLUX q_las, F2_COMMIT q_evap, F2_SIGMA Zt
+  double* out;        // F2_STORE target, F2_TOPFLUX q_evap (into the q_evap_old array), F2_COMMIT T_surf,
+                      // F2_SIGMA and F2_RELAX sigma
+  double* out2;       // unused
+  const double* in2;  // F2_TOPFLUX q_las, F2_SIGMA and F2_RELAX Zt
   int scaled;
-  const double* in3;  // F2_SIGMA W_tt
+  const double* in3;  // F2_SIGMA and F2_RELAX W_tt
+  // F2_RELAX only
+  const double* Yt;
+  const double* Qtt;
+  const double* part_n1;  // volume-pass norm partials
+  double* part;           // relaxation partials, 2 per tile
+  cudaGraphConditionalHandle h_picard;
+  int in_graph;
 };
 
 // FP32 tile of 128 x NB results in shared memory: element (m, n) at
@@ -618,7 +716,7 @@ __device__ __forceinline__ int f2_prime(const F2Smem& m, int n, const Load& load
 // with the full bound, every copy and MMA in flight; returns false then.
 // stall: first wait on a barrier that nothing completes (the wait test).
 template <class Load>
-__device__ bool f2_run(const F2Smem& m, int n, int issued, const Load& load, uint32_t tmem, unsigned lim,
+__device__ bool f2_run(const F2Smem& m, int n, int nb, int issued, const Load& load, uint32_t tmem, unsigned lim,
                        bool stall, int* err) {
   using namespace umma;
   constexpr int S = f2::STAGES, NB = f2::NB;
@@ -632,18 +730,24 @@ __device__ bool f2_run(const F2Smem& m, int n, int issued, const Load& load, uin
     }
     tc_fence_after();
     const uint32_t ah = smem_u32(m.ring + (g % S) * f2::STAGE), al = ah + f2::CA;
-    const uint32_t bh = ah + 2 * f2::CA, bl = bh + f2::CBN;
 #pragma unroll
     for (int k = 0; k < KC / 16; ++k) {
       const uint32_t oa = (uint32_t)(2 * k * (TM / 8) * 128), ob = (uint32_t)(2 * k * (NB / 8) * 128);
       const uint64_t dah = smem_desc(ah + oa, (TM / 8) * 128, 128);
       const uint64_t dal = smem_desc(al + oa, (TM / 8) * 128, 128);
-      const uint64_t dbh = smem_desc(bh + ob, (NB / 8) * 128, 128);
-      const uint64_t dbl = smem_desc(bl + ob, (NB / 8) * 128, 128);
       const uint32_t acc = (g > 0 || k > 0) ? 1u : 0u;
-      mma_bf16(tmem, dah, dbh, idesc, acc);
-      mma_bf16(tmem, dah, dbl, idesc, 1u);
-      mma_bf16(tmem, dal, dbh, idesc, 1u);
+#pragma unroll
+      for (int j = 0; j < f2::CB; ++j) {
+        if (j < nb) {  // block j: B chunk at 2 CA + j 2 CBN, accumulator columns j NB..
+          const uint32_t bh = ah + 2 * f2::CA + (uint32_t)(j * 2 * f2::CBN), bl = bh + f2::CBN;
+          const uint64_t dbh = smem_desc(bh + ob, (NB / 8) * 128, 128);
+          const uint64_t dbl = smem_desc(bl + ob, (NB / 8) * 128, 128);
+          const uint32_t tj = tmem + (uint32_t)(j * NB);
+          mma_bf16(tj, dah, dbh, idesc, acc);
+          mma_bf16(tj, dah, dbl, idesc, 1u);
+          mma_bf16(tj, dal, dbh, idesc, 1u);
+        }
+      }
     }
     mma_commit(&m.done[g % S]);
     committed = g + 1;
@@ -676,7 +780,7 @@ __device__ bool f2_run(const F2Smem& m, int n, int issued, const Load& load, uin
 __device__ __forceinline__ void f2_read16(uint32_t ta, float (&x)[16]) { umma::tmem_ld16(ta, x); }
 
 template <bool INV, bool SKIP_DONE>
-__global__ void __launch_bounds__(f2::THREADS, 3) kb_fx(BView v) {
+__global__ void __launch_bounds__(f2::THREADS, f2::CTAS) kb_fx(BView v) {
   using namespace umma;
   constexpr int CA = f2::CA, CBN = f2::CBN, NB = f2::NB;
   extern __shared__ __align__(128) char sm[];
@@ -686,17 +790,20 @@ __global__ void __launch_bounds__(f2::THREADS, 3) kb_fx(BView v) {
   const BState& st = v.st[s];
   if (!st.active || (SKIP_DONE && st.done)) return;
   const int nx = sl.nx, ny = sl.ny;
-  const int ncb = (nx + NB - 1) / NB, t = b - sl.utile0, rt = t / ncb, cb = t - rt * ncb;
+  // tile t: row tile rt, column blocks cb0 .. cb0 + nb - 1
+  const int ncb = (nx + NB - 1) / NB, ngb = (ncb + f2::CB - 1) / f2::CB;
+  const int t = b - sl.utile0, rt = t / ngb, cb0 = (t - rt * ngb) * f2::CB, nb = min(f2::CB, ncb - cb0);
   const int nkx = (nx + KC - 1) / KC, nky = (ny + KC - 1) / KC;
   const F2Smem m(sm);
-  const char* pp = (INV ? v.xa : v.xq) + sl.xa + (size_t)rt * nkx * 2 * CA;       // 128-row pair chunks
-  const char* mx = v.mp + (INV ? sl.mpx_inv : sl.mpx) + (size_t)cb * nkx * 2 * CBN;  // 128-row pair chunks
-  auto load = [&](int g) {  // P chunk (rt, g) and Mx chunk (cb, g)
+  const char* pp = (INV ? v.xa : v.xq) + sl.xa + (size_t)rt * nkx * 2 * CA;        // 128-row pair chunks
+  const char* mx = v.mp + (INV ? sl.mpx_inv : sl.mpx) + (size_t)cb0 * nkx * 2 * CBN;  // 128-row pair chunks
+  auto load = [&](int g) {  // P chunk (rt, g) and the Mx chunks (cb0 + j, g)
     char* stg = m.ring + (g % f2::STAGES) * f2::STAGE;
     uint64_t* bar = &m.full[g % f2::STAGES];
-    mbar_expect_tx(bar, f2::STAGE);
+    mbar_expect_tx(bar, (uint32_t)(2 * CA + nb * 2 * CBN));
     bulk_g2s(stg, pp + (size_t)g * 2 * CA, 2 * CA, bar);
-    bulk_g2s(stg + 2 * CA, mx + (size_t)g * 2 * CBN, 2 * CBN, bar);
+    for (int j = 0; j < nb; ++j)
+      bulk_g2s(stg + 2 * CA + j * 2 * CBN, mx + ((size_t)j * nkx + g) * 2 * CBN, 2 * CBN, bar);
   };
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   int issued = 0;
@@ -709,7 +816,7 @@ __global__ void __launch_bounds__(f2::THREADS, 3) kb_fx(BView v) {
   const uint32_t tmem = *m.tslot;
   if (tid == 0) {
     const unsigned lim = v.g->wait_limit ? v.g->wait_limit : WAIT_LIMIT;
-    f2_run(m, nkx, issued, load, tmem, lim, false, &v.g->umma_err);
+    f2_run(m, nkx, nb, issued, load, tmem, lim, false, &v.g->umma_err);
   }
   __syncthreads();
   if (*m.okflag) {
@@ -720,11 +827,12 @@ __global__ void __launch_bounds__(f2::THREADS, 3) kb_fx(BView v) {
     const int y = rt * TM + q * 32 + lane;
     const bool keep = y < nky * KC;
     const int c = half * (NB / 2);
-    char* x1 = v.x1 + sl.x1 + (size_t)cb * nky * 2 * CBN + (size_t)(y >> 5) * 2 * CBN;
 #pragma unroll 1
-    for (int cc = 0; cc < NB / 2; cc += 16) {
+    for (int jc = 0; jc < nb * (NB / 2); jc += 16) {
+      const int j = jc / (NB / 2), cc = jc - j * (NB / 2);  // column block j, its columns c + cc ..
+      char* x1 = v.x1 + sl.x1 + (size_t)(cb0 + j) * nky * 2 * CBN + (size_t)(y >> 5) * 2 * CBN;
       float x16[16];
-      f2_read16(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(c + cc), x16);
+      f2_read16(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(j * NB + c + cc), x16);
 #pragma unroll
       for (int i = 0; i < 16; ++i) {
         __nv_bfloat16 h, l;
@@ -746,11 +854,11 @@ __global__ void __launch_bounds__(f2::THREADS, 3) kb_fx(BView v) {
 }
 
 template <bool INV, bool SKIP_DONE, int KIND>
-__global__ void __launch_bounds__(f2::THREADS, 3) kb_fy(BView v, F2Args args, double* part_tile) {
+__global__ void __launch_bounds__(f2::THREADS, f2::CTAS) kb_fy(BView v, F2Args args, double* part_tile) {
   using namespace umma;
   constexpr int CA = f2::CA, CBN = f2::CBN, NB = f2::NB;
   extern __shared__ __align__(128) char sm[];
-  __shared__ double red[f2::THREADS / 32];
+  __shared__ double red[2 * (f2::THREADS / 32)];
   const int b = blockIdx.x;
   const int s = v.utile_slot[b];
   const BSlot& sl = v.slot[s];
@@ -761,17 +869,20 @@ __global__ void __launch_bounds__(f2::THREADS, 3) kb_fy(BView v, F2Args args, do
   fp.recon_scale = sl.recon_scale; fp.dct_scale = sl.dct_scale; fp.T_liquidus = sl.T_liquidus;
   fp.T_boil = sl.T_boil; fp.evap_f1 = sl.evap_f1; fp.evap_f2 = sl.evap_f2;
   const int nx = fp.nx, ny = fp.ny;
-  const int ncb = (nx + NB - 1) / NB, t = b - sl.utile0, rt = t / ncb, cb = t - rt * ncb;
+  // tile t: row tile rt, column blocks cb0 .. cb0 + nb - 1
+  const int ncb = (nx + NB - 1) / NB, ngb = (ncb + f2::CB - 1) / f2::CB;
+  const int t = b - sl.utile0, rt = t / ngb, cb0 = (t - rt * ngb) * f2::CB, nb = min(f2::CB, ncb - cb0);
   const int nkx = (nx + KC - 1) / KC, nky = (ny + KC - 1) / KC;
   const F2Smem m(sm);
   const char* my = v.mp + (INV ? sl.mpy_inv : sl.mpy) + (size_t)rt * nky * 2 * CA;  // 128-row pair chunks
-  const char* x1 = v.x1 + sl.x1 + (size_t)cb * nky * 2 * CBN;                       // NB-row pair chunks
-  auto load = [&](int g) {  // My chunk (rt, g) and x1 chunk (cb, g)
+  const char* x1 = v.x1 + sl.x1 + (size_t)cb0 * nky * 2 * CBN;                      // NB-row pair chunks
+  auto load = [&](int g) {  // My chunk (rt, g) and the x1 chunks (cb0 + j, g)
     char* stg = m.ring + (g % f2::STAGES) * f2::STAGE;
     uint64_t* bar = &m.full[g % f2::STAGES];
-    mbar_expect_tx(bar, f2::STAGE);
+    mbar_expect_tx(bar, (uint32_t)(2 * CA + nb * 2 * CBN));
     bulk_g2s(stg, my + (size_t)g * 2 * CA, 2 * CA, bar);
-    bulk_g2s(stg + 2 * CA, x1 + (size_t)g * 2 * CBN, 2 * CBN, bar);
+    for (int j = 0; j < nb; ++j)
+      bulk_g2s(stg + 2 * CA + j * 2 * CBN, x1 + ((size_t)j * nky + g) * 2 * CBN, 2 * CBN, bar);
   };
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   int issued = 0;
@@ -785,15 +896,18 @@ __global__ void __launch_bounds__(f2::THREADS, 3) kb_fy(BView v, F2Args args, do
   if (tid == 0) {
     // the wait test: a wait that can only run out, with copies in flight
     const unsigned lim = v.g->wait_limit ? v.g->wait_limit : WAIT_LIMIT;
-    f2_run(m, nky, issued, load, tmem, lim, v.g->stall_test != 0, &v.g->umma_err);
+    f2_run(m, nky, nb, issued, load, tmem, lim, v.g->stall_test != 0, &v.g->umma_err);
   }
   __syncthreads();
 
   constexpr int ITEMS = TM * NB / f2::THREADS;  // tile elements per thread
-  double mx = -INFINITY;
-  const int c0 = cb * NB, r0 = rt * TM;
-  float* tile = reinterpret_cast<float*>(m.ring);
+  double mx = -INFINITY, r2 = 0.0, o2 = 0.0;
+  const int r0 = rt * TM;
+  float* tile = reinterpret_cast<float*>(m.ring);  // 128 x NB FP32 (64 KB) over the drained ring
   const bool good = *m.okflag != 0;
+#pragma unroll 1
+  for (int j = 0; j < nb; ++j) {  // column block cb0 + j: accumulator columns j NB ..
+  const int c0 = (cb0 + j) * NB;
   if (good) {
     tc_fence_after();
     const int q = warp & 3, half = warp >> 2;
@@ -802,7 +916,7 @@ __global__ void __launch_bounds__(f2::THREADS, 3) kb_fy(BView v, F2Args args, do
 #pragma unroll 1
     for (int cc = 0; cc < NB / 2; cc += 16) {
       float x16[16];
-      f2_read16(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(c + cc), x16);
+      f2_read16(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(j * NB + c + cc), x16);
 #pragma unroll
       for (int i = 0; i < 16; ++i) tile[mrow * NB + ((c + cc + i) ^ (mrow & 31))] = x16[i];
     }
@@ -834,6 +948,41 @@ __global__ void __launch_bounds__(f2::THREADS, 3) kb_fy(BView v, F2Args args, do
             qn = ql[u] - qe;
           }
           plane_put8_warp(v.xq + fp.xa, y, x, nkx, qn, in);
+        }
+      }
+    } else if (KIND == F2_RELAX) {
+      const double omega = sl.omega;
+      constexpr int U = 4;
+      for (int it0 = 0; it0 < ITEMS; it0 += U) {
+        double sg[U], q[U], yt[U], zt[U], wt[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          const int e = tid + (it0 + u) * f2::THREADS;
+          const int y = r0 + e / NB, x = c0 + e % NB;
+          const bool in = y < ny && x < nx;
+          const long long j = fp.face + (long long)y * nx + x;
+          sg[u] = in ? args.out[j] : 0.0;
+          q[u] = in ? __ldg(args.Qtt + j) : 0.0;
+          yt[u] = in ? __ldg(args.Yt + j) : 0.0;
+          zt[u] = in ? __ldg(args.in2 + j) : 0.0;
+          wt[u] = in ? __ldg(args.in3 + j) : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          const int e = tid + (it0 + u) * f2::THREADS;
+          const int mm = e / NB, n = e % NB;
+          const int y = r0 + mm, x = c0 + n;
+          const bool in = y < ny && x < nx;
+          double a = 0.0;
+          if (in) {  // kb_relax's update, with S_top from the tile
+            const double d = fp.dct_scale * (double)f2_tile(tile, mm, n) - sg[u];
+            r2 += d * d * q[u];
+            o2 += 2.0 * sg[u] * yt[u] + sg[u] * sg[u] * q[u];
+            const double ns = d * omega + sg[u];
+            a = zt[u] + wt[u] * ns;
+            args.out[fp.face + (long long)y * nx + x] = ns;
+          }
+          plane_put8_warp(v.xa + fp.xa, y, x, nkx, a, in);
         }
       }
     } else if (KIND == F2_SIGMA) {
@@ -868,13 +1017,11 @@ __global__ void __launch_bounds__(f2::THREADS, 3) kb_fy(BView v, F2Args args, do
       constexpr int U = 4;
       for (int it0 = 0; it0 < ITEMS; it0 += U) {
         long long idx[U];
-        double src[U];
 #pragma unroll
         for (int u = 0; u < U; ++u) {
           const int e = tid + (it0 + u) * f2::THREADS;
           const int y = r0 + e / NB, x = c0 + e % NB;
           idx[u] = (y < ny && x < nx) ? fp.face + (long long)y * nx + x : -1;
-          src[u] = (KIND == F2_COMMIT && idx[u] >= 0) ? __ldg(args.in2 + idx[u]) : 0.0;
         }
 #pragma unroll
         for (int u = 0; u < U; ++u) {
@@ -886,16 +1033,22 @@ __global__ void __launch_bounds__(f2::THREADS, 3) kb_fy(BView v, F2Args args, do
           } else {  // F2_COMMIT
             const double T = fp.recon_scale * val;
             args.out[idx[u]] = T;
-            args.out2[idx[u]] = src[u];
             mx = fmax(mx, T);
           }
         }
       }
     }
   }
+  __syncthreads();  // every thread is done with the tile before the next block fills it
+  }
   tc_fence_before();
   __syncthreads();
   if (warp == 0) tmem_dealloc(tmem, f2::TCOLS);
+  if (KIND == F2_RELAX) {
+    if (!good) r2 = nan("");  // a transform whose wait ran out ends the slot's step as non-finite
+    relax_finish<f2::THREADS>(v, s, b, sl.utile0, sl.nutile, r2, o2, args.part, args.part_n1, args.h_picard,
+                              args.in_graph, red);
+  }
   if (KIND == F2_COMMIT) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_down_sync(0xffffffffu, mx, o));
@@ -918,6 +1071,10 @@ struct EB_Store {  // out = v * (scaled ? dct_scale : 1)
   }
 };
 
+// The evaporation flux of the latest Picard iterate is written straight into
+// the q_evap_old array: its one reader, the next step's warm-start shift in
+// kb_face_begin, runs before this step's Picard loop, so the commit's copy
+// q_evap_old <- q_evap (solvers/spectral.py:502-512) has nothing left to do.
 struct EB_TopFlux {  // T_s -> evaporation -> q_net (solvers/spectral.py:388-404)
   static constexpr int kMax = 0;
   const double* q_las;
@@ -931,15 +1088,12 @@ struct EB_TopFlux {  // T_s -> evaporation -> q_net (solvers/spectral.py:388-404
   }
 };
 
-struct EB_CommitSurface {  // T_temp, its max, q_evap_old <- q_evap (solvers/spectral.py:502-512)
+struct EB_CommitSurface {  // T_temp and its max (solvers/spectral.py:502-512)
   static constexpr int kMax = 1;
   double* T_surf;
-  const double* q_ev;
-  double* q_evold;
   __device__ __forceinline__ void operator()(const BSlot& sl, const BState&, long long i, double v, Red& r) const {
     const double T = sl.recon_scale * v;
     T_surf[i] = T;
-    q_evold[i] = q_ev[i];
     r.mx = fmax(r.mx, T);
   }
 };
@@ -960,12 +1114,10 @@ kb_relax(BView v, const double* Zt, const double* Yt, const double* Wtt, const d
          const double* S_top, double* sigma, double* A, double* part, const double* part_n1,
          cudaGraphConditionalHandle h_picard, int in_graph) {
   __shared__ double sh[2 * (BT / 32)];
-  __shared__ unsigned ticket;
-  __shared__ int last, count;
   const int b = blockIdx.x;
   const int s = v.rblk_slot[b];
   const BSlot& sl = v.slot[s];
-  BState& st = v.st[s];
+  const BState& st = v.st[s];
   if (!st.active || st.done) return;
   const int i0 = (b - sl.rblk0) * RB;
   const long long face = sl.face;
@@ -1003,61 +1155,7 @@ kb_relax(BView v, const double* Zt, const double* Yt, const double* Wtt, const d
       plane_put_block(v.xa, sl, i, ok ? a : 0.0, ok);
     }
   }
-  block_sum2<BT>(r2, o2, sh);
-  if (threadIdx.x == 0) {
-    part[2 * b] = r2;
-    part[2 * b + 1] = o2;
-    __threadfence();
-    ticket = atomicAdd(&st.tickets, 1u);
-  }
-  __syncthreads();
-  if (ticket != (unsigned)sl.nrblk - 1u) return;
-  // this block finishes the slot
-  __threadfence();
-  double rs = 0.0, os = 0.0;
-  for (int k = threadIdx.x; k < sl.nrblk; k += BT) {
-    rs += __ldcg(part + 2 * (sl.rblk0 + k));
-    os += __ldcg(part + 2 * (sl.rblk0 + k) + 1);
-  }
-  for (int k = threadIdx.x; k < sl.nblk; k += BT) os += __ldcg(part_n1 + sl.blk0 + k);
-  block_sum2<BT>(rs, os, sh);
-  if (threadIdx.x == 0) {
-    const double n = sl.n_elements;
-    const double rel = sqrt(rs / n) / fmax(sqrt(os / n), 1e-9);
-    const int it = st.iter + 1;
-    st.iter = it;
-    st.rel_err = rel;
-    if (rel < sl.tol) {
-      st.status = SGH_STEP_CONVERGED;
-      st.done = 1;
-    } else if (!isfinite(rel)) {
-      st.status = SGH_STEP_NONFINITE;
-      st.done = 1;
-    } else if (it >= sl.max_iter) {
-      st.status = SGH_STEP_CAPPED;
-      st.done = 1;
-    }
-    st.tickets = 0u;
-    const int expect = __ldcg(&v.g->n_iter_slots);  // read before the ticket: the last finisher rewrites it
-    __threadfence();
-    last = atomicAdd(&v.g->slots_done, 1u) == (unsigned)expect - 1u;
-    count = 0;
-  }
-  __syncthreads();
-  if (!last) return;
-  // the last finisher: slots iterating next, loop condition
-  __threadfence();
-  int c = 0;
-  for (int k = threadIdx.x; k < v.n; k += BT)
-    if (__ldcg(&v.st[k].active) && !__ldcg(&v.st[k].done)) ++c;
-  if (c) atomicAdd(&count, c);
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    v.g->slots_done = 0u;
-    v.g->n_iter_slots = count;
-    v.g->picard_any = count > 0;
-    if (in_graph) cudaGraphSetConditional(h_picard, count > 0 ? 1u : 0u);
-  }
+  relax_finish<BT>(v, s, b, sl.rblk0, sl.nrblk, r2, o2, part, part_n1, h_picard, in_graph, sh);
 }
 
 // ---- volume passes ----------------------------------------------------------
@@ -1104,9 +1202,12 @@ __device__ __forceinline__ void vstore(R* p, const R (&o)[VEC]) {
 // in FP32 from the FP64-derived 1-D tables, a <- K a + KK Ct sigma as two
 // FP32 products and a fused add (relative rounding a few 1e-7, the order of
 // the FP32 storage of a), and the face sums Zt, Yt and the norm partial
-// accumulated in FP64. No FP64 arithmetic or conversion sits on the per-mode
-// path except the three accumulations and the widening of their two FP32
-// inputs, so the pass stays close to its 8 bytes per mode of HBM traffic.
+// gathered per column in FP32 over groups of VOL_FLUSH z-planes, each group's
+// sum added in FP64 (a few 1e-7 relative, the order of the FP32 state). No
+// FP64 arithmetic or conversion sits on the per-mode path, so the pass stays
+// close to its 8 bytes per mode of HBM traffic. Every volume-pass variant
+// groups the planes alike, so a slot's face sums do not depend on the vector
+// width its batch runs at.
 // FP64 modes: K and KK read from the volume arenas, everything in FP64.
 template <class R, int VEC, bool COMMIT, int U>
 __global__ void __launch_bounds__(BT / VEC, (sizeof(R) == 4 ? 3 : 2) * VEC)
@@ -1131,6 +1232,7 @@ kb_volume(BView v, R* a, const R* K, const R* KK, const double* sigma, double* Z
     const double* lz = ez + 2 * nsum;
     const double dt_rc = sl.dt / (sl.rho * sl.cp);
     double zt[VEC], yt[VEC], sg[VEC];
+    float zs[VEC], ys[VEC], ns[VEC];  // FP32 partial sums over VOL_FLUSH planes (FP32 modes)
     float sg32[VEC], exy32[VEC], dxy32[VEC], lxy32[VEC];
 #pragma unroll
     for (int c = 0; c < VEC; ++c) {
@@ -1143,6 +1245,7 @@ kb_volume(BView v, R* a, const R* K, const R* KK, const double* sigma, double* Z
       lxy32[c] = TAB ? (float)(E[2 * nsum + ix] + E[2 * nsum + iy]) : 0.0f;
       zt[c] = 0.0;
       yt[c] = 0.0;
+      zs[c] = ys[c] = ns[c] = 0.0f;
     }
     // U planes per round: every load of the round is issued before its
     // arithmetic, so U x VEC values per thread are in flight
@@ -1173,14 +1276,23 @@ kb_volume(BView v, R* a, const R* K, const R* KK, const double* sigma, double* Z
               const float num = fmaf(exy32[c], dz32, dxy32[c]);
               const float den = lxy32[c] + lz32;
               const float kk = den > 0.0f ? __fdividef(num, den) : (float)dt_rc;
+              const float t = kk * cp32;
               float x = (float)av[u][c];
-              if (COMMIT) x = fmaf(x, kv, kk * (cp32 * sg32[c]));
+              if (COMMIT) x = fmaf(x, kv, t * sg32[c]);
               av[u][c] = (R)x;
               const float ak = x * kv;
-              const double ak64 = (double)ak, akk64 = (double)(ak * kk);
-              zt[c] = fma(cp, ak64, zt[c]);
-              yt[c] = fma(akk64, cp, yt[c]);
-              n1 = fma(ak64, ak64, n1);
+              zs[c] = fmaf(cp32, ak, zs[c]);
+              ys[c] = fmaf(ak, t, ys[c]);
+              ns[c] = fmaf(ak, ak, ns[c]);
+            }
+            if ((p + 1) % VOL_FLUSH == 0 || p + 1 == sl.nz) {
+#pragma unroll
+              for (int c = 0; c < VEC; ++c) {
+                zt[c] += (double)zs[c];
+                yt[c] += (double)ys[c];
+                n1 += (double)ns[c];
+                zs[c] = ys[c] = ns[c] = 0.0f;
+              }
             }
           } else {
 #pragma unroll
@@ -1215,16 +1327,18 @@ kb_volume(BView v, R* a, const R* K, const R* KK, const double* sigma, double* Z
 // columns of each z-plane (FP32 modes: 1 KB, contiguous) arrive by one bulk
 // copy per plane, completing on that stage's mbarrier, RING planes ahead of
 // the arithmetic. The bytes in flight then come from shared memory, not from
-// registers. Arithmetic and outputs are those of kb_volume's FP32 path. A copy
+// registers. Arithmetic and outputs are those of kb_volume's FP32 path (the
+// face sums per column in FP32 over groups of VOL_FLUSH planes). A copy
 // wait that expires sets the batch's error flag; the block then waits (with
 // the full bound) for its copies in flight, writes a NaN norm partial so the
 // Picard test stops, and leaves its face sums unwritten.
 template <bool COMMIT, int RING>
-__global__ void __launch_bounds__(BT / 4, 16)
+__global__ void __launch_bounds__(BT / 4, 12)
 kb_volume_ring(BView v, float* a, const double* sigma, double* Zt, double* Yt, double* part_n1) {
-  constexpr int VEC = 4, NT = BT / VEC, TABMAX = 256;
+  constexpr int VEC = 4, NT = BT / VEC;
+  static_assert(RING % 2 == 0, "planes are consumed two at a time");
   __shared__ __align__(128) float ring[RING][BT];
-  __shared__ float ztab[4][TABMAX];  // Ct, Ez, 1 - Ez, L_z of each plane in FP32 (nz <= TABMAX)
+  __shared__ float ztab[4][RING_TABMAX];  // Ct, Ez, 1 - Ez, L_z of each plane in FP32 (nz <= RING_TABMAX)
   __shared__ uint64_t full[RING];
   __shared__ double sh[2 * (NT / 32)];
   __shared__ int bad;
@@ -1239,20 +1353,17 @@ kb_volume_ring(BView v, float* a, const double* sigma, double* Zt, double* Yt, d
   const uint32_t bytes = (uint32_t)ncol * 4u;
   const int nz = sl.nz;
   float* col = a + sl.vol + base;  // plane p of the block at col + p * S (16-byte aligned)
-  const double* ct = v.Ct + sl.zoff;
-  const int nsum = sl.nx + sl.ny + sl.nz;
-  const double* E = v.E + sl.eoff;
-  const double* ez = E + sl.nx + sl.ny;
-  const double* dz = ez + nsum;
-  const double* lz = ez + 2 * nsum;
-  const bool tabbed = nz <= TABMAX;  // the per-plane constants converted once per block
-  if (tabbed)
-    for (int p = threadIdx.x; p < nz; p += NT) {
+  {
+    const double* ct = v.Ct + sl.zoff;
+    const int nsum = sl.nx + sl.ny + sl.nz;
+    const double* ez = v.E + sl.eoff + sl.nx + sl.ny;
+    for (int p = threadIdx.x; p < nz; p += NT) {  // the per-plane constants, converted once per block
       ztab[0][p] = (float)ct[p];
       ztab[1][p] = (float)ez[p];
-      ztab[2][p] = (float)dz[p];
-      ztab[3][p] = (float)lz[p];
+      ztab[2][p] = (float)ez[nsum + p];
+      ztab[3][p] = (float)ez[2 * nsum + p];
     }
+  }
   if (threadIdx.x == 0) {
     for (int k = 0; k < RING; ++k) umma::mbar_init(&full[k], 1);
     bad = 0;
@@ -1266,54 +1377,81 @@ kb_volume_ring(BView v, float* a, const double* sigma, double* Zt, double* Yt, d
   const bool live = i0 < sl.S;
   const float dt_rc = (float)(sl.dt / (sl.rho * sl.cp));
   double zt[VEC], yt[VEC], n1 = 0.0, dummy = 0.0;
+  // FP32 partial sums over VOL_FLUSH planes, added into the FP64 sums at the
+  // end of each group: three conversions per column and group instead of two
+  // per mode (conversions and the quotient's reciprocal share the XU pipe)
+  float zs[VEC], ys[VEC], ns[VEC];
   float sg32[VEC], exy32[VEC], dxy32[VEC], lxy32[VEC];
+  {
+    const double* E = v.E + sl.eoff;
+    const int nsum = sl.nx + sl.ny + sl.nz;
 #pragma unroll
-  for (int c = 0; c < VEC; ++c) {
-    const int i = live ? i0 + c : 0;
-    const int ix = i % sl.nx, iy = sl.nx + i / sl.nx;
-    sg32[c] = (COMMIT && live) ? (float)sigma[sl.face + i] : 0.0f;
-    exy32[c] = (float)(E[ix] * E[iy]);
-    dxy32[c] = (float)(E[nsum + ix] + E[ix] * E[nsum + iy]);
-    lxy32[c] = (float)(E[2 * nsum + ix] + E[2 * nsum + iy]);
-    zt[c] = 0.0;
-    yt[c] = 0.0;
+    for (int c = 0; c < VEC; ++c) {
+      const int i = live ? i0 + c : 0;
+      const int ix = i % sl.nx, iy = sl.nx + i / sl.nx;
+      sg32[c] = (COMMIT && live) ? (float)sigma[sl.face + i] : 0.0f;
+      exy32[c] = (float)(E[ix] * E[iy]);
+      dxy32[c] = (float)(E[nsum + ix] + E[ix] * E[nsum + iy]);
+      lxy32[c] = (float)(E[2 * nsum + ix] + E[2 * nsum + iy]);
+      zt[c] = 0.0;
+      yt[c] = 0.0;
+      zs[c] = ys[c] = ns[c] = 0.0f;
+    }
   }
-  const unsigned lim = v.g->wait_limit ? v.g->wait_limit : umma::WAIT_LIMIT;
-  int p = 0;
-  for (; p < nz; ++p) {
-    const int k = p % RING;
-    const bool arrived = umma::mbar_wait_bounded(&full[k], (uint32_t)((p / RING) & 1), lim);
-    if (!arrived) bad = 1;
-    if (arrived && live) {
-      const double cp = ct[p];
-      const float cp32 = tabbed ? ztab[0][p] : (float)cp, ez32 = tabbed ? ztab[1][p] : (float)ez[p];
-      const float dz32 = tabbed ? ztab[2][p] : (float)dz[p], lz32 = tabbed ? ztab[3][p] : (float)lz[p];
-      float4 x4 = *reinterpret_cast<const float4*>(&ring[k][VEC * threadIdx.x]);
-      float av[VEC] = {x4.x, x4.y, x4.z, x4.w};
+  // one z-plane of this thread's VEC columns (mode_kk's arithmetic, FP32)
+  auto plane = [&](int p, const float* src) {
+    const float cp32 = ztab[0][p], ez32 = ztab[1][p], dz32 = ztab[2][p], lz32 = ztab[3][p];
+    const float4 x4 = *reinterpret_cast<const float4*>(src + VEC * threadIdx.x);
+    float av[VEC] = {x4.x, x4.y, x4.z, x4.w};
+    const bool zero_mode = (p | i0) == 0;  // column 0 (x = y = 0), plane 0: the quotient there is 0 / 0
+#pragma unroll
+    for (int c = 0; c < VEC; ++c) {
+      float kk = __fdividef(fmaf(exy32[c], dz32, dxy32[c]), lxy32[c] + lz32);
+      if (c == 0 && zero_mode) kk = dt_rc;  // KK of the zero mode
+      const float kv = exy32[c] * ez32, t = kk * cp32;
+      float x = av[c];
+      if (COMMIT) x = fmaf(x, kv, t * sg32[c]);
+      av[c] = x;
+      const float ak = x * kv;
+      zs[c] = fmaf(cp32, ak, zs[c]);
+      ys[c] = fmaf(ak, t, ys[c]);
+      ns[c] = fmaf(ak, ak, ns[c]);
+    }
+    if (COMMIT) *reinterpret_cast<float4*>(col + (size_t)p * sl.S + VEC * threadIdx.x) =
+        make_float4(av[0], av[1], av[2], av[3]);
+    if ((p + 1) % VOL_FLUSH == 0 || p + 1 == nz) {
 #pragma unroll
       for (int c = 0; c < VEC; ++c) {
-        const float kv = exy32[c] * ez32;
-        const float num = fmaf(exy32[c], dz32, dxy32[c]);
-        const float den = lxy32[c] + lz32;
-        const float kk = den > 0.0f ? __fdividef(num, den) : dt_rc;
-        float x = av[c];
-        if (COMMIT) x = fmaf(x, kv, kk * (cp32 * sg32[c]));
-        av[c] = x;
-        const float ak = x * kv;
-        const double ak64 = (double)ak, akk64 = (double)(ak * kk);
-        zt[c] = fma(cp, ak64, zt[c]);
-        yt[c] = fma(akk64, cp, yt[c]);
-        n1 = fma(ak64, ak64, n1);
+        zt[c] += (double)zs[c];
+        yt[c] += (double)ys[c];
+        n1 += (double)ns[c];
+        zs[c] = ys[c] = ns[c] = 0.0f;
       }
-      if (COMMIT) *reinterpret_cast<float4*>(col + (size_t)p * sl.S + VEC * threadIdx.x) =
-          make_float4(av[0], av[1], av[2], av[3]);
     }
-    __syncthreads();  // stage k is consumed by every thread; `bad` is visible
+  };
+  const unsigned lim = v.g->wait_limit ? v.g->wait_limit : umma::WAIT_LIMIT;
+  // two planes per round (stages k and k + 1; RING is even): one barrier and
+  // one refill round per two planes
+  int p = 0;
+  for (; p < nz; p += 2) {
+    const int k = p % RING;
+    const bool two = p + 1 < nz;
+    bool arrived = umma::mbar_wait_bounded(&full[k], (uint32_t)((p / RING) & 1), lim);
+    if (arrived && two) arrived = umma::mbar_wait_bounded(&full[k + 1], (uint32_t)((p / RING) & 1), lim);
+    if (!arrived) bad = 1;
+    if (arrived && live) {
+      plane(p, ring[k]);
+      if (two) plane(p + 1, ring[k + 1]);
+    }
+    __syncthreads();  // stages k, k + 1 are consumed by every thread; `bad` is visible
     if (bad) break;
-    if (threadIdx.x == 0 && p + RING < nz) {
+    if (threadIdx.x == 0) {
       umma::fence_proxy_async();
-      umma::mbar_expect_tx(&full[k], bytes);
-      umma::bulk_g2s(ring[k], col + (size_t)(p + RING) * sl.S, bytes, &full[k]);
+      for (int q = 0; q < 2; ++q)
+        if (p + q + RING < nz) {
+          umma::mbar_expect_tx(&full[k + q], bytes);
+          umma::bulk_g2s(ring[k + q], col + (size_t)(p + q + RING) * sl.S, bytes, &full[k + q]);
+        }
     }
   }
   if (bad) {  // planes p .. min(nz, p + RING) - 1 were issued and not all consumed
@@ -1405,7 +1543,7 @@ struct sgh_batch {
   size_t o_slot, o_state, o_g, o_blk, o_rblk, o_tile, o_vblk, o_utile, o_mats, o_ct;
   size_t o_a, o_K, o_KK, o_E;
   long long tot_e = 0;
-  size_t o_qlas, o_qnet, o_qev, o_qevold, o_Stop, o_f1, o_sigma, o_A, o_Tsurf, o_Zt, o_Yt, o_Wtt, o_Qtt;
+  size_t o_qlas, o_qnet, o_qevold, o_Stop, o_f1, o_sigma, o_A, o_Tsurf, o_Zt, o_Yt, o_Wtt, o_Qtt;
   size_t o_plas, o_pn1, o_prelax, o_ptile;
   size_t o_xa = 0, o_xq = 0, o_mp = 0, o_x1 = 0;  // operand pair planes (mixed)
   size_t xa_bytes = 0, mp_bytes = 0, x1_bytes = 0;
@@ -1496,7 +1634,9 @@ void launch_volume(sgh_batch* B, cudaStream_t s, R* a, const R* K, const R* KK) 
     else go(vec, std::integral_constant<int, 4>{});
   };
   if constexpr (sizeof(R) == 4) {
-    if (B->vec == 4) {  // the ring form: 2 U planes of each block in flight
+    int max_nz = 0;
+    for (const BSlot& sl : B->slots) max_nz = std::max(max_nz, sl.nz);
+    if (B->vec == 4 && max_nz <= RING_TABMAX) {  // the ring form: 2 U planes of each block in flight
       float* af = reinterpret_cast<float*>(a);
       const int u = B->vol_unroll;
       if (u == 2) kb_volume_ring<COMMIT, 4><<<B->tot_blk, BT / 4, 0, s>>>(v, af, sg, zt, yt, pn);
@@ -1505,7 +1645,7 @@ void launch_volume(sgh_batch* B, cudaStream_t s, R* a, const R* K, const R* KK) 
       return;
     }
   }
-  if (B->vec == 2) with_u(std::integral_constant<int, 2>{});
+  if (B->vec >= 2) with_u(std::integral_constant<int, 2>{});  // vec 4 with nz > RING_TABMAX: float2
   else with_u(std::integral_constant<int, 1>{});
 }
 
@@ -1516,7 +1656,10 @@ void enqueue_pre(sgh_batch* B, cudaStream_t s, cudaGraphConditionalHandle h, int
   R* K = B->precision == SGH_PRECISION_MIXED ? nullptr : reinterpret_cast<R*>(B->ws + B->o_K);
   R* KK = B->precision == SGH_PRECISION_MIXED ? nullptr : reinterpret_cast<R*>(B->ws + B->o_KK);
   kb_begin<<<1, CT, 0, s>>>(v, h, in_graph);
-  kb_face_begin<<<B->tot_rblk, BT, 0, s>>>(v, B->d(B->o_qlas), B->d(B->o_qnet), B->d(B->o_qevold), B->d(B->o_plas));
+  // mixed precision: q_net goes only into the operand plane of the transform
+  kb_face_begin<<<B->tot_rblk, BT, 0, s>>>(v, B->d(B->o_qlas),
+                                           B->precision == SGH_PRECISION_MIXED ? nullptr : B->d(B->o_qnet),
+                                           B->d(B->o_qevold), B->d(B->o_plas));
   launch_volume<R, false>(B, s, a, K, KK);
   g_blaunch += 3;
   // initial guess: sigma = dct_scale * DCT2(q_las - shift(q_evap_old)), then A = Zt + W_tt sigma
@@ -1535,13 +1678,18 @@ void enqueue_picard(sgh_batch* B, cudaStream_t s, cudaGraphConditionalHandle h, 
   const BView v = B->view();
   const bool mixed = B->precision == SGH_PRECISION_MIXED;
   // T_s = IDCT2(A) -> evaporation -> q_net; S_top = dct_scale * DCT2(q_net)
-  face2d<true, true, F2_TOPFLUX>(B, s, B->d(B->o_A), EB_TopFlux{B->d(B->o_qlas), B->d(B->o_qev), B->d(B->o_qnet)},
-                                 F2Args{B->d(B->o_qev), nullptr, B->d(B->o_qlas), 0}, nullptr);
+  face2d<true, true, F2_TOPFLUX>(B, s, B->d(B->o_A), EB_TopFlux{B->d(B->o_qlas), B->d(B->o_qevold), B->d(B->o_qnet)},
+                                 F2Args{B->d(B->o_qevold), nullptr, B->d(B->o_qlas), 0}, nullptr);
+  if (mixed) {  // S_top straight into the relaxation and the convergence test (one launch less)
+    F2Args fa{B->d(B->o_sigma), nullptr, B->d(B->o_Zt), 1, B->d(B->o_Wtt), B->d(B->o_Yt), B->d(B->o_Qtt),
+              B->d(B->o_pn1), B->d(B->o_prelax), h, in_graph};
+    face2d<false, true, F2_RELAX>(B, s, B->d(B->o_qnet), EB_Store{B->d(B->o_Stop), 1}, fa, nullptr);
+    return;
+  }
   face2d<false, true, F2_STORE>(B, s, B->d(B->o_qnet), EB_Store{B->d(B->o_Stop), 1},
                                 F2Args{B->d(B->o_Stop), nullptr, nullptr, 1}, nullptr);
-  // mixed precision keeps A only as the xa operand plane
   kb_relax<<<B->tot_rblk, BT, 0, s>>>(v, B->d(B->o_Zt), B->d(B->o_Yt), B->d(B->o_Wtt), B->d(B->o_Qtt),
-                                     B->d(B->o_Stop), B->d(B->o_sigma), mixed ? nullptr : B->d(B->o_A),
+                                     B->d(B->o_Stop), B->d(B->o_sigma), B->d(B->o_A),
                                      B->d(B->o_prelax), B->d(B->o_pn1), h, in_graph);
   g_blaunch += 1;
 }
@@ -1553,8 +1701,8 @@ void enqueue_post(sgh_batch* B, cudaStream_t s, cudaGraphConditionalHandle h, in
   R* K = B->precision == SGH_PRECISION_MIXED ? nullptr : reinterpret_cast<R*>(B->ws + B->o_K);
   R* KK = B->precision == SGH_PRECISION_MIXED ? nullptr : reinterpret_cast<R*>(B->ws + B->o_KK);
   face2d<true, false, F2_COMMIT>(B, s, B->d(B->o_A),
-                                 EB_CommitSurface{B->d(B->o_Tsurf), B->d(B->o_qev), B->d(B->o_qevold)},
-                                 F2Args{B->d(B->o_Tsurf), B->d(B->o_qevold), B->d(B->o_qev), 0}, B->d(B->o_ptile));
+                                 EB_CommitSurface{B->d(B->o_Tsurf)},
+                                 F2Args{B->d(B->o_Tsurf), nullptr, nullptr, 0}, B->d(B->o_ptile));
   launch_volume<R, true>(B, s, a, K, KK);
   kb_commit<<<1, CT, 0, s>>>(v, B->d(B->o_plas), B->d(B->o_ptile),
                              B->precision == SGH_PRECISION_MIXED ? 1 : 0, h, in_graph);
@@ -1696,15 +1844,12 @@ int sgh_batch_create(const sgh_config* cfgs, int32_t n, int32_t precision, sgh_b
     sl.eoff = (int)B->tot_e;
     sl.mx = (int)mats[c.nx];
     sl.my = (int)mats[c.ny];
-    sl.blk0 = B->tot_blk;
     sl.nblk = cdivl(sl.S, BT);
     sl.rblk0 = B->tot_rblk;
     sl.nrblk = cdivl(sl.S, RB);
-    sl.tile0 = B->tot_tile;
     sl.ntile = face_tiles(c.nx, c.ny);
     sl.vblk0 = B->tot_vblk;
     sl.nvblk = cdivl(sl.V, BT);
-    sl.utile0 = B->tot_utile;
     sl.nutile = face_utiles(c.nx, c.ny);
     if (precision == SGH_PRECISION_MIXED) {
       sl.xa = (long long)B->xa_bytes;
@@ -1741,16 +1886,40 @@ int sgh_batch_create(const sgh_config* cfgs, int32_t n, int32_t precision, sgh_b
     B->tot_face += sl.S;
     B->tot_z += c.nz;
     B->tot_e += 3 * (c.nx + c.ny + c.nz);  // E, 1 - E and kbar k^2 per axis
-    B->tot_blk += sl.nblk;
     B->tot_rblk += sl.nrblk;
-    B->tot_tile += sl.ntile;
     B->tot_vblk += sl.nvblk;
-    B->tot_utile += sl.nutile;
-    B->blk_slot.insert(B->blk_slot.end(), sl.nblk, i);
     B->rblk_slot.insert(B->rblk_slot.end(), sl.nrblk, i);
-    B->tile_slot.insert(B->tile_slot.end(), sl.ntile, i);
     B->vblk_slot.insert(B->vblk_slot.end(), sl.nvblk, i);
-    B->utile_slot.insert(B->utile_slot.end(), sl.nutile, i);
+  }
+  // Column blocks and face tiles: the slots with the longest blocks take the
+  // first block indices of a launch (a column block runs over nz planes, a face
+  // tile over nx / 32 or ny / 32 chunks), so that a launch's last wave holds
+  // its shortest blocks. Every slot keeps one contiguous range, and per-slot
+  // partials are summed over it in a fixed order: a slot's results do not
+  // depend on this order.
+  {
+    std::vector<int> by_z(n), by_face(n);
+    for (int i = 0; i < n; ++i) by_z[i] = by_face[i] = i;
+    const std::vector<BSlot>& S = B->slots;
+    std::stable_sort(by_z.begin(), by_z.end(), [&](int a, int b) { return S[a].nz > S[b].nz; });
+    std::stable_sort(by_face.begin(), by_face.end(), [&](int a, int b) {
+      return S[a].nx != S[b].nx ? S[a].nx > S[b].nx : S[a].ny > S[b].ny;
+    });
+    for (int i : by_z) {
+      BSlot& sl = B->slots[i];
+      sl.blk0 = B->tot_blk;
+      B->tot_blk += sl.nblk;
+      B->blk_slot.insert(B->blk_slot.end(), sl.nblk, i);
+    }
+    for (int i : by_face) {
+      BSlot& sl = B->slots[i];
+      sl.tile0 = B->tot_tile;
+      sl.utile0 = B->tot_utile;
+      B->tot_tile += sl.ntile;
+      B->tot_utile += sl.nutile;
+      B->tile_slot.insert(B->tile_slot.end(), sl.ntile, i);
+      B->utile_slot.insert(B->utile_slot.end(), sl.nutile, i);
+    }
   }
   {
     const int vw = precision == SGH_PRECISION_MIXED ? 4 : 2;
@@ -1776,10 +1945,9 @@ int sgh_batch_create(const sgh_config* cfgs, int32_t n, int32_t precision, sgh_b
   B->o_KK = L.take(precision == SGH_PRECISION_MIXED ? 0 : VE);  // mixed: KK from the 1-D tables
   B->o_E = L.take(sizeof(double) * (size_t)B->tot_e);
   B->o_qlas = L.take(F8);
-  B->o_qnet = L.take(F8);
-  B->o_qev = L.take(F8);
+  B->o_qnet = L.take(precision == SGH_PRECISION_MIXED ? 0 : F8);  // mixed: the xq operand plane only
   B->o_qevold = L.take(F8);
-  B->o_Stop = L.take(F8);
+  B->o_Stop = L.take(precision == SGH_PRECISION_MIXED ? 0 : F8);  // mixed: S_top stays in the transform
   B->o_f1 = L.take(F8);
   B->o_sigma = L.take(F8);
   B->o_A = L.take(F8);
@@ -1790,7 +1958,7 @@ int sgh_batch_create(const sgh_config* cfgs, int32_t n, int32_t precision, sgh_b
   B->o_Qtt = L.take(F8);
   B->o_plas = L.take(sizeof(double) * B->tot_blk);
   B->o_pn1 = L.take(sizeof(double) * B->tot_blk);
-  B->o_prelax = L.take(sizeof(double) * 2 * B->tot_blk);
+  B->o_prelax = L.take(sizeof(double) * 2 * std::max(B->tot_rblk, B->tot_utile));  // per relaxation block or tile
   B->o_ptile = L.take(sizeof(double) * std::max(B->tot_tile, B->tot_utile));
   if (precision == SGH_PRECISION_MIXED) {
     B->o_xa = L.take(B->xa_bytes);
@@ -1858,7 +2026,6 @@ int sgh_batch_bind(sgh_batch* B, void* workspace, uint64_t bytes, void* stream) 
   SGB_CK(put(B->o_vblk, B->vblk_slot));
   SGB_CK(put(B->o_utile, B->utile_slot));
   SGB_CK(cudaMemsetAsync(B->ws + B->o_qevold, 0, sizeof(double) * B->tot_face, s));
-  SGB_CK(cudaMemsetAsync(B->ws + B->o_qev, 0, sizeof(double) * B->tot_face, s));
   for (auto& m : B->mat_list)
     kb_dct_matrix<<<cdivl((long long)m.first * m.first, BT), BT, 0, s>>>(m.first, B->d(B->o_mats) + m.second);
   const BView v = B->view();
@@ -1907,11 +2074,11 @@ int sgh_batch_slot_start(sgh_batch* B, int32_t slot, const sgh_laser* lasers_dev
   const int g = cdivl(std::max<long long>(sl.V, sl.S), BT);
   if (B->precision == SGH_PRECISION_MIXED)
     kb_slot_start<float><<<g, BT, 0, s>>>(B->view(), slot, reinterpret_cast<float*>(B->ws + B->o_a),
-                                          B->d(B->o_qevold), B->d(B->o_qev), B->d(B->o_sigma), lasers_dev,
+                                          B->d(B->o_qevold), B->d(B->o_sigma), lasers_dev,
                                           n_steps, outs_dev);
   else
-    kb_slot_start<double><<<g, BT, 0, s>>>(B->view(), slot, B->d(B->o_a), B->d(B->o_qevold), B->d(B->o_qev),
-                                           B->d(B->o_sigma), lasers_dev, n_steps, outs_dev);
+    kb_slot_start<double><<<g, BT, 0, s>>>(B->view(), slot, B->d(B->o_a), B->d(B->o_qevold), B->d(B->o_sigma),
+                                           lasers_dev, n_steps, outs_dev);
   SGB_CK(cudaGetLastError());
   return SGH_OK;
 }
