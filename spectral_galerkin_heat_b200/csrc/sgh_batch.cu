@@ -1948,9 +1948,9 @@ int sgh_batch_create(const sgh_config* cfgs, int32_t n, int32_t precision, sgh_b
   B->o_qnet = L.take(precision == SGH_PRECISION_MIXED ? 0 : F8);  // mixed: the xq operand plane only
   B->o_qevold = L.take(F8);
   B->o_Stop = L.take(precision == SGH_PRECISION_MIXED ? 0 : F8);  // mixed: S_top stays in the transform
-  B->o_f1 = L.take(F8);
+  B->o_f1 = L.take(precision == SGH_PRECISION_MIXED ? 0 : F8);  // the FP64 transforms' intermediate
   B->o_sigma = L.take(F8);
-  B->o_A = L.take(F8);
+  B->o_A = L.take(precision == SGH_PRECISION_MIXED ? 0 : F8);  // mixed: A only as the xa operand plane
   B->o_Tsurf = L.take(F8);
   B->o_Zt = L.take(F8);
   B->o_Yt = L.take(F8);
