@@ -5,7 +5,7 @@ requests of uneven size (grids 64x32x16 .. 512x256x64 on the 2 x 1 x 0.5 mm
 316L cuboid, straight-track physics = one forcing pass per step, 200-2000
 steps of 5 us, random power and speed) served by the continuous-batching
 engine in mixed precision (FP32 modal state, split-BF16 tensor-core face
-transforms, FP64 faces, norms and coefficient tables).
+transforms, FP64 face fields, norms and coefficient tables, FP32 face sums).
 
 * ``value``: timesteps/s of the engine on a saturated queue of that mix: all
   requests queued, slots sized from free HBM, K batched steps timed with CUDA
@@ -775,8 +775,8 @@ def run_serving(args, rank, world, local_rank):
     torch.cuda.synchronize()
     vp_ms = sum(a.elapsed_time(b) for a, b in kev) / R
     # per mode: read a (4 B), write a (4 B) -- K and KK are formed from 1-D
-    # tables in registers; per column: sigma in, Zt, Yt out (8 B each)
-    vp_bytes = 8 * modes + 24 * faces
+    # tables in registers; per column: sigma in (8 B), Zt, Yt out (FP32, 4 B each)
+    vp_bytes = 8 * modes + 16 * faces
     eng.reset()
     # latency: Poisson arrivals in real time, host inputs
     lat_reqs = _serving_requests(poisson, templates)
@@ -1034,8 +1034,9 @@ def run_batch(args, rank, world, local_rank):
             torch.cuda.synchronize()
             faces = sum(int(c.num.nx) * int(c.num.ny) for c in ctxs)
             out["vp_ms"] = sum(a.elapsed_time(c) for a, c in kev) / R
-            # mixed: a in, a out per mode (K, KK from 1-D tables); FP64: a, K, KK in, a out
-            out["vp_bytes"] = (8 if prec == "mixed" else 32) * modes + 24 * faces
+            # mixed: a in, a out per mode (K, KK from 1-D tables), sigma in and the
+            # FP32 face sums out per column; FP64: a, K, KK in, a out, FP64 face sums
+            out["vp_bytes"] = (8 * modes + 16 * faces) if prec == "mixed" else (32 * modes + 24 * faces)
             out["modes"] = modes
         b.close()
         return out

@@ -9,8 +9,9 @@ its face-space form, so the supported physics is laser + evaporation without
 convection, latent heat or a T-dependent model.
 
 ``precision="fp64"`` keeps the modes and K/KK in FP64; ``precision="mixed"``
-stores them in FP32 (computed in FP64 and rounded once) with FP64 faces and
-norms, halving the bytes each step moves.
+stores the modes in FP32 (K and KK formed from FP64 1-D tables), with FP64 face
+fields (fluxes, sigma, surface) and norms and FP32 face sums and weights,
+moving a third of the bytes per step.
 """
 from __future__ import annotations
 

@@ -18,9 +18,9 @@
 //
 // Volume state is FP64 modes with stored K and KK (plain), or FP32 modes only
 // (mixed: K and KK formed in registers from per-axis FP64 tables, the mode
-// update in FP32). Faces, face sums and norms are FP64 in both; in mixed
-// precision the face transforms run on the tensor cores from split-BF16
-// operand planes.
+// update in FP32). Face fields and norms are FP64 in both; the face sums and
+// weights (Zt, Yt, W_tt, Q_tt) are FP32 in mixed batches, where the face
+// transforms run on the tensor cores from split-BF16 operand planes.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -246,7 +246,7 @@ __global__ void __launch_bounds__(BT) kb_tables(BView v, R* K, R* KK, double* Ct
 
 // Face weights from the stored KK: W_tt = sum Ct^2 KK, Q_tt = sum (KK Ct)^2.
 template <class R>
-__global__ void __launch_bounds__(BT) kb_weights(BView v, const R* KK, double* Wtt, double* Qtt) {
+__global__ void __launch_bounds__(BT) kb_weights(BView v, const R* KK, R* Wtt, R* Qtt) {
   const int b = blockIdx.x;
   const int s = v.blk_slot[b];
   const BSlot& sl = v.slot[s];
@@ -269,8 +269,8 @@ __global__ void __launch_bounds__(BT) kb_weights(BView v, const R* KK, double* W
     w += ct * ct * kk;
     q += (kk * ct) * (kk * ct);
   }
-  Wtt[sl.face + i] = w;
-  Qtt[sl.face + i] = q;
+  Wtt[sl.face + i] = (R)w;
+  Qtt[sl.face + i] = (R)q;
 }
 
 // (Re)start one slot at the initial condition (solvers/spectral.py:176-180).
@@ -657,12 +657,13 @@ struct F2Args {
   double* out;        // F2_STORE target, F2_TOPFLUX q_evap (into the q_evap_old array), F2_COMMIT T_surf,
                       // F2_SIGMA and F2_RELAX sigma
   double* out2;       // unused
-  const double* in2;  // F2_TOPFLUX q_las, F2_SIGMA and F2_RELAX Zt
+  const double* in2;  // F2_TOPFLUX q_las
   int scaled;
-  const double* in3;  // F2_SIGMA and F2_RELAX W_tt
+  const float* Zt;    // F2_SIGMA and F2_RELAX: the face sums and weights (FP32 in mixed batches)
+  const float* Wtt;
   // F2_RELAX only
-  const double* Yt;
-  const double* Qtt;
+  const float* Yt;
+  const float* Qtt;
   const double* part_n1;  // volume-pass norm partials
   double* part;           // relaxation partials, 2 per tile
   cudaGraphConditionalHandle h_picard;
@@ -962,10 +963,10 @@ __global__ void __launch_bounds__(f2::THREADS, f2::CTAS) kb_fy(BView v, F2Args a
           const bool in = y < ny && x < nx;
           const long long j = fp.face + (long long)y * nx + x;
           sg[u] = in ? args.out[j] : 0.0;
-          q[u] = in ? __ldg(args.Qtt + j) : 0.0;
-          yt[u] = in ? __ldg(args.Yt + j) : 0.0;
-          zt[u] = in ? __ldg(args.in2 + j) : 0.0;
-          wt[u] = in ? __ldg(args.in3 + j) : 0.0;
+          q[u] = in ? (double)__ldg(args.Qtt + j) : 0.0;
+          yt[u] = in ? (double)__ldg(args.Yt + j) : 0.0;
+          zt[u] = in ? (double)__ldg(args.Zt + j) : 0.0;
+          wt[u] = in ? (double)__ldg(args.Wtt + j) : 0.0;
         }
 #pragma unroll
         for (int u = 0; u < U; ++u) {
@@ -995,8 +996,8 @@ __global__ void __launch_bounds__(f2::THREADS, f2::CTAS) kb_fy(BView v, F2Args a
           const int y = r0 + e / NB, x = c0 + e % NB;
           const bool in = y < ny && x < nx;
           const long long j = fp.face + (long long)y * nx + x;
-          zt[u] = in ? __ldg(args.in2 + j) : 0.0;
-          wt[u] = in ? __ldg(args.in3 + j) : 0.0;
+          zt[u] = in ? (double)__ldg(args.Zt + j) : 0.0;
+          wt[u] = in ? (double)__ldg(args.Wtt + j) : 0.0;
         }
 #pragma unroll
         for (int u = 0; u < U; ++u) {
@@ -1211,7 +1212,7 @@ __device__ __forceinline__ void vstore(R* p, const R (&o)[VEC]) {
 // FP64 modes: K and KK read from the volume arenas, everything in FP64.
 template <class R, int VEC, bool COMMIT, int U>
 __global__ void __launch_bounds__(BT / VEC, (sizeof(R) == 4 ? 3 : 2) * VEC)
-kb_volume(BView v, R* a, const R* K, const R* KK, const double* sigma, double* Zt, double* Yt,
+kb_volume(BView v, R* a, const R* K, const R* KK, const double* sigma, R* Zt, R* Yt,
           double* part_n1) {
   constexpr bool TAB = sizeof(R) == 4;
   constexpr int NT = BT / VEC;
@@ -1312,8 +1313,8 @@ kb_volume(BView v, R* a, const R* K, const R* KK, const double* sigma, double* Z
     }
 #pragma unroll
     for (int c = 0; c < VEC; ++c) {
-      Zt[sl.face + i0 + c] = zt[c];
-      Yt[sl.face + i0 + c] = yt[c];
+      Zt[sl.face + i0 + c] = (R)zt[c];
+      Yt[sl.face + i0 + c] = (R)yt[c];
     }
   }
   block_sum2<NT>(n1, dummy, sh);
@@ -1334,7 +1335,7 @@ kb_volume(BView v, R* a, const R* K, const R* KK, const double* sigma, double* Z
 // Picard test stops, and leaves its face sums unwritten.
 template <bool COMMIT, int RING>
 __global__ void __launch_bounds__(BT / 4, 12)
-kb_volume_ring(BView v, float* a, const double* sigma, double* Zt, double* Yt, double* part_n1) {
+kb_volume_ring(BView v, float* a, const double* sigma, float* Zt, float* Yt, double* part_n1) {
   constexpr int VEC = 4, NT = BT / VEC;
   static_assert(RING % 2 == 0, "planes are consumed two at a time");
   __shared__ __align__(128) float ring[RING][BT];
@@ -1466,8 +1467,8 @@ kb_volume_ring(BView v, float* a, const double* sigma, double* Zt, double* Yt, d
   if (live) {
 #pragma unroll
     for (int c = 0; c < VEC; ++c) {
-      Zt[sl.face + i0 + c] = zt[c];
-      Yt[sl.face + i0 + c] = yt[c];
+      Zt[sl.face + i0 + c] = (float)zt[c];
+      Yt[sl.face + i0 + c] = (float)yt[c];
     }
   }
   block_sum2<NT>(n1, dummy, sh);
@@ -1560,6 +1561,7 @@ struct sgh_batch {
 
   size_t elem() const { return precision == SGH_PRECISION_MIXED ? sizeof(float) : sizeof(double); }
   double* d(size_t off) const { return reinterpret_cast<double*>(ws + off); }
+  float* f(size_t off) const { return reinterpret_cast<float*>(ws + off); }
   BView view() const {
     BView v;
     v.slot = reinterpret_cast<const BSlot*>(ws + o_slot);
@@ -1622,7 +1624,9 @@ void face2d(sgh_batch* B, cudaStream_t s, const double* in, const EpiF& ef, cons
 template <class R, bool COMMIT>
 void launch_volume(sgh_batch* B, cudaStream_t s, R* a, const R* K, const R* KK) {
   const BView v = B->view();
-  double *sg = B->d(B->o_sigma), *zt = B->d(B->o_Zt), *yt = B->d(B->o_Yt), *pn = B->d(B->o_pn1);
+  double *sg = B->d(B->o_sigma), *pn = B->d(B->o_pn1);
+  R* zt = reinterpret_cast<R*>(B->ws + B->o_Zt);  // face sums in the modes' type
+  R* yt = reinterpret_cast<R*>(B->ws + B->o_Yt);
   auto go = [&](auto vec, auto u) {
     constexpr int V_ = decltype(vec)::value, U_ = decltype(u)::value;
     kb_volume<R, V_, COMMIT, U_><<<B->tot_blk, BT / V_, 0, s>>>(v, a, K, KK, sg, zt, yt, pn);
@@ -1665,7 +1669,8 @@ void enqueue_pre(sgh_batch* B, cudaStream_t s, cudaGraphConditionalHandle h, int
   // initial guess: sigma = dct_scale * DCT2(q_las - shift(q_evap_old)), then A = Zt + W_tt sigma
   if (B->precision == SGH_PRECISION_MIXED) {
     face2d<false, false, F2_SIGMA>(B, s, B->d(B->o_qnet), EB_Store{B->d(B->o_sigma), 1},
-                                   F2Args{B->d(B->o_sigma), nullptr, B->d(B->o_Zt), 1, B->d(B->o_Wtt)}, nullptr);
+                                   F2Args{B->d(B->o_sigma), nullptr, nullptr, 1, B->f(B->o_Zt), B->f(B->o_Wtt)},
+                                   nullptr);
   } else {
     face2d<false, false, F2_STORE>(B, s, B->d(B->o_qnet), EB_Store{B->d(B->o_sigma), 1},
                                    F2Args{B->d(B->o_sigma), nullptr, nullptr, 1, nullptr}, nullptr);
@@ -1681,7 +1686,7 @@ void enqueue_picard(sgh_batch* B, cudaStream_t s, cudaGraphConditionalHandle h, 
   face2d<true, true, F2_TOPFLUX>(B, s, B->d(B->o_A), EB_TopFlux{B->d(B->o_qlas), B->d(B->o_qevold), B->d(B->o_qnet)},
                                  F2Args{B->d(B->o_qevold), nullptr, B->d(B->o_qlas), 0}, nullptr);
   if (mixed) {  // S_top straight into the relaxation and the convergence test (one launch less)
-    F2Args fa{B->d(B->o_sigma), nullptr, B->d(B->o_Zt), 1, B->d(B->o_Wtt), B->d(B->o_Yt), B->d(B->o_Qtt),
+    F2Args fa{B->d(B->o_sigma), nullptr, nullptr, 1, B->f(B->o_Zt), B->f(B->o_Wtt), B->f(B->o_Yt), B->f(B->o_Qtt),
               B->d(B->o_pn1), B->d(B->o_prelax), h, in_graph};
     face2d<false, true, F2_RELAX>(B, s, B->d(B->o_qnet), EB_Store{B->d(B->o_Stop), 1}, fa, nullptr);
     return;
@@ -1952,10 +1957,14 @@ int sgh_batch_create(const sgh_config* cfgs, int32_t n, int32_t precision, sgh_b
   B->o_sigma = L.take(F8);
   B->o_A = L.take(precision == SGH_PRECISION_MIXED ? 0 : F8);  // mixed: A only as the xa operand plane
   B->o_Tsurf = L.take(F8);
-  B->o_Zt = L.take(F8);
-  B->o_Yt = L.take(F8);
-  B->o_Wtt = L.take(F8);
-  B->o_Qtt = L.take(F8);
+  // face sums and weights in the modes' type: FP32 in mixed batches (their
+  // rounding, 6e-8 relative, sits far below the BF16 split of the transform
+  // operands they feed), FP64 otherwise
+  const size_t FR = precision == SGH_PRECISION_MIXED ? sizeof(float) * (size_t)B->tot_face : F8;
+  B->o_Zt = L.take(FR);
+  B->o_Yt = L.take(FR);
+  B->o_Wtt = L.take(FR);
+  B->o_Qtt = L.take(FR);
   B->o_plas = L.take(sizeof(double) * B->tot_blk);
   B->o_pn1 = L.take(sizeof(double) * B->tot_blk);
   B->o_prelax = L.take(sizeof(double) * 2 * std::max(B->tot_rblk, B->tot_utile));  // per relaxation block or tile
@@ -2047,7 +2056,7 @@ int sgh_batch_bind(sgh_batch* B, void* workspace, uint64_t bytes, void* stream) 
       }
     }
     kb_tables<float><<<B->tot_vblk, BT, 0, s>>>(v, nullptr, nullptr, B->d(B->o_ct), B->d(B->o_E));
-    kb_weights<float><<<B->tot_blk, BT, 0, s>>>(v, nullptr, B->d(B->o_Wtt), B->d(B->o_Qtt));
+    kb_weights<float><<<B->tot_blk, BT, 0, s>>>(v, nullptr, B->f(B->o_Wtt), B->f(B->o_Qtt));
   } else {
     double* K = B->d(B->o_K);
     double* KK = B->d(B->o_KK);

@@ -5,8 +5,8 @@ For one configuration and laser path this runs, side by side on the device:
 * ``fp64``: the plain single-instance solver (:class:`B200SpectralSolver`),
   which matches the reference to 1e-10 relative L2;
 * ``mixed``: the mixed-precision form (a batch of one slot: FP32 modal state,
-  split-BF16 tensor-core face transforms with FP32 accumulation, FP64 faces,
-  norms and coefficient tables);
+  split-BF16 tensor-core face transforms with FP32 accumulation, FP64 face
+  fields, norms and coefficient tables, FP32 face sums and weights);
 * ``fp32``: the single-instance plan with every contraction in FP32
   arithmetic on the CUDA cores and the modal iterates in FP32 (FP64 faces,
   norms and tables), the plain FP32 arm against which the split-BF16
