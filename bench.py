@@ -61,12 +61,11 @@ import numpy as np  # noqa: E402
 
 METRIC = "timesteps/s"
 L2_FLUSH_BYTES = 256 << 20
-# dram__bytes_read.sum + dram__bytes_write.sum of the dominant kernel from ncu
-# captures (one launch): the serving volume pass at the benchmark's size (288
-# slots, 467,927,040 active modes) moved 4.034 GB (dram__bytes.sum.per_second
-# 5.963 TB/s x gpu__time_duration.sum 676.6 us, --cache-control none); traffic
-# scales with the modes of the same class mix.
-NCU_VOLUME_TRAFFIC_PER_MODE = 4.034e9 / 467927040
+# dram__bytes_read.sum + dram__bytes_write.sum of the dominant kernel from an
+# ncu capture of one launch: the serving volume pass at the benchmark's size
+# (288 slots, 467,927,040 active modes) read 1.976 GB and wrote 1.968 GB
+# (--cache-control none); traffic scales with the modes of the same class mix.
+NCU_VOLUME_TRAFFIC_PER_MODE = (1975895808 + 1967578624) / 467927040
 # the raster workload's dominant kernel (k_axis) was captured on the same
 # 128x64x32 case: 2.14 MB for one contiguous-axis pass (field resident in L2)
 NCU_TRAFFIC_BYTES = 2.14e6

@@ -164,6 +164,37 @@ def test_odd_shapes_mixed_batch_vs_oracle_and_alone():
     mix.close()
 
 
+def test_deep_slot_moves_the_mixed_volume_pass_off_the_ring_form_results_unchanged():
+    """A slot deeper than the ring-staged volume pass's per-plane table (nz >
+    256) moves its whole mixed batch to the float2 register form of the
+    volume pass. Every variant groups the z-planes of the face sums alike, so
+    the other slot's result is bit for bit that of the same slot alone (ring
+    form), and the deep slot stays within 1e-4 of the FP64 oracle."""
+    from oracle.sgh_oracle import OracleSolver
+    from spectral_galerkin_heat_b200.batch import BatchSolver
+    steps = 6
+    ctxs = [_ctx(16, 8, 264, seed=41, steps=steps), _ctx(32, 16, 24, seed=42, steps=steps)]
+    for c in ctxs:
+        c.num.picard_tol = 1e-8
+        c.num.max_picard_iter = 300
+    mix = BatchSolver(ctxs, "mixed")
+    for i in range(2):
+        mix.start(i, steps)
+    mix.step(steps)
+    assert mix.tensor_core_error() == 0
+    alone = BatchSolver([ctxs[1]], "mixed")
+    alone.start(0, steps)
+    alone.step(steps)
+    assert np.array_equal(alone.modes(0).cpu().numpy(), mix.modes(1).cpu().numpy())
+    o = OracleSolver(ctxs[0])
+    o.initialize()
+    for k in range(steps):
+        o.step(k * ctxs[0].num.dt, ctxs[0].num.dt)
+    assert rel_l2(mix.modes(0).double().cpu().numpy(), o.a) < 1e-4
+    alone.close()
+    mix.close()
+
+
 def test_mixed_batch_tall_faces_vs_oracle():
     """ny = 300 and nx = 72: three 128-row tiles per column block, the last
     one ragged, and a ragged second column block, in both face passes."""
