@@ -987,7 +987,9 @@ __global__ void __launch_bounds__(f2::THREADS, f2::CTAS) kb_fy(BView v, F2Args a
         }
       }
     } else if (KIND == F2_SIGMA) {
-      constexpr int U = 8;
+      // 4 elements per round: at 8 the epilogue spilled at the 80-register
+      // cap of three CTAs per SM, and the serving step measured 1.2% slower
+      constexpr int U = 4;
       for (int it0 = 0; it0 < ITEMS; it0 += U) {
         double zt[U], wt[U];
 #pragma unroll
