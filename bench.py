@@ -644,6 +644,16 @@ def _mix_rate(rates, shares):
     return 1.0 / sum(sh / rates[c] for c, sh in shares.items())
 
 
+def _volume_pass_bytes(modes, faces, precision):
+    """Algorithmic bytes of one batch volume pass (the modal commit fused with
+    the next step's face sums). Mixed: a in and out (FP32; K and KK formed from
+    1-D tables), per face column sigma in (FP64) and Zt, Yt out (FP32). FP64:
+    a, K, KK in and a out, sigma in and Zt, Yt out, all FP64."""
+    if precision == "mixed":
+        return 8 * modes + 16 * faces
+    return 32 * modes + 24 * faces
+
+
 def _demand_shares(stream):
     """Per-class share of the timesteps the stream asks for."""
     d = {}
@@ -773,9 +783,7 @@ def run_serving(args, rank, world, local_rank):
             kev[i - 2][1].record(eng.batch.stream)
     torch.cuda.synchronize()
     vp_ms = sum(a.elapsed_time(b) for a, b in kev) / R
-    # per mode: read a (4 B), write a (4 B) -- K and KK are formed from 1-D
-    # tables in registers; per column: sigma in (8 B), Zt, Yt out (FP32, 4 B each)
-    vp_bytes = 8 * modes + 16 * faces
+    vp_bytes = _volume_pass_bytes(modes, faces, "mixed")
     eng.reset()
     # latency: Poisson arrivals in real time, host inputs
     lat_reqs = _serving_requests(poisson, templates)
@@ -1033,9 +1041,7 @@ def run_batch(args, rank, world, local_rank):
             torch.cuda.synchronize()
             faces = sum(int(c.num.nx) * int(c.num.ny) for c in ctxs)
             out["vp_ms"] = sum(a.elapsed_time(c) for a, c in kev) / R
-            # mixed: a in, a out per mode (K, KK from 1-D tables), sigma in and the
-            # FP32 face sums out per column; FP64: a, K, KK in, a out, FP64 face sums
-            out["vp_bytes"] = (8 * modes + 16 * faces) if prec == "mixed" else (32 * modes + 24 * faces)
+            out["vp_bytes"] = _volume_pass_bytes(modes, faces, prec)
             out["modes"] = modes
         b.close()
         return out
